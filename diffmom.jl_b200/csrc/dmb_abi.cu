@@ -1,0 +1,363 @@
+// dmb_abi.cu -- extern "C" entry points of libdiffmom_b200.
+//
+// Each entry point validates its arguments with the reference's fail-closed
+// rules, takes the context mutex, runs the device path and maps exceptions to
+// status codes.  Host buffers are copied through pinned staging.
+#include <cmath>
+#include <cstring>
+
+#include "dmb_device.cuh"
+#include "dmb_internal.h"
+
+namespace {
+
+template <class F> dmb_status guarded(dmb_ctx *c, F &&f) {
+  if (!c) return DMB_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  try {
+    cudaSetDevice(c->device);
+    f();
+    c->err.clear();
+    return DMB_OK;
+  } catch (const DmbError &e) {
+    c->err = e.msg;
+    return e.code;
+  } catch (const std::exception &e) {
+    c->err = e.what();
+    return DMB_ERR_STATE;
+  }
+}
+
+struct Staging {
+  DevBuf buf;
+  void *dev(size_t bytes) {
+    buf.ensure(bytes);
+    return buf.p;
+  }
+};
+
+void check_finite(const double *p, int64_t n, const char *what) {
+  for (int64_t i = 0; i < n; i++)
+    if (!std::isfinite(p[i]))
+      throw DmbError{DMB_ERR_ARGUMENT, std::string(what) + " must contain only finite values"};
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dmb_version(void) { return "diffmom_b200 0.1 sm_100a"; }
+
+dmb_status dmb_ctx_create(int device, dmb_ctx **out) {
+  if (!out) return DMB_ERR_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return DMB_ERR_CUDA;
+  if (device < 0 || device >= count) return DMB_ERR_ARGUMENT;
+  dmb_ctx *c = new dmb_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return DMB_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return DMB_OK;
+}
+
+dmb_status dmb_ctx_destroy(dmb_ctx *c) {
+  if (!c) return DMB_OK;
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf *bufs[] = {&c->d_xyz, &c->d_tri, &c->d_tcache, &c->d_rwg_slot, &c->d_tplus,
+                      &c->d_tminus, &c->d_vpo, &c->d_vmo, &c->d_len, &c->d_ap, &c->d_am,
+                      &c->d_slot_rwg, &c->d_slot_side, &c->d_wq, &c->d_centers, &c->d_adj_off,
+                      &c->d_adj_nb, &c->d_near_rec, &c->d_near_val, &c->d_near_entry_mn,
+                      &c->d_near_entry_off, &c->d_Z, &c->d_S, &c->d_F, &c->d_dinv, &c->d_W,
+                      &c->d_flags, &c->d_li_idx, &c->d_li_cnt, &c->d_li_inv, &c->d_net, &c->d_V,
+                      &c->d_H, &c->d_work, &c->d_vecs, &c->d_scal};
+    for (DevBuf *b : bufs) b->release();
+    cudaStreamDestroy(c->stream);
+  }
+  delete c;
+  return DMB_OK;
+}
+
+const char *dmb_last_error(const dmb_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+dmb_status dmb_get_timings(dmb_ctx *c, dmb_timings *out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(out, DMB_ERR_ARGUMENT, "timings output is NULL");
+    c->tm.kernels = c->launches;
+    *out = c->tm;
+  });
+}
+
+dmb_status dmb_mesh_upload(dmb_ctx *c, const double *xyz, const int64_t *tri, int64_t nv, int64_t nt) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(xyz && tri, DMB_ERR_ARGUMENT, "mesh arrays must be non-NULL");
+    DMB_REQUIRE(nv >= 3 && nt >= 1, DMB_ERR_ARGUMENT, "mesh needs at least 3 vertices and 1 triangle");
+    DMB_REQUIRE(nt < (1LL << 28) && nv < (1LL << 30), DMB_ERR_BUDGET, "mesh exceeds supported size");
+    check_finite(xyz, 3 * nv, "mesh coordinates");
+    c->h_xyz.assign(xyz, xyz + 3 * nv);
+    c->h_tri.resize(3 * nt);
+    for (int64_t i = 0; i < 3 * nt; i++) {
+      DMB_REQUIRE(tri[i] >= 1 && tri[i] <= nv, DMB_ERR_ARGUMENT,
+                  "triangle vertex index out of range at position " + std::to_string(i + 1));
+      c->h_tri[i] = (int32_t)(tri[i] - 1);
+    }
+    c->nv = nv;
+    c->nt = nt;
+    c->d_xyz.ensure(sizeof(double) * 3 * nv);
+    c->d_tri.ensure(sizeof(int32_t) * 3 * nt);
+    DMB_CUDA(cudaMemcpy(c->d_xyz.p, c->h_xyz.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice));
+    DMB_CUDA(cudaMemcpy(c->d_tri.p, c->h_tri.data(), sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice));
+    c->have_mesh = true;
+    c->have_rwg = false;
+    c->cache_valid = false;
+    c->z_valid = false;
+    c->pc_valid = false;
+  });
+}
+
+dmb_status dmb_rwg_upload(dmb_ctx *c, int64_t n, const int64_t *tplus, const int64_t *tminus,
+                          const int64_t *evert, const int64_t *vplus_opp, const int64_t *vminus_opp,
+                          const double *len, const double *area_plus, const double *area_minus) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->have_mesh, DMB_ERR_STATE, "upload the mesh before the RWG data");
+    DMB_REQUIRE(n >= 1, DMB_ERR_ARGUMENT,
+                "mesh produces no RWG unknowns; at least two triangles sharing an edge are required");
+    DMB_REQUIRE(tplus && tminus && vplus_opp && vminus_opp && len && area_plus && area_minus,
+                DMB_ERR_ARGUMENT, "RWG arrays must be non-NULL");
+    DMB_REQUIRE(n <= 3 * c->nt, DMB_ERR_DIMENSION, "more RWG functions than triangle edges");
+    auto idx = [&](const int64_t *a, int64_t lim, std::vector<int32_t> &o, const char *what) {
+      o.resize(n);
+      for (int64_t i = 0; i < n; i++) {
+        DMB_REQUIRE(a[i] >= 1 && a[i] <= lim, DMB_ERR_ARGUMENT,
+                    std::string(what) + " index out of range at RWG " + std::to_string(i + 1));
+        o[i] = (int32_t)(a[i] - 1);
+      }
+    };
+    idx(tplus, c->nt, c->h_tplus, "tplus");
+    idx(tminus, c->nt, c->h_tminus, "tminus");
+    idx(vplus_opp, c->nv, c->h_vpo, "vplus_opp");
+    idx(vminus_opp, c->nv, c->h_vmo, "vminus_opp");
+    for (int64_t i = 0; i < n; i++) {
+      DMB_REQUIRE(c->h_tplus[i] != c->h_tminus[i], DMB_ERR_ARGUMENT,
+                  "RWG " + std::to_string(i + 1) + " has identical T+ and T-");
+      DMB_REQUIRE(std::isfinite(len[i]) && len[i] > 0, DMB_ERR_ARGUMENT,
+                  "RWG edge has zero or unrepresentable length");
+      DMB_REQUIRE(std::isfinite(area_plus[i]) && area_plus[i] > 0 && std::isfinite(area_minus[i]) &&
+                      area_minus[i] > 0,
+                  DMB_ERR_ARGUMENT, "RWG triangle areas must be finite and positive");
+    }
+    (void)evert;
+    c->h_len.assign(len, len + n);
+    c->h_ap.assign(area_plus, area_plus + n);
+    c->h_am.assign(area_minus, area_minus + n);
+    c->n = n;
+    auto up = [&](DevBuf &b, const void *src, size_t bytes) {
+      b.ensure(bytes);
+      DMB_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+    };
+    up(c->d_tplus, c->h_tplus.data(), 4 * n);
+    up(c->d_tminus, c->h_tminus.data(), 4 * n);
+    up(c->d_vpo, c->h_vpo.data(), 4 * n);
+    up(c->d_vmo, c->h_vmo.data(), 4 * n);
+    up(c->d_len, c->h_len.data(), 8 * n);
+    up(c->d_ap, c->h_ap.data(), 8 * n);
+    up(c->d_am, c->h_am.data(), 8 * n);
+    dmb::build_host_topology(c);
+    c->have_rwg = true;
+    c->cache_valid = false;
+    c->z_valid = false;
+    c->pc_valid = false;
+  });
+}
+
+dmb_status dmb_assemble_z(dmb_ctx *c, double k, double eta0, int quad_order, int precision,
+                          double *Z_out) {
+  return guarded(c, [&] {
+    dmb::assemble(c, k, eta0, quad_order, precision);
+    if (Z_out) dmb::copy_z_out(c, Z_out);
+  });
+}
+
+dmb_status dmb_z_entries(dmb_ctx *c, const int64_t *m, const int64_t *n, int64_t count, double *out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(count >= 0 && (count == 0 || (m && n && out)), DMB_ERR_ARGUMENT, "bad entry arrays");
+    for (int64_t i = 0; i < count; i++)
+      DMB_REQUIRE(m[i] >= 1 && m[i] <= c->n && n[i] >= 1 && n[i] <= c->n, DMB_ERR_ARGUMENT,
+                  "entry index out of range");
+    dmb::z_entries(c, m, n, count, out);
+  });
+}
+
+dmb_status dmb_apply_impedance(dmb_ctx *c, const double *zs) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(zs, DMB_ERR_ARGUMENT, "surface impedance array is NULL");
+    check_finite(zs, 2 * c->nt, "surface impedance");
+    dmb::apply_impedance(c, zs);
+  });
+}
+
+dmb_status dmb_matvec(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(x && y && nrhs >= 1, DMB_ERR_ARGUMENT, "bad matvec arguments");
+    size_t bytes = sizeof(double2) * c->n * nrhs;
+    DevBuf bx, by;
+    bx.ensure(bytes);
+    by.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bx.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    dmb::matvec_dev(c, bx.p, by.p, nrhs);
+    DMB_CUDA(cudaMemcpyAsync(y, by.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order) {
+  return guarded(c, [&] { dmb::prepare_operator(c, k, eta0, quad_order); });
+}
+
+dmb_status dmb_matvec_free(dmb_ctx *c, const double *x, double *y) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(x && y, DMB_ERR_ARGUMENT, "bad matvec arguments");
+    size_t bytes = sizeof(double2) * c->n;
+    DevBuf bx, by;
+    bx.ensure(bytes);
+    by.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bx.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    dmb::matvec_free_dev(c, bx.as<double>(), by.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(y, by.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_nf_build(dmb_ctx *c, double cutoff, int kind, double *nnz_ratio_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(!std::isnan(cutoff) && cutoff >= 0.0, DMB_ERR_ARGUMENT,
+                "near-field cutoff must be nonnegative and not NaN");
+    DMB_REQUIRE(kind == DMB_PRECOND_NF_LU || kind == DMB_PRECOND_NF_DIAG, DMB_ERR_ARGUMENT,
+                "invalid factorization; expected :lu or :diag");
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    dmb::nf_build(c, cutoff, kind);
+    if (nnz_ratio_out) *nnz_ratio_out = c->nnz_ratio;
+  });
+}
+
+dmb_status dmb_nf_apply(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->pc_valid, DMB_ERR_STATE, "no near-field preconditioner built");
+    DMB_REQUIRE(x && y && nrhs >= 1, DMB_ERR_ARGUMENT, "bad apply arguments");
+    size_t bytes = sizeof(double2) * c->n * nrhs;
+    DevBuf bx;
+    bx.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bx.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    dmb::pc_apply_dev(c, bx.as<double>(), nrhs);
+    DMB_CUDA(cudaMemcpyAsync(y, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_rhs_plane_waves(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
+                               int64_t R, int quad_order, double *V_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(kvecs && E0s && pols && V_out && R >= 1, DMB_ERR_ARGUMENT, "bad plane-wave arrays");
+    check_finite(kvecs, 3 * R, "plane-wave k_vec");
+    check_finite(E0s, R, "plane-wave amplitude E0");
+    check_finite(pols, 3 * R, "plane-wave polarization");
+    for (int64_t r = 0; r < R; r++) {
+      const double *kv = kvecs + 3 * r, *pl = pols + 3 * r;
+      double kn = std::sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]);
+      double pn = std::sqrt(pl[0] * pl[0] + pl[1] * pl[1] + pl[2] * pl[2]);
+      DMB_REQUIRE(kn > 0, DMB_ERR_ARGUMENT, "plane-wave k_vec must have a finite, nonzero norm.");
+      DMB_REQUIRE(std::fabs(pn - 1.0) <= 1e-10 * std::max(1.0, pn) + 1e-12, DMB_ERR_ARGUMENT,
+                  "plane-wave polarization must be a unit vector");
+      double dt = std::fabs((kv[0] * pl[0] + kv[1] * pl[1] + kv[2] * pl[2]) / (kn * pn));
+      DMB_REQUIRE(dt <= 1e-10, DMB_ERR_ARGUMENT, "plane-wave polarization must be transverse to k_vec");
+    }
+    size_t bytes = sizeof(double2) * c->n * R;
+    DevBuf bv;
+    bv.ensure(bytes);
+    dmb::rhs_plane_waves_dev(c, kvecs, E0s, pols, R, quad_order, bv.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(V_out, bv.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_gmres(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs, double tol, int maxiter,
+                     int precond_kind, int precond_side, int check_convergence,
+                     dmb_gmres_stats *stats) {
+  dmb_gmres_stats st{};
+  dmb_status s = guarded(c, [&] {
+    DMB_REQUIRE(std::isfinite(tol) && tol > 0, DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive");
+    DMB_REQUIRE(maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
+    DMB_REQUIRE(precond_side == DMB_SIDE_LEFT || precond_side == DMB_SIDE_RIGHT, DMB_ERR_ARGUMENT,
+                "Invalid precond_side (expected :left or :right)");
+    DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad GMRES arrays");
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
+    size_t bytes = sizeof(double2) * c->n * nrhs;
+    DevBuf bb, bx;
+    bb.ensure(bytes);
+    bx.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bb.p, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
+    dmb::gmres_dev(c, bb.as<double>(), bx.as<double>(), nrhs, tol, maxiter, precond_kind,
+                   precond_side, &st);
+    DMB_CUDA(cudaMemcpyAsync(x, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    if (check_convergence && !st.solved)
+      throw DmbError{DMB_ERR_NOT_CONVERGED,
+                     "forward GMRES did not converge consistently: niter=" + std::to_string(st.niter) +
+                         ", final_residual=" + std::to_string(st.residual) +
+                         ", tol=" + std::to_string(tol) + ", maxiter=" + std::to_string(maxiter)};
+  });
+  if (stats) *stats = st;
+  return s;
+}
+
+dmb_status dmb_solve_direct(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs,
+                            double *backward_error_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad solve arrays");
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
+    size_t bytes = sizeof(double2) * c->n * nrhs;
+    DevBuf bb, bx;
+    bb.ensure(bytes);
+    bx.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bb.p, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
+    double berr = 0;
+    dmb::solve_direct_dev(c, bb.as<double>(), bx.as<double>(), nrhs, &berr);
+    DMB_CUDA(cudaMemcpyAsync(x, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    if (backward_error_out) *backward_error_out = berr;
+  });
+}
+
+dmb_status dmb_farfield(dmb_ctx *c, const double *rhat, int64_t NO, double k, double eta0,
+                        int quad_order, const double *I, int64_t nrhs, double *E_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(rhat && I && E_out && NO >= 1 && nrhs >= 1, DMB_ERR_ARGUMENT, "bad far-field arrays");
+    DMB_REQUIRE(std::isfinite(k) && k > 0 && std::isfinite(eta0), DMB_ERR_ARGUMENT,
+                "far-field wavenumber and eta0 must be finite");
+    check_finite(rhat, 3 * NO, "far-field directions");
+    check_finite(I, 2 * c->n * nrhs, "current coefficients");
+    size_t ib = sizeof(double2) * c->n * nrhs, eb = sizeof(double2) * 3 * NO * nrhs;
+    DevBuf bi, be;
+    bi.ensure(ib);
+    be.ensure(eb);
+    DMB_CUDA(cudaMemcpyAsync(bi.p, I, ib, cudaMemcpyHostToDevice, c->stream));
+    dmb::farfield_dev(c, rhat, NO, k, eta0, quad_order, bi.as<double>(), nrhs, be.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(E_out, be.p, eb, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+// dmb_excitation.cu -- plane-wave right-hand sides, far field, and the
+// matrix-free operator.
+//
+//   * assemble_plane_wave (Excitation.jl:2866-2896): v_n = sum over T+/T- and
+//     quadrature points of -2 w_q A_t conj(f_n) . E0 pol exp(-i k.r_q)
+//   * radiation_vectors + compute_farfield (FarField.jl:425-611):
+//     E(rh) = i k eta0/(4 pi) sum_n I_n sum rh x (rh x f_n) w 2A exp(+i k rh.r')
+//   * MatrixFreeEFIEOperator mul! (EFIE.jl:867-909): Z x recomputed from the
+//     geometry without an N^2 store -- far triangle pairs on the fly in
+//     triangle-slot space, near records precomputed once.
+#include <algorithm>
+#include <cmath>
+
+#include "dmb_device.cuh"
+#include "dmb_internal.h"
+
+namespace {
+
+unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// V (N x R column-major)
+__global__ void k_plane_wave(int64_t N, int64_t R, const TriCache *__restrict__ tc, const int *__restrict__ rslot,
+                             int nq, const double *__restrict__ wq, const double *__restrict__ kv,
+                             const double *__restrict__ E0, const double *__restrict__ pol,
+                             double2 *__restrict__ V) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  int64_t r = idx / N, n = idx % N;
+  double k0 = kv[3 * r], k1 = kv[3 * r + 1], k2 = kv[3 * r + 2];
+  double e0 = E0[r];
+  double p0 = pol[3 * r] * e0, p1 = pol[3 * r + 1] * e0, p2 = pol[3 * r + 2] * e0;
+  double2 acc = make_double2(0, 0);
+  for (int s = 0; s < 2; s++) {
+    int sl = rslot[2 * n + s];
+    const TriCache &T = tc[sl / 3];
+    int i = sl % 3;
+    for (int q = 0; q < nq; q++) {
+      double f0 = T.s[i] * (T.qp[q][0] - T.p[i][0]);
+      double f1 = T.s[i] * (T.qp[q][1] - T.p[i][1]);
+      double f2 = T.s[i] * (T.qp[q][2] - T.p[i][2]);
+      double arg = k0 * T.qp[q][0] + k1 * T.qp[q][1] + k2 * T.qp[q][2];
+      double sn, cs;
+      sincos(arg, &sn, &cs);
+      // E = pol*E0*(cos arg - i sin arg); inner = f . E
+      double fe = f0 * p0 + f1 * p1 + f2 * p2;
+      double2 ip = make_double2(fe * cs, -fe * sn);
+      double2 ap = cscale(ip, T.area);
+      acc = cadd(acc, cscale(ap, -(2 * wq[q])));
+    }
+  }
+  V[idx] = acc;
+}
+
+// radiation matrix G (3*NO x N, row-major) for directions rh
+__global__ void k_radiation(int64_t N, int64_t NO, const TriCache *__restrict__ tc, const int *__restrict__ rslot,
+                            int nq, const double *__restrict__ wq, const double *__restrict__ rh, double k,
+                            double eta0, double2 *__restrict__ G) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t q = blockIdx.y;
+  if (n >= N) return;
+  double r0 = rh[3 * q], r1 = rh[3 * q + 1], r2 = rh[3 * q + 2];
+  double rn2 = r0 * r0 + r1 * r1 + r2 * r2;
+  double2 c0 = make_double2(0, 0), c1 = c0, c2 = c0;
+  for (int s = 0; s < 2; s++) {
+    int sl = rslot[2 * n + s];
+    const TriCache &T = tc[sl / 3];
+    int i = sl % 3;
+    for (int qs = 0; qs < nq; qs++) {
+      double f0 = T.s[i] * (T.qp[qs][0] - T.p[i][0]);
+      double f1 = T.s[i] * (T.qp[qs][1] - T.p[i][1]);
+      double f2 = T.s[i] * (T.qp[qs][2] - T.p[i][2]);
+      double wt = wq[qs] * 2 * T.area;
+      double arg = k * (r0 * T.qp[qs][0] + r1 * T.qp[qs][1] + r2 * T.qp[qs][2]);
+      double sn, cs;
+      sincos(arg, &sn, &cs);
+      double2 ph = make_double2(wt * cs, wt * sn);
+      c0 = cadd(c0, cscale(ph, f0));
+      c1 = cadd(c1, cscale(ph, f1));
+      c2 = cadd(c2, cscale(ph, f2));
+    }
+  }
+  // rh x (rh x C) / |rh|^2 = (rh (rh.C) - C |rh|^2) / |rh|^2
+  double2 d = cadd(cadd(cscale(c0, r0), cscale(c1, r1)), cscale(c2, r2));
+  double2 v0 = cscale(csub(cscale(d, r0), cscale(c0, rn2)), 1.0 / rn2);
+  double2 v1 = cscale(csub(cscale(d, r1), cscale(c1, rn2)), 1.0 / rn2);
+  double2 v2 = cscale(csub(cscale(d, r2), cscale(c2, rn2)), 1.0 / rn2);
+  double2 pref = make_double2(0, k * eta0 * DMB_INV_FOUR_PI);
+  G[(3 * q + 0) * N + n] = cmul(pref, v0);
+  G[(3 * q + 1) * N + n] = cmul(pref, v1);
+  G[(3 * q + 2) * N + n] = cmul(pref, v2);
+}
+
+// C (M x R col-major) = A (M x K row-major) B (K x R col-major)
+__global__ void __launch_bounds__(256) k_gemm_rc(int64_t M, int64_t K, int64_t R, const double2 *__restrict__ A,
+                                                 const double2 *__restrict__ B, double2 *__restrict__ C) {
+  __shared__ double2 As[16][65];
+  __shared__ double2 Bs[16][65];
+  int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  int64_t m0 = (int64_t)blockIdx.x * 64, r0 = (int64_t)blockIdx.y * 64;
+  double2 acc[4][4];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0, 0);
+  for (int64_t k0 = 0; k0 < K; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int kk = e & 15, mm = e >> 4;
+      int64_t m = m0 + mm, kx = k0 + kk, r = r0 + mm;
+      As[kk][mm] = (m < M && kx < K) ? A[m * K + kx] : make_double2(0, 0);
+      Bs[kk][mm] = (r < R && kx < K) ? B[r * K + kx] : make_double2(0, 0);
+    }
+    __syncthreads();
+    for (int kk = 0; kk < 16; kk++)
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) acc[i][j] = cadd(acc[i][j], cmul(As[kk][ty + 16 * i], Bs[kk][tx + 16 * j]));
+    __syncthreads();
+  }
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      int64_t m = m0 + ty + 16 * i, r = r0 + tx + 16 * j;
+      if (m < M && r < R) C[r * M + m] = acc[i][j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// matrix-free operator
+// ---------------------------------------------------------------------------
+__global__ void k_scatter_slots(int64_t N, const int *__restrict__ rslot, const double2 *__restrict__ x,
+                                double2 *__restrict__ Xs) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  Xs[rslot[2 * m]] = x[m];
+  Xs[rslot[2 * m + 1]] = x[m];
+}
+
+__device__ __forceinline__ bool tri_adjacent2(const int *__restrict__ off, const int *__restrict__ nb, int ta, int tb) {
+  for (int i = off[ta]; i < off[ta + 1]; i++)
+    if (nb[i] == tb) return true;
+  return false;
+}
+
+// Ys[3ta+i] = sum_{tb far from ta} sum_j block(ta,tb)[i][j] Xs[3tb+j]
+__global__ void __launch_bounds__(256) k_mf_far(int nt, int nq, const TriCache *__restrict__ tc,
+                                                const int *__restrict__ aoff, const int *__restrict__ anb,
+                                                double k, double inv_k2, const double2 *__restrict__ Xs,
+                                                double2 *__restrict__ Ys) {
+  __shared__ double2 red[8][3];
+  int ta = blockIdx.x;
+  const TriCache &A = tc[ta];
+  double2 y[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  for (int tb = threadIdx.x; tb < nt; tb += blockDim.x) {
+    if (tb == ta || tri_adjacent2(aoff, anb, ta, tb)) continue;
+    const TriCache &B = tc[tb];
+    double2 xs[3];
+    bool any = false;
+    for (int j = 0; j < 3; j++) {
+      xs[j] = B.rwg[j] >= 0 ? Xs[3 * tb + j] : make_double2(0, 0);
+      any |= B.rwg[j] >= 0;
+    }
+    if (!any) continue;
+    double m0r = 0, m0i = 0, mar[3] = {0, 0, 0}, mai[3] = {0, 0, 0}, mbr[3] = {0, 0, 0}, mbi[3] = {0, 0, 0},
+           mabr = 0, mabi = 0;
+    for (int b = 0; b < nq; b++)
+      for (int a = 0; a < nq; a++) {
+        double dx = A.qp[a][0] - B.qp[b][0], dy = A.qp[a][1] - B.qp[b][1], dz = A.qp[a][2] - B.qp[b][2];
+        double R = sqrt(dx * dx + dy * dy + dz * dz);
+        double sn, cs;
+        sincos(k * R, &sn, &cs);
+        double g = (DMB_INV_FOUR_PI / R) * (A.w2a[a] * B.w2a[b]);
+        double gr = cs * g, gi = -sn * g;
+        m0r += gr;
+        m0i += gi;
+        for (int d = 0; d < 3; d++) {
+          mar[d] += gr * A.ql[a][d];
+          mai[d] += gi * A.ql[a][d];
+          mbr[d] += gr * B.ql[b][d];
+          mbi[d] += gi * B.ql[b][d];
+        }
+        double dd = A.ql[a][0] * B.ql[b][0] + A.ql[a][1] * B.ql[b][1] + A.ql[a][2] * B.ql[b][2];
+        mabr += gr * dd;
+        mabi += gi * dd;
+      }
+    for (int i = 0; i < 3; i++) {
+      if (A.rwg[i] < 0) continue;
+      double mbpr = mbr[0] * A.pl[i][0] + mbr[1] * A.pl[i][1] + mbr[2] * A.pl[i][2];
+      double mbpi = mbi[0] * A.pl[i][0] + mbi[1] * A.pl[i][1] + mbi[2] * A.pl[i][2];
+      for (int j = 0; j < 3; j++) {
+        if (B.rwg[j] < 0) continue;
+        double mapr = mar[0] * B.pl[j][0] + mar[1] * B.pl[j][1] + mar[2] * B.pl[j][2];
+        double mapi = mai[0] * B.pl[j][0] + mai[1] * B.pl[j][1] + mai[2] * B.pl[j][2];
+        double pp = A.pl[i][0] * B.pl[j][0] + A.pl[i][1] * B.pl[j][1] + A.pl[i][2] * B.pl[j][2];
+        double ss = A.s[i] * B.s[j], sc = A.dv[i] * B.dv[j] * inv_k2;
+        double2 v = make_double2(ss * (mabr - mapr - mbpr + pp * m0r) - sc * m0r,
+                                 ss * (mabi - mapi - mbpi + pp * m0i) - sc * m0i);
+        y[i] = cadd(y[i], cmul(v, xs[j]));
+      }
+    }
+  }
+  for (int i = 0; i < 3; i++) {
+    double2 v = warp_sum2(y[i]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32][i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double2 s = make_double2(0, 0);
+    for (int w = 0; w < 8; w++) s = cadd(s, red[w][threadIdx.x]);
+    Ys[3 * ta + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_mf_gather(int64_t N, const int *__restrict__ rslot, const double2 *__restrict__ Ys,
+                            double2 *__restrict__ y) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  y[m] = cadd(Ys[rslot[2 * m]], Ys[rslot[2 * m + 1]]);
+}
+
+// near entries: y[m] += v x[n]; y[n] += v x[m] (m != n)
+__global__ void k_mf_near(int64_t nent, const int2 *__restrict__ mn, const int64_t *__restrict__ off,
+                          const double2 *__restrict__ vals, const double2 *__restrict__ x, double2 *__restrict__ y) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  double2 v = make_double2(0, 0);
+  for (int64_t r = off[e]; r < off[e + 1]; r++) v = cadd(v, vals[r]);
+  int2 p = mn[e];
+  double2 a = cmul(v, x[p.y]);
+  atomicAdd(&y[p.x].x, a.x);
+  atomicAdd(&y[p.x].y, a.y);
+  if (p.x != p.y) {
+    double2 b = cmul(v, x[p.x]);
+    atomicAdd(&y[p.y].x, b.x);
+    atomicAdd(&y[p.y].y, b.y);
+  }
+}
+
+__global__ void k_times_minus_i_w(int64_t N, double w, double2 *__restrict__ y) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  double2 v = y[m];
+  y[m] = make_double2(w * v.y, -w * v.x);
+}
+
+}  // namespace
+
+namespace dmb {
+
+void near_values(dmb_ctx *c, double k, double inv_k2);
+
+void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols, int64_t R,
+                         int quad_order, double *V_dev) {
+  double t0 = now_ms();
+  ensure_cache(c, quad_order);
+  DevBuf p;
+  p.ensure(sizeof(double) * 7 * R);
+  double *dk = p.as<double>(), *de = dk + 3 * R, *dp = de + R;
+  DMB_CUDA(cudaMemcpyAsync(dk, kvecs, 24 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(de, E0s, 8 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(dp, pols, 24 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_LAUNCH(c, k_plane_wave, blocks_for(c->n * R, 128), 128, 0, c->n, R, c->d_tcache.as<TriCache>(),
+             c->d_rwg_slot.as<int>(), c->nq, c->d_wq.as<double>(), dk, de, dp, (double2 *)V_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  c->tm.rhs_ms = now_ms() - t0;
+}
+
+void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double eta0, int quad_order,
+                  const double *I_dev, int64_t nrhs, double *E_dev) {
+  ensure_cache(c, quad_order);
+  const int64_t N = c->n;
+  DevBuf dr, G;
+  dr.ensure(24 * NO);
+  G.ensure(sizeof(double2) * 3 * NO * N);
+  DMB_CUDA(cudaMemcpyAsync(dr.p, rhat, 24 * NO, cudaMemcpyHostToDevice, c->stream));
+  dim3 g(blocks_for(N, 128), (unsigned)NO);
+  DMB_LAUNCH(c, k_radiation, g, 128, 0, N, NO, c->d_tcache.as<TriCache>(), c->d_rwg_slot.as<int>(), c->nq,
+             c->d_wq.as<double>(), dr.as<double>(), k, eta0, G.as<double2>());
+  dim3 g2(blocks_for(3 * NO, 64), blocks_for(nrhs, 64));
+  DMB_LAUNCH(c, k_gemm_rc, g2, 256, 0, 3 * NO, N, nrhs, G.as<double2>(), (const double2 *)I_dev,
+             (double2 *)E_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order) {
+  DMB_REQUIRE(std::isfinite(k) && k != 0.0, DMB_ERR_ARGUMENT, "EFIE wavenumber must be finite and nonzero");
+  DMB_REQUIRE(std::isfinite(eta0) && eta0 != 0.0, DMB_ERR_ARGUMENT, "EFIE eta0 must be finite and nonzero");
+  ensure_cache(c, quad_order);
+  c->k = k;
+  c->eta0 = eta0;
+  near_values(c, k, 1.0 / (k * k));
+}
+
+void matvec_free_dev(dmb_ctx *c, const double *x, double *y) {
+  DMB_REQUIRE(c->cache_valid && c->k != 0.0, DMB_ERR_STATE, "operator not prepared");
+  const int64_t N = c->n, nt = c->nt;
+  DevBuf xs, ys;
+  xs.ensure(sizeof(double2) * 3 * nt);
+  ys.ensure(sizeof(double2) * 3 * nt);
+  DMB_CUDA(cudaMemsetAsync(xs.p, 0, sizeof(double2) * 3 * nt, c->stream));
+  DMB_LAUNCH(c, k_scatter_slots, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(), (const double2 *)x,
+             xs.as<double2>());
+  DMB_LAUNCH(c, k_mf_far, (unsigned)nt, 256, 0, (int)nt, c->nq, c->d_tcache.as<TriCache>(),
+             c->d_adj_off.as<int>(), c->d_adj_nb.as<int>(), c->k, 1.0 / (c->k * c->k), xs.as<double2>(),
+             ys.as<double2>());
+  DMB_LAUNCH(c, k_mf_gather, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(), ys.as<double2>(),
+             (double2 *)y);
+  if (c->n_near_entry > 0)
+    DMB_LAUNCH(c, k_mf_near, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
+               c->d_near_entry_mn.as<int2>(), c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(),
+               (const double2 *)x, (double2 *)y);
+  DMB_LAUNCH(c, k_times_minus_i_w, blocks_for(N, 256), 256, 0, N, c->k * c->eta0, (double2 *)y);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+}  // namespace dmb

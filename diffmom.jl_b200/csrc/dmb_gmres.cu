@@ -1,0 +1,368 @@
+// dmb_gmres.cu -- GMRES on the device (solve_gmres, IterativeSolve.jl:341-392).
+//
+// Semantics follow Krylov.gmres as the reference calls it: x0 = 0, no restart
+// (the basis grows up to maxiter vectors), rtol = tol, atol = 0, left
+// preconditioning stops on the preconditioned residual estimate
+// |g_{j+1}| <= tol * ||M b||, right preconditioning on the true residual
+// estimate |g_{j+1}| <= tol * ||b||.  Arnoldi orthogonalisation uses
+// classical Gram-Schmidt applied twice (same Krylov basis as Krylov.jl's
+// modified Gram-Schmidt up to rounding, two reductions per step instead of
+// j+1 sequential ones); Givens rotations and the triangular solve are FP64.
+//
+// nrhs systems are solved together: every operator application is one Z*X
+// product (GEMM) over all still-active columns, while each system keeps its
+// own Hessenberg matrix, rotations and stopping test.  When the basis would
+// exceed the memory budget the iteration restarts from the current iterate.
+#include <algorithm>
+#include <cmath>
+
+#include "dmb_device.cuh"
+#include "dmb_internal.h"
+
+namespace {
+
+unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// h[r][i] = <V_i(r), w(r)> for i in [0, j]
+__global__ void k_dots(int64_t N, int64_t R, int j, int64_t vstride, const double2 *__restrict__ V,
+                       const double2 *__restrict__ w, double2 *__restrict__ h, int hld) {
+  __shared__ double2 red[32];
+  int i = blockIdx.x;
+  int64_t r = blockIdx.y;
+  const double2 *vi = V + (int64_t)i * vstride + r * N;
+  const double2 *wr = w + r * N;
+  double re = 0, im = 0;
+  for (int64_t n = threadIdx.x; n < N; n += blockDim.x) {
+    double2 a = vi[n], b = wr[n];
+    re = fma(a.x, b.x, fma(a.y, b.y, re));
+    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+  }
+  double2 v = warp_sum2(make_double2(re, im));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : make_double2(0, 0);
+    v = warp_sum2(v);
+    if (threadIdx.x == 0) h[r * hld + i] = v;
+  }
+  (void)j;
+}
+
+// w(r) -= sum_i h[r][i] V_i(r); H[r][:, j] += h
+__global__ void k_cgs_update(int64_t N, int64_t R, int j, int64_t vstride, const double2 *__restrict__ V,
+                             const double2 *__restrict__ h, int hld, double2 *__restrict__ w) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  int64_t r = idx / N, n = idx % N;
+  double2 acc = w[idx];
+  for (int i = 0; i <= j; i++) acc = csub(acc, cmul(h[r * hld + i], V[(int64_t)i * vstride + r * N + n]));
+  w[idx] = acc;
+}
+
+__global__ void k_hacc(int64_t R, int j, const double2 *__restrict__ h, int hld, double2 *__restrict__ H,
+                       int kcap) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  double2 *Hr = H + r * (int64_t)(kcap + 1) * kcap + (int64_t)j * (kcap + 1);
+  for (int i = 0; i <= j; i++) Hr[i] = cadd(Hr[i], h[r * hld + i]);
+}
+
+__global__ void k_norms(int64_t N, const double2 *__restrict__ w, double *__restrict__ out) {
+  __shared__ double red[32];
+  int64_t r = blockIdx.x;
+  const double2 *wr = w + r * N;
+  double s = 0;
+  for (int64_t n = threadIdx.x; n < N; n += blockDim.x) s += cabs2(wr[n]);
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out[r] = sqrt(s);
+  }
+}
+
+__global__ void k_scale_cols(int64_t N, int64_t R, const double *__restrict__ nrm, const double2 *__restrict__ w,
+                             double2 *__restrict__ out) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  double d = nrm[idx / N];
+  out[idx] = d > 0 ? cscale(w[idx], 1.0 / d) : make_double2(0, 0);
+}
+
+struct SysState {
+  double beta;   // ||r0||
+  double eps;    // stopping threshold
+  double resid;  // |g_{j+1}|
+  int k;         // basis size used (iterations)
+  int done;      // 1 converged, 2 breakdown/zero rhs
+};
+
+// start: g = (beta, 0, ...); thresholds
+__global__ void k_init_state(int64_t R, const double *__restrict__ nrm, double tol, SysState *__restrict__ st,
+                             double2 *__restrict__ g, int kcap) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  SysState s;
+  s.beta = nrm[r];
+  s.eps = tol * nrm[r];
+  s.resid = nrm[r];
+  s.k = 0;
+  s.done = nrm[r] == 0.0 ? 2 : 0;
+  st[r] = s;
+  double2 *gr = g + r * (int64_t)(kcap + 1);
+  for (int i = 0; i <= kcap; i++) gr[i] = make_double2(0, 0);
+  gr[0] = make_double2(nrm[r], 0);
+}
+
+// Givens update of column j for every active system
+__global__ void k_givens(int64_t R, int j, int kcap, double2 *__restrict__ H, const double *__restrict__ hnext,
+                         double *__restrict__ cs, double2 *__restrict__ sn, double2 *__restrict__ g,
+                         SysState *__restrict__ st, unsigned *__restrict__ active) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  SysState s = st[r];
+  if (s.done) return;
+  double2 *Hc = H + r * (int64_t)(kcap + 1) * kcap + (int64_t)j * (kcap + 1);
+  double *c = cs + r * (int64_t)kcap;
+  double2 *sv = sn + r * (int64_t)kcap;
+  double2 *gr = g + r * (int64_t)(kcap + 1);
+  Hc[j + 1] = make_double2(hnext[r], 0);
+  // previous rotations: [c s; -conj(s) c]
+  for (int i = 0; i < j; i++) {
+    double2 a = Hc[i], b = Hc[i + 1];
+    Hc[i] = cadd(cscale(a, c[i]), cmul(sv[i], b));
+    Hc[i + 1] = csub(cscale(b, c[i]), cmul(cconj(sv[i]), a));
+  }
+  double2 a = Hc[j], b = Hc[j + 1];
+  double na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
+  double cc;
+  double2 ss, rho;
+  if (nb == 0.0) {
+    cc = 1.0; ss = make_double2(0, 0); rho = a;
+  } else if (na == 0.0) {
+    cc = 0.0; ss = cdiv(cconj(b), make_double2(nb, 0)); rho = make_double2(nb, 0);
+  } else {
+    double t = hypot(na, nb);
+    double2 sa = cscale(a, 1.0 / na);
+    cc = na / t;
+    ss = cscale(cmul(sa, cconj(b)), 1.0 / t);
+    rho = cscale(sa, t);
+  }
+  c[j] = cc;
+  sv[j] = ss;
+  Hc[j] = rho;
+  Hc[j + 1] = make_double2(0, 0);
+  double2 gj = gr[j];
+  gr[j] = cscale(gj, cc);
+  gr[j + 1] = cscale(cmul(cconj(ss), gj), -1.0);
+  s.k = j + 1;
+  s.resid = hypot(gr[j + 1].x, gr[j + 1].y);
+  if (s.resid <= s.eps) s.done = 1;
+  else if (hnext[r] == 0.0) s.done = 2;  // lucky breakdown: exact solution in the space
+  if (!isfinite(s.resid)) s.done = 3;
+  st[r] = s;
+  if (!s.done) atomicAdd(active, 1u);
+}
+
+// y = R^-1 g (back substitution, per system), stored in y[r][i]
+__global__ void k_backsolve(int64_t R, int kcap, const double2 *__restrict__ H, const double2 *__restrict__ g,
+                            const SysState *__restrict__ st, double2 *__restrict__ y) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  int k = st[r].k;
+  const double2 *Hr = H + r * (int64_t)(kcap + 1) * kcap;
+  const double2 *gr = g + r * (int64_t)(kcap + 1);
+  double2 *yr = y + r * (int64_t)kcap;
+  for (int i = k - 1; i >= 0; i--) {
+    double2 v = gr[i];
+    for (int l = i + 1; l < k; l++) v = csub(v, cmul(Hr[(int64_t)l * (kcap + 1) + i], yr[l]));
+    double2 d = Hr[(int64_t)i * (kcap + 1) + i];
+    yr[i] = (d.x == 0 && d.y == 0) ? make_double2(0, 0) : cdiv(v, d);
+  }
+  for (int i = k; i < kcap; i++) yr[i] = make_double2(0, 0);
+}
+
+// x(r) += sum_i y[r][i] V_i(r)
+__global__ void k_combine(int64_t N, int64_t R, int kmax, int64_t vstride, const double2 *__restrict__ V,
+                          const double2 *__restrict__ y, int kcap, double2 *__restrict__ x) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  int64_t r = idx / N, n = idx % N;
+  double2 acc = make_double2(0, 0);
+  for (int i = 0; i < kmax; i++) acc = cadd(acc, cmul(y[r * kcap + i], V[(int64_t)i * vstride + r * N + n]));
+  x[idx] = cadd(x[idx], acc);
+}
+
+__global__ void k_sub(int64_t count, const double2 *__restrict__ a, double2 *__restrict__ b) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) b[i] = csub(a[i], b[i]);
+}
+__global__ void k_add(int64_t count, const double2 *__restrict__ a, double2 *__restrict__ b) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) b[i] = cadd(b[i], a[i]);
+}
+
+}  // namespace
+
+namespace dmb {
+
+void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, double2 *w, double2 *tmp,
+                    int64_t R) {
+  const int64_t N = c->n;
+  if (precond_kind == DMB_PRECOND_NONE) {
+    matvec_dev(c, v, w, R);
+  } else if (side == DMB_SIDE_LEFT) {
+    matvec_dev(c, v, w, R);
+    pc_apply_dev(c, (double *)w, R);
+  } else {
+    DMB_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double2) * N * R, cudaMemcpyDeviceToDevice, c->stream));
+    pc_apply_dev(c, (double *)tmp, R);
+    matvec_dev(c, tmp, w, R);
+  }
+}
+
+unsigned read_err_word(dmb_ctx *c);
+
+void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double tol, int maxiter,
+               int precond_kind, int side, dmb_gmres_stats *out) {
+  double t0 = now_ms();
+  const int64_t N = c->n;
+  if (precond_kind != DMB_PRECOND_NONE)
+    DMB_REQUIRE(c->pc_valid, DMB_ERR_STATE, "preconditioner requested but not built");
+  DMB_REQUIRE(precond_kind == DMB_PRECOND_NONE || precond_kind == c->pc_kind, DMB_ERR_STATE,
+              "requested preconditioner kind differs from the one built");
+  // basis capacity: maxiter vectors, bounded by a 40% share of free memory
+  size_t freeb = 0, totb = 0;
+  DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
+  size_t vec_bytes = sizeof(double2) * N * R;
+  int64_t cap_mem = (int64_t)((freeb * 0.4) / vec_bytes) - 1;
+  int kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
+  const int64_t vstride = N * R;
+  c->d_V.ensure(vec_bytes * (kcap + 1));
+  c->d_work.ensure(vec_bytes * 2);
+  // layout: H[R][(k+1)k] g[R][k+1] sn[R][k] hb[R][k+1] y[R][k] | cs[R][k] nrm[2R] | st[R] | active
+  size_t small = sizeof(double2) * R * ((size_t)(kcap + 1) * kcap + 2 * (kcap + 1) + 2 * kcap) +
+                 sizeof(double) * R * (kcap + 2) + sizeof(SysState) * R + 64;
+  c->d_H.ensure(small);
+  double2 *V = c->d_V.as<double2>();
+  double2 *w = c->d_work.as<double2>();
+  double2 *tmp = w + N * R;
+  double2 *H = c->d_H.as<double2>();
+  double2 *g = H + R * (int64_t)(kcap + 1) * kcap;
+  double2 *sn = g + R * (int64_t)(kcap + 1);
+  double2 *hb = sn + R * (int64_t)kcap;
+  double2 *ybuf = hb + R * (int64_t)(kcap + 1);
+  double *cs = (double *)(ybuf + R * (int64_t)kcap);
+  double *nrm = cs + R * (int64_t)kcap;
+  SysState *st = (SysState *)(nrm + 2 * R);
+  unsigned *active = (unsigned *)(st + R);
+  const double2 *b = (const double2 *)b_dev;
+  double2 *x = (double2 *)x_dev;
+
+  DMB_CUDA(cudaMemsetAsync(x, 0, vec_bytes, c->stream));
+  int total_iters = 0, restarts = 0;
+  bool all_done = false;
+  std::vector<SysState> hst(R);
+  while (!all_done) {
+    // r0 = b - Z x (x = 0 on the first cycle), preconditioned on the left
+    if (total_iters == 0) {
+      DMB_CUDA(cudaMemcpyAsync(V, b, vec_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      matvec_dev(c, x, V, R);
+      DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, V);
+    }
+    if (precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_LEFT) pc_apply_dev(c, (double *)V, R);
+    DMB_CUDA(cudaMemsetAsync(H, 0, sizeof(double2) * R * (int64_t)(kcap + 1) * kcap, c->stream));
+    DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, V, nrm);
+    if (total_iters == 0) {
+      DMB_LAUNCH(c, k_init_state, blocks_for(R, 128), 128, 0, R, nrm, tol, st, g, kcap);
+    } else {
+      // restart keeps each system's original threshold; reset the basis state
+      std::vector<double> hn(R);
+      DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm, 8 * R, cudaMemcpyDeviceToHost, c->stream));
+      DMB_CUDA(cudaStreamSynchronize(c->stream));
+      std::vector<double2> hg((size_t)R * (kcap + 1), make_double2(0, 0));
+      for (int64_t r = 0; r < R; r++) {
+        hst[r].k = 0;
+        hst[r].resid = hn[r];
+        if (!hst[r].done) hg[(size_t)r * (kcap + 1)] = make_double2(hn[r], 0);
+      }
+      DMB_CUDA(cudaMemcpyAsync(st, hst.data(), sizeof(SysState) * R, cudaMemcpyHostToDevice, c->stream));
+      DMB_CUDA(cudaMemcpyAsync(g, hg.data(), sizeof(double2) * hg.size(), cudaMemcpyHostToDevice, c->stream));
+    }
+    DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, V, V);
+    int j = 0;
+    for (; j < kcap && total_iters < maxiter; j++, total_iters++) {
+      double2 *Vj = V + (int64_t)j * vstride;
+      apply_operator(c, precond_kind, side, Vj, w, tmp, R);
+      for (int pass = 0; pass < 2; pass++) {
+        DMB_LAUNCH(c, k_dots, dim3(j + 1, (unsigned)R), 256, 0, N, R, j, vstride, V, w, hb, kcap + 1);
+        DMB_LAUNCH(c, k_cgs_update, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, hb, kcap + 1, w);
+        DMB_LAUNCH(c, k_hacc, blocks_for(R, 128), 128, 0, R, j, hb, kcap + 1, H, kcap);
+      }
+      DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, nrm);
+      DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, w, V + (int64_t)(j + 1) * vstride);
+      DMB_CUDA(cudaMemsetAsync(active, 0, 4, c->stream));
+      DMB_LAUNCH(c, k_givens, blocks_for(R, 128), 128, 0, R, j, kcap, H, nrm, cs, sn, g, st, active);
+      unsigned h_active = 0;
+      DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
+      DMB_CUDA(cudaStreamSynchronize(c->stream));
+      if (h_active == 0) {
+        j++;
+        total_iters++;
+        break;
+      }
+    }
+    // solution update from this cycle
+    DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);
+    if (precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_RIGHT) {
+      DMB_CUDA(cudaMemsetAsync(tmp, 0, vec_bytes, c->stream));
+      DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, tmp);
+      pc_apply_dev(c, (double *)tmp, R);
+      DMB_LAUNCH(c, k_add, blocks_for(N * R, 256), 256, 0, N * R, tmp, x);
+    } else {
+      DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, x);
+    }
+    DMB_CUDA(cudaMemcpyAsync(hst.data(), st, sizeof(SysState) * R, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    all_done = true;
+    for (auto &s : hst)
+      if (!s.done) all_done = false;
+    if (total_iters >= maxiter) break;
+    if (!all_done) restarts++;
+  }
+  unsigned e = read_err_word(c);
+  DMB_REQUIRE((e & 4u) == 0, DMB_ERR_TIMEOUT, "triangular solve wait expired");
+  // true FP64 residual ||b - Z x|| / ||b|| per system
+  matvec_dev(c, x, w, R);
+  DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
+  DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, nrm);
+  DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);
+  std::vector<double> hn(2 * R);
+  DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm, 16 * R, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  double tres = 0, eres = 0;
+  bool solved = true;
+  for (int64_t r = 0; r < R; r++) {
+    double rel = hn[R + r] > 0 ? hn[r] / hn[R + r] : (hn[r] > 0 ? INFINITY : 0.0);
+    tres = std::max(tres, rel);
+    double est = hst[r].beta > 0 ? hst[r].resid / hst[r].beta : 0.0;
+    if (hst[r].done == 1 || hst[r].done == 2) {
+      if (hst[r].done == 1) eres = std::max(eres, est);
+    } else {
+      solved = false;
+      eres = std::max(eres, est);
+    }
+    if (!std::isfinite(rel)) solved = false;
+  }
+  out->niter = total_iters;
+  out->solved = solved ? 1 : 0;
+  out->residual = eres;
+  out->true_residual = tres;
+  out->restarts = restarts;
+  c->tm.solve_ms = now_ms() - t0;
+}
+
+}  // namespace dmb

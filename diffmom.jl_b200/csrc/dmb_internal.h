@@ -1,0 +1,190 @@
+// dmb_internal.h -- shared declarations of libdiffmom_b200 (not installed).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <array>
+#include <chrono>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/diffmom_b200.h"
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+struct DmbError {
+  int code;
+  std::string msg;
+};
+
+#define DMB_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e__ = (call);                                                       \
+    if (e__ != cudaSuccess)                                                         \
+      throw DmbError{DMB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)}; \
+  } while (0)
+
+#define DMB_REQUIRE(cond, code, text)                 \
+  do {                                                \
+    if (!(cond)) throw DmbError{(code), (text)};      \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffer (grow-only, owned by the context)
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  template <class T> T *as() const { return static_cast<T *>(p); }
+  void ensure(size_t want) {
+    if (want <= bytes && p) return;
+    release();
+    if (want == 0) want = 16;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      bytes = 0;
+      throw DmbError{DMB_ERR_BUDGET, std::string("device allocation of ") + std::to_string(want) +
+                                         " bytes failed: " + cudaGetErrorString(e)};
+    }
+    bytes = want;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// per-triangle cache (device, FP64).  Quadrature points are stored both in
+// global coordinates (FP64 path, as the reference's cache) and relative to the
+// triangle centroid (used by the moment contractions and the FP32 far pairs).
+// ---------------------------------------------------------------------------
+struct TriCache {
+  double v[3][3];     // vertices
+  double cen[3];      // centroid
+  double area;        // triangle_area
+  double w2a[7];      // w_q * 2A for the standard rule
+  double w2ah[7];     // w_q * 2A for the 7-point rule
+  double qp[7][3];    // standard-rule points (global)
+  double qph[7][3];   // 7-point-rule points (global)
+  double ql[7][3];    // standard-rule points minus centroid
+  // basis slots: RWG functions supported on this triangle (<= 3)
+  int rwg[3];         // RWG index (0-based) or -1
+  int side[3];        // 0 = T+, 1 = T-
+  double s[3];        // signed scale: f(r) = s * (r - p)
+  double dv[3];       // surface divergence (+len/A+ or -len/A-)
+  double p[3][3];     // opposite vertex (global)
+  double pl[3][3];    // opposite vertex minus centroid
+};
+
+// near-field record: one (near triangle pair, test slot, source slot)
+struct NearRec {
+  int ta, tb;     // ta == tb: self; otherwise ta outer (test), tb analytic (source)
+  int ia, ib;     // slots
+};
+
+struct dmb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  std::string err;
+  int sm_count = 148;
+
+  // mesh / basis (host copies, 0-based)
+  int64_t nv = 0, nt = 0, n = 0;
+  std::vector<double> h_xyz;
+  std::vector<int32_t> h_tri;
+  std::vector<int32_t> h_tplus, h_tminus, h_vpo, h_vmo;
+  std::vector<double> h_len, h_ap, h_am;
+  bool have_mesh = false, have_rwg = false, cache_valid = false;
+  int cache_quad_order = 0;
+
+  // device geometry
+  DevBuf d_xyz, d_tri, d_tcache, d_rwg_slot;  // rwg_slot: 2 ints per RWG (3t+i)
+  DevBuf d_tplus, d_tminus;                   // int32
+  DevBuf d_vpo, d_vmo;                        // int32 opposite vertices (0-based)
+  DevBuf d_len, d_ap, d_am;                   // RWG edge length / areas
+  DevBuf d_slot_rwg, d_slot_side;             // 3 per triangle
+  DevBuf d_wq;                                // 7 standard + 7 high-order weights
+  DevBuf d_centers;                           // RWG centres (N x 3)
+  int nq = 3;
+  double wq[7], wqh[7];
+  double xi1[7], xi2[7], xh1[7], xh2[7];
+
+  // adjacency + near records
+  std::vector<int32_t> adj_off, adj_nb;
+  DevBuf d_adj_off, d_adj_nb;
+  DevBuf d_near_rec, d_near_val, d_near_entry_mn, d_near_entry_off;
+  int64_t n_near_rec = 0, n_near_entry = 0;
+
+  // impedance matrix (row-major == column-major since Z is symmetric)
+  DevBuf d_Z;
+  int z_prec = -1;    // DMB_PREC_*
+  bool z_valid = false;
+  double k = 0, eta0 = 376.730313668;
+  DevBuf d_S;         // triangle-slot scratch (3Nt x 3Nt)
+
+  // preconditioner
+  int pc_kind = DMB_PRECOND_NONE;
+  int pc_prec = -1;
+  DevBuf d_F;         // factor storage (N x N, L strictly lower + D diagonal)
+  DevBuf d_dinv;      // Jacobi inverse diagonal
+  DevBuf d_W;         // LDL^T panel workspace
+  DevBuf d_flags;     // triangular-solve progress flags / error word
+  double nnz_ratio = 0;
+  bool pc_valid = false;
+
+  // local-inverse / learned preconditioner
+  DevBuf d_li_idx, d_li_cnt, d_li_inv;  // neighbour lists and inverse rows
+  int li_kmax = 0;
+  DevBuf d_net;       // learned weights
+  bool net_loaded = false;
+
+  // GMRES workspace
+  DevBuf d_V, d_H, d_work, d_vecs, d_scal;
+
+  // timings
+  dmb_timings tm{};
+  int64_t launches = 0;
+};
+
+// ---------------------------------------------------------------------------
+// helpers shared by translation units
+// ---------------------------------------------------------------------------
+namespace dmb {
+void ensure_cache(dmb_ctx *c, int quad_order);
+void build_host_topology(dmb_ctx *c);
+void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision);
+void copy_z_out(dmb_ctx *c, double *Z_out);
+void z_entries(dmb_ctx *c, const int64_t *m, const int64_t *n, int64_t count, double *out);
+void apply_impedance(dmb_ctx *c, const double *zs);
+void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs);  // device buffers, c128
+void nf_build(dmb_ctx *c, double cutoff, int kind);
+void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs);             // in place, c128 device
+void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
+                         int64_t R, int quad_order, double *V_dev);
+void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs, double tol,
+               int maxiter, int precond_kind, int precond_side, dmb_gmres_stats *st);
+void solve_direct_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs,
+                      double *berr);
+void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double eta0,
+                  int quad_order, const double *I_dev, int64_t nrhs, double *E_dev);
+void prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order);
+void matvec_free_dev(dmb_ctx *c, const double *x, double *y);
+void local_inverse_build(dmb_ctx *c, double radius, int kmax);
+double now_ms();
+}  // namespace dmb
+
+// launch bookkeeping: every library kernel launch goes through this macro so
+// the context can report how many of its kernels ran.
+#define DMB_LAUNCH(ctx, kernel, grid, block, smem, ...)                        \
+  do {                                                                         \
+    kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);          \
+    DMB_CUDA(cudaGetLastError());                                              \
+    (ctx)->launches++;                                                         \
+  } while (0)

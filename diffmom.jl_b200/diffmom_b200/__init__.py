@@ -1,0 +1,18 @@
+"""diffmom_b200 -- B200 library for DiffMoM.jl's dense surface-EFIE hot path.
+
+Host-side mirror of the Julia API (mesh generators, RWG construction and the
+EFIE / solver / far-field entry points) over the C ABI of libdiffmom_b200.so.
+"""
+from .mesh import (TriMesh, make_rect_plate, make_circular_plate, make_icosphere,
+                   make_perturbed_ellipsoid, triangle_area, triangle_areas, triangle_centers,
+                   nvertices, ntriangles)
+from .rwg import RWGData, build_rwg, rwg_centers, basis_triangles
+from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixFreeEFIEOperator,
+                  PlaneWaveExcitation, make_plane_wave, assemble_plane_wave, assemble_excitation,
+                  assemble_multiple_excitations, build_nearfield_preconditioner, NearFieldOperator,
+                  solve_gmres, solve_forward, solve_scattering, ScatteringResult, SphGrid,
+                  make_sph_grid, phi_cut_grid, compute_farfield, bistatic_rcs, backscatter_rcs,
+                  C0_DEFAULT, ETA0_DEFAULT)
+from ._native import load_library, LIB_PATH, DiffMoMError, NotConvergedError, FactorizationBreakdown
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,479 @@
+"""Host-side mirror of DiffMoM.jl's public API for the dense EFIE path.
+
+Same names, argument meaning and error behaviour as the Julia functions; the
+numerical work runs in libdiffmom_b200.so on the GPU.
+
+* ``EFIEDevice``            -- one device context bound to (mesh, rwg): the
+                               resident cache, Z and preconditioner.
+* ``assemble_Z_efie``       -- src/assembly/EFIE.jl:699-753
+* ``matrixfree_efie_operator`` -- src/assembly/EFIE.jl:975-1000
+* ``make_plane_wave`` / ``assemble_excitation`` / ``assemble_plane_wave`` /
+  ``assemble_multiple_excitations`` -- src/assembly/Excitation.jl
+* ``precompute_patch_mass`` / ``assemble_full_Z`` (per-triangle impedance)
+  -- src/assembly/Impedance.jl:304-408, src/solver/Solve.jl:1412-1449
+* ``build_nearfield_preconditioner`` / ``NearFieldOperator`` --
+  src/solver/NearFieldPreconditioner.jl:670-1054
+* ``solve_gmres`` -- src/solver/IterativeSolve.jl:341-392
+* ``solve_forward`` -- src/solver/Solve.jl:1342-1382
+* ``solve_scattering`` / ``ScatteringResult`` -- src/Workflow.jl:67-317
+* ``make_sph_grid`` / ``radiation_vectors``-free ``compute_farfield`` /
+  ``bistatic_rcs`` / ``backscatter_rcs`` -- FarField.jl, Diagnostics.jl
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+from .mesh import TriMesh, mesh_edge_max
+from .rwg import RWGData, build_rwg
+
+C0_DEFAULT = 299792458.0
+ETA0_DEFAULT = 376.730313668
+
+_PRECISIONS = {"fp64": nat.PREC_FP64, "mixed": nat.PREC_MIXED}
+
+
+def _frequency_to_wavenumber(freq_hz: float, c0: float = C0_DEFAULT) -> float:
+    """Excitation.jl:358-372: k = 2 pi f / c0."""
+    w = 2 * math.pi * float(freq_hz)
+    k = w / c0 if math.isfinite(w) else float(freq_hz) * (2 * math.pi / c0)
+    if not (math.isfinite(k) and k > 0):
+        raise ValueError("frequency is outside the representable wavenumber range")
+    return k
+
+
+# ---------------------------------------------------------------------------
+# device-bound system
+# ---------------------------------------------------------------------------
+class EFIEDevice:
+    """Device context holding one mesh + RWG basis (and then Z, preconditioner)."""
+
+    def __init__(self, mesh: TriMesh, rwg: RWGData, device: int = 0):
+        if rwg.mesh is not mesh:
+            raise ValueError("RWG data was built for a different mesh")
+        self.mesh = mesh
+        self.rwg = rwg
+        self.N = rwg.nedges
+        self.ctx = nat.Context(device)
+        self.ctx.call("dmb_mesh_upload", nat.dptr(mesh.xyz), nat.lptr(mesh.tri),
+                      mesh.nvertices, mesh.ntriangles)
+        self._evert = np.ascontiguousarray(rwg.evert, dtype=np.int64)
+        self._arrs = [np.ascontiguousarray(a, dtype=t) for a, t in (
+            (rwg.tplus, np.int64), (rwg.tminus, np.int64), (rwg.vplus_opp, np.int64),
+            (rwg.vminus_opp, np.int64), (rwg.len, np.float64), (rwg.area_plus, np.float64),
+            (rwg.area_minus, np.float64))]
+        tp, tm, vp, vm, ln, ap, am = self._arrs
+        self.ctx.call("dmb_rwg_upload", rwg.nedges, nat.lptr(tp), nat.lptr(tm),
+                      nat.lptr(self._evert), nat.lptr(vp), nat.lptr(vm), nat.dptr(ln),
+                      nat.dptr(ap), nat.dptr(am))
+        self.k = None
+        self.precision = None
+        self.quad_order = 3
+        self.preconditioner = None
+
+    # -- impedance matrix -----------------------------------------------
+    def assemble(self, k: float, quad_order: int = 3, eta0: float = ETA0_DEFAULT,
+                 precision: str = "fp64", copy_out: bool = False):
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        Z = np.empty((self.N, self.N), dtype=np.complex128, order="F") if copy_out else None
+        self.ctx.call("dmb_assemble_z", float(k), float(eta0), int(quad_order),
+                      _PRECISIONS[precision], nat.dptr(Z) if copy_out else None)
+        self.k, self.eta0, self.quad_order, self.precision = float(k), float(eta0), quad_order, precision
+        self.preconditioner = None
+        return Z
+
+    def z_host(self) -> np.ndarray:
+        m = np.repeat(np.arange(1, self.N + 1), self.N).astype(np.int64)
+        n = np.tile(np.arange(1, self.N + 1), self.N).astype(np.int64)
+        return self.entries(m, n).reshape(self.N, self.N)
+
+    def entries(self, m, n) -> np.ndarray:
+        m = np.ascontiguousarray(m, dtype=np.int64)
+        n = np.ascontiguousarray(n, dtype=np.int64)
+        out = np.empty(m.size, dtype=np.complex128)
+        self.ctx.call("dmb_z_entries", nat.lptr(m), nat.lptr(n), m.size, nat.dptr(out))
+        return out
+
+    def apply_impedance(self, zs_per_triangle) -> None:
+        zs = np.ascontiguousarray(np.broadcast_to(np.asarray(zs_per_triangle, dtype=np.complex128),
+                                                  (self.mesh.ntriangles,)))
+        self.ctx.call("dmb_apply_impedance", nat.dptr(zs))
+        self.preconditioner = None
+
+    def matvec(self, x) -> np.ndarray:
+        X = nat.c128(x)
+        nrhs = 1 if X.ndim == 1 else X.shape[1]
+        Y = np.empty_like(X)
+        self.ctx.call("dmb_matvec", nat.dptr(X), nat.dptr(Y), nrhs)
+        return Y
+
+    # -- preconditioner ---------------------------------------------------
+    def build_nearfield(self, cutoff: float, factorization: str = "lu") -> "NearFieldPreconditionerData":
+        kinds = {"lu": nat.PRECOND_NF_LU, "diag": nat.PRECOND_NF_DIAG}
+        if factorization not in kinds:
+            raise ValueError(f"invalid factorization={factorization}; expected one of (:lu, :diag)")
+        ratio = ctypes.c_double()
+        self.ctx.call("dmb_nf_build", float(cutoff), kinds[factorization], ctypes.byref(ratio))
+        self.preconditioner = NearFieldPreconditionerData(self, kinds[factorization], float(cutoff),
+                                                          ratio.value)
+        return self.preconditioner
+
+    def nf_apply(self, x) -> np.ndarray:
+        X = nat.c128(x)
+        nrhs = 1 if X.ndim == 1 else X.shape[1]
+        Y = np.empty_like(X)
+        self.ctx.call("dmb_nf_apply", nat.dptr(X), nat.dptr(Y), nrhs)
+        return Y
+
+    # -- excitation -------------------------------------------------------
+    def plane_wave_rhs(self, kvecs, E0s, pols, quad_order: int = 3) -> np.ndarray:
+        kv = np.ascontiguousarray(np.atleast_2d(kvecs), dtype=np.float64)
+        pl = np.ascontiguousarray(np.atleast_2d(pols), dtype=np.float64)
+        e0 = np.ascontiguousarray(np.atleast_1d(E0s), dtype=np.float64)
+        R = kv.shape[0]
+        V = np.empty((self.N, R), dtype=np.complex128, order="F")
+        self.ctx.call("dmb_rhs_plane_waves", nat.dptr(kv), nat.dptr(e0), nat.dptr(pl), R,
+                      int(quad_order), nat.dptr(V))
+        return V
+
+    # -- solvers ----------------------------------------------------------
+    def gmres(self, rhs, tol=1e-8, maxiter=200, preconditioner=None, precond_side="left",
+              check_gmres_convergence=True):
+        B = nat.c128(rhs)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        X = np.empty_like(B)
+        st = nat.GmresStats()
+        kind = nat.PRECOND_NONE if preconditioner is None else preconditioner.kind
+        side = {"left": nat.SIDE_LEFT, "right": nat.SIDE_RIGHT}.get(precond_side)
+        if side is None:
+            raise ValueError(f"Invalid precond_side: {precond_side} (expected :left or :right)")
+        status = self.ctx.lib.dmb_gmres(self.ctx.h, nat.dptr(B),
+                                        nat.dptr(X), nrhs, float(tol), int(maxiter),
+                                        kind, side, 1 if check_gmres_convergence else 0,
+                                        ctypes.byref(st))
+        self.ctx._check(status)
+        return X, GmresResult(st.niter, bool(st.solved), st.residual, st.true_residual, st.restarts)
+
+    def solve_direct(self, rhs):
+        B = nat.c128(rhs)
+        nrhs = 1 if B.ndim == 1 else B.shape[1]
+        X = np.empty_like(B)
+        berr = ctypes.c_double()
+        self.ctx.call("dmb_solve_direct", nat.dptr(B), nat.dptr(X),
+                      nrhs, ctypes.byref(berr))
+        self.preconditioner = None
+        return X, berr.value
+
+    def farfield(self, rhat, I, k=None, eta0=ETA0_DEFAULT, quad_order=3) -> np.ndarray:
+        rh = np.ascontiguousarray(np.atleast_2d(rhat), dtype=np.float64)
+        Ic = nat.c128(I)
+        nrhs = 1 if Ic.ndim == 1 else Ic.shape[1]
+        NO = rh.shape[0]
+        E = np.empty((3, NO, nrhs), dtype=np.complex128, order="F")
+        kk = self.k if k is None else k
+        self.ctx.call("dmb_farfield", nat.dptr(rh), NO, float(kk), float(eta0), int(quad_order),
+                      nat.dptr(Ic), nrhs, nat.dptr(E))
+        return E[:, :, 0] if nrhs == 1 else E
+
+    def timings(self):
+        return self.ctx.timings()
+
+    def close(self):
+        self.ctx.close()
+
+
+@dataclass
+class GmresResult:
+    niter: int
+    solved: bool
+    residual: float
+    true_residual: float
+    restarts: int = 0
+
+    @property
+    def residuals(self):
+        return [self.residual]
+
+
+@dataclass
+class NearFieldPreconditionerData:
+    device: EFIEDevice
+    kind: int
+    cutoff: float
+    nnz_ratio: float
+
+
+class NearFieldOperator:
+    """Callable preconditioner y = Z_nf^-1 x (NearFieldPreconditioner.jl:1034)."""
+
+    def __init__(self, P: NearFieldPreconditionerData):
+        self.P = P
+
+    def __matmul__(self, x):
+        return self.P.device.nf_apply(x)
+
+    def apply(self, x):
+        return self.P.device.nf_apply(x)
+
+
+# ---------------------------------------------------------------------------
+# Julia-named entry points
+# ---------------------------------------------------------------------------
+def assemble_Z_efie(mesh: TriMesh, rwg: RWGData, k, quad_order: int = 3, eta0=ETA0_DEFAULT,
+                    precision: str = "fp64", device: EFIEDevice | None = None) -> np.ndarray:
+    """Dense EFIE matrix Z (N x N complex128); EFIE.jl:699-753."""
+    dev = device or EFIEDevice(mesh, rwg)
+    try:
+        return dev.assemble(k, quad_order=quad_order, eta0=eta0, precision=precision, copy_out=True)
+    finally:
+        if device is None:
+            dev.close()
+
+
+class MatrixFreeEFIEOperator:
+    """y = Z x with entries recomputed on the device per product (EFIE.jl:759-909)."""
+
+    def __init__(self, mesh, rwg, k, quad_order=3, eta0=ETA0_DEFAULT):
+        self.dev = EFIEDevice(mesh, rwg)
+        self.dev.ctx.call("dmb_prepare_operator", float(k), float(eta0), int(quad_order))
+        self.shape = (rwg.nedges, rwg.nedges)
+
+    def __matmul__(self, x):
+        xc = np.ascontiguousarray(np.asarray(x, dtype=np.complex128))
+        y = np.empty_like(xc)
+        self.dev.ctx.call("dmb_matvec_free", nat.dptr(xc), nat.dptr(y))
+        return y
+
+    def mul(self, x):
+        return self @ x
+
+
+def matrixfree_efie_operator(mesh, rwg, k, quad_order=3, eta0=ETA0_DEFAULT):
+    return MatrixFreeEFIEOperator(mesh, rwg, k, quad_order=quad_order, eta0=eta0)
+
+
+@dataclass
+class PlaneWaveExcitation:
+    k_vec: np.ndarray
+    E0: float
+    pol: np.ndarray
+
+
+def make_plane_wave(k_vec, E0, pol) -> PlaneWaveExcitation:
+    """Excitation.jl:97-101 with the validation of Excitation.jl:1549-1616."""
+    kv = np.asarray(k_vec, dtype=np.float64).reshape(3)
+    pl = np.asarray(pol, dtype=np.float64).reshape(3)
+    if not np.all(np.isfinite(kv)):
+        raise ValueError("plane-wave k_vec components must be finite.")
+    if not math.isfinite(float(E0)):
+        raise ValueError(f"plane-wave amplitude E0 must be finite, got {E0}.")
+    kn = float(np.linalg.norm(kv))
+    if not kn > 0:
+        raise ValueError("plane-wave k_vec must have a finite, nonzero norm.")
+    pn = float(np.linalg.norm(pl))
+    if not math.isclose(pn, 1.0, rel_tol=1e-10, abs_tol=1e-12):
+        raise ValueError(f"plane-wave polarization must be a unit vector; norm={pn}.")
+    if abs(float(kv @ pl)) / (kn * pn) > 1e-10:
+        raise ValueError("plane-wave polarization must be transverse to k_vec")
+    return PlaneWaveExcitation(kv, float(E0), pl)
+
+
+def assemble_plane_wave(mesh, rwg, pw: PlaneWaveExcitation, quad_order=3, device=None) -> np.ndarray:
+    dev = device or EFIEDevice(mesh, rwg)
+    try:
+        return dev.plane_wave_rhs(pw.k_vec[None], [pw.E0], pw.pol[None], quad_order)[:, 0]
+    finally:
+        if device is None:
+            dev.close()
+
+
+def assemble_excitation(mesh, rwg, excitation, quad_order=3, device=None) -> np.ndarray:
+    if not isinstance(excitation, PlaneWaveExcitation):
+        raise TypeError(f"Unsupported excitation type: {type(excitation).__name__}")
+    return assemble_plane_wave(mesh, rwg, excitation, quad_order=quad_order, device=device)
+
+
+def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=None) -> np.ndarray:
+    dev = device or EFIEDevice(mesh, rwg)
+    try:
+        kv = np.stack([e.k_vec for e in excitations])
+        pl = np.stack([e.pol for e in excitations])
+        e0 = np.array([e.E0 for e in excitations])
+        return dev.plane_wave_rhs(kv, e0, pl, quad_order)
+    finally:
+        if device is None:
+            dev.close()
+
+
+# ---------------------------------------------------------------------------
+# solvers
+# ---------------------------------------------------------------------------
+def build_nearfield_preconditioner(device: EFIEDevice, cutoff: float, factorization: str = "lu"):
+    return device.build_nearfield(cutoff, factorization)
+
+
+def solve_gmres(device: EFIEDevice, rhs, preconditioner=None, precond_side="left", tol=1e-8,
+                maxiter=200, check_gmres_convergence=True):
+    return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
+                        precond_side=precond_side, check_gmres_convergence=check_gmres_convergence)
+
+
+def solve_forward(device: EFIEDevice, v, solver="direct"):
+    if solver != "direct":
+        raise ValueError("solve_forward: only solver=:direct is provided on the device")
+    x, _ = device.solve_direct(v)
+    return x
+
+
+@dataclass
+class ScatteringResult:
+    I_coeffs: np.ndarray
+    method: str
+    N: int
+    assembly_time_s: float
+    solve_time_s: float
+    preconditioner_time_s: float
+    gmres_iters: int
+    gmres_residual: float
+    true_residual: float = float("nan")
+    warnings: list = field(default_factory=list)
+    timings: dict = field(default_factory=dict)
+
+
+def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
+                     dense_direct_limit: int = 2000, dense_gmres_limit: int = 10000,
+                     gmres_tol: float = 1e-6, gmres_maxiter: int = 300,
+                     check_gmres_convergence: bool = True, nf_cutoff_lambda: float = 1.0,
+                     preconditioner: str = "auto", precond_side: str = "left", quad_order: int = 3,
+                     c0: float = C0_DEFAULT, precision: str = "fp64", surface_impedance=None,
+                     verbose: bool = False, device: EFIEDevice | None = None, rwg: RWGData | None = None):
+    """Workflow.jl:67-317 for the dense methods, on the GPU.
+
+    method: "auto" | "dense_direct" | "dense_gmres".  precision "fp64" is the
+    plain path; "mixed" assembles far pairs in FP32 (complex64 Z) and factors
+    the preconditioner in FP32 while GMRES keeps FP64 Arnoldi and residuals.
+    """
+    f = float(freq_hz)
+    if not (math.isfinite(f) and f > 0):
+        raise ValueError(f"solve_scattering: freq_hz must be finite and positive, got {freq_hz}")
+    if method not in ("auto", "dense_direct", "dense_gmres"):
+        raise ValueError("solve_scattering: method must be :auto, :dense_direct, or :dense_gmres")
+    if preconditioner not in ("auto", "lu", "diag", "none"):
+        raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, or :none")
+    lam = c0 / f
+    k = _frequency_to_wavenumber(f, c0)
+    warnings = []
+    if isinstance(excitation, PlaneWaveExcitation):
+        kn = float(np.linalg.norm(excitation.k_vec))
+        if abs(kn - k) > 1e-8 * k:
+            raise ValueError("solve_scattering: plane-wave |k_vec| must equal 2*pi*freq/c0")
+    if mesh_edge_max(mesh) / lam > 0.1:
+        warnings.append("Mesh under-resolved")
+    rwg = rwg if rwg is not None else build_rwg(mesh)
+    N = rwg.nedges
+    if N < 1:
+        raise ValueError("solve_scattering: mesh produces no RWG unknowns")
+    sel = method
+    if method == "auto":
+        sel = "dense_direct" if N <= dense_direct_limit else "dense_gmres"
+    dev = device or EFIEDevice(mesh, rwg)
+    own = device is None
+    try:
+        if isinstance(excitation, PlaneWaveExcitation):
+            v = dev.plane_wave_rhs(excitation.k_vec[None], [excitation.E0], excitation.pol[None],
+                                   quad_order)[:, 0]
+        else:
+            v = np.asarray(excitation, dtype=np.complex128)
+            if v.shape != (N,):
+                raise nat.DimensionMismatch(f"solve_scattering: excitation length {v.size} != N={N}")
+        t0 = time.perf_counter()
+        dev.assemble(k, quad_order=quad_order, precision=precision)
+        if surface_impedance is not None:
+            dev.apply_impedance(surface_impedance)
+        t_asm = time.perf_counter() - t0
+        t_pc = 0.0
+        iters, resid, tres = -1, float("nan"), float("nan")
+        t1 = time.perf_counter()
+        if sel == "dense_direct":
+            I, berr = dev.solve_direct(v)
+            tres = berr
+        else:
+            pc_used = "lu" if preconditioner == "auto" else preconditioner
+            P = None
+            if pc_used != "none":
+                tp = time.perf_counter()
+                P = dev.build_nearfield(nf_cutoff_lambda * lam, pc_used)
+                t_pc = time.perf_counter() - tp
+            t1 = time.perf_counter()
+            I, st = dev.gmres(v, tol=gmres_tol, maxiter=gmres_maxiter, preconditioner=P,
+                              precond_side=precond_side,
+                              check_gmres_convergence=check_gmres_convergence)
+            iters, resid, tres = st.niter, st.residual, st.true_residual
+        t_solve = time.perf_counter() - t1
+        tm = dev.timings()
+        return ScatteringResult(I_coeffs=np.asarray(I).reshape(N), method=sel, N=N,
+                                assembly_time_s=t_asm, solve_time_s=t_solve,
+                                preconditioner_time_s=t_pc, gmres_iters=iters,
+                                gmres_residual=resid, true_residual=tres, warnings=warnings,
+                                timings={f: getattr(tm, f) for f, _ in nat.Timings._fields_})
+    finally:
+        if own:
+            dev.close()
+
+
+# ---------------------------------------------------------------------------
+# far field / RCS
+# ---------------------------------------------------------------------------
+@dataclass
+class SphGrid:
+    rhat: np.ndarray   # (NO, 3)
+    theta: np.ndarray
+    phi: np.ndarray
+    w: np.ndarray
+
+
+def make_sph_grid(Ntheta: int, Nphi: int) -> SphGrid:
+    """FarField.jl:216-277: midpoint grid in theta and phi."""
+    if Ntheta <= 0 or Nphi <= 0:
+        raise ValueError("Ntheta and Nphi must be positive")
+    dth, dph = math.pi / Ntheta, 2 * math.pi / Nphi
+    th = (np.arange(1, Ntheta + 1) - 0.5) * dth
+    ph = (np.arange(1, Nphi + 1) - 0.5) * dph
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    T, P = T.ravel(), P.ravel()
+    rh = np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], axis=1)
+    return SphGrid(rh, T, P, np.sin(T) * dth * dph)
+
+
+def phi_cut_grid(phi: float, thetas_deg) -> SphGrid:
+    th = np.deg2rad(np.asarray(thetas_deg, dtype=np.float64))
+    rh = np.stack([np.sin(th) * math.cos(phi), np.sin(th) * math.sin(phi), np.cos(th)], axis=1)
+    return SphGrid(rh, th, np.full(th.shape, phi), np.ones(th.shape))
+
+
+def compute_farfield(device: EFIEDevice, grid: SphGrid, I, k=None, eta0=ETA0_DEFAULT, quad_order=3):
+    """E_ff (3 x NO [x nrhs]) = G_mat * I on the device."""
+    return device.farfield(grid.rhat, I, k=k, eta0=eta0, quad_order=quad_order)
+
+
+def bistatic_rcs(E_ff: np.ndarray, E0: float = 1.0) -> np.ndarray:
+    """Diagnostics.jl:460-474: sigma = 4 pi |E_inf|^2 / |E0|^2."""
+    if E_ff.shape[0] != 3:
+        raise nat.DimensionMismatch(f"E_ff has {E_ff.shape[0]} rows, expected 3")
+    return 4 * math.pi * np.sum(np.abs(E_ff) ** 2, axis=0) / abs(E0) ** 2
+
+
+def backscatter_rcs(E_ff: np.ndarray, grid: SphGrid, k_inc_hat, E0: float = 1.0):
+    kh = np.asarray(k_inc_hat, dtype=np.float64)
+    kh = kh / np.linalg.norm(kh)
+    d = grid.rhat @ (-kh)
+    idx = int(np.argmax(d))
+    sig = bistatic_rcs(E_ff[:, idx:idx + 1], E0)[0]
+    return dict(sigma=sig, index=idx, theta=grid.theta[idx], phi=grid.phi[idx],
+                angular_error_deg=math.degrees(math.acos(max(-1.0, min(1.0, d[idx])))))

@@ -1,0 +1,164 @@
+/*
+ * diffmom_b200.h -- C ABI of the B200 library for DiffMoM.jl's dense
+ * surface-EFIE hot path (libdiffmom_b200.so).
+ *
+ * Plain C types only: pointers, sizes, doubles.  Complex arrays are
+ * interleaved (re, im) doubles in Julia's ComplexF64 layout; matrices are
+ * column-major.  Index arrays are Julia's 1-based Int64.  Every entry point
+ * returns a dmb_status; dmb_last_error() holds the message of the last
+ * failure on that context.
+ *
+ * Status codes map onto the Julia exceptions the reference raises:
+ *   DMB_ERR_ARGUMENT   -> ArgumentError      (invalid input, e.g. EFIE.jl:297-330)
+ *   DMB_ERR_OVERFLOW   -> OverflowError      (non-finite results)
+ *   DMB_ERR_DIMENSION  -> DimensionMismatch
+ *   DMB_ERR_BUDGET     -> ArgumentError      (resource limit, Types.jl:85)
+ *   DMB_ERR_NOT_CONVERGED -> ErrorException  (IterativeSolve.jl:50-61)
+ *   DMB_ERR_BREAKDOWN  -> SingularException  (factorisation pivot failure)
+ *   DMB_ERR_CUDA / DMB_ERR_STATE / DMB_ERR_TIMEOUT -> ErrorException
+ *
+ * Thread safety: calls on one context are serialised by a context mutex;
+ * contexts are independent.  All entry points block until their device work
+ * has finished unless stated otherwise.
+ */
+#ifndef DIFFMOM_B200_H
+#define DIFFMOM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dmb_ctx dmb_ctx;
+typedef int dmb_status;
+
+#define DMB_OK 0
+#define DMB_ERR_ARGUMENT 1
+#define DMB_ERR_OVERFLOW 2
+#define DMB_ERR_DIMENSION 3
+#define DMB_ERR_BUDGET 4
+#define DMB_ERR_NOT_CONVERGED 5
+#define DMB_ERR_CUDA 6
+#define DMB_ERR_STATE 7
+#define DMB_ERR_BREAKDOWN 8
+#define DMB_ERR_TIMEOUT 9
+
+/* precision of the impedance matrix */
+#define DMB_PREC_FP64 0  /* FP64 everywhere, complex128 Z */
+#define DMB_PREC_MIXED 1 /* FP32 far pairs, FP64 singular terms, complex64 Z */
+
+/* preconditioner kinds */
+#define DMB_PRECOND_NONE 0
+#define DMB_PRECOND_NF_LU 1      /* near-field matrix, exact factorisation */
+#define DMB_PRECOND_NF_DIAG 2    /* Jacobi on the diagonal, 1e-10*max floor */
+#define DMB_PRECOND_LOCAL_INV 3  /* per-RWG near-block local inverses */
+#define DMB_PRECOND_LEARNED 4    /* learned correction of the local inverses */
+
+#define DMB_SIDE_LEFT 0
+#define DMB_SIDE_RIGHT 1
+
+typedef struct {
+  int32_t niter;        /* Arnoldi steps taken (max over right-hand sides) */
+  int32_t solved;       /* 1 when every right-hand side met the tolerance */
+  double residual;      /* last residual estimate (max over RHS), relative */
+  double true_residual; /* ||b - Z x|| / ||b|| in FP64 (max over RHS) */
+  int32_t restarts;
+  int32_t reserved;
+} dmb_gmres_stats;
+
+typedef struct {
+  double geometry_ms;   /* cache precompute (areas, quadrature, RWG values) */
+  double assembly_ms;   /* impedance matrix assembly */
+  double precond_ms;    /* preconditioner build */
+  double rhs_ms;        /* excitation assembly */
+  double solve_ms;      /* GMRES / direct solve */
+  double nnz_ratio;     /* near-field fill of the last preconditioner */
+  int64_t kernels;      /* kernels launched by this context so far */
+} dmb_timings;
+
+/* ---- context ----------------------------------------------------------- */
+/* No reference counterpart: owns device buffers, stream and error text. */
+dmb_status dmb_ctx_create(int device, dmb_ctx **out);
+dmb_status dmb_ctx_destroy(dmb_ctx *ctx);
+const char *dmb_last_error(const dmb_ctx *ctx);
+dmb_status dmb_get_timings(dmb_ctx *ctx, dmb_timings *out);
+/* Library version string, e.g. "diffmom_b200 0.1 sm_100a". */
+const char *dmb_version(void);
+
+/* ---- mesh and basis ---------------------------------------------------- */
+/* TriMesh (src/Types.jl:123-126): xyz 3 x Nv column-major, tri 3 x Nt
+ * 1-based.  Replaces the host-side cache geometry of _build_efie_cache
+ * (src/assembly/EFIE.jl:332-398). */
+dmb_status dmb_mesh_upload(dmb_ctx *ctx, const double *xyz, const int64_t *tri, int64_t nv,
+                           int64_t nt);
+/* RWGData (src/Types.jl:138-152, built by src/basis/RWG.jl:102-143).
+ * evert is 2 x N column-major 1-based. */
+dmb_status dmb_rwg_upload(dmb_ctx *ctx, int64_t n, const int64_t *tplus, const int64_t *tminus,
+                          const int64_t *evert, const int64_t *vplus_opp,
+                          const int64_t *vminus_opp, const double *len,
+                          const double *area_plus, const double *area_minus);
+
+/* ---- impedance matrix -------------------------------------------------- */
+/* assemble_Z_efie (src/assembly/EFIE.jl:699-753).  Z stays resident on the
+ * device; when Z_out is non-NULL the N x N ComplexF64 matrix is also copied
+ * out (column-major).  precision: DMB_PREC_FP64 or DMB_PREC_MIXED. */
+dmb_status dmb_assemble_z(dmb_ctx *ctx, double k, double eta0, int quad_order, int precision,
+                          double *Z_out);
+/* Copy selected entries of the resident Z (1-based m, n); for efie_entry
+ * (src/assembly/EFIE.jl:1002-1007). */
+dmb_status dmb_z_entries(dmb_ctx *ctx, const int64_t *m, const int64_t *n, int64_t count,
+                         double *out);
+/* Impedance loading Z -= sum_t zs[t] M_t (src/assembly/Impedance.jl:304-408,
+ * src/solver/Solve.jl:1412-1449 with one patch per triangle). zs: Nt complex. */
+dmb_status dmb_apply_impedance(dmb_ctx *ctx, const double *zs);
+
+/* ---- operators --------------------------------------------------------- */
+/* Dense Z*x (the zgemv inside Krylov.gmres) for nrhs column-major
+ * right-hand sides: y = Z x. */
+dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
+/* Matrix-free Z*x (MatrixFreeEFIEOperator mul!, src/assembly/EFIE.jl:867-909):
+ * entries are recomputed from the geometry on every call, nothing of size
+ * N^2 is stored.  Requires a prior dmb_assemble_z or dmb_prepare_operator. */
+dmb_status dmb_prepare_operator(dmb_ctx *ctx, double k, double eta0, int quad_order);
+dmb_status dmb_matvec_free(dmb_ctx *ctx, const double *x, double *y);
+
+/* ---- near-field preconditioner ---------------------------------------- */
+/* build_nearfield_preconditioner(Z, mesh, rwg, cutoff; factorization)
+ * (src/solver/NearFieldPreconditioner.jl:670-758).  kind: DMB_PRECOND_NF_LU
+ * or DMB_PRECOND_NF_DIAG.  nnz_ratio_out may be NULL. */
+dmb_status dmb_nf_build(dmb_ctx *ctx, double cutoff, int kind, double *nnz_ratio_out);
+/* NearFieldOperator apply y = Z_nf^-1 x (NearFieldPreconditioner.jl:1034-1054). */
+dmb_status dmb_nf_apply(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
+
+/* ---- excitation -------------------------------------------------------- */
+/* assemble_plane_wave / assemble_multiple_excitations for R plane waves
+ * (src/assembly/Excitation.jl:2738-2797, 2866-2896).  kvecs, pols: 3 x R
+ * column-major, E0s: R.  V_out: N x R complex column-major. */
+dmb_status dmb_rhs_plane_waves(dmb_ctx *ctx, const double *kvecs, const double *E0s,
+                               const double *pols, int64_t R, int quad_order, double *V_out);
+
+/* ---- solvers ----------------------------------------------------------- */
+/* solve_gmres (src/solver/IterativeSolve.jl:341-392): GMRES without
+ * restart (Krylov.gmres, memory grows), rtol=tol, atol=0, left or right
+ * preconditioner, nrhs independent right-hand sides solved as a block.
+ * rhs, x: N x nrhs column-major.  Returns DMB_ERR_NOT_CONVERGED (x still
+ * written) when check_convergence != 0 and a system did not converge. */
+dmb_status dmb_gmres(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs, double tol,
+                     int maxiter, int precond_kind, int precond_side, int check_convergence,
+                     dmb_gmres_stats *stats);
+/* solve_forward(Z, v; solver=:direct) (src/solver/Solve.jl:1342-1382):
+ * factorisation of the resident Z plus FP64 iterative refinement. */
+dmb_status dmb_solve_direct(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs,
+                            double *backward_error_out);
+
+/* ---- far field --------------------------------------------------------- */
+/* radiation_vectors + compute_farfield (src/postprocessing/FarField.jl:
+ * 425-611): E_out is 3 x NO x nrhs complex for directions rhat (3 x NO). */
+dmb_status dmb_farfield(dmb_ctx *ctx, const double *rhat, int64_t NO, double k, double eta0,
+                        int quad_order, const double *I, int64_t nrhs, double *E_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIFFMOM_B200_H */
