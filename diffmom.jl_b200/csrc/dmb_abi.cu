@@ -80,6 +80,10 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
                       &c->d_flags, &c->d_li_idx, &c->d_li_cnt, &c->d_li_inv, &c->d_net, &c->d_V,
                       &c->d_H, &c->d_work, &c->d_vecs, &c->d_scal};
     for (DevBuf *b : bufs) b->release();
+    c->d_rhs.release();
+    c->d_sol.release();
+    for (auto &e : c->kt_ev)
+      if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
   }
   delete c;
@@ -338,6 +342,74 @@ dmb_status dmb_solve_direct(dmb_ctx *c, const double *rhs, double *x, int64_t nr
     DMB_CUDA(cudaMemcpyAsync(x, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
     if (backward_error_out) *backward_error_out = berr;
+  });
+}
+
+dmb_status dmb_solve_resident(dmb_ctx *c, const dmb_solve_params *p, dmb_gmres_stats *stats) {
+  dmb_gmres_stats st{};
+  dmb_status s = guarded(c, [&] {
+    DMB_REQUIRE(p, DMB_ERR_ARGUMENT, "solve parameters are NULL");
+    DMB_REQUIRE(std::isfinite(p->tol) && p->tol > 0, DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive");
+    DMB_REQUIRE(p->maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
+    check_finite(p->kvec, 3, "plane-wave k_vec");
+    check_finite(p->pol, 3, "plane-wave polarization");
+    double t0 = dmb::now_ms();
+    dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
+    if (p->precond_kind == DMB_PRECOND_NF_LU || p->precond_kind == DMB_PRECOND_NF_DIAG) {
+      DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
+                  "near-field cutoff must be nonnegative and not NaN");
+      dmb::nf_build(c, p->cutoff, p->precond_kind);
+    } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV || p->precond_kind == DMB_PRECOND_LEARNED) {
+      dmb::local_inverse_build(c, p->cutoff, 64);
+    }
+    size_t bytes = sizeof(double2) * c->n;
+    c->d_rhs.ensure(bytes);
+    c->d_sol.ensure(bytes);
+    dmb::rhs_plane_waves_dev(c, p->kvec, &p->E0, p->pol, 1, p->quad_order, c->d_rhs.as<double>());
+    dmb::gmres_dev(c, c->d_rhs.as<double>(), c->d_sol.as<double>(), 1, p->tol, p->maxiter, p->precond_kind,
+                   p->precond_side, &st);
+    c->tm.solve_ms = dmb::now_ms() - t0;
+    if (!st.solved)
+      throw DmbError{DMB_ERR_NOT_CONVERGED, "forward GMRES did not converge: niter=" + std::to_string(st.niter) +
+                                                ", final_residual=" + std::to_string(st.residual)};
+  });
+  if (stats) *stats = st;
+  return s;
+}
+
+dmb_status dmb_copy_solution(dmb_ctx *c, double *I_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(I_out && c->d_sol.p, DMB_ERR_STATE, "no resident solution");
+    DMB_CUDA(cudaMemcpyAsync(I_out, c->d_sol.p, sizeof(double2) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_get_stream(dmb_ctx *c, void **stream_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(stream_out, DMB_ERR_ARGUMENT, "stream output is NULL");
+    *stream_out = (void *)c->stream;
+  });
+}
+
+dmb_status dmb_set_kernel_timing(dmb_ctx *c, int enable) {
+  return guarded(c, [&] {
+    if (!c->kt_ev[0]) {
+      DMB_CUDA(cudaEventCreate(&c->kt_ev[0]));
+      DMB_CUDA(cudaEventCreate(&c->kt_ev[1]));
+    }
+    c->kt_enabled = enable != 0;
+    c->kt_ms = 0;
+    c->kt_flops = 0;
+    c->kt_launches = 0;
+  });
+}
+
+dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *flops) {
+  return guarded(c, [&] {
+    if (ms) *ms = c->kt_ms;
+    if (launches) *launches = c->kt_launches;
+    if (flops) *flops = c->kt_flops;
   });
 }
 

@@ -148,9 +148,16 @@ struct dmb_ctx {
   // GMRES workspace
   DevBuf d_V, d_H, d_work, d_vecs, d_scal;
 
+  // resident solution of dmb_solve_resident
+  DevBuf d_rhs, d_sol;
+
   // timings
   dmb_timings tm{};
   int64_t launches = 0;
+  bool kt_enabled = false;     // dominant-kernel event timing
+  double kt_ms = 0, kt_flops = 0;
+  int64_t kt_launches = 0;
+  cudaEvent_t kt_ev[2] = {nullptr, nullptr};
 };
 
 // ---------------------------------------------------------------------------

@@ -647,7 +647,18 @@ template <class FC> static void ldlt_factor(dmb_ctx *c, FC *F) {
     DMB_LAUNCH(c, k_ldlt_panel<FC>, blocks_for(rest, 8), 256, 0, N, j, b, F, c->d_W.as<double2>());
     int T = (int)((rest + 63) / 64);
     int64_t tiles = (int64_t)T * (T + 1) / 2;
+    if (c->kt_enabled) DMB_CUDA(cudaEventRecord(c->kt_ev[0], c->stream));
     DMB_LAUNCH(c, k_ldlt_update<FC>, (unsigned)tiles, 256, 0, N, j + b, j, b, T, F, c->d_W.as<double2>());
+    if (c->kt_enabled) {
+      DMB_CUDA(cudaEventRecord(c->kt_ev[1], c->stream));
+      DMB_CUDA(cudaEventSynchronize(c->kt_ev[1]));
+      float ms = 0;
+      DMB_CUDA(cudaEventElapsedTime(&ms, c->kt_ev[0], c->kt_ev[1]));
+      c->kt_ms += ms;
+      c->kt_launches++;
+      // algorithmic work: lower triangle (incl. diagonal) x b complex MACs
+      c->kt_flops += 8.0 * (double)b * (double)rest * (double)(rest + 1) / 2.0;
+    }
   }
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));

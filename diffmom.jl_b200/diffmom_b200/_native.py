@@ -83,6 +83,14 @@ class Timings(ctypes.Structure):
                 ("kernels", ctypes.c_int64)]
 
 
+class SolveParams(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_double), ("eta0", ctypes.c_double), ("cutoff", ctypes.c_double),
+                ("tol", ctypes.c_double), ("quad_order", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("precond_kind", ctypes.c_int32), ("precond_side", ctypes.c_int32),
+                ("maxiter", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("kvec", ctypes.c_double * 3), ("pol", ctypes.c_double * 3), ("E0", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _D = ctypes.c_double
 _I = ctypes.c_int
@@ -110,6 +118,11 @@ SIGNATURES = {
     "dmb_gmres": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
     "dmb_solve_direct": ([_P, _DP, _DP, _L, _DP], _I),
     "dmb_farfield": ([_P, _DP, _L, _D, _D, _I, _DP, _L, _DP], _I),
+    "dmb_solve_resident": ([_P, ctypes.POINTER(SolveParams), ctypes.POINTER(GmresStats)], _I),
+    "dmb_copy_solution": ([_P, _DP], _I),
+    "dmb_get_stream": ([_P, ctypes.POINTER(ctypes.c_void_p)], _I),
+    "dmb_set_kernel_timing": ([_P, _I], _I),
+    "dmb_kernel_timing": ([_P, _DP, _LP, _DP], _I),
 }
 
 _lib = None

