@@ -309,3 +309,74 @@ void matvec_free_dev(dmb_ctx *c, const double *x, double *y) {
 }
 
 }  // namespace dmb
+
+// ---------------------------------------------------------------------------
+// Matrix-free product that allocates nothing.
+//
+// Some callers cannot allocate device memory in the middle of a run: codes
+// whose device memory is owned by an external pool (a framework allocator that
+// must see every byte), or fixed-budget solvers that forbid allocation after
+// set-up.  dmb_matvec_free_noalloc serves them: the caller passes device
+// input/output vectors, and the slot-space scratch of the product lives in the
+// file-scope array below instead of per-call cudaMalloc buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocMaxTriangles = 32768;
+// slot-space input (first half) and output (second half): 2 x 3 x max triangles
+// complex128 = 3 MiB, held by every GPU that loads the library until exit.
+static __device__ __align__(256) double2 g_mf_noalloc_scratch[2 * 3 * kNoAllocMaxTriangles];
+
+std::mutex g_noalloc_mu;
+double2 *g_noalloc_addr[64] = {};  // device address of the array, per device ordinal
+
+// Host code must not use g_mf_noalloc_scratch directly (its host-side name is a
+// stand-in, not a device address); look the address up once per device.
+double2 *noalloc_scratch(int device) {
+  DMB_REQUIRE(device >= 0 && device < 64, DMB_ERR_ARGUMENT, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    DMB_CUDA(cudaGetSymbolAddress(&p, g_mf_noalloc_scratch));
+    g_noalloc_addr[device] = static_cast<double2 *>(p);
+  }
+  return g_noalloc_addr[device];
+}
+
+}  // namespace
+
+extern "C" dmb_status dmb_matvec_free_noalloc(dmb_ctx *c, const double *x_dev, double *y_dev) {
+  if (!c) return DMB_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  try {
+    DMB_CUDA(cudaSetDevice(c->device));
+    DMB_REQUIRE(x_dev && y_dev, DMB_ERR_ARGUMENT, "x and y must be device pointers");
+    DMB_REQUIRE(c->cache_valid && c->k != 0.0, DMB_ERR_STATE,
+                "operator not prepared: call dmb_prepare_operator first");
+    DMB_REQUIRE(c->nt <= kNoAllocMaxTriangles, DMB_ERR_BUDGET,
+                "dmb_matvec_free_noalloc supports at most " + std::to_string(kNoAllocMaxTriangles) +
+                    " triangles, mesh has " + std::to_string(c->nt));
+    const int64_t N = c->n, nt = c->nt;
+    double2 *xs = noalloc_scratch(c->device);
+    double2 *ys = xs + 3 * kNoAllocMaxTriangles;
+    // slots without a basis function are never read, but the input half is
+    // cleared so no value of an earlier call can leak into this one
+    DMB_CUDA(cudaMemsetAsync(xs, 0, sizeof(double2) * 3 * nt, c->stream));
+    DMB_LAUNCH(c, k_scatter_slots, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(),
+               (const double2 *)x_dev, xs);
+    DMB_LAUNCH(c, k_mf_far, (unsigned)nt, 256, 0, (int)nt, c->nq, c->d_tcache.as<TriCache>(),
+               c->d_adj_off.as<int>(), c->d_adj_nb.as<int>(), c->k, 1.0 / (c->k * c->k), xs, ys);
+    DMB_LAUNCH(c, k_mf_gather, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(), ys, (double2 *)y_dev);
+    if (c->n_near_entry > 0)
+      DMB_LAUNCH(c, k_mf_near, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
+                 c->d_near_entry_mn.as<int2>(), c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(),
+                 (const double2 *)x_dev, (double2 *)y_dev);
+    DMB_LAUNCH(c, k_times_minus_i_w, blocks_for(N, 256), 256, 0, N, c->k * c->eta0, (double2 *)y_dev);
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    c->err.clear();
+    return DMB_OK;
+  } catch (const DmbError &e) {
+    c->err = e.msg;
+    return e.code;
+  }
+}

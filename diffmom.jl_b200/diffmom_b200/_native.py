@@ -112,6 +112,7 @@ SIGNATURES = {
     "dmb_matvec": ([_P, _DP, _DP, _L], _I),
     "dmb_prepare_operator": ([_P, _D, _D, _I], _I),
     "dmb_matvec_free": ([_P, _DP, _DP], _I),
+    "dmb_matvec_free_noalloc": ([_P, _P, _P], _I),
     "dmb_nf_build": ([_P, _D, _I, _DP], _I),
     "dmb_nf_apply": ([_P, _DP, _DP, _L], _I),
     "dmb_rhs_plane_waves": ([_P, _DP, _DP, _DP, _L, _I, _DP], _I),

@@ -122,6 +122,19 @@ dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
  * N^2 is stored.  Requires a prior dmb_assemble_z or dmb_prepare_operator. */
 dmb_status dmb_prepare_operator(dmb_ctx *ctx, double k, double eta0, int quad_order);
 dmb_status dmb_matvec_free(dmb_ctx *ctx, const double *x, double *y);
+/* No counterpart in the reference.  The same matrix-free product for callers
+ * that cannot allocate device memory mid-run (device memory owned by an
+ * external pool, or a fixed budget that forbids allocation after set-up):
+ * x_dev and y_dev are DEVICE pointers to N complex128 values, and the call
+ * allocates nothing -- its slot-space scratch is a static device array of
+ * 3 MiB held by every GPU that loads the library until exit.  Meshes with more
+ * than 32,768 triangles are rejected with DMB_ERR_BUDGET.  The first call on
+ * a device looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array and
+ * it keeps the last call's contents, so calls that overlap on the GPU (other
+ * contexts or threads on the same device at the same time) race.  Requires a
+ * prior dmb_prepare_operator (or dmb_assemble_z) on the context. */
+dmb_status dmb_matvec_free_noalloc(dmb_ctx *ctx, const double *x_dev, double *y_dev);
 
 /* ---- near-field preconditioner ---------------------------------------- */
 /* build_nearfield_preconditioner(Z, mesh, rwg, cutoff; factorization)
