@@ -139,6 +139,9 @@ def run_ours(args):
         "mixed_nf_lu": params(nat.PREC_MIXED, nat.PRECOND_NF_LU, 1.0 * lam),
     }
     headline = "mixed_nf_lu"
+    if args.only:
+        variants = {args.only: variants[args.only]}
+        headline = args.only
     stream_ptr = ctypes.c_void_p()
     dev.ctx.call("dmb_get_stream", ctypes.byref(stream_ptr))
     ext = torch.cuda.ExternalStream(stream_ptr.value, device=local)
@@ -187,9 +190,13 @@ def run_ours(args):
         launches = dev.timings().kernels - t0
         ms = max_over_ranks(ms)
         per = ms / args.steps
+        tm = dev.timings()
         results[name] = {"solves_per_s": ws * args.steps / (ms / 1e3), "ms_per_step": per,
                          "gmres_iters": iters[-1][0], "true_residual": iters[-1][1],
-                         "kernels_per_step": launches / args.steps}
+                         "kernels_per_step": launches / args.steps,
+                         "stage_ms_last_step": {"geometry": tm.geometry_ms, "assembly": tm.assembly_ms,
+                                                "preconditioner": tm.precond_ms, "rhs": tm.rhs_ms,
+                                                "total": tm.solve_ms}}
         if name == headline:
             results[name]["kernel"] = (kms.value, kl.value, kf.value)
             results[name]["launches"] = launches
@@ -209,19 +216,21 @@ def run_ours(args):
                                nf_cutoff_lambda=1.0, device=dev, rwg=rwg)
         return res
 
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    for _ in range(args.steps):
-        res = e2e_step()
-    e1.record(ext)
-    torch.cuda.synchronize()
-    barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_val = ws * args.steps / (e2e_ms / 1e3)
+    e2e_val = None
+    if not args.skip_e2e:
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(args.steps):
+            res = e2e_step()
+        e1.record(ext)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e_val = ws * args.steps / (e2e_ms / 1e3)
 
     if rank == 0:
         hbm, bf16, src = measured_peaks()
@@ -343,6 +352,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--only", default=None, help="run a single variant (profiling)")
+    ap.add_argument("--skip-e2e", action="store_true", help="omit the e2e leg (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -82,8 +82,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     for (DevBuf *b : bufs) b->release();
     c->d_rhs.release();
     c->d_sol.release();
-    for (auto &e : c->kt_ev)
-      if (e) cudaEventDestroy(e);
+    for (auto &e : c->kt_pool) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
   }
   delete c;
@@ -394,9 +393,11 @@ dmb_status dmb_get_stream(dmb_ctx *c, void **stream_out) {
 
 dmb_status dmb_set_kernel_timing(dmb_ctx *c, int enable) {
   return guarded(c, [&] {
-    if (!c->kt_ev[0]) {
-      DMB_CUDA(cudaEventCreate(&c->kt_ev[0]));
-      DMB_CUDA(cudaEventCreate(&c->kt_ev[1]));
+    kt_collect(c);
+    while (enable && c->kt_pool.size() < 4096) {
+      cudaEvent_t e;
+      DMB_CUDA(cudaEventCreate(&e));
+      c->kt_pool.push_back(e);
     }
     c->kt_enabled = enable != 0;
     c->kt_ms = 0;
@@ -407,6 +408,7 @@ dmb_status dmb_set_kernel_timing(dmb_ctx *c, int enable) {
 
 dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *flops) {
   return guarded(c, [&] {
+    kt_collect(c);
     if (ms) *ms = c->kt_ms;
     if (launches) *launches = c->kt_launches;
     if (flops) *flops = c->kt_flops;

@@ -41,6 +41,37 @@ __host__ __device__ __forceinline__ float2 cdivf(float2 a, float2 b) {
   }
 }
 
+// float2 overloads so templates can use one spelling for both precisions
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cdiv(float2 a, float2 b) { return cdivf(a, b); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+// a += b * c
+__device__ __forceinline__ void cfma(double2 &a, double2 b, double2 c) {
+  a.x = fma(b.x, c.x, a.x);
+  a.x = fma(-b.y, c.y, a.x);
+  a.y = fma(b.x, c.y, a.y);
+  a.y = fma(b.y, c.x, a.y);
+}
+__device__ __forceinline__ void cfma(float2 &a, float2 b, float2 c) {
+  a.x = fmaf(b.x, c.x, a.x);
+  a.x = fmaf(-b.y, c.y, a.x);
+  a.y = fmaf(b.x, c.y, a.y);
+  a.y = fmaf(b.y, c.x, a.y);
+}
+template <class C> __device__ __forceinline__ C czero();
+template <> __device__ __forceinline__ double2 czero<double2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
+template <class C> __device__ __forceinline__ C cone();
+template <> __device__ __forceinline__ double2 cone<double2>() { return make_double2(1.0, 0.0); }
+template <> __device__ __forceinline__ float2 cone<float2>() { return make_float2(1.f, 0.f); }
+__device__ __forceinline__ double cabsv(double2 a) { return hypot(a.x, a.y); }
+__device__ __forceinline__ float cabsv(float2 a) { return hypotf(a.x, a.y); }
+
 // storage conversion
 template <class T> struct CplxOf;
 template <> struct CplxOf<double> { typedef double2 type; };

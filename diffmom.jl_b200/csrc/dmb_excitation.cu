@@ -248,9 +248,8 @@ void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, con
                          int quad_order, double *V_dev) {
   double t0 = now_ms();
   ensure_cache(c, quad_order);
-  DevBuf p;
-  p.ensure(sizeof(double) * 7 * R);
-  double *dk = p.as<double>(), *de = dk + 3 * R, *dp = de + R;
+  c->d_small.ensure(std::max<size_t>(65536, 64 + sizeof(double) * 7 * R));
+  double *dk = (double *)((char *)c->d_small.p + 64), *de = dk + 3 * R, *dp = de + R;
   DMB_CUDA(cudaMemcpyAsync(dk, kvecs, 24 * R, cudaMemcpyHostToDevice, c->stream));
   DMB_CUDA(cudaMemcpyAsync(de, E0s, 8 * R, cudaMemcpyHostToDevice, c->stream));
   DMB_CUDA(cudaMemcpyAsync(dp, pols, 24 * R, cudaMemcpyHostToDevice, c->stream));

@@ -1,0 +1,682 @@
+// dmb_factor.cu -- near-field preconditioner: extraction, factorisation, apply.
+//
+//   * extraction (NearFieldPreconditioner.jl:247-369, 429-464, 670-716):
+//     Z_nf[m][n] = Z[m][n] when the RWG centres are within `cutoff`
+//     (inclusive, exact tie-break), else 0; nnz counted for nnz_ratio.
+//   * Jacobi (:623-668): 1 / z_ii with the 1e-10 * max|z_ii| floor.
+//   * factorisation: Z_nf is complex symmetric (Z is, and the distance test is
+//     symmetric), so it is factored as L D L^T -- unit lower L, diagonal D, no
+//     pivoting -- which has the same inverse as the reference's UMFPACK LU up to
+//     rounding, at half the flops.  Right-looking, panel width NB = 64:
+//       k_ldlt_diag    one CTA factors the 64x64 diagonal block and writes the
+//                      inverse of its unit-lower factor (used twice: by the panel
+//                      and by the triangular solves);
+//       k_ldlt_panel   L21 D1 = A21 L11^-T as a small GEMM with that inverse,
+//                      L21 = (L21 D1) D1^-1, rows in parallel;
+//       k_ldlt_update  trailing update A22 -= (L21 D1) L21^T on lower tiles
+//                      (FP64 SIMT for complex128 factors, FP32 SIMT or the
+//                      tensor-core kernel for complex64 factors).
+//     A zero or non-finite pivot stops with DMB_ERR_BREAKDOWN.
+//   * apply (NearFieldOperator, :1034-1054): L y = x, z = y / D, L^T x = z as
+//     one kernel per sweep.  Each CTA draws a ticket (block row, launch order),
+//     accumulates the contributions of already-solved block rows in registers as
+//     their flags appear, then multiplies by the precomputed inverse of its
+//     diagonal block.  Every wait is bounded: on expiry the kernel sets an error
+//     bit and returns; the host raises DMB_ERR_TIMEOUT.
+#include <algorithm>
+#include <type_traits>
+#include <cmath>
+#include <cstring>
+
+#include "dmb_device.cuh"
+#include "dmb_internal.h"
+
+namespace dmb {
+void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W);
+bool tc_available(dmb_ctx *c);
+}  // namespace dmb
+
+namespace {
+
+constexpr int NB = 64;                      // panel width == triangular-solve block
+constexpr long long SPIN_LIMIT = 20000000;  // ~2-4 s with nanosleep
+
+unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ---------------------------------------------------------------------------
+// near-field extraction
+// ---------------------------------------------------------------------------
+__device__ bool within_cutoff_exact(const double *a, const double *b, double cutoff) {
+  // compare the exact squared distance with cutoff^2 in double-double
+  double s = 0, e = 0;
+  double v[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+  for (int i = 0; i < 3; i++) {
+    double p = v[i] * v[i], pe = fma(v[i], v[i], -p);
+    double t = s + p, bb = t - s;
+    e += (s - (t - bb)) + (p - bb) + pe;
+    s = t;
+  }
+  double c2 = cutoff * cutoff, c2e = fma(cutoff, cutoff, -c2);
+  return (s - c2) + (e - c2e) <= 0.0;
+}
+
+// 32 x 32 tiles; centres staged in shared memory; the squared distance is
+// compared with a band around cutoff^2 and only the band goes to the exact test
+template <class ZC, class FC>
+__global__ void __launch_bounds__(256) k_nf_mask(int64_t N, const ZC *__restrict__ Z, const double *__restrict__ cen,
+                                                 double cutoff, FC *__restrict__ F,
+                                                 unsigned long long *__restrict__ nnz) {
+  __shared__ double cm[32][3], cn[32][3];
+  int64_t m0 = (int64_t)blockIdx.y * 32, n0 = (int64_t)blockIdx.x * 32;
+  int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  if (threadIdx.x < 96) {
+    int i = threadIdx.x / 3, d = threadIdx.x % 3;
+    cm[i][d] = (m0 + i < N) ? cen[3 * (m0 + i) + d] : 0.0;
+    cn[i][d] = (n0 + i < N) ? cen[3 * (n0 + i) + d] : 0.0;
+  }
+  __syncthreads();
+  const bool all_in = !isfinite(cutoff);
+  const double c2 = cutoff * cutoff;
+  const double lo = c2 * (1 - 1e-12), hi = c2 * (1 + 1e-12);
+  unsigned keep_cnt = 0;
+  int64_t n = n0 + tx;
+  for (int i = ty; i < 32; i += 8) {
+    int64_t m = m0 + i;
+    if (m >= N || n >= N) continue;
+    bool keep;
+    if (all_in) keep = true;
+    else if (cutoff <= 0.0) keep = (m == n);
+    else {
+      double dx = cm[i][0] - cn[tx][0], dy = cm[i][1] - cn[tx][1], dz = cm[i][2] - cn[tx][2];
+      double d2 = dx * dx + dy * dy + dz * dz;
+      keep = (m == n) || d2 < lo || (d2 <= hi && within_cutoff_exact(cm[i], cn[tx], cutoff));
+    }
+    store_c(F + m * N + n, keep ? to_d2(Z[m * N + n]) : make_double2(0, 0));
+    keep_cnt += keep;
+  }
+  unsigned cnt = __reduce_add_sync(0xffffffffu, keep_cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(nnz, (unsigned long long)cnt);
+}
+
+template <class ZC>
+__global__ void k_diag_max(int64_t N, const ZC *__restrict__ Z, double *__restrict__ out, unsigned *__restrict__ bad) {
+  __shared__ double red[32];
+  double mx = 0;
+  for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+    double2 z = to_d2(Z[i * N + i]);
+    double a = hypot(z.x, z.y);
+    if (!isfinite(a)) atomicOr(bad, 1u);
+    mx = fmax(mx, a);
+  }
+  mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    mx = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0;
+    mx = warp_max(mx);
+    if (threadIdx.x == 0) *out = mx;
+  }
+}
+
+template <class ZC>
+__global__ void k_diag_inv(int64_t N, const ZC *__restrict__ Z, const double *__restrict__ maxabs,
+                           double2 *__restrict__ dinv) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double floor_abs = 1e-10 * (*maxabs);
+  if (floor_abs == 0.0) floor_abs = 4.9406564584124654e-324;
+  double2 z = to_d2(Z[i * N + i]);
+  if (hypot(z.x, z.y) < floor_abs) z = make_double2(floor_abs, 0);
+  dinv[i] = cdiv(make_double2(1, 0), z);
+}
+
+// ---------------------------------------------------------------------------
+// LDL^T kernels; C is the storage and compute type (double2 or float2)
+// ---------------------------------------------------------------------------
+// Diagonal block: factor in shared memory, write L (strict lower) and D back,
+// and write Linv = L11^-1 (unit lower, b x b, row-major NB stride).
+//
+// 256 threads as 16 x 16; thread (tx, ty) keeps entries (ty + 16p, tx + 16q),
+// p, q in 0..3, in registers.  Step k broadcasts column k through shared
+// memory; the pivot reciprocal is formed once per step.
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
+                                                   C *__restrict__ Linv, unsigned *__restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C(*A)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
+  C *colk = reinterpret_cast<C *>(smem_raw + sizeof(C) * NB * (NB + 1));
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  C a[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; p++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int i = ty + 16 * p, c = tx + 16 * q;
+      a[p][q] = (i < b && c <= i) ? F[(j + i) * N + j + c] : czero<C>();
+    }
+  for (int k = 0; k < b; k++) {
+    const int kq = k >> 4;
+    if (tx == (k & 15)) {
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (q == kq) colk[ty + 16 * p] = a[p][q];
+    }
+    __syncthreads();
+    const C d = colk[k];
+    const double ad = (double)cabsv(d);
+    if (!(ad > 0.0) || !isfinite(ad)) {
+      if (threadIdx.x == 0) atomicOr(err, 2u);
+      return;  // uniform: every thread read the same pivot
+    }
+    const C inv_d = cdiv(cone<C>(), d);
+    C l[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) l[q] = cmul(colk[tx + 16 * q], inv_d);
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const int i = ty + 16 * p;
+      const C ci = colk[i];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int c = tx + 16 * q;
+        if (c > k && c <= i) a[p][q] = csub(a[p][q], cmul(ci, l[q]));
+        if (c == k && i > k) a[p][q] = cmul(ci, inv_d);  // L entry of column k
+      }
+    }
+    __syncthreads();
+  }
+  // write L (strict lower) and D back; keep L in shared memory for the inverse
+#pragma unroll
+  for (int p = 0; p < 4; p++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int i = ty + 16 * p, c = tx + 16 * q;
+      if (i < b && c <= i) F[(j + i) * N + j + c] = a[p][q];
+      A[i][c] = (i < b && c < i) ? a[p][q] : czero<C>();
+    }
+  __syncthreads();
+  // Linv = L^-1 (unit lower): X = I; for k: X[i][:] -= L[i][k] X[k][:], i > k
+  C x[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; p++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) x[p][q] = (ty + 16 * p == tx + 16 * q) ? cone<C>() : czero<C>();
+  for (int k = 0; k < b; k++) {
+    const int kp = k >> 4;
+    if (ty == (k & 15)) {
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (p == kp) colk[tx + 16 * q] = x[p][q];  // row k of X
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const int i = ty + 16 * p;
+      if (i > k) {
+        const C lik = A[i][k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) x[p][q] = csub(x[p][q], cmul(lik, colk[tx + 16 * q]));
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; p++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) Linv[(ty + 16 * p) * NB + tx + 16 * q] = x[p][q];
+}
+
+// Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
+// then L21 = W D^-1.  64 rows per CTA.
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b, C *__restrict__ F,
+                                                    const C *__restrict__ Linv, C *__restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
+  C(*Li)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw + sizeof(C) * NB * (NB + 1));
+  C *dg = reinterpret_cast<C *>(smem_raw + 2 * sizeof(C) * NB * (NB + 1));
+  int64_t r0 = j + b + (int64_t)blockIdx.x * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    int rr = e / NB, k = e % NB;
+    int64_t r = r0 + rr;
+    As[rr][k] = (r < N && k < b) ? F[r * N + j + k] : czero<C>();
+    Li[rr][k] = Linv[rr * NB + k];
+  }
+  if (threadIdx.x < b) dg[threadIdx.x] = F[(j + threadIdx.x) * N + j + threadIdx.x];
+  __syncthreads();
+  int c = threadIdx.x & 63, rq = threadIdx.x >> 6;
+  if (c >= b) return;
+  for (int rr = rq; rr < NB; rr += 4) {
+    int64_t r = r0 + rr;
+    if (r >= N) break;
+    C acc = czero<C>();
+    for (int k = 0; k <= c; k++) cfma(acc, As[rr][k], Li[c][k]);
+    W[r * NB + c] = acc;
+    F[r * N + j + c] = cdiv(acc, dg[c]);
+  }
+}
+
+__device__ __forceinline__ void lower_tile(int64_t t, int &bi, int &bj) {
+  int i = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
+  while ((int64_t)i * (i + 1) / 2 > t) i--;
+  while ((int64_t)(i + 1) * (i + 2) / 2 <= t) i++;
+  bi = i;
+  bj = (int)(t - (int64_t)i * (i + 1) / 2);
+}
+
+// C[r][c] -= sum_k W[r][k] L[c][k]  for r, c >= j0 (lower tiles), SIMT
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t j0, int64_t jcol, int b,
+                                                     C *__restrict__ F, const C *__restrict__ W) {
+  __shared__ C Ws[16][65];
+  __shared__ C Ls[16][65];
+  int bi, bj;
+  lower_tile(blockIdx.x, bi, bj);
+  int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  int64_t r0 = j0 + (int64_t)bi * 64, c0 = j0 + (int64_t)bj * 64;
+  C acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) acc[i][jj] = czero<C>();
+  for (int k0 = 0; k0 < b; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int kk = e & 15, rr = e >> 4;
+      int64_t r = r0 + rr, cc = c0 + rr;
+      bool kin = k0 + kk < b;
+      Ws[kk][rr] = (r < N && kin) ? W[r * NB + k0 + kk] : czero<C>();
+      Ls[kk][rr] = (cc < N && kin) ? F[cc * N + jcol + k0 + kk] : czero<C>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      C a[4], l[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = Ws[kk][ty + 16 * i];
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) l[jj] = Ls[kk][tx + 16 * jj];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) cfma(acc[i][jj], a[i], l[jj]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      int64_t r = r0 + ty + 16 * i, cc = c0 + tx + 16 * jj;
+      if (r < N && cc < N && cc <= r) {
+        C *p = F + r * N + cc;
+        *p = csub(*p, acc[i][jj]);
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ticket-ordered triangular solves (one right-hand side per grid.y)
+// ---------------------------------------------------------------------------
+// wait until flag[cb] is set; return how many consecutive flags from cb on are
+// set (>= 1), or 0 when the wait expired (error bit 4 recorded)
+__device__ int wait_flags(const volatile unsigned *fl, int cb, int limit, unsigned *err) {
+  long long it = 0;
+  while (fl[cb] == 0u) {
+    if (++it > SPIN_LIMIT) {
+      atomicOr(err, 4u);
+      return 0;
+    }
+    if (*((volatile unsigned *)err) & 4u) return 0;
+    __nanosleep(64);
+  }
+  int r = cb + 1;
+  while (r < limit && fl[r] != 0u) r++;
+  return r - cb;
+}
+
+// L y = x (x overwritten), L unit lower.  256 threads = 4 row groups x 64
+// columns; each thread accumulates its 16 rows across all solved block rows in
+// registers.  The L block of the last dependency (block row t-1) and the
+// inverse diagonal block are staged in shared memory before any wait, so the
+// critical path after the last flag is an L2 read of y plus on-chip work.
+template <class FC>
+__global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restrict__ F, const FC *__restrict__ Linv,
+                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC *Lp = reinterpret_cast<FC *>(smem_raw);
+  FC *Li = Lp + NB * NB;
+  __shared__ double2 acc[NB];
+  __shared__ double2 part[2][NB];
+  __shared__ int s_t, s_n;
+  const int nblk = (int)((N + NB - 1) / NB);
+  const int rhs = blockIdx.y;
+  double2 *xr = x + (int64_t)rhs * N;
+  unsigned *fl = flags + (int64_t)rhs * nblk;
+  if (threadIdx.x == 0) s_t = (int)atomicAdd(tickets + rhs, 1u);
+  __syncthreads();
+  const int t = s_t;
+  const int64_t r0 = (int64_t)t * NB;
+  const int bs = (int)(N - r0 < NB ? N - r0 : NB);
+  const int col = threadIdx.x & 63, rg = threadIdx.x >> 6, half = (threadIdx.x >> 5) & 1;
+  // stage Linv_tt and, for t > 0, L[r0.., (t-1)*NB..]
+  const FC *Lit = Linv + (int64_t)t * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += 256) {
+    Li[e] = Lit[e];
+    int row = e >> 6, cc = e & 63;
+    if (t > 0) Lp[e] = row < bs ? F[(r0 + row) * N + (int64_t)(t - 1) * NB + cc] : FC{};
+  }
+  double2 p[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) p[i] = make_double2(0, 0);
+  int cb = 0;
+  while (cb < t - 1) {
+    if (threadIdx.x == 0) s_n = wait_flags(fl, cb, t - 1, err);
+    __syncthreads();
+    const int n = s_n;
+    __syncthreads();
+    if (n == 0) return;
+    __threadfence();
+    for (int q = cb; q < cb + n; q++) {
+      const int64_t c0 = (int64_t)q * NB;
+      const double2 yv = __ldcg(xr + c0 + col);
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        int row = rg + 4 * i;
+        if (row < bs) cfma(p[i], to_d2(F[(r0 + row) * N + c0 + col]), yv);
+      }
+    }
+    cb += n;
+  }
+  if (t > 0) {
+    if (threadIdx.x == 0) s_n = wait_flags(fl, t - 1, t, err);
+    __syncthreads();
+    if (s_n == 0) return;
+    __threadfence();
+    const double2 yv = __ldcg(xr + (int64_t)(t - 1) * NB + col);
+#pragma unroll
+    for (int i = 0; i < 16; i++) cfma(p[i], to_d2(Lp[(rg + 4 * i) * NB + col]), yv);
+  }
+  if (threadIdx.x < NB) acc[threadIdx.x] = threadIdx.x < bs ? xr[r0 + threadIdx.x] : make_double2(0, 0);
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    double2 v = warp_sum2(p[i]);
+    if ((threadIdx.x & 31) == 0) part[half][rg + 4 * i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NB) acc[threadIdx.x] = csub(acc[threadIdx.x], cadd(part[0][threadIdx.x], part[1][threadIdx.x]));
+  __syncthreads();
+  // y_t = Linv_tt acc
+#pragma unroll
+  for (int i = 0; i < 16; i++) p[i] = make_double2(0, 0);
+  const double2 av = acc[col];
+#pragma unroll
+  for (int i = 0; i < 16; i++) cfma(p[i], to_d2(Li[(rg + 4 * i) * NB + col]), av);
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    double2 v = warp_sum2(p[i]);
+    if ((threadIdx.x & 31) == 0) part[half][rg + 4 * i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < bs) xr[r0 + threadIdx.x] = cadd(part[0][threadIdx.x], part[1][threadIdx.x]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicExch(fl + t, 1u);
+}
+
+// L^T x = z (x overwritten), block rows bottom-up; flags indexed by ticket
+// (ticket 0 = last block row).  Thread (rq, col) handles column col of the
+// solved block rows' L entries, rows rq + 4i.  The L block of the last
+// dependency (block row t+1) and Linv_tt are staged before any wait.
+template <class FC>
+__global__ void __launch_bounds__(256) k_trsv_bwd(int64_t N, const FC *__restrict__ F, const FC *__restrict__ Linv,
+                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC *Lp = reinterpret_cast<FC *>(smem_raw);
+  FC *Li = Lp + NB * NB;
+  __shared__ double2 acc[NB];
+  __shared__ double2 part[4][NB];
+  __shared__ int s_t, s_n;
+  const int nblk = (int)((N + NB - 1) / NB);
+  const int rhs = blockIdx.y;
+  double2 *xr = x + (int64_t)rhs * N;
+  unsigned *fl = flags + (int64_t)rhs * nblk;
+  if (threadIdx.x == 0) s_t = (int)atomicAdd(tickets + rhs, 1u);
+  __syncthreads();
+  const int tk = s_t;
+  const int t = nblk - 1 - tk;
+  const int64_t r0 = (int64_t)t * NB;
+  const int bs = (int)(N - r0 < NB ? N - r0 : NB);
+  const int col = threadIdx.x & 63, rq = threadIdx.x >> 6;
+  const FC *Lit = Linv + (int64_t)t * NB * NB;
+  const int64_t cl0 = (int64_t)(t + 1) * NB;  // last dependency block row
+  const int cls = tk > 0 ? (int)(N - cl0 < NB ? N - cl0 : NB) : 0;
+  for (int e = threadIdx.x; e < NB * NB; e += 256) {
+    Li[e] = Lit[e];
+    int r = e >> 6, cc = e & 63;
+    if (tk > 0) Lp[e] = (r < cls && cc < bs) ? F[(cl0 + r) * N + r0 + cc] : FC{};
+  }
+  double2 s = make_double2(0, 0);
+  int q0 = 0;
+  while (q0 < tk - 1) {
+    if (threadIdx.x == 0) s_n = wait_flags(fl, q0, tk - 1, err);
+    __syncthreads();
+    const int n = s_n;
+    __syncthreads();
+    if (n == 0) return;
+    __threadfence();
+    for (int q = q0; q < q0 + n; q++) {
+      const int cb = nblk - 1 - q;
+      const int64_t c0 = (int64_t)cb * NB;
+      const int cbs = (int)(N - c0 < NB ? N - c0 : NB);
+      if (col < bs)
+        for (int r = rq; r < cbs; r += 4) cfma(s, to_d2(F[(c0 + r) * N + r0 + col]), __ldcg(xr + c0 + r));
+    }
+    q0 += n;
+  }
+  if (tk > 0) {
+    if (threadIdx.x == 0) s_n = wait_flags(fl, tk - 1, tk, err);
+    __syncthreads();
+    if (s_n == 0) return;
+    __threadfence();
+    for (int r = rq; r < cls; r += 4) cfma(s, to_d2(Lp[r * NB + col]), __ldcg(xr + cl0 + r));
+  }
+  part[rq][col] = s;
+  if (threadIdx.x < NB) acc[threadIdx.x] = threadIdx.x < bs ? xr[r0 + threadIdx.x] : make_double2(0, 0);
+  __syncthreads();
+  if (threadIdx.x < NB)
+    acc[threadIdx.x] = csub(acc[threadIdx.x], cadd(cadd(part[0][threadIdx.x], part[1][threadIdx.x]),
+                                                   cadd(part[2][threadIdx.x], part[3][threadIdx.x])));
+  __syncthreads();
+  // x_t = Linv_tt^T acc: x[c] = sum_r Linv[r][c] acc[r]
+  s = make_double2(0, 0);
+  for (int r = rq; r < NB; r += 4) cfma(s, to_d2(Li[r * NB + col]), acc[r]);
+  part[rq][col] = s;
+  __syncthreads();
+  if (threadIdx.x < bs)
+    xr[r0 + threadIdx.x] = cadd(cadd(part[0][threadIdx.x], part[1][threadIdx.x]),
+                                cadd(part[2][threadIdx.x], part[3][threadIdx.x]));
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicExch(fl + tk, 1u);
+}
+
+template <class FC>
+__global__ void k_scale_by_dinv(int64_t N, int64_t R, const FC *__restrict__ F, double2 *__restrict__ x) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * R) return;
+  int64_t n = i % N;
+  x[i] = cdiv(x[i], to_d2(F[n * N + n]));
+}
+
+__global__ void k_scale_vec(int64_t N, int64_t R, const double2 *__restrict__ d, double2 *__restrict__ x) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * R) return;
+  x[i] = cmul(x[i], d[i % N]);
+}
+
+template <class C> void set_smem_attrs() {
+  static bool done = false;
+  if (done) return;
+  size_t diag = sizeof(C) * (NB * (NB + 1) + NB);
+  size_t panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
+  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_diag<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag));
+  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
+  DMB_CUDA(cudaFuncSetAttribute(k_trsv_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * sizeof(C) * NB * NB)));
+  DMB_CUDA(cudaFuncSetAttribute(k_trsv_bwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * sizeof(C) * NB * NB)));
+  done = true;
+}
+
+template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
+  const int64_t N = c->n;
+  set_smem_attrs<C>();
+  const int nblk = (int)((N + NB - 1) / NB);
+  c->d_W.ensure(sizeof(C) * N * NB);
+  c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
+  c->d_flags.ensure(64);
+  unsigned *err = c->d_flags.as<unsigned>();
+  C *W = c->d_W.as<C>();
+  C *Linv = c->d_dinv.as<C>();
+  DMB_CUDA(cudaMemsetAsync(err, 0, 4, c->stream));
+  const size_t sm_diag = sizeof(C) * (NB * (NB + 1) + NB);
+  const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
+  const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
+  for (int64_t j = 0; j < N; j += NB) {
+    int b = (int)std::min<int64_t>(NB, N - j);
+    C *Lblk = Linv + (j / NB) * NB * NB;
+    DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
+    int64_t rest = N - j - b;
+    if (rest <= 0) break;
+    DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W);
+    kt_begin(c);
+    if (use_tc) {
+      dmb::tc_ldlt_update_c64(c, N, j + b, j, b, (float2 *)F, (const float2 *)W);
+    } else {
+      int T = (int)((rest + 63) / 64);
+      int64_t tiles = (int64_t)T * (T + 1) / 2;
+      DMB_LAUNCH(c, k_ldlt_update<C>, (unsigned)tiles, 256, 0, N, j + b, j, b, F, W);
+    }
+    // algorithmic work: lower triangle (incl. diagonal) x b complex MACs
+    kt_end(c, 8.0 * (double)b * (double)rest * (double)(rest + 1) / 2.0);
+  }
+  unsigned h_err = 0;
+  DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  DMB_REQUIRE(h_err == 0, DMB_ERR_BREAKDOWN, "near-field factorisation broke down: zero or non-finite pivot");
+}
+
+template <class C> void ldlt_solve(dmb_ctx *c, const C *F, double2 *x, int64_t R) {
+  const int64_t N = c->n;
+  const int nblk = (int)((N + NB - 1) / NB);
+  const size_t flag_words = (size_t)R * nblk + R;
+  c->d_flags.ensure(std::max<size_t>(64, 4 * (flag_words + 2)));
+  unsigned *err = c->d_flags.as<unsigned>();
+  unsigned *tickets = err + 1;
+  unsigned *flags = tickets + R;
+  const C *Linv = c->d_dinv.as<C>();
+  dim3 g(nblk, (unsigned)R);
+  DMB_CUDA(cudaMemsetAsync(err, 0, 4 * (flag_words + 1), c->stream));
+  set_smem_attrs<C>();
+  const size_t sm = 2 * sizeof(C) * NB * NB;
+  DMB_LAUNCH(c, k_trsv_fwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err);
+  DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, x);
+  DMB_CUDA(cudaMemsetAsync(tickets, 0, 4 * flag_words, c->stream));
+  DMB_LAUNCH(c, k_trsv_bwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err);
+}
+
+}  // namespace
+
+namespace dmb {
+
+unsigned read_err_word(dmb_ctx *c) {
+  unsigned e = 0;
+  DMB_CUDA(cudaMemcpyAsync(&e, c->d_flags.p, 4, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  return e;
+}
+
+void nf_build(dmb_ctx *c, double cutoff, int kind) {
+  double t0 = now_ms();
+  const int64_t N = c->n;
+  const bool f64 = c->z_prec == DMB_PREC_FP64;
+  c->pc_valid = false;
+  if (kind == DMB_PRECOND_NF_DIAG) {
+    DevBuf tmp;
+    tmp.ensure(16);
+    DMB_CUDA(cudaMemsetAsync(tmp.p, 0, 16, c->stream));
+    c->d_dinv.ensure(sizeof(double2) * N);
+    unsigned *bad = (unsigned *)(tmp.as<double>() + 1);
+    if (f64) {
+      DMB_LAUNCH(c, k_diag_max<double2>, 1, 1024, 0, N, c->d_Z.as<double2>(), tmp.as<double>(), bad);
+      DMB_LAUNCH(c, k_diag_inv<double2>, blocks_for(N, 256), 256, 0, N, c->d_Z.as<double2>(), tmp.as<double>(),
+                 c->d_dinv.as<double2>());
+    } else {
+      DMB_LAUNCH(c, k_diag_max<float2>, 1, 1024, 0, N, c->d_Z.as<float2>(), tmp.as<double>(), bad);
+      DMB_LAUNCH(c, k_diag_inv<float2>, blocks_for(N, 256), 256, 0, N, c->d_Z.as<float2>(), tmp.as<double>(),
+                 c->d_dinv.as<double2>());
+    }
+    double mx[2];
+    DMB_CUDA(cudaMemcpyAsync(mx, tmp.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    unsigned hb;
+    memcpy(&hb, &mx[1], 4);
+    DMB_REQUIRE(hb == 0, DMB_ERR_ARGUMENT, "near-field diagonal entries must be finite");
+    DMB_REQUIRE(mx[0] > 0, DMB_ERR_ARGUMENT, "cannot build a diagonal preconditioner from an all-zero diagonal");
+    c->nnz_ratio = 1.0 / (double)N;
+    c->pc_kind = kind;
+    c->pc_prec = c->z_prec;
+    c->pc_valid = true;
+    c->tm.precond_ms = now_ms() - t0;
+    return;
+  }
+  size_t esz = f64 ? sizeof(double2) : sizeof(float2);
+  c->d_F.ensure(esz * N * N);
+  c->d_small.ensure(65536);
+  DevBuf cnt;  // view into the persistent scratch (first 8 bytes), not owned
+  cnt.p = c->d_small.p;
+  DMB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, c->stream));
+  dim3 g(blocks_for(N, 32), blocks_for(N, 32));
+  if (f64)
+    DMB_LAUNCH(c, (k_nf_mask<double2, double2>), g, 256, 0, N, c->d_Z.as<double2>(), c->d_centers.as<double>(),
+               cutoff, c->d_F.as<double2>(), cnt.as<unsigned long long>());
+  else
+    DMB_LAUNCH(c, (k_nf_mask<float2, float2>), g, 256, 0, N, c->d_Z.as<float2>(), c->d_centers.as<double>(),
+               cutoff, c->d_F.as<float2>(), cnt.as<unsigned long long>());
+  unsigned long long h_cnt = 0;
+  DMB_CUDA(cudaMemcpyAsync(&h_cnt, cnt.p, 8, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  c->nnz_ratio = ((double)h_cnt / (double)N) / (double)N;
+  if (f64)
+    ldlt_factor(c, c->d_F.as<double2>());
+  else
+    ldlt_factor(c, c->d_F.as<float2>());
+  c->pc_kind = kind;
+  c->pc_prec = c->z_prec;
+  c->pc_valid = true;
+  c->tm.precond_ms = now_ms() - t0;
+}
+
+void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs) {
+  DMB_REQUIRE(c->pc_valid, DMB_ERR_STATE, "no preconditioner built");
+  const int64_t N = c->n;
+  double2 *xd = (double2 *)x;
+  if (c->pc_kind == DMB_PRECOND_NF_DIAG) {
+    DMB_LAUNCH(c, k_scale_vec, blocks_for(N * nrhs, 256), 256, 0, N, nrhs, c->d_dinv.as<double2>(), xd);
+    return;
+  }
+  if (c->pc_kind == DMB_PRECOND_NF_LU) {
+    if (c->pc_prec == DMB_PREC_FP64)
+      ldlt_solve(c, c->d_F.as<double2>(), xd, nrhs);
+    else
+      ldlt_solve(c, c->d_F.as<float2>(), xd, nrhs);
+    return;
+  }
+  throw DmbError{DMB_ERR_STATE, "preconditioner kind not available"};
+}
+
+}  // namespace dmb

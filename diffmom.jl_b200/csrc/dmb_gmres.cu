@@ -234,11 +234,19 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   DMB_REQUIRE(precond_kind == DMB_PRECOND_NONE || precond_kind == c->pc_kind, DMB_ERR_STATE,
               "requested preconditioner kind differs from the one built");
   // basis capacity: maxiter vectors, bounded by a 40% share of free memory
-  size_t freeb = 0, totb = 0;
-  DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
+  // (decided once per problem shape; repeated solves reuse the buffers)
   size_t vec_bytes = sizeof(double2) * N * R;
-  int64_t cap_mem = (int64_t)((freeb * 0.4) / vec_bytes) - 1;
-  int kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
+  if (!(c->gm_key_n == N && c->gm_key_r == R && c->gm_key_maxiter == maxiter && c->gm_kcap > 0)) {
+    size_t freeb = 0, totb = 0;
+    DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
+    freeb += c->d_V.bytes;  // the current basis can be reused
+    int64_t cap_mem = (int64_t)((freeb * 0.4) / vec_bytes) - 1;
+    c->gm_kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
+    c->gm_key_n = N;
+    c->gm_key_r = R;
+    c->gm_key_maxiter = maxiter;
+  }
+  const int kcap = c->gm_kcap;
   const int64_t vstride = N * R;
   c->d_V.ensure(vec_bytes * (kcap + 1));
   c->d_work.ensure(vec_bytes * 2);

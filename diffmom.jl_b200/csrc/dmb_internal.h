@@ -150,6 +150,12 @@ struct dmb_ctx {
 
   // resident solution of dmb_solve_resident
   DevBuf d_rhs, d_sol;
+  // small persistent scratch (counters, plane-wave parameters): the solve path
+  // allocates nothing after its first call
+  DevBuf d_small;
+  int gm_kcap = 0;              // cached GMRES basis capacity
+  int64_t gm_key_n = 0, gm_key_r = 0;
+  int gm_key_maxiter = 0;
 
   // timings
   dmb_timings tm{};
@@ -157,8 +163,44 @@ struct dmb_ctx {
   bool kt_enabled = false;     // dominant-kernel event timing
   double kt_ms = 0, kt_flops = 0;
   int64_t kt_launches = 0;
-  cudaEvent_t kt_ev[2] = {nullptr, nullptr};
+  std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
+  std::vector<double> kt_pending;     // algorithmic flops of each recorded launch
+  size_t kt_used = 0;
 };
+
+// Bracket one launch of the dominant kernel with events from a pre-created
+// pool (no host synchronisation inside the timed region).
+inline void kt_begin(dmb_ctx *c) {
+  if (!c->kt_enabled) return;
+  if (c->kt_used + 2 > c->kt_pool.size()) {
+    for (int i = 0; i < 256; i++) {
+      cudaEvent_t e;
+      DMB_CUDA(cudaEventCreate(&e));
+      c->kt_pool.push_back(e);
+    }
+  }
+  DMB_CUDA(cudaEventRecord(c->kt_pool[c->kt_used], c->stream));
+}
+inline void kt_end(dmb_ctx *c, double flops) {
+  if (!c->kt_enabled) return;
+  DMB_CUDA(cudaEventRecord(c->kt_pool[c->kt_used + 1], c->stream));
+  c->kt_used += 2;
+  c->kt_pending.push_back(flops);
+}
+// fold the recorded pairs into the totals (synchronises the stream)
+inline void kt_collect(dmb_ctx *c) {
+  if (c->kt_used == 0) return;
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i + 1 < c->kt_used; i += 2) {
+    float ms = 0;
+    DMB_CUDA(cudaEventElapsedTime(&ms, c->kt_pool[i], c->kt_pool[i + 1]));
+    c->kt_ms += ms;
+    c->kt_launches++;
+    c->kt_flops += c->kt_pending[i / 2];
+  }
+  c->kt_used = 0;
+  c->kt_pending.clear();
+}
 
 // ---------------------------------------------------------------------------
 // helpers shared by translation units
