@@ -99,6 +99,17 @@ dmb_status dmb_get_timings(dmb_ctx *c, dmb_timings *out) {
   });
 }
 
+dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
+  return guarded(c, [&] {
+    if (option == DMB_OPT_TENSOR_CORES) {
+      c->use_tensor_cores = value != 0;
+      c->pc_valid = false;
+      return;
+    }
+    throw DmbError{DMB_ERR_ARGUMENT, "unknown option " + std::to_string(option)};
+  });
+}
+
 dmb_status dmb_mesh_upload(dmb_ctx *c, const double *xyz, const int64_t *tri, int64_t nv, int64_t nt) {
   return guarded(c, [&] {
     DMB_REQUIRE(xyz && tri, DMB_ERR_ARGUMENT, "mesh arrays must be non-NULL");

@@ -34,6 +34,7 @@
 namespace dmb {
 void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W);
 bool tc_available(dmb_ctx *c);
+unsigned tc_error_word(dmb_ctx *c);
 }  // namespace dmb
 
 namespace {
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
 // then L21 = W D^-1.  64 rows per CTA.
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b, C *__restrict__ F,
-                                                    const C *__restrict__ Linv, C *__restrict__ W) {
+                                                    const C *__restrict__ Linv, C *__restrict__ W, int wstride,
+                                                    int woff) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
   C(*Li)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw + sizeof(C) * NB * (NB + 1));
@@ -255,41 +257,35 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b,
     if (r >= N) break;
     C acc = czero<C>();
     for (int k = 0; k <= c; k++) cfma(acc, As[rr][k], Li[c][k]);
-    W[r * NB + c] = acc;
+    W[r * wstride + woff + c] = acc;
     F[r * N + j + c] = cdiv(acc, dg[c]);
   }
 }
 
-__device__ __forceinline__ void lower_tile(int64_t t, int &bi, int &bj) {
-  int i = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) / 2.0);
-  while ((int64_t)i * (i + 1) / 2 > t) i--;
-  while ((int64_t)(i + 1) * (i + 2) / 2 <= t) i++;
-  bi = i;
-  bj = (int)(t - (int64_t)i * (i + 1) / 2);
-}
-
-// C[r][c] -= sum_k W[r][k] L[c][k]  for r, c >= j0 (lower tiles), SIMT
+// C[r][c] -= sum_{k<K} W[r][woff+k] F[c][jcol+k]  for c in [r_lo, c_hi), r >= c,
+// r < N (SIMT, 64 x 64 tiles; grid.x row tiles, grid.y column tiles; tiles
+// entirely above the diagonal exit at once)
 template <class C>
-__global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t j0, int64_t jcol, int b,
-                                                     C *__restrict__ F, const C *__restrict__ W) {
+__global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, int64_t c_hi, int64_t jcol, int K,
+                                                     C *__restrict__ F, const C *__restrict__ W, int wstride,
+                                                     int woff) {
   __shared__ C Ws[16][65];
   __shared__ C Ls[16][65];
-  int bi, bj;
-  lower_tile(blockIdx.x, bi, bj);
+  const int64_t r0 = r_lo + (int64_t)blockIdx.x * 64, c0 = r_lo + (int64_t)blockIdx.y * 64;
+  if (r0 >= N || c0 >= c_hi || c0 > r0 + 63) return;
   int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  int64_t r0 = j0 + (int64_t)bi * 64, c0 = j0 + (int64_t)bj * 64;
   C acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int jj = 0; jj < 4; jj++) acc[i][jj] = czero<C>();
-  for (int k0 = 0; k0 < b; k0 += 16) {
+  for (int k0 = 0; k0 < K; k0 += 16) {
     for (int e = threadIdx.x; e < 16 * 64; e += 256) {
       int kk = e & 15, rr = e >> 4;
       int64_t r = r0 + rr, cc = c0 + rr;
-      bool kin = k0 + kk < b;
-      Ws[kk][rr] = (r < N && kin) ? W[r * NB + k0 + kk] : czero<C>();
-      Ls[kk][rr] = (cc < N && kin) ? F[cc * N + jcol + k0 + kk] : czero<C>();
+      bool kin = k0 + kk < K;
+      Ws[kk][rr] = (r < N && kin) ? W[r * wstride + woff + k0 + kk] : czero<C>();
+      Ls[kk][rr] = (cc < c_hi && kin) ? F[cc * N + jcol + k0 + kk] : czero<C>();
     }
     __syncthreads();
 #pragma unroll
@@ -311,7 +307,7 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t j0, int6
 #pragma unroll
     for (int jj = 0; jj < 4; jj++) {
       int64_t r = r0 + ty + 16 * i, cc = c0 + tx + 16 * jj;
-      if (r < N && cc < N && cc <= r) {
+      if (r < N && cc < c_hi && cc <= r) {
         C *p = F + r * N + cc;
         *p = csub(*p, acc[i][jj]);
       }
@@ -532,11 +528,19 @@ template <class C> void set_smem_attrs() {
   done = true;
 }
 
+// Two-level right-looking LDL^T.  Block columns of NBO = 256 are factored as
+// four 64-wide panels whose updates stay inside the block column (narrow SIMT
+// strips); the rest of the trailing matrix then receives ONE update with
+// K = 256 -- on the tensor cores for complex64 factors.  This keeps the big
+// update compute-dominated and reads/writes the trailing matrix once per 256
+// columns instead of once per 64.
+constexpr int NBO = 256;
+
 template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const int64_t N = c->n;
   set_smem_attrs<C>();
   const int nblk = (int)((N + NB - 1) / NB);
-  c->d_W.ensure(sizeof(C) * N * NB);
+  c->d_W.ensure(sizeof(C) * N * NBO);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   c->d_flags.ensure(64);
   unsigned *err = c->d_flags.as<unsigned>();
@@ -546,28 +550,39 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const size_t sm_diag = sizeof(C) * (NB * (NB + 1) + NB);
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
-  for (int64_t j = 0; j < N; j += NB) {
-    int b = (int)std::min<int64_t>(NB, N - j);
-    C *Lblk = Linv + (j / NB) * NB * NB;
-    DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
-    int64_t rest = N - j - b;
+  for (int64_t J = 0; J < N; J += NBO) {
+    const int64_t JB = std::min<int64_t>(NBO, N - J);
+    for (int64_t j = J; j < J + JB; j += NB) {
+      const int b = (int)std::min<int64_t>(NB, N - j);
+      C *Lblk = Linv + (j / NB) * NB * NB;
+      DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
+      const int64_t rest = N - j - b;
+      if (rest <= 0) break;
+      DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W, NBO, (int)(j - J));
+      const int64_t c_hi = J + JB;  // strip update inside the block column
+      if (j + b < c_hi) {
+        dim3 g(blocks_for(rest, 64), blocks_for(c_hi - (j + b), 64));
+        DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, c_hi, j, b, F, W, NBO, (int)(j - J));
+      }
+    }
+    const int64_t r_lo = J + JB, rest = N - r_lo;
     if (rest <= 0) break;
-    DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W);
     kt_begin(c);
     if (use_tc) {
-      dmb::tc_ldlt_update_c64(c, N, j + b, j, b, (float2 *)F, (const float2 *)W);
+      dmb::tc_ldlt_update_c64(c, N, r_lo, J, (int)JB, (float2 *)F, (const float2 *)W);
     } else {
-      int T = (int)((rest + 63) / 64);
-      int64_t tiles = (int64_t)T * (T + 1) / 2;
-      DMB_LAUNCH(c, k_ldlt_update<C>, (unsigned)tiles, 256, 0, N, j + b, j, b, F, W);
+      dim3 g(blocks_for(rest, 64), blocks_for(rest, 64));
+      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r_lo, N, J, (int)JB, F, W, NBO, 0);
     }
-    // algorithmic work: lower triangle (incl. diagonal) x b complex MACs
-    kt_end(c, 8.0 * (double)b * (double)rest * (double)(rest + 1) / 2.0);
+    // algorithmic work: lower triangle (incl. diagonal) x JB complex MACs
+    kt_end(c, 8.0 * (double)JB * (double)rest * (double)(rest + 1) / 2.0);
   }
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   DMB_REQUIRE(h_err == 0, DMB_ERR_BREAKDOWN, "near-field factorisation broke down: zero or non-finite pivot");
+  if (use_tc)
+    DMB_REQUIRE(dmb::tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core update: a pipeline wait expired");
 }
 
 template <class C> void ldlt_solve(dmb_ctx *c, const C *F, double2 *x, int64_t R) {

@@ -153,6 +153,7 @@ struct dmb_ctx {
   // small persistent scratch (counters, plane-wave parameters): the solve path
   // allocates nothing after its first call
   DevBuf d_small;
+  bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
   int gm_kcap = 0;              // cached GMRES basis capacity
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;

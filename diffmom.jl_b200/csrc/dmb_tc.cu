@@ -1,15 +1,376 @@
-// dmb_tc.cu -- tensor-core (tcgen05) kernels.  Placeholder until the sm_100a
-// 3xTF32 complex update lands: reports no tensor-core path.
+// dmb_tc.cu -- tensor-core (tcgen05, sm_100a) trailing update of the complex64
+// near-field factorisation:  C -= W L^T  on the lower tiles of the trailing
+// matrix, W = L21 D1 and L = L21 (both rows >= j0, 64 complex columns).
+//
+// Precision: 3xTF32.  Each FP32 value x is split into hi = tf32(x) and
+// lo = tf32(x - hi); the product keeps hi*hi + hi*lo + lo*hi (~21-22 bit
+// accurate per term, FP32 accumulation in TMEM).
+//
+// Complex as one real GEMM.  With A' = [[Wr, -Wi], [Wi, Wr]] (2M x 128) and
+// B' = [Lr, Li] (N x 128), A' B'^T = [C_re; C_im].  The 3xTF32 split stacks
+// along K:  A'' = [A'hi, A'hi, A'lo],  B'' = [B'hi, B'lo, B'hi],  K = 384.
+// k_tc_pack writes A'' so that every 64 complex rows occupy 128 consecutive
+// rows (64 real-part rows, then 64 imaginary-part rows): one M = 128 UMMA tile
+// therefore holds both parts of 64 complex rows, and the epilogue writes
+// interleaved complex64 directly.
+//
+// Kernel k_tc_syrk (one CTA = 4 warps per 64 x 256 complex output tile):
+//   warp 0 / lane 0   TMA producer, 4-stage ring of 128-B-swizzled K chunks
+//                     (A 128 x 32 floats, B 256 x 32 floats per stage);
+//   warp 1 / lane 0   issues tcgen05.mma.cta_group::1.kind::tf32
+//                     (M 128, N 256, K 8) into a 256-column TMEM accumulator,
+//                     tcgen05.commit frees each stage and finally signals done;
+//   all 4 warps       tcgen05.ld the accumulator (warp w owns lanes 32w..),
+//                     stage through shared memory, C -= acc on c <= r.
+// No TMA multicast, no clusters.  Every mbarrier wait is bounded: on expiry
+// the kernel records an error bit, stops issuing, frees its TMEM and returns.
+#include <cuda.h>
+
+#include <cstring>
+
 #include "dmb_device.cuh"
 #include "dmb_internal.h"
 
-namespace dmb {
-bool tc_available(dmb_ctx *c) {
-  (void)c;
+namespace {
+
+constexpr int TC_BM = 128;                 // real rows per tile (64 complex rows)
+constexpr int TC_BN = 256;                 // complex columns per tile
+constexpr int TC_BK = 32;                  // floats per stage (one 128-B swizzle row)
+constexpr int TC_KC = 256;                 // complex K of one update (block column width)
+constexpr int TC_K = 6 * TC_KC;            // 3 (split) x 2 (re/im) x 256 = 1536
+constexpr int TC_STAGES = 4;
+constexpr int TC_KCHUNKS = TC_K / TC_BK;   // 12
+constexpr int TC_A_STAGE = TC_BM * TC_BK * 4;  // 16 KB
+constexpr int TC_B_STAGE = TC_BN * TC_BK * 4;  // 32 KB
+constexpr int TC_SMEM = TC_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 /*barriers*/ + 1024 /*align*/;
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// bounded wait for the phase with the given parity; false on expiry
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned *err, volatile int *abort) {
+  for (long long it = 0; it < TC_WAIT_LIMIT; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 1023) == 1023 && *abort) return false;
+  }
+  atomicOr(err, 8u);
+  *abort = 1;
   return false;
 }
-void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W) {
-  (void)c; (void)N; (void)j0; (void)jcol; (void)b; (void)F; (void)W;
-  throw DmbError{DMB_ERR_STATE, "tensor-core update not available"};
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
 }
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups of
+// 1024 B (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset
+  d |= (uint64_t)1 << 46;             // descriptor version
+  d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------------------
+// operand packing: rows m in [0, rest) relative to j0
+//   A'' real row (128*(m/64) + m%64):      [Wr_h, -Wi_h, Wr_h, -Wi_h, Wr_l, -Wi_l]
+//   A'' imag row (128*(m/64) + 64 + m%64): [Wi_h,  Wr_h, Wi_h,  Wr_h, Wi_l,  Wr_l]
+//   B'' row m:                             [Lr_h,  Li_h, Lr_l,  Li_l, Lr_h,  Li_h]
+// columns k >= b are zero.
+// ---------------------------------------------------------------------------
+__global__ void k_tc_pack(int64_t rest, int64_t N, int64_t j0, int64_t jcol, int b, const float2 *__restrict__ F,
+                          const float2 *__restrict__ W, float *__restrict__ Ap, float *__restrict__ Bp) {
+  int64_t m = blockIdx.x;
+  int k = threadIdx.x;  // TC_KC threads
+  if (m >= rest) return;
+  float2 w = make_float2(0.f, 0.f), l = make_float2(0.f, 0.f);
+  if (k < b) {
+    w = W[(j0 + m) * TC_KC + k];
+    l = F[(j0 + m) * N + jcol + k];
+  }
+  float wrh = tf32_rna(w.x), wih = tf32_rna(w.y);
+  float wrl = tf32_rna(w.x - wrh), wil = tf32_rna(w.y - wih);
+  float lrh = tf32_rna(l.x), lih = tf32_rna(l.y);
+  float lrl = tf32_rna(l.x - lrh), lil = tf32_rna(l.y - lih);
+  int64_t bi = m / 64, r = m % 64;
+  float *ar = Ap + (128 * bi + r) * TC_K;
+  float *ai = Ap + (128 * bi + 64 + r) * TC_K;
+  float *br = Bp + m * TC_K;
+  const int S = TC_KC;
+  ar[k] = wrh; ar[S + k] = -wih; ar[2 * S + k] = wrh; ar[3 * S + k] = -wih; ar[4 * S + k] = wrl; ar[5 * S + k] = -wil;
+  ai[k] = wih; ai[S + k] = wrh;  ai[2 * S + k] = wih; ai[3 * S + k] = wrh;  ai[4 * S + k] = wil; ai[5 * S + k] = wrl;
+  br[k] = lrh; br[S + k] = lih;  br[2 * S + k] = lrl; br[3 * S + k] = lil;  br[4 * S + k] = lrh; br[5 * S + k] = lih;
+}
+
+__global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
+                                                    const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
+                                                    int64_t N, int64_t j0, int64_t rest, unsigned *err) {
+  // grid.x walks row blocks fastest, so CTAs running together share the
+  // column block's B operand in L2
+  const int64_t row0 = (int64_t)blockIdx.x * 64;   // complex rows of the tile (relative to j0)
+  const int64_t col0 = (int64_t)blockIdx.y * TC_BN;
+  if (row0 >= rest || col0 > row0 + 63) return;  // uniform: tile outside the lower triangle
+
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char *gbase = smem_raw + (base - raw);
+  const uint32_t sA = base;                                  // TC_STAGES x 16 KB
+  const uint32_t sB = base + TC_STAGES * TC_A_STAGE;         // TC_STAGES x 32 KB
+  const uint32_t sBar = sB + TC_STAGES * TC_B_STAGE;         // full[4], empty[4], done
+  uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
+  volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * TC_STAGES, done = sBar + 16 * TC_STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(const_cast<uint32_t *>(tmem_slot))),
+                 "r"(TC_BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // TMA producer
+    for (int kc = 0; kc < TC_KCHUNKS; kc++) {
+      const int s = kc % TC_STAGES;
+      if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
+      mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
+      tma_load_2d(sA + s * TC_A_STAGE, &tmA, kc * TC_BK, (int)(2 * row0), full0 + 8 * s);
+      tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    bool ok = true;
+    for (int kc = 0; kc < TC_KCHUNKS && ok; kc++) {
+      const int s = kc % TC_STAGES;
+      if (!mbar_wait(full0 + 8 * s, (kc / TC_STAGES) & 1, err, abort_flag)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int k = 0; k < TC_BK / 8; k++) {
+        const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
+        const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
+        umma_tf32(tmem_d, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+      }
+      umma_commit(empty0 + 8 * s);
+    }
+    if (ok) umma_commit(done);
+  }
+  __syncwarp();
+
+  // epilogue (the decision to write back is made uniformly for the CTA)
+  const int have = __syncthreads_and(mbar_wait(done, 0, err, abort_flag) ? 1 : 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (have) {
+    float *E = reinterpret_cast<float *>(gbase);  // 128 x 33 staging (pipeline buffers are idle now)
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    for (int cc = 0; cc < TC_BN / 32; cc++) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(tmem_d + lane_base + (uint32_t)(cc * 32)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int row = warp * 32 + lane;
+#pragma unroll
+      for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
+      __syncthreads();
+      // thread -> (complex row r = rr + 4i, column q)
+      const int q = threadIdx.x & 31, rr = threadIdx.x >> 5;
+      const int64_t gc = j0 + col0 + cc * 32 + q;
+#pragma unroll 4
+      for (int i = 0; i < 16; i++) {
+        const int r = rr + 4 * i;
+        const int64_t gr = j0 + row0 + r;
+        if (gr < N && gc < N && gc <= gr) {
+          float2 *p = F + gr * N + gc;
+          float2 cv = *p;
+          cv.x -= E[r * 33 + q];
+          cv.y -= E[(64 + r) * 33 + q];
+          *p = cv;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TC_BN) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  DMB_REQUIRE(enc, DMB_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  cuuint64_t dims[2] = {(cuuint64_t)TC_K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)TC_K * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  DMB_REQUIRE(r == CUDA_SUCCESS, DMB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+struct TcState {
+  DevBuf A, B, err;
+  CUtensorMap mapA, mapB;
+  int64_t n_key = -1;
+  bool attr = false;
+};
+
+TcState &tc_state(dmb_ctx *c) {
+  static std::mutex mu;
+  static std::vector<std::pair<dmb_ctx *, TcState *>> states;
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto &p : states)
+    if (p.first == c) return *p.second;
+  states.push_back({c, new TcState()});
+  return *states.back().second;
+}
+
+}  // namespace
+
+namespace dmb {
+
+bool tc_available(dmb_ctx *c) {
+  if (!c->use_tensor_cores) return false;
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c->device);
+  return major == 10 && encode_fn() != nullptr;
+}
+
+void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W) {
+  TcState &st = tc_state(c);
+  const int64_t npadA = ((N + 63) / 64) * 64;
+  const int64_t npadB = ((N + TC_BN - 1) / TC_BN) * TC_BN;
+  if (st.n_key != N) {
+    st.A.ensure(sizeof(float) * 2 * npadA * TC_K);
+    st.B.ensure(sizeof(float) * npadB * TC_K);
+    st.err.ensure(16);
+    DMB_CUDA(cudaMemsetAsync(st.A.p, 0, sizeof(float) * 2 * npadA * TC_K, c->stream));
+    DMB_CUDA(cudaMemsetAsync(st.B.p, 0, sizeof(float) * npadB * TC_K, c->stream));
+    DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
+    make_map(&st.mapA, st.A.as<float>(), (uint64_t)(2 * npadA), TC_BM);
+    make_map(&st.mapB, st.B.as<float>(), (uint64_t)npadB, TC_BN);
+    st.n_key = N;
+  }
+  if (!st.attr) {
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    st.attr = true;
+  }
+  const int64_t rest = N - j0;
+  DMB_REQUIRE(b <= TC_KC, DMB_ERR_STATE, "tensor-core update width exceeds 256");
+  DMB_LAUNCH(c, k_tc_pack, (unsigned)rest, TC_KC, 0, rest, N, j0, jcol, b, F, W, st.A.as<float>(),
+             st.B.as<float>());
+  dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((rest + TC_BN - 1) / TC_BN));
+  DMB_LAUNCH(c, k_tc_syrk, grid, 128, TC_SMEM, st.mapA, st.mapB, F, N, j0, rest, st.err.as<unsigned>());
+}
+
+unsigned tc_error_word(dmb_ctx *c) {
+  TcState &st = tc_state(c);
+  if (!st.err.p) return 0;
+  unsigned e = 0;
+  DMB_CUDA(cudaMemcpyAsync(&e, st.err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  return e;
+}
+
+void tc_release(dmb_ctx *c) {
+  TcState &st = tc_state(c);
+  st.A.release();
+  st.B.release();
+  st.err.release();
+  st.n_key = -1;
+}
+
 }  // namespace dmb

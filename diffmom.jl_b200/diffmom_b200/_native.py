@@ -104,6 +104,7 @@ SIGNATURES = {
     "dmb_ctx_destroy": ([_P], _I),
     "dmb_last_error": ([_P], ctypes.c_char_p),
     "dmb_get_timings": ([_P, ctypes.POINTER(Timings)], _I),
+    "dmb_set_option": ([_P, _I, _I], _I),
     "dmb_mesh_upload": ([_P, _DP, _LP, _L, _L], _I),
     "dmb_rwg_upload": ([_P, _L, _LP, _LP, _LP, _LP, _LP, _DP, _DP, _DP], _I),
     "dmb_assemble_z": ([_P, _D, _D, _I, _I, _DP], _I),

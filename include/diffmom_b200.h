@@ -86,6 +86,12 @@ dmb_status dmb_get_timings(dmb_ctx *ctx, dmb_timings *out);
 /* Library version string, e.g. "diffmom_b200 0.1 sm_100a". */
 const char *dmb_version(void);
 
+/* Implementation options (no reference counterpart).
+ * DMB_OPT_TENSOR_CORES: 1 (default) runs the complex64 factorisation update on
+ * the tcgen05 tensor cores (3xTF32), 0 on FP32 SIMT units. */
+#define DMB_OPT_TENSOR_CORES 1
+dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
+
 /* ---- mesh and basis ---------------------------------------------------- */
 /* TriMesh (src/Types.jl:123-126): xyz 3 x Nv column-major, tri 3 x Nt
  * 1-based.  Replaces the host-side cache geometry of _build_efie_cache

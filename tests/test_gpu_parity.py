@@ -151,6 +151,37 @@ def test_nearfield_apply(sphere2):
         assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-10, cut
 
 
+def test_mixed_factor_tensor_cores_vs_simt():
+    # complex64 near-field LDL^T with the tcgen05 3xTF32 update vs the FP32
+    # SIMT update: both must be single-precision factorisations of the same
+    # matrix, backward error ||Z_nf y - x|| / ||x|| <= 1e-4 (the factor is a
+    # preconditioner: GMRES enforces the FP64 residual); N = 1,920 runs 8
+    # block columns, the largest update 1,664 x 1,664 with K = 256.
+    from diffmom_b200 import _native as nat
+    m = make_icosphere(0.05, 3)
+    r = build_rwg(m)
+    k = 2 * math.pi * 3e9 / C0
+    dev = EFIEDevice(m, r)
+    dev.assemble(k, precision="mixed")
+    Zm = dev.z_host()
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(r.nedges) + 1j * rng.standard_normal(r.nedges)
+    out = {}
+    for tc in (1, 0):
+        dev.ctx.call("dmb_set_option", 1, tc)
+        dev.build_nearfield(math.inf, "lu")
+        y = dev.nf_apply(x)
+        out[tc] = y
+        berr = np.linalg.norm(Zm @ y - x) / np.linalg.norm(x)
+        print(f"tensor_cores={tc} backward error {berr:.3e}")
+        assert berr < 1e-4, tc
+    dev.ctx.call("dmb_set_option", 1, 1)
+    ref = np.linalg.solve(Zm, x)
+    for tc in (1, 0):
+        assert np.linalg.norm(out[tc] - ref) / np.linalg.norm(ref) < 1e-3
+    dev.close()
+
+
 def test_diag_preconditioner(plate6):
     m, r, k, dev, c = plate6
     dev.assemble(k)
