@@ -279,6 +279,58 @@ dmb_status dmb_nf_apply(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
   });
 }
 
+dmb_status dmb_local_build(dmb_ctx *c, double radius, int mode) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(mode >= 0 && mode <= 3, DMB_ERR_ARGUMENT, "local preconditioner mode must be 0, 1, 2 or 3");
+    if (mode == 1)
+      dmb::learned_build(c, radius);
+    else if (mode == 2)
+      dmb::ls_build(c, radius);
+    else if (mode == 3)
+      dmb::ring_step_build(c, radius, false);
+    else
+      dmb::local_inverse_build(c, radius, 64);
+  });
+}
+
+dmb_status dmb_net_train(dmb_ctx *c, double radius, int epochs, int batch, double lr, uint64_t seed,
+                         double *loss_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(std::isfinite(lr) && lr > 0, DMB_ERR_ARGUMENT, "learning rate must be positive");
+    double l = dmb::learned_train_body(c, radius, epochs, batch, lr, seed);
+    if (loss_out) *loss_out = l;
+    c->pc_valid = false;
+  });
+}
+
+int dmb_net_param_count(void) { return dmb::net_param_count(); }
+
+dmb_status dmb_net_get(dmb_ctx *c, float *w) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(w, DMB_ERR_ARGUMENT, "weights output is NULL");
+    dmb::net_get(c, w);
+  });
+}
+
+dmb_status dmb_net_set(dmb_ctx *c, const float *w) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(w, DMB_ERR_ARGUMENT, "weights are NULL");
+    for (int i = 0; i < dmb::net_param_count(); i++)
+      DMB_REQUIRE(std::isfinite(w[i]), DMB_ERR_ARGUMENT, "weights must be finite");
+    dmb::net_set(c, w);
+  });
+}
+
+dmb_status dmb_net_loss_grad(dmb_ctx *c, const float *feat, const float *tgt, const float *wgt, const int *cnt,
+                             int64_t nrows, float *grad, float *loss) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(feat && tgt && wgt && cnt && grad && loss && nrows >= 1, DMB_ERR_ARGUMENT, "bad arrays");
+    for (int64_t i = 0; i < nrows; i++)
+      DMB_REQUIRE(cnt[i] >= 1 && cnt[i] <= 64, DMB_ERR_ARGUMENT, "row sizes must be in 1..64");
+    dmb::net_loss_grad(c, feat, tgt, wgt, cnt, nrows, grad, loss);
+  });
+}
+
 dmb_status dmb_rhs_plane_waves(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
                                int64_t R, int quad_order, double *V_out) {
   return guarded(c, [&] {
@@ -369,8 +421,10 @@ dmb_status dmb_solve_resident(dmb_ctx *c, const dmb_solve_params *p, dmb_gmres_s
       DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
                   "near-field cutoff must be nonnegative and not NaN");
       dmb::nf_build(c, p->cutoff, p->precond_kind);
-    } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV || p->precond_kind == DMB_PRECOND_LEARNED) {
+    } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV) {
       dmb::local_inverse_build(c, p->cutoff, 64);
+    } else if (p->precond_kind == DMB_PRECOND_LEARNED) {
+      dmb::learned_build(c, p->cutoff);
     }
     size_t bytes = sizeof(double2) * c->n;
     c->d_rhs.ensure(bytes);

@@ -610,6 +610,7 @@ namespace dmb {
 
 unsigned read_err_word(dmb_ctx *c) {
   unsigned e = 0;
+  if (!c->d_flags.p) return 0;  // no triangular solve has run on this context
   DMB_CUDA(cudaMemcpyAsync(&e, c->d_flags.p, 4, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   return e;
@@ -689,6 +690,10 @@ void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs) {
       ldlt_solve(c, c->d_F.as<double2>(), xd, nrhs);
     else
       ldlt_solve(c, c->d_F.as<float2>(), xd, nrhs);
+    return;
+  }
+  if (c->pc_kind == DMB_PRECOND_LOCAL_INV || c->pc_kind == DMB_PRECOND_LEARNED) {
+    dmb::local_apply_dev(c, x, nrhs);
     return;
   }
   throw DmbError{DMB_ERR_STATE, "preconditioner kind not available"};

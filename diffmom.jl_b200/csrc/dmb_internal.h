@@ -227,6 +227,16 @@ void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double e
 void prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order);
 void matvec_free_dev(dmb_ctx *c, const double *x, double *y);
 void local_inverse_build(dmb_ctx *c, double radius, int kmax);
+void learned_build(dmb_ctx *c, double radius);
+void ring_step_build(dmb_ctx *c, double radius, bool learned);
+void ls_build(dmb_ctx *c, double radius);
+void local_apply_dev(dmb_ctx *c, double *x, int64_t nrhs);
+double learned_train_body(dmb_ctx *c, double radius, int epochs, int batch, double lr, uint64_t seed);
+void net_loss_grad(dmb_ctx *c, const float *feat, const float *tgt, const float *wgt, const int *cnt,
+                   int64_t nrows, float *grad, float *loss);
+int net_param_count();
+void net_set(dmb_ctx *c, const float *w);
+void net_get(dmb_ctx *c, float *w);
 double now_ms();
 }  // namespace dmb
 

@@ -97,6 +97,8 @@ _I = ctypes.c_int
 _L = ctypes.c_int64
 _DP = ctypes.POINTER(ctypes.c_double)
 _LP = ctypes.POINTER(ctypes.c_int64)
+_FP = ctypes.POINTER(ctypes.c_float)
+_IP = ctypes.POINTER(ctypes.c_int32)
 
 SIGNATURES = {
     "dmb_version": ([], ctypes.c_char_p),
@@ -120,6 +122,12 @@ SIGNATURES = {
     "dmb_gmres": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
     "dmb_solve_direct": ([_P, _DP, _DP, _L, _DP], _I),
     "dmb_farfield": ([_P, _DP, _L, _D, _D, _I, _DP, _L, _DP], _I),
+    "dmb_local_build": ([_P, _D, _I], _I),
+    "dmb_net_train": ([_P, _D, _I, _I, _D, ctypes.c_uint64, _DP], _I),
+    "dmb_net_param_count": ([], _I),
+    "dmb_net_get": ([_P, _FP], _I),
+    "dmb_net_set": ([_P, _FP], _I),
+    "dmb_net_loss_grad": ([_P, _FP, _FP, _FP, _IP, _L, _FP, _FP], _I),
     "dmb_solve_resident": ([_P, ctypes.POINTER(SolveParams), ctypes.POINTER(GmresStats)], _I),
     "dmb_copy_solution": ([_P, _DP], _I),
     "dmb_get_stream": ([_P, ctypes.POINTER(ctypes.c_void_p)], _I),

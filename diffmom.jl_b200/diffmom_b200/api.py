@@ -36,6 +36,7 @@ C0_DEFAULT = 299792458.0
 ETA0_DEFAULT = 376.730313668
 
 _PRECISIONS = {"fp64": nat.PREC_FP64, "mixed": nat.PREC_MIXED}
+NET_MAGIC = b"DMBNET1\0"
 
 
 def _frequency_to_wavenumber(freq_hz: float, c0: float = C0_DEFAULT) -> float:
@@ -54,12 +55,16 @@ class EFIEDevice:
     """Device context holding one mesh + RWG basis (and then Z, preconditioner)."""
 
     def __init__(self, mesh: TriMesh, rwg: RWGData, device: int = 0):
+        self.ctx = nat.Context(device)
+        self.upload(mesh, rwg)
+
+    def upload(self, mesh: TriMesh, rwg: RWGData) -> None:
+        """(Re)bind the context to a mesh and basis; trained network weights stay."""
         if rwg.mesh is not mesh:
             raise ValueError("RWG data was built for a different mesh")
         self.mesh = mesh
         self.rwg = rwg
         self.N = rwg.nedges
-        self.ctx = nat.Context(device)
         self.ctx.call("dmb_mesh_upload", nat.dptr(mesh.xyz), nat.lptr(mesh.tri),
                       mesh.nvertices, mesh.ntriangles)
         self._evert = np.ascontiguousarray(rwg.evert, dtype=np.int64)
@@ -123,6 +128,60 @@ class EFIEDevice:
         self.preconditioner = NearFieldPreconditionerData(self, kinds[factorization], float(cutoff),
                                                           ratio.value)
         return self.preconditioner
+
+    def build_local(self, radius: float, learned: bool = False, mode: str | None = None
+                    ) -> "NearFieldPreconditionerData":
+        """Sparse right preconditioner from per-RWG near blocks.
+
+        mode "local" (default): exact local-inverse rows; "ring": plus one
+        line-searched ring-residual step; "learned" (or learned=True): that
+        step with the trained network's per-entry direction; "ls": the
+        least-squares sparse-inverse rows the network is trained toward."""
+        mode = mode or ("learned" if learned else "local")
+        codes = {"local": 0, "learned": 1, "ls": 2, "ring": 3}
+        if mode not in codes:
+            raise ValueError(f"unknown local preconditioner mode {mode!r}")
+        self.ctx.call("dmb_local_build", float(radius), codes[mode])
+        kind = nat.PRECOND_LEARNED if mode == "learned" else nat.PRECOND_LOCAL_INV
+        self.preconditioner = NearFieldPreconditionerData(self, kind, float(radius), 64.0 / self.N)
+        return self.preconditioner
+
+    def train_network(self, radius: float, epochs: int = 4, batch: int = 512, lr: float = 2e-3,
+                      seed: int = 0) -> float:
+        loss = ctypes.c_double()
+        self.ctx.call("dmb_net_train", float(radius), int(epochs), int(batch), float(lr), int(seed),
+                      ctypes.byref(loss))
+        self.preconditioner = None
+        return loss.value
+
+    def network_weights(self) -> np.ndarray:
+        w = np.empty(self.ctx.lib.dmb_net_param_count(), dtype=np.float32)
+        self.ctx.call("dmb_net_get", w.ctypes.data_as(nat._FP))
+        return w
+
+    def set_network_weights(self, w) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if w.size != self.ctx.lib.dmb_net_param_count():
+            raise nat.DimensionMismatch("network weight vector has the wrong length")
+        self.ctx.call("dmb_net_set", w.ctypes.data_as(nat._FP))
+
+    def save_network(self, path) -> None:
+        """Checkpoint: 8-byte magic, int32 count, float32 weights."""
+        w = self.network_weights()
+        with open(path, "wb") as f:
+            f.write(NET_MAGIC)
+            f.write(np.int32(w.size).tobytes())
+            f.write(w.tobytes())
+
+    def load_network(self, path) -> None:
+        with open(path, "rb") as f:
+            if f.read(8) != NET_MAGIC:
+                raise ValueError("not a diffmom_b200 network checkpoint")
+            n = int(np.frombuffer(f.read(4), dtype=np.int32)[0])
+            w = np.frombuffer(f.read(4 * n), dtype=np.float32)
+        if w.size != n:
+            raise ValueError("truncated network checkpoint")
+        self.set_network_weights(w)
 
     def nf_apply(self, x) -> np.ndarray:
         X = nat.c128(x)

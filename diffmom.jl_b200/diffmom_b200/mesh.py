@@ -176,6 +176,44 @@ def make_icosphere(radius: float, subdivisions: int = 2) -> TriMesh:
     return TriMesh(xyz, np.array(faces, dtype=np.int64))
 
 
+def make_geodesic_sphere(radius: float, frequency: int) -> TriMesh:
+    """Icosahedron with every face split into frequency^2 triangles on a
+    barycentric grid, projected onto the sphere: Nt = 20 f^2, N_rwg = 30 f^2
+    (f = 18 gives 9,720 RWG; f = 24 gives 17,280)."""
+    if frequency < 1:
+        raise ValueError("frequency must be >= 1")
+    base = make_icosphere(1.0, 0)
+    V = base.xyz
+    f = frequency
+    keys = {}
+    verts = []
+
+    def vid(key, p):
+        # key: the barycentric weights on the icosahedron's vertices, exact
+        # integers, so points on shared edges/corners coincide across faces
+        if key not in keys:
+            keys[key] = len(verts) + 1
+            verts.append(p / math.sqrt(p @ p))
+        return keys[key]
+
+    tris = []
+    for a, b, c in base.tri - 1:
+        A, B, C = V[a], V[b], V[c]
+        grid = {}
+        for i in range(f + 1):
+            for j in range(f + 1 - i):
+                w = f - i - j
+                key = tuple(sorted((int(v), int(x)) for v, x in ((a, w), (b, i), (c, j)) if x))
+                p = (A * w + B * i + C * j) / f
+                grid[(i, j)] = vid(key, p)
+        for i in range(f):
+            for j in range(f - i):
+                tris.append((grid[(i, j)], grid[(i + 1, j)], grid[(i, j + 1)]))
+                if j + i + 1 < f:
+                    tris.append((grid[(i + 1, j)], grid[(i + 1, j + 1)], grid[(i, j + 1)]))
+    return TriMesh(radius * np.array(verts), np.array(tris, dtype=np.int64))
+
+
 def _real_sph_harm(l, m, theta, phi):
     """Real spherical harmonic (unnormalised Legendre form) for perturbations."""
     from scipy.special import lpmv
@@ -186,16 +224,18 @@ def _real_sph_harm(l, m, theta, phi):
     return p * np.sin(-m * phi)
 
 
-def make_perturbed_ellipsoid(wavelength: float, seed: int, subdivisions: int = 5,
-                             n_modes: int = 8, max_amplitude: float = 0.10) -> TriMesh:
-    """Seeded closed body: icosphere mapped to an ellipsoid with semi-axes
+def make_perturbed_ellipsoid(wavelength: float, seed: int, subdivisions: int = 4,
+                             n_modes: int = 8, max_amplitude: float = 0.10,
+                             frequency: int | None = None) -> TriMesh:
+    """Seeded closed body: a sphere mesh mapped to an ellipsoid with semi-axes
     U[0.5,1.5] wavelengths, radially perturbed by ``n_modes`` random spherical
     harmonics with total relative amplitude <= ``max_amplitude``.
 
-    subdivisions=5 gives 20,480 triangles / 30,720 RWG; 4 gives 7,680 RWG.
+    The base mesh is the icosphere of ``subdivisions`` (4 gives 7,680 RWG), or
+    the geodesic sphere of ``frequency`` when given (18 gives 9,720 RWG).
     """
     rng = np.random.default_rng(seed)
-    base = make_icosphere(1.0, subdivisions)
+    base = make_geodesic_sphere(1.0, frequency) if frequency else make_icosphere(1.0, subdivisions)
     semi = rng.uniform(0.5, 1.5, size=3) * wavelength
     u = base.xyz
     theta = np.arccos(np.clip(u[:, 2], -1, 1))

@@ -150,6 +150,38 @@ dmb_status dmb_nf_build(dmb_ctx *ctx, double cutoff, int kind, double *nnz_ratio
 /* NearFieldOperator apply y = Z_nf^-1 x (NearFieldPreconditioner.jl:1034-1054). */
 dmb_status dmb_nf_apply(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
 
+/* ---- local-inverse and learned preconditioners ------------------------- */
+/* No reference counterpart (the near-field preconditioner above is their
+ * fallback).  dmb_local_build: per-RWG near blocks (the <= 64 nearest RWG
+ * centres within `radius`) are solved exactly; their rows form a sparse right
+ * preconditioner (DMB_PRECOND_LOCAL_INV).  The "ring" of m is the rest of its
+ * 2x-radius neighbourhood E_m (<= 128); the ring residual of a row z is
+ * r = Z[E_m, S_m] z - e_m.
+ *   mode 0: local inverse rows.
+ *   mode 1: local inverse + one exactly line-searched ring-residual step along
+ *           g (1 + o), g = Z[E,S]^H r, o the trained network's per-entry
+ *           modulation (DMB_PRECOND_LEARNED).
+ *   mode 2: least-squares rows min || Z[E_m, S_m] z - e_m || (the exact rows
+ *           the network is trained toward).
+ *   mode 3: local inverse + one plain line-searched ring step (o = 0). */
+dmb_status dmb_local_build(dmb_ctx *ctx, double radius, int mode);
+/* Train the network on the current body (resident Z): features of the
+ * local-inverse rows and their ring gradients as input; targets from the
+ * least-squares rows (exact local block solves the method generates); Adam
+ * over minibatches; mean loss of the last epoch in loss_out.  Weights persist
+ * in the context across bodies. */
+dmb_status dmb_net_train(dmb_ctx *ctx, double radius, int epochs, int batch, double lr, uint64_t seed,
+                         double *loss_out);
+/* Flat FP32 weight vector (save/load/check): count, get, set. */
+int dmb_net_param_count(void);
+dmb_status dmb_net_get(dmb_ctx *ctx, float *w);
+dmb_status dmb_net_set(dmb_ctx *ctx, const float *w);
+/* Loss and gradient of the network for caller-supplied rows (gradient check):
+ * feat nrows x 64 x 13, tgt nrows x 64 x 2, per-entry weights nrows x 64,
+ * cnt nrows (1..64).  loss = mean over rows of sum_j w_j |out_j - tgt_j|^2. */
+dmb_status dmb_net_loss_grad(dmb_ctx *ctx, const float *feat, const float *tgt, const float *wgt,
+                             const int *cnt, int64_t nrows, float *grad, float *loss);
+
 /* ---- excitation -------------------------------------------------------- */
 /* assemble_plane_wave / assemble_multiple_excitations for R plane waves
  * (src/assembly/Excitation.jl:2738-2797, 2866-2896).  kvecs, pols: 3 x R
