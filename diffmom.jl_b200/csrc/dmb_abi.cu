@@ -82,6 +82,10 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     for (DevBuf *b : bufs) b->release();
     c->d_rhs.release();
     c->d_sol.release();
+    c->d_mono.release();
+    c->d_small.release();
+    dmb::tc_release(c);
+    dmb::local_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
   }
@@ -104,6 +108,11 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
     if (option == DMB_OPT_TENSOR_CORES) {
       c->use_tensor_cores = value != 0;
       c->pc_valid = false;
+      return;
+    }
+    if (option == DMB_OPT_TC_MIN_RHS) {
+      DMB_REQUIRE(value >= 1, DMB_ERR_ARGUMENT, "minimum right-hand-side count must be >= 1");
+      c->tc_min_rhs = value;
       return;
     }
     throw DmbError{DMB_ERR_ARGUMENT, "unknown option " + std::to_string(option)};
@@ -229,7 +238,9 @@ dmb_status dmb_matvec(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
     bx.ensure(bytes);
     by.ensure(bytes);
     DMB_CUDA(cudaMemcpyAsync(bx.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
-    dmb::matvec_dev(c, bx.p, by.p, nrhs);
+    dmb::matvec_op(c, bx.as<double2>(), by.as<double2>(), nrhs);
+    if (dmb::matvec_op_inexact(c, nrhs))
+      DMB_REQUIRE(dmb::tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait expired");
     DMB_CUDA(cudaMemcpyAsync(y, by.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
   });
@@ -407,35 +418,92 @@ dmb_status dmb_solve_direct(dmb_ctx *c, const double *rhs, double *x, int64_t nr
   });
 }
 
+namespace {
+void check_solve_params(const dmb_solve_params *p) {
+  DMB_REQUIRE(p, DMB_ERR_ARGUMENT, "solve parameters are NULL");
+  DMB_REQUIRE(std::isfinite(p->tol) && p->tol > 0, DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive");
+  DMB_REQUIRE(p->maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
+}
+
+// assemble + preconditioner of the resident solves
+void resident_setup(dmb_ctx *c, const dmb_solve_params *p) {
+  dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
+  if (p->precond_kind == DMB_PRECOND_NF_LU || p->precond_kind == DMB_PRECOND_NF_DIAG) {
+    DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
+                "near-field cutoff must be nonnegative and not NaN");
+    dmb::nf_build(c, p->cutoff, p->precond_kind);
+  } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV) {
+    dmb::local_inverse_build(c, p->cutoff, 64);
+  } else if (p->precond_kind == DMB_PRECOND_LEARNED) {
+    dmb::learned_build(c, p->cutoff);
+  }
+}
+
+void resident_check(const dmb_gmres_stats &st) {
+  if (!st.solved)
+    throw DmbError{DMB_ERR_NOT_CONVERGED, "forward GMRES did not converge: niter=" + std::to_string(st.niter) +
+                                              ", final_residual=" + std::to_string(st.residual)};
+}
+}  // namespace
+
 dmb_status dmb_solve_resident(dmb_ctx *c, const dmb_solve_params *p, dmb_gmres_stats *stats) {
   dmb_gmres_stats st{};
   dmb_status s = guarded(c, [&] {
-    DMB_REQUIRE(p, DMB_ERR_ARGUMENT, "solve parameters are NULL");
-    DMB_REQUIRE(std::isfinite(p->tol) && p->tol > 0, DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive");
-    DMB_REQUIRE(p->maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
+    check_solve_params(p);
     check_finite(p->kvec, 3, "plane-wave k_vec");
     check_finite(p->pol, 3, "plane-wave polarization");
     double t0 = dmb::now_ms();
-    dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
-    if (p->precond_kind == DMB_PRECOND_NF_LU || p->precond_kind == DMB_PRECOND_NF_DIAG) {
-      DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
-                  "near-field cutoff must be nonnegative and not NaN");
-      dmb::nf_build(c, p->cutoff, p->precond_kind);
-    } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV) {
-      dmb::local_inverse_build(c, p->cutoff, 64);
-    } else if (p->precond_kind == DMB_PRECOND_LEARNED) {
-      dmb::learned_build(c, p->cutoff);
-    }
+    resident_setup(c, p);
     size_t bytes = sizeof(double2) * c->n;
     c->d_rhs.ensure(bytes);
     c->d_sol.ensure(bytes);
+    c->sol_r = 0;
     dmb::rhs_plane_waves_dev(c, p->kvec, &p->E0, p->pol, 1, p->quad_order, c->d_rhs.as<double>());
     dmb::gmres_dev(c, c->d_rhs.as<double>(), c->d_sol.as<double>(), 1, p->tol, p->maxiter, p->precond_kind,
                    p->precond_side, &st);
+    c->sol_r = 1;
     c->tm.solve_ms = dmb::now_ms() - t0;
-    if (!st.solved)
-      throw DmbError{DMB_ERR_NOT_CONVERGED, "forward GMRES did not converge: niter=" + std::to_string(st.niter) +
-                                                ", final_residual=" + std::to_string(st.residual)};
+    resident_check(st);
+  });
+  if (stats) *stats = st;
+  return s;
+}
+
+dmb_status dmb_solve_resident_many(dmb_ctx *c, const dmb_solve_params *p, int64_t R, const double *kvecs,
+                                   const double *E0s, const double *pols, double *sigma_out,
+                                   dmb_gmres_stats *stats) {
+  dmb_gmres_stats st{};
+  dmb_status s = guarded(c, [&] {
+    check_solve_params(p);
+    DMB_REQUIRE(R >= 1 && kvecs && E0s && pols, DMB_ERR_ARGUMENT, "need R >= 1 incidences with k_vec, E0, pol");
+    check_finite(kvecs, 3 * R, "plane-wave k_vecs");
+    check_finite(pols, 3 * R, "plane-wave polarizations");
+    check_finite(E0s, R, "plane-wave amplitudes");
+    for (int64_t r = 0; r < R; r++) {
+      const double *kv = kvecs + 3 * r;
+      DMB_REQUIRE(kv[0] != 0.0 || kv[1] != 0.0 || kv[2] != 0.0, DMB_ERR_ARGUMENT, "plane-wave k_vec is zero");
+      DMB_REQUIRE(E0s[r] != 0.0 || !sigma_out, DMB_ERR_ARGUMENT, "RCS needs a nonzero incident amplitude");
+    }
+    double t0 = dmb::now_ms();
+    resident_setup(c, p);
+    const size_t bytes = sizeof(double2) * c->n * R;
+    c->d_rhs.ensure(bytes);
+    c->d_sol.ensure(bytes);
+    c->sol_r = 0;
+    dmb::rhs_plane_waves_dev(c, kvecs, E0s, pols, R, p->quad_order, c->d_rhs.as<double>());
+    dmb::gmres_dev(c, c->d_rhs.as<double>(), c->d_sol.as<double>(), R, p->tol, p->maxiter, p->precond_kind,
+                   p->precond_side, &st);
+    c->sol_r = R;
+    if (sigma_out) {
+      c->d_mono.ensure(sizeof(double2) * 3 * R + sizeof(double) * R);
+      double *E = c->d_mono.as<double>();
+      double *sig = E + 6 * R;
+      dmb::monostatic_dev(c, R, p->k, p->eta0, p->quad_order, c->d_sol.as<double>(), E, sig);
+      DMB_CUDA(cudaMemcpyAsync(sigma_out, sig, sizeof(double) * R, cudaMemcpyDeviceToHost, c->stream));
+      DMB_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    c->tm.solve_ms = dmb::now_ms() - t0;
+    resident_check(st);
   });
   if (stats) *stats = st;
   return s;
@@ -443,8 +511,9 @@ dmb_status dmb_solve_resident(dmb_ctx *c, const dmb_solve_params *p, dmb_gmres_s
 
 dmb_status dmb_copy_solution(dmb_ctx *c, double *I_out) {
   return guarded(c, [&] {
-    DMB_REQUIRE(I_out && c->d_sol.p, DMB_ERR_STATE, "no resident solution");
-    DMB_CUDA(cudaMemcpyAsync(I_out, c->d_sol.p, sizeof(double2) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    DMB_REQUIRE(I_out && c->d_sol.p && c->sol_r > 0, DMB_ERR_STATE, "no resident solution");
+    DMB_CUDA(cudaMemcpyAsync(I_out, c->d_sol.p, sizeof(double2) * c->n * c->sol_r, cudaMemcpyDeviceToHost,
+                             c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

@@ -90,6 +90,70 @@ __global__ void k_radiation(int64_t N, int64_t NO, const TriCache *__restrict__ 
   G[(3 * q + 2) * N + n] = cmul(pref, v2);
 }
 
+// Monostatic far field: for incidence r the field of current column I_r in
+// the direction -k_hat_r (one CTA per incidence, block reduction over RWGs),
+// E (3 complex per r) and sigma_r = 4 pi |E|^2 / |E0_r|^2 (Diagnostics.jl:460-474).
+__global__ void __launch_bounds__(256) k_monostatic(int64_t N, const TriCache *__restrict__ tc,
+                                                    const int *__restrict__ rslot, int nq,
+                                                    const double *__restrict__ wq, const double *__restrict__ kv,
+                                                    const double *__restrict__ E0s, double k, double eta0,
+                                                    const double2 *__restrict__ I, double2 *__restrict__ E,
+                                                    double *__restrict__ sigma) {
+  __shared__ double2 red[3][8];
+  const int64_t r = blockIdx.x;
+  const double kx = kv[3 * r], ky = kv[3 * r + 1], kz = kv[3 * r + 2];
+  const double kn = sqrt(kx * kx + ky * ky + kz * kz);
+  const double r0 = -kx / kn, r1 = -ky / kn, r2 = -kz / kn;
+  double2 c0 = make_double2(0, 0), c1 = c0, c2 = c0;
+  const double2 *Ir = I + r * N;
+  for (int64_t n = threadIdx.x; n < N; n += blockDim.x) {
+    const double2 in = Ir[n];
+    for (int s = 0; s < 2; s++) {
+      const int sl = rslot[2 * n + s];
+      const TriCache &T = tc[sl / 3];
+      const int i = sl % 3;
+      for (int qs = 0; qs < nq; qs++) {
+        const double wt = wq[qs] * 2 * T.area * T.s[i];
+        const double arg = k * (r0 * T.qp[qs][0] + r1 * T.qp[qs][1] + r2 * T.qp[qs][2]);
+        double sn, cs;
+        sincos(arg, &sn, &cs);
+        const double2 ph = cmul(make_double2(wt * cs, wt * sn), in);
+        c0 = cadd(c0, cscale(ph, T.qp[qs][0] - T.p[i][0]));
+        c1 = cadd(c1, cscale(ph, T.qp[qs][1] - T.p[i][1]));
+        c2 = cadd(c2, cscale(ph, T.qp[qs][2] - T.p[i][2]));
+      }
+    }
+  }
+  c0 = warp_sum2(c0);
+  c1 = warp_sum2(c1);
+  c2 = warp_sum2(c2);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = c0;
+    red[1][w] = c1;
+    red[2][w] = c2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int u = 1; u < (int)(blockDim.x >> 5); u++) {
+      c0 = cadd(c0, red[0][u]);
+      c1 = cadd(c1, red[1][u]);
+      c2 = cadd(c2, red[2][u]);
+    }
+    // rh x (rh x C) = rh (rh.C) - C for the unit direction rh
+    const double2 d = cadd(cadd(cscale(c0, r0), cscale(c1, r1)), cscale(c2, r2));
+    const double2 pref = make_double2(0, k * eta0 * DMB_INV_FOUR_PI);
+    const double2 v0 = cmul(pref, csub(cscale(d, r0), c0));
+    const double2 v1 = cmul(pref, csub(cscale(d, r1), c1));
+    const double2 v2 = cmul(pref, csub(cscale(d, r2), c2));
+    E[3 * r] = v0;
+    E[3 * r + 1] = v1;
+    E[3 * r + 2] = v2;
+    const double e0 = E0s[r];
+    sigma[r] = 4.0 * 3.14159265358979323846 * (cabs2(v0) + cabs2(v1) + cabs2(v2)) / (e0 * e0);
+  }
+}
+
 // C (M x R col-major) = A (M x K row-major) B (K x R col-major)
 __global__ void __launch_bounds__(256) k_gemm_rc(int64_t M, int64_t K, int64_t R, const double2 *__restrict__ A,
                                                  const double2 *__restrict__ B, double2 *__restrict__ C) {
@@ -274,6 +338,16 @@ void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double e
   DMB_LAUNCH(c, k_gemm_rc, g2, 256, 0, 3 * NO, N, nrhs, G.as<double2>(), (const double2 *)I_dev,
              (double2 *)E_dev);
   DMB_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// monostatic fields of R resident solutions; kv / E0s are the device copies
+// that rhs_plane_waves_dev staged in d_small
+void monostatic_dev(dmb_ctx *c, int64_t R, double k, double eta0, int quad_order, const double *I_dev,
+                    double *E_dev, double *sigma_dev) {
+  ensure_cache(c, quad_order);
+  const double *dk = (const double *)((const char *)c->d_small.p + 64), *de = dk + 3 * R;
+  DMB_LAUNCH(c, k_monostatic, (unsigned)R, 256, 0, c->n, c->d_tcache.as<TriCache>(), c->d_rwg_slot.as<int>(),
+             c->nq, c->d_wq.as<double>(), dk, de, k, eta0, (const double2 *)I_dev, (double2 *)E_dev, sigma_dev);
 }
 
 void prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order) {

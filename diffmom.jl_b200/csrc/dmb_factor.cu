@@ -33,8 +33,6 @@
 
 namespace dmb {
 void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W);
-bool tc_available(dmb_ctx *c);
-unsigned tc_error_word(dmb_ctx *c);
 }  // namespace dmb
 
 namespace {
@@ -604,6 +602,192 @@ template <class C> void ldlt_solve(dmb_ctx *c, const C *F, double2 *x, int64_t R
   DMB_LAUNCH(c, k_trsv_bwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err);
 }
 
+// ---------------------------------------------------------------------------
+// Batched triangular solves for many right-hand sides (X column-major N x R).
+// The factor is walked in 256-row panels: the in-panel part (four 64-blocks
+// with their stored Linv) runs in k_trsm_panel, where one CTA owns TP_COLS
+// right-hand sides; the rest of the rows receive one GEMM-shaped update per
+// panel (tensor cores for the complex64 factor, SIMT otherwise).  F is read
+// once per sweep instead of once per right-hand side.
+// ---------------------------------------------------------------------------
+constexpr int TP = 256;      // panel rows
+constexpr int TP_COLS = 8;   // right-hand sides per CTA
+
+// T[i][j] <- G(i, j) for i, j < 64 (zero outside bi x bj); TR reads G(j, i)
+template <class FC, bool TR>
+__device__ __forceinline__ void stage_tile(FC (*T)[65], const FC *__restrict__ G, int64_t ld, int bi, int bj) {
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int a = e >> 6, b = e & 63;  // consecutive threads: consecutive b
+    if (TR) {
+      // element (i = b, j = a) = G[a * ld + b]
+      T[b][a] = (b < bi && a < bj) ? G[(int64_t)a * ld + b] : FC{};
+    } else {
+      T[a][b] = (a < bi && b < bj) ? G[(int64_t)a * ld + b] : FC{};
+    }
+  }
+}
+
+template <class FC, bool BWD>
+__global__ void __launch_bounds__(256) k_trsm_panel(int64_t N, int64_t R, int64_t p0, int width,
+                                                    const FC *__restrict__ F, const FC *__restrict__ Linv,
+                                                    double2 *__restrict__ X) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FC(*T)[65] = reinterpret_cast<FC(*)[65]>(smem_raw);
+  double2(*xs)[TP_COLS + 1] = reinterpret_cast<double2(*)[TP_COLS + 1]>(smem_raw + sizeof(FC) * 64 * 65);
+  const int64_t r0 = (int64_t)blockIdx.x * TP_COLS;
+  for (int e = threadIdx.x; e < width * TP_COLS; e += 256) {
+    const int q = e / width, i = e % width;
+    xs[i][q] = (r0 + q < R) ? X[(r0 + q) * N + p0 + i] : make_double2(0, 0);
+  }
+  const int nb = (width + 63) / 64;
+  const int i = threadIdx.x & 63, qh = threadIdx.x >> 6;  // rows i, columns qh and qh + 4
+  for (int s = 0; s < nb; s++) {
+    const int b = BWD ? nb - 1 - s : s;
+    const int bs = min(64, width - 64 * b);
+    const int64_t t = (p0 >> 6) + b;  // global 64-block index
+    __syncthreads();
+    // BWD: x_b = Linv_b^T y_b, FWD: y_b = Linv_b x_b
+    stage_tile<FC, BWD>(T, Linv + t * 4096, 64, bs, bs);
+    __syncthreads();
+    double2 acc0 = make_double2(0, 0), acc1 = make_double2(0, 0);
+    if (i < bs) {
+      for (int j = 0; j < bs; j++) {
+        const double2 l = to_d2(T[i][j]);
+        cfma(acc0, l, xs[64 * b + j][qh]);
+        cfma(acc1, l, xs[64 * b + j][qh + 4]);
+      }
+    }
+    __syncthreads();
+    if (i < bs) {
+      xs[64 * b + i][qh] = acc0;
+      xs[64 * b + i][qh + 4] = acc1;
+    }
+    // the other blocks of the panel that depend on block b
+    for (int s2 = s + 1; s2 < nb; s2++) {
+      const int b2 = BWD ? nb - 1 - s2 : s2;
+      const int bs2 = min(64, width - 64 * b2);
+      __syncthreads();
+      if (BWD)  // x_{b2} -= L[b, b2]^T x_b : T[i][j] = L[p0 + 64 b + j][p0 + 64 b2 + i]
+        stage_tile<FC, true>(T, F + (p0 + 64 * b) * N + p0 + 64 * b2, N, bs2, bs);
+      else      // y_{b2} -= L[b2, b] y_b  : T[i][j] = L[p0 + 64 b2 + i][p0 + 64 b + j]
+        stage_tile<FC, false>(T, F + (p0 + 64 * b2) * N + p0 + 64 * b, N, bs2, bs);
+      __syncthreads();
+      if (i < bs2) {
+        double2 u0 = make_double2(0, 0), u1 = make_double2(0, 0);
+        for (int j = 0; j < bs; j++) {
+          const double2 l = to_d2(T[i][j]);
+          cfma(u0, l, xs[64 * b + j][qh]);
+          cfma(u1, l, xs[64 * b + j][qh + 4]);
+        }
+        xs[64 * b2 + i][qh] = csub(xs[64 * b2 + i][qh], u0);
+        xs[64 * b2 + i][qh + 4] = csub(xs[64 * b2 + i][qh + 4], u1);
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < width * TP_COLS; e += 256) {
+    const int q = e / width, ii = e % width;
+    if (r0 + q < R) X[(r0 + q) * N + p0 + ii] = xs[ii][q];
+  }
+}
+
+// SIMT panel update  Y[m, r] -= sum_k A(m, k) B[k, r]  (FP64 accumulation),
+// A(m, k) = A[m lda + k] or, TR, A[k lda + m]; B, Y column-major.  64 x 64
+// output tiles, K in chunks of 16.
+template <class FC, bool TR>
+__global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t R, int K, const FC *__restrict__ A, int64_t lda,
+                                                  const double2 *__restrict__ B, int64_t ldb, double2 *__restrict__ Y,
+                                                  int64_t ldy) {
+  __shared__ double2 As[16][65];
+  __shared__ double2 Bs[16][65];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int64_t m0 = (int64_t)blockIdx.x * 64, r0 = (int64_t)blockIdx.y * 64;
+  double2 acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = make_double2(0, 0);
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int kk, mm;
+      if (TR) { mm = e & 63; kk = e >> 6; } else { kk = e & 15; mm = e >> 4; }
+      const int64_t m = m0 + mm;
+      const int kx = k0 + kk;
+      As[kk][mm] = (m < M && kx < K) ? to_d2(TR ? A[(int64_t)kx * lda + m] : A[m * lda + kx]) : make_double2(0, 0);
+      const int kb = e & 15, rb = e >> 4;
+      const int64_t r = r0 + rb;
+      Bs[kb][rb] = (r < R && k0 + kb < K) ? B[r * ldb + k0 + kb] : make_double2(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) a[u] = As[kk][ty + 16 * u];
+#pragma unroll
+      for (int v = 0; v < 4; v++) b[v] = Bs[kk][tx + 16 * v];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) cfma(acc[u][v], a[u], b[v]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int64_t m = m0 + ty + 16 * u, r = r0 + tx + 16 * v;
+      if (m < M && r < R) Y[r * ldy + m] = csub(Y[r * ldy + m], acc[u][v]);
+    }
+}
+
+template <class C> void trsm_panel_attrs() {
+  static bool done = false;
+  if (done) return;
+  const int sm = (int)(sizeof(C) * 64 * 65 + sizeof(double2) * TP * (TP_COLS + 1));
+  DMB_CUDA(cudaFuncSetAttribute(k_trsm_panel<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  DMB_CUDA(cudaFuncSetAttribute(k_trsm_panel<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  done = true;
+}
+
+template <class C> void panel_update(dmb_ctx *c, const C *F, int64_t N, int64_t p0, int w, bool bwd, double2 *X,
+                                     int64_t R) {
+  const int64_t M = bwd ? p0 : N - (p0 + w);
+  if (M <= 0) return;
+  if (std::is_same<C, float2>::value && R >= c->tc_min_rhs && dmb::tc_available(c)) {
+    dmb::tc_panel_update(c, (const float2 *)F, N, p0, w, bwd, X, R);
+    return;
+  }
+  dim3 g(blocks_for(M, 64), blocks_for(R, 64));
+  if (bwd)
+    DMB_LAUNCH(c, (k_gemm_sub<C, true>), g, 256, 0, M, R, w, F + p0 * N, N, X + p0, N, X, N);
+  else
+    DMB_LAUNCH(c, (k_gemm_sub<C, false>), g, 256, 0, M, R, w, F + (p0 + w) * N + p0, N, X + p0, N, X + p0 + w, N);
+}
+
+template <class C> void ldlt_solve_batched(dmb_ctx *c, const C *F, double2 *X, int64_t R) {
+  const int64_t N = c->n;
+  const C *Linv = c->d_dinv.as<C>();
+  trsm_panel_attrs<C>();
+  const size_t sm = sizeof(C) * 64 * 65 + sizeof(double2) * TP * (TP_COLS + 1);
+  const unsigned gcols = blocks_for(R, TP_COLS);
+  const int64_t npan = (N + TP - 1) / TP;
+  for (int64_t p = 0; p < npan; p++) {
+    const int64_t p0 = p * TP;
+    const int w = (int)std::min<int64_t>(TP, N - p0);
+    DMB_LAUNCH(c, (k_trsm_panel<C, false>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
+    panel_update<C>(c, F, N, p0, w, false, X, R);
+  }
+  DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, X);
+  for (int64_t p = npan - 1; p >= 0; p--) {
+    const int64_t p0 = p * TP;
+    const int w = (int)std::min<int64_t>(TP, N - p0);
+    DMB_LAUNCH(c, (k_trsm_panel<C, true>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
+    panel_update<C>(c, F, N, p0, w, true, X, R);
+  }
+}
+
 }  // namespace
 
 namespace dmb {
@@ -686,10 +870,16 @@ void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs) {
     return;
   }
   if (c->pc_kind == DMB_PRECOND_NF_LU) {
-    if (c->pc_prec == DMB_PREC_FP64)
-      ldlt_solve(c, c->d_F.as<double2>(), xd, nrhs);
-    else
-      ldlt_solve(c, c->d_F.as<float2>(), xd, nrhs);
+    // one right-hand side at a time streams F per column; from 8 columns on
+    // the panel-blocked solves read F once per sweep
+    const bool batched = nrhs >= 8;
+    if (c->pc_prec == DMB_PREC_FP64) {
+      if (batched) ldlt_solve_batched(c, c->d_F.as<double2>(), xd, nrhs);
+      else ldlt_solve(c, c->d_F.as<double2>(), xd, nrhs);
+    } else {
+      if (batched) ldlt_solve_batched(c, c->d_F.as<float2>(), xd, nrhs);
+      else ldlt_solve(c, c->d_F.as<float2>(), xd, nrhs);
+    }
     return;
   }
   if (c->pc_kind == DMB_PRECOND_LOCAL_INV || c->pc_kind == DMB_PRECOND_LEARNED) {

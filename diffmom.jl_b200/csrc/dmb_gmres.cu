@@ -212,14 +212,14 @@ void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, do
                     int64_t R) {
   const int64_t N = c->n;
   if (precond_kind == DMB_PRECOND_NONE) {
-    matvec_dev(c, v, w, R);
+    matvec_op(c, v, w, R);
   } else if (side == DMB_SIDE_LEFT) {
-    matvec_dev(c, v, w, R);
+    matvec_op(c, v, w, R);
     pc_apply_dev(c, (double *)w, R);
   } else {
     DMB_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double2) * N * R, cudaMemcpyDeviceToDevice, c->stream));
     pc_apply_dev(c, (double *)tmp, R);
-    matvec_dev(c, tmp, w, R);
+    matvec_op(c, tmp, w, R);
   }
 }
 
@@ -252,7 +252,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   c->d_work.ensure(vec_bytes * 2);
   // layout: H[R][(k+1)k] g[R][k+1] sn[R][k] hb[R][k+1] y[R][k] | cs[R][k] nrm[2R] | st[R] | active
   size_t small = sizeof(double2) * R * ((size_t)(kcap + 1) * kcap + 2 * (kcap + 1) + 2 * kcap) +
-                 sizeof(double) * R * (kcap + 2) + sizeof(SysState) * R + 64;
+                 sizeof(double) * R * (kcap + 3) + sizeof(SysState) * R + 64;
   c->d_H.ensure(small);
   double2 *V = c->d_V.as<double2>();
   double2 *w = c->d_work.as<double2>();
@@ -263,43 +263,62 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   double2 *hb = sn + R * (int64_t)kcap;
   double2 *ybuf = hb + R * (int64_t)(kcap + 1);
   double *cs = (double *)(ybuf + R * (int64_t)kcap);
-  double *nrm = cs + R * (int64_t)kcap;
-  SysState *st = (SysState *)(nrm + 2 * R);
+  double *nrm = cs + R * (int64_t)kcap;   // [0,R) Krylov norms, [R,2R) ||b||, [2R,3R) ||b - Z x||
+  double *tnrm = nrm + 2 * R;
+  SysState *st = (SysState *)(nrm + 3 * R);
   unsigned *active = (unsigned *)(st + R);
   const double2 *b = (const double2 *)b_dev;
   double2 *x = (double2 *)x_dev;
 
+  // With the tensor-core operator (FP32 accumulation) the Krylov recurrence
+  // is only as exact as that product: a system whose estimate converged is
+  // re-checked against the residual computed in FP64 and, if that is still
+  // above its threshold, refined by another cycle from the current x.
+  const bool inexact = matvec_op_inexact(c, R);
   DMB_CUDA(cudaMemsetAsync(x, 0, vec_bytes, c->stream));
   int total_iters = 0, restarts = 0;
-  bool all_done = false;
+  bool first = true, have_true = false;
   std::vector<SysState> hst(R);
-  while (!all_done) {
+  while (true) {
     // r0 = b - Z x (x = 0 on the first cycle), preconditioned on the left
-    if (total_iters == 0) {
+    if (first) {
       DMB_CUDA(cudaMemcpyAsync(V, b, vec_bytes, cudaMemcpyDeviceToDevice, c->stream));
     } else {
       matvec_dev(c, x, V, R);
       DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, V);
+      if (inexact) DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, V, tnrm);
     }
     if (precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_LEFT) pc_apply_dev(c, (double *)V, R);
-    DMB_CUDA(cudaMemsetAsync(H, 0, sizeof(double2) * R * (int64_t)(kcap + 1) * kcap, c->stream));
     DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, V, nrm);
-    if (total_iters == 0) {
+    if (first) {
       DMB_LAUNCH(c, k_init_state, blocks_for(R, 128), 128, 0, R, nrm, tol, st, g, kcap);
     } else {
-      // restart keeps each system's original threshold; reset the basis state
+      // restart or refinement: keep each system's original threshold
       std::vector<double> hn(R);
       DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm, 8 * R, cudaMemcpyDeviceToHost, c->stream));
       DMB_CUDA(cudaStreamSynchronize(c->stream));
       std::vector<double2> hg((size_t)R * (kcap + 1), make_double2(0, 0));
+      bool any = false;
       for (int64_t r = 0; r < R; r++) {
         hst[r].k = 0;
         hst[r].resid = hn[r];
-        if (!hst[r].done) hg[(size_t)r * (kcap + 1)] = make_double2(hn[r], 0);
+        if (inexact && hst[r].done == 1 && !(hn[r] <= hst[r].eps)) hst[r].done = 0;
+        if (!hst[r].done) {
+          hg[(size_t)r * (kcap + 1)] = make_double2(hn[r], 0);
+          any = true;
+        }
       }
+      if (!any) {
+        have_true = inexact;  // x has not changed since tnrm was formed
+        break;
+      }
+      if (total_iters >= maxiter) break;
+      restarts++;
       DMB_CUDA(cudaMemcpyAsync(st, hst.data(), sizeof(SysState) * R, cudaMemcpyHostToDevice, c->stream));
       DMB_CUDA(cudaMemcpyAsync(g, hg.data(), sizeof(double2) * hg.size(), cudaMemcpyHostToDevice, c->stream));
     }
+    first = false;
+    DMB_CUDA(cudaMemsetAsync(H, 0, sizeof(double2) * R * (int64_t)(kcap + 1) * kcap, c->stream));
     DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, V, V);
     int j = 0;
     for (; j < kcap && total_iters < maxiter; j++, total_iters++) {
@@ -335,26 +354,30 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     }
     DMB_CUDA(cudaMemcpyAsync(hst.data(), st, sizeof(SysState) * R, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
-    all_done = true;
+    bool all_done = true;
     for (auto &s : hst)
       if (!s.done) all_done = false;
-    if (total_iters >= maxiter) break;
-    if (!all_done) restarts++;
+    if (all_done && !inexact) break;
+    if (!all_done && total_iters >= maxiter) break;
   }
   unsigned e = read_err_word(c);
   DMB_REQUIRE((e & 4u) == 0, DMB_ERR_TIMEOUT, "triangular solve wait expired");
+  if (inexact) DMB_REQUIRE(tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait expired");
   // true FP64 residual ||b - Z x|| / ||b|| per system
-  matvec_dev(c, x, w, R);
-  DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
-  DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, nrm);
+  if (!have_true) {
+    matvec_dev(c, x, w, R);
+    DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
+    DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, tnrm);
+  }
   DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);
   std::vector<double> hn(2 * R);
-  DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm, 16 * R, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm + R, 16 * R, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   double tres = 0, eres = 0;
   bool solved = true;
   for (int64_t r = 0; r < R; r++) {
-    double rel = hn[R + r] > 0 ? hn[r] / hn[R + r] : (hn[r] > 0 ? INFINITY : 0.0);
+    const double bn = hn[r], rn = hn[R + r];
+    double rel = bn > 0 ? rn / bn : (rn > 0 ? INFINITY : 0.0);
     tres = std::max(tres, rel);
     double est = hst[r].beta > 0 ? hst[r].resid / hst[r].beta : 0.0;
     if (hst[r].done == 1 || hst[r].done == 2) {

@@ -148,12 +148,15 @@ struct dmb_ctx {
   // GMRES workspace
   DevBuf d_V, d_H, d_work, d_vecs, d_scal;
 
-  // resident solution of dmb_solve_resident
-  DevBuf d_rhs, d_sol;
+  // resident solution of dmb_solve_resident / dmb_solve_resident_many
+  DevBuf d_rhs, d_sol, d_mono;
+  int64_t sol_r = 0;
   // small persistent scratch (counters, plane-wave parameters): the solve path
   // allocates nothing after its first call
   DevBuf d_small;
   bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
+  int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
+  uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   int gm_kcap = 0;              // cached GMRES basis capacity
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;
@@ -225,8 +228,20 @@ void solve_direct_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nr
 void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double eta0,
                   int quad_order, const double *I_dev, int64_t nrhs, double *E_dev);
 void prepare_operator(dmb_ctx *c, double k, double eta0, int quad_order);
+void monostatic_dev(dmb_ctx *c, int64_t R, double k, double eta0, int quad_order, const double *I_dev,
+                    double *E_dev, double *sigma_dev);
 void matvec_free_dev(dmb_ctx *c, const double *x, double *y);
 void local_inverse_build(dmb_ctx *c, double radius, int kmax);
+// tensor-core complex GEMMs (dmb_tc.cu)
+bool tc_available(dmb_ctx *c);
+void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R);
+void tc_panel_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t p0, int width, bool backward, double2 *X,
+                     int64_t R);
+unsigned tc_error_word(dmb_ctx *c);
+void tc_release(dmb_ctx *c);
+void local_release(dmb_ctx *c);
+void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs);  // Krylov operator (may be TC)
+bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs);
 void learned_build(dmb_ctx *c, double radius);
 void ring_step_build(dmb_ctx *c, double radius, bool learned);
 void ls_build(dmb_ctx *c, double radius);

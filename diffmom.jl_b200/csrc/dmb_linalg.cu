@@ -232,6 +232,7 @@ void apply_impedance(dmb_ctx *c, const double *zs) {
   }
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   c->pc_valid = false;
+  c->z_version++;
 }
 
 void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
@@ -251,6 +252,20 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
     else
       DMB_LAUNCH(c, k_gemm_zx<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);
   }
+}
+
+// The Krylov operator of the batched solves: complex64 Z with many
+// right-hand sides runs on the tensor cores (3xTF32, FP32 accumulation), so
+// GMRES then verifies convergence with the FP64 residual of matvec_dev.
+bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs) {
+  return c->z_prec == DMB_PREC_MIXED && nrhs >= c->tc_min_rhs && tc_available(c);
+}
+
+void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs) {
+  if (matvec_op_inexact(c, nrhs))
+    tc_zx(c, x, y, nrhs);
+  else
+    matvec_dev(c, x, y, nrhs);
 }
 
 unsigned read_err_word(dmb_ctx *c);

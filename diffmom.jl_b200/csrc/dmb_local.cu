@@ -673,14 +673,15 @@ struct LocalState {
   double radius = 0;
 };
 
+std::mutex g_local_mu;
+std::vector<std::pair<dmb_ctx *, LocalState *>> g_local_states;
+
 LocalState &lstate(dmb_ctx *c) {
-  static std::mutex mu;
-  static std::vector<std::pair<dmb_ctx *, LocalState *>> st;
-  std::lock_guard<std::mutex> lk(mu);
-  for (auto &p : st)
+  std::lock_guard<std::mutex> lk(g_local_mu);
+  for (auto &p : g_local_states)
     if (p.first == c) return *p.second;
-  st.push_back({c, new LocalState()});
-  return *st.back().second;
+  g_local_states.push_back({c, new LocalState()});
+  return *g_local_states.back().second;
 }
 
 template <int KM, class CT> void launch_local_inverse(dmb_ctx *c, const int *idx, const int *cnt, double2 *rows,
@@ -793,6 +794,23 @@ void check_err(dmb_ctx *c, const DevBuf &e) {
 }  // namespace
 
 namespace dmb {
+
+// drop the context's local-preconditioner buffers (called when the context is destroyed)
+void local_release(dmb_ctx *c) {
+  std::lock_guard<std::mutex> lk(g_local_mu);
+  for (size_t i = 0; i < g_local_states.size(); i++) {
+    if (g_local_states[i].first != c) continue;
+    LocalState *st = g_local_states[i].second;
+    for (DevBuf *b : {&st->idx_s, &st->cnt_s, &st->rows_s, &st->idx_l, &st->cnt_l, &st->rows_l, &st->feat,
+                      &st->tgt, &st->wgt, &st->partial, &st->lossr, &st->grad, &st->m1, &st->m2, &st->lossv,
+                      &st->rowid, &st->rows_corr, &st->apply_tmp, &st->rring, &st->gring, &st->eta, &st->outs})
+      b->release();
+    delete st;
+    g_local_states.erase(g_local_states.begin() + i);
+    return;
+  }
+}
+
 
 // plain local inverses (kind LOCAL_INV) or learned rows (kind LEARNED)
 void local_inverse_build(dmb_ctx *c, double radius, int kmax) {

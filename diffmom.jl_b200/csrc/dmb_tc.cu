@@ -268,6 +268,192 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 }
 
 // ---------------------------------------------------------------------------
+// General complex GEMM  Y (op)= A B^T  for many right-hand sides.
+//
+// A'' (2 Mpad rows) and B'' (Rpad rows) hold K'' = 6 Kpad floats per row in
+// blocks of 256 complex K: block kb occupies floats [1536 kb, 1536 kb + 1536)
+// with the six 256-wide segments of the layout above.  One CTA computes a
+// 64 x 256 complex tile over all nchunks 32-float K chunks (same warp roles and
+// bounded waits as k_tc_syrk); the output is complex128 column-major,
+// Y[m + r ldy] = acc (mode 0) or -= acc (mode 1).  grid.x walks the column
+// tiles fastest, so the CTAs that share an A row tile run together and read it
+// from DRAM once.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
+                                                    const __grid_constant__ CUtensorMap tmB, int nchunks, int64_t M,
+                                                    int64_t Rv, double2 *__restrict__ Y, int64_t ldy, int mode,
+                                                    unsigned *err) {
+  const int64_t col0 = (int64_t)blockIdx.x * TC_BN;
+  const int64_t row0 = (int64_t)blockIdx.y * 64;
+  if (row0 >= M || col0 >= Rv) return;  // uniform
+
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char *gbase = smem_raw + (base - raw);
+  const uint32_t sA = base;
+  const uint32_t sB = base + TC_STAGES * TC_A_STAGE;
+  const uint32_t sBar = sB + TC_STAGES * TC_B_STAGE;
+  uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
+  volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * TC_STAGES, done = sBar + 16 * TC_STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(const_cast<uint32_t *>(tmem_slot))),
+                 "r"(TC_BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    for (int kc = 0; kc < nchunks; kc++) {
+      const int s = kc % TC_STAGES;
+      if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
+      mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
+      tma_load_2d(sA + s * TC_A_STAGE, &tmA, kc * TC_BK, (int)(2 * row0), full0 + 8 * s);
+      tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
+    }
+  } else if (warp == 1 && lane == 0) {
+    bool ok = true;
+    for (int kc = 0; kc < nchunks && ok; kc++) {
+      const int s = kc % TC_STAGES;
+      if (!mbar_wait(full0 + 8 * s, (kc / TC_STAGES) & 1, err, abort_flag)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int k = 0; k < TC_BK / 8; k++) {
+        const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
+        const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
+        umma_tf32(tmem_d, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+      }
+      umma_commit(empty0 + 8 * s);
+    }
+    if (ok) umma_commit(done);
+  }
+  __syncwarp();
+
+  const int have = __syncthreads_and(mbar_wait(done, 0, err, abort_flag) ? 1 : 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (have) {
+    float *E = reinterpret_cast<float *>(gbase);  // 128 x 33 staging
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int rl = threadIdx.x & 63, qh = threadIdx.x >> 6;
+    const int64_t gr = row0 + rl;
+    for (int cc = 0; cc < TC_BN / 32; cc++) {
+      if (col0 + cc * 32 >= Rv) break;  // uniform
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(tmem_d + lane_base + (uint32_t)(cc * 32)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int row = warp * 32 + lane;
+#pragma unroll
+      for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
+      __syncthreads();
+      // thread -> complex row rl (consecutive threads: consecutive rows of a column)
+      if (gr < M) {
+#pragma unroll 4
+        for (int i = 0; i < 16; i++) {
+          const int q = qh + 2 * i;
+          const int64_t gc = col0 + cc * 32 + q;
+          if (gc < Rv) {
+            double2 *p = Y + gc * ldy + gr;
+            const double re = E[rl * 33 + q], im = E[(64 + rl) * 33 + q];
+            if (mode == 0) {
+              *p = make_double2(re, im);
+            } else {
+              double2 cv = *p;
+              cv.x -= re;
+              cv.y -= im;
+              *p = cv;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TC_BN) : "memory");
+}
+
+// split one complex value into the six 256-strided A'' / B'' segment entries
+__device__ __forceinline__ void put_a(float *ar, float *ai, int kk, float vr, float vi) {
+  const float rh = tf32_rna(vr), ih = tf32_rna(vi);
+  const float rl = tf32_rna(vr - rh), il = tf32_rna(vi - ih);
+  ar[kk] = rh; ar[256 + kk] = -ih; ar[512 + kk] = rh; ar[768 + kk] = -ih; ar[1024 + kk] = rl; ar[1280 + kk] = -il;
+  ai[kk] = ih; ai[256 + kk] = rh;  ai[512 + kk] = ih; ai[768 + kk] = rh;  ai[1024 + kk] = il; ai[1280 + kk] = rl;
+}
+
+// A'' from a complex64 matrix: element (m, k) = S[m ld + k] (TRANS: S[k ld + m]),
+// zero outside M x K.  32 x 32 tiles through shared memory so both the read
+// and the write are coalesced; the grid covers exactly Mpad x Kpad.
+template <bool TRANS>
+__global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kpad, const float2 *__restrict__ S,
+                                                int64_t ld, float *__restrict__ Ap) {
+  __shared__ float2 tile[32][33];
+  const int64_t m0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int i = ty; i < 32; i += 8) {
+    if (TRANS) {
+      const int64_t k = k0 + i, m = m0 + tx;
+      tile[tx][i] = (m < M && k < K) ? S[k * ld + m] : make_float2(0.f, 0.f);
+    } else {
+      const int64_t m = m0 + i, k = k0 + tx;
+      tile[i][tx] = (m < M && k < K) ? S[m * ld + k] : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  const int64_t lda = 6 * Kpad;
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t m = m0 + i, k = k0 + tx;
+    const float2 v = tile[i][tx];
+    float *ar = Ap + (128 * (m / 64) + m % 64) * lda + (k / 256) * 1536;
+    put_a(ar, ar + 64 * lda, (int)(k % 256), v.x, v.y);
+  }
+}
+
+// B'' from complex128 column-major right-hand sides: row r, complex K index k
+// holds X[k + r ldx] (zero for k >= Kv or r >= R).  The grid covers Rpad rows.
+__global__ void k_pack_b(int64_t R, int64_t Kv, int64_t Kpad, const double2 *__restrict__ X, int64_t ldx,
+                         float *__restrict__ Bp) {
+  const int64_t r = blockIdx.y;
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Kpad) return;
+  const double2 v = (r < R && k < Kv) ? X[r * ldx + k] : make_double2(0, 0);
+  const float rh = tf32_rna((float)v.x), ih = tf32_rna((float)v.y);
+  const float rl = tf32_rna((float)(v.x - (double)rh)), il = tf32_rna((float)(v.y - (double)ih));
+  float *br = Bp + r * 6 * Kpad + (k / 256) * 1536;
+  const int kk = (int)(k % 256);
+  br[kk] = rh; br[256 + kk] = ih; br[512 + kk] = rl; br[768 + kk] = il; br[1024 + kk] = rh; br[1280 + kk] = ih;
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -288,11 +474,13 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows) {
+// 2-D FP32 tensor map over a packed operand: `rows` rows of `ld` floats, boxes
+// of 32 floats (one 128-byte swizzle row) x box_rows rows.
+void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows, uint64_t ld = TC_K) {
   EncodeTiledFn enc = encode_fn();
   DMB_REQUIRE(enc, DMB_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-  cuuint64_t dims[2] = {(cuuint64_t)TC_K, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)TC_K * sizeof(float)};
+  cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
   cuuint32_t box[2] = {(cuuint32_t)TC_BK, box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
@@ -306,16 +494,37 @@ struct TcState {
   CUtensorMap mapA, mapB;
   int64_t n_key = -1;
   bool attr = false;
+  // general GEMMs: packed Z (keyed by the Z version), packed right-hand
+  // sides, packed triangular-solve panels
+  DevBuf Zp, Xp, Pa, Pb;
+  CUtensorMap mapZ, mapX, mapPa, mapPb;
+  uint64_t zp_version = ~0ull;
+  int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key = -1;
+  bool gemm_attr = false;
 };
 
+int64_t round_up(int64_t v, int64_t m) { return ((v + m - 1) / m) * m; }
+
+std::mutex g_tc_mu;
+std::vector<std::pair<dmb_ctx *, TcState *>> g_tc_states;
+
 TcState &tc_state(dmb_ctx *c) {
-  static std::mutex mu;
-  static std::vector<std::pair<dmb_ctx *, TcState *>> states;
-  std::lock_guard<std::mutex> lk(mu);
-  for (auto &p : states)
+  std::lock_guard<std::mutex> lk(g_tc_mu);
+  for (auto &p : g_tc_states)
     if (p.first == c) return *p.second;
-  states.push_back({c, new TcState()});
-  return *states.back().second;
+  g_tc_states.push_back({c, new TcState()});
+  return *g_tc_states.back().second;
+}
+
+void ensure_gemm(dmb_ctx *c, TcState &st) {
+  if (!st.err.p) {
+    st.err.ensure(16);
+    DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
+  }
+  if (!st.gemm_attr) {
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    st.gemm_attr = true;
+  }
 }
 
 }  // namespace
@@ -365,12 +574,86 @@ unsigned tc_error_word(dmb_ctx *c) {
   return e;
 }
 
-void tc_release(dmb_ctx *c) {
+// Packed Z (re-packed whenever Z changes), Y = Z X for R right-hand sides
+// (X, Y complex128 column-major N x R) on the tensor cores.
+void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
+  DMB_REQUIRE(c->z_prec == DMB_PREC_MIXED, DMB_ERR_STATE, "tensor-core Z X needs the complex64 matrix");
   TcState &st = tc_state(c);
-  st.A.release();
-  st.B.release();
-  st.err.release();
-  st.n_key = -1;
+  ensure_gemm(c, st);
+  const int64_t N = c->n, Kpad = round_up(N, 256), Mpad = round_up(N, 64), Rpad = round_up(R, TC_BN);
+  const int64_t ld = 6 * Kpad;
+  if (st.zp_version != c->z_version || st.zp_n != N) {
+    st.Zp.ensure(sizeof(float) * 2 * Mpad * ld);
+    dim3 g((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
+    DMB_LAUNCH(c, k_pack_a<false>, g, 256, 0, N, N, Kpad, c->d_Z.as<float2>(), N, st.Zp.as<float>());
+    make_map(&st.mapZ, st.Zp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
+    st.zp_version = c->z_version;
+    st.zp_n = N;
+  }
+  st.Xp.ensure(sizeof(float) * Rpad * ld);
+  if (st.xp_key != Rpad || st.xp_n != N) {
+    make_map(&st.mapX, st.Xp.as<float>(), (uint64_t)Rpad, TC_BN, (uint64_t)ld);
+    st.xp_key = Rpad;
+    st.xp_n = N;
+  }
+  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, N, Kpad, X, N,
+             st.Xp.as<float>());
+  dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
+  kt_begin(c);
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapZ, st.mapX, (int)(ld / TC_BK), N, R, Y, N, 0,
+             st.err.as<unsigned>());
+  kt_end(c, 8.0 * (double)N * (double)N * (double)R);
+}
+
+// One panel update of the batched triangular solves with the complex64
+// factor F (L strictly lower, row-major N x N):
+//   forward:  X[p0+w : N]  -= L[p0+w : N, p0 : p0+w]   X[p0 : p0+w]
+//   backward: X[0 : p0]    -= L[p0 : p0+w, 0 : p0]^T   X[p0 : p0+w]
+void tc_panel_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t p0, int width, bool backward, double2 *X,
+                     int64_t R) {
+  DMB_REQUIRE(width >= 1 && width <= 256, DMB_ERR_STATE, "panel width must be 1..256");
+  TcState &st = tc_state(c);
+  ensure_gemm(c, st);
+  const int64_t M = backward ? p0 : N - (p0 + width);
+  if (M <= 0) return;
+  const int64_t Npad = round_up(N, 64), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
+  if (st.pa_key != Npad) {
+    st.Pa.ensure(sizeof(float) * 2 * Npad * 1536);
+    make_map(&st.mapPa, st.Pa.as<float>(), (uint64_t)(2 * Npad), TC_BM, 1536);
+    st.pa_key = Npad;
+  }
+  if (st.pb_key != Rpad) {
+    st.Pb.ensure(sizeof(float) * Rpad * 1536);
+    make_map(&st.mapPb, st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536);
+    st.pb_key = Rpad;
+  }
+  dim3 ga(256 / 32, (unsigned)(Mpad / 32));
+  if (backward)
+    DMB_LAUNCH(c, k_pack_a<true>, ga, 256, 0, M, (int64_t)width, (int64_t)256, F + p0 * N, N, st.Pa.as<float>());
+  else
+    DMB_LAUNCH(c, k_pack_a<false>, ga, 256, 0, M, (int64_t)width, (int64_t)256, F + (p0 + width) * N + p0, N,
+               st.Pa.as<float>());
+  DMB_LAUNCH(c, k_pack_b, dim3(1, (unsigned)Rpad), 256, 0, R, (int64_t)width, (int64_t)256, X + p0, N,
+             st.Pb.as<float>());
+  dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
+  double2 *Yo = backward ? X : X + (p0 + width);
+  kt_begin(c);
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPa, st.mapPb, 1536 / TC_BK, M, R, Yo, N, 1,
+             st.err.as<unsigned>());
+  kt_end(c, 8.0 * (double)M * (double)width * (double)R);
+}
+
+// drop the context's packed operands (called when the context is destroyed)
+void tc_release(dmb_ctx *c) {
+  std::lock_guard<std::mutex> lk(g_tc_mu);
+  for (size_t i = 0; i < g_tc_states.size(); i++) {
+    if (g_tc_states[i].first != c) continue;
+    TcState *st = g_tc_states[i].second;
+    for (DevBuf *b : {&st->A, &st->B, &st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb}) b->release();
+    delete st;
+    g_tc_states.erase(g_tc_states.begin() + i);
+    return;
+  }
 }
 
 }  // namespace dmb

@@ -40,6 +40,9 @@ PRECOND_LEARNED = 4
 SIDE_LEFT = 0
 SIDE_RIGHT = 1
 
+OPT_TENSOR_CORES = 1
+OPT_TC_MIN_RHS = 2
+
 
 class DiffMoMError(RuntimeError):
     """Generic library failure (ErrorException in the reference)."""
@@ -129,6 +132,8 @@ SIGNATURES = {
     "dmb_net_set": ([_P, _FP], _I),
     "dmb_net_loss_grad": ([_P, _FP, _FP, _FP, _IP, _L, _FP, _FP], _I),
     "dmb_solve_resident": ([_P, ctypes.POINTER(SolveParams), ctypes.POINTER(GmresStats)], _I),
+    "dmb_solve_resident_many": ([_P, ctypes.POINTER(SolveParams), _L, _DP, _DP, _DP, _DP,
+                                 ctypes.POINTER(GmresStats)], _I),
     "dmb_copy_solution": ([_P, _DP], _I),
     "dmb_get_stream": ([_P, ctypes.POINTER(ctypes.c_void_p)], _I),
     "dmb_set_kernel_timing": ([_P, _I], _I),

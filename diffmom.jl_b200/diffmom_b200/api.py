@@ -81,6 +81,17 @@ class EFIEDevice:
         self.quad_order = 3
         self.preconditioner = None
 
+    def set_option(self, name: str, value: int) -> None:
+        """Implementation switches: "tensor_cores" (0/1) for the complex64
+        factorisation update, "tc_min_rhs" (>= 1) for the right-hand-side count
+        from which Z X and the batched near-field solves use the tensor cores."""
+        codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS}
+        if name not in codes:
+            raise ValueError(f"unknown option {name!r}")
+        self.ctx.call("dmb_set_option", codes[name], int(value))
+        if name == "tensor_cores":
+            self.preconditioner = None
+
     # -- impedance matrix -----------------------------------------------
     def assemble(self, k: float, quad_order: int = 3, eta0: float = ETA0_DEFAULT,
                  precision: str = "fp64", copy_out: bool = False):
@@ -200,6 +211,52 @@ class EFIEDevice:
         self.ctx.call("dmb_rhs_plane_waves", nat.dptr(kv), nat.dptr(e0), nat.dptr(pl), R,
                       int(quad_order), nat.dptr(V))
         return V
+
+    # -- batched resident solve -------------------------------------------
+    _PC_CODES = {"none": nat.PRECOND_NONE, "lu": nat.PRECOND_NF_LU, "diag": nat.PRECOND_NF_DIAG,
+                 "local": nat.PRECOND_LOCAL_INV, "learned": nat.PRECOND_LEARNED}
+
+    def solve_many(self, k: float, kvecs, pols, E0s=None, precision: str = "mixed",
+                   preconditioner: str = "lu", cutoff: float = math.inf, tol: float = 1e-6,
+                   maxiter: int = 300, precond_side: str = "left", quad_order: int = 3,
+                   eta0: float = ETA0_DEFAULT, rcs: bool = True):
+        """Assemble Z, build the preconditioner, solve all incidences by block
+        GMRES and (rcs=True) return the monostatic sigma of each; the currents
+        stay on the device (``currents()``)."""
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        if preconditioner not in self._PC_CODES:
+            raise ValueError(f"unknown preconditioner {preconditioner!r}")
+        side = {"left": nat.SIDE_LEFT, "right": nat.SIDE_RIGHT}.get(precond_side)
+        if side is None:
+            raise ValueError(f"Invalid precond_side: {precond_side} (expected :left or :right)")
+        kv = np.ascontiguousarray(np.atleast_2d(kvecs), dtype=np.float64)
+        pl = np.ascontiguousarray(np.atleast_2d(pols), dtype=np.float64)
+        R = kv.shape[0]
+        e0 = np.ascontiguousarray(np.ones(R) if E0s is None else np.broadcast_to(E0s, (R,)), dtype=np.float64)
+        if kv.shape != (R, 3) or pl.shape != (R, 3):
+            raise nat.DimensionMismatch("kvecs and pols must both be R x 3")
+        p = nat.SolveParams()
+        p.k, p.eta0, p.cutoff, p.tol = float(k), float(eta0), float(cutoff), float(tol)
+        p.quad_order, p.precision, p.precond_kind = int(quad_order), _PRECISIONS[precision], \
+            self._PC_CODES[preconditioner]
+        p.precond_side, p.maxiter = side, int(maxiter)
+        sig = np.empty(R, dtype=np.float64) if rcs else None
+        st = nat.GmresStats()
+        self.ctx.call("dmb_solve_resident_many", ctypes.byref(p), R, nat.dptr(kv), nat.dptr(e0), nat.dptr(pl),
+                      nat.dptr(sig) if rcs else None, ctypes.byref(st))
+        self.k, self.eta0, self.quad_order, self.precision = float(k), float(eta0), quad_order, precision
+        self._sol_r = R
+        return sig, GmresResult(st.niter, bool(st.solved), st.residual, st.true_residual, st.restarts)
+
+    def currents(self) -> np.ndarray:
+        """The resident N x R currents of the last solve_many."""
+        R = getattr(self, "_sol_r", 0)
+        if R < 1:
+            raise nat.DiffMoMError("no resident solution")
+        I = np.empty((self.N, R), dtype=np.complex128, order="F")
+        self.ctx.call("dmb_copy_solution", nat.dptr(I))
+        return I
 
     # -- solvers ----------------------------------------------------------
     def gmres(self, rhs, tol=1e-8, maxiter=200, preconditioner=None, precond_side="left",
@@ -481,6 +538,54 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                                 preconditioner_time_s=t_pc, gmres_iters=iters,
                                 gmres_residual=resid, true_residual=tres, warnings=warnings,
                                 timings={f: getattr(tm, f) for f, _ in nat.Timings._fields_})
+    finally:
+        if own:
+            dev.close()
+
+
+@dataclass
+class MonostaticResult:
+    sigma: np.ndarray            # (R,) monostatic RCS, m^2
+    gmres_iters: int
+    true_residual: float         # max over incidences of ||b - Z x|| / ||b||
+    refinements: int
+    currents: np.ndarray | None  # N x R when requested
+
+
+def monostatic_rcs_sweep(mesh: TriMesh, freq_hz, excitations, precision: str = "mixed",
+                         preconditioner: str = "lu", nf_cutoff_lambda: float = math.inf,
+                         gmres_tol: float = 1e-6, gmres_maxiter: int = 300, precond_side: str = "left",
+                         quad_order: int = 3, c0: float = C0_DEFAULT, return_currents: bool = False,
+                         device: EFIEDevice | None = None, rwg: RWGData | None = None) -> MonostaticResult:
+    """Monostatic RCS over many plane-wave incidences: what a loop of
+    solve_scattering (Workflow.jl:67-317) + backscatter_rcs (Diagnostics.jl:
+    476-517) per incidence computes, with Z and its preconditioner built once
+    and all incidences solved together by block GMRES on the device.
+
+    With nf_cutoff_lambda = inf the preconditioner is the complete complex64
+    LDL^T of Z (GMRES with FP64-residual refinement); a finite cutoff gives
+    the reference's near-field preconditioner."""
+    f = float(freq_hz)
+    if not (math.isfinite(f) and f > 0):
+        raise ValueError(f"monostatic_rcs_sweep: freq_hz must be finite and positive, got {freq_hz}")
+    k = _frequency_to_wavenumber(f, c0)
+    exc = list(excitations)
+    if not exc or not all(isinstance(e, PlaneWaveExcitation) for e in exc):
+        raise ValueError("monostatic_rcs_sweep: excitations must be a non-empty list of plane waves")
+    for e in exc:
+        if abs(float(np.linalg.norm(e.k_vec)) - k) > 1e-8 * k:
+            raise ValueError("monostatic_rcs_sweep: plane-wave |k_vec| must equal 2*pi*freq/c0")
+    rwg = rwg if rwg is not None else build_rwg(mesh)
+    dev = device or EFIEDevice(mesh, rwg)
+    own = device is None
+    try:
+        lam = c0 / f
+        sig, st = dev.solve_many(k, [e.k_vec for e in exc], [e.pol for e in exc], [e.E0 for e in exc],
+                                 precision=precision, preconditioner=preconditioner,
+                                 cutoff=nf_cutoff_lambda * lam, tol=gmres_tol, maxiter=gmres_maxiter,
+                                 precond_side=precond_side, quad_order=quad_order)
+        cur = dev.currents() if return_currents else None
+        return MonostaticResult(sig, st.niter, st.true_residual, st.restarts, cur)
     finally:
         if own:
             dev.close()

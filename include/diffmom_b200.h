@@ -88,8 +88,13 @@ const char *dmb_version(void);
 
 /* Implementation options (no reference counterpart).
  * DMB_OPT_TENSOR_CORES: 1 (default) runs the complex64 factorisation update on
- * the tcgen05 tensor cores (3xTF32), 0 on FP32 SIMT units. */
+ * the tcgen05 tensor cores (3xTF32), 0 on FP32 SIMT units.
+ * DMB_OPT_TC_MIN_RHS: from this many right-hand sides (default 64) a complex64
+ * Z X (dmb_matvec and the GMRES operator) and the panel updates of the batched
+ * near-field solves run on the tensor cores (3xTF32, FP32 accumulation); GMRES
+ * then confirms convergence on the FP64 residual and refines where needed. */
 #define DMB_OPT_TENSOR_CORES 1
+#define DMB_OPT_TC_MIN_RHS 2
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 
 /* ---- mesh and basis ---------------------------------------------------- */
@@ -121,7 +126,9 @@ dmb_status dmb_apply_impedance(dmb_ctx *ctx, const double *zs);
 
 /* ---- operators --------------------------------------------------------- */
 /* Dense Z*x (the zgemv inside Krylov.gmres) for nrhs column-major
- * right-hand sides: y = Z x. */
+ * right-hand sides: y = Z x.  FP64 accumulation, except for a complex64 Z
+ * with nrhs >= DMB_OPT_TC_MIN_RHS: then a tensor-core 3xTF32 GEMM
+ * (~1e-6 relative). */
 dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
 /* Matrix-free Z*x (MatrixFreeEFIEOperator mul!, src/assembly/EFIE.jl:867-909):
  * entries are recomputed from the geometry on every call, nothing of size
@@ -215,6 +222,20 @@ typedef struct {
   double kvec[3], pol[3], E0;
 } dmb_solve_params;
 dmb_status dmb_solve_resident(dmb_ctx *ctx, const dmb_solve_params *p, dmb_gmres_stats *stats);
+/* Many incidences at once: the per-column loop over
+ * assemble_multiple_excitations (src/assembly/Excitation.jl:2738-2797) with
+ * solve_scattering's dense GMRES, and backscatter_rcs
+ * (src/postprocessing/Diagnostics.jl:460-517) of each solution.  Z and the
+ * preconditioner are built once, the R right-hand sides (kvecs, pols R x 3
+ * row-major, E0s R; p->kvec/pol/E0 are ignored) are solved by block GMRES,
+ * and, when sigma_out is non-NULL, sigma_out[r] = 4 pi |E_inf(-k_hat_r)|^2 /
+ * |E0_r|^2 is computed on the device (only these R values are copied back).
+ * The N x R currents stay on the device. */
+dmb_status dmb_solve_resident_many(dmb_ctx *ctx, const dmb_solve_params *p, int64_t R, const double *kvecs,
+                                   const double *E0s, const double *pols, double *sigma_out,
+                                   dmb_gmres_stats *stats);
+/* Copy the resident currents (N x 1, or N x R after dmb_solve_resident_many,
+ * column-major complex128). */
 dmb_status dmb_copy_solution(dmb_ctx *ctx, double *I_out);
 
 /* ---- measurement hooks -------------------------------------------------- */

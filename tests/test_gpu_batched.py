@@ -1,0 +1,148 @@
+"""Many right-hand sides: the tensor-core complex GEMM Z X, the panel-blocked
+near-field solves and block GMRES with FP64-residual refinement, each checked
+against its FP64-accumulated counterpart on the same inputs."""
+import math
+
+import numpy as np
+import pytest
+
+from diffmom_b200 import EFIEDevice, build_rwg, make_rect_plate
+
+pytestmark = pytest.mark.gpu
+
+C0 = 299792458.0
+K3 = 2 * math.pi * 3e9 / C0
+
+
+def _plate(n, side=0.1):
+    m = make_rect_plate(side, side, n, n)
+    return EFIEDevice(m, build_rwg(m))
+
+
+def _rand(N, R, seed):
+    rng = np.random.default_rng(seed)
+    return np.asfortranarray(rng.standard_normal((N, R)) + 1j * rng.standard_normal((N, R)))
+
+
+def _waves(k, R, seed):
+    # theta in [0, 80) deg, phi in [0, 360) deg; half theta-, half phi-polarised
+    rng = np.random.default_rng(seed)
+    th = np.deg2rad(rng.uniform(0, 80, R))
+    ph = np.deg2rad(rng.uniform(0, 360, R))
+    rhat = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], 1)
+    tha = np.stack([np.cos(th) * np.cos(ph), np.cos(th) * np.sin(ph), -np.sin(th)], 1)
+    pha = np.stack([-np.sin(ph), np.cos(ph), np.zeros(R)], 1)
+    pol = np.where((np.arange(R) % 2 == 0)[:, None], tha, pha)
+    return -k * rhat, np.ones(R), pol
+
+
+def test_tensor_core_zx_matches_fp64_accumulation():
+    dev = _plate(24)  # 1,680 RWG: K = 6.6 panels of 256, ragged edges in M, K and R
+    dev.assemble(K3, precision="mixed")
+    for R in (64, 300):
+        X = _rand(dev.N, R, R)
+        dev.set_option("tc_min_rhs", 1 << 30)
+        Y64 = dev.matvec(X)
+        dev.set_option("tc_min_rhs", 64)
+        Ytc = dev.matvec(X)
+        err = np.linalg.norm(Ytc - Y64, axis=0) / np.linalg.norm(Y64, axis=0)
+        print(f"R={R}: tensor-core Z X max column error {err.max():.2e}")
+        # 3xTF32 operands (~2^-22) with FP32 accumulation in TMEM over
+        # K'' = 6 x 1,792 floats
+        assert err.max() < 5e-5
+    dev.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batched_nearfield_solve_matches_column_solves(precision):
+    dev = _plate(24)
+    dev.assemble(K3, precision=precision)
+    dev.build_nearfield(0.05, "lu")
+    for R in (8, 37, 200):
+        X = _rand(dev.N, R, 7 + R)
+        Yb = dev.nf_apply(X)
+        cols = sorted({0, R // 2, R - 1})
+        Ys = np.stack([dev.nf_apply(X[:, j]) for j in cols], 1)
+        err = np.linalg.norm(Yb[:, cols] - Ys) / np.linalg.norm(Ys)
+        print(f"{precision} R={R}: batched vs column solves {err:.2e}")
+        assert err < (2e-5 if precision == "mixed" else 1e-12)
+    dev.close()
+
+
+@pytest.mark.parametrize("side", ["left", "right"])
+def test_block_gmres_many_plane_waves(side):
+    # 1,680 RWG plate (1 lambda), 256 incidences, complex64 Z, full c64 LDL^T as
+    # the preconditioner: the Krylov products run on the tensor cores, the
+    # returned currents must meet 1e-6 on the FP64 residual and match the FP64
+    # solution of the same systems
+    dev = _plate(24)
+    kv, e0, pol = _waves(K3, 256, 20260001)
+    dev.assemble(K3, precision="fp64")
+    V = dev.plane_wave_rhs(kv, e0, pol)
+    dev.build_nearfield(float("inf"), "lu")
+    x64, st64 = dev.gmres(V, tol=1e-10, maxiter=100, preconditioner=dev.preconditioner)
+    dev.assemble(K3, precision="mixed")
+    P = dev.build_nearfield(float("inf"), "lu")
+    x, st = dev.gmres(V, tol=1e-6, maxiter=100, preconditioner=P, precond_side=side)
+    err = np.linalg.norm(x - x64, axis=0) / np.linalg.norm(x64, axis=0)
+    print(f"{side}: {st.niter} iterations, {st.restarts} refinement cycles, true residual "
+          f"{st.true_residual:.2e}, max current error vs FP64 {err.max():.2e}")
+    assert st.solved and st.true_residual <= 1e-6
+    assert err.max() < 1e-4
+    dev.close()
+
+
+def test_monostatic_sweep_matches_oracle():
+    # C1 plate (72 triangles, 96 RWG), six incidences: currents by dense
+    # solves of the oracle's Z, far field by its radiation vectors
+    import oracle as orc
+    from diffmom_b200 import make_plane_wave, monostatic_rcs_sweep
+    m = make_rect_plate(0.1, 0.1, 6, 6)
+    rwg = build_rwg(m)
+    k = 2 * math.pi / 0.1
+    kv, e0, pol = _waves(k, 6, 3)
+    exc = [make_plane_wave(kv[i], 1.0, pol[i]) for i in range(6)]
+    res = monostatic_rcs_sweep(m, k * C0 / (2 * math.pi), exc, precision="fp64", gmres_tol=1e-12,
+                               rwg=rwg, return_currents=True)
+    oc = orc.OracleCache(m, rwg, 3)
+    Z = oc.assemble_z(k)
+    sig = []
+    for i in range(6):
+        I = np.linalg.solve(Z, oc.plane_wave_rhs(kv[i], 1.0, pol[i]))
+        G = oc.radiation_vectors(-kv[i] / k, k)
+        E = G @ I
+        sig.append(4 * math.pi * np.sum(np.abs(E) ** 2))
+        assert np.linalg.norm(res.currents[:, i] - I) <= 1e-8 * np.linalg.norm(I)
+    sig = np.array(sig)
+    err = np.abs(res.sigma - sig) / sig
+    print(f"monostatic sigma vs oracle: max rel {err.max():.2e}")
+    assert err.max() < 1e-8
+
+
+def test_monostatic_sweep_mixed_vs_fp64():
+    # 1,680-RWG plate, 96 incidences: complex64 Z + tensor-core block GMRES
+    # against the plain FP64 path (reference near-field preconditioner, 1 lambda)
+    from diffmom_b200 import EFIEDevice, make_plane_wave, monostatic_rcs_sweep
+    from diffmom_b200 import compute_farfield, bistatic_rcs, SphGrid
+    m = make_rect_plate(0.1, 0.1, 24, 24)
+    rwg = build_rwg(m)
+    dev = EFIEDevice(m, rwg)
+    kv, e0, pol = _waves(K3, 96, 11)
+    exc = [make_plane_wave(kv[i], 1.0, pol[i]) for i in range(96)]
+    r64 = monostatic_rcs_sweep(m, 3e9, exc, precision="fp64", nf_cutoff_lambda=1.0, gmres_tol=1e-10,
+                               device=dev, rwg=rwg, return_currents=True)
+    # the fused monostatic kernel agrees with the general far-field path
+    for i in (0, 47, 95):
+        grid = SphGrid(rhat=(-kv[i] / K3)[None], theta=np.zeros(1), phi=np.zeros(1), w=np.ones(1))
+        E = compute_farfield(dev, grid, r64.currents[:, i])
+        s_ff = bistatic_rcs(np.asarray(E).reshape(3, -1)[:, :1])[0]
+        assert abs(s_ff - r64.sigma[i]) <= 1e-12 * s_ff
+    rm = monostatic_rcs_sweep(m, 3e9, exc, precision="mixed", gmres_tol=1e-6, device=dev, rwg=rwg,
+                              return_currents=True)
+    rel = np.abs(rm.sigma - r64.sigma) / r64.sigma.max()
+    cur = np.linalg.norm(rm.currents - r64.currents, axis=0) / np.linalg.norm(r64.currents, axis=0)
+    print(f"mixed sweep: {rm.gmres_iters} iterations, {rm.refinements} refinements, true residual "
+          f"{rm.true_residual:.2e}; RCS error {rel.max():.2e} of max sigma, current error {cur.max():.2e}")
+    assert rm.true_residual <= 1e-6
+    assert rel.max() <= 1e-4
+    dev.close()
