@@ -90,6 +90,82 @@ __global__ void __launch_bounds__(256) k_gemm_zx(int64_t N, int64_t R, const ZC 
     }
 }
 
+// Y = Z X (complex64 Z) with FP64 accumulation for many right-hand sides (the
+// refinement residual and true-residual products).  128 x 64 complex output tile per
+// 256-thread CTA, 8 x 4 complex accumulators per thread; Z stays in its
+// storage type in shared memory (complex64: half the bytes), K chunks of 16
+// with the next chunk prefetched into registers while the current one is
+// consumed.  Thread (tx, ty): rows ty + 16 i, columns tx + 16 j.
+template <class ZC>
+__global__ void __launch_bounds__(256, 1) k_gemm_zx_wide(int64_t N, int64_t R, const ZC *__restrict__ Z,
+                                                         const double2 *__restrict__ X,
+                                                         double2 *__restrict__ Y) {
+  __shared__ ZC As[16][128 + 1];
+  __shared__ double2 Bs[16][64 + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int64_t m0 = (int64_t)blockIdx.x * 128, r0 = (int64_t)blockIdx.y * 64;
+  // loader mapping: A element e = threadIdx.x + 256 u (u < 8): row e / 16, k e % 16
+  //                 B element e = threadIdx.x + 256 u (u < 4): column e / 16, k e % 16
+  const int lk = threadIdx.x & 15, lrow = threadIdx.x >> 4;
+  ZC pa[8];
+  double2 pb[4];
+  auto fetch = [&](int64_t k0) {
+    const int64_t kx = k0 + lk;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int64_t m = m0 + lrow + 16 * u;
+      pa[u] = (m < N && kx < N) ? Z[m * N + kx] : ZC{};
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int64_t r = r0 + lrow + 16 * u;
+      pb[u] = (r < R && kx < N) ? X[r * N + kx] : make_double2(0, 0);
+    }
+  };
+  double2 acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0, 0);
+  fetch(0);
+  for (int64_t k0 = 0; k0 < N; k0 += 16) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) As[lk][lrow + 16 * u] = pa[u];
+#pragma unroll
+    for (int u = 0; u < 4; u++) Bs[lk][lrow + 16 * u] = pb[u];
+    __syncthreads();
+    if (k0 + 16 < N) fetch(k0 + 16);
+#pragma unroll 4
+    for (int kk = 0; kk < 16; kk++) {
+      double2 a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = to_d2(As[kk][ty + 16 * i]);
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int64_t r = r0 + tx + 16 * j;
+    if (r >= R) continue;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int64_t m = m0 + ty + 16 * i;
+      if (m < N) Y[r * N + m] = acc[i][j];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Z out / entries / conversions
 // ---------------------------------------------------------------------------
@@ -245,12 +321,15 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
       DMB_LAUNCH(c, k_gemv<double2>, g, 256, 0, N, c->d_Z.as<double2>(), xd, yd);
     else
       DMB_LAUNCH(c, k_gemv<float2>, g, 256, 0, N, c->d_Z.as<float2>(), xd, yd);
-  } else {
+  } else if (nrhs < 32 || c->z_prec == DMB_PREC_FP64) {
     dim3 g(blocks_for(N, 64), blocks_for(nrhs, 64));
     if (c->z_prec == DMB_PREC_FP64)
       DMB_LAUNCH(c, k_gemm_zx<double2>, g, 256, 0, N, nrhs, c->d_Z.as<double2>(), xd, yd);
     else
       DMB_LAUNCH(c, k_gemm_zx<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);
+  } else {
+    dim3 g(blocks_for(N, 128), blocks_for(nrhs, 64));
+    DMB_LAUNCH(c, k_gemm_zx_wide<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);
   }
 }
 

@@ -373,23 +373,28 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
 #pragma unroll
       for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
       __syncthreads();
-      // thread -> complex row rl (consecutive threads: consecutive rows of a column)
+      // thread -> complex row rl (consecutive threads: consecutive rows of a
+      // column); for the subtracting form all 16 loads are issued before any
+      // store so they are in flight together
       if (gr < M) {
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-          const int q = qh + 2 * i;
-          const int64_t gc = col0 + cc * 32 + q;
-          if (gc < Rv) {
-            double2 *p = Y + gc * ldy + gr;
-            const double re = E[rl * 33 + q], im = E[(64 + rl) * 33 + q];
-            if (mode == 0) {
-              *p = make_double2(re, im);
-            } else {
-              double2 cv = *p;
-              cv.x -= re;
-              cv.y -= im;
-              *p = cv;
-            }
+        const int64_t gc0 = col0 + cc * 32 + qh;
+        if (mode == 0) {
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            const int q = qh + 2 * i;
+            if (gc0 + 2 * i < Rv) Y[(gc0 + 2 * i) * ldy + gr] = make_double2(E[rl * 33 + q], E[(64 + rl) * 33 + q]);
+          }
+        } else {
+          double2 cv[16];
+#pragma unroll
+          for (int i = 0; i < 16; i++)
+            cv[i] = (gc0 + 2 * i < Rv) ? __ldcs(Y + (gc0 + 2 * i) * ldy + gr) : make_double2(0, 0);
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            const int q = qh + 2 * i;
+            if (gc0 + 2 * i < Rv)
+              __stcs(Y + (gc0 + 2 * i) * ldy + gr,
+                     make_double2(cv[i].x - E[rl * 33 + q], cv[i].y - E[(64 + rl) * 33 + q]));
           }
         }
       }

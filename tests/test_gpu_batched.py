@@ -53,6 +53,20 @@ def test_tensor_core_zx_matches_fp64_accumulation():
     dev.close()
 
 
+def test_fp64_accumulated_zx_matches_column_products():
+    # the wide-tile FP64-accumulated Z X (refinement residuals) against the
+    # one-column product, ragged M and R
+    dev = _plate(24)
+    dev.assemble(K3, precision="mixed")
+    dev.set_option("tc_min_rhs", 1 << 30)
+    X = _rand(dev.N, 70, 5)
+    Y = dev.matvec(X)
+    for j in (0, 35, 69):
+        y = dev.matvec(np.ascontiguousarray(X[:, j]))
+        assert np.linalg.norm(Y[:, j] - y) <= 1e-13 * np.linalg.norm(y)
+    dev.close()
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_batched_nearfield_solve_matches_column_solves(precision):
     dev = _plate(24)
