@@ -751,20 +751,28 @@ template <class C> void trsm_panel_attrs() {
   done = true;
 }
 
-template <class C> void panel_update(dmb_ctx *c, const C *F, int64_t N, int64_t p0, int w, bool bwd, double2 *X,
-                                     int64_t R) {
-  const int64_t M = bwd ? p0 : N - (p0 + w);
+// X[r_lo : r_hi] -= L[r_lo : r_hi, k_lo : k_lo + w] X[k_lo : k_lo + w]   (forward)
+// X[r_lo : r_hi] -= L[k_lo : k_lo + w, r_lo : r_hi]^T X[k_lo : k_lo + w] (backward)
+template <class C> void trsm_update(dmb_ctx *c, const C *F, int64_t N, int64_t r_lo, int64_t r_hi, int64_t k_lo,
+                                    int w, bool bwd, double2 *X, int64_t R) {
+  const int64_t M = r_hi - r_lo;
   if (M <= 0) return;
   if (std::is_same<C, float2>::value && R >= c->tc_min_rhs && dmb::tc_available(c)) {
-    dmb::tc_panel_update(c, (const float2 *)F, N, p0, w, bwd, X, R);
+    dmb::tc_trsm_update(c, (const float2 *)F, N, r_lo, r_hi, k_lo, w, bwd, X, R);
     return;
   }
   dim3 g(blocks_for(M, 64), blocks_for(R, 64));
   if (bwd)
-    DMB_LAUNCH(c, (k_gemm_sub<C, true>), g, 256, 0, M, R, w, F + p0 * N, N, X + p0, N, X, N);
+    DMB_LAUNCH(c, (k_gemm_sub<C, true>), g, 256, 0, M, R, w, F + k_lo * N + r_lo, N, X + k_lo, N, X + r_lo, N);
   else
-    DMB_LAUNCH(c, (k_gemm_sub<C, false>), g, 256, 0, M, R, w, F + (p0 + w) * N + p0, N, X + p0, N, X + p0 + w, N);
+    DMB_LAUNCH(c, (k_gemm_sub<C, false>), g, 256, 0, M, R, w, F + r_lo * N + k_lo, N, X + k_lo, N, X + r_lo, N);
 }
+
+// Two levels: 1024-row outer panels whose rows below (forward) / above
+// (backward) receive one K = 1024 update, and inside each outer panel
+// 256-row panels solved by k_trsm_panel with K = 256 updates restricted to
+// the outer panel.
+constexpr int TP_OUTER = 1024;
 
 template <class C> void ldlt_solve_batched(dmb_ctx *c, const C *F, double2 *X, int64_t R) {
   const int64_t N = c->n;
@@ -772,19 +780,27 @@ template <class C> void ldlt_solve_batched(dmb_ctx *c, const C *F, double2 *X, i
   trsm_panel_attrs<C>();
   const size_t sm = sizeof(C) * 64 * 65 + sizeof(double2) * TP * (TP_COLS + 1);
   const unsigned gcols = blocks_for(R, TP_COLS);
-  const int64_t npan = (N + TP - 1) / TP;
-  for (int64_t p = 0; p < npan; p++) {
-    const int64_t p0 = p * TP;
-    const int w = (int)std::min<int64_t>(TP, N - p0);
-    DMB_LAUNCH(c, (k_trsm_panel<C, false>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
-    panel_update<C>(c, F, N, p0, w, false, X, R);
+  const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
+  for (int64_t o = 0; o < nout; o++) {
+    const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
+    for (int64_t p0 = o0; p0 < o1; p0 += TP) {
+      const int w = (int)std::min<int64_t>(TP, o1 - p0);
+      DMB_LAUNCH(c, (k_trsm_panel<C, false>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
+      trsm_update<C>(c, F, N, p0 + w, o1, p0, w, false, X, R);
+    }
+    trsm_update<C>(c, F, N, o1, N, o0, (int)(o1 - o0), false, X, R);
   }
   DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, X);
-  for (int64_t p = npan - 1; p >= 0; p--) {
-    const int64_t p0 = p * TP;
-    const int w = (int)std::min<int64_t>(TP, N - p0);
-    DMB_LAUNCH(c, (k_trsm_panel<C, true>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
-    panel_update<C>(c, F, N, p0, w, true, X, R);
+  for (int64_t o = nout - 1; o >= 0; o--) {
+    const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
+    const int64_t np = (o1 - o0 + TP - 1) / TP;
+    for (int64_t pi = np - 1; pi >= 0; pi--) {
+      const int64_t p0 = o0 + pi * TP;
+      const int w = (int)std::min<int64_t>(TP, o1 - p0);
+      DMB_LAUNCH(c, (k_trsm_panel<C, true>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
+      trsm_update<C>(c, F, N, o0, p0, p0, w, true, X, R);
+    }
+    trsm_update<C>(c, F, N, 0, o0, o0, (int)(o1 - o0), true, X, R);
   }
 }
 

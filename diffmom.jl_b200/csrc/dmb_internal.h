@@ -235,8 +235,8 @@ void local_inverse_build(dmb_ctx *c, double radius, int kmax);
 // tensor-core complex GEMMs (dmb_tc.cu)
 bool tc_available(dmb_ctx *c);
 void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R);
-void tc_panel_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t p0, int width, bool backward, double2 *X,
-                     int64_t R);
+void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_t r_hi, int64_t k_lo, int width,
+                    bool backward, double2 *X, int64_t R);
 unsigned tc_error_word(dmb_ctx *c);
 void tc_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);

@@ -502,7 +502,7 @@ struct TcState {
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
   // sides, packed triangular-solve panels
   DevBuf Zp, Xp, Pa, Pb;
-  CUtensorMap mapZ, mapX, mapPa, mapPb;
+  CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4];
   uint64_t zp_version = ~0ull;
   int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key = -1;
   bool gemm_attr = false;
@@ -610,41 +610,43 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
 
-// One panel update of the batched triangular solves with the complex64
-// factor F (L strictly lower, row-major N x N):
-//   forward:  X[p0+w : N]  -= L[p0+w : N, p0 : p0+w]   X[p0 : p0+w]
-//   backward: X[0 : p0]    -= L[p0 : p0+w, 0 : p0]^T   X[p0 : p0+w]
-void tc_panel_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t p0, int width, bool backward, double2 *X,
-                     int64_t R) {
-  DMB_REQUIRE(width >= 1 && width <= 256, DMB_ERR_STATE, "panel width must be 1..256");
+// One update of the batched triangular solves with the complex64 factor F
+// (L strictly lower, row-major N x N), rows [r_lo, r_hi), K = [k_lo, k_lo + w):
+//   forward:  X[r_lo : r_hi] -= L[r_lo : r_hi, k_lo : k_lo + w]   X[k_lo : k_lo + w]
+//   backward: X[r_lo : r_hi] -= L[k_lo : k_lo + w, r_lo : r_hi]^T X[k_lo : k_lo + w]
+// w <= 1024.  The packed panels live in buffers sized for w = 1024; one tensor
+// map per (buffer, K width) is kept.
+void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_t r_hi, int64_t k_lo, int width,
+                    bool backward, double2 *X, int64_t R) {
+  DMB_REQUIRE(width >= 1 && width <= 1024, DMB_ERR_STATE, "panel width must be 1..1024");
   TcState &st = tc_state(c);
   ensure_gemm(c, st);
-  const int64_t M = backward ? p0 : N - (p0 + width);
+  const int64_t M = r_hi - r_lo;
   if (M <= 0) return;
   const int64_t Npad = round_up(N, 64), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
+  const int64_t Kpad = round_up(width, 256), ld = 6 * Kpad;
+  const int kslot = (int)(Kpad / 256) - 1;  // 0..3
   if (st.pa_key != Npad) {
-    st.Pa.ensure(sizeof(float) * 2 * Npad * 1536);
-    make_map(&st.mapPa, st.Pa.as<float>(), (uint64_t)(2 * Npad), TC_BM, 1536);
+    st.Pa.ensure(sizeof(float) * 2 * Npad * 6 * 1024);
+    for (int i = 0; i < 4; i++) make_map(&st.mapPaK[i], st.Pa.as<float>(), (uint64_t)(2 * Npad), TC_BM, 1536 * (i + 1));
     st.pa_key = Npad;
   }
   if (st.pb_key != Rpad) {
-    st.Pb.ensure(sizeof(float) * Rpad * 1536);
-    make_map(&st.mapPb, st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536);
+    st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
+    for (int i = 0; i < 4; i++) make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
     st.pb_key = Rpad;
   }
-  dim3 ga(256 / 32, (unsigned)(Mpad / 32));
+  dim3 ga((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
   if (backward)
-    DMB_LAUNCH(c, k_pack_a<true>, ga, 256, 0, M, (int64_t)width, (int64_t)256, F + p0 * N, N, st.Pa.as<float>());
+    DMB_LAUNCH(c, k_pack_a<true>, ga, 256, 0, M, (int64_t)width, Kpad, F + k_lo * N + r_lo, N, st.Pa.as<float>());
   else
-    DMB_LAUNCH(c, k_pack_a<false>, ga, 256, 0, M, (int64_t)width, (int64_t)256, F + (p0 + width) * N + p0, N,
-               st.Pa.as<float>());
-  DMB_LAUNCH(c, k_pack_b, dim3(1, (unsigned)Rpad), 256, 0, R, (int64_t)width, (int64_t)256, X + p0, N,
-             st.Pb.as<float>());
+    DMB_LAUNCH(c, k_pack_a<false>, ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo, N, st.Pa.as<float>());
+  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)width, Kpad, X + k_lo,
+             N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
-  double2 *Yo = backward ? X : X + (p0 + width);
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPa, st.mapPb, 1536 / TC_BK, M, R, Yo, N, 1,
-             st.err.as<unsigned>());
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], (int)(ld / TC_BK), M, R,
+             X + r_lo, N, 1, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
 
