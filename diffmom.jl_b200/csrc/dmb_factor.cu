@@ -535,6 +535,7 @@ template <class C> void set_smem_attrs() {
 constexpr int NBO = 256;
 
 template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
+  c->f_version++;  // F changes from here on: packed copies are stale
   const int64_t N = c->n;
   set_smem_attrs<C>();
   const int nblk = (int)((N + NB - 1) / NB);
@@ -774,20 +775,63 @@ template <class C> void trsm_update(dmb_ctx *c, const C *F, int64_t N, int64_t r
 // the outer panel.
 constexpr int TP_OUTER = 1024;
 
+// forward solve restricted to rows [o0, o1): L[o0:o1, o0:o1] y = x
+template <class C> void forward_block(dmb_ctx *c, const C *F, int64_t o0, int64_t o1, double2 *X, int64_t R) {
+  const int64_t N = c->n;
+  const size_t sm = sizeof(C) * 64 * 65 + sizeof(double2) * TP * (TP_COLS + 1);
+  for (int64_t p0 = o0; p0 < o1; p0 += TP) {
+    const int w = (int)std::min<int64_t>(TP, o1 - p0);
+    DMB_LAUNCH(c, (k_trsm_panel<C, false>), blocks_for(R, TP_COLS), 256, sm, N, R, p0, w, F, c->d_dinv.as<C>(), X);
+    trsm_update<C>(c, F, N, p0 + w, o1, p0, w, false, X, R);
+  }
+}
+
+__global__ void k_identity_block(int64_t N, int64_t o0, int ow, double2 *__restrict__ X) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)ow * ow) return;
+  const int64_t r = i % ow, col = i / ow;
+  X[col * N + o0 + r] = make_double2(r == col ? 1.0 : 0.0, 0.0);
+}
+
+// Pack the complex64 factor for the tensor-core sweeps (once per
+// factorisation): L'' and (L^T)'', and the inverses of the 1024-row diagonal
+// blocks of L, obtained by solving identity blocks with the panel machinery.
+void prepare_packed_factor(dmb_ctx *c, const float2 *F) {
+  if (c->f_packed == c->f_version) return;
+  const int64_t N = c->n;
+  trsm_panel_attrs<float2>();
+  dmb::tc_trsm_pack_factor(c, F, N);
+  c->d_trsm_id.ensure(sizeof(double2) * N * TP_OUTER);
+  double2 *Xid = c->d_trsm_id.as<double2>();
+  const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
+  for (int64_t o = 0; o < nout; o++) {
+    const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
+    const int ow = (int)(o1 - o0);
+    DMB_LAUNCH(c, k_identity_block, blocks_for((int64_t)ow * ow, 256), 256, 0, N, o0, ow, Xid);
+    forward_block<float2>(c, F, o0, o1, Xid, ow);
+    dmb::tc_trsm_pack_diag(c, o, Xid + o0, N, ow);
+  }
+  c->f_packed = c->f_version;
+}
+
 template <class C> void ldlt_solve_batched(dmb_ctx *c, const C *F, double2 *X, int64_t R) {
   const int64_t N = c->n;
   const C *Linv = c->d_dinv.as<C>();
   trsm_panel_attrs<C>();
+  if (std::is_same<C, float2>::value && R >= c->tc_min_rhs && dmb::tc_available(c)) {
+    // tensor cores: every step is a GEMM on operands packed once per factor
+    prepare_packed_factor(c, (const float2 *)F);
+    dmb::tc_trsm_sweep(c, N, X, R, false);
+    DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, X);
+    dmb::tc_trsm_sweep(c, N, X, R, true);
+    return;
+  }
   const size_t sm = sizeof(C) * 64 * 65 + sizeof(double2) * TP * (TP_COLS + 1);
   const unsigned gcols = blocks_for(R, TP_COLS);
   const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
   for (int64_t o = 0; o < nout; o++) {
     const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
-    for (int64_t p0 = o0; p0 < o1; p0 += TP) {
-      const int w = (int)std::min<int64_t>(TP, o1 - p0);
-      DMB_LAUNCH(c, (k_trsm_panel<C, false>), gcols, 256, sm, N, R, p0, w, F, Linv, X);
-      trsm_update<C>(c, F, N, p0 + w, o1, p0, w, false, X, R);
-    }
+    forward_block<C>(c, F, o0, o1, X, R);
     trsm_update<C>(c, F, N, o1, N, o0, (int)(o1 - o0), false, X, R);
   }
   DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, X);

@@ -157,6 +157,9 @@ struct dmb_ctx {
   bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
+  uint64_t f_version = 0;        // bumped by every LDL^T factorisation
+  uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves
+  DevBuf d_trsm_id;              // scratch: identity blocks solved into diagonal-block inverses
   int gm_kcap = 0;              // cached GMRES basis capacity
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;
@@ -237,6 +240,9 @@ bool tc_available(dmb_ctx *c);
 void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R);
 void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_t r_hi, int64_t k_lo, int width,
                     bool backward, double2 *X, int64_t R);
+void tc_trsm_pack_factor(dmb_ctx *c, const float2 *F, int64_t N);
+void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int ow);
+void tc_trsm_sweep(dmb_ctx *c, int64_t N, double2 *X, int64_t R, bool backward);
 unsigned tc_error_word(dmb_ctx *c);
 void tc_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);

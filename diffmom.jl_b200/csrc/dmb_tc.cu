@@ -26,6 +26,7 @@
 // the kernel records an error bit, stops issuing, frees its TMEM and returns.
 #include <cuda.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "dmb_device.cuh"
@@ -275,14 +276,16 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 // with the six 256-wide segments of the layout above.  One CTA computes a
 // 64 x 256 complex tile over all nchunks 32-float K chunks (same warp roles and
 // bounded waits as k_tc_syrk); the output is complex128 column-major,
-// Y[m + r ldy] = acc (mode 0) or -= acc (mode 1).  grid.x walks the column
+// Y[m + r ldy] = acc (mode 0) or -= acc (mode 1).  A tiles start at row
+// a_row0 + 2 row0 and float column a_kx0 of the A'' map (sub-blocks of a
+// matrix packed once), B tiles at column 0.  grid.x walks the column
 // tiles fastest, so the CTAs that share an A row tile run together and read it
 // from DRAM once.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
-                                                    const __grid_constant__ CUtensorMap tmB, int nchunks, int64_t M,
-                                                    int64_t Rv, double2 *__restrict__ Y, int64_t ldy, int mode,
-                                                    unsigned *err) {
+                                                    const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
+                                                    int nchunks, int64_t M, int64_t Rv, double2 *__restrict__ Y,
+                                                    int64_t ldy, int mode, unsigned *err) {
   const int64_t col0 = (int64_t)blockIdx.x * TC_BN;
   const int64_t row0 = (int64_t)blockIdx.y * 64;
   if (row0 >= M || col0 >= Rv) return;  // uniform
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
       const int s = kc % TC_STAGES;
       if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
-      tma_load_2d(sA + s * TC_A_STAGE, &tmA, kc * TC_BK, (int)(2 * row0), full0 + 8 * s);
+      tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kc * TC_BK, a_row0 + (int)(2 * row0), full0 + 8 * s);
       tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
@@ -415,11 +418,13 @@ __device__ __forceinline__ void put_a(float *ar, float *ai, int kk, float vr, fl
   ai[kk] = ih; ai[256 + kk] = rh;  ai[512 + kk] = ih; ai[768 + kk] = rh;  ai[1024 + kk] = il; ai[1280 + kk] = rl;
 }
 
-// A'' from a complex64 matrix: element (m, k) = S[m ld + k] (TRANS: S[k ld + m]),
-// zero outside M x K.  32 x 32 tiles through shared memory so both the read
-// and the write are coalesced; the grid covers exactly Mpad x Kpad.
-template <bool TRANS>
-__global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kpad, const float2 *__restrict__ S,
+// A'' from a complex matrix: element (m, k) = S[m ld + k] (TRANS: S[k ld + m]),
+// zero outside M x K and, with LOWER, unless the element is strictly below the
+// diagonal of the source (k < m, or k > m for TRANS: L^T from the lower
+// factor).  32 x 32 tiles through shared memory so both the read and the
+// write are coalesced; the grid covers exactly Mpad x Kpad.
+template <bool TRANS, bool LOWER, class SC>
+__global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kpad, const SC *__restrict__ S,
                                                 int64_t ld, float *__restrict__ Ap) {
   __shared__ float2 tile[32][33];
   const int64_t m0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32;
@@ -427,10 +432,14 @@ __global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kp
   for (int i = ty; i < 32; i += 8) {
     if (TRANS) {
       const int64_t k = k0 + i, m = m0 + tx;
-      tile[tx][i] = (m < M && k < K) ? S[k * ld + m] : make_float2(0.f, 0.f);
+      const bool in = m < M && k < K && (!LOWER || k > m);
+      const SC v = in ? S[k * ld + m] : SC{};
+      tile[tx][i] = make_float2((float)v.x, (float)v.y);
     } else {
       const int64_t m = m0 + i, k = k0 + tx;
-      tile[i][tx] = (m < M && k < K) ? S[m * ld + k] : make_float2(0.f, 0.f);
+      const bool in = m < M && k < K && (!LOWER || k < m);
+      const SC v = in ? S[m * ld + k] : SC{};
+      tile[i][tx] = make_float2((float)v.x, (float)v.y);
     }
   }
   __syncthreads();
@@ -504,6 +513,12 @@ struct TcState {
   DevBuf Zp, Xp, Pa, Pb;
   CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4];
   uint64_t zp_version = ~0ull;
+  // factor packed once per factorisation for the batched triangular solves:
+  // L'' (strict lower), (L^T)'' and the inverses of the 1024-row diagonal
+  // blocks of L (forward) and of L^T (backward)
+  DevBuf Lp, Ltp, Dfp, Dbp;
+  CUtensorMap mapL, mapLt, mapDf, mapDb;
+  int64_t lp_n = -1;
   int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key = -1;
   bool gemm_attr = false;
 };
@@ -590,7 +605,8 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
   if (st.zp_version != c->z_version || st.zp_n != N) {
     st.Zp.ensure(sizeof(float) * 2 * Mpad * ld);
     dim3 g((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
-    DMB_LAUNCH(c, k_pack_a<false>, g, 256, 0, N, N, Kpad, c->d_Z.as<float2>(), N, st.Zp.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<false, false, float2>), g, 256, 0, N, N, Kpad, c->d_Z.as<float2>(), N,
+               st.Zp.as<float>());
     make_map(&st.mapZ, st.Zp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
     st.zp_version = c->z_version;
     st.zp_n = N;
@@ -605,7 +621,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapZ, st.mapX, (int)(ld / TC_BK), N, R, Y, N, 0,
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -638,16 +654,99 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
   }
   dim3 ga((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
   if (backward)
-    DMB_LAUNCH(c, k_pack_a<true>, ga, 256, 0, M, (int64_t)width, Kpad, F + k_lo * N + r_lo, N, st.Pa.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<true, false, float2>), ga, 256, 0, M, (int64_t)width, Kpad, F + k_lo * N + r_lo, N,
+               st.Pa.as<float>());
   else
-    DMB_LAUNCH(c, k_pack_a<false>, ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo, N, st.Pa.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<false, false, float2>), ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo, N,
+               st.Pa.as<float>());
   DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)width, Kpad, X + k_lo,
              N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], (int)(ld / TC_BK), M, R,
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
              X + r_lo, N, 1, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
+}
+
+// ---- batched triangular solves with the factor packed once ---------------
+constexpr int TB = 1024;  // outer block rows
+
+// L'' and (L^T)'' of the complex64 factor (strict lower part of F)
+void tc_trsm_pack_factor(dmb_ctx *c, const float2 *F, int64_t N) {
+  TcState &st = tc_state(c);
+  ensure_gemm(c, st);
+  const int64_t Mpad = round_up(N, 64), Kpad = round_up(N, 256), ld = 6 * Kpad;
+  const int64_t nout = (N + TB - 1) / TB;
+  if (st.lp_n != N) {
+    st.Lp.ensure(sizeof(float) * 2 * Mpad * ld);
+    st.Ltp.ensure(sizeof(float) * 2 * Mpad * ld);
+    st.Dfp.ensure(sizeof(float) * 2 * TB * nout * 6 * TB);
+    st.Dbp.ensure(sizeof(float) * 2 * TB * nout * 6 * TB);
+    make_map(&st.mapL, st.Lp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
+    make_map(&st.mapLt, st.Ltp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
+    make_map(&st.mapDf, st.Dfp.as<float>(), (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
+    make_map(&st.mapDb, st.Dbp.as<float>(), (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
+    // diagonal-block buffers: rows of a short last block stay zero
+    DMB_CUDA(cudaMemsetAsync(st.Dfp.p, 0, st.Dfp.bytes, c->stream));
+    DMB_CUDA(cudaMemsetAsync(st.Dbp.p, 0, st.Dbp.bytes, c->stream));
+    st.lp_n = N;
+  }
+  dim3 g((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
+  DMB_LAUNCH(c, (k_pack_a<false, true, float2>), g, 256, 0, N, N, Kpad, F, N, st.Lp.as<float>());
+  DMB_LAUNCH(c, (k_pack_a<true, true, float2>), g, 256, 0, N, N, Kpad, F, N, st.Ltp.as<float>());
+}
+
+// inverse of diagonal block o (ow x ow, column-major in Xb with leading
+// dimension ld) -> forward operand, its transpose -> backward operand
+void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int ow) {
+  TcState &st = tc_state(c);
+  float *df = st.Dfp.as<float>() + o * 2 * TB * 6 * TB;
+  float *db = st.Dbp.as<float>() + o * 2 * TB * 6 * TB;
+  dim3 g(TB / 32, TB / 32);
+  // forward: A(m, k) = Linv[m][k] = Xb[m + k ld]
+  DMB_LAUNCH(c, (k_pack_a<true, false, double2>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld, df);
+  // backward: A(m, k) = Linv[k][m] = Xb[k + m ld]
+  DMB_LAUNCH(c, (k_pack_a<false, false, double2>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld, db);
+}
+
+// Y (op)= A_packed[rows a_row0.., K from a_kx0] * X[k0 : k0 + w], B packed here
+void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0, int a_kx0, int64_t M, int w,
+                    const double2 *Xk, double2 *Y, int64_t N, int64_t R, int mode) {
+  if (M <= 0) return;
+  const int64_t Kpad = round_up(w, 256), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
+  const int kslot = (int)(Kpad / 256) - 1;
+  if (st.pb_key != Rpad) {
+    st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
+    for (int i = 0; i < 4; i++) make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+    st.pb_key = Rpad;
+  }
+  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk, N,
+             st.Pb.as<float>());
+  dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
+  kt_begin(c);
+  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0, (int)(6 * Kpad / TC_BK), M,
+             R, Y, N, mode, st.err.as<unsigned>());
+  kt_end(c, 8.0 * (double)M * (double)w * (double)R);
+}
+
+// one sweep of the batched solve with the packed factor:
+//   forward  (L y = x):   per block o: X_o = Linv_o X_o; X[o1:] -= L[o1:, o] X_o
+//   backward (L^T x = z): per block o, last first: X_o = Linv_o^T X_o;
+//                         X[:o0] -= L[o, :o0]^T X_o
+void tc_trsm_sweep(dmb_ctx *c, int64_t N, double2 *X, int64_t R, bool backward) {
+  TcState &st = tc_state(c);
+  DMB_REQUIRE(st.lp_n == N, DMB_ERR_STATE, "factor not packed for the batched solves");
+  const int64_t nout = (N + TB - 1) / TB;
+  for (int64_t s = 0; s < nout; s++) {
+    const int64_t o = backward ? nout - 1 - s : s;
+    const int64_t o0 = o * TB, o1 = std::min<int64_t>(N, o0 + TB);
+    const int ow = (int)(o1 - o0);
+    gemm_prepacked(c, st, backward ? st.mapDb : st.mapDf, (int)(2 * TB * o), 0, ow, ow, X + o0, X + o0, N, R, 0);
+    if (backward)
+      gemm_prepacked(c, st, st.mapLt, 0, (int)(6 * o0), o0, ow, X + o0, X, N, R, 1);
+    else
+      gemm_prepacked(c, st, st.mapL, (int)(2 * o1), (int)(6 * o0), N - o1, ow, X + o0, X + o1, N, R, 1);
+  }
 }
 
 // drop the context's packed operands (called when the context is destroyed)
@@ -656,7 +755,9 @@ void tc_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_tc_states.size(); i++) {
     if (g_tc_states[i].first != c) continue;
     TcState *st = g_tc_states[i].second;
-    for (DevBuf *b : {&st->A, &st->B, &st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb}) b->release();
+    for (DevBuf *b : {&st->A, &st->B, &st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb, &st->Lp, &st->Ltp, &st->Dfp,
+                      &st->Dbp})
+      b->release();
     delete st;
     g_tc_states.erase(g_tc_states.begin() + i);
     return;
