@@ -86,6 +86,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     c->d_trsm_id.release();
     c->d_small.release();
     dmb::tc_release(c);
+    dmb::oz_release(c);
     dmb::local_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);

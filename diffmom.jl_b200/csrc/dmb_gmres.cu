@@ -363,6 +363,8 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   unsigned e = read_err_word(c);
   DMB_REQUIRE((e & 4u) == 0, DMB_ERR_TIMEOUT, "triangular solve wait expired");
   if (inexact) DMB_REQUIRE(tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait expired");
+  if (R >= 32 && oz_available(c))
+    DMB_REQUIRE(oz_error_word(c) == 0, DMB_ERR_TIMEOUT, "int8 tensor-core GEMM: a pipeline wait expired");
   // true FP64 residual ||b - Z x|| / ||b|| per system
   if (!have_true) {
     matvec_dev(c, x, w, R);

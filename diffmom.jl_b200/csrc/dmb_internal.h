@@ -245,6 +245,11 @@ void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int
 void tc_trsm_sweep(dmb_ctx *c, int64_t N, double2 *X, int64_t R, bool backward);
 unsigned tc_error_word(dmb_ctx *c);
 void tc_release(dmb_ctx *c);
+// FP64-accurate complex64 Z X on the INT8 tensor cores (dmb_ozaki.cu)
+bool oz_available(dmb_ctx *c);
+void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R);
+unsigned oz_error_word(dmb_ctx *c);
+void oz_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);
 void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs);  // Krylov operator (may be TC)
 bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs);

@@ -327,6 +327,8 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
       DMB_LAUNCH(c, k_gemm_zx<double2>, g, 256, 0, N, nrhs, c->d_Z.as<double2>(), xd, yd);
     else
       DMB_LAUNCH(c, k_gemm_zx<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);
+  } else if (oz_available(c)) {
+    oz_zx(c, xd, yd, nrhs);
   } else {
     dim3 g(blocks_for(N, 128), blocks_for(nrhs, 64));
     DMB_LAUNCH(c, k_gemm_zx_wide<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);

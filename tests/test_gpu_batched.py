@@ -54,16 +54,26 @@ def test_tensor_core_zx_matches_fp64_accumulation():
 
 
 def test_fp64_accumulated_zx_matches_column_products():
-    # the wide-tile FP64-accumulated Z X (refinement residuals) against the
-    # one-column product, ragged M and R
+    # the FP64-accurate Z X of the refinement residuals (int8 tensor-core
+    # slices for complex64 Z from 32 right-hand sides, else SIMT FP64) against
+    # the one-column FP64 product; ragged M and R
     dev = _plate(24)
     dev.assemble(K3, precision="mixed")
     dev.set_option("tc_min_rhs", 1 << 30)
-    X = _rand(dev.N, 70, 5)
-    Y = dev.matvec(X)
-    for j in (0, 35, 69):
-        y = dev.matvec(np.ascontiguousarray(X[:, j]))
-        assert np.linalg.norm(Y[:, j] - y) <= 1e-13 * np.linalg.norm(y)
+    for R in (70, 300):
+        X = _rand(dev.N, R, 5)
+        Y = dev.matvec(X)
+        dev.set_option("tensor_cores", 0)
+        Ys = dev.matvec(X)
+        dev.set_option("tensor_cores", 1)
+        worst = 0.0
+        for j in (0, R // 2, R - 1):
+            y = dev.matvec(np.ascontiguousarray(X[:, j]))
+            worst = max(worst, np.linalg.norm(Y[:, j] - y) / np.linalg.norm(y))
+            assert np.linalg.norm(Ys[:, j] - y) <= 1e-13 * np.linalg.norm(y)
+        print(f"R={R}: int8-slice FP64 product vs one-column FP64 {worst:.2e}, "
+              f"vs SIMT FP64 {np.max(np.linalg.norm(Y - Ys, axis=0) / np.linalg.norm(Ys, axis=0)):.2e}")
+        assert worst <= 2e-11
     dev.close()
 
 
