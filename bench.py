@@ -60,14 +60,19 @@ METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
+PLATE_CELLS = 60
+
+
 def plate_c3():
     from diffmom_b200 import make_rect_plate, build_rwg
-    mesh = make_rect_plate(0.3, 0.3, 60, 60)
+    side = 0.3 * PLATE_CELLS / 60.0   # 60 cells: the 0.3 m, 10,680-RWG plate
+    mesh = make_rect_plate(side, side, PLATE_CELLS, PLATE_CELLS)
     return mesh, build_rwg(mesh)
 
 
-def waves(R=R_WAVES, seed=SEED):
+def waves(R=None, seed=SEED):
     """theta ~ U[0, 80) deg, phi ~ U[0, 360) deg; even: theta-pol, odd: phi-pol."""
+    R = R_WAVES if R is None else R
     rng = np.random.default_rng(seed)
     th = np.deg2rad(rng.uniform(0.0, 80.0, R))
     ph = np.deg2rad(rng.uniform(0.0, 360.0, R))
@@ -487,7 +492,14 @@ def main():
     ap.add_argument("--only", default=None, help="comma-separated variants to run (profiling)")
     ap.add_argument("--quick", action="store_true", help="headline only (profiling)")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the e2e leg (profiling)")
+    ap.add_argument("--plate-cells", type=int, default=60,
+                    help="profiling case: plate of this many cells per side (same cell size)")
+    ap.add_argument("--waves", type=int, default=1024, help="profiling case: number of incidences")
     args = ap.parse_args()
+    global PLATE_CELLS, R_WAVES, WORKLOAD
+    if args.plate_cells != 60 or args.waves != 1024:
+        PLATE_CELLS, R_WAVES = args.plate_cells, args.waves
+        WORKLOAD = f"profiling case: plate {PLATE_CELLS}x{PLATE_CELLS} cells, {R_WAVES} plane waves"
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -28,14 +28,6 @@ template <class F> dmb_status guarded(dmb_ctx *c, F &&f) {
   }
 }
 
-struct Staging {
-  DevBuf buf;
-  void *dev(size_t bytes) {
-    buf.ensure(bytes);
-    return buf.p;
-  }
-};
-
 void check_finite(const double *p, int64_t n, const char *what) {
   for (int64_t i = 0; i < n; i++)
     if (!std::isfinite(p[i]))
@@ -138,8 +130,9 @@ dmb_status dmb_mesh_upload(dmb_ctx *c, const double *xyz, const int64_t *tri, in
     c->nt = nt;
     c->d_xyz.ensure(sizeof(double) * 3 * nv);
     c->d_tri.ensure(sizeof(int32_t) * 3 * nt);
-    DMB_CUDA(cudaMemcpy(c->d_xyz.p, c->h_xyz.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice));
-    DMB_CUDA(cudaMemcpy(c->d_tri.p, c->h_tri.data(), sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice));
+    DMB_CUDA(cudaMemcpyAsync(c->d_xyz.p, c->h_xyz.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, c->stream));
+    DMB_CUDA(cudaMemcpyAsync(c->d_tri.p, c->h_tri.data(), sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
     c->have_mesh = true;
     c->have_rwg = false;
     c->cache_valid = false;
@@ -186,7 +179,7 @@ dmb_status dmb_rwg_upload(dmb_ctx *c, int64_t n, const int64_t *tplus, const int
     c->n = n;
     auto up = [&](DevBuf &b, const void *src, size_t bytes) {
       b.ensure(bytes);
-      DMB_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+      DMB_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream));
     };
     up(c->d_tplus, c->h_tplus.data(), 4 * n);
     up(c->d_tminus, c->h_tminus.data(), 4 * n);

@@ -801,7 +801,8 @@ void ensure_cache(dmb_ctx *c, int quad_order) {
     hw[7 + i] = c->wqh[i];
   }
   c->d_wq.ensure(sizeof(hw));
-  DMB_CUDA(cudaMemcpy(c->d_wq.p, hw, sizeof(hw), cudaMemcpyHostToDevice));
+  DMB_CUDA(cudaMemcpyAsync(c->d_wq.p, hw, sizeof(hw), cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
   c->cache_valid = true;
   c->cache_quad_order = quad_order;
 }

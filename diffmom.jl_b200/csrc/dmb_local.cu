@@ -728,12 +728,12 @@ void ensure_net(dmb_ctx *c, uint64_t seed = 1234) {
   for (int i = 0; i < NH * 2 * NH; i++) p[P_W2 + i] = nd(rng) * std::sqrt(1.f / (2 * NH));
   for (int i = 0; i < 2 * NH; i++) p[P_W3 + i] = nd(rng) * 0.01f;  // start near the plain local inverse
   c->d_net.ensure(sizeof(float) * P_TOTAL);
-  DMB_CUDA(cudaMemcpy(c->d_net.p, p.data(), sizeof(float) * P_TOTAL, cudaMemcpyHostToDevice));
+  DMB_CUDA(cudaMemcpyAsync(c->d_net.p, p.data(), sizeof(float) * P_TOTAL, cudaMemcpyHostToDevice, c->stream));
   LocalState &st = lstate(c);
   st.m1.ensure(sizeof(float) * P_TOTAL);
   st.m2.ensure(sizeof(float) * P_TOTAL);
-  DMB_CUDA(cudaMemset(st.m1.p, 0, sizeof(float) * P_TOTAL));
-  DMB_CUDA(cudaMemset(st.m2.p, 0, sizeof(float) * P_TOTAL));
+  DMB_CUDA(cudaMemsetAsync(st.m1.p, 0, sizeof(float) * P_TOTAL, c->stream));
+  DMB_CUDA(cudaMemsetAsync(st.m2.p, 0, sizeof(float) * P_TOTAL, c->stream));
   st.adam_step = 0;
   c->net_loaded = true;
 }
@@ -1000,16 +1000,17 @@ void net_loss_grad(dmb_ctx *c, const float *feat, const float *tgt, const float 
   lr.ensure(sizeof(float) * nrows);
   g.ensure(sizeof(float) * P_TOTAL);
   lv.ensure(16);
-  DMB_CUDA(cudaMemcpy(f.p, feat, sizeof(float) * nrows * KS * NF, cudaMemcpyHostToDevice));
-  DMB_CUDA(cudaMemcpy(t.p, tgt, sizeof(float) * nrows * KS * 2, cudaMemcpyHostToDevice));
-  DMB_CUDA(cudaMemcpy(s.p, wgt, sizeof(float) * nrows * KS, cudaMemcpyHostToDevice));
-  DMB_CUDA(cudaMemcpy(k.p, cnt, sizeof(int) * nrows, cudaMemcpyHostToDevice));
+  DMB_CUDA(cudaMemcpyAsync(f.p, feat, sizeof(float) * nrows * KS * NF, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(t.p, tgt, sizeof(float) * nrows * KS * 2, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(s.p, wgt, sizeof(float) * nrows * KS, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(k.p, cnt, sizeof(int) * nrows, cudaMemcpyHostToDevice, c->stream));
   DMB_LAUNCH(c, k_net_grad, (unsigned)nrows, KS, 0, nrows, (const int64_t *)nullptr, c->d_net.as<float>(),
              f.as<float>(), k.as<int>(), t.as<float>(), s.as<float>(), part.as<float>(), lr.as<float>());
   DMB_LAUNCH(c, k_grad_reduce, blocks_for(P_TOTAL + 1, 128), 128, 0, nrows, part.as<float>(), lr.as<float>(),
              g.as<float>(), lv.as<float>());
-  DMB_CUDA(cudaMemcpy(grad, g.p, sizeof(float) * P_TOTAL, cudaMemcpyDeviceToHost));
-  DMB_CUDA(cudaMemcpy(loss, lv.p, sizeof(float), cudaMemcpyDeviceToHost));
+  DMB_CUDA(cudaMemcpyAsync(grad, g.p, sizeof(float) * P_TOTAL, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(loss, lv.p, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
   for (DevBuf *b : {&f, &t, &s, &k, &part, &lr, &g, &lv}) b->release();
 }
 
@@ -1017,21 +1018,22 @@ int net_param_count() { return P_TOTAL; }
 
 void net_set(dmb_ctx *c, const float *w) {
   c->d_net.ensure(sizeof(float) * P_TOTAL);
-  DMB_CUDA(cudaMemcpy(c->d_net.p, w, sizeof(float) * P_TOTAL, cudaMemcpyHostToDevice));
+  DMB_CUDA(cudaMemcpyAsync(c->d_net.p, w, sizeof(float) * P_TOTAL, cudaMemcpyHostToDevice, c->stream));
   if (!c->net_loaded) {
     c->net_loaded = true;
     LocalState &st = lstate(c);
     st.m1.ensure(sizeof(float) * P_TOTAL);
     st.m2.ensure(sizeof(float) * P_TOTAL);
-    DMB_CUDA(cudaMemset(st.m1.p, 0, sizeof(float) * P_TOTAL));
-    DMB_CUDA(cudaMemset(st.m2.p, 0, sizeof(float) * P_TOTAL));
+    DMB_CUDA(cudaMemsetAsync(st.m1.p, 0, sizeof(float) * P_TOTAL, c->stream));
+    DMB_CUDA(cudaMemsetAsync(st.m2.p, 0, sizeof(float) * P_TOTAL, c->stream));
     st.adam_step = 0;
   }
 }
 
 void net_get(dmb_ctx *c, float *w) {
   ensure_net(c);
-  DMB_CUDA(cudaMemcpy(w, c->d_net.p, sizeof(float) * P_TOTAL, cudaMemcpyDeviceToHost));
+  DMB_CUDA(cudaMemcpyAsync(w, c->d_net.p, sizeof(float) * P_TOTAL, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
 }
 
 }  // namespace dmb

@@ -225,6 +225,9 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 // tiles fastest, so the CTAs that share an A row tile run together and read it
 // from DRAM once.
 // ---------------------------------------------------------------------------
+// ROLE only names the launch site for profilers: 0 = Z X of the Krylov
+// operator, 1 = triangular-solve GEMMs.
+template <int ROLE>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
                                                     int nchunks, int64_t M, int64_t Rv, double2 *__restrict__ Y,
@@ -458,7 +461,8 @@ void ensure_gemm(dmb_ctx *c, TcState &st) {
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.gemm_attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     st.gemm_attr = true;
   }
 }
@@ -537,7 +541,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0,
+  DMB_LAUNCH(c, k_tc_gemm<0>, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -579,7 +583,7 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
              N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
+  DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
              X + r_lo, N, 1, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
@@ -640,7 +644,7 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
              st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm, grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0, (int)(6 * Kpad / TC_BK), M,
+  DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0, (int)(6 * Kpad / TC_BK), M,
              R, Y, N, mode, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)w * (double)R);
 }
