@@ -2,9 +2,13 @@
 //
 // Each entry point validates its arguments with the reference's fail-closed
 // rules, takes the context mutex, runs the device path and maps exceptions to
-// status codes.  Host buffers are copied through pinned staging.
+// status codes.  Host buffers are copied on the context's stream.
 #include <cmath>
 #include <cstring>
+
+#include <algorithm>
+#include <atomic>
+#include <thread>
 
 #include "dmb_device.cuh"
 #include "dmb_internal.h"
@@ -104,12 +108,25 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->pc_valid = false;
       return;
     }
+    if (option == DMB_OPT_FAR_TILE) {
+      DMB_REQUIRE(value == 0 || value == 8 || value == 16 || value == 32, DMB_ERR_ARGUMENT,
+                  "far tile rows must be 0 (autotune), 8, 16 or 32");
+      c->far_tile = value;
+      return;
+    }
     if (option == DMB_OPT_TC_MIN_RHS) {
       DMB_REQUIRE(value >= 1, DMB_ERR_ARGUMENT, "minimum right-hand-side count must be >= 1");
       c->tc_min_rhs = value;
       return;
     }
     throw DmbError{DMB_ERR_ARGUMENT, "unknown option " + std::to_string(option)};
+  });
+}
+
+dmb_status dmb_get_far_tile(dmb_ctx *c, int *rows_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(rows_out, DMB_ERR_ARGUMENT, "output is NULL");
+    *rows_out = c->far_tile_used;
   });
 }
 
@@ -420,9 +437,13 @@ void check_solve_params(const dmb_solve_params *p) {
   DMB_REQUIRE(p->maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
 }
 
-// assemble + preconditioner of the resident solves
-void resident_setup(dmb_ctx *c, const dmb_solve_params *p) {
+// assemble (+ surface impedance) + preconditioner of the resident solves
+void resident_setup(dmb_ctx *c, const dmb_solve_params *p, const double *zs = nullptr) {
   dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
+  if (zs) {
+    check_finite(zs, 2 * c->nt, "surface impedance");
+    dmb::apply_impedance(c, zs);
+  }
   if (p->precond_kind == DMB_PRECOND_NF_LU || p->precond_kind == DMB_PRECOND_NF_DIAG) {
     DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
                 "near-field cutoff must be nonnegative and not NaN");
@@ -561,6 +582,150 @@ dmb_status dmb_farfield(dmb_ctx *c, const double *rhat, int64_t NO, double k, do
     DMB_CUDA(cudaMemcpyAsync(E_out, be.p, eb, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
   });
+}
+
+// ---- batches of independent surfaces -----------------------------------
+struct dmb_batch {
+  int device = 0;
+  std::vector<dmb_ctx *> lanes;
+  std::string err;
+};
+
+dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out) {
+  if (!out || lanes < 1 || lanes > 64) return DMB_ERR_ARGUMENT;
+  *out = nullptr;
+  auto *b = new dmb_batch();
+  b->device = device;
+  for (int i = 0; i < lanes; i++) {
+    dmb_ctx *c = nullptr;
+    dmb_status st = dmb_ctx_create(device, &c);
+    if (st != DMB_OK) {
+      for (dmb_ctx *l : b->lanes) dmb_ctx_destroy(l);
+      delete b;
+      return st;
+    }
+    b->lanes.push_back(c);
+  }
+  *out = b;
+  return DMB_OK;
+}
+
+dmb_status dmb_batch_destroy(dmb_batch *b) {
+  if (!b) return DMB_OK;
+  for (dmb_ctx *c : b->lanes) dmb_ctx_destroy(c);
+  delete b;
+  return DMB_OK;
+}
+
+const char *dmb_batch_last_error(const dmb_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+namespace {
+// one surface on one lane: upload, assemble (+ impedance), preconditioner,
+// RHS, GMRES, monostatic sigma; device times from events on the lane stream
+dmb_status batch_item(dmb_ctx *c, const dmb_solve_params *p, dmb_batch_item &it, cudaEvent_t ev_start) {
+  dmb_status st = dmb_mesh_upload(c, it.xyz, it.tri, it.nv, it.nt);
+  if (st == DMB_OK)
+    st = dmb_rwg_upload(c, it.n, it.tplus, it.tminus, it.evert, it.vplus_opp, it.vminus_opp, it.len,
+                        it.area_plus, it.area_minus);
+  if (st != DMB_OK) return st;
+  return guarded(c, [&] {
+    check_finite(it.kvec, 3, "plane-wave k_vec");
+    check_finite(it.pol, 3, "plane-wave polarization");
+    DMB_REQUIRE(std::isfinite(it.E0) && it.E0 != 0.0, DMB_ERR_ARGUMENT, "plane-wave E0 must be finite, nonzero");
+    cudaEvent_t e0, e1;
+    DMB_CUDA(cudaEventCreate(&e0));
+    DMB_CUDA(cudaEventCreate(&e1));
+    DMB_CUDA(cudaEventRecord(e0, c->stream));
+    resident_setup(c, p, it.zs);
+    const size_t bytes = sizeof(double2) * c->n;
+    c->d_rhs.ensure(bytes);
+    c->d_sol.ensure(bytes);
+    c->sol_r = 0;
+    dmb::rhs_plane_waves_dev(c, it.kvec, &it.E0, it.pol, 1, p->quad_order, c->d_rhs.as<double>());
+    dmb_gmres_stats gs{};
+    dmb::gmres_dev(c, c->d_rhs.as<double>(), c->d_sol.as<double>(), 1, p->tol, p->maxiter, p->precond_kind,
+                   p->precond_side, &gs);
+    c->sol_r = 1;
+    c->d_mono.ensure(sizeof(double2) * 3 + sizeof(double));
+    double *E = c->d_mono.as<double>();
+    dmb::monostatic_dev(c, 1, p->k, p->eta0, p->quad_order, c->d_sol.as<double>(), E, E + 6);
+    DMB_CUDA(cudaMemcpyAsync(&it.sigma, E + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (it.I_out)
+      DMB_CUDA(cudaMemcpyAsync(it.I_out, c->d_sol.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaEventRecord(e1, c->stream));
+    DMB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    DMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    it.solve_ms = ms;
+    DMB_CUDA(cudaEventElapsedTime(&ms, ev_start, e1));
+    it.latency_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    it.stats = gs;
+    resident_check(gs);
+  });
+}
+}  // namespace
+
+dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_item *items, int64_t count,
+                           double *device_ms_out) {
+  if (!b) return DMB_ERR_ARGUMENT;
+  b->err.clear();
+  auto fail = [&](dmb_status s, const std::string &m) {
+    b->err = m;
+    return s;
+  };
+  if (!p || !items || count < 1) return fail(DMB_ERR_ARGUMENT, "batch needs parameters and >= 1 surface");
+  if (!(std::isfinite(p->tol) && p->tol > 0) || p->maxiter < 1)
+    return fail(DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive and maxiter >= 1");
+  if (cudaSetDevice(b->device) != cudaSuccess) return fail(DMB_ERR_CUDA, "cudaSetDevice failed");
+  std::vector<int64_t> order(count);
+  for (int64_t i = 0; i < count; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t c2) { return items[a].n > items[c2].n; });
+  const int L = (int)b->lanes.size();
+  cudaEvent_t ev_start;
+  std::vector<cudaEvent_t> ev_end(L);
+  if (cudaEventCreate(&ev_start) != cudaSuccess) return fail(DMB_ERR_CUDA, "cudaEventCreate failed");
+  for (auto &e : ev_end) cudaEventCreate(&e);
+  cudaEventRecord(ev_start, b->lanes[0]->stream);
+  std::atomic<int64_t> next{0};
+  std::atomic<int> failed{0};
+  std::mutex emu;
+  dmb_status first_code = DMB_OK;
+  std::vector<std::thread> workers;
+  for (int l = 0; l < L; l++) {
+    workers.emplace_back([&, l] {
+      cudaSetDevice(b->device);
+      dmb_ctx *c = b->lanes[l];
+      cudaStreamWaitEvent(c->stream, ev_start, 0);
+      while (!failed.load()) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= count) break;
+        dmb_batch_item &it = items[order[i]];
+        const dmb_status st = batch_item(c, p, it, ev_start);  // each call takes the lane's mutex
+        if (st != DMB_OK) {
+          std::lock_guard<std::mutex> lk(emu);
+          if (first_code == DMB_OK) {
+            first_code = st;
+            b->err = "surface " + std::to_string(order[i]) + ": " + c->err;
+          }
+          failed.store(1);
+        }
+      }
+      cudaEventRecord(ev_end[l], c->stream);
+    });
+  }
+  for (auto &w : workers) w.join();
+  double total = 0;
+  for (int l = 0; l < L; l++) {
+    cudaEventSynchronize(ev_end[l]);
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev_start, ev_end[l]) == cudaSuccess) total = std::max(total, (double)ms);
+  }
+  cudaEventDestroy(ev_start);
+  for (auto &e : ev_end) cudaEventDestroy(e);
+  if (device_ms_out) *device_ms_out = total;
+  return first_code;
 }
 
 }  // extern "C"

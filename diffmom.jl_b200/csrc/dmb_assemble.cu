@@ -224,31 +224,20 @@ __device__ __forceinline__ bool tri_adjacent(const int *__restrict__ off, const 
 //   block(i,j) = s_i s_j [Mab - Ma.pj' - Mb.pi' + (pi'.pj') M0] - dv_i dv_j M0 / k^2
 // FP64 flavour: R from the global quadrature points as the reference does.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tile_coords(int64_t tile, int T, int &bi, int &bj) {
-  // tile enumerates (bi <= bj) row by row: row bi holds T - bi tiles
-  int64_t r = tile;
-  int i = 0;
-  // closed-form start, then fix up
-  double Tt = (double)T;
-  double disc = (2 * Tt + 1) * (2 * Tt + 1) - 8.0 * (double)tile;
-  i = (int)floor(((2 * Tt + 1) - sqrt(fmax(disc, 0.0))) / 2);
-  if (i < 0) i = 0;
-  auto start = [&](int ii) { return (int64_t)ii * T - (int64_t)ii * (ii - 1) / 2; };
-  while (i > 0 && start(i) > r) i--;
-  while (i + 1 < T && start(i + 1) <= r) i++;
-  bi = i;
-  bj = i + (int)(r - start(i));
-}
-
-template <int NQ>
-__global__ void __launch_bounds__(256) k_far_f64(int nt, int T, const TriCache *__restrict__ tc,
+// Tiles of TY test triangles x TX = 256 / TY source triangles, one thread per
+// pair; the grid covers the whole nt x nt square and tiles entirely below the
+// diagonal return at once (only ta <= tb pairs are computed).  The tile shape
+// is picked per mesh-size bucket by the autotuner in assemble().
+template <int NQ, int TY>
+__global__ void __launch_bounds__(256) k_far_f64(int nt, const TriCache *__restrict__ tc,
                                                  const int *__restrict__ aoff, const int *__restrict__ anb,
                                                  double k, double inv_k2, double2 *__restrict__ S,
                                                  int64_t ldS) {
-  int bi, bj;
-  tile_coords(blockIdx.x, T, bi, bj);
-  int ta = bi * 16 + threadIdx.y;
-  int tb = bj * 16 + threadIdx.x;
+  constexpr int TX = 256 / TY;
+  const int rb = blockIdx.y * TY, cb = blockIdx.x * TX;
+  if (rb > cb + TX - 1) return;  // uniform: tile below the diagonal
+  int ta = rb + (int)threadIdx.x / TX;
+  int tb = cb + (int)threadIdx.x % TX;
   if (ta >= nt || tb >= nt || ta > tb) return;
   const TriCache &A = tc[ta];
   const TriCache &B = tc[tb];
@@ -320,15 +309,16 @@ __global__ void __launch_bounds__(256) k_far_f64(int nt, int T, const TriCache *
 
 // FP32 flavour: R from centroid difference (rounded from FP64) plus local
 // offsets, all quadrature arithmetic in FP32.
-template <int NQ>
-__global__ void __launch_bounds__(256) k_far_f32(int nt, int T, const TriCache *__restrict__ tc,
+template <int NQ, int TY>
+__global__ void __launch_bounds__(256) k_far_f32(int nt, const TriCache *__restrict__ tc,
                                                  const int *__restrict__ aoff, const int *__restrict__ anb,
                                                  float k, float inv_k2, float2 *__restrict__ S,
                                                  int64_t ldS) {
-  int bi, bj;
-  tile_coords(blockIdx.x, T, bi, bj);
-  int ta = bi * 16 + threadIdx.y;
-  int tb = bj * 16 + threadIdx.x;
+  constexpr int TX = 256 / TY;
+  const int rb = blockIdx.y * TY, cb = blockIdx.x * TX;
+  if (rb > cb + TX - 1) return;  // uniform: tile below the diagonal
+  int ta = rb + (int)threadIdx.x / TX;
+  int tb = cb + (int)threadIdx.x % TX;
   if (ta >= nt || tb >= nt || ta > tb) return;
   const TriCache &A = tc[ta];
   const TriCache &B = tc[tb];
@@ -816,6 +806,50 @@ void near_values(dmb_ctx *c, double k, double inv_k2) {
              c->d_near_val.as<double2>());
 }
 
+// Far-pair tile autotuner: per (device, mesh-size bucket, precision,
+// quadrature size) the three tile shapes (8 x 32, 16 x 16, 32 x 8 triangle
+// pairs per CTA) are each timed once with CUDA events on the context stream
+// (after one untimed launch that loads the kernel) and the fastest is kept for
+// the process.  DMB_OPT_FAR_TILE pins a shape instead.  Every shape computes
+// the same pair blocks bit for bit; the caller's final launch writes S.
+template <class Launch>
+int far_tile_rows(dmb_ctx *c, int64_t nt, bool f64, Launch &&launch) {
+  if (c->far_tile > 0) return c->far_tile_used = c->far_tile;
+  int bucket = 0;
+  while ((int64_t)1 << (bucket + 1) <= nt) bucket++;
+  const int64_t key = ((int64_t)c->device << 24) | ((int64_t)bucket << 8) | ((f64 ? 1 : 0) << 4) | c->nq;
+  static std::mutex mu;
+  static std::vector<std::pair<int64_t, int>> table;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto &e : table)
+      if (e.first == key) return c->far_tile_used = e.second;
+  }
+  cudaEvent_t e0, e1;
+  DMB_CUDA(cudaEventCreate(&e0));
+  DMB_CUDA(cudaEventCreate(&e1));
+  int best = 16;
+  float best_ms = 0;
+  for (int ty : {8, 16, 32}) {
+    launch(ty);
+    DMB_CUDA(cudaEventRecord(e0, c->stream));
+    launch(ty);
+    DMB_CUDA(cudaEventRecord(e1, c->stream));
+    DMB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    DMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (best_ms == 0 || ms < best_ms) {
+      best_ms = ms;
+      best = ty;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lk(mu);
+  table.push_back({key, best});
+  return c->far_tile_used = best;
+}
+
 void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) {
   DMB_REQUIRE(std::isfinite(k) && k != 0.0, DMB_ERR_ARGUMENT,
               "EFIE wavenumber must be finite and nonzero, got " + std::to_string(k));
@@ -838,29 +872,31 @@ void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) 
   size_t esz = f64 ? sizeof(double2) : sizeof(float2);
   c->d_S.ensure((size_t)ldS * ldS * esz);
   c->d_Z.ensure((size_t)N * N * esz);
-  int T = (int)((nt + 15) / 16);
-  int64_t ntiles = (int64_t)T * (T + 1) / 2;
-  dim3 blk(16, 16);
   const TriCache *tc = c->d_tcache.as<TriCache>();
   const int *aoff = c->d_adj_off.as<int>(), *anb = c->d_adj_nb.as<int>();
-#define FAR_CASE(NQV)                                                                              \
-  case NQV:                                                                                        \
+  DMB_REQUIRE(c->nq == 1 || c->nq == 3 || c->nq == 4 || c->nq == 7, DMB_ERR_ARGUMENT,
+              "unsupported quadrature size");
+  auto far = [&](int ty) {
+    const int tx = 256 / ty;
+    dim3 g((unsigned)((nt + tx - 1) / tx), (unsigned)((nt + ty - 1) / ty));
+#define FAR_CASE(NQV, TYV)                                                                          \
+  if (c->nq == NQV && ty == TYV) {                                                                 \
     if (f64)                                                                                       \
-      DMB_LAUNCH(c, k_far_f64<NQV>, (unsigned)ntiles, blk, 0, (int)nt, T, tc, aoff, anb, k, inv_k2,  \
+      DMB_LAUNCH(c, (k_far_f64<NQV, TYV>), g, 256, 0, (int)nt, tc, aoff, anb, k, inv_k2,          \
                  c->d_S.as<double2>(), ldS);                                                       \
     else                                                                                           \
-      DMB_LAUNCH(c, k_far_f32<NQV>, (unsigned)ntiles, blk, 0, (int)nt, T, tc, aoff, anb, (float)k,   \
+      DMB_LAUNCH(c, (k_far_f32<NQV, TYV>), g, 256, 0, (int)nt, tc, aoff, anb, (float)k,            \
                  (float)inv_k2, c->d_S.as<float2>(), ldS);                                         \
-    break;
-  switch (c->nq) {
-    FAR_CASE(1)
-    FAR_CASE(3)
-    FAR_CASE(4)
-    FAR_CASE(7)
-    default:
-      throw DmbError{DMB_ERR_ARGUMENT, "unsupported quadrature size"};
   }
+#define FAR_SHAPES(NQV) FAR_CASE(NQV, 8) FAR_CASE(NQV, 16) FAR_CASE(NQV, 32)
+    FAR_SHAPES(1)
+    FAR_SHAPES(3)
+    FAR_SHAPES(4)
+    FAR_SHAPES(7)
+#undef FAR_SHAPES
 #undef FAR_CASE
+  };
+  far(far_tile_rows(c, nt, f64, far));
   dim3 g((unsigned)((N + 255) / 256), (unsigned)N);
   if (f64)
     DMB_LAUNCH(c, (k_gather<double2, double2>), g, 256, 0, N, c->d_rwg_slot.as<int>(),

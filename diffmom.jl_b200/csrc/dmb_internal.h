@@ -156,6 +156,8 @@ struct dmb_ctx {
   DevBuf d_small;
   bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
+  int far_tile = 0;              // far-pair tile rows (8/16/32), 0 = autotuned
+  int far_tile_used = 0;         // shape of the last assembly
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves

@@ -11,7 +11,8 @@ from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixF
                   PlaneWaveExcitation, make_plane_wave, assemble_plane_wave, assemble_excitation,
                   assemble_multiple_excitations, build_nearfield_preconditioner, NearFieldOperator,
                   solve_gmres, solve_forward, solve_scattering, ScatteringResult, SphGrid,
-                  monostatic_rcs_sweep, MonostaticResult,
+                  monostatic_rcs_sweep, MonostaticResult, BatchSurface, BatchResult,
+                  SurfaceBatch, solve_surfaces,
                   make_sph_grid, phi_cut_grid, compute_farfield, bistatic_rcs, backscatter_rcs,
                   C0_DEFAULT, ETA0_DEFAULT)
 from ._native import load_library, LIB_PATH, DiffMoMError, NotConvergedError, FactorizationBreakdown

@@ -42,6 +42,7 @@ SIDE_RIGHT = 1
 
 OPT_TENSOR_CORES = 1
 OPT_TC_MIN_RHS = 2
+OPT_FAR_TILE = 3
 
 
 class DiffMoMError(RuntimeError):
@@ -94,6 +95,17 @@ class SolveParams(ctypes.Structure):
                 ("kvec", ctypes.c_double * 3), ("pol", ctypes.c_double * 3), ("E0", ctypes.c_double)]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("xyz", ctypes.c_void_p), ("tri", ctypes.c_void_p), ("nv", ctypes.c_int64),
+                ("nt", ctypes.c_int64), ("n", ctypes.c_int64), ("tplus", ctypes.c_void_p),
+                ("tminus", ctypes.c_void_p), ("evert", ctypes.c_void_p), ("vplus_opp", ctypes.c_void_p),
+                ("vminus_opp", ctypes.c_void_p), ("len", ctypes.c_void_p), ("area_plus", ctypes.c_void_p),
+                ("area_minus", ctypes.c_void_p), ("zs", ctypes.c_void_p), ("kvec", ctypes.c_double * 3),
+                ("pol", ctypes.c_double * 3), ("E0", ctypes.c_double), ("I_out", ctypes.c_void_p),
+                ("sigma", ctypes.c_double), ("stats", GmresStats), ("latency_ms", ctypes.c_double),
+                ("solve_ms", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _D = ctypes.c_double
 _I = ctypes.c_int
@@ -110,6 +122,11 @@ SIGNATURES = {
     "dmb_last_error": ([_P], ctypes.c_char_p),
     "dmb_get_timings": ([_P, ctypes.POINTER(Timings)], _I),
     "dmb_set_option": ([_P, _I, _I], _I),
+    "dmb_get_far_tile": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
+    "dmb_batch_create": ([_I, _I, ctypes.POINTER(_P)], _I),
+    "dmb_batch_destroy": ([_P], _I),
+    "dmb_batch_last_error": ([_P], ctypes.c_char_p),
+    "dmb_batch_solve": ([_P, ctypes.POINTER(SolveParams), ctypes.POINTER(BatchItem), _L, _DP], _I),
     "dmb_mesh_upload": ([_P, _DP, _LP, _L, _L], _I),
     "dmb_rwg_upload": ([_P, _L, _LP, _LP, _LP, _LP, _LP, _DP, _DP, _DP], _I),
     "dmb_assemble_z": ([_P, _D, _D, _I, _I, _DP], _I),

@@ -84,13 +84,21 @@ class EFIEDevice:
     def set_option(self, name: str, value: int) -> None:
         """Implementation switches: "tensor_cores" (0/1) for the complex64
         factorisation update, "tc_min_rhs" (>= 1) for the right-hand-side count
-        from which Z X and the batched near-field solves use the tensor cores."""
-        codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS}
+        from which Z X and the batched near-field solves use the tensor cores,
+        "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles."""
+        codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
+                 "far_tile": nat.OPT_FAR_TILE}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))
         if name == "tensor_cores":
             self.preconditioner = None
+
+    def far_tile(self) -> int:
+        """Far-pair tile rows the last assembly used (autotuned unless pinned)."""
+        v = ctypes.c_int()
+        self.ctx.call("dmb_get_far_tile", ctypes.byref(v))
+        return v.value
 
     # -- impedance matrix -----------------------------------------------
     def assemble(self, k: float, quad_order: int = 3, eta0: float = ETA0_DEFAULT,
@@ -589,6 +597,129 @@ def monostatic_rcs_sweep(mesh: TriMesh, freq_hz, excitations, precision: str = "
     finally:
         if own:
             dev.close()
+
+
+@dataclass
+class BatchSurface:
+    mesh: TriMesh
+    rwg: RWGData
+    excitation: "PlaneWaveExcitation"
+    zs: np.ndarray | None = None   # per-triangle complex surface impedance (ohm), None = PEC
+
+
+@dataclass
+class BatchResult:
+    sigma: np.ndarray          # monostatic RCS per surface, m^2
+    gmres_iters: np.ndarray
+    true_residual: np.ndarray
+    latency_ms: np.ndarray     # device time from the batch start to each surface's end
+    solve_ms: np.ndarray       # device time of each surface's own solve
+    device_ms: float           # device time of the whole batch
+    N: np.ndarray
+    currents: list | None
+
+
+class SurfaceBatch:
+    """Many independent surfaces (each its own mesh, basis, impedance and
+    plane wave) solved by `lanes` concurrent device contexts, largest first."""
+
+    def __init__(self, lanes: int = 8, device: int = 0):
+        self.lib = nat.load_library()
+        h = ctypes.c_void_p()
+        st = self.lib.dmb_batch_create(int(device), int(lanes), ctypes.byref(h))
+        if st != nat.DMB_OK:
+            raise nat.DiffMoMError(f"dmb_batch_create failed ({st})")
+        self.h = h
+        self.lanes = lanes
+
+    def close(self):
+        if self.h:
+            self.lib.dmb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, surfaces, k: float, precision: str = "mixed", preconditioner: str = "lu",
+              cutoff: float = math.inf, tol: float = 1e-6, maxiter: int = 300, precond_side: str = "left",
+              quad_order: int = 3, eta0: float = ETA0_DEFAULT, return_currents: bool = False) -> BatchResult:
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        if preconditioner not in EFIEDevice._PC_CODES:
+            raise ValueError(f"unknown preconditioner {preconditioner!r}")
+        side = {"left": nat.SIDE_LEFT, "right": nat.SIDE_RIGHT}.get(precond_side)
+        if side is None:
+            raise ValueError(f"Invalid precond_side: {precond_side} (expected :left or :right)")
+        surfaces = list(surfaces)
+        if not surfaces:
+            raise ValueError("solve: need at least one surface")
+        items = (nat.BatchItem * len(surfaces))()
+        keep, outs = [], []
+        for it, sf in zip(items, surfaces):
+            m, r = sf.mesh, sf.rwg
+            if r.mesh is not m:
+                raise ValueError("RWG data was built for a different mesh")
+            arrs = [np.ascontiguousarray(m.xyz, dtype=np.float64), np.ascontiguousarray(m.tri, dtype=np.int64)]
+            arrs += [np.ascontiguousarray(a, dtype=np.int64)
+                     for a in (r.tplus, r.tminus, r.evert, r.vplus_opp, r.vminus_opp)]
+            arrs += [np.ascontiguousarray(a, dtype=np.float64) for a in (r.len, r.area_plus, r.area_minus)]
+            zs = None
+            if sf.zs is not None:
+                zs = np.ascontiguousarray(np.broadcast_to(np.asarray(sf.zs, dtype=np.complex128),
+                                                          (m.ntriangles,)))
+            I = np.empty(r.nedges, dtype=np.complex128) if return_currents else None
+            keep.append((arrs, zs, I))
+            outs.append(I)
+            it.xyz, it.tri = arrs[0].ctypes.data, arrs[1].ctypes.data
+            it.nv, it.nt, it.n = m.nvertices, m.ntriangles, r.nedges
+            it.tplus, it.tminus, it.evert, it.vplus_opp, it.vminus_opp = (a.ctypes.data for a in arrs[2:7])
+            it.len, it.area_plus, it.area_minus = (a.ctypes.data for a in arrs[7:10])
+            it.zs = zs.ctypes.data if zs is not None else None
+            e = sf.excitation
+            it.kvec[:] = [float(v) for v in e.k_vec]
+            it.pol[:] = [float(v) for v in e.pol]
+            it.E0 = float(e.E0)
+            it.I_out = I.ctypes.data if I is not None else None
+        p = nat.SolveParams()
+        p.k, p.eta0, p.cutoff, p.tol = float(k), float(eta0), float(cutoff), float(tol)
+        p.quad_order, p.precision = int(quad_order), _PRECISIONS[precision]
+        p.precond_kind, p.precond_side, p.maxiter = EFIEDevice._PC_CODES[preconditioner], side, int(maxiter)
+        dms = ctypes.c_double()
+        st = self.lib.dmb_batch_solve(self.h, ctypes.byref(p), items, len(surfaces), ctypes.byref(dms))
+        if st != nat.DMB_OK:
+            msg = (self.lib.dmb_batch_last_error(self.h) or b"").decode()
+            raise nat._EXC.get(st, nat.DiffMoMError)(msg)
+        return BatchResult(sigma=np.array([it.sigma for it in items]),
+                           gmres_iters=np.array([it.stats.niter for it in items]),
+                           true_residual=np.array([it.stats.true_residual for it in items]),
+                           latency_ms=np.array([it.latency_ms for it in items]),
+                           solve_ms=np.array([it.solve_ms for it in items]),
+                           device_ms=dms.value, N=np.array([it.n for it in items]),
+                           currents=outs if return_currents else None)
+
+
+def solve_surfaces(surfaces, freq_hz, lanes: int = 8, precision: str = "mixed", preconditioner: str = "lu",
+                   nf_cutoff_lambda: float = math.inf, gmres_tol: float = 1e-6, gmres_maxiter: int = 300,
+                   precond_side: str = "left", quad_order: int = 3, c0: float = C0_DEFAULT,
+                   return_currents: bool = False, batch: SurfaceBatch | None = None) -> BatchResult:
+    """solve_scattering (Workflow.jl:67-317) + backscatter_rcs for many
+    independent surfaces (BatchSurface: mesh, rwg, plane wave, optional
+    per-triangle impedance) in one call; see SurfaceBatch."""
+    f = float(freq_hz)
+    if not (math.isfinite(f) and f > 0):
+        raise ValueError(f"solve_surfaces: freq_hz must be finite and positive, got {freq_hz}")
+    k = _frequency_to_wavenumber(f, c0)
+    b = batch or SurfaceBatch(lanes)
+    try:
+        return b.solve(surfaces, k, precision=precision, preconditioner=preconditioner,
+                       cutoff=nf_cutoff_lambda * (c0 / f), tol=gmres_tol, maxiter=gmres_maxiter,
+                       precond_side=precond_side, quad_order=quad_order, return_currents=return_currents)
+    finally:
+        if batch is None:
+            b.close()
 
 
 # ---------------------------------------------------------------------------

@@ -95,7 +95,13 @@ const char *dmb_version(void);
  * then confirms convergence on the FP64 residual and refines where needed. */
 #define DMB_OPT_TENSOR_CORES 1
 #define DMB_OPT_TC_MIN_RHS 2
+/* DMB_OPT_FAR_TILE: far triangle-pair tile shape of the assembly, as test
+ * rows per 256-pair CTA (8, 16 or 32); 0 (default) lets the autotuner pick it
+ * per mesh-size bucket (timed once per process). */
+#define DMB_OPT_FAR_TILE 3
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
+/* The far-pair tile rows used by the last assembly on this context. */
+dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
 
 /* ---- mesh and basis ---------------------------------------------------- */
 /* TriMesh (src/Types.jl:123-126): xyz 3 x Nv column-major, tri 3 x Nt
@@ -237,6 +243,40 @@ dmb_status dmb_solve_resident_many(dmb_ctx *ctx, const dmb_solve_params *p, int6
 /* Copy the resident currents (N x 1, or N x R after dmb_solve_resident_many,
  * column-major complex128). */
 dmb_status dmb_copy_solution(dmb_ctx *ctx, double *I_out);
+
+/* ---- many independent surfaces ------------------------------------------ */
+/* No single reference call: the loop of solve_scattering (src/Workflow.jl:
+ * 67-317) over independent bodies, each with its own mesh and RWG basis, an
+ * optional per-triangle surface impedance (assemble_full_Z with
+ * precompute_patch_mass, Impedance.jl:304-408) and its own plane wave, plus
+ * backscatter_rcs (Diagnostics.jl:460-517).  A batch owns `lanes` contexts,
+ * each with its own stream and host thread; surfaces are taken largest-first
+ * and the GPU runs the lanes' kernels concurrently.  The solve of each surface
+ * follows dmb_solve_resident with `p` (kvec/pol/E0 of p are ignored). */
+typedef struct dmb_batch dmb_batch;
+typedef struct {
+  /* inputs: host arrays in the layouts of dmb_mesh_upload / dmb_rwg_upload */
+  const double *xyz;
+  const int64_t *tri;
+  int64_t nv, nt;
+  int64_t n;
+  const int64_t *tplus, *tminus, *evert, *vplus_opp, *vminus_opp;
+  const double *len, *area_plus, *area_minus;
+  const double *zs;       /* nt complex surface impedances (re, im interleaved), or NULL for PEC */
+  double kvec[3], pol[3], E0;
+  /* outputs */
+  double *I_out;          /* n complex currents, or NULL */
+  double sigma;           /* monostatic RCS at -k_hat */
+  dmb_gmres_stats stats;
+  double latency_ms;      /* device time from the batch start to the end of this surface */
+  double solve_ms;        /* device time of this surface's solve */
+} dmb_batch_item;
+dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out);
+dmb_status dmb_batch_destroy(dmb_batch *b);
+const char *dmb_batch_last_error(const dmb_batch *b);
+/* device_ms_out (may be NULL): device time of the whole batch. */
+dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_item *items, int64_t count,
+                           double *device_ms_out);
 
 /* ---- measurement hooks -------------------------------------------------- */
 /* No reference counterpart.  The CUDA stream the context launches on (a

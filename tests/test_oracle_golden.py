@@ -200,3 +200,15 @@ def test_areas_match_oracle():
         v = m.xyz[m.tri[t] - 1]
         ref = orc.lib().orc_triangle_area(*[orc._d(np.ascontiguousarray(v[i])) for i in range(3)])
         assert a[t] == ref
+
+
+def test_golden_fixtures_reproduce():
+    # the committed fixtures (tests/golden/make_golden.py) still match the oracle
+    from pathlib import Path
+    g = np.load(Path(__file__).parent / "golden" / "c1_plate.npz")
+    m = make_rect_plate(0.1, 0.1, 6, 6)
+    oc = orc.OracleCache(m, build_rwg(m), 3)
+    Z = oc.assemble_z(float(g["k"]))
+    assert np.array_equal(Z, g["Z"])
+    assert np.linalg.norm(g["Z"] @ g["I"] - g["v"]) <= 1e-10 * np.linalg.norm(g["v"])
+    assert np.all(g["sigma_cut"] > 0) and np.all(g["sigma_mono"] > 0)
