@@ -18,6 +18,10 @@ Variants reported beside it (same timing rules, fewer steps where slow):
                   near-field LDL^T at 1 lambda, FP64 block GMRES)
   c2_*            PEC sphere r = 0.5 lambda, 7,680 RWG, one incidence,
                   FP64 / mixed with the 1-lambda near-field preconditioner
+  c4_*            64 impedance-loaded rectangular / circular plates, 0.5-3
+                  lambda, 500-6,000 RWG, one incidence each (seed 20260004):
+                  mixed on 8 lanes vs plain FP64 one surface at a time;
+                  per size-bucket solve times
   c5_*            perturbed ellipsoid (seed 99), 9,720 RWG, one incidence:
                   FP64 near-field vs mixed + learned right preconditioner
                   (network trained beforehand, untimed, on 3 other bodies)
@@ -282,6 +286,38 @@ def run_ours(args):
                "api": "diffmom_b200.monostatic_rcs_sweep(precision=mixed) incl. mesh/RWG upload"}
     dev.close()
 
+    # ---- C4 uneven batch of 64 impedance-loaded surfaces -------------------
+    if not args.quick and any(want(n) for n in ("c4_batch64_mixed", "c4_batch64_fp64_1lane")):
+        from diffmom_b200 import SurfaceBatch
+        from diffmom_b200.workloads import impedance_surface_batch
+        surf = impedance_surface_batch(64)
+        for name, prec, lanes in (("c4_batch64_mixed", "mixed", 8), ("c4_batch64_fp64_1lane", "fp64", 1)):
+            if not want(name):
+                continue
+            batch = SurfaceBatch(lanes, device=local)
+            reps = min(args.steps, 3) if prec == "mixed" else 1
+            for _ in range(1 if prec == "fp64" else args.warmup):
+                batch.solve(surf, K, precision=prec)
+            run.barrier()
+            dms, last = [], None
+            for _ in range(reps):
+                last = batch.solve(surf, K, precision=prec)
+                dms.append(last.device_ms)
+            batch.close()
+            ms = run.max_over_ranks(float(np.mean(dms)))
+            buckets = {}
+            for lo, hi in ((500, 1500), (1500, 3000), (3000, 4500), (4500, 6500)):
+                sel = (last.N >= lo) & (last.N < hi)
+                if sel.any():
+                    buckets[f"N{lo}-{hi}"] = {"surfaces": int(sel.sum()),
+                                             "solve_ms_mean": float(last.solve_ms[sel].mean()),
+                                             "latency_ms_max": float(last.latency_ms[sel].max()),
+                                             "surfaces_per_s_alone": float(1e3 / last.solve_ms[sel].mean())}
+            variants[name] = {"ms_per_step": ms, "solves_per_s": ws * 64 / (ms / 1e3), "steps": reps,
+                              "warmup": 1 if prec == "fp64" else args.warmup, "launches": None, "lanes": lanes,
+                              "last": (int(last.gmres_iters.max()), float(last.true_residual.max())),
+                              "buckets": buckets, "sum_N2": float(np.sum(last.N.astype(float) ** 2))}
+
     # ---- C2 sphere, one incidence -----------------------------------------
     if not args.quick and (want("c2_fp64_nf_lu") or want("c2_mixed_nf_lu")):
         sph = make_icosphere(0.5 * LAM, 4)
@@ -353,7 +389,8 @@ def clean(v):
         out["true_residual"] = float(last[1])
         if len(last) > 2:
             out["refinement_cycles"] = int(last[2])
-    out["kernels_per_step"] = v["launches"] / v["steps"]
+    if v.get("launches") is not None:
+        out["kernels_per_step"] = v["launches"] / v["steps"]
     return out
 
 
@@ -363,7 +400,8 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
     speed = {}
     if head is not None and base is not None:
         speed["c3_mixed_batched_vs_c3_fp64_plain"] = head["solves_per_s"] / base["solves_per_s"]
-    for a, b in (("c2_mixed_nf_lu", "c2_fp64_nf_lu"), ("c5_mixed_learned", "c5_fp64_nf_lu"),
+    for a, b in (("c4_batch64_mixed", "c4_batch64_fp64_1lane"),
+                 ("c2_mixed_nf_lu", "c2_fp64_nf_lu"), ("c5_mixed_learned", "c5_fp64_nf_lu"),
                  ("c5_mixed_nf_lu", "c5_fp64_nf_lu"), ("c5_mixed_local", "c5_fp64_nf_lu")):
         if a in variants and b in variants:
             speed[f"{a}_vs_{b}"] = variants[a]["solves_per_s"] / variants[b]["solves_per_s"]
