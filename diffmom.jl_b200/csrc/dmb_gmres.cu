@@ -275,6 +275,13 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   // re-checked against the residual computed in FP64 and, if that is still
   // above its threshold, refined by another cycle from the current x.
   const bool inexact = matvec_op_inexact(c, R);
+  // few systems with a cheap preconditioner (none, Jacobi, sparse local rows):
+  // iterations are short, so host round trips are amortised over several;
+  // otherwise an iteration (many systems, or triangular solves) costs far more
+  // than the round trip and every one is checked
+  const bool cheap = precond_kind != DMB_PRECOND_NF_LU;
+  const int check_every = (R < 32 && cheap) ? 4 : 1;
+  int iters_used = 0;
   DMB_CUDA(cudaMemsetAsync(x, 0, vec_bytes, c->stream));
   int total_iters = 0, restarts = 0;
   bool first = true, have_true = false;
@@ -333,13 +340,18 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, w, V + (int64_t)(j + 1) * vstride);
       DMB_CUDA(cudaMemsetAsync(active, 0, 4, c->stream));
       DMB_LAUNCH(c, k_givens, blocks_for(R, 128), 128, 0, R, j, kcap, H, nrm, cs, sn, g, st, active);
-      unsigned h_active = 0;
-      DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
-      DMB_CUDA(cudaStreamSynchronize(c->stream));
-      if (h_active == 0) {
-        j++;
-        total_iters++;
-        break;
+      // the host looks at the active count every check_every iterations (a
+      // system that converged in between keeps its own k; its extra basis
+      // vectors are never combined)
+      if ((j + 1) % check_every == 0 || j + 1 == kcap || total_iters + 1 >= maxiter) {
+        unsigned h_active = 0;
+        DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
+        DMB_CUDA(cudaStreamSynchronize(c->stream));
+        if (h_active == 0) {
+          j++;
+          total_iters++;
+          break;
+        }
       }
     }
     // solution update from this cycle
@@ -354,6 +366,11 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     }
     DMB_CUDA(cudaMemcpyAsync(hst.data(), st, sizeof(SysState) * R, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
+    {
+      int kmax = 0;
+      for (auto &s : hst) kmax = std::max(kmax, s.k);
+      iters_used += kmax;
+    }
     bool all_done = true;
     for (auto &s : hst)
       if (!s.done) all_done = false;
@@ -390,7 +407,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     }
     if (!std::isfinite(rel)) solved = false;
   }
-  out->niter = total_iters;
+  out->niter = iters_used;
   out->solved = solved ? 1 : 0;
   out->residual = eres;
   out->true_residual = tres;
