@@ -61,6 +61,10 @@ K = 2 * math.pi * FREQ / C0
 R_WAVES = 1024
 SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
+# DRAM bytes per launch of the tensor-core GEMM family (k_tc_syrk + k_tc_gemm)
+# on the headline step, measured with ncu one-pass dram__bytes_read/write.sum
+# over every launch of one step: 104.4 GB in 288 launches
+TC_TRAFFIC_PER_LAUNCH = 104.4e9 / 288
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
@@ -432,7 +436,9 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         line["roofline"] = {
             "kernel": "k_tc_gemm + k_tc_syrk (tcgen05 3xTF32 complex GEMMs: Z X, panel and factor updates)",
             "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-            "frac": achieved / bf16 if bf16 else None, "traffic": None,
+            "frac": achieved / bf16 if bf16 else None,
+            "traffic": TC_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
+            "traffic_note": "DRAM bytes per launch (ncu, one-pass dram__bytes metrics, headline step)",
             "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic complex flops (8 per "
                            f"complex MAC), the 3xTF32 split executes 3x that at half the bf16 rate",
             "launches_timed": kl, "kernel_ms_total": kms,
