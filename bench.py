@@ -92,10 +92,8 @@ def waves(R=None, seed=SEED):
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from diffmom_b200 import replicas
+    return replicas.replica_env()
 
 
 class Clocks:
@@ -158,17 +156,12 @@ class Runner:
         self.local, self.ws = local, ws
 
     def barrier(self):
-        if self.ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        from diffmom_b200 import replicas
+        replicas.barrier()
 
     def max_over_ranks(self, x):
-        if self.ws > 1:
-            import torch.distributed as dist
-            t = self.torch.tensor([x], device=f"cuda:{self.local}", dtype=self.torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        from diffmom_b200 import replicas
+        return replicas.max_over_ranks(x, device=f"cuda:{self.local}")
 
     def timed(self, dev, step, steps, warmup, per_step_units, kernel_timing=False, clocks=False):
         """Device-timed loop on the library's stream: warm-up, barrier + sync,
@@ -228,11 +221,9 @@ def run_ours(args):
     from diffmom_b200 import _native as nat
 
     ws, rank, local = dist_env()
+    from diffmom_b200 import replicas
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    replicas.init("nccl", timeout_s=300)
     run = Runner(local, ws)
     variants = {}
     only = set(args.only.split(",")) if args.only else None
@@ -380,9 +371,7 @@ def run_ours(args):
 
     if rank == 0:
         print(json.dumps(make_line(args, ws, N, mesh, head, variants, e2e)), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 def clean(v):
