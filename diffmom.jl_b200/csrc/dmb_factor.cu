@@ -32,7 +32,8 @@
 #include "dmb_internal.h"
 
 namespace dmb {
-void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W);
+void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t jcol, int K, float2 *F,
+                        const float2 *W, int wstride, int woff);
 }  // namespace dmb
 
 namespace {
@@ -526,20 +527,23 @@ template <class C> void set_smem_attrs() {
   done = true;
 }
 
-// Two-level right-looking LDL^T.  Block columns of NBO = 256 are factored as
-// four 64-wide panels whose updates stay inside the block column (narrow SIMT
-// strips); the rest of the trailing matrix then receives ONE update with
-// K = 256 -- on the tensor cores for complex64 factors.  This keeps the big
-// update compute-dominated and reads/writes the trailing matrix once per 256
-// columns instead of once per 64.
+// Three-level right-looking LDL^T.  Block columns of NBW = 1024 are factored
+// as 256-wide middle panels, each made of four 64-wide panels (diagonal block,
+// panel, SIMT strip updates inside the 256 columns).  After each middle panel
+// the rest of the 1024-wide block column receives one K = 256 update, and after
+// the block column the whole trailing matrix receives one K = 1024 update --
+// both on the tensor cores for complex64 factors.  The big update is long-K
+// (compute-dominated) and the trailing matrix is read and written once per
+// 1024 columns.  W (N x NBW) holds L21 D1 for the current block column.
 constexpr int NBO = 256;
+constexpr int NBW = 1024;
 
 template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   c->f_version++;  // F changes from here on: packed copies are stale
   const int64_t N = c->n;
   set_smem_attrs<C>();
   const int nblk = (int)((N + NB - 1) / NB);
-  c->d_W.ensure(sizeof(C) * N * NBO);
+  c->d_W.ensure(sizeof(C) * N * NBW);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   c->d_flags.ensure(64);
   unsigned *err = c->d_flags.as<unsigned>();
@@ -549,32 +553,42 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const size_t sm_diag = sizeof(C) * (NB * (NB + 1) + NB);
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
-  for (int64_t J = 0; J < N; J += NBO) {
-    const int64_t JB = std::min<int64_t>(NBO, N - J);
-    for (int64_t j = J; j < J + JB; j += NB) {
-      const int b = (int)std::min<int64_t>(NB, N - j);
-      C *Lblk = Linv + (j / NB) * NB * NB;
-      DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
-      const int64_t rest = N - j - b;
-      if (rest <= 0) break;
-      DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W, NBO, (int)(j - J));
-      const int64_t c_hi = J + JB;  // strip update inside the block column
-      if (j + b < c_hi) {
-        dim3 g(blocks_for(rest, 64), blocks_for(c_hi - (j + b), 64));
-        DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, c_hi, j, b, F, W, NBO, (int)(j - J));
-      }
-    }
-    const int64_t r_lo = J + JB, rest = N - r_lo;
-    if (rest <= 0) break;
+  // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
+  // rows >= r0, columns [r0, c_hi)
+  auto update = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, int woff) {
+    const int64_t rest = N - r0;
+    if (rest <= 0 || c_hi <= r0) return;
     kt_begin(c);
     if (use_tc) {
-      dmb::tc_ldlt_update_c64(c, N, r_lo, J, (int)JB, (float2 *)F, (const float2 *)W);
+      dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)W, NBW, woff);
     } else {
-      dim3 g(blocks_for(rest, 64), blocks_for(rest, 64));
-      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r_lo, N, J, (int)JB, F, W, NBO, 0);
+      dim3 g(blocks_for(rest, 64), blocks_for(c_hi - r0, 64));
+      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, W, NBW, woff);
     }
-    // algorithmic work: lower triangle (incl. diagonal) x JB complex MACs
-    kt_end(c, 8.0 * (double)JB * (double)rest * (double)(rest + 1) / 2.0);
+    // algorithmic work: K complex MACs per updated lower-triangle entry
+    const double cols = (double)(c_hi - r0), rows = (double)rest;
+    kt_end(c, 8.0 * K * (cols * rows - cols * (cols - 1) / 2.0));
+  };
+  for (int64_t J2 = 0; J2 < N; J2 += NBW) {
+    const int64_t J2E = std::min<int64_t>(N, J2 + NBW);
+    for (int64_t J = J2; J < J2E; J += NBO) {
+      const int64_t JE = std::min<int64_t>(J2E, J + NBO);
+      for (int64_t j = J; j < JE; j += NB) {
+        const int b = (int)std::min<int64_t>(NB, N - j);
+        C *Lblk = Linv + (j / NB) * NB * NB;
+        DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
+        const int64_t rest = N - j - b;
+        if (rest <= 0) break;
+        DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W, NBW,
+                   (int)(j - J2));
+        if (j + b < JE) {  // strip update inside the middle panel
+          dim3 g(blocks_for(rest, 64), blocks_for(JE - (j + b), 64));
+          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, W, NBW, (int)(j - J2));
+        }
+      }
+      update(JE, J2E, J, (int)(JE - J), (int)(J - J2));  // rest of the block column
+    }
+    update(J2E, N, J2, (int)(J2E - J2), 0);              // trailing matrix
   }
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));

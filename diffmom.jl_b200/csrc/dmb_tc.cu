@@ -40,10 +40,8 @@ using namespace dmb_tc;
 constexpr int TC_BM = 128;                 // real rows per tile (64 complex rows)
 constexpr int TC_BN = 256;                 // complex columns per tile
 constexpr int TC_BK = 32;                  // floats per stage (one 128-B swizzle row)
-constexpr int TC_KC = 256;                 // complex K of one update (block column width)
-constexpr int TC_K = 6 * TC_KC;            // 3 (split) x 2 (re/im) x 256 = 1536
+constexpr int TC_K = 6 * 256;              // floats per 256-wide complex K block: 3 (split) x 2 (re/im) x 256
 constexpr int TC_STAGES = 4;
-constexpr int TC_KCHUNKS = TC_K / TC_BK;   // 12
 constexpr int TC_A_STAGE = TC_BM * TC_BK * 4;  // 16 KB
 constexpr int TC_B_STAGE = TC_BN * TC_BK * 4;  // 32 KB
 constexpr int TC_SMEM = TC_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 /*barriers*/ + 1024 /*align*/;
@@ -62,44 +60,50 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
 }
 
 // ---------------------------------------------------------------------------
-// operand packing: rows m in [0, rest) relative to j0
+// operand packing for the trailing update, rows m in [0, rest) relative to r0,
+// complex K in blocks of 256 (block kb at floats 1536 kb of a row):
 //   A'' real row (128*(m/64) + m%64):      [Wr_h, -Wi_h, Wr_h, -Wi_h, Wr_l, -Wi_l]
 //   A'' imag row (128*(m/64) + 64 + m%64): [Wi_h,  Wr_h, Wi_h,  Wr_h, Wi_l,  Wr_l]
-//   B'' row m:                             [Lr_h,  Li_h, Lr_l,  Li_l, Lr_h,  Li_h]
-// columns k >= b are zero.
+//   B'' row m (m < ncols):                 [Lr_h,  Li_h, Lr_l,  Li_l, Lr_h,  Li_h]
+// with W[r0 + m][woff + k] (stride wstride) and L[r0 + m][jcol + k]; k >= K zero.
+// grid (rest, Kpad / 256), 256 threads.
 // ---------------------------------------------------------------------------
-__global__ void k_tc_pack(int64_t rest, int64_t N, int64_t j0, int64_t jcol, int b, const float2 *__restrict__ F,
-                          const float2 *__restrict__ W, float *__restrict__ Ap, float *__restrict__ Bp) {
-  int64_t m = blockIdx.x;
-  int k = threadIdx.x;  // TC_KC threads
+__global__ void k_tc_pack(int64_t rest, int64_t ncols, int64_t N, int64_t r0, int64_t jcol, int K, int64_t ld,
+                          const float2 *__restrict__ F, const float2 *__restrict__ W, int wstride, int woff,
+                          float *__restrict__ Ap, float *__restrict__ Bp) {
+  const int64_t m = blockIdx.x;
+  const int kb = blockIdx.y, kk = threadIdx.x, k = kb * 256 + kk;
   if (m >= rest) return;
   float2 w = make_float2(0.f, 0.f), l = make_float2(0.f, 0.f);
-  if (k < b) {
-    w = W[(j0 + m) * TC_KC + k];
-    l = F[(j0 + m) * N + jcol + k];
+  if (k < K) {
+    w = W[(r0 + m) * wstride + woff + k];
+    if (m < ncols) l = F[(r0 + m) * N + jcol + k];
   }
   float wrh = tf32_rna(w.x), wih = tf32_rna(w.y);
   float wrl = tf32_rna(w.x - wrh), wil = tf32_rna(w.y - wih);
-  float lrh = tf32_rna(l.x), lih = tf32_rna(l.y);
-  float lrl = tf32_rna(l.x - lrh), lil = tf32_rna(l.y - lih);
   int64_t bi = m / 64, r = m % 64;
-  float *ar = Ap + (128 * bi + r) * TC_K;
-  float *ai = Ap + (128 * bi + 64 + r) * TC_K;
-  float *br = Bp + m * TC_K;
-  const int S = TC_KC;
-  ar[k] = wrh; ar[S + k] = -wih; ar[2 * S + k] = wrh; ar[3 * S + k] = -wih; ar[4 * S + k] = wrl; ar[5 * S + k] = -wil;
-  ai[k] = wih; ai[S + k] = wrh;  ai[2 * S + k] = wih; ai[3 * S + k] = wrh;  ai[4 * S + k] = wil; ai[5 * S + k] = wrl;
-  br[k] = lrh; br[S + k] = lih;  br[2 * S + k] = lrl; br[3 * S + k] = lil;  br[4 * S + k] = lrh; br[5 * S + k] = lih;
+  float *ar = Ap + (128 * bi + r) * ld + kb * 1536;
+  float *ai = Ap + (128 * bi + 64 + r) * ld + kb * 1536;
+  const int S = 256;
+  ar[kk] = wrh; ar[S + kk] = -wih; ar[2 * S + kk] = wrh; ar[3 * S + kk] = -wih; ar[4 * S + kk] = wrl; ar[5 * S + kk] = -wil;
+  ai[kk] = wih; ai[S + kk] = wrh;  ai[2 * S + kk] = wih; ai[3 * S + kk] = wrh;  ai[4 * S + kk] = wil; ai[5 * S + kk] = wrl;
+  if (m < ncols) {
+    float lrh = tf32_rna(l.x), lih = tf32_rna(l.y);
+    float lrl = tf32_rna(l.x - lrh), lil = tf32_rna(l.y - lih);
+    float *br = Bp + m * ld + kb * 1536;
+    br[kk] = lrh; br[S + kk] = lih;  br[2 * S + kk] = lrl; br[3 * S + kk] = lil;  br[4 * S + kk] = lrh; br[5 * S + kk] = lih;
+  }
 }
 
 __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
-                                                    int64_t N, int64_t j0, int64_t rest, unsigned *err) {
+                                                    int64_t N, int64_t j0, int64_t rest, int64_t c_hi, int nchunks,
+                                                    unsigned *err) {
   // grid.x walks row blocks fastest, so CTAs running together share the
   // column block's B operand in L2
   const int64_t row0 = (int64_t)blockIdx.x * 64;   // complex rows of the tile (relative to j0)
   const int64_t col0 = (int64_t)blockIdx.y * TC_BN;
-  if (row0 >= rest || col0 > row0 + 63) return;  // uniform: tile outside the lower triangle
+  if (row0 >= rest || col0 > row0 + 63 || j0 + col0 >= c_hi) return;  // uniform: tile outside the update
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 
   if (warp == 0 && lane == 0) {
     // TMA producer
-    for (int kc = 0; kc < TC_KCHUNKS; kc++) {
+    for (int kc = 0; kc < nchunks; kc++) {
       const int s = kc % TC_STAGES;
       if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
     bool ok = true;
-    for (int kc = 0; kc < TC_KCHUNKS && ok; kc++) {
+    for (int kc = 0; kc < nchunks && ok; kc++) {
       const int s = kc % TC_STAGES;
       if (!mbar_wait(full0 + 8 * s, (kc / TC_STAGES) & 1, err, abort_flag)) {
         ok = false;
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
       for (int i = 0; i < 16; i++) {
         const int r = rr + 4 * i;
         const int64_t gr = j0 + row0 + r;
-        if (gr < N && gc < N && gc <= gr) {
+        if (gr < N && gc < c_hi && gc <= gr) {
           float2 *p = F + gr * N + gc;
           float2 cv = *p;
           cv.x -= E[r * 33 + q];
@@ -424,7 +428,7 @@ void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows, u
 
 struct TcState {
   DevBuf A, B, err;
-  CUtensorMap mapA, mapB;
+  CUtensorMap mapAK[4], mapBK[4];
   int64_t n_key = -1;
   bool attr = false;
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
@@ -478,31 +482,44 @@ bool tc_available(dmb_ctx *c) {
   return major == 10 && encode_fn() != nullptr;
 }
 
-void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t j0, int64_t jcol, int b, float2 *F, const float2 *W) {
+// Trailing update of the complex64 LDL^T on the tensor cores:
+//   F[r][c] -= sum_{k < K} W[r][woff + k] L[c][jcol + k],  r0 <= c < c_hi, c <= r < N
+// K <= 1024 (the packed buffers are sized for that).
+void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t jcol, int K, float2 *F,
+                        const float2 *W, int wstride, int woff) {
+  DMB_REQUIRE(K >= 1 && K <= 1024, DMB_ERR_STATE, "tensor-core update width must be 1..1024");
   TcState &st = tc_state(c);
   const int64_t npadA = ((N + 63) / 64) * 64;
   const int64_t npadB = ((N + TC_BN - 1) / TC_BN) * TC_BN;
+  const int64_t Kpad = ((K + 255) / 256) * 256, ld = 6 * Kpad;
   if (st.n_key != N) {
-    st.A.ensure(sizeof(float) * 2 * npadA * TC_K);
-    st.B.ensure(sizeof(float) * npadB * TC_K);
-    st.err.ensure(16);
-    DMB_CUDA(cudaMemsetAsync(st.A.p, 0, sizeof(float) * 2 * npadA * TC_K, c->stream));
-    DMB_CUDA(cudaMemsetAsync(st.B.p, 0, sizeof(float) * npadB * TC_K, c->stream));
-    DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
-    make_map(&st.mapA, st.A.as<float>(), (uint64_t)(2 * npadA), TC_BM);
-    make_map(&st.mapB, st.B.as<float>(), (uint64_t)npadB, TC_BN);
+    st.A.ensure(sizeof(float) * 2 * npadA * 6 * 1024);
+    st.B.ensure(sizeof(float) * npadB * 6 * 1024);
+    DMB_CUDA(cudaMemsetAsync(st.B.p, 0, sizeof(float) * npadB * 6 * 1024, c->stream));
+    for (int i = 0; i < 4; i++) {
+      make_map(&st.mapAK[i], st.A.as<float>(), (uint64_t)(2 * npadA), TC_BM, 1536 * (i + 1));
+      make_map(&st.mapBK[i], st.B.as<float>(), (uint64_t)npadB, TC_BN, 1536 * (i + 1));
+    }
     st.n_key = N;
+  }
+  if (!st.err.p) {
+    st.err.ensure(16);
+    DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.attr) {
     DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     st.attr = true;
   }
-  const int64_t rest = N - j0;
-  DMB_REQUIRE(b <= TC_KC, DMB_ERR_STATE, "tensor-core update width exceeds 256");
-  DMB_LAUNCH(c, k_tc_pack, (unsigned)rest, TC_KC, 0, rest, N, j0, jcol, b, F, W, st.A.as<float>(),
-             st.B.as<float>());
-  dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((rest + TC_BN - 1) / TC_BN));
-  DMB_LAUNCH(c, k_tc_syrk, grid, 128, TC_SMEM, st.mapA, st.mapB, F, N, j0, rest, st.err.as<unsigned>());
+  const int64_t rest = N - r0, ncols = std::min<int64_t>(c_hi, N) - r0;
+  if (rest <= 0 || ncols <= 0) return;
+  const int kslot = (int)(Kpad / 256) - 1;
+  // A'' rows past `rest` and B'' rows past `ncols` keep stale values: they only
+  // feed output rows >= N and columns >= c_hi, which the epilogue skips
+  DMB_LAUNCH(c, k_tc_pack, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
+             N, r0, jcol, K, ld, F, W, wstride, woff, st.A.as<float>(), st.B.as<float>());
+  dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
+  DMB_LAUNCH(c, k_tc_syrk, grid, 128, TC_SMEM, st.mapAK[kslot], st.mapBK[kslot], F, N, r0, rest,
+             std::min<int64_t>(c_hi, N), (int)(ld / TC_BK), st.err.as<unsigned>());
 }
 
 unsigned tc_error_word(dmb_ctx *c) {
