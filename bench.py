@@ -190,8 +190,11 @@ class Runner:
         torch.cuda.synchronize()
         self.barrier()
         ms = self.max_over_ranks(e0.elapsed_time(e1))
+        tm = dev.timings()
         res = {"ms_per_step": ms / steps, "solves_per_s": self.ws * steps * per_step_units / (ms / 1e3),
-               "steps": steps, "warmup": warmup, "launches": dev.timings().kernels - k0}
+               "steps": steps, "warmup": warmup, "launches": tm.kernels - k0,
+               "stage_ms_last_step": {"assembly": tm.assembly_ms, "preconditioner": tm.precond_ms,
+                                      "rhs": tm.rhs_ms, "gmres": tm.gmres_ms, "total": tm.solve_ms}}
         if clk:
             res["clocks"] = clk.stop()
         if kernel_timing:

@@ -413,6 +413,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   out->true_residual = tres;
   out->restarts = restarts;
   c->tm.solve_ms = now_ms() - t0;
+  c->tm.gmres_ms = c->tm.solve_ms;
 }
 
 }  // namespace dmb

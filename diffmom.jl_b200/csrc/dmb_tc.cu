@@ -235,10 +235,16 @@ template <int ROLE>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
                                                     int nchunks, int64_t M, int64_t Rv, double2 *__restrict__ Y,
-                                                    int64_t ldy, int mode, unsigned *err) {
+                                                    int64_t ldy, int mode, int tri, unsigned *err) {
   const int64_t col0 = (int64_t)blockIdx.x * TC_BN;
   const int64_t row0 = (int64_t)blockIdx.y * 64;
   if (row0 >= M || col0 >= Rv) return;  // uniform
+  // triangular A (tri 1: lower, A[m][k] = 0 for k > m; tri 2: upper): only the
+  // 256-wide K blocks that meet this row tile's rows are streamed (48 chunks each)
+  int kc0 = 0, kc1 = nchunks;
+  if (tri == 1) kc1 = min(nchunks, 48 * (int)((row0 + 64 + 255) / 256));
+  else if (tri == 2) kc0 = 48 * (int)(row0 / 256);
+  const int nk = kc1 - kc0;
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -274,18 +280,18 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   const uint32_t tmem_d = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    for (int kc = 0; kc < nchunks; kc++) {
-      const int s = kc % TC_STAGES;
-      if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
+    for (int i = 0; i < nk; i++) {
+      const int s = i % TC_STAGES, kc = kc0 + i;
+      if (i >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((i / TC_STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
       tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kc * TC_BK, a_row0 + (int)(2 * row0), full0 + 8 * s);
       tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
-    for (int kc = 0; kc < nchunks && ok; kc++) {
-      const int s = kc % TC_STAGES;
-      if (!mbar_wait(full0 + 8 * s, (kc / TC_STAGES) & 1, err, abort_flag)) {
+    for (int i = 0; i < nk && ok; i++) {
+      const int s = i % TC_STAGES;
+      if (!mbar_wait(full0 + 8 * s, (i / TC_STAGES) & 1, err, abort_flag)) {
         ok = false;
         break;
       }
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
       for (int k = 0; k < TC_BK / 8; k++) {
         const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
         const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
-        umma_tf32(tmem_d, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+        umma_tf32(tmem_d, ad, bd, (i > 0 || k > 0) ? 1u : 0u);
       }
       umma_commit(empty0 + 8 * s);
     }
@@ -558,7 +564,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm<0>, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0,
+  DMB_LAUNCH(c, k_tc_gemm<0>, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -601,7 +607,7 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
   DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
-             X + r_lo, N, 1, st.err.as<unsigned>());
+             X + r_lo, N, 1, 0, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
 
@@ -648,7 +654,7 @@ void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int
 
 // Y (op)= A_packed[rows a_row0.., K from a_kx0] * X[k0 : k0 + w], B packed here
 void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0, int a_kx0, int64_t M, int w,
-                    const double2 *Xk, double2 *Y, int64_t N, int64_t R, int mode) {
+                    const double2 *Xk, double2 *Y, int64_t N, int64_t R, int mode, int tri) {
   if (M <= 0) return;
   const int64_t Kpad = round_up(w, 256), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
   const int kslot = (int)(Kpad / 256) - 1;
@@ -662,8 +668,9 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
   DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0, (int)(6 * Kpad / TC_BK), M,
-             R, Y, N, mode, st.err.as<unsigned>());
-  kt_end(c, 8.0 * (double)M * (double)w * (double)R);
+             R, Y, N, mode, tri, st.err.as<unsigned>());
+  // a triangular A does half the MACs
+  kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
 }
 
 // one sweep of the batched solve with the packed factor:
@@ -678,11 +685,12 @@ void tc_trsm_sweep(dmb_ctx *c, int64_t N, double2 *X, int64_t R, bool backward) 
     const int64_t o = backward ? nout - 1 - s : s;
     const int64_t o0 = o * TB, o1 = std::min<int64_t>(N, o0 + TB);
     const int ow = (int)(o1 - o0);
-    gemm_prepacked(c, st, backward ? st.mapDb : st.mapDf, (int)(2 * TB * o), 0, ow, ow, X + o0, X + o0, N, R, 0);
+    gemm_prepacked(c, st, backward ? st.mapDb : st.mapDf, (int)(2 * TB * o), 0, ow, ow, X + o0, X + o0, N, R, 0,
+                   backward ? 2 : 1);
     if (backward)
-      gemm_prepacked(c, st, st.mapLt, 0, (int)(6 * o0), o0, ow, X + o0, X, N, R, 1);
+      gemm_prepacked(c, st, st.mapLt, 0, (int)(6 * o0), o0, ow, X + o0, X, N, R, 1, 0);
     else
-      gemm_prepacked(c, st, st.mapL, (int)(2 * o1), (int)(6 * o0), N - o1, ow, X + o0, X + o1, N, R, 1);
+      gemm_prepacked(c, st, st.mapL, (int)(2 * o1), (int)(6 * o0), N - o1, ow, X + o0, X + o1, N, R, 1, 0);
   }
 }
 

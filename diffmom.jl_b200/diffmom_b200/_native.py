@@ -84,7 +84,7 @@ class Timings(ctypes.Structure):
     _fields_ = [("geometry_ms", ctypes.c_double), ("assembly_ms", ctypes.c_double),
                 ("precond_ms", ctypes.c_double), ("rhs_ms", ctypes.c_double),
                 ("solve_ms", ctypes.c_double), ("nnz_ratio", ctypes.c_double),
-                ("kernels", ctypes.c_int64)]
+                ("kernels", ctypes.c_int64), ("gmres_ms", ctypes.c_double)]
 
 
 class SolveParams(ctypes.Structure):

@@ -75,6 +75,7 @@ typedef struct {
   double solve_ms;      /* GMRES / direct solve */
   double nnz_ratio;     /* near-field fill of the last preconditioner */
   int64_t kernels;      /* kernels launched by this context so far */
+  double gmres_ms;      /* the GMRES part alone (resident solves put their total in solve_ms) */
 } dmb_timings;
 
 /* ---- context ----------------------------------------------------------- */
