@@ -241,8 +241,8 @@ def run_ours(args):
     dev = EFIEDevice(mesh, rwg, device=local)
     sig = np.empty(R_WAVES)
 
-    def c3_step(precision, precond, cutoff):
-        p = solve_params(nat, K, precision, precond, cutoff, maxiter=200)
+    def c3_step(precision, precond, cutoff, side=1):
+        p = solve_params(nat, K, precision, precond, cutoff, side=side, maxiter=200)
         st = nat.GmresStats()
 
         def step():
@@ -414,7 +414,7 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         "data": "synthetic plate mesh and seeded incidences (seed 20260001)",
         "config": {"workload": WORKLOAD, "N_rwg": N, "N_tri": mesh.ntriangles, "incidences": R_WAVES,
                    "quad_order": 3, "gmres_tol": 1e-6,
-                   "precond": "complex64 LDL^T of Z (near-field cutoff = inf), left",
+                   "precond": "complex64 LDL^T of Z (near-field cutoff = inf), right (flexible form)",
                    "variant": "c3_mixed_batched", "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (Z 912 MB complex64; packed 3xTF32 Z 5.5 GB)"},
         "variants": {k: clean(v) for k, v in variants.items()},

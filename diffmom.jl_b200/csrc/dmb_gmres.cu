@@ -199,16 +199,15 @@ __global__ void k_sub(int64_t count, const double2 *__restrict__ a, double2 *__r
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < count) b[i] = csub(a[i], b[i]);
 }
-__global__ void k_add(int64_t count, const double2 *__restrict__ a, double2 *__restrict__ b) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < count) b[i] = cadd(b[i], a[i]);
-}
 
 }  // namespace
 
 namespace dmb {
 
-void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, double2 *w, double2 *tmp,
+// w = op(v).  Right preconditioning keeps z = M^-1 v (flexible GMRES form):
+// the solution is then sum y_i z_i and needs no further preconditioner
+// application, and an inexact (tensor-core) preconditioner stays consistent.
+void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, double2 *w, double2 *z,
                     int64_t R) {
   const int64_t N = c->n;
   if (precond_kind == DMB_PRECOND_NONE) {
@@ -217,9 +216,9 @@ void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, do
     matvec_op(c, v, w, R);
     pc_apply_dev(c, (double *)w, R);
   } else {
-    DMB_CUDA(cudaMemcpyAsync(tmp, v, sizeof(double2) * N * R, cudaMemcpyDeviceToDevice, c->stream));
-    pc_apply_dev(c, (double *)tmp, R);
-    matvec_op(c, tmp, w, R);
+    DMB_CUDA(cudaMemcpyAsync(z, v, sizeof(double2) * N * R, cudaMemcpyDeviceToDevice, c->stream));
+    pc_apply_dev(c, (double *)z, R);
+    matvec_op(c, z, w, R);
   }
 }
 
@@ -234,21 +233,27 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   DMB_REQUIRE(precond_kind == DMB_PRECOND_NONE || precond_kind == c->pc_kind, DMB_ERR_STATE,
               "requested preconditioner kind differs from the one built");
   // basis capacity: maxiter vectors, bounded by a 40% share of free memory
-  // (decided once per problem shape; repeated solves reuse the buffers)
+  // (decided once per problem shape; repeated solves reuse the buffers); the
+  // right-preconditioned form also keeps the preconditioned vectors
+  const bool flex = precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_RIGHT;
   size_t vec_bytes = sizeof(double2) * N * R;
-  if (!(c->gm_key_n == N && c->gm_key_r == R && c->gm_key_maxiter == maxiter && c->gm_kcap > 0)) {
+  if (!(c->gm_key_n == N && c->gm_key_r == R && c->gm_key_maxiter == maxiter && c->gm_key_flex == flex &&
+        c->gm_kcap > 0)) {
     size_t freeb = 0, totb = 0;
     DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
-    freeb += c->d_V.bytes;  // the current basis can be reused
-    int64_t cap_mem = (int64_t)((freeb * 0.4) / vec_bytes) - 1;
+    freeb += c->d_V.bytes + c->d_Zv.bytes;  // the current buffers can be reused
+    int64_t cap_mem = (int64_t)((freeb * 0.4) / (vec_bytes * (flex ? 2 : 1))) - 1;
     c->gm_kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
     c->gm_key_n = N;
     c->gm_key_r = R;
     c->gm_key_maxiter = maxiter;
+    c->gm_key_flex = flex;
   }
   const int kcap = c->gm_kcap;
   const int64_t vstride = N * R;
   c->d_V.ensure(vec_bytes * (kcap + 1));
+  if (flex) c->d_Zv.ensure(vec_bytes * kcap);
+  double2 *Zv = flex ? c->d_Zv.as<double2>() : nullptr;
   c->d_work.ensure(vec_bytes * 2);
   // layout: H[R][(k+1)k] g[R][k+1] sn[R][k] hb[R][k+1] y[R][k] | cs[R][k] nrm[2R] | st[R] | active
   size_t small = sizeof(double2) * R * ((size_t)(kcap + 1) * kcap + 2 * (kcap + 1) + 2 * kcap) +
@@ -330,7 +335,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     int j = 0;
     for (; j < kcap && total_iters < maxiter; j++, total_iters++) {
       double2 *Vj = V + (int64_t)j * vstride;
-      apply_operator(c, precond_kind, side, Vj, w, tmp, R);
+      apply_operator(c, precond_kind, side, Vj, w, flex ? Zv + (int64_t)j * vstride : tmp, R);
       for (int pass = 0; pass < 2; pass++) {
         DMB_LAUNCH(c, k_dots, dim3(j + 1, (unsigned)R), 256, 0, N, R, j, vstride, V, w, hb, kcap + 1);
         DMB_LAUNCH(c, k_cgs_update, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, hb, kcap + 1, w);
@@ -356,11 +361,8 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     }
     // solution update from this cycle
     DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);
-    if (precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_RIGHT) {
-      DMB_CUDA(cudaMemsetAsync(tmp, 0, vec_bytes, c->stream));
-      DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, tmp);
-      pc_apply_dev(c, (double *)tmp, R);
-      DMB_LAUNCH(c, k_add, blocks_for(N * R, 256), 256, 0, N * R, tmp, x);
+    if (flex) {
+      DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, Zv, ybuf, kcap, x);
     } else {
       DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, x);
     }

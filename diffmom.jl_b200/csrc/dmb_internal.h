@@ -145,8 +145,8 @@ struct dmb_ctx {
   DevBuf d_net;       // learned weights
   bool net_loaded = false;
 
-  // GMRES workspace
-  DevBuf d_V, d_H, d_work, d_vecs, d_scal;
+  // GMRES workspace (d_Zv: preconditioned basis of the right-preconditioned form)
+  DevBuf d_V, d_H, d_work, d_vecs, d_scal, d_Zv;
 
   // resident solution of dmb_solve_resident / dmb_solve_resident_many
   DevBuf d_rhs, d_sol, d_mono;
@@ -165,6 +165,7 @@ struct dmb_ctx {
   int gm_kcap = 0;              // cached GMRES basis capacity
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;
+  bool gm_key_flex = false;
 
   // timings
   dmb_timings tm{};

@@ -45,10 +45,23 @@ constexpr int TC_STAGES = 4;
 constexpr int TC_A_STAGE = TC_BM * TC_BK * 4;  // 16 KB
 constexpr int TC_B_STAGE = TC_BN * TC_BK * 4;  // 32 KB
 constexpr int TC_SMEM = TC_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 /*barriers*/ + 1024 /*align*/;
+constexpr int TC_SMEM_128 = TC_STAGES * (TC_A_STAGE + TC_B_STAGE / 2) + 1024 + 1024;
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
                               ((uint32_t)(TC_BM >> 4) << 24);
+
+template <int BN>
+__device__ __forceinline__ void umma_tf32_n(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                             ((uint32_t)(TC_BM >> 4) << 24);
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
@@ -230,13 +243,16 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 // from DRAM once.
 // ---------------------------------------------------------------------------
 // ROLE only names the launch site for profilers: 0 = Z X of the Krylov
-// operator, 1 = triangular-solve GEMMs.
-template <int ROLE>
+// operator, 1 = triangular-solve GEMMs.  BN (256 or 128) is the tile width in
+// complex columns: the 128-wide form doubles the CTAs of launches that would
+// otherwise fill fewer than two waves.
+template <int ROLE, int BN>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
                                                     int nchunks, int64_t M, int64_t Rv, double2 *__restrict__ Y,
                                                     int64_t ldy, int mode, int tri, unsigned *err) {
-  const int64_t col0 = (int64_t)blockIdx.x * TC_BN;
+  constexpr int B_STAGE = BN * TC_BK * 4;
+  const int64_t col0 = (int64_t)blockIdx.x * BN;
   const int64_t row0 = (int64_t)blockIdx.y * 64;
   if (row0 >= M || col0 >= Rv) return;  // uniform
   // triangular A (tri 1: lower, A[m][k] = 0 for k > m; tri 2: upper): only the
@@ -252,7 +268,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   unsigned char *gbase = smem_raw + (base - raw);
   const uint32_t sA = base;
   const uint32_t sB = base + TC_STAGES * TC_A_STAGE;
-  const uint32_t sBar = sB + TC_STAGES * TC_B_STAGE;
+  const uint32_t sBar = sB + TC_STAGES * B_STAGE;
   uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
   volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
@@ -271,7 +287,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(const_cast<uint32_t *>(tmem_slot))),
-                 "r"(TC_BN)
+                 "r"(BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -283,9 +299,9 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
     for (int i = 0; i < nk; i++) {
       const int s = i % TC_STAGES, kc = kc0 + i;
       if (i >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((i / TC_STAGES) - 1) & 1, err, abort_flag)) break;
-      mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
+      mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + B_STAGE);
       tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kc * TC_BK, a_row0 + (int)(2 * row0), full0 + 8 * s);
-      tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
+      tma_load_2d(sB + s * B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
@@ -299,8 +315,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
 #pragma unroll
       for (int k = 0; k < TC_BK / 8; k++) {
         const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
-        const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
-        umma_tf32(tmem_d, ad, bd, (i > 0 || k > 0) ? 1u : 0u);
+        const uint64_t bd = sw128_desc(sB + s * B_STAGE + k * 32);
+        umma_tf32_n<BN>(tmem_d, ad, bd, (i > 0 || k > 0) ? 1u : 0u);
       }
       umma_commit(empty0 + 8 * s);
     }
@@ -315,7 +331,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     const int rl = threadIdx.x & 63, qh = threadIdx.x >> 6;
     const int64_t gr = row0 + rl;
-    for (int cc = 0; cc < TC_BN / 32; cc++) {
+    for (int cc = 0; cc < BN / 32; cc++) {
       if (col0 + cc * 32 >= Rv) break;  // uniform
       uint32_t v[32];
       asm volatile(
@@ -363,7 +379,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TC_BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(BN) : "memory");
 }
 
 // split one complex value into the six 256-strided A'' / B'' segment entries
@@ -440,7 +456,7 @@ struct TcState {
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
   // sides, packed triangular-solve panels
   DevBuf Zp, Xp, Pa, Pb;
-  CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4];
+  CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4], mapPbK128[4];
   uint64_t zp_version = ~0ull;
   // factor packed once per factorisation for the batched triangular solves:
   // L'' (strict lower), (L^T)'' and the inverses of the 1024-row diagonal
@@ -471,8 +487,9 @@ void ensure_gemm(dmb_ctx *c, TcState &st) {
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.gemm_attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<0, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
     st.gemm_attr = true;
   }
 }
@@ -564,7 +581,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm<0>, grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0, 0,
+  DMB_LAUNCH(c, (k_tc_gemm<0, 256>), grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -592,7 +609,10 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
   }
   if (st.pb_key != Rpad) {
     st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
-    for (int i = 0; i < 4; i++) make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+    for (int i = 0; i < 4; i++) {
+      make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+      make_map(&st.mapPbK128[i], st.Pb.as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
+    }
     st.pb_key = Rpad;
   }
   dim3 ga((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
@@ -606,7 +626,7 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
              N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
+  DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
              X + r_lo, N, 1, 0, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
@@ -660,15 +680,27 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   const int kslot = (int)(Kpad / 256) - 1;
   if (st.pb_key != Rpad) {
     st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
-    for (int i = 0; i < 4; i++) make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+    for (int i = 0; i < 4; i++) {
+      make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+      make_map(&st.mapPbK128[i], st.Pb.as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
+    }
     st.pb_key = Rpad;
   }
   DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk, N,
              st.Pb.as<float>());
-  dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
+  // triangular diagonal-block products with few row tiles: 128-wide tiles
+  // double the CTAs (measured faster only there)
+  const bool narrow = tri != 0 && (Rpad / TC_BN) * (Mpad / 64) < 2 * (int64_t)c->sm_count;
   kt_begin(c);
-  DMB_LAUNCH(c, k_tc_gemm<1>, grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0, (int)(6 * Kpad / TC_BK), M,
-             R, Y, N, mode, tri, st.err.as<unsigned>());
+  if (narrow) {
+    dim3 grid((unsigned)(Rpad / 128), (unsigned)(Mpad / 64));
+    DMB_LAUNCH(c, (k_tc_gemm<1, 128>), grid, 128, TC_SMEM_128, mapA, st.mapPbK128[kslot], a_row0, a_kx0,
+               (int)(6 * Kpad / TC_BK), M, R, Y, N, mode, tri, st.err.as<unsigned>());
+  } else {
+    dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
+    DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0,
+               (int)(6 * Kpad / TC_BK), M, R, Y, N, mode, tri, st.err.as<unsigned>());
+  }
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
 }

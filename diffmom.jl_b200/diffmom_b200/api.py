@@ -226,7 +226,7 @@ class EFIEDevice:
 
     def solve_many(self, k: float, kvecs, pols, E0s=None, precision: str = "mixed",
                    preconditioner: str = "lu", cutoff: float = math.inf, tol: float = 1e-6,
-                   maxiter: int = 300, precond_side: str = "left", quad_order: int = 3,
+                   maxiter: int = 300, precond_side: str = "right", quad_order: int = 3,
                    eta0: float = ETA0_DEFAULT, rcs: bool = True):
         """Assemble Z, build the preconditioner, solve all incidences by block
         GMRES and (rcs=True) return the monostatic sigma of each; the currents
@@ -562,7 +562,7 @@ class MonostaticResult:
 
 def monostatic_rcs_sweep(mesh: TriMesh, freq_hz, excitations, precision: str = "mixed",
                          preconditioner: str = "lu", nf_cutoff_lambda: float = math.inf,
-                         gmres_tol: float = 1e-6, gmres_maxiter: int = 300, precond_side: str = "left",
+                         gmres_tol: float = 1e-6, gmres_maxiter: int = 300, precond_side: str = "right",
                          quad_order: int = 3, c0: float = C0_DEFAULT, return_currents: bool = False,
                          device: EFIEDevice | None = None, rwg: RWGData | None = None) -> MonostaticResult:
     """Monostatic RCS over many plane-wave incidences: what a loop of
