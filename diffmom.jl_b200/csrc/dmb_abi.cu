@@ -86,6 +86,9 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     dmb::oz_release(c);
     dmb::local_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
+    for (auto &e : c->la_ev)
+      if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
   }
   delete c;

@@ -532,9 +532,14 @@ template <class C> void set_smem_attrs() {
 // panel, SIMT strip updates inside the 256 columns).  After each middle panel
 // the rest of the 1024-wide block column receives one K = 256 update, and after
 // the block column the whole trailing matrix receives one K = 1024 update --
-// both on the tensor cores for complex64 factors.  The big update is long-K
-// (compute-dominated) and the trailing matrix is read and written once per
-// 1024 columns.  W (N x NBW) holds L21 D1 for the current block column.
+// both on the tensor cores for complex64 factors.
+//
+// Lookahead: every such update is split into the next 256 columns (main
+// stream, needed by the next panel) and the rest (second stream).  The next
+// panel's latency-bound diagonal/panel/strip kernels then run while the rest of
+// the update streams through the tensor cores; they touch disjoint columns, W
+// is double-buffered per block column, and the next update on the main stream
+// first joins the second stream (it reuses the packed-operand buffers).
 constexpr int NBO = 256;
 constexpr int NBW = 1024;
 
@@ -543,11 +548,13 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const int64_t N = c->n;
   set_smem_attrs<C>();
   const int nblk = (int)((N + NB - 1) / NB);
-  c->d_W.ensure(sizeof(C) * N * NBW);
+  c->d_W.ensure(sizeof(C) * N * NBW * 2);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   c->d_flags.ensure(64);
+  if (!c->stream2) DMB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+  for (auto &e : c->la_ev)
+    if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   unsigned *err = c->d_flags.as<unsigned>();
-  C *W = c->d_W.as<C>();
   C *Linv = c->d_dinv.as<C>();
   DMB_CUDA(cudaMemsetAsync(err, 0, 4, c->stream));
   const size_t sm_diag = sizeof(C) * (NB * (NB + 1) + NB);
@@ -555,21 +562,45 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
   // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
   // rows >= r0, columns [r0, c_hi)
-  auto update = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, int woff) {
+  auto update = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
     const int64_t rest = N - r0;
     if (rest <= 0 || c_hi <= r0) return;
     kt_begin(c);
     if (use_tc) {
-      dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)W, NBW, woff);
+      dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)Wb, NBW, woff);
     } else {
       dim3 g(blocks_for(rest, 64), blocks_for(c_hi - r0, 64));
-      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, W, NBW, woff);
+      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, Wb, NBW, woff);
     }
     // algorithmic work: K complex MACs per updated lower-triangle entry
     const double cols = (double)(c_hi - r0), rows = (double)rest;
     kt_end(c, 8.0 * K * (cols * rows - cols * (cols - 1) / 2.0));
   };
-  for (int64_t J2 = 0; J2 < N; J2 += NBW) {
+  bool pending = false;  // the second stream holds an update not yet joined
+  auto join = [&] {
+    if (pending) {
+      DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[1], 0));
+      pending = false;
+    }
+  };
+  auto update_split = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
+    join();
+    const int64_t cmid = std::min<int64_t>(c_hi, r0 + NBO);
+    update(r0, cmid, jcol, K, Wb, woff);
+    if (cmid < c_hi && cmid < N) {
+      DMB_CUDA(cudaEventRecord(c->la_ev[0], c->stream));
+      DMB_CUDA(cudaStreamWaitEvent(c->stream2, c->la_ev[0], 0));
+      {
+        StreamSwap sw(c, c->stream2);
+        update(cmid, c_hi, jcol, K, Wb, woff);
+      }
+      DMB_CUDA(cudaEventRecord(c->la_ev[1], c->stream2));
+      pending = true;
+    }
+  };
+  int64_t bc = 0;
+  for (int64_t J2 = 0; J2 < N; J2 += NBW, bc++) {
+    C *Wb = c->d_W.as<C>() + (bc & 1) * N * NBW;
     const int64_t J2E = std::min<int64_t>(N, J2 + NBW);
     for (int64_t J = J2; J < J2E; J += NBO) {
       const int64_t JE = std::min<int64_t>(J2E, J + NBO);
@@ -579,17 +610,18 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
         DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
         const int64_t rest = N - j - b;
         if (rest <= 0) break;
-        DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, W, NBW,
+        DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, Wb, NBW,
                    (int)(j - J2));
         if (j + b < JE) {  // strip update inside the middle panel
           dim3 g(blocks_for(rest, 64), blocks_for(JE - (j + b), 64));
-          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, W, NBW, (int)(j - J2));
+          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, Wb, NBW, (int)(j - J2));
         }
       }
-      update(JE, J2E, J, (int)(JE - J), (int)(J - J2));  // rest of the block column
+      update_split(JE, J2E, J, (int)(JE - J), Wb, (int)(J - J2));  // rest of the block column
     }
-    update(J2E, N, J2, (int)(J2E - J2), 0);              // trailing matrix
+    update_split(J2E, N, J2, (int)(J2E - J2), Wb, 0);              // trailing matrix
   }
+  join();
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));

@@ -91,6 +91,8 @@ struct NearRec {
 struct dmb_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;      // factorisation lookahead (created on first use)
+  cudaEvent_t la_ev[2] = {nullptr, nullptr};
   std::mutex mu;
   std::string err;
   int sm_count = 148;
@@ -211,6 +213,15 @@ inline void kt_collect(dmb_ctx *c) {
   c->kt_used = 0;
   c->kt_pending.clear();
 }
+
+// Runs the enclosed launches of a context on another stream (the context is
+// used by one thread at a time).
+struct StreamSwap {
+  dmb_ctx *c;
+  cudaStream_t saved;
+  StreamSwap(dmb_ctx *ctx, cudaStream_t s) : c(ctx), saved(ctx->stream) { ctx->stream = s; }
+  ~StreamSwap() { c->stream = saved; }
+};
 
 // ---------------------------------------------------------------------------
 // helpers shared by translation units
