@@ -265,25 +265,6 @@ def run_ours(args):
             v["rcs_rel_err_vs_mixed"] = float(np.max(np.abs(sig_mixed - sig)) / np.max(sig))
         variants["c3_fp64_plain"] = v
 
-    # the same sweep at 20,008 RWG (0.41 m plate, 82 x 82 cells, same cell size)
-    if want("c3_20k_mixed_batched") and not args.quick and PLATE_CELLS == 60:
-        from diffmom_b200 import make_rect_plate as _plate
-        m20 = _plate(0.41, 0.41, 82, 82)
-        r20 = build_rwg(m20)
-        dev20 = EFIEDevice(m20, r20, device=local)
-        sig20 = np.empty(R_WAVES)
-        p20 = solve_params(nat, K, nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf, side=1, maxiter=200)
-        st20 = nat.GmresStats()
-
-        def step20():
-            dev20.ctx.call("dmb_solve_resident_many", ctypes.byref(p20), R_WAVES, nat.dptr(kv), nat.dptr(e0),
-                           nat.dptr(pol), nat.dptr(sig20), ctypes.byref(st20))
-            return st20.niter, st20.true_residual, st20.restarts
-        v20 = run.timed(dev20, step20, 1, 1, R_WAVES)
-        v20["N_rwg"] = r20.nedges
-        variants["c3_20k_mixed_batched"] = v20
-        dev20.close()
-
     # e2e through the public API (host buffers in, sigma out)
     e2e = None
     if head is not None and not args.skip_e2e:
@@ -303,6 +284,25 @@ def run_ours(args):
                "d2h_bytes_per_step": int(8 * R_WAVES),
                "api": "diffmom_b200.monostatic_rcs_sweep(precision=mixed) incl. mesh/RWG upload"}
     dev.close()
+
+    # the same sweep at 20,008 RWG (0.41 m plate, 82 x 82 cells, same cell size)
+    if want("c3_20k_mixed_batched") and not args.quick and PLATE_CELLS == 60:
+        from diffmom_b200 import make_rect_plate as _plate
+        m20 = _plate(0.41, 0.41, 82, 82)
+        r20 = build_rwg(m20)
+        dev20 = EFIEDevice(m20, r20, device=local)
+        sig20 = np.empty(R_WAVES)
+        p20 = solve_params(nat, K, nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf, side=1, maxiter=200)
+        st20 = nat.GmresStats()
+
+        def step20():
+            dev20.ctx.call("dmb_solve_resident_many", ctypes.byref(p20), R_WAVES, nat.dptr(kv), nat.dptr(e0),
+                           nat.dptr(pol), nat.dptr(sig20), ctypes.byref(st20))
+            return st20.niter, st20.true_residual, st20.restarts
+        v20 = run.timed(dev20, step20, 1, 1, R_WAVES)
+        v20["N_rwg"] = r20.nedges
+        variants["c3_20k_mixed_batched"] = v20
+        dev20.close()
 
     # ---- C4 uneven batch of 64 impedance-loaded surfaces -------------------
     if not args.quick and any(want(n) for n in ("c4_batch64_mixed", "c4_batch64_fp64_1lane")):

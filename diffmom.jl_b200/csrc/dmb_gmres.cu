@@ -242,7 +242,11 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     size_t freeb = 0, totb = 0;
     DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
     freeb += c->d_V.bytes + c->d_Zv.bytes;  // the current buffers can be reused
-    int64_t cap_mem = (int64_t)((freeb * 0.4) / (vec_bytes * (flex ? 2 : 1))) - 1;
+    // many right-hand sides: at most 8 GiB of basis (a strong preconditioner
+    // needs a handful of vectors; GMRES restarts if the capacity runs out)
+    double budget = freeb * 0.4;
+    if (R >= 8) budget = std::min(budget, 8.0 * 1024 * 1024 * 1024);
+    int64_t cap_mem = (int64_t)(budget / (double)(vec_bytes * (flex ? 2 : 1))) - 1;
     c->gm_kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
     c->gm_key_n = N;
     c->gm_key_r = R;
