@@ -14,6 +14,8 @@ GMRES preconditioned by the complex64 LDL^T of Z, FP64 Arnoldi and
 refinement residual).
 
 Variants reported beside it (same timing rules, fewer steps where slow):
+  c3_mixed_tf32_refined  the headline with the Krylov product in 3xTF32 and
+                  FP64-residual refinement instead of INT8 slices
   c3_fp64_plain   the same job in plain FP64 (FP64 Z, the reference's
                   near-field LDL^T at 1 lambda, FP64 block GMRES)
   c3_20k_*        the same sweep on a 0.41 m plate (82 x 82 cells, 20,008 RWG)
@@ -199,9 +201,10 @@ class Runner:
         if clk:
             res["clocks"] = clk.stop()
         if kernel_timing:
-            kms, kl, kf = ct.c_double(), ct.c_int64(), ct.c_double()
-            dev.ctx.call("dmb_kernel_timing", ct.byref(kms), ct.byref(kl), ct.byref(kf))
-            res["kernel"] = (kms.value, kl.value, kf.value)
+            for fam, key in ((0, "kernel"), (1, "kernel_int8")):
+                kms, kl, kf = ct.c_double(), ct.c_int64(), ct.c_double()
+                dev.ctx.call("dmb_kernel_timing_family", fam, ct.byref(kms), ct.byref(kl), ct.byref(kf))
+                res[key] = (kms.value, kl.value, kf.value)
         dev.ctx.call("dmb_set_kernel_timing", 0)
         res["last"] = out
         return res
@@ -254,6 +257,11 @@ def run_ours(args):
 
     head = None
     sig_mixed = None
+    if want("c3_mixed_tf32_refined") and not args.quick:
+        dev.set_option("exact_krylov", 0)
+        variants["c3_mixed_tf32_refined"] = run.timed(dev, c3_step(nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf),
+                                                      min(args.steps, 3), args.warmup, R_WAVES)
+        dev.set_option("exact_krylov", 1)
     if want("c3_mixed_batched"):
         head = run.timed(dev, c3_step(nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf), args.steps, args.warmup,
                          R_WAVES, kernel_timing=True, clocks=True)
@@ -398,7 +406,7 @@ def run_ours(args):
 
 
 def clean(v):
-    out = {k: x for k, x in v.items() if k not in ("kernel", "launches", "last", "clocks")}
+    out = {k: x for k, x in v.items() if k not in ("kernel", "kernel_int8", "launches", "last", "clocks")}
     last = v.get("last")
     if last is not None:
         out["gmres_iters"] = int(last[0])
@@ -430,11 +438,12 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "c64 Z (fp32 far pairs, fp64 singular terms), 3xTF32 tensor-core GEMMs, fp64 Arnoldi/residual",
+        "dtype": "c64 Z (fp32 far pairs, fp64 singular terms), 3xTF32 factor/sweeps, int8-slice FP64-accurate Z X, fp64 Arnoldi",
         "data": "synthetic plate mesh and seeded incidences (seed 20260001)",
         "config": {"workload": WORKLOAD, "N_rwg": N, "N_tri": mesh.ntriangles, "incidences": R_WAVES,
                    "quad_order": 3, "gmres_tol": 1e-6,
                    "precond": "complex64 LDL^T of Z (near-field cutoff = inf), right (flexible form)",
+                   "krylov_product": "FP64-accurate INT8-slice Z X on tcgen05 (kind::i8)",
                    "variant": "c3_mixed_batched", "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (Z 912 MB complex64; packed 3xTF32 Z 5.5 GB)"},
         "variants": {k: clean(v) for k, v in variants.items()},
@@ -455,6 +464,16 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                            f"complex MAC), the 3xTF32 split executes 3x that at half the bf16 rate",
             "launches_timed": kl, "kernel_ms_total": kms,
             "kernel_share_of_step": kms / (head["ms_per_step"] * head["steps"])}
+        ims, il, iw = head["kernel_int8"]
+        if il > 0:
+            line["roofline_int8"] = {
+                "kernel": "k_oz_gemm (FP64-accurate Z X from exact int8 slice products, tcgen05 kind::i8)",
+                "bound": "tensor", "achieved": (iw / 1e15) / (ims / 1e3), "peak": 4.5, "unit": "POPS (int8)",
+                "frac": (iw / 1e15) / (ims / 1e3) / 4.5,
+                "peak_source": "nominal dense INT8 (not in MEASURED_PEAKS.json)",
+                "traffic": 17.06e9 if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
+                "launches_timed": il, "kernel_ms_total": ims,
+                "kernel_share_of_step": ims / (head["ms_per_step"] * head["steps"])}
         line["clocks"] = head.get("clocks")
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds)

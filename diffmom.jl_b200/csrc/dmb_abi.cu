@@ -112,6 +112,10 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->pc_valid = false;
       return;
     }
+    if (option == DMB_OPT_EXACT_KRYLOV) {
+      c->exact_krylov = value != 0;
+      return;
+    }
     if (option == DMB_OPT_FAR_TILE) {
       DMB_REQUIRE(value == 0 || value == 8 || value == 16 || value == 32, DMB_ERR_ARGUMENT,
                   "far tile rows must be 0 (autotune), 8, 16 or 32");
@@ -554,18 +558,25 @@ dmb_status dmb_set_kernel_timing(dmb_ctx *c, int enable) {
       c->kt_pool.push_back(e);
     }
     c->kt_enabled = enable != 0;
-    c->kt_ms = 0;
-    c->kt_flops = 0;
-    c->kt_launches = 0;
+    for (int f = 0; f < 2; f++) {
+      c->kt_ms[f] = 0;
+      c->kt_flops[f] = 0;
+      c->kt_launches[f] = 0;
+    }
   });
 }
 
 dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *flops) {
+  return dmb_kernel_timing_family(c, 0, ms, launches, flops);
+}
+
+dmb_status dmb_kernel_timing_family(dmb_ctx *c, int family, double *ms, int64_t *launches, double *work) {
   return guarded(c, [&] {
+    DMB_REQUIRE(family == 0 || family == 1, DMB_ERR_ARGUMENT, "kernel family must be 0 or 1");
     kt_collect(c);
-    if (ms) *ms = c->kt_ms;
-    if (launches) *launches = c->kt_launches;
-    if (flops) *flops = c->kt_flops;
+    if (ms) *ms = c->kt_ms[family];
+    if (launches) *launches = c->kt_launches[family];
+    if (work) *work = c->kt_flops[family];
   });
 }
 

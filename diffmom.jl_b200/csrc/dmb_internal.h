@@ -159,6 +159,7 @@ struct dmb_ctx {
   bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
   int far_tile = 0;              // far-pair tile rows (8/16/32), 0 = autotuned
+  bool exact_krylov = true;      // many-RHS Krylov product on the INT8 slices (FP64-accurate)
   int far_tile_used = 0;         // shape of the last assembly
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
@@ -173,14 +174,15 @@ struct dmb_ctx {
   dmb_timings tm{};
   int64_t launches = 0;
   bool kt_enabled = false;     // dominant-kernel event timing
-  double kt_ms = 0, kt_flops = 0;
-  int64_t kt_launches = 0;
+  double kt_ms[2] = {0, 0}, kt_flops[2] = {0, 0};   // per family: 0 tf32 GEMMs, 1 int8 GEMMs
+  int64_t kt_launches[2] = {0, 0};
   std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
-  std::vector<double> kt_pending;     // algorithmic flops of each recorded launch
+  std::vector<double> kt_pending;     // algorithmic work of each recorded launch
+  std::vector<int> kt_family;         // family of each recorded launch
   size_t kt_used = 0;
 };
 
-// Bracket one launch of the dominant kernel with events from a pre-created
+// Bracket one launch of a timed kernel family with events from a pre-created
 // pool (no host synchronisation inside the timed region).
 inline void kt_begin(dmb_ctx *c) {
   if (!c->kt_enabled) return;
@@ -193,25 +195,29 @@ inline void kt_begin(dmb_ctx *c) {
   }
   DMB_CUDA(cudaEventRecord(c->kt_pool[c->kt_used], c->stream));
 }
-inline void kt_end(dmb_ctx *c, double flops) {
+inline void kt_end(dmb_ctx *c, double work, int family = 0) {
   if (!c->kt_enabled) return;
   DMB_CUDA(cudaEventRecord(c->kt_pool[c->kt_used + 1], c->stream));
   c->kt_used += 2;
-  c->kt_pending.push_back(flops);
+  c->kt_pending.push_back(work);
+  c->kt_family.push_back(family);
 }
-// fold the recorded pairs into the totals (synchronises the stream)
+// fold the recorded pairs into the totals (synchronises the device work)
 inline void kt_collect(dmb_ctx *c) {
   if (c->kt_used == 0) return;
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   for (size_t i = 0; i + 1 < c->kt_used; i += 2) {
     float ms = 0;
+    DMB_CUDA(cudaEventSynchronize(c->kt_pool[i + 1]));
     DMB_CUDA(cudaEventElapsedTime(&ms, c->kt_pool[i], c->kt_pool[i + 1]));
-    c->kt_ms += ms;
-    c->kt_launches++;
-    c->kt_flops += c->kt_pending[i / 2];
+    const int f = c->kt_family[i / 2];
+    c->kt_ms[f] += ms;
+    c->kt_launches[f]++;
+    c->kt_flops[f] += c->kt_pending[i / 2];
   }
   c->kt_used = 0;
   c->kt_pending.clear();
+  c->kt_family.clear();
 }
 
 // Runs the enclosed launches of a context on another stream (the context is

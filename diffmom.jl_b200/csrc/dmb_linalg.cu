@@ -336,14 +336,25 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
 }
 
 // The Krylov operator of the batched solves: complex64 Z with many
-// right-hand sides runs on the tensor cores (3xTF32, FP32 accumulation), so
-// GMRES then verifies convergence with the FP64 residual of matvec_dev.
+// right-hand sides runs on the tensor cores.  Default: 3xTF32 with FP32
+// accumulation in TMEM (2e-5 relative), so GMRES then verifies convergence
+// with the FP64-accurate residual of matvec_dev and refines where needed.
+// With DMB_OPT_EXACT_KRYLOV the operator itself is the FP64-accurate INT8-slice
+// product: the Krylov recurrence then tracks the true residual and no
+// refinement cycle is needed.
+bool krylov_exact_int8(dmb_ctx *c, int64_t nrhs) {
+  return c->exact_krylov && c->z_prec == DMB_PREC_MIXED && nrhs >= 32 && oz_available(c);
+}
+
 bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs) {
-  return c->z_prec == DMB_PREC_MIXED && nrhs >= c->tc_min_rhs && tc_available(c);
+  return !krylov_exact_int8(c, nrhs) && c->z_prec == DMB_PREC_MIXED && nrhs >= c->tc_min_rhs &&
+         tc_available(c);
 }
 
 void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs) {
-  if (matvec_op_inexact(c, nrhs))
+  if (krylov_exact_int8(c, nrhs))
+    oz_zx(c, x, y, nrhs);
+  else if (matvec_op_inexact(c, nrhs))
     tc_zx(c, x, y, nrhs);
   else
     matvec_dev(c, x, y, nrhs);

@@ -429,8 +429,11 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
   sc.n = n;
   sc.ngroups = g;
   dim3 grid((unsigned)(Rpad / OZ_BN), (unsigned)(Mpad / 64));
+  kt_begin(c);
   DMB_LAUNCH(c, k_oz_gemm, grid, 192, OZ_SMEM, st.mapA, st.mapB, sc, (int)(ld / OZ_BK), N, R, Y, N,
              st.rs.as<double>(), st.cs.as<double>(), st.err.as<unsigned>());
+  // int8 work: every kept slice pair is a real (2N x 2N) x (2N x R) product
+  kt_end(c, 2.0 * n * (2.0 * N) * (2.0 * N) * (double)R, 1);
 }
 
 unsigned oz_error_word(dmb_ctx *c) {

@@ -43,6 +43,7 @@ SIDE_RIGHT = 1
 OPT_TENSOR_CORES = 1
 OPT_TC_MIN_RHS = 2
 OPT_FAR_TILE = 3
+OPT_EXACT_KRYLOV = 4
 
 
 class DiffMoMError(RuntimeError):
@@ -123,6 +124,7 @@ SIGNATURES = {
     "dmb_get_timings": ([_P, ctypes.POINTER(Timings)], _I),
     "dmb_set_option": ([_P, _I, _I], _I),
     "dmb_get_far_tile": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
+    "dmb_kernel_timing_family": ([_P, _I, _DP, ctypes.POINTER(ctypes.c_int64), _DP], _I),
     "dmb_batch_create": ([_I, _I, ctypes.POINTER(_P)], _I),
     "dmb_batch_destroy": ([_P], _I),
     "dmb_batch_last_error": ([_P], ctypes.c_char_p),

@@ -85,9 +85,10 @@ class EFIEDevice:
         """Implementation switches: "tensor_cores" (0/1) for the complex64
         factorisation update, "tc_min_rhs" (>= 1) for the right-hand-side count
         from which Z X and the batched near-field solves use the tensor cores,
-        "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles."""
+        "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles,
+        "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
-                 "far_tile": nat.OPT_FAR_TILE}
+                 "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))

@@ -100,6 +100,10 @@ const char *dmb_version(void);
  * rows per 256-pair CTA (8, 16 or 32); 0 (default) lets the autotuner pick it
  * per mesh-size bucket (timed once per process). */
 #define DMB_OPT_FAR_TILE 3
+/* DMB_OPT_EXACT_KRYLOV: 1 (default) runs the many-RHS GMRES operator on the
+ * FP64-accurate INT8-slice product (no refinement cycle needed); 0 runs it in
+ * 3xTF32 with FP64-residual refinement. */
+#define DMB_OPT_EXACT_KRYLOV 4
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair tile rows used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
@@ -133,9 +137,10 @@ dmb_status dmb_apply_impedance(dmb_ctx *ctx, const double *zs);
 
 /* ---- operators --------------------------------------------------------- */
 /* Dense Z*x (the zgemv inside Krylov.gmres) for nrhs column-major
- * right-hand sides: y = Z x.  FP64 accumulation, except for a complex64 Z
- * with nrhs >= DMB_OPT_TC_MIN_RHS: then a tensor-core 3xTF32 GEMM
- * (~1e-6 relative). */
+ * right-hand sides: y = Z x.  FP64 accumulation; for a complex64 Z with many
+ * right-hand sides on the tensor cores: the FP64-accurate INT8-slice product
+ * (nrhs >= 32, DMB_OPT_EXACT_KRYLOV on) or 3xTF32 (nrhs >= DMB_OPT_TC_MIN_RHS,
+ * ~2e-5 relative). */
 dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
 /* Matrix-free Z*x (MatrixFreeEFIEOperator mul!, src/assembly/EFIE.jl:867-909):
  * entries are recomputed from the geometry on every call, nothing of size
@@ -288,6 +293,10 @@ dmb_status dmb_get_stream(dmb_ctx *ctx, void **stream_out);
  * device time, launch count and algorithmic FLOPs. */
 dmb_status dmb_set_kernel_timing(dmb_ctx *ctx, int enable);
 dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double *flops);
+/* Same per kernel family: 0 = tensor-core 3xTF32 GEMMs (work in complex
+ * flops, 8 per complex MAC), 1 = INT8-slice FP64-accurate GEMMs (work in int8
+ * multiply-adds x 2). */
+dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
 
 /* ---- far field --------------------------------------------------------- */
 /* radiation_vectors + compute_farfield (src/postprocessing/FarField.jl:
