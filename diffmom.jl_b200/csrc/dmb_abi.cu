@@ -419,6 +419,43 @@ dmb_status dmb_gmres(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs, dou
   return s;
 }
 
+dmb_status dmb_gmres_adjoint(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs, double tol, int maxiter,
+                             int precond_kind, int precond_side, int check_convergence, dmb_gmres_stats *stats) {
+  dmb_gmres_stats st{};
+  dmb_status s = guarded(c, [&] {
+    DMB_REQUIRE(std::isfinite(tol) && tol > 0, DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive");
+    DMB_REQUIRE(maxiter >= 1, DMB_ERR_ARGUMENT, "GMRES maxiter must be at least 1");
+    DMB_REQUIRE(precond_side == DMB_SIDE_LEFT || precond_side == DMB_SIDE_RIGHT, DMB_ERR_ARGUMENT,
+                "Invalid precond_side (expected :left or :right)");
+    DMB_REQUIRE(precond_kind == DMB_PRECOND_NONE || precond_kind == DMB_PRECOND_NF_LU ||
+                    precond_kind == DMB_PRECOND_NF_DIAG,
+                DMB_ERR_ARGUMENT, "adjoint GMRES takes no preconditioner or a near-field one");
+    DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad GMRES arrays");
+    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
+    const int64_t cnt = c->n * nrhs;
+    size_t bytes = sizeof(double2) * cnt;
+    DevBuf bb, bx;
+    bb.ensure(bytes);
+    bx.ensure(bytes);
+    DMB_CUDA(cudaMemcpyAsync(bb.p, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
+    // Z and the near-field matrix are complex symmetric: Z^H x = b  <=>
+    // Z conj(x) = conj(b), and the adjoint preconditioner is conj(M^-1)
+    dmb::conj_dev(c, bb.as<double2>(), cnt);
+    dmb::gmres_dev(c, bb.as<double>(), bx.as<double>(), nrhs, tol, maxiter, precond_kind, precond_side, &st);
+    dmb::conj_dev(c, bx.as<double2>(), cnt);
+    DMB_CUDA(cudaMemcpyAsync(x, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    if (check_convergence && !st.solved)
+      throw DmbError{DMB_ERR_NOT_CONVERGED,
+                     "adjoint GMRES did not converge consistently: niter=" + std::to_string(st.niter) +
+                         ", final_residual=" + std::to_string(st.residual) +
+                         ", tol=" + std::to_string(tol) + ", maxiter=" + std::to_string(maxiter)};
+  });
+  if (stats) *stats = st;
+  return s;
+}
+
 dmb_status dmb_solve_direct(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs,
                             double *backward_error_out) {
   return guarded(c, [&] {

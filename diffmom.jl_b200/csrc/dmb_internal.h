@@ -240,6 +240,7 @@ void copy_z_out(dmb_ctx *c, double *Z_out);
 void z_entries(dmb_ctx *c, const int64_t *m, const int64_t *n, int64_t count, double *out);
 void apply_impedance(dmb_ctx *c, const double *zs);
 void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs);  // device buffers, c128
+void conj_dev(dmb_ctx *c, double2 *x, int64_t count);
 void nf_build(dmb_ctx *c, double cutoff, int kind);
 void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs);             // in place, c128 device
 void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,

@@ -169,6 +169,11 @@ __global__ void __launch_bounds__(256, 1) k_gemm_zx_wide(int64_t N, int64_t R, c
 // ---------------------------------------------------------------------------
 // Z out / entries / conversions
 // ---------------------------------------------------------------------------
+__global__ void k_conj(int64_t count, double2 *__restrict__ x) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) x[i].y = -x[i].y;
+}
+
 __global__ void k_f2_to_d2(int64_t count, const float2 *__restrict__ a, double2 *__restrict__ b) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < count) b[i] = make_double2(a[i].x, a[i].y);
@@ -333,6 +338,10 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
     dim3 g(blocks_for(N, 128), blocks_for(nrhs, 64));
     DMB_LAUNCH(c, k_gemm_zx_wide<float2>, g, 256, 0, N, nrhs, c->d_Z.as<float2>(), xd, yd);
   }
+}
+
+void conj_dev(dmb_ctx *c, double2 *x, int64_t count) {
+  DMB_LAUNCH(c, k_conj, blocks_for(count, 256), 256, 0, count, x);
 }
 
 // The Krylov operator of the batched solves: complex64 Z with many

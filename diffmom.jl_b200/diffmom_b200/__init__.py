@@ -10,6 +10,7 @@ from .rwg import RWGData, build_rwg, rwg_centers, basis_triangles
 from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixFreeEFIEOperator,
                   PlaneWaveExcitation, make_plane_wave, assemble_plane_wave, assemble_excitation,
                   assemble_multiple_excitations, build_nearfield_preconditioner, NearFieldOperator,
+                  NearFieldAdjointOperator, solve_gmres_adjoint,
                   solve_gmres, solve_forward, solve_scattering, ScatteringResult, SphGrid,
                   monostatic_rcs_sweep, MonostaticResult, BatchSurface, BatchResult,
                   SurfaceBatch, solve_surfaces,

@@ -269,7 +269,8 @@ class EFIEDevice:
 
     # -- solvers ----------------------------------------------------------
     def gmres(self, rhs, tol=1e-8, maxiter=200, preconditioner=None, precond_side="left",
-              check_gmres_convergence=True):
+              check_gmres_convergence=True, adjoint=False):
+        """GMRES on Z x = rhs (adjoint=True: Z^H x = rhs, IterativeSolve.jl:409)."""
         B = nat.c128(rhs)
         nrhs = 1 if B.ndim == 1 else B.shape[1]
         X = np.empty_like(B)
@@ -278,10 +279,9 @@ class EFIEDevice:
         side = {"left": nat.SIDE_LEFT, "right": nat.SIDE_RIGHT}.get(precond_side)
         if side is None:
             raise ValueError(f"Invalid precond_side: {precond_side} (expected :left or :right)")
-        status = self.ctx.lib.dmb_gmres(self.ctx.h, nat.dptr(B),
-                                        nat.dptr(X), nrhs, float(tol), int(maxiter),
-                                        kind, side, 1 if check_gmres_convergence else 0,
-                                        ctypes.byref(st))
+        fn = self.ctx.lib.dmb_gmres_adjoint if adjoint else self.ctx.lib.dmb_gmres
+        status = fn(self.ctx.h, nat.dptr(B), nat.dptr(X), nrhs, float(tol), int(maxiter), kind, side,
+                    1 if check_gmres_convergence else 0, ctypes.byref(st))
         self.ctx._check(status)
         return X, GmresResult(st.niter, bool(st.solved), st.residual, st.true_residual, st.restarts)
 
@@ -345,6 +345,20 @@ class NearFieldOperator:
 
     def apply(self, x):
         return self.P.device.nf_apply(x)
+
+
+class NearFieldAdjointOperator:
+    """y = (Z_nf^-1)^H x (NearFieldPreconditioner.jl:1237-1290); Z_nf is complex
+    symmetric, so this is conj(Z_nf^-1 conj(x))."""
+
+    def __init__(self, P: NearFieldPreconditionerData):
+        self.P = P
+
+    def __matmul__(self, x):
+        return self.apply(x)
+
+    def apply(self, x):
+        return np.conj(self.P.device.nf_apply(np.conj(nat.c128(x))))
 
 
 # ---------------------------------------------------------------------------
@@ -447,6 +461,14 @@ def solve_gmres(device: EFIEDevice, rhs, preconditioner=None, precond_side="left
                 maxiter=200, check_gmres_convergence=True):
     return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
                         precond_side=precond_side, check_gmres_convergence=check_gmres_convergence)
+
+
+def solve_gmres_adjoint(device: EFIEDevice, rhs, preconditioner=None, precond_side="left", tol=1e-8,
+                        maxiter=200, check_gmres_convergence=True):
+    """IterativeSolve.jl:409-470: GMRES on Z^H x = rhs with the adjoint
+    near-field preconditioner."""
+    return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
+                        precond_side=precond_side, check_gmres_convergence=check_gmres_convergence, adjoint=True)
 
 
 def solve_forward(device: EFIEDevice, v, solver="direct"):

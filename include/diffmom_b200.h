@@ -217,6 +217,13 @@ dmb_status dmb_rhs_plane_waves(dmb_ctx *ctx, const double *kvecs, const double *
 dmb_status dmb_gmres(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs, double tol,
                      int maxiter, int precond_kind, int precond_side, int check_convergence,
                      dmb_gmres_stats *stats);
+/* solve_gmres_adjoint (IterativeSolve.jl:409-470) with NearFieldAdjointOperator
+ * (NearFieldPreconditioner.jl:1237): GMRES on Z^H x = rhs.  Z (and its
+ * near-field matrix) is complex symmetric, so this is the conjugate of the
+ * forward solve with conj(rhs); the near-field preconditioners only (none,
+ * NF_LU, NF_DIAG). */
+dmb_status dmb_gmres_adjoint(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs, double tol, int maxiter,
+                             int precond_kind, int precond_side, int check_convergence, dmb_gmres_stats *stats);
 /* solve_forward(Z, v; solver=:direct) (src/solver/Solve.jl:1342-1382):
  * factorisation of the resident Z plus FP64 iterative refinement. */
 dmb_status dmb_solve_direct(dmb_ctx *ctx, const double *rhs, double *x, int64_t nrhs,
