@@ -362,6 +362,29 @@ dmb_status dmb_net_loss_grad(dmb_ctx *c, const float *feat, const float *tgt, co
   });
 }
 
+dmb_status dmb_rhs_dipoles(dmb_ctx *c, int64_t R, const double *positions, const double *moments,
+                           const int *magnetic, const double *frequencies, int quad_order, double *V_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->have_rwg, DMB_ERR_STATE, "mesh and RWG data must be uploaded first");
+    DMB_REQUIRE(R >= 1 && positions && moments && magnetic && frequencies && V_out, DMB_ERR_ARGUMENT,
+                "bad dipole arrays");
+    check_finite(positions, 3 * R, "dipole positions");
+    check_finite(moments, 6 * R, "dipole moments");
+    for (int64_t r = 0; r < R; r++) {
+      DMB_REQUIRE(magnetic[r] == 0 || magnetic[r] == 1, DMB_ERR_ARGUMENT,
+                  "Dipole type must be :electric or :magnetic");
+      DMB_REQUIRE(std::isfinite(frequencies[r]) && frequencies[r] > 0, DMB_ERR_ARGUMENT,
+                  "dipole frequency must be finite and positive");
+    }
+    const size_t bytes = sizeof(double2) * c->n * R;
+    DevBuf bv;
+    bv.ensure(bytes);
+    dmb::rhs_dipoles_dev(c, R, positions, moments, magnetic, frequencies, quad_order, bv.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(V_out, bv.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 dmb_status dmb_rhs_plane_waves(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
                                int64_t R, int quad_order, double *V_out) {
   return guarded(c, [&] {

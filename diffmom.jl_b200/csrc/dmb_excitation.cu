@@ -51,6 +51,99 @@ __global__ void k_plane_wave(int64_t N, int64_t R, const TriCache *__restrict__ 
   V[idx] = acc;
 }
 
+// Dipole sources (electric or magnetic; a loop is the magnetic dipole of
+// moment I pi a^2 n): field _dipole_incident_field_unchecked
+// (Excitation.jl:2131-2185) at every quadrature point, folded with the RWG
+// basis as assemble_dipole (Excitation.jl:2924-2953).  V (N x R column-major).
+__device__ __forceinline__ double dop(double a, double b, double c, double d) {
+  const double cd = c * d;
+  return fma(a, b, -cd) + fma(-c, d, cd);
+}
+// complex a x real b
+__device__ __forceinline__ void ccross(const double2 *a, const double *b, double2 *o) {
+  o[0] = make_double2(dop(a[1].x, b[2], a[2].x, b[1]), dop(a[1].y, b[2], a[2].y, b[1]));
+  o[1] = make_double2(dop(a[2].x, b[0], a[0].x, b[2]), dop(a[2].y, b[0], a[0].y, b[2]));
+  o[2] = make_double2(dop(a[0].x, b[1], a[1].x, b[0]), dop(a[0].y, b[1], a[1].y, b[0]));
+}
+
+__device__ void dipole_field(const double *r, const double *pos, const double2 *p, int magnetic, double k,
+                             double eta0, double eps0, double2 *E) {
+  double d[3] = {r[0] - pos[0], r[1] - pos[1], r[2] - pos[2]};
+  const double R = hypot(hypot(d[0], d[1]), d[2]);
+  if (R == 0.0) {
+    E[0] = E[1] = E[2] = make_double2(0, 0);
+    return;
+  }
+  // direction rescaled by a power of two (largest component in [1, 2)) as
+  // _source_power_of_two_scaled_direction (Excitation.jl:632-646): the
+  // formulas only use d through d/|d| and d d^T/|d|^2
+  {
+    int e = -1 << 30;
+    for (int i = 0; i < 3; i++)
+      if (d[i] != 0.0) e = max(e, ilogb(d[i]));
+    for (int i = 0; i < 3; i++) d[i] = scalbn(d[i], -e);
+  }
+  const double dn2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  double sn, cs;
+  sincos(-k * R, &sn, &cs);
+  const double2 phase = make_double2(cs, sn);
+  if (!magnetic) {
+    double2 pxd[3], dxp[3], t1[3];
+    ccross(p, d, pxd);
+    for (int i = 0; i < 3; i++) dxp[i] = make_double2(-pxd[i].x, -pxd[i].y);
+    ccross(dxp, d, t1);
+    double2 dp = make_double2(0, 0);
+    for (int i = 0; i < 3; i++) dp = cadd(dp, cscale(p[i], d[i]));
+    const double2 fac = make_double2(1.0 / (R * R), k / R);
+    const double inv = 1.0 / (4.0 * 3.14159265358979323846 * eps0 * R);
+    for (int i = 0; i < 3; i++) {
+      const double2 term1 = cscale(cscale(t1[i], 1.0 / dn2), k * k);
+      const double2 radial = cscale(cscale(dp, d[i]), 1.0 / dn2);
+      const double2 term2 = cmul(csub(cscale(radial, 3.0), p[i]), fac);
+      E[i] = cscale(cmul(cadd(term1, term2), phase), inv);
+    }
+  } else {
+    const double2 rf = make_double2((eta0 / (4.0 * 3.14159265358979323846)) * (k * k / R),
+                                    -(eta0 / (4.0 * 3.14159265358979323846)) * (k / (R * R)));
+    const double2 pf = cmul(rf, phase);
+    double2 ang[3];
+    ccross(p, d, ang);
+    const double nd = sqrt(dn2);
+    for (int i = 0; i < 3; i++) E[i] = cmul(pf, cscale(ang[i], 1.0 / nd));
+  }
+}
+
+__global__ void k_dipole_rhs(int64_t N, int64_t R, const TriCache *__restrict__ tc, const int *__restrict__ rslot,
+                             int nq, const double *__restrict__ wq, const double *__restrict__ pos,
+                             const double *__restrict__ mom, const int *__restrict__ magnetic,
+                             const double *__restrict__ freq, double2 *__restrict__ V) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  const int64_t r = idx / N, n = idx % N;
+  const double eps0 = 8.854187817e-12, mu0 = 4.0 * 3.14159265358979323846 * 1e-7;
+  const double eta0 = sqrt(mu0 / eps0), c0 = 1.0 / sqrt(eps0 * mu0);
+  const double k = (2.0 * 3.14159265358979323846 * freq[r]) / c0;
+  const double2 p[3] = {make_double2(mom[6 * r], mom[6 * r + 1]), make_double2(mom[6 * r + 2], mom[6 * r + 3]),
+                        make_double2(mom[6 * r + 4], mom[6 * r + 5])};
+  double2 acc = make_double2(0, 0);
+  for (int s = 0; s < 2; s++) {
+    const int sl = rslot[2 * n + s];
+    const TriCache &T = tc[sl / 3];
+    const int i = sl % 3;
+    for (int q = 0; q < nq; q++) {
+      const double f0 = T.s[i] * (T.qp[q][0] - T.p[i][0]);
+      const double f1 = T.s[i] * (T.qp[q][1] - T.p[i][1]);
+      const double f2 = T.s[i] * (T.qp[q][2] - T.p[i][2]);
+      double2 E[3];
+      dipole_field(T.qp[q], pos + 3 * r, p, magnetic[r], k, eta0, eps0, E);
+      const double2 ip = cadd(cadd(cscale(E[0], f0), cscale(E[1], f1)), cscale(E[2], f2));
+      const double2 ap = cscale(ip, T.area);
+      acc = cadd(acc, cscale(ap, -(2 * wq[q])));
+    }
+  }
+  V[idx] = acc;
+}
+
 // radiation matrix G (3*NO x N, row-major) for directions rh
 __global__ void k_radiation(int64_t N, int64_t NO, const TriCache *__restrict__ tc, const int *__restrict__ rslot,
                             int nq, const double *__restrict__ wq, const double *__restrict__ rh, double k,
@@ -338,6 +431,26 @@ void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double e
   DMB_LAUNCH(c, k_gemm_rc, g2, 256, 0, 3 * NO, N, nrhs, G.as<double2>(), (const double2 *)I_dev,
              (double2 *)E_dev);
   DMB_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void rhs_dipoles_dev(dmb_ctx *c, int64_t R, const double *pos, const double *moments, const int *magnetic,
+                     const double *freqs, int quad_order, double *V_dev) {
+  double t0 = now_ms();
+  ensure_cache(c, quad_order);
+  DevBuf bp, bm, bt, bf;
+  bp.ensure(24 * R);
+  bm.ensure(48 * R);
+  bt.ensure(4 * R);
+  bf.ensure(8 * R);
+  DMB_CUDA(cudaMemcpyAsync(bp.p, pos, 24 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bm.p, moments, 48 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bt.p, magnetic, 4 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bf.p, freqs, 8 * R, cudaMemcpyHostToDevice, c->stream));
+  DMB_LAUNCH(c, k_dipole_rhs, blocks_for(c->n * R, 128), 128, 0, c->n, R, c->d_tcache.as<TriCache>(),
+             c->d_rwg_slot.as<int>(), c->nq, c->d_wq.as<double>(), bp.as<double>(), bm.as<double>(), bt.as<int>(),
+             bf.as<double>(), (double2 *)V_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  c->tm.rhs_ms = now_ms() - t0;
 }
 
 // monostatic fields of R resident solutions; kv / E0s are the device copies

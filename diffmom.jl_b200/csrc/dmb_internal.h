@@ -245,6 +245,8 @@ void nf_build(dmb_ctx *c, double cutoff, int kind);
 void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs);             // in place, c128 device
 void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
                          int64_t R, int quad_order, double *V_dev);
+void rhs_dipoles_dev(dmb_ctx *c, int64_t R, const double *pos, const double *moments, const int *magnetic,
+                     const double *freqs, int quad_order, double *V_dev);
 void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs, double tol,
                int maxiter, int precond_kind, int precond_side, dmb_gmres_stats *st);
 void solve_direct_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs,

@@ -9,6 +9,8 @@ from .mesh import (TriMesh, make_rect_plate, make_circular_plate, make_icosphere
 from .rwg import RWGData, build_rwg, rwg_centers, basis_triangles
 from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixFreeEFIEOperator,
                   PlaneWaveExcitation, make_plane_wave, assemble_plane_wave, assemble_excitation,
+                  DipoleExcitation, LoopExcitation, make_dipole, make_loop, assemble_dipole,
+                  assemble_loop,
                   assemble_multiple_excitations, build_nearfield_preconditioner, NearFieldOperator,
                   NearFieldAdjointOperator, solve_gmres_adjoint,
                   solve_gmres, solve_forward, solve_scattering, ScatteringResult, SphGrid,

@@ -142,6 +142,7 @@ SIGNATURES = {
     "dmb_nf_apply": ([_P, _DP, _DP, _L], _I),
     "dmb_rhs_plane_waves": ([_P, _DP, _DP, _DP, _L, _I, _DP], _I),
     "dmb_gmres": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
+    "dmb_rhs_dipoles": ([_P, _L, _DP, _DP, _IP, _DP, _I, _DP], _I),
     "dmb_gmres_adjoint": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
     "dmb_solve_direct": ([_P, _DP, _DP, _L, _DP], _I),
     "dmb_farfield": ([_P, _DP, _L, _D, _D, _I, _DP, _L, _DP], _I),
@@ -187,6 +188,12 @@ def dptr(a: np.ndarray):
     if a is None:
         return None
     return a.ctypes.data_as(_DP)
+
+
+def iptr(a: np.ndarray):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_IP)
 
 
 def lptr(a: np.ndarray):

@@ -221,6 +221,28 @@ class EFIEDevice:
                       int(quad_order), nat.dptr(V))
         return V
 
+    def dipole_rhs(self, positions, moments, types, frequencies, quad_order: int = 3) -> np.ndarray:
+        """assemble_dipole (Excitation.jl:2924-2953) for R dipoles at once:
+        positions (R, 3), complex moments (R, 3), types 'electric'/'magnetic'
+        per dipole, frequencies (R,) in Hz.  Returns V (N, R)."""
+        pos = np.ascontiguousarray(np.atleast_2d(positions), dtype=np.float64)
+        mom = np.ascontiguousarray(np.atleast_2d(moments), dtype=np.complex128)
+        R = pos.shape[0]
+        if isinstance(types, str):
+            types = [types] * R
+        codes = {"electric": 0, "magnetic": 1}
+        try:
+            mag = np.ascontiguousarray([codes[str(t).lstrip(":")] for t in types], dtype=np.int32)
+        except KeyError as e:
+            raise ValueError(f"Dipole type must be :electric or :magnetic, got {e.args[0]}") from None
+        fr = np.ascontiguousarray(np.broadcast_to(np.asarray(frequencies, dtype=np.float64), (R,)))
+        if pos.shape != (R, 3) or mom.shape != (R, 3) or mag.shape != (R,):
+            raise ValueError("dipole positions and moments must be (R, 3)")
+        V = np.empty((self.N, R), dtype=np.complex128, order="F")
+        self.ctx.call("dmb_rhs_dipoles", R, nat.dptr(pos), nat.dptr(mom), nat.iptr(mag), nat.dptr(fr),
+                      int(quad_order), nat.dptr(V))
+        return V
+
     # -- batched resident solve -------------------------------------------
     _PC_CODES = {"none": nat.PRECOND_NONE, "lu": nat.PRECOND_NF_LU, "diag": nat.PRECOND_NF_DIAG,
                  "local": nat.PRECOND_LOCAL_INV, "learned": nat.PRECOND_LEARNED}
@@ -432,22 +454,135 @@ def assemble_plane_wave(mesh, rwg, pw: PlaneWaveExcitation, quad_order=3, device
             dev.close()
 
 
-def assemble_excitation(mesh, rwg, excitation, quad_order=3, device=None) -> np.ndarray:
-    if not isinstance(excitation, PlaneWaveExcitation):
-        raise TypeError(f"Unsupported excitation type: {type(excitation).__name__}")
-    return assemble_plane_wave(mesh, rwg, excitation, quad_order=quad_order, device=device)
+@dataclass
+class DipoleExcitation:
+    """Excitation.jl:130-136: electric (C m) or magnetic (A m^2) dipole."""
+    position: np.ndarray
+    moment: np.ndarray
+    orientation: np.ndarray
+    type: str
+    frequency: float
 
 
-def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=None) -> np.ndarray:
+@dataclass
+class LoopExcitation:
+    """Excitation.jl:143-149: small circular loop of current I, radiating as
+    the magnetic dipole I pi a^2 n."""
+    center: np.ndarray
+    normal: np.ndarray
+    radius: float
+    current: complex
+    frequency: float
+
+    def equivalent_moment(self) -> np.ndarray:
+        """_loop_equivalent_moment (Excitation.jl:936-942)."""
+        return complex(self.current) * math.pi * self.radius ** 2 * self.normal.astype(np.complex128)
+
+
+def _finite_vec3(v, what, dtype=np.float64):
+    a = np.asarray(v, dtype=dtype).reshape(3)
+    if not np.all(np.isfinite(a)):
+        raise ValueError(f"{what} must have finite components.")
+    return a
+
+
+def _unit_vec3(v, what):
+    a = _finite_vec3(v, what)
+    n = float(np.linalg.norm(a))
+    if not (math.isfinite(n) and math.isclose(n, 1.0, rel_tol=1e-10, abs_tol=1e-12)):
+        raise ValueError(f"{what} must be a unit vector; norm={n}.")
+    return a
+
+
+def _positive_frequency(f, what):
+    f = float(f)
+    if not (math.isfinite(f) and f > 0.0):
+        raise ValueError(f"{what} frequency must be finite and positive, got {f}.")
+    return f
+
+
+def make_dipole(position, moment, orientation, type, frequency=1e9) -> DipoleExcitation:
+    """Excitation.jl:313-317 with the validation of Excitation.jl:1662-1678."""
+    pos = _finite_vec3(position, "DipoleExcitation position")
+    mom = _finite_vec3(moment, "DipoleExcitation moment", np.complex128)
+    ori = _unit_vec3(orientation, "DipoleExcitation orientation")
+    t = str(type).lstrip(":")
+    if t not in ("electric", "magnetic"):
+        raise ValueError(f"DipoleExcitation type must be :electric or :magnetic, got {type}.")
+    return DipoleExcitation(pos, mom, ori, t, _positive_frequency(frequency, "DipoleExcitation"))
+
+
+def make_loop(center, normal, radius, current, frequency=1e9) -> LoopExcitation:
+    """Excitation.jl:319-323 with the validation of Excitation.jl:1680-1698."""
+    c = _finite_vec3(center, "LoopExcitation center")
+    n = _unit_vec3(normal, "LoopExcitation normal")
+    a = float(radius)
+    if not (math.isfinite(a) and a > 0.0):
+        raise ValueError(f"LoopExcitation radius must be finite and positive, got {radius}.")
+    cur = complex(current)
+    if not (math.isfinite(cur.real) and math.isfinite(cur.imag)):
+        raise ValueError(f"LoopExcitation current must be finite, got {current}.")
+    return LoopExcitation(c, n, a, cur, _positive_frequency(frequency, "LoopExcitation"))
+
+
+def _as_dipole(e):
+    if isinstance(e, LoopExcitation):
+        return e.center, e.equivalent_moment(), "magnetic", e.frequency
+    return e.position, e.moment, e.type, e.frequency
+
+
+def _with_device(mesh, rwg, device, fn):
     dev = device or EFIEDevice(mesh, rwg)
     try:
-        kv = np.stack([e.k_vec for e in excitations])
-        pl = np.stack([e.pol for e in excitations])
-        e0 = np.array([e.E0 for e in excitations])
-        return dev.plane_wave_rhs(kv, e0, pl, quad_order)
+        return fn(dev)
     finally:
         if device is None:
             dev.close()
+
+
+def assemble_dipole(mesh, rwg, dipole: DipoleExcitation, quad_order=3, device=None) -> np.ndarray:
+    """Excitation.jl:2924-2953 on the device."""
+    p, m, t, f = _as_dipole(dipole)
+    return _with_device(mesh, rwg, device, lambda d: d.dipole_rhs(p[None], m[None], [t], [f], quad_order)[:, 0])
+
+
+def assemble_loop(mesh, rwg, loop: LoopExcitation, quad_order=3, device=None) -> np.ndarray:
+    """Excitation.jl:2955-2977: the loop's equivalent magnetic dipole."""
+    return assemble_dipole(mesh, rwg, loop, quad_order=quad_order, device=device)
+
+
+_EXCITATION_TYPES = (PlaneWaveExcitation, DipoleExcitation, LoopExcitation)
+
+
+def assemble_excitation(mesh, rwg, excitation, quad_order=3, device=None) -> np.ndarray:
+    if not isinstance(excitation, _EXCITATION_TYPES):
+        raise TypeError(f"Unsupported excitation type: {type(excitation).__name__}")
+    return assemble_multiple_excitations(mesh, rwg, [excitation], quad_order=quad_order, device=device)[:, 0]
+
+
+def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=None) -> np.ndarray:
+    """One column per excitation; plane waves and dipoles/loops are each
+    assembled in one launch."""
+    excitations = list(excitations)
+    for e in excitations:
+        if not isinstance(e, _EXCITATION_TYPES):
+            raise TypeError(f"Unsupported excitation type: {type(e).__name__}")
+
+    def run(dev):
+        V = np.empty((dev.N, len(excitations)), dtype=np.complex128, order="F")
+        pw = [i for i, e in enumerate(excitations) if isinstance(e, PlaneWaveExcitation)]
+        dp = [i for i, e in enumerate(excitations) if not isinstance(e, PlaneWaveExcitation)]
+        if pw:
+            es = [excitations[i] for i in pw]
+            V[:, pw] = dev.plane_wave_rhs(np.stack([e.k_vec for e in es]), np.array([e.E0 for e in es]),
+                                          np.stack([e.pol for e in es]), quad_order)
+        if dp:
+            src = [_as_dipole(excitations[i]) for i in dp]
+            V[:, dp] = dev.dipole_rhs(np.stack([s[0] for s in src]), np.stack([s[1] for s in src]),
+                                      [s[2] for s in src], np.array([s[3] for s in src]), quad_order)
+        return V
+
+    return _with_device(mesh, rwg, device, run)
 
 
 # ---------------------------------------------------------------------------

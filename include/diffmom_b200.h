@@ -207,6 +207,14 @@ dmb_status dmb_net_loss_grad(dmb_ctx *ctx, const float *feat, const float *tgt, 
  * column-major, E0s: R.  V_out: N x R complex column-major. */
 dmb_status dmb_rhs_plane_waves(dmb_ctx *ctx, const double *kvecs, const double *E0s,
                                const double *pols, int64_t R, int quad_order, double *V_out);
+/* assemble_dipole / assemble_loop (src/assembly/Excitation.jl:2924-2985) for R
+ * sources: positions R x 3, complex moments R x 3 (re, im interleaved: R x 6
+ * doubles), magnetic[r] 0 = electric (C m), 1 = magnetic (A m^2; a loop of
+ * radius a, current I and normal n is the magnetic dipole I pi a^2 n),
+ * frequencies R (Hz; k = 2 pi f sqrt(eps0 mu0) as the reference).  V_out
+ * N x R column-major. */
+dmb_status dmb_rhs_dipoles(dmb_ctx *ctx, int64_t R, const double *positions, const double *moments,
+                           const int *magnetic, const double *frequencies, int quad_order, double *V_out);
 
 /* ---- solvers ----------------------------------------------------------- */
 /* solve_gmres (src/solver/IterativeSolve.jl:341-392): GMRES without

@@ -36,6 +36,7 @@
 
 typedef double _Complex cplx;
 
+static const double ORC_PI = 3.14159265358979323846;
 static const double INV_FOUR_PI = 1.0 / (4.0 * 3.14159265358979323846);
 static long g_fallback_count = 0;
 
@@ -681,6 +682,101 @@ int orc_plane_wave_rhs(const orc_cache *c, const double *kvec, double E0, const 
     }
     v[2 * n] = creal(acc);
     v[2 * n + 1] = cimag(acc);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Dipole / loop sources (Excitation.jl:2017-2170 _dipole_incident_field_ */
+/* unchecked, 2187-2198 loop = magnetic dipole of moment I pi a^2 n,     */
+/* 2924-2985 assemble_dipole / assemble_loop).  The power-of-two scaling  */
+/* of the direction in the reference is exact and omitted; the BigFloat   */
+/* fallback only triggers for non-finite or extreme magnitudes.           */
+/* ------------------------------------------------------------------ */
+static double dop(double a, double b, double c, double d) {  /* a b - c d */
+  double cd = c * d;
+  return fma(a, b, -cd) + fma(-c, d, cd);
+}
+static void ccross_cv(const cplx *a, v3 b, cplx *out) {  /* complex a x real b */
+  out[0] = dop(creal(a[1]), b.z, creal(a[2]), b.y) + I * dop(cimag(a[1]), b.z, cimag(a[2]), b.y);
+  out[1] = dop(creal(a[2]), b.x, creal(a[0]), b.z) + I * dop(cimag(a[2]), b.x, cimag(a[0]), b.z);
+  out[2] = dop(creal(a[0]), b.y, creal(a[1]), b.x) + I * dop(cimag(a[0]), b.y, cimag(a[1]), b.x);
+}
+
+/* E(r) of a dipole at pos with complex moment p (magnetic != 0: magnetic) */
+static void dipole_field(v3 r, v3 pos, const cplx *p, int magnetic, double freq, cplx *E) {
+  const double eps0 = 8.854187817e-12, mu0 = 4.0 * ORC_PI * 1e-7;
+  const double eta0 = sqrt(mu0 / eps0), c0 = 1.0 / sqrt(eps0 * mu0);
+  const double k = (2.0 * ORC_PI * freq) / c0;
+  v3 d = {r.x - pos.x, r.y - pos.y, r.z - pos.z};
+  double R = hypot(hypot(d.x, d.y), d.z);
+  if (R == 0.0) { E[0] = E[1] = E[2] = 0.0; return; }
+  double dn2 = d.x * d.x + d.y * d.y + d.z * d.z;
+  cplx phase = cos(-k * R) + I * sin(-k * R);
+  if (!magnetic) {
+    cplx dxp[3], t1[3];
+    ccross_cv(p, d, dxp);           /* p x d */
+    for (int i = 0; i < 3; i++) dxp[i] = -dxp[i];   /* d x p */
+    ccross_cv(dxp, d, t1);           /* (d x p) x d */
+    cplx dp = d.x * p[0] + d.y * p[1] + d.z * p[2];
+    double dv[3] = {d.x, d.y, d.z};
+    cplx fac = 1.0 / (R * R) + I * k / R;
+    for (int i = 0; i < 3; i++) {
+      cplx term1 = t1[i] / dn2 * (k * k);
+      cplx radial = dv[i] * dp / dn2;
+      cplx term2 = (3.0 * radial - p[i]) * fac;
+      E[i] = (term1 + term2) * phase / (4.0 * ORC_PI * eps0 * R);
+    }
+  } else {
+    cplx rf = (eta0 / (4.0 * ORC_PI)) * (k * k / R - I * k / (R * R));
+    cplx pf = rf * phase;
+    cplx ang[3];
+    ccross_cv(p, d, ang);            /* m x d */
+    double nd = sqrt(dn2);
+    for (int i = 0; i < 3; i++) E[i] = pf * (ang[i] / nd);
+  }
+}
+
+int orc_dipole_rhs(const orc_cache *c, const double *pos, const double *moment, int magnetic, double freq,
+                   double *v) {
+  int64_t N = c->n;
+  int nq = c->nq;
+  v3 ps = {pos[0], pos[1], pos[2]};
+  cplx p[3] = {moment[0] + I * moment[1], moment[2] + I * moment[3], moment[4] + I * moment[5]};
+  for (int64_t n = 0; n < N; n++) {
+    cplx acc = 0.0;
+    for (int s = 0; s < 2; s++) {
+      int64_t t = (s == 0 ? c->tplus[n] : c->tminus[n]) - 1;
+      double A = c->area[t];
+      for (int q = 0; q < nq; q++) {
+        v3 rq = c->qp[t * nq + q];
+        v3 fn = c->fv[(n * 2 + s) * nq + q];
+        cplx E[3];
+        dipole_field(rq, ps, p, magnetic, freq, E);
+        cplx ip = fn.x * E[0] + fn.y * E[1] + fn.z * E[2];
+        cplx ap = A * ip;
+        acc += -(2 * c->wq[q]) * ap;
+      }
+    }
+    v[2 * n] = creal(acc);
+    v[2 * n + 1] = cimag(acc);
+  }
+  return 0;
+}
+
+/* incident field at points r (npts x 3) for the tests */
+int orc_dipole_field(const double *r, int64_t npts, const double *pos, const double *moment, int magnetic,
+                     double freq, double *E) {
+  v3 ps = {pos[0], pos[1], pos[2]};
+  cplx p[3] = {moment[0] + I * moment[1], moment[2] + I * moment[3], moment[4] + I * moment[5]};
+  for (int64_t i = 0; i < npts; i++) {
+    v3 rr = {r[3 * i], r[3 * i + 1], r[3 * i + 2]};
+    cplx e[3];
+    dipole_field(rr, ps, p, magnetic, freq, e);
+    for (int a = 0; a < 3; a++) {
+      E[6 * i + 2 * a] = creal(e[a]);
+      E[6 * i + 2 * a + 1] = cimag(e[a]);
+    }
   }
   return 0;
 }

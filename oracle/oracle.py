@@ -64,6 +64,8 @@ def lib():
         L.orc_assemble_rows.argtypes = [_P, _D, _D, _L, _L, _DP, _I]
         L.orc_efie_entries.argtypes = [_P, _D, _D, _LP, _LP, _L, _DP]
         L.orc_plane_wave_rhs.argtypes = [_P, _DP, _D, _DP, _DP]
+        L.orc_dipole_rhs.argtypes = [_P, _DP, _DP, _I, _D, _DP]
+        L.orc_dipole_field.argtypes = [_DP, _L, _DP, _DP, _I, _D, _DP]
         L.orc_apply_impedance.argtypes = [_P, _DP, _DP]
         L.orc_radiation_vectors.argtypes = [_P, _DP, _L, _D, _D, _DP]
         L.orc_adjacent_pair_count.restype = _L
@@ -183,6 +185,16 @@ class OracleCache:
                                  _d(v))
         return v
 
+    def dipole_rhs(self, position, moment, dipole_type="electric", frequency=1e9) -> np.ndarray:
+        """assemble_dipole (Excitation.jl:2924-2953); loop: magnetic dipole of
+        moment I pi a^2 n (Excitation.jl:936-942, 2187-2198)."""
+        m = np.asarray(moment, dtype=np.complex128)
+        mm = np.ascontiguousarray(np.stack([m.real, m.imag], 1).ravel())
+        v = np.zeros(self.N, dtype=np.complex128)
+        lib().orc_dipole_rhs(self.h, _d(_v3(position)), _d(mm), 1 if dipole_type == "magnetic" else 0,
+                             float(frequency), _d(v))
+        return v
+
     def apply_impedance(self, Z: np.ndarray, zs) -> np.ndarray:
         Zc = np.asfortranarray(Z.copy())
         zsa = np.ascontiguousarray(np.broadcast_to(np.asarray(zs, dtype=np.complex128),
@@ -196,6 +208,17 @@ class OracleCache:
         G = np.zeros((3 * NO, self.N), dtype=np.complex128, order="F")
         lib().orc_radiation_vectors(self.h, _d(rh), NO, float(k), float(eta0), _d(G))
         return G
+
+
+def dipole_field(points, position, moment, dipole_type="electric", frequency=1e9) -> np.ndarray:
+    """_dipole_incident_field_unchecked (Excitation.jl:2131-2185) at points (n x 3)."""
+    r = np.ascontiguousarray(np.atleast_2d(points), dtype=np.float64)
+    m = np.asarray(moment, dtype=np.complex128)
+    mm = np.ascontiguousarray(np.stack([m.real, m.imag], 1).ravel())
+    E = np.zeros((r.shape[0], 3), dtype=np.complex128)
+    lib().orc_dipole_field(_d(r), r.shape[0], _d(_v3(position)), _d(mm), 1 if dipole_type == "magnetic" else 0,
+                           float(frequency), _d(E))
+    return E
 
 
 def fallback_count() -> int:
