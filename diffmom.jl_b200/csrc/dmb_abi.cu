@@ -52,8 +52,13 @@ dmb_status dmb_ctx_create(int device, dmb_ctx **out) {
   if (device < 0 || device >= count) return DMB_ERR_ARGUMENT;
   dmb_ctx *c = new dmb_ctx();
   c->device = device;
+  // the context stream runs at the highest priority: during the factorisation
+  // its latency-bound panel chain is scheduled ahead of the lookahead updates
+  // queued on the low-priority second stream
+  int prio_least = 0, prio_greatest = 0;
   if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess) {
     delete c;
     return DMB_ERR_CUDA;
   }

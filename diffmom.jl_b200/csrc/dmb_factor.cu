@@ -137,22 +137,26 @@ __global__ void k_diag_inv(int64_t N, const ZC *__restrict__ Z, const double *__
 // and write Linv = L11^-1 (unit lower, b x b, row-major NB stride).
 //
 // 256 threads as 16 x 16; thread (tx, ty) keeps entries (ty + 16p, tx + 16q),
-// p, q in 0..3, in registers.  Step k broadcasts column k through shared
-// memory; the pivot reciprocal is formed once per step.
+// p, q in 0..3, of the block and of X = L^-1 in registers.  Elimination step k
+// broadcasts column k of the block and row k of X through shared memory and
+// applies both updates: L = L_0 L_1 ... with L_k = I + l_k e_k^T, so
+// X = ... (I - l_1 e_1^T)(I - l_0 e_0^T), and row k of X is final once steps
+// 0..k-1 have run.  One barrier pair per step covers both.
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
                                                    C *__restrict__ Linv, unsigned *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C(*A)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
-  C *colk = reinterpret_cast<C *>(smem_raw + sizeof(C) * NB * (NB + 1));
+  C *colk = reinterpret_cast<C *>(smem_raw);
+  C *rowk = colk + NB;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  C a[4][4];
+  C a[4][4], x[4][4];
 #pragma unroll
   for (int p = 0; p < 4; p++)
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       int i = ty + 16 * p, c = tx + 16 * q;
       a[p][q] = (i < b && c <= i) ? F[(j + i) * N + j + c] : czero<C>();
+      x[p][q] = (i == c) ? cone<C>() : czero<C>();
     }
   for (int k = 0; k < b; k++) {
     const int kq = k >> 4;
@@ -163,6 +167,13 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
         for (int q = 0; q < 4; q++)
           if (q == kq) colk[ty + 16 * p] = a[p][q];
     }
+    if (ty == (k & 15)) {
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (p == kq) rowk[tx + 16 * q] = x[p][q];
+    }
     __syncthreads();
     const C d = colk[k];
     const double ad = (double)cabsv(d);
@@ -171,63 +182,35 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
       return;  // uniform: every thread read the same pivot
     }
     const C inv_d = cdiv(cone<C>(), d);
-    C l[4];
+    C l[4], xr[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) l[q] = cmul(colk[tx + 16 * q], inv_d);
+    for (int q = 0; q < 4; q++) {
+      l[q] = cmul(colk[tx + 16 * q], inv_d);
+      xr[q] = rowk[tx + 16 * q];
+    }
 #pragma unroll
     for (int p = 0; p < 4; p++) {
       const int i = ty + 16 * p;
       const C ci = colk[i];
+      const C lik = cmul(ci, inv_d);
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const int c = tx + 16 * q;
         if (c > k && c <= i) a[p][q] = csub(a[p][q], cmul(ci, l[q]));
-        if (c == k && i > k) a[p][q] = cmul(ci, inv_d);  // L entry of column k
+        if (c == k && i > k) a[p][q] = lik;  // L entry of column k
+        if (i > k) x[p][q] = csub(x[p][q], cmul(lik, xr[q]));
       }
     }
     __syncthreads();
   }
-  // write L (strict lower) and D back; keep L in shared memory for the inverse
 #pragma unroll
   for (int p = 0; p < 4; p++)
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       int i = ty + 16 * p, c = tx + 16 * q;
       if (i < b && c <= i) F[(j + i) * N + j + c] = a[p][q];
-      A[i][c] = (i < b && c < i) ? a[p][q] : czero<C>();
+      Linv[i * NB + c] = x[p][q];
     }
-  __syncthreads();
-  // Linv = L^-1 (unit lower): X = I; for k: X[i][:] -= L[i][k] X[k][:], i > k
-  C x[4][4];
-#pragma unroll
-  for (int p = 0; p < 4; p++)
-#pragma unroll
-    for (int q = 0; q < 4; q++) x[p][q] = (ty + 16 * p == tx + 16 * q) ? cone<C>() : czero<C>();
-  for (int k = 0; k < b; k++) {
-    const int kp = k >> 4;
-    if (ty == (k & 15)) {
-#pragma unroll
-      for (int p = 0; p < 4; p++)
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          if (p == kp) colk[tx + 16 * q] = x[p][q];  // row k of X
-    }
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      const int i = ty + 16 * p;
-      if (i > k) {
-        const C lik = A[i][k];
-#pragma unroll
-        for (int q = 0; q < 4; q++) x[p][q] = csub(x[p][q], cmul(lik, colk[tx + 16 * q]));
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int p = 0; p < 4; p++)
-#pragma unroll
-    for (int q = 0; q < 4; q++) Linv[(ty + 16 * p) * NB + tx + 16 * q] = x[p][q];
 }
 
 // Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
@@ -516,7 +499,7 @@ __global__ void k_scale_vec(int64_t N, int64_t R, const double2 *__restrict__ d,
 template <class C> void set_smem_attrs() {
   static bool done = false;
   if (done) return;
-  size_t diag = sizeof(C) * (NB * (NB + 1) + NB);
+  size_t diag = sizeof(C) * 2 * NB;
   size_t panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_diag<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag));
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
@@ -551,13 +534,17 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   c->d_W.ensure(sizeof(C) * N * NBW * 2);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   c->d_flags.ensure(64);
-  if (!c->stream2) DMB_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+  if (!c->stream2) {
+    int least = 0, greatest = 0;
+    DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
+  }
   for (auto &e : c->la_ev)
     if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   unsigned *err = c->d_flags.as<unsigned>();
   C *Linv = c->d_dinv.as<C>();
   DMB_CUDA(cudaMemsetAsync(err, 0, 4, c->stream));
-  const size_t sm_diag = sizeof(C) * (NB * (NB + 1) + NB);
+  const size_t sm_diag = sizeof(C) * 2 * NB;
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
   // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
