@@ -188,16 +188,25 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
       l[q] = cmul(colk[tx + 16 * q], inv_d);
       xr[q] = rowk[tx + 16 * q];
     }
+    // warp-uniform skips: row blocks entirely at or above k, column blocks of
+    // the block entirely left of k, and columns of X right of k (row k of X
+    // is zero there) hold nothing to update
 #pragma unroll
     for (int p = 0; p < 4; p++) {
+      if (16 * p + 15 <= k) continue;
       const int i = ty + 16 * p;
       const C ci = colk[i];
       const C lik = cmul(ci, inv_d);
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
+      for (int q = 0; q <= p; q++) {
+        if (16 * q + 15 < k) continue;
         const int c = tx + 16 * q;
         if (c > k && c <= i) a[p][q] = csub(a[p][q], cmul(ci, l[q]));
         if (c == k && i > k) a[p][q] = lik;  // L entry of column k
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (16 * q > k) continue;
         if (i > k) x[p][q] = csub(x[p][q], cmul(lik, xr[q]));
       }
     }
@@ -232,15 +241,26 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b,
   }
   if (threadIdx.x < b) dg[threadIdx.x] = F[(j + threadIdx.x) * N + j + threadIdx.x];
   __syncthreads();
-  int c = threadIdx.x & 63, rq = threadIdx.x >> 6;
+  // thread (c, rq) owns column c of rows rq, rq + 4, ..., rq + 60: sixteen
+  // independent accumulators per Linv entry
+  const int c = threadIdx.x & 63, rq = threadIdx.x >> 6;
   if (c >= b) return;
-  for (int rr = rq; rr < NB; rr += 4) {
-    int64_t r = r0 + rr;
-    if (r >= N) break;
-    C acc = czero<C>();
-    for (int k = 0; k <= c; k++) cfma(acc, As[rr][k], Li[c][k]);
-    W[r * wstride + woff + c] = acc;
-    F[r * N + j + c] = cdiv(acc, dg[c]);
+  C acc[16];
+#pragma unroll
+  for (int t = 0; t < 16; t++) acc[t] = czero<C>();
+  for (int k = 0; k <= c; k++) {
+    const C lk = Li[c][k];
+#pragma unroll
+    for (int t = 0; t < 16; t++) cfma(acc[t], As[rq + 4 * t][k], lk);
+  }
+  const C inv = cdiv(cone<C>(), dg[c]);
+#pragma unroll
+  for (int t = 0; t < 16; t++) {
+    const int64_t r = r0 + rq + 4 * t;
+    if (r < N) {
+      W[r * wstride + woff + c] = acc[t];
+      F[r * N + j + c] = cmul(acc[t], inv);
+    }
   }
 }
 
