@@ -15,7 +15,9 @@
 //                      L21 = (L21 D1) D1^-1, rows in parallel;
 //       k_ldlt_update  trailing update A22 -= (L21 D1) L21^T on lower tiles
 //                      (FP64 SIMT for complex128 factors, FP32 SIMT or the
-//                      tensor-core kernel for complex64 factors).
+//                      tensor-core kernel for complex64 factors); inside a
+//                      256-wide panel its first CTA then factors the next
+//                      diagonal block, so that block needs no launch of its own.
 //     A zero or non-finite pivot stops with DMB_ERR_BREAKDOWN.
 //   * apply (NearFieldOperator, :1034-1054): L y = x, z = y / D, L^T x = z as
 //     one kernel per sweep.  Each CTA draws a ticket (block row, launch order),
@@ -143,10 +145,8 @@ __global__ void k_diag_inv(int64_t N, const ZC *__restrict__ Z, const double *__
 // X = ... (I - l_1 e_1^T)(I - l_0 e_0^T), and row k of X is final once steps
 // 0..k-1 have run.  One barrier pair per step covers both.
 template <class C>
-__global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
-                                                   C *__restrict__ Linv, unsigned *__restrict__ err) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *colk = reinterpret_cast<C *>(smem_raw);
+__device__ __forceinline__ void ldlt_diag_block(int64_t N, int64_t j, int b, C *__restrict__ F,
+                                                C *__restrict__ Linv, unsigned *__restrict__ err, C *colk) {
   C *rowk = colk + NB;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   C a[4][4], x[4][4];
@@ -222,6 +222,13 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
     }
 }
 
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
+                                                   C *__restrict__ Linv, unsigned *__restrict__ err) {
+  __shared__ C colk[2 * NB];
+  ldlt_diag_block<C>(N, j, b, F, Linv, err, colk);
+}
+
 // Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
 // then L21 = W D^-1.  64 rows per CTA.
 template <class C>
@@ -267,10 +274,15 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b,
 // C[r][c] -= sum_{k<K} W[r][woff+k] F[c][jcol+k]  for c in [r_lo, c_hi), r >= c,
 // r < N (SIMT, 64 x 64 tiles; grid.x row tiles, grid.y column tiles; tiles
 // entirely above the diagonal exit at once)
+//
+// diag_b > 0: the CTA of tile (0, 0) -- the diagonal block at r_lo, which is
+// the next panel's -- factors that block right after updating it
+// (ldlt_diag_block, Linv_next), while the other CTAs finish the strip.
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, int64_t c_hi, int64_t jcol, int K,
                                                      C *__restrict__ F, const C *__restrict__ W, int wstride,
-                                                     int woff) {
+                                                     int woff, int diag_b, C *__restrict__ Linv_next,
+                                                     unsigned *__restrict__ err) {
   __shared__ C Ws[16][65];
   __shared__ C Ls[16][65];
   const int64_t r0 = r_lo + (int64_t)blockIdx.x * 64, c0 = r_lo + (int64_t)blockIdx.y * 64;
@@ -314,6 +326,10 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, in
         *p = csub(*p, acc[i][jj]);
       }
     }
+  if (diag_b > 0 && blockIdx.x == 0 && blockIdx.y == 0) {
+    __syncthreads();  // the tile's writes are visible to the whole CTA
+    ldlt_diag_block<C>(N, r_lo, diag_b, F, Linv_next, err, &Ws[0][0]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -519,9 +535,7 @@ __global__ void k_scale_vec(int64_t N, int64_t R, const double2 *__restrict__ d,
 template <class C> void set_smem_attrs() {
   static bool done = false;
   if (done) return;
-  size_t diag = sizeof(C) * 2 * NB;
   size_t panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
-  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_diag<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag));
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * sizeof(C) * NB * NB)));
@@ -564,7 +578,6 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   unsigned *err = c->d_flags.as<unsigned>();
   C *Linv = c->d_dinv.as<C>();
   DMB_CUDA(cudaMemsetAsync(err, 0, 4, c->stream));
-  const size_t sm_diag = sizeof(C) * 2 * NB;
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
   // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
@@ -577,7 +590,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
       dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)Wb, NBW, woff);
     } else {
       dim3 g(blocks_for(rest, 64), blocks_for(c_hi - r0, 64));
-      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, Wb, NBW, woff);
+      DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, Wb, NBW, woff, 0, (C *)nullptr, err);
     }
     // algorithmic work: K complex MACs per updated lower-triangle entry
     const double cols = (double)(c_hi - r0), rows = (double)rest;
@@ -611,17 +624,22 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     const int64_t J2E = std::min<int64_t>(N, J2 + NBW);
     for (int64_t J = J2; J < J2E; J += NBO) {
       const int64_t JE = std::min<int64_t>(J2E, J + NBO);
+      bool diag_done = false;  // the previous strip update factored this block
       for (int64_t j = J; j < JE; j += NB) {
         const int b = (int)std::min<int64_t>(NB, N - j);
         C *Lblk = Linv + (j / NB) * NB * NB;
-        DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, sm_diag, N, j, b, F, Lblk, err);
+        if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, 0, N, j, b, F, Lblk, err);
+        diag_done = false;
         const int64_t rest = N - j - b;
         if (rest <= 0) break;
         DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, Wb, NBW,
                    (int)(j - J2));
-        if (j + b < JE) {  // strip update inside the middle panel
+        if (j + b < JE) {  // strip update inside the middle panel, fused with the next diagonal block
+          const int nb_next = (int)std::min<int64_t>(NB, N - (j + b));
           dim3 g(blocks_for(rest, 64), blocks_for(JE - (j + b), 64));
-          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, Wb, NBW, (int)(j - J2));
+          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, Wb, NBW, (int)(j - J2), nb_next,
+                     Lblk + NB * NB, err);
+          diag_done = true;
         }
       }
       update_split(JE, J2E, J, (int)(JE - J), Wb, (int)(J - J2));  // rest of the block column
