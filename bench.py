@@ -201,7 +201,7 @@ class Runner:
         if clk:
             res["clocks"] = clk.stop()
         if kernel_timing:
-            for fam, key in ((0, "kernel"), (1, "kernel_int8")):
+            for fam, key in ((0, "kernel_gemm"), (1, "kernel_int8"), (2, "kernel_factor")):
                 kms, kl, kf = ct.c_double(), ct.c_int64(), ct.c_double()
                 dev.ctx.call("dmb_kernel_timing_family", fam, ct.byref(kms), ct.byref(kl), ct.byref(kf))
                 res[key] = (kms.value, kl.value, kf.value)
@@ -406,7 +406,8 @@ def run_ours(args):
 
 
 def clean(v):
-    out = {k: x for k, x in v.items() if k not in ("kernel", "kernel_int8", "launches", "last", "clocks")}
+    out = {k: x for k, x in v.items()
+           if k not in ("kernel_gemm", "kernel_int8", "kernel_factor", "launches", "last", "clocks")}
     last = v.get("last")
     if last is not None:
         out["gmres_iters"] = int(last[0])
@@ -452,7 +453,11 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         "gpu_launches": int(head["launches"]) if head else 0,
     }
     if head is not None:
-        kms, kl, kf = head["kernel"]
+        fams = {"k_tc_gemm (Krylov / triangular-sweep GEMMs)": head["kernel_gemm"],
+                "k_tc_syrk + k_tc_pack (factorisation trailing updates)": head["kernel_factor"]}
+        kms = sum(f[0] for f in fams.values())
+        kl = sum(f[1] for f in fams.values())
+        kf = sum(f[2] for f in fams.values())
         achieved = (kf / 1e12) / (kms / 1e3) if kms > 0 else 0.0
         line["roofline"] = {
             "kernel": "k_tc_gemm + k_tc_syrk (tcgen05 3xTF32 complex GEMMs: Z X, panel and factor updates)",
@@ -463,7 +468,11 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
             "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic complex flops (8 per "
                            f"complex MAC), the 3xTF32 split executes 3x that at half the bf16 rate",
             "launches_timed": kl, "kernel_ms_total": kms,
-            "kernel_share_of_step": kms / (head["ms_per_step"] * head["steps"])}
+            "kernel_share_of_step": kms / (head["ms_per_step"] * head["steps"]),
+            "families": {name: {"achieved": (f[2] / 1e12) / (f[0] / 1e3) if f[0] > 0 else 0.0,
+                                "frac": (f[2] / 1e12) / (f[0] / 1e3) / bf16 if f[0] > 0 and bf16 else None,
+                                "launches_timed": f[1], "kernel_ms_total": f[0]}
+                         for name, f in fams.items()}}
         ims, il, iw = head["kernel_int8"]
         if il > 0:
             line["roofline_int8"] = {

@@ -623,7 +623,7 @@ dmb_status dmb_set_kernel_timing(dmb_ctx *c, int enable) {
       c->kt_pool.push_back(e);
     }
     c->kt_enabled = enable != 0;
-    for (int f = 0; f < 2; f++) {
+    for (int f = 0; f < dmb_ctx::KT_FAMILIES; f++) {
       c->kt_ms[f] = 0;
       c->kt_flops[f] = 0;
       c->kt_launches[f] = 0;
@@ -637,7 +637,7 @@ dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *
 
 dmb_status dmb_kernel_timing_family(dmb_ctx *c, int family, double *ms, int64_t *launches, double *work) {
   return guarded(c, [&] {
-    DMB_REQUIRE(family == 0 || family == 1, DMB_ERR_ARGUMENT, "kernel family must be 0 or 1");
+    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1 or 2");
     kt_collect(c);
     if (ms) *ms = c->kt_ms[family];
     if (launches) *launches = c->kt_launches[family];

@@ -230,23 +230,22 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
 }
 
 // Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
-// then L21 = W D^-1.  64 rows per CTA.
+// then L21 = W D^-1, for the 64 rows from r0.  Reads go through L2 (the
+// fused step kernel reads blocks written by another CTA of the same launch).
 template <class C>
-__global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b, C *__restrict__ F,
-                                                    const C *__restrict__ Linv, C *__restrict__ W, int wstride,
-                                                    int woff) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void ldlt_panel_rows(int64_t N, int64_t j, int b, int64_t r0, C *__restrict__ F,
+                                                const C *__restrict__ Linv, C *__restrict__ W, int wstride,
+                                                int woff, unsigned char *smem_raw) {
   C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
   C(*Li)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw + sizeof(C) * NB * (NB + 1));
   C *dg = reinterpret_cast<C *>(smem_raw + 2 * sizeof(C) * NB * (NB + 1));
-  int64_t r0 = j + b + (int64_t)blockIdx.x * NB;
   for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
     int rr = e / NB, k = e % NB;
     int64_t r = r0 + rr;
-    As[rr][k] = (r < N && k < b) ? F[r * N + j + k] : czero<C>();
-    Li[rr][k] = Linv[rr * NB + k];
+    As[rr][k] = (r < N && k < b) ? __ldcg(F + r * N + j + k) : czero<C>();
+    Li[rr][k] = __ldcg(Linv + rr * NB + k);
   }
-  if (threadIdx.x < b) dg[threadIdx.x] = F[(j + threadIdx.x) * N + j + threadIdx.x];
+  if (threadIdx.x < b) dg[threadIdx.x] = __ldcg(F + (j + threadIdx.x) * N + j + threadIdx.x);
   __syncthreads();
   // thread (c, rq) owns column c of rows rq, rq + 4, ..., rq + 60: sixteen
   // independent accumulators per Linv entry
@@ -271,22 +270,20 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b,
   }
 }
 
-// C[r][c] -= sum_{k<K} W[r][woff+k] F[c][jcol+k]  for c in [r_lo, c_hi), r >= c,
-// r < N (SIMT, 64 x 64 tiles; grid.x row tiles, grid.y column tiles; tiles
-// entirely above the diagonal exit at once)
-//
-// diag_b > 0: the CTA of tile (0, 0) -- the diagonal block at r_lo, which is
-// the next panel's -- factors that block right after updating it
-// (ldlt_diag_block, Linv_next), while the other CTAs finish the strip.
 template <class C>
-__global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, int64_t c_hi, int64_t jcol, int K,
-                                                     C *__restrict__ F, const C *__restrict__ W, int wstride,
-                                                     int woff, int diag_b, C *__restrict__ Linv_next,
-                                                     unsigned *__restrict__ err) {
-  __shared__ C Ws[16][65];
-  __shared__ C Ls[16][65];
-  const int64_t r0 = r_lo + (int64_t)blockIdx.x * 64, c0 = r_lo + (int64_t)blockIdx.y * 64;
-  if (r0 >= N || c0 >= c_hi || c0 > r0 + 63) return;
+__global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b, C *__restrict__ F,
+                                                    const C *__restrict__ Linv, C *__restrict__ W, int wstride,
+                                                    int woff) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ldlt_panel_rows<C>(N, j, b, j + b + (int64_t)blockIdx.x * NB, F, Linv, W, wstride, woff, smem_raw);
+}
+
+// F[r][c] -= sum_{k<K} W[r][woff+k] F[c][jcol+k] on the 64 x 64 tile at
+// (r0, c0), c < c_hi, r >= c, r < N (SIMT; Ws / Ls: 2 x 16 x 65 staging)
+template <class C>
+__device__ __forceinline__ void ldlt_tile_update(int64_t N, int64_t r0, int64_t c0, int64_t c_hi, int64_t jcol,
+                                                 int K, C *__restrict__ F, const C *__restrict__ W, int wstride,
+                                                 int woff, C (*Ws)[65], C (*Ls)[65]) {
   int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   C acc[4][4];
 #pragma unroll
@@ -326,10 +323,82 @@ __global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, in
         *p = csub(*p, acc[i][jj]);
       }
     }
+}
+
+// Trailing / strip update on tiles (grid.x row tiles, grid.y column tiles from
+// r_lo; tiles entirely above the diagonal exit at once).
+//
+// diag_b > 0: the CTA of tile (0, 0) -- the diagonal block at r_lo, which is
+// the next panel's -- factors that block right after updating it
+// (ldlt_diag_block, Linv_next), while the other CTAs finish the strip.
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_update(int64_t N, int64_t r_lo, int64_t c_hi, int64_t jcol, int K,
+                                                     C *__restrict__ F, const C *__restrict__ W, int wstride,
+                                                     int woff, int diag_b, C *__restrict__ Linv_next,
+                                                     unsigned *__restrict__ err) {
+  __shared__ C Ws[16][65];
+  __shared__ C Ls[16][65];
+  const int64_t r0 = r_lo + (int64_t)blockIdx.x * 64, c0 = r_lo + (int64_t)blockIdx.y * 64;
+  if (r0 >= N || c0 >= c_hi || c0 > r0 + 63) return;
+  ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
   if (diag_b > 0 && blockIdx.x == 0 && blockIdx.y == 0) {
     __syncthreads();  // the tile's writes are visible to the whole CTA
     ldlt_diag_block<C>(N, r_lo, diag_b, F, Linv_next, err, &Ws[0][0]);
   }
+}
+
+// One panel step inside a 256-wide middle panel, fused: strip update of the
+// columns [r_lo, c_hi) by the panel at jcol; the CTA holding ticket 0 updates
+// the next diagonal block (tile (0, 0)), factors it and publishes its inverse
+// (sync[1]); every other CTA of column tile 0 then runs the next panel on its
+// own rows (W at woff_next, L21 = W D^-1).  Tickets are drawn in launch order,
+// so the CTA that the others wait for is already running; the wait is bounded
+// (error bit 4 on expiry).
+template <class C>
+__global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int64_t c_hi, int64_t jcol, int K,
+                                                   C *__restrict__ F, C *__restrict__ W, int wstride, int woff,
+                                                   int woff_next, int nb_next, C *__restrict__ Linv_next,
+                                                   unsigned *__restrict__ sync, unsigned *__restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned s_ticket;
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(&sync[0], 1u);
+  __syncthreads();
+  const unsigned t = s_ticket;
+  const int nct = (int)((c_hi - r_lo + 63) / 64);
+  const int64_t rt = t / nct;
+  const int ct = (int)(t % nct);
+  const int64_t r0 = r_lo + rt * 64, c0 = r_lo + (int64_t)ct * 64;
+  if (r0 >= N || c0 > r0 + 63) return;
+  C(*Ws)[65] = reinterpret_cast<C(*)[65]>(smem_raw);
+  C(*Ls)[65] = reinterpret_cast<C(*)[65]>(smem_raw + sizeof(C) * 16 * 65);
+  ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
+  if (t == 0) {
+    __syncthreads();
+    ldlt_diag_block<C>(N, r_lo, nb_next, F, Linv_next, err, reinterpret_cast<C *>(smem_raw));
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
+    return;
+  }
+  if (ct != 0) return;
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    int ok = 1;
+    while (*((volatile unsigned *)&sync[1]) == 0u) {
+      if (++it > SPIN_LIMIT) {
+        atomicOr(err, 4u);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -537,6 +606,7 @@ template <class C> void set_smem_attrs() {
   if (done) return;
   size_t panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
+  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * sizeof(C) * NB * NB)));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_bwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -567,7 +637,8 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   const int nblk = (int)((N + NB - 1) / NB);
   c->d_W.ensure(sizeof(C) * N * NBW * 2);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
-  c->d_flags.ensure(64);
+  // err word, then two words (ticket, ready flag) per panel step
+  c->d_flags.ensure(std::max<size_t>(64, 4 * (4 + 2 * (size_t)nblk)));
   if (!c->stream2) {
     int least = 0, greatest = 0;
     DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -577,7 +648,12 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   unsigned *err = c->d_flags.as<unsigned>();
   C *Linv = c->d_dinv.as<C>();
-  DMB_CUDA(cudaMemsetAsync(err, 0, 4, c->stream));
+  unsigned *step_sync = err + 4;
+  DMB_CUDA(cudaMemsetAsync(err, 0, 4 * (4 + 2 * (size_t)nblk), c->stream));
+  // the fused panel step (strip + next diagonal block + next panel) for
+  // complex64 factors; complex128 factors keep separate launches (their
+  // 134 KB panel staging would allow one CTA per SM)
+  const bool fuse_step = std::is_same<C, float2>::value;
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
   // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
@@ -594,7 +670,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     }
     // algorithmic work: K complex MACs per updated lower-triangle entry
     const double cols = (double)(c_hi - r0), rows = (double)rest;
-    kt_end(c, 8.0 * K * (cols * rows - cols * (cols - 1) / 2.0));
+    kt_end(c, 8.0 * K * (cols * rows - cols * (cols - 1) / 2.0), 2);
   };
   bool pending = false;  // the second stream holds an update not yet joined
   auto join = [&] {
@@ -624,21 +700,30 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     const int64_t J2E = std::min<int64_t>(N, J2 + NBW);
     for (int64_t J = J2; J < J2E; J += NBO) {
       const int64_t JE = std::min<int64_t>(J2E, J + NBO);
-      bool diag_done = false;  // the previous strip update factored this block
+      // diag_done / panel_done: the previous step's kernel already factored
+      // this diagonal block / ran this panel
+      bool diag_done = false, panel_done = false;
       for (int64_t j = J; j < JE; j += NB) {
         const int b = (int)std::min<int64_t>(NB, N - j);
         C *Lblk = Linv + (j / NB) * NB * NB;
         if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, 0, N, j, b, F, Lblk, err);
-        diag_done = false;
         const int64_t rest = N - j - b;
         if (rest <= 0) break;
-        DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, Wb, NBW,
-                   (int)(j - J2));
+        if (!panel_done)
+          DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, Wb, NBW,
+                     (int)(j - J2));
+        diag_done = panel_done = false;
         if (j + b < JE) {  // strip update inside the middle panel, fused with the next diagonal block
           const int nb_next = (int)std::min<int64_t>(NB, N - (j + b));
           dim3 g(blocks_for(rest, 64), blocks_for(JE - (j + b), 64));
-          DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, Wb, NBW, (int)(j - J2), nb_next,
-                     Lblk + NB * NB, err);
+          if (fuse_step) {
+            DMB_LAUNCH(c, k_ldlt_step<C>, g.x * g.y, 256, sm_panel, N, j + b, JE, j, b, F, Wb, NBW,
+                       (int)(j - J2), (int)(j + b - J2), nb_next, Lblk + NB * NB, step_sync + 2 * (j / NB), err);
+            panel_done = true;
+          } else {
+            DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, j + b, JE, j, b, F, Wb, NBW, (int)(j - J2), nb_next,
+                       Lblk + NB * NB, err);
+          }
           diag_done = true;
         }
       }
@@ -650,6 +735,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
+  DMB_REQUIRE(!(h_err & 4u), DMB_ERR_TIMEOUT, "factorisation: a panel-step wait expired");
   DMB_REQUIRE(h_err == 0, DMB_ERR_BREAKDOWN, "near-field factorisation broke down: zero or non-finite pivot");
   if (use_tc)
     DMB_REQUIRE(dmb::tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core update: a pipeline wait expired");

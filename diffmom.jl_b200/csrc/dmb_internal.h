@@ -174,8 +174,10 @@ struct dmb_ctx {
   dmb_timings tm{};
   int64_t launches = 0;
   bool kt_enabled = false;     // dominant-kernel event timing
-  double kt_ms[2] = {0, 0}, kt_flops[2] = {0, 0};   // per family: 0 tf32 GEMMs, 1 int8 GEMMs
-  int64_t kt_launches[2] = {0, 0};
+  // per family: 0 3xTF32 Krylov / sweep GEMMs, 1 int8 GEMMs, 2 factor updates
+  static constexpr int KT_FAMILIES = 3;
+  double kt_ms[KT_FAMILIES] = {0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0};
+  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0};
   std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
   std::vector<double> kt_pending;     // algorithmic work of each recorded launch
   std::vector<int> kt_family;         // family of each recorded launch

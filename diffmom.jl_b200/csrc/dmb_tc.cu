@@ -46,6 +46,10 @@ constexpr int TC_A_STAGE = TC_BM * TC_BK * 4;  // 16 KB
 constexpr int TC_B_STAGE = TC_BN * TC_BK * 4;  // 32 KB
 constexpr int TC_SMEM = TC_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 /*barriers*/ + 1024 /*align*/;
 constexpr int TC_SMEM_128 = TC_STAGES * (TC_A_STAGE + TC_B_STAGE / 2) + 1024 + 1024;
+// factor-update pipeline depth: 4 stages, one CTA per SM (measured ahead of
+// 2 stages with two co-resident CTAs per SM, 119 vs 113 TFLOP/s)
+constexpr int TC_SYRK_STAGES = 4;
+constexpr int TC_SYRK_SMEM = TC_SYRK_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 + 1024;
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
@@ -108,7 +112,8 @@ __global__ void k_tc_pack(int64_t rest, int64_t ncols, int64_t N, int64_t r0, in
   }
 }
 
-__global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
+template <int STAGES>
+__global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
                                                     int64_t N, int64_t j0, int64_t rest, int64_t c_hi, int nchunks,
                                                     unsigned *err) {
@@ -122,17 +127,17 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char *gbase = smem_raw + (base - raw);
-  const uint32_t sA = base;                                  // TC_STAGES x 16 KB
-  const uint32_t sB = base + TC_STAGES * TC_A_STAGE;         // TC_STAGES x 32 KB
-  const uint32_t sBar = sB + TC_STAGES * TC_B_STAGE;         // full[4], empty[4], done
+  const uint32_t sA = base;                                  // STAGES x 16 KB
+  const uint32_t sB = base + STAGES * TC_A_STAGE;         // STAGES x 32 KB
+  const uint32_t sBar = sB + STAGES * TC_B_STAGE;         // full[4], empty[4], done
   uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
   volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
-  const uint32_t full0 = sBar, empty0 = sBar + 8 * TC_STAGES, done = sBar + 16 * TC_STAGES;
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * STAGES, done = sBar + 16 * STAGES;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < TC_STAGES; s++) {
+    for (int s = 0; s < STAGES; s++) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
@@ -154,8 +159,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
   if (warp == 0 && lane == 0) {
     // TMA producer
     for (int kc = 0; kc < nchunks; kc++) {
-      const int s = kc % TC_STAGES;
-      if (kc >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((kc / TC_STAGES) - 1) & 1, err, abort_flag)) break;
+      const int s = kc % STAGES;
+      if (kc >= STAGES && !mbar_wait(empty0 + 8 * s, ((kc / STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
       tma_load_2d(sA + s * TC_A_STAGE, &tmA, kc * TC_BK, (int)(2 * row0), full0 + 8 * s);
       tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
@@ -164,8 +169,8 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
     // MMA issuer
     bool ok = true;
     for (int kc = 0; kc < nchunks && ok; kc++) {
-      const int s = kc % TC_STAGES;
-      if (!mbar_wait(full0 + 8 * s, (kc / TC_STAGES) & 1, err, abort_flag)) {
+      const int s = kc % STAGES;
+      if (!mbar_wait(full0 + 8 * s, (kc / STAGES) & 1, err, abort_flag)) {
         ok = false;
         break;
       }
@@ -204,20 +209,22 @@ __global__ void __launch_bounds__(128, 1) k_tc_syrk(const __grid_constant__ CUte
 #pragma unroll
       for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
       __syncthreads();
-      // thread -> (complex row r = rr + 4i, column q)
+      // thread -> (complex row r = rr + 4i, column q); all 16 loads are
+      // issued before any store so they are in flight together
       const int q = threadIdx.x & 31, rr = threadIdx.x >> 5;
       const int64_t gc = j0 + col0 + cc * 32 + q;
-#pragma unroll 4
+      float2 cv[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const int64_t gr = j0 + row0 + rr + 4 * i;
+        cv[i] = (gr < N && gc < c_hi && gc <= gr) ? F[gr * N + gc] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
       for (int i = 0; i < 16; i++) {
         const int r = rr + 4 * i;
         const int64_t gr = j0 + row0 + r;
-        if (gr < N && gc < c_hi && gc <= gr) {
-          float2 *p = F + gr * N + gc;
-          float2 cv = *p;
-          cv.x -= E[r * 33 + q];
-          cv.y -= E[(64 + r) * 33 + q];
-          *p = cv;
-        }
+        if (gr < N && gc < c_hi && gc <= gr)
+          F[gr * N + gc] = make_float2(cv[i].x - E[r * 33 + q], cv[i].y - E[(64 + r) * 33 + q]);
       }
       __syncthreads();
     }
@@ -530,7 +537,8 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<TC_SYRK_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TC_SYRK_SMEM));
     st.attr = true;
   }
   const int64_t rest = N - r0, ncols = std::min<int64_t>(c_hi, N) - r0;
@@ -541,7 +549,7 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   DMB_LAUNCH(c, k_tc_pack, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
              N, r0, jcol, K, ld, F, W, wstride, woff, st.A.as<float>(), st.B.as<float>());
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
-  DMB_LAUNCH(c, k_tc_syrk, grid, 128, TC_SMEM, st.mapAK[kslot], st.mapBK[kslot], F, N, r0, rest,
+  DMB_LAUNCH(c, k_tc_syrk<TC_SYRK_STAGES>, grid, 128, TC_SYRK_SMEM, st.mapAK[kslot], st.mapBK[kslot], F, N, r0, rest,
              std::min<int64_t>(c_hi, N), (int)(ld / TC_BK), st.err.as<unsigned>());
 }
 

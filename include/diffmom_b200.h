@@ -308,9 +308,11 @@ dmb_status dmb_get_stream(dmb_ctx *ctx, void **stream_out);
  * device time, launch count and algorithmic FLOPs. */
 dmb_status dmb_set_kernel_timing(dmb_ctx *ctx, int enable);
 dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double *flops);
-/* Same per kernel family: 0 = tensor-core 3xTF32 GEMMs (work in complex
- * flops, 8 per complex MAC), 1 = INT8-slice FP64-accurate GEMMs (work in int8
- * multiply-adds x 2). */
+/* Same per kernel family: 0 = tensor-core 3xTF32 Krylov and triangular-sweep
+ * GEMMs (work in complex flops, 8 per complex MAC), 1 = INT8-slice
+ * FP64-accurate GEMMs (work in int8 multiply-adds x 2), 2 = factorisation
+ * trailing updates (3xTF32 tensor cores for complex64 factors; complex flops).
+ * dmb_kernel_timing reports family 0. */
 dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
 
 /* ---- far field --------------------------------------------------------- */
