@@ -263,9 +263,14 @@ dmb_status dmb_matvec(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
     bx.ensure(bytes);
     by.ensure(bytes);
     DMB_CUDA(cudaMemcpyAsync(bx.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
-    dmb::matvec_op(c, bx.as<double2>(), by.as<double2>(), nrhs);
-    if (dmb::matvec_op_inexact(c, nrhs))
+    // the 3xTF32 operator when it is the Krylov operator, else the
+    // FP64-accurate product (every int8 slice level for many columns)
+    if (dmb::matvec_op_inexact(c, nrhs)) {
+      dmb::matvec_op(c, bx.as<double2>(), by.as<double2>(), nrhs);
       DMB_REQUIRE(dmb::tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core GEMM: a pipeline wait expired");
+    } else {
+      dmb::matvec_dev(c, bx.as<double2>(), by.as<double2>(), nrhs);
+    }
     DMB_CUDA(cudaMemcpyAsync(y, by.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
   });

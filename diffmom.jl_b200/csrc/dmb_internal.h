@@ -272,7 +272,10 @@ unsigned tc_error_word(dmb_ctx *c);
 void tc_release(dmb_ctx *c);
 // FP64-accurate complex64 Z X on the INT8 tensor cores (dmb_ozaki.cu)
 bool oz_available(dmb_ctx *c);
-void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R);
+// lmax: slice-pair levels p + q <= lmax are kept (6: 26 int8 products, ~7e-13
+// normwise; 5: 21 products, ~4e-11 -- enough for the Krylov recurrence)
+constexpr int OZ_LEVELS_RESIDUAL = 6, OZ_LEVELS_KRYLOV = 5;
+void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax = OZ_LEVELS_RESIDUAL);
 unsigned oz_error_word(dmb_ctx *c);
 void oz_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);

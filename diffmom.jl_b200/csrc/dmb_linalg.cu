@@ -345,12 +345,14 @@ void conj_dev(dmb_ctx *c, double2 *x, int64_t count) {
 }
 
 // The Krylov operator of the batched solves: complex64 Z with many
-// right-hand sides runs on the tensor cores.  Default: 3xTF32 with FP32
-// accumulation in TMEM (2e-5 relative), so GMRES then verifies convergence
-// with the FP64-accurate residual of matvec_dev and refines where needed.
-// With DMB_OPT_EXACT_KRYLOV the operator itself is the FP64-accurate INT8-slice
-// product: the Krylov recurrence then tracks the true residual and no
-// refinement cycle is needed.
+// right-hand sides runs on the tensor cores.  Without DMB_OPT_EXACT_KRYLOV:
+// 3xTF32 with FP32 accumulation in TMEM (2e-5 relative), so GMRES then
+// verifies convergence with the FP64-accurate residual of matvec_dev and
+// refines where needed.
+// With DMB_OPT_EXACT_KRYLOV (the default) the operator itself is the INT8-slice
+// product at OZ_LEVELS_KRYLOV (~4e-11 normwise): the Krylov recurrence then
+// tracks the true residual to far below the 1e-6 tolerance and no refinement
+// cycle is needed; the final true residual uses every level.
 bool krylov_exact_int8(dmb_ctx *c, int64_t nrhs) {
   return c->exact_krylov && c->z_prec == DMB_PREC_MIXED && nrhs >= 32 && oz_available(c);
 }
@@ -362,7 +364,7 @@ bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs) {
 
 void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs) {
   if (krylov_exact_int8(c, nrhs))
-    oz_zx(c, x, y, nrhs);
+    oz_zx(c, x, y, nrhs, OZ_LEVELS_KRYLOV);
   else if (matvec_op_inexact(c, nrhs))
     tc_zx(c, x, y, nrhs);
   else

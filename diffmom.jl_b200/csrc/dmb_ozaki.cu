@@ -17,15 +17,17 @@
 //     pairs with p + q <= OZ_LMAX (0-based) are kept, summed in TMEM per level
 //     (as many pairs per drain as int32 allows) and drained into FP64 with the
 //     exact power-of-two weights sigma_m tau_r 2^(-7(L+2)).
-// With OZ_S = 6 and OZ_LMAX = 6 (26 int8 products) the dropped pair terms are
-// below 2^-49 and the slice truncation below 2^-42 of sigma_m tau_r per
-// product term: ~1e-12 relative on EFIE rows (the residuals need ~1e-9).
+// With OZ_S = 6 and all levels up to OZ_LMAX = 6 (26 int8 products) the
+// product is ~7e-13 relative (normwise) on EFIE rows; the Krylov products of
+// GMRES keep levels <= 5 (21 products, ~4e-11), the true residuals all levels.
 //
 // Kernel k_oz_gemm: one CTA per 64 x 256 complex output tile, 6 warps:
 //   warp 4 / lane 0   TMA producer over (pair, K chunk) into a 4-stage ring of
 //                     128-byte-swizzled int8 stages (A 128 x 128 B, B 256 x 128 B);
-//   warp 5 / lane 0   tcgen05.mma.kind::i8 (M 128, N 256, K 32) into a
-//                     256-column s32 TMEM accumulator, one commit per drain;
+//   warp 5 / lane 0   tcgen05.mma.kind::i8 (M 128, N 256, K 32) into two
+//                     256-column s32 TMEM accumulators used in turn (one
+//                     level accumulates while the other drains), one commit
+//                     per drain;
 //   warps 0-3         drain each level: tcgen05.ld, scale, FP64 store / add.
 // Every wait is bounded (error bit, abort flag, TMEM freed); no multicast.
 #include <algorithm>
@@ -97,7 +99,8 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
   volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
   volatile int *epi_ok = reinterpret_cast<volatile int *>(bar_ptr + 18);
-  const uint32_t full0 = sBar, empty0 = sBar + 8 * OZ_STAGES, accf = sBar + 16 * OZ_STAGES, acce = accf + 8;
+  // accf[b] / acce[b]: TMEM accumulator b (of two) full / drained
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * OZ_STAGES, accf0 = sBar + 16 * OZ_STAGES, acce0 = accf0 + 16;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -105,15 +108,17 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(accf, 1);
-    mbar_init(acce, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, 1);
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(const_cast<uint32_t *>(tmem_slot))),
-                 "r"(OZ_BN)
+                 "r"(2 * OZ_BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -141,10 +146,12 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
       int g = 0;
       bool first = true, ok = true;
       for (int i = 0; i < sc.n && ok; i++) {
-        if (first && g > 0 && !mbar_wait(acce, (uint32_t)(g - 1) & 1u, err, abort_flag)) {
+        // group g accumulates in buffer g & 1, free once group g - 2 drained
+        if (first && g >= 2 && !mbar_wait(acce0 + 8 * (g & 1), (uint32_t)((g >> 1) - 1) & 1u, err, abort_flag)) {
           ok = false;
           break;
         }
+        const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
         for (int kc = 0; kc < kchunks; kc++, t++) {
           const int s = (int)(t % OZ_STAGES);
           if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / OZ_STAGES) & 1u, err, abort_flag)) {
@@ -156,13 +163,13 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
           for (int k = 0; k < OZ_BK / 32; k++) {
             const uint64_t ad = sw128_desc(sA + s * OZ_A_STAGE + k * 32);
             const uint64_t bd = sw128_desc(sB + s * OZ_B_STAGE + k * 32);
-            umma_i8(tmem_d, ad, bd, (first && kc == 0 && k == 0) ? 0u : 1u);
+            umma_i8(tmem_acc, ad, bd, (first && kc == 0 && k == 0) ? 0u : 1u);
           }
           umma_commit(empty0 + 8 * s);
         }
         first = false;
         if (ok && sc.close[i]) {
-          umma_commit(accf);
+          umma_commit(accf0 + 8 * (g & 1));
           g++;
           first = true;
         }
@@ -175,7 +182,8 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
     const int64_t gr = row0 + rl;
     const double rsc = gr < M ? rs[gr] : 0.0;
     for (int g = 0; g < sc.ngroups; g++) {
-      const bool got = mbar_wait(accf, (uint32_t)g & 1u, err, abort_flag);
+      const bool got = mbar_wait(accf0 + 8 * (g & 1), (uint32_t)(g >> 1) & 1u, err, abort_flag);
+      const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
       if (threadIdx.x == 0) *epi_ok = 1;
       epi_sync();
       if (!got) *epi_ok = 0;
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
               "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
               "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
               "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-            : "r"(tmem_d + lane_base + (uint32_t)(cc * 32)));
+            : "r"(tmem_acc + lane_base + (uint32_t)(cc * 32)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int row = warp * 32 + lane;
 #pragma unroll
@@ -226,13 +234,13 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       epi_sync();
-      if (threadIdx.x == 0) mbar_arrive(acce);
+      if (threadIdx.x == 0) mbar_arrive(acce0 + 8 * (g & 1));
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(OZ_BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * OZ_BN) : "memory");
 }
 
 // sigma (power of two, max/sigma in [0.5, 1)) of each complex row of Z
@@ -366,7 +374,8 @@ bool oz_available(dmb_ctx *c) {
   return 16129.0 * (double)K < 2147483647.0;
 }
 
-void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
+void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
+  DMB_REQUIRE(lmax >= 0 && lmax <= OZ_LMAX, DMB_ERR_ARGUMENT, "int8 slice levels out of range");
   DMB_REQUIRE(oz_available(c), DMB_ERR_STATE, "int8 tensor-core product unavailable for this matrix");
   OzState &st = oz_state(c);
   const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64), Rpad = round_up(R, OZ_BN);
@@ -406,7 +415,7 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
   const int64_t maxp = (int64_t)(2147483647.0 / (16129.0 * (double)ld));
   OzSched sc{};
   int n = 0, g = 0;
-  for (int L = 0; L <= OZ_LMAX; L++) {
+  for (int L = 0; L <= lmax; L++) {
     int in_group = 0;
     for (int p = 0; p <= L; p++) {
       const int q = L - p;
