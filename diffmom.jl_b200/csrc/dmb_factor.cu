@@ -943,16 +943,107 @@ template <class C> void forward_block(dmb_ctx *c, const C *F, int64_t o0, int64_
   }
 }
 
-__global__ void k_identity_block(int64_t N, int64_t o0, int ow, double2 *__restrict__ X) {
+// Inverses of the 1024-row diagonal blocks of the unit lower factor by
+// recursive doubling from the 64 x 64 block inverses of the factorisation:
+// for consecutive s-blocks A, B inside one outer block,
+//   [A 0; C B]^-1 = [A^-1 0; -B^-1 C A^-1  B^-1],
+// s = 64, 128, 256, 512, all pairs of a level in one launch per product.
+// X (column-major, leading dimension N; outer block o occupies rows o0..o1 and
+// block-local columns 0..o1-o0) receives the inverses.
+
+// X <- the 64-block inverses on the diagonal of every outer block, 0 elsewhere
+__global__ void k_inv_init(int64_t N, const float2 *__restrict__ Linv, double2 *__restrict__ X) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (int64_t)ow * ow) return;
-  const int64_t r = i % ow, col = i / ow;
-  X[col * N + o0 + r] = make_double2(r == col ? 1.0 : 0.0, 0.0);
+  if (i >= N * TP_OUTER) return;
+  const int64_t col = i / N, r = i % N;  // consecutive threads: consecutive rows
+  const int64_t o0 = r - r % TP_OUTER;
+  double2 v = make_double2(0.0, 0.0);
+  if (o0 + col < N && (o0 + col) / NB == r / NB) {
+    const float2 l = Linv[(r / NB) * NB * NB + (r % NB) * NB + (o0 + col) % NB];
+    v = make_double2(l.x, l.y);
+  }
+  X[col * N + r] = v;
+}
+
+// one product of a doubling level; pair slot y of outer block y / ppo covers
+// A = [i0, i0 + s), B = [i0 + s, i0 + s + sb), i0 = o0 + 2 s (y % ppo)
+//   STEP 1: T = F[B, A] (strict lower part of L) x A^-1     (sb x s)
+//   STEP 2: X[B, A] = -B^-1 x T                             (sb x s)
+// 64 x 64 output tiles (grid.x), FP32 SIMT with 16-deep shared stages
+template <int STEP>
+__global__ void __launch_bounds__(256) k_inv_level(int64_t N, int s, const float2 *__restrict__ F,
+                                                   double2 *__restrict__ X, float2 *__restrict__ T) {
+  __shared__ float2 As[16][65];
+  __shared__ float2 Bs[16][65];
+  const int ppo = TP_OUTER / (2 * s);
+  const int64_t o0 = (int64_t)(blockIdx.y / ppo) * TP_OUTER;
+  const int64_t o1 = min(N, o0 + TP_OUTER);
+  const int64_t i0 = o0 + 2 * (int64_t)s * (blockIdx.y % ppo);
+  const int64_t a0 = i0, b0 = i0 + s;
+  if (b0 >= o1) return;  // no B block in this slot
+  const int sb = (int)min((int64_t)s, o1 - b0);
+  const int nt = (s + 63) / 64;
+  const int ti = blockIdx.x / nt, tj = blockIdx.x % nt;
+  if (64 * ti >= sb) return;
+  float2 *Tp = T + (int64_t)blockIdx.y * s * s;  // column-major sb x s, leading dimension s
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+  // STEP 1: k runs over A's columns from the tile's first column (A^-1 is
+  // lower); STEP 2: over B's columns up to the tile's last row (B^-1 is lower)
+  const int k_lo = STEP == 1 ? 64 * tj : 0;
+  const int k_hi = STEP == 1 ? s : min(sb, 64 * ti + 64);
+  for (int k0 = k_lo; k0 < k_hi; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      if (STEP == 1) {
+        const int kk = e & 15, rr = e >> 4;  // k fastest: F rows and X columns are k-contiguous
+        const int k = k0 + kk, i = 64 * ti + rr, j = 64 * tj + rr;
+        As[kk][rr] = (k < k_hi && i < sb) ? F[(b0 + i) * N + a0 + k] : make_float2(0.f, 0.f);
+        const double2 x = (k < k_hi) ? X[(a0 - o0 + j) * N + a0 + k] : make_double2(0.0, 0.0);
+        Bs[kk][rr] = make_float2((float)x.x, (float)x.y);
+      } else {
+        const int rr = e & 63, kk = e >> 6;  // rows fastest for B^-1 (column-major)
+        const int k = k0 + kk, i = 64 * ti + rr;
+        const double2 x = (k < k_hi && i < sb) ? X[(b0 - o0 + k) * N + b0 + i] : make_double2(0.0, 0.0);
+        As[kk][rr] = make_float2((float)x.x, (float)x.y);
+        const int kk2 = e & 15, cc = e >> 4, k2 = k0 + kk2, j = 64 * tj + cc;
+        Bs[kk2][cc] = (k2 < k_hi && j < s) ? Tp[(int64_t)j * s + k2] : make_float2(0.f, 0.f);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      float2 a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) cfma(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int r = 64 * ti + ty + 16 * i, cidx = 64 * tj + tx + 16 * j;
+      if (r >= sb || cidx >= s) continue;
+      if (STEP == 1)
+        Tp[(int64_t)cidx * s + r] = acc[i][j];
+      else
+        X[(a0 - o0 + cidx) * N + b0 + r] = make_double2(-(double)acc[i][j].x, -(double)acc[i][j].y);
+    }
 }
 
 // Pack the complex64 factor for the tensor-core sweeps (once per
 // factorisation): L'' and (L^T)'', and the inverses of the 1024-row diagonal
-// blocks of L, obtained by solving identity blocks with the panel machinery.
+// blocks of L (recursive doubling, k_inv_init / k_inv_level).
 void prepare_packed_factor(dmb_ctx *c, const float2 *F) {
   if (c->f_packed == c->f_version) return;
   const int64_t N = c->n;
@@ -961,12 +1052,19 @@ void prepare_packed_factor(dmb_ctx *c, const float2 *F) {
   c->d_trsm_id.ensure(sizeof(double2) * N * TP_OUTER);
   double2 *Xid = c->d_trsm_id.as<double2>();
   const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
+  // scratch for the products T: (pair slots) x s x s <= nout x 1024 x 256
+  c->d_trsm_t.ensure(sizeof(float2) * nout * TP_OUTER * (TP_OUTER / 4));
+  float2 *T = c->d_trsm_t.as<float2>();
+  DMB_LAUNCH(c, k_inv_init, blocks_for(N * TP_OUTER, 256), 256, 0, N, c->d_dinv.as<float2>(), Xid);
+  for (int s = NB; s < TP_OUTER; s *= 2) {
+    const int nt = (s + 63) / 64;
+    dim3 g((unsigned)(nt * nt), (unsigned)(nout * (TP_OUTER / (2 * s))));
+    DMB_LAUNCH(c, k_inv_level<1>, g, 256, 0, N, s, F, Xid, T);
+    DMB_LAUNCH(c, k_inv_level<2>, g, 256, 0, N, s, F, Xid, T);
+  }
   for (int64_t o = 0; o < nout; o++) {
     const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
-    const int ow = (int)(o1 - o0);
-    DMB_LAUNCH(c, k_identity_block, blocks_for((int64_t)ow * ow, 256), 256, 0, N, o0, ow, Xid);
-    forward_block<float2>(c, F, o0, o1, Xid, ow);
-    dmb::tc_trsm_pack_diag(c, o, Xid + o0, N, ow);
+    dmb::tc_trsm_pack_diag(c, o, Xid + o0, N, (int)(o1 - o0));
   }
   c->f_packed = c->f_version;
 }

@@ -164,7 +164,8 @@ struct dmb_ctx {
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves
-  DevBuf d_trsm_id;              // scratch: identity blocks solved into diagonal-block inverses
+  DevBuf d_trsm_id;              // scratch: inverses of the 1024-row diagonal blocks of L
+  DevBuf d_trsm_t;               // scratch: products of the recursive-doubling levels
   int gm_kcap = 0;              // cached GMRES basis capacity
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;

@@ -36,6 +36,15 @@
 
 typedef double _Complex cplx;
 
+/* threads the OpenMP loops can use (1 for a serial build) */
+int orc_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
 static const double ORC_PI = 3.14159265358979323846;
 static const double INV_FOUR_PI = 1.0 / (4.0 * 3.14159265358979323846);
 static long g_fallback_count = 0;

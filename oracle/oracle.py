@@ -61,6 +61,8 @@ def lib():
         L.orc_cache_build.argtypes = [_DP, _L, _LP, _L, _L, _LP, _LP, _LP, _LP, _DP, _DP, _DP, _I]
         L.orc_cache_free.argtypes = [_P]
         L.orc_assemble_z.argtypes = [_P, _D, _D, _DP, _I]
+        L.orc_max_threads.argtypes = []
+        L.orc_max_threads.restype = ctypes.c_int
         L.orc_assemble_rows.argtypes = [_P, _D, _D, _L, _L, _DP, _I]
         L.orc_efie_entries.argtypes = [_P, _D, _D, _LP, _LP, _L, _DP]
         L.orc_plane_wave_rhs.argtypes = [_P, _DP, _D, _DP, _DP]
@@ -352,3 +354,8 @@ def mie_bistatic_rcs_pec(k, a, k_inc_hat, pol_inc, rhat):
     c_para = ph @ e_par_i
     S1, S2 = mie_s1s2_pec(k * a, mu)
     return 4 * math.pi / k ** 2 * (abs(S1 * c_perp) ** 2 + abs(S2 * c_para) ** 2)
+
+
+def max_threads() -> int:
+    """Threads the oracle's OpenMP loops can use (1 when built serial)."""
+    return int(lib().orc_max_threads())
