@@ -267,6 +267,14 @@ def run_ours(args):
                          R_WAVES, kernel_timing=True, clocks=True)
         sig_mixed = sig.copy()
         variants["c3_mixed_batched"] = head
+    if want("c3_mixed_precond_tf32x1") and (not args.quick or (only and "c3_mixed_precond_tf32x1" in only)):
+        # the same job with the preconditioner's tensor-core work in 1xTF32
+        dev.set_option("precond_tf32_terms", 1)
+        v = run.timed(dev, c3_step(nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf), args.steps, args.warmup, R_WAVES)
+        dev.set_option("precond_tf32_terms", 3)
+        if sig_mixed is not None:
+            v["rcs_rel_err_vs_mixed"] = float(np.max(np.abs(sig_mixed - sig)) / np.max(sig_mixed))
+        variants["c3_mixed_precond_tf32x1"] = v
     if want("c3_fp64_plain") and not args.quick:
         v = run.timed(dev, c3_step(nat.PREC_FP64, nat.PRECOND_NF_LU, 1.0 * LAM), 1, 1, R_WAVES)
         if sig_mixed is not None:

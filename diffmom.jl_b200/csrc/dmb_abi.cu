@@ -93,6 +93,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     dmb::local_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->stream3) cudaStreamDestroy(c->stream3);
     for (auto &e : c->la_ev)
       if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
@@ -126,6 +127,12 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       DMB_REQUIRE(value == 0 || value == 8 || value == 16 || value == 32, DMB_ERR_ARGUMENT,
                   "far tile rows must be 0 (autotune), 8, 16 or 32");
       c->far_tile = value;
+      return;
+    }
+    if (option == DMB_OPT_PRECOND_TF32_TERMS) {
+      DMB_REQUIRE(value == 1 || value == 3, DMB_ERR_ARGUMENT, "TF32 products per complex64 factor MAC must be 1 or 3");
+      c->precond_tf32_terms = value;
+      c->pc_valid = false;
       return;
     }
     if (option == DMB_OPT_TC_MIN_RHS) {

@@ -35,7 +35,7 @@
 
 namespace dmb {
 void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t jcol, int K, float2 *F,
-                        const float2 *W, int wstride, int woff);
+                        const float2 *W, int wstride, int woff, int slot);
 }  // namespace dmb
 
 namespace {
@@ -222,11 +222,162 @@ __device__ __forceinline__ void ldlt_diag_block(int64_t N, int64_t j, int b, C *
     }
 }
 
+// Blocked form of ldlt_diag_block for complex64 blocks (same results up to
+// rounding): four 16-wide sub-panels; warp 0 eliminates the 16 x 16 diagonal
+// sub-block with warp-level synchronisation only (and forms its unit-lower
+// inverse), then the CTA computes the sub-panel below it and the trailing
+// update.  The 64 x 64 inverse is assembled from the four 16 x 16 inverses by
+// block forward substitution.  About 20 CTA barriers instead of 128.
+// Rows and columns at or beyond b are padded with the identity (D = 1, L = 0).
+constexpr size_t DIAG_BLOCKED_SMEM = sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17) + 16;
+
+__device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restrict__ F, float2 *__restrict__ Linv,
+                                  unsigned *__restrict__ err, unsigned char *smem) {
+  float2(*A)[65] = reinterpret_cast<float2(*)[65]>(smem);
+  float2(*Wp)[17] = reinterpret_cast<float2(*)[17]>(smem + sizeof(float2) * 64 * 65);
+  float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem + sizeof(float2) * (64 * 65 + 64 * 17));
+  float2(*LI)[65] = reinterpret_cast<float2(*)[65]>(smem + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
+  volatile int *bad =
+      reinterpret_cast<volatile int *>(smem + sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17));
+  const int t = threadIdx.x;  // 256 threads
+  {
+    // all 16 loads of a thread in flight before the shared stores
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = t + 256 * m, i = e >> 6, c = e & 63;
+      v[m] = make_float2(0.f, 0.f);
+      if (i < b && c < b) {
+        if (c <= i) v[m] = F[(j + i) * N + j + c];
+      } else if (i == c) {
+        v[m] = make_float2(1.f, 0.f);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = t + 256 * m;
+      A[e >> 6][e & 63] = v[m];
+    }
+  }
+  if (t == 0) *bad = 0;
+  __syncthreads();
+  for (int s = 0; s < 4; s++) {
+    const int s0 = 16 * s;
+    if (t < 32) {
+      // lane owns sub-block elements (i, c) = ((lane >> 4) + 2 m, lane & 15)
+      const int c = t & 15, ih = t >> 4;
+#pragma unroll
+      for (int m = 0; m < 8; m++) {
+        const int i = ih + 2 * m;
+        Xd[s][i][c] = (i == c) ? make_float2(1.f, 0.f) : make_float2(0.f, 0.f);
+      }
+      __syncwarp();
+      for (int k = 0; k < 16; k++) {
+        // 1/d = conj(d) / |d|^2 with one reciprocal on the serial path; a
+        // pivot whose |d|^2 is zero, non-finite or outside the FP32 range
+        // (|d| below ~1e-19 or above ~1e19) counts as a breakdown
+        const float2 d = A[s0 + k][s0 + k];
+        const float d2 = d.x * d.x + d.y * d.y;
+        if (!(d2 > 0.f) || !isfinite(d2)) {  // uniform over the warp
+          if (t == 0) {
+            atomicOr(err, 2u);
+            *bad = 1;
+          }
+          break;
+        }
+        const float rd = __frcp_rn(d2);
+        const float2 inv_d = make_float2(d.x * rd, -d.y * rd);
+        const float2 lc = cmul(A[s0 + c][s0 + k], inv_d);  // L[c][k] (c > k)
+        const float2 xk = Xd[s][k][c];                     // X[k][c], final at step k
+        float2 na[8], nx[8];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          const int i = ih + 2 * m;
+          const float2 aik = A[s0 + i][s0 + k];
+          na[m] = A[s0 + i][s0 + c];
+          nx[m] = Xd[s][i][c];
+          if (c > k && c <= i) na[m] = csub(na[m], cmul(aik, lc));
+          if (c == k && i > k) na[m] = cmul(aik, inv_d);
+          if (i > k) nx[m] = csub(nx[m], cmul(cmul(aik, inv_d), xk));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          const int i = ih + 2 * m;
+          if (c <= i) A[s0 + i][s0 + c] = na[m];
+          Xd[s][i][c] = nx[m];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (*bad) return;  // uniform
+    if (s == 3) break;
+    // sub-panel below: W = A21 X^T, L21 = W D^-1 (rows s0 + 16 .. 63)
+    const int nr = 48 - s0;
+    for (int e = t; e < nr * 16; e += blockDim.x) {
+      const int r = s0 + 16 + (e >> 4), c = e & 15;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = 0; k <= c; k++) cfma(acc, A[r][s0 + k], Xd[s][c][k]);
+      Wp[r][c] = acc;
+    }
+    __syncthreads();
+    for (int e = t; e < nr * 16; e += blockDim.x) {
+      const int r = s0 + 16 + (e >> 4), c = e & 15;
+      A[r][s0 + c] = cdiv(Wp[r][c], A[s0 + c][s0 + c]);
+    }
+    __syncthreads();
+    // trailing update A22 -= W L21^T on the lower part
+    for (int e = t; e < nr * nr; e += blockDim.x) {
+      const int i = s0 + 16 + e / nr, jj = s0 + 16 + e % nr;
+      if (jj > i) continue;
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 16; k++) cfma(acc, Wp[i][k], A[jj][s0 + k]);
+      A[i][jj] = csub(A[i][jj], acc);
+    }
+    __syncthreads();
+  }
+  // L (strict lower) and D back to F
+  for (int e = t; e < 64 * 64; e += blockDim.x) {
+    const int i = e >> 6, c = e & 63;
+    if (i < b && c <= i) F[(j + i) * N + j + c] = A[i][c];
+  }
+  // Linv (LI in shared memory): diagonal 16-blocks from Xd, zero above, then
+  // block rows I = 1..3: LI[I][J] = -X_I sum_{K=J..I-1} L[I][K] LI[K][J]
+  for (int e = t; e < 64 * 64; e += blockDim.x) {
+    const int i = e >> 6, c = e & 63;
+    LI[i][c] = ((i >> 4) == (c >> 4)) ? Xd[i >> 4][i & 15][c & 15] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int I = 1; I < 4; I++) {
+    // Wp rows 16 J + r hold T_J = sum_K L[I][K] LI[K][J] for J < I
+    for (int e = t; e < I * 256; e += blockDim.x) {
+      const int J = e >> 8, r = (e >> 4) & 15, c = e & 15;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = 16 * J; k < 16 * I; k++) cfma(acc, A[16 * I + r][k], LI[k][16 * J + c]);
+      Wp[16 * J + r][c] = acc;
+    }
+    __syncthreads();
+    for (int e = t; e < I * 256; e += blockDim.x) {
+      const int J = e >> 8, r = (e >> 4) & 15, c = e & 15;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = 0; k <= r; k++) cfma(acc, Xd[I][r][k], Wp[16 * J + k][c]);
+      LI[16 * I + r][16 * J + c] = make_float2(-acc.x, -acc.y);
+    }
+    __syncthreads();
+  }
+  for (int e = t; e < 64 * 64; e += blockDim.x) Linv[e] = LI[e >> 6][e & 63];
+}
+
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
                                                    C *__restrict__ Linv, unsigned *__restrict__ err) {
-  __shared__ C colk[2 * NB];
-  ldlt_diag_block<C>(N, j, b, F, Linv, err, colk);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if constexpr (std::is_same<C, float2>::value)
+    ldlt_diag_blocked(N, j, b, F, Linv, err, smem_raw);
+  else
+    ldlt_diag_block<C>(N, j, b, F, Linv, err, reinterpret_cast<C *>(smem_raw));
 }
 
 // Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
@@ -239,11 +390,22 @@ __device__ __forceinline__ void ldlt_panel_rows(int64_t N, int64_t j, int b, int
   C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
   C(*Li)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw + sizeof(C) * NB * (NB + 1));
   C *dg = reinterpret_cast<C *>(smem_raw + 2 * sizeof(C) * NB * (NB + 1));
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-    int rr = e / NB, k = e % NB;
-    int64_t r = r0 + rr;
-    As[rr][k] = (r < N && k < b) ? __ldcg(F + r * N + j + k) : czero<C>();
-    Li[rr][k] = __ldcg(Linv + rr * NB + k);
+  {
+    // 256 threads: all 32 loads of a thread in flight before the shared stores
+    C va[16], vl[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m, rr = e / NB, k = e % NB;
+      const int64_t r = r0 + rr;
+      va[m] = (r < N && k < b) ? __ldcg(F + r * N + j + k) : czero<C>();
+      vl[m] = __ldcg(Linv + rr * NB + k);
+    }
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m;
+      As[e / NB][e % NB] = va[m];
+      Li[e / NB][e % NB] = vl[m];
+    }
   }
   if (threadIdx.x < b) dg[threadIdx.x] = __ldcg(F + (j + threadIdx.x) * N + j + threadIdx.x);
   __syncthreads();
@@ -375,7 +537,10 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
   ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
   if (t == 0) {
     __syncthreads();
-    ldlt_diag_block<C>(N, r_lo, nb_next, F, Linv_next, err, reinterpret_cast<C *>(smem_raw));
+    if constexpr (std::is_same<C, float2>::value)
+      ldlt_diag_blocked(N, r_lo, nb_next, F, Linv_next, err, smem_raw);
+    else
+      ldlt_diag_block<C>(N, r_lo, nb_next, F, Linv_next, err, reinterpret_cast<C *>(smem_raw));
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
@@ -601,12 +766,19 @@ __global__ void k_scale_vec(int64_t N, int64_t R, const double2 *__restrict__ d,
   x[i] = cmul(x[i], d[i % N]);
 }
 
+template <class C> size_t diag_smem() {
+  return std::is_same<C, float2>::value ? DIAG_BLOCKED_SMEM : sizeof(C) * 2 * NB;
+}
+
 template <class C> void set_smem_attrs() {
   static bool done = false;
   if (done) return;
   size_t panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_panel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
-  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel));
+  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_diag<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)diag_smem<C>()));
+  DMB_CUDA(cudaFuncSetAttribute(k_ldlt_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)std::max(panel, diag_smem<C>())));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * sizeof(C) * NB * NB)));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_bwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -621,12 +793,10 @@ template <class C> void set_smem_attrs() {
 // the block column the whole trailing matrix receives one K = 1024 update --
 // both on the tensor cores for complex64 factors.
 //
-// Lookahead: every such update is split into the next 256 columns (main
-// stream, needed by the next panel) and the rest (second stream).  The next
-// panel's latency-bound diagonal/panel/strip kernels then run while the rest of
-// the update streams through the tensor cores; they touch disjoint columns, W
-// is double-buffered per block column, and the next update on the main stream
-// first joins the second stream (it reuses the packed-operand buffers).
+// Lookahead (details at update_block_column / update_trailing): the next
+// panel's latency-bound diagonal/panel/strip kernels run on the main stream
+// while the rest of each update streams through the tensor cores on two side
+// streams, always on columns disjoint from the main stream's.
 constexpr int NBO = 256;
 constexpr int NBW = 1024;
 
@@ -639,10 +809,11 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   // err word, then two words (ticket, ready flag) per panel step
   c->d_flags.ensure(std::max<size_t>(64, 4 * (4 + 2 * (size_t)nblk)));
-  if (!c->stream2) {
+  if (!c->stream2 || !c->stream3) {
     int least = 0, greatest = 0;
     DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
+    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
+    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, least));
   }
   for (auto &e : c->la_ev)
     if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -655,15 +826,17 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   // 134 KB panel staging would allow one CTA per SM)
   const bool fuse_step = std::is_same<C, float2>::value;
   const size_t sm_panel = sizeof(C) * (2 * NB * (NB + 1) + NB);
+  const size_t sm_step = std::max(sm_panel, diag_smem<C>());  // panel rows or the diagonal block
   const bool use_tc = std::is_same<C, float2>::value && dmb::tc_available(c);
   // trailing update F[r][cc] -= W[r][woff..woff+K) L[cc][jcol..jcol+K) on
-  // rows >= r0, columns [r0, c_hi)
-  auto update = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
+  // rows >= r0, columns [r0, c_hi); slot: the packed-operand buffers of the
+  // issuing stream (0 main, 1 stream2, 2 stream3)
+  auto update = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff, int slot) {
     const int64_t rest = N - r0;
     if (rest <= 0 || c_hi <= r0) return;
     kt_begin(c);
     if (use_tc) {
-      dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)Wb, NBW, woff);
+      dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)Wb, NBW, woff, slot);
     } else {
       dim3 g(blocks_for(rest, 64), blocks_for(c_hi - r0, 64));
       DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, Wb, NBW, woff, 0, (C *)nullptr, err);
@@ -672,27 +845,54 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     const double cols = (double)(c_hi - r0), rows = (double)rest;
     kt_end(c, 8.0 * K * (cols * rows - cols * (cols - 1) / 2.0), 2);
   };
-  bool pending = false;  // the second stream holds an update not yet joined
-  auto join = [&] {
-    if (pending) {
-      DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[1], 0));
-      pending = false;
-    }
+  // Lookahead.  Updates of one panel are split by columns: the next 256
+  // columns on the main stream (the next panel needs them), the rest of the
+  // current 1024-wide block column on stream2 and, for the trailing update at
+  // the end of a block column, everything beyond the next block column on
+  // stream3.  Concurrent updates always cover disjoint column ranges; before
+  // an update of columns that a side stream may still be updating, the main
+  // stream joins that stream (pend2 / pend3).  Each stream packs into its own
+  // buffer slot, and W is double-buffered per block column, so a stream3
+  // update may run through the whole next block column.
+  bool pend2 = false, pend3 = false;
+  auto join2 = [&] {
+    if (pend2) DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[1], 0));
+    pend2 = false;
   };
-  auto update_split = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
-    join();
-    const int64_t cmid = std::min<int64_t>(c_hi, r0 + NBO);
-    update(r0, cmid, jcol, K, Wb, woff);
-    if (cmid < c_hi && cmid < N) {
-      DMB_CUDA(cudaEventRecord(c->la_ev[0], c->stream));
-      DMB_CUDA(cudaStreamWaitEvent(c->stream2, c->la_ev[0], 0));
-      {
-        StreamSwap sw(c, c->stream2);
-        update(cmid, c_hi, jcol, K, Wb, woff);
-      }
-      DMB_CUDA(cudaEventRecord(c->la_ev[1], c->stream2));
-      pending = true;
+  auto join3 = [&] {
+    if (pend3) DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[3], 0));
+    pend3 = false;
+  };
+  // columns [lo, hi) updated on a side stream (1: stream2, 2: stream3) after
+  // everything issued so far on the main stream
+  auto side = [&](int which, int64_t lo, int64_t hi, int64_t jcol, int K, const C *Wb, int woff) {
+    if (lo >= hi || lo >= N) return;
+    cudaStream_t s = which == 1 ? c->stream2 : c->stream3;
+    cudaEvent_t start = c->la_ev[which == 1 ? 0 : 2], done = c->la_ev[which == 1 ? 1 : 3];
+    DMB_CUDA(cudaEventRecord(start, c->stream));
+    DMB_CUDA(cudaStreamWaitEvent(s, start, 0));
+    {
+      StreamSwap sw(c, s);
+      update(lo, hi, jcol, K, Wb, woff, which);
     }
+    DMB_CUDA(cudaEventRecord(done, s));
+    (which == 1 ? pend2 : pend3) = true;
+  };
+  // after a 256-wide middle panel: the rest of its block column
+  auto update_block_column = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
+    join2();
+    const int64_t cmid = std::min<int64_t>(c_hi, r0 + NBO);
+    update(r0, cmid, jcol, K, Wb, woff, 0);
+    side(1, cmid, c_hi, jcol, K, Wb, woff);
+  };
+  // after a block column: the trailing matrix
+  auto update_trailing = [&](int64_t r0, int64_t jcol, int K, const C *Wb) {
+    join2();
+    join3();
+    const int64_t c1 = std::min<int64_t>(N, r0 + NBO), c2 = std::min<int64_t>(N, r0 + NBW);
+    update(r0, c1, jcol, K, Wb, 0, 0);
+    side(1, c1, c2, jcol, K, Wb, 0);
+    side(2, c2, N, jcol, K, Wb, 0);
   };
   int64_t bc = 0;
   for (int64_t J2 = 0; J2 < N; J2 += NBW, bc++) {
@@ -706,7 +906,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
       for (int64_t j = J; j < JE; j += NB) {
         const int b = (int)std::min<int64_t>(NB, N - j);
         C *Lblk = Linv + (j / NB) * NB * NB;
-        if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, 0, N, j, b, F, Lblk, err);
+        if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, diag_smem<C>(), N, j, b, F, Lblk, err);
         const int64_t rest = N - j - b;
         if (rest <= 0) break;
         if (!panel_done)
@@ -717,7 +917,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
           const int nb_next = (int)std::min<int64_t>(NB, N - (j + b));
           dim3 g(blocks_for(rest, 64), blocks_for(JE - (j + b), 64));
           if (fuse_step) {
-            DMB_LAUNCH(c, k_ldlt_step<C>, g.x * g.y, 256, sm_panel, N, j + b, JE, j, b, F, Wb, NBW,
+            DMB_LAUNCH(c, k_ldlt_step<C>, g.x * g.y, 256, sm_step, N, j + b, JE, j, b, F, Wb, NBW,
                        (int)(j - J2), (int)(j + b - J2), nb_next, Lblk + NB * NB, step_sync + 2 * (j / NB), err);
             panel_done = true;
           } else {
@@ -727,11 +927,12 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
           diag_done = true;
         }
       }
-      update_split(JE, J2E, J, (int)(JE - J), Wb, (int)(J - J2));  // rest of the block column
+      update_block_column(JE, J2E, J, (int)(JE - J), Wb, (int)(J - J2));
     }
-    update_split(J2E, N, J2, (int)(J2E - J2), Wb, 0);              // trailing matrix
+    update_trailing(J2E, J2, (int)(J2E - J2), Wb);
   }
-  join();
+  join2();
+  join3();
   unsigned h_err = 0;
   DMB_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
@@ -1155,17 +1356,23 @@ void nf_build(dmb_ctx *c, double cutoff, int kind) {
   DevBuf cnt;  // view into the persistent scratch (first 8 bytes), not owned
   cnt.p = c->d_small.p;
   DMB_CUDA(cudaMemsetAsync(cnt.p, 0, 8, c->stream));
-  dim3 g(blocks_for(N, 32), blocks_for(N, 32));
-  if (f64)
-    DMB_LAUNCH(c, (k_nf_mask<double2, double2>), g, 256, 0, N, c->d_Z.as<double2>(), c->d_centers.as<double>(),
-               cutoff, c->d_F.as<double2>(), cnt.as<unsigned long long>());
-  else
-    DMB_LAUNCH(c, (k_nf_mask<float2, float2>), g, 256, 0, N, c->d_Z.as<float2>(), c->d_centers.as<double>(),
-               cutoff, c->d_F.as<float2>(), cnt.as<unsigned long long>());
-  unsigned long long h_cnt = 0;
-  DMB_CUDA(cudaMemcpyAsync(&h_cnt, cnt.p, 8, cudaMemcpyDeviceToHost, c->stream));
-  DMB_CUDA(cudaStreamSynchronize(c->stream));
-  c->nnz_ratio = ((double)h_cnt / (double)N) / (double)N;
+  if (!std::isfinite(cutoff) && cutoff > 0) {
+    // every entry is kept: a plain device copy of Z
+    DMB_CUDA(cudaMemcpyAsync(c->d_F.p, c->d_Z.p, esz * N * N, cudaMemcpyDeviceToDevice, c->stream));
+    c->nnz_ratio = 1.0;
+  } else {
+    dim3 g(blocks_for(N, 32), blocks_for(N, 32));
+    if (f64)
+      DMB_LAUNCH(c, (k_nf_mask<double2, double2>), g, 256, 0, N, c->d_Z.as<double2>(), c->d_centers.as<double>(),
+                 cutoff, c->d_F.as<double2>(), cnt.as<unsigned long long>());
+    else
+      DMB_LAUNCH(c, (k_nf_mask<float2, float2>), g, 256, 0, N, c->d_Z.as<float2>(), c->d_centers.as<double>(),
+                 cutoff, c->d_F.as<float2>(), cnt.as<unsigned long long>());
+    unsigned long long h_cnt = 0;
+    DMB_CUDA(cudaMemcpyAsync(&h_cnt, cnt.p, 8, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+    c->nnz_ratio = ((double)h_cnt / (double)N) / (double)N;
+  }
   if (f64)
     ldlt_factor(c, c->d_F.as<double2>());
   else

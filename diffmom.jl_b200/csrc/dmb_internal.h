@@ -91,8 +91,11 @@ struct NearRec {
 struct dmb_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t stream2 = nullptr;      // factorisation lookahead (created on first use)
-  cudaEvent_t la_ev[2] = {nullptr, nullptr};
+  // factorisation lookahead (created on first use): stream2 takes the rest of
+  // each block column's updates, stream3 the trailing matrix beyond the next
+  // block column
+  cudaStream_t stream2 = nullptr, stream3 = nullptr;
+  cudaEvent_t la_ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
   std::string err;
   int sm_count = 148;
@@ -160,6 +163,7 @@ struct dmb_ctx {
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
   int far_tile = 0;              // far-pair tile rows (8/16/32), 0 = autotuned
   bool exact_krylov = true;      // many-RHS Krylov product on the INT8 slices (FP64-accurate)
+  int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
   int far_tile_used = 0;         // shape of the last assembly
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation

@@ -112,11 +112,16 @@ __global__ void k_tc_pack(int64_t rest, int64_t ncols, int64_t N, int64_t r0, in
   }
 }
 
+// Packed K blocks hold 1536 floats per 256 complex K: segments [hi x hi |
+// hi x lo | lo x hi] of 512 floats each.  cpb = K chunks of 32 floats streamed
+// per block: 48 (3xTF32, all three products) or 16 (1xTF32, hi x hi only).
+__device__ __forceinline__ int tc_kx(int kc, int cpb) { return (kc / cpb) * 1536 + (kc % cpb) * TC_BK; }
+
 template <int STAGES>
 __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
                                                     int64_t N, int64_t j0, int64_t rest, int64_t c_hi, int nchunks,
-                                                    unsigned *err) {
+                                                    int cpb, unsigned *err) {
   // grid.x walks row blocks fastest, so CTAs running together share the
   // column block's B operand in L2
   const int64_t row0 = (int64_t)blockIdx.x * 64;   // complex rows of the tile (relative to j0)
@@ -162,8 +167,9 @@ __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __
       const int s = kc % STAGES;
       if (kc >= STAGES && !mbar_wait(empty0 + 8 * s, ((kc / STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
-      tma_load_2d(sA + s * TC_A_STAGE, &tmA, kc * TC_BK, (int)(2 * row0), full0 + 8 * s);
-      tma_load_2d(sB + s * TC_B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
+      const int kx = tc_kx(kc, cpb);
+      tma_load_2d(sA + s * TC_A_STAGE, &tmA, kx, (int)(2 * row0), full0 + 8 * s);
+      tma_load_2d(sB + s * TC_B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -256,17 +262,18 @@ __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __
 template <int ROLE, int BN>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
-                                                    int nchunks, int64_t M, int64_t Rv, double2 *__restrict__ Y,
-                                                    int64_t ldy, int mode, int tri, unsigned *err) {
+                                                    int nchunks, int cpb, int64_t M, int64_t Rv,
+                                                    double2 *__restrict__ Y, int64_t ldy, int mode, int tri,
+                                                    unsigned *err) {
   constexpr int B_STAGE = BN * TC_BK * 4;
   const int64_t col0 = (int64_t)blockIdx.x * BN;
   const int64_t row0 = (int64_t)blockIdx.y * 64;
   if (row0 >= M || col0 >= Rv) return;  // uniform
   // triangular A (tri 1: lower, A[m][k] = 0 for k > m; tri 2: upper): only the
-  // 256-wide K blocks that meet this row tile's rows are streamed (48 chunks each)
+  // 256-wide K blocks that meet this row tile's rows are streamed (cpb chunks each)
   int kc0 = 0, kc1 = nchunks;
-  if (tri == 1) kc1 = min(nchunks, 48 * (int)((row0 + 64 + 255) / 256));
-  else if (tri == 2) kc0 = 48 * (int)(row0 / 256);
+  if (tri == 1) kc1 = min(nchunks, cpb * (int)((row0 + 64 + 255) / 256));
+  else if (tri == 2) kc0 = cpb * (int)(row0 / 256);
   const int nk = kc1 - kc0;
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -307,8 +314,9 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
       const int s = i % TC_STAGES, kc = kc0 + i;
       if (i >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((i / TC_STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + B_STAGE);
-      tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kc * TC_BK, a_row0 + (int)(2 * row0), full0 + 8 * s);
-      tma_load_2d(sB + s * B_STAGE, &tmB, kc * TC_BK, (int)col0, full0 + 8 * s);
+      const int kx = tc_kx(kc, cpb);
+      tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kx, a_row0 + (int)(2 * row0), full0 + 8 * s);
+      tma_load_2d(sB + s * B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
@@ -406,6 +414,9 @@ template <bool TRANS, bool LOWER, class SC>
 __global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kpad, const SC *__restrict__ S,
                                                 int64_t ld, float *__restrict__ Ap) {
   __shared__ float2 tile[32][33];
+  // LOWER: tiles holding only excluded (zero) elements are not written -- the
+  // triangular-sweep GEMMs read the packed factor only in the included part
+  if (LOWER && (TRANS ? blockIdx.x < blockIdx.y : blockIdx.x > blockIdx.y)) return;
   const int64_t m0 = (int64_t)blockIdx.y * 32, k0 = (int64_t)blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (int i = ty; i < 32; i += 8) {
@@ -455,10 +466,15 @@ void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows, u
   make_map_bytes(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ld, ld * sizeof(float), rows, TC_BK, box_rows);
 }
 
+// factor updates pack their operands into one of TC_UPD_SLOTS buffer pairs,
+// one per stream that issues them, so updates of disjoint column ranges run
+// concurrently
+constexpr int TC_UPD_SLOTS = 3;
+
 struct TcState {
-  DevBuf A, B, err;
-  CUtensorMap mapAK[4], mapBK[4];
-  int64_t n_key = -1;
+  DevBuf A[TC_UPD_SLOTS], B[TC_UPD_SLOTS], err;
+  CUtensorMap mapAK[TC_UPD_SLOTS][4], mapBK[TC_UPD_SLOTS][4];
+  int64_t n_key[TC_UPD_SLOTS] = {-1, -1, -1};
   bool attr = false;
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
   // sides, packed triangular-solve panels
@@ -516,21 +532,23 @@ bool tc_available(dmb_ctx *c) {
 //   F[r][c] -= sum_{k < K} W[r][woff + k] L[c][jcol + k],  r0 <= c < c_hi, c <= r < N
 // K <= 1024 (the packed buffers are sized for that).
 void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t jcol, int K, float2 *F,
-                        const float2 *W, int wstride, int woff) {
+                        const float2 *W, int wstride, int woff, int slot) {
   DMB_REQUIRE(K >= 1 && K <= 1024, DMB_ERR_STATE, "tensor-core update width must be 1..1024");
+  DMB_REQUIRE(slot >= 0 && slot < TC_UPD_SLOTS, DMB_ERR_STATE, "bad update buffer slot");
   TcState &st = tc_state(c);
+  DevBuf &bA = st.A[slot], &bB = st.B[slot];
   const int64_t npadA = ((N + 63) / 64) * 64;
   const int64_t npadB = ((N + TC_BN - 1) / TC_BN) * TC_BN;
   const int64_t Kpad = ((K + 255) / 256) * 256, ld = 6 * Kpad;
-  if (st.n_key != N) {
-    st.A.ensure(sizeof(float) * 2 * npadA * 6 * 1024);
-    st.B.ensure(sizeof(float) * npadB * 6 * 1024);
-    DMB_CUDA(cudaMemsetAsync(st.B.p, 0, sizeof(float) * npadB * 6 * 1024, c->stream));
+  if (st.n_key[slot] != N) {
+    bA.ensure(sizeof(float) * 2 * npadA * 6 * 1024);
+    bB.ensure(sizeof(float) * npadB * 6 * 1024);
+    DMB_CUDA(cudaMemsetAsync(bB.p, 0, sizeof(float) * npadB * 6 * 1024, c->stream));
     for (int i = 0; i < 4; i++) {
-      make_map(&st.mapAK[i], st.A.as<float>(), (uint64_t)(2 * npadA), TC_BM, 1536 * (i + 1));
-      make_map(&st.mapBK[i], st.B.as<float>(), (uint64_t)npadB, TC_BN, 1536 * (i + 1));
+      make_map(&st.mapAK[slot][i], bA.as<float>(), (uint64_t)(2 * npadA), TC_BM, 1536 * (i + 1));
+      make_map(&st.mapBK[slot][i], bB.as<float>(), (uint64_t)npadB, TC_BN, 1536 * (i + 1));
     }
-    st.n_key = N;
+    st.n_key[slot] = N;
   }
   if (!st.err.p) {
     st.err.ensure(16);
@@ -547,10 +565,11 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   // A'' rows past `rest` and B'' rows past `ncols` keep stale values: they only
   // feed output rows >= N and columns >= c_hi, which the epilogue skips
   DMB_LAUNCH(c, k_tc_pack, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
-             N, r0, jcol, K, ld, F, W, wstride, woff, st.A.as<float>(), st.B.as<float>());
+             N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<float>(), bB.as<float>());
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
-  DMB_LAUNCH(c, k_tc_syrk<TC_SYRK_STAGES>, grid, 128, TC_SYRK_SMEM, st.mapAK[kslot], st.mapBK[kslot], F, N, r0, rest,
-             std::min<int64_t>(c_hi, N), (int)(ld / TC_BK), st.err.as<unsigned>());
+  const int cpb = 16 * c->precond_tf32_terms;
+  DMB_LAUNCH(c, k_tc_syrk<TC_SYRK_STAGES>, grid, 128, TC_SYRK_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
+             r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
 }
 
 unsigned tc_error_word(dmb_ctx *c) {
@@ -589,7 +608,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, (k_tc_gemm<0, 256>), grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), N, R, Y, N, 0, 0,
+  DMB_LAUNCH(c, (k_tc_gemm<0, 256>), grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), 48, N, R, Y, N, 0, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -634,7 +653,7 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
              N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), M, R,
+  DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), 48, M, R,
              X + r_lo, N, 1, 0, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
@@ -699,15 +718,16 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   // triangular diagonal-block products with few row tiles: 128-wide tiles
   // double the CTAs (measured faster only there)
   const bool narrow = tri != 0 && (Rpad / TC_BN) * (Mpad / 64) < 2 * (int64_t)c->sm_count;
+  const int cpb = 16 * c->precond_tf32_terms;
   kt_begin(c);
   if (narrow) {
     dim3 grid((unsigned)(Rpad / 128), (unsigned)(Mpad / 64));
     DMB_LAUNCH(c, (k_tc_gemm<1, 128>), grid, 128, TC_SMEM_128, mapA, st.mapPbK128[kslot], a_row0, a_kx0,
-               (int)(6 * Kpad / TC_BK), M, R, Y, N, mode, tri, st.err.as<unsigned>());
+               (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>());
   } else {
     dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
     DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0,
-               (int)(6 * Kpad / TC_BK), M, R, Y, N, mode, tri, st.err.as<unsigned>());
+               (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>());
   }
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
@@ -740,9 +760,12 @@ void tc_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_tc_states.size(); i++) {
     if (g_tc_states[i].first != c) continue;
     TcState *st = g_tc_states[i].second;
-    for (DevBuf *b : {&st->A, &st->B, &st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb, &st->Lp, &st->Ltp, &st->Dfp,
-                      &st->Dbp})
+    for (DevBuf *b : {&st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb, &st->Lp, &st->Ltp, &st->Dfp, &st->Dbp})
       b->release();
+    for (int slot = 0; slot < TC_UPD_SLOTS; slot++) {
+      st->A[slot].release();
+      st->B[slot].release();
+    }
     delete st;
     g_tc_states.erase(g_tc_states.begin() + i);
     return;

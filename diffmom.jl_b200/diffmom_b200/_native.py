@@ -44,6 +44,7 @@ OPT_TENSOR_CORES = 1
 OPT_TC_MIN_RHS = 2
 OPT_FAR_TILE = 3
 OPT_EXACT_KRYLOV = 4
+OPT_PRECOND_TF32_TERMS = 5
 
 
 class DiffMoMError(RuntimeError):

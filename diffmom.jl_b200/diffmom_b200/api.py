@@ -86,13 +86,16 @@ class EFIEDevice:
         factorisation update, "tc_min_rhs" (>= 1) for the right-hand-side count
         from which Z X and the batched near-field solves use the tensor cores,
         "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles,
-        "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product."""
+        "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product,
+        "precond_tf32_terms" (3/1) for the TF32 products per complex MAC of the
+        complex64 factorisation updates and batched triangular sweeps."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
-                 "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV}
+                 "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
+                 "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))
-        if name == "tensor_cores":
+        if name in ("tensor_cores", "precond_tf32_terms"):
             self.preconditioner = None
 
     def far_tile(self) -> int:
