@@ -403,6 +403,67 @@ dmb_status dmb_rhs_dipoles(dmb_ctx *c, int64_t R, const double *positions, const
   });
 }
 
+dmb_status dmb_rhs_pattern_feed(dmb_ctx *c, int ntheta, const double *theta, int nphi, const double *phi,
+                                const double *Ftheta, const double *Fphi, double frequency,
+                                const double *phase_center, int conj_convention, int quad_order, double *V_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->have_rwg, DMB_ERR_STATE, "mesh and RWG data must be uploaded first");
+    DMB_REQUIRE(theta && phi && Ftheta && Fphi && phase_center && V_out, DMB_ERR_ARGUMENT, "bad pattern arrays");
+    DMB_REQUIRE(ntheta >= 2, DMB_ERR_ARGUMENT, "Pattern feed requires at least 2 theta samples.");
+    DMB_REQUIRE(nphi >= 2, DMB_ERR_ARGUMENT, "Pattern feed requires at least 2 phi samples.");
+    check_finite(theta, ntheta, "Theta grid");
+    check_finite(phi, nphi, "Phi grid");
+    for (int i = 1; i < ntheta; i++)
+      DMB_REQUIRE(theta[i] > theta[i - 1], DMB_ERR_ARGUMENT, "Theta grid must be strictly increasing.");
+    for (int i = 1; i < nphi; i++)
+      DMB_REQUIRE(phi[i] > phi[i - 1], DMB_ERR_ARGUMENT, "Phi grid must be strictly increasing.");
+    DMB_REQUIRE(theta[0] >= -1e-12 && theta[ntheta - 1] <= 3.14159265358979323846 + 1e-12, DMB_ERR_ARGUMENT,
+                "Theta grid must lie in [0, pi] (radians).");
+    const double span = phi[nphi - 1] - phi[0];
+    DMB_REQUIRE(span > 0 && span < 2.0 * 3.14159265358979323846 - 1e-12, DMB_ERR_ARGUMENT,
+                "Phi grid should cover one open 2 pi period without a duplicate endpoint.");
+    check_finite(Ftheta, 2 * (int64_t)ntheta * nphi, "pattern Ftheta");
+    check_finite(Fphi, 2 * (int64_t)ntheta * nphi, "pattern Fphi");
+    check_finite(phase_center, 3, "pattern phase_center");
+    DMB_REQUIRE(std::isfinite(frequency) && frequency > 0, DMB_ERR_ARGUMENT,
+                "Pattern feed frequency must be finite and positive.");
+    const size_t bytes = sizeof(double2) * c->n;
+    DevBuf bv;
+    bv.ensure(bytes);
+    dmb::rhs_pattern_dev(c, ntheta, theta, nphi, phi, Ftheta, Fphi, frequency, phase_center,
+                         conj_convention ? 1 : 0, quad_order, bv.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(V_out, bv.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+dmb_status dmb_gradient_impedance(dmb_ctx *c, int64_t R, const double *I, const double *lambda,
+                                  const int *tri_patch, int64_t P, int reactive, int quad_order, double *g_out) {
+  return guarded(c, [&] {
+    DMB_REQUIRE(c->have_rwg, DMB_ERR_STATE, "mesh and RWG data must be uploaded first");
+    DMB_REQUIRE(R >= 1 && I && lambda && tri_patch && g_out && P >= 0, DMB_ERR_ARGUMENT,
+                "bad gradient arguments");
+    DMB_REQUIRE(P <= 65535 && R <= 65535, DMB_ERR_ARGUMENT, "at most 65,535 patches and columns per call");
+    for (int64_t t = 0; t < c->nt; t++)
+      DMB_REQUIRE(tri_patch[t] >= 0 && tri_patch[t] < P, DMB_ERR_ARGUMENT,
+                  "partition.tri_patch entries must lie in 0..P-1");
+    check_finite(I, 2 * c->n * R, "I must contain only finite values");
+    check_finite(lambda, 2 * c->n * R, "lambda must contain only finite values");
+    if (P == 0) return;
+    const size_t vb = sizeof(double2) * c->n * R;
+    DevBuf bi, bl, bg;
+    bi.ensure(vb);
+    bl.ensure(vb);
+    bg.ensure(sizeof(double) * P * R);
+    DMB_CUDA(cudaMemcpyAsync(bi.p, I, vb, cudaMemcpyHostToDevice, c->stream));
+    DMB_CUDA(cudaMemcpyAsync(bl.p, lambda, vb, cudaMemcpyHostToDevice, c->stream));
+    dmb::gradient_impedance_dev(c, R, bi.as<double2>(), bl.as<double2>(), tri_patch, P, reactive ? 1 : 0,
+                                quad_order, bg.as<double>());
+    DMB_CUDA(cudaMemcpyAsync(g_out, bg.p, sizeof(double) * P * R, cudaMemcpyDeviceToHost, c->stream));
+    DMB_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 dmb_status dmb_rhs_plane_waves(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
                                int64_t R, int quad_order, double *V_out) {
   return guarded(c, [&] {

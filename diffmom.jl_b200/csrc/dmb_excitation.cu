@@ -144,6 +144,128 @@ __global__ void k_dipole_rhs(int64_t N, int64_t R, const TriCache *__restrict__ 
   V[idx] = acc;
 }
 
+// Pattern feed (Excitation.jl:1170-1340, 1417-1460): E(r) = exp(-ikR)/R
+// (F_theta e_theta + F_phi e_phi) of r - phase_center, F bilinear in
+// (theta, phi) on the grid -- theta clamped to its range, phi periodic with
+// the interval from the last sample back to the first + 2 pi -- and conjugated
+// for exp(-i omega t) data.  F matrices column-major (ntheta x nphi).  Folded
+// with the RWG basis as assemble_pattern_feed (Excitation.jl:3044-3071).
+struct PatternDev {
+  int nth, nph;
+  const double *th, *ph;
+  const double2 *Ft, *Fp;
+  double k, pc[3];
+  int conj;
+};
+
+// largest i with g[i] <= x (g strictly increasing, x >= g[0])
+__device__ int pat_search_last(const double *g, int n, double x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ double2 pat_bilinear(const double2 *M, int nth, int it, int jt, double tt, int ip, int jp, double tp) {
+  const double2 c00 = M[it + (int64_t)ip * nth];
+  if (it == jt && ip == jp) return c00;
+  if (it == jt) return cadd(cscale(c00, 1 - tp), cscale(M[it + (int64_t)jp * nth], tp));
+  if (ip == jp) return cadd(cscale(c00, 1 - tt), cscale(M[jt + (int64_t)ip * nth], tt));
+  const double2 c10 = M[jt + (int64_t)ip * nth], c01 = M[it + (int64_t)jp * nth], c11 = M[jt + (int64_t)jp * nth];
+  return cadd(cadd(cadd(cscale(c00, (1 - tt) * (1 - tp)), cscale(c10, tt * (1 - tp))), cscale(c01, (1 - tt) * tp)),
+              cscale(c11, tt * tp));
+}
+
+__device__ void pattern_field(const double *r, const PatternDev &P, double2 *E) {
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  const double d[3] = {r[0] - P.pc[0], r[1] - P.pc[1], r[2] - P.pc[2]};
+  const double R = hypot(hypot(d[0], d[1]), d[2]);
+  if (R == 0.0) {
+    E[0] = E[1] = E[2] = make_double2(0, 0);
+    return;
+  }
+  const double th = acos(fmin(1.0, fmax(-1.0, d[2] / R)));
+  double ph = atan2(d[1], d[0]);
+  if (ph < 0) ph += two_pi;
+  double st, ct, sp, cp;
+  sincos(th, &st, &ct);
+  sincos(ph, &sp, &cp);
+  const double et[3] = {ct * cp, ct * sp, -st}, ep[3] = {-sp, cp, 0.0};
+  // theta: clamped
+  int it, jt;
+  double tt;
+  if (th <= P.th[0]) {
+    it = jt = 0;
+    tt = 0.0;
+  } else if (th >= P.th[P.nth - 1]) {
+    it = jt = P.nth - 1;
+    tt = 0.0;
+  } else {
+    it = min(pat_search_last(P.th, P.nth, th), P.nth - 2);
+    jt = it + 1;
+    tt = (th - P.th[it]) / (P.th[jt] - P.th[it]);
+  }
+  // phi: periodic (floored modulo)
+  double m = fmod(ph - P.ph[0], two_pi);
+  if (m != 0.0 && m < 0.0) m += two_pi;
+  const double w = m + P.ph[0];
+  int ip, jp;
+  double tp;
+  const int n = P.nph;
+  if (w <= P.ph[n - 1]) {
+    const int a = pat_search_last(P.ph, n, w);
+    if (a == n - 1) {
+      ip = n - 1;
+      jp = 0;
+      tp = (w - P.ph[n - 1]) / (P.ph[0] + two_pi - P.ph[n - 1]);
+    } else {
+      ip = a;
+      jp = a + 1;
+      tp = (w - P.ph[a]) / (P.ph[a + 1] - P.ph[a]);
+    }
+  } else {
+    ip = n - 1;
+    jp = 0;
+    tp = (w - P.ph[n - 1]) / (P.ph[0] + two_pi - P.ph[n - 1]);
+  }
+  double2 Ft = pat_bilinear(P.Ft, P.nth, it, jt, tt, ip, jp, tp);
+  double2 Fp = pat_bilinear(P.Fp, P.nth, it, jt, tt, ip, jp, tp);
+  if (P.conj) {
+    Ft = cconj(Ft);
+    Fp = cconj(Fp);
+  }
+  double sn, cs;
+  sincos(-P.k * R, &sn, &cs);
+  const double2 phase = make_double2(cs, sn);
+  for (int a = 0; a < 3; a++)
+    E[a] = cmul(cscale(cadd(cscale(Ft, et[a]), cscale(Fp, ep[a])), 1.0 / R), phase);
+}
+
+__global__ void k_pattern_rhs(int64_t N, const TriCache *__restrict__ tc, const int *__restrict__ rslot, int nq,
+                              const double *__restrict__ wq, PatternDev P, double2 *__restrict__ V) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double2 acc = make_double2(0, 0);
+  for (int s = 0; s < 2; s++) {
+    const int sl = rslot[2 * n + s];
+    const TriCache &T = tc[sl / 3];
+    const int i = sl % 3;
+    for (int q = 0; q < nq; q++) {
+      const double f0 = T.s[i] * (T.qp[q][0] - T.p[i][0]);
+      const double f1 = T.s[i] * (T.qp[q][1] - T.p[i][1]);
+      const double f2 = T.s[i] * (T.qp[q][2] - T.p[i][2]);
+      double2 E[3];
+      pattern_field(T.qp[q], P, E);
+      const double2 ip = cadd(cadd(cscale(E[0], f0), cscale(E[1], f1)), cscale(E[2], f2));
+      acc = cadd(acc, cscale(cscale(ip, T.area), -(2 * wq[q])));
+    }
+  }
+  V[n] = acc;
+}
+
 // radiation matrix G (3*NO x N, row-major) for directions rh
 __global__ void k_radiation(int64_t N, int64_t NO, const TriCache *__restrict__ tc, const int *__restrict__ rslot,
                             int nq, const double *__restrict__ wq, const double *__restrict__ rh, double k,
@@ -449,6 +571,36 @@ void rhs_dipoles_dev(dmb_ctx *c, int64_t R, const double *pos, const double *mom
   DMB_LAUNCH(c, k_dipole_rhs, blocks_for(c->n * R, 128), 128, 0, c->n, R, c->d_tcache.as<TriCache>(),
              c->d_rwg_slot.as<int>(), c->nq, c->d_wq.as<double>(), bp.as<double>(), bm.as<double>(), bt.as<int>(),
              bf.as<double>(), (double2 *)V_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  c->tm.rhs_ms = now_ms() - t0;
+}
+
+void rhs_pattern_dev(dmb_ctx *c, int nth, const double *theta, int nph, const double *phi, const double *Ft,
+                     const double *Fp, double freq, const double *pc, int conj_conv, int quad_order, double *V_dev) {
+  double t0 = now_ms();
+  ensure_cache(c, quad_order);
+  DevBuf bth, bph, bft, bfp;
+  const size_t nf = (size_t)nth * nph;
+  bth.ensure(8 * nth);
+  bph.ensure(8 * nph);
+  bft.ensure(16 * nf);
+  bfp.ensure(16 * nf);
+  DMB_CUDA(cudaMemcpyAsync(bth.p, theta, 8 * nth, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bph.p, phi, 8 * nph, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bft.p, Ft, 16 * nf, cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(bfp.p, Fp, 16 * nf, cudaMemcpyHostToDevice, c->stream));
+  PatternDev P;
+  P.nth = nth;
+  P.nph = nph;
+  P.th = bth.as<double>();
+  P.ph = bph.as<double>();
+  P.Ft = (const double2 *)bft.p;
+  P.Fp = (const double2 *)bfp.p;
+  P.k = 2.0 * 3.14159265358979323846 * freq / 299792458.0;
+  for (int a = 0; a < 3; a++) P.pc[a] = pc[a];
+  P.conj = conj_conv;
+  DMB_LAUNCH(c, k_pattern_rhs, blocks_for(c->n, 128), 128, 0, c->n, c->d_tcache.as<TriCache>(),
+             c->d_rwg_slot.as<int>(), c->nq, c->d_wq.as<double>(), P, (double2 *)V_dev);
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   c->tm.rhs_ms = now_ms() - t0;
 }

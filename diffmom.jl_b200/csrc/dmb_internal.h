@@ -241,6 +241,8 @@ struct StreamSwap {
 // ---------------------------------------------------------------------------
 namespace dmb {
 void ensure_cache(dmb_ctx *c, int quad_order);
+void gradient_impedance_dev(dmb_ctx *c, int64_t R, const double2 *I_dev, const double2 *L_dev,
+                            const int *tri_patch, int64_t P, int reactive, int quad_order, double *g_dev);
 void build_host_topology(dmb_ctx *c);
 void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision);
 void copy_z_out(dmb_ctx *c, double *Z_out);
@@ -254,6 +256,8 @@ void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, con
                          int64_t R, int quad_order, double *V_dev);
 void rhs_dipoles_dev(dmb_ctx *c, int64_t R, const double *pos, const double *moments, const int *magnetic,
                      const double *freqs, int quad_order, double *V_dev);
+void rhs_pattern_dev(dmb_ctx *c, int nth, const double *theta, int nph, const double *phi, const double *Ft,
+                     const double *Fp, double freq, const double *pc, int conj_conv, int quad_order, double *V_dev);
 void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs, double tol,
                int maxiter, int precond_kind, int precond_side, dmb_gmres_stats *st);
 void solve_direct_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t nrhs,

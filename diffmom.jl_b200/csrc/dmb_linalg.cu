@@ -1,11 +1,13 @@
 // dmb_linalg.cu -- dense operators on the resident impedance matrix:
 //   * Z*x (the zgemv Krylov.gmres performs every iteration) and Z*X,
 //   * Z copy-out and entry gather (efie_entry, EFIE.jl:1002-1007),
-//   * per-triangle impedance loading (Impedance.jl:304-408),
+//   * per-triangle impedance loading (Impedance.jl:304-408) and the
+//     impedance gradient (Adjoint.jl:1081-1119),
 //   * direct solve: factorisation of Z itself (cutoff = Inf, dmb_factor.cu)
 //     plus FP64 iterative refinement (Solve.jl:1124-1198).
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "dmb_device.cuh"
 #include "dmb_internal.h"
@@ -314,6 +316,71 @@ void apply_impedance(dmb_ctx *c, const double *zs) {
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   c->pc_valid = false;
   c->z_version++;
+}
+
+// gradient_impedance (optimization/Adjoint.jl:1081-1119): for every patch p
+// and column r, s = lambda_r^H M_p I_r with M_p[m][n] the integral of f_m . f_n
+// over the patch's triangles (precompute_patch_mass, Impedance.jl:304-377,
+// evaluated here per triangle as in k_impedance_offdiag); g = 2 Re s
+// (resistive) or -2 Im s (reactive).  One CTA per (patch, column) walks the
+// patch's triangles (CSR poff / ptri) and reduces in a fixed order.
+__global__ void __launch_bounds__(128) k_grad_impedance(int64_t N, int64_t P, const TriCache *__restrict__ tc,
+                                                        int nq, const double *__restrict__ wq,
+                                                        const int *__restrict__ poff, const int *__restrict__ ptri,
+                                                        const double2 *__restrict__ I, const double2 *__restrict__ L,
+                                                        int reactive, double *__restrict__ g) {
+  __shared__ double2 red[128];
+  const int64_t p = blockIdx.x, r = blockIdx.y;
+  const double2 *Ir = I + r * N, *Lr = L + r * N;
+  double2 acc = make_double2(0, 0);
+  for (int e = poff[p] + threadIdx.x; e < poff[p + 1]; e += blockDim.x) {
+    const TriCache &T = tc[ptri[e]];
+    for (int i = 0; i < 3; i++) {
+      const int m = T.rwg[i];
+      if (m < 0) continue;
+      for (int j = 0; j < 3; j++) {
+        const int n = T.rwg[j];
+        if (n < 0) continue;
+        double v = 0;
+        for (int q = 0; q < nq; q++) {
+          double fa[3], fb[3];
+          for (int d = 0; d < 3; d++) {
+            fa[d] = T.s[i] * (T.qp[q][d] - T.p[i][d]);
+            fb[d] = T.s[j] * (T.qp[q][d] - T.p[j][d]);
+          }
+          v += wq[q] * (fa[0] * fb[0] + fa[1] * fb[1] + fa[2] * fb[2]);
+        }
+        v *= 2 * T.area;
+        acc = cadd(acc, cscale(cmul(cconj(Lr[m]), Ir[n]), v));
+      }
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 64; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] = cadd(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) g[p + r * P] = reactive ? -2.0 * red[0].y : 2.0 * red[0].x;
+}
+
+void gradient_impedance_dev(dmb_ctx *c, int64_t R, const double2 *I_dev, const double2 *L_dev,
+                            const int *tri_patch, int64_t P, int reactive, int quad_order, double *g_dev) {
+  ensure_cache(c, quad_order);
+  // patch -> triangles (CSR, triangles in increasing order within a patch)
+  std::vector<int> off(P + 1, 0), tri(c->nt);
+  for (int64_t t = 0; t < c->nt; t++) off[tri_patch[t] + 1]++;
+  for (int64_t p = 0; p < P; p++) off[p + 1] += off[p];
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int64_t t = 0; t < c->nt; t++) tri[pos[tri_patch[t]]++] = (int)t;
+  DevBuf boff, btri;
+  boff.ensure(sizeof(int) * (P + 1));
+  btri.ensure(sizeof(int) * std::max<int64_t>(1, c->nt));
+  DMB_CUDA(cudaMemcpyAsync(boff.p, off.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(btri.p, tri.data(), sizeof(int) * c->nt, cudaMemcpyHostToDevice, c->stream));
+  DMB_LAUNCH(c, k_grad_impedance, dim3((unsigned)P, (unsigned)R), 128, 0, c->n, P, c->d_tcache.as<TriCache>(),
+             c->nq, c->d_wq.as<double>(), boff.as<int>(), btri.as<int>(), I_dev, L_dev, reactive, g_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));  // the staging buffers are released on return
 }
 
 void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {

@@ -10,9 +10,11 @@ from .rwg import RWGData, build_rwg, rwg_centers, basis_triangles
 from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixFreeEFIEOperator,
                   PlaneWaveExcitation, make_plane_wave, assemble_plane_wave, assemble_excitation,
                   DipoleExcitation, LoopExcitation, make_dipole, make_loop, assemble_dipole,
-                  assemble_loop,
+                  assemble_loop, PatternFeedExcitation, make_pattern_feed, make_analytic_dipole_pattern_feed,
+                  assemble_pattern_feed,
                   assemble_multiple_excitations, build_nearfield_preconditioner, NearFieldOperator,
-                  NearFieldAdjointOperator, solve_gmres_adjoint,
+                  NearFieldAdjointOperator, solve_gmres_adjoint, solve_adjoint_rhs, PatchPartition, PatchMass,
+                  precompute_patch_mass, gradient_impedance,
                   solve_gmres, solve_forward, solve_scattering, ScatteringResult, SphGrid,
                   monostatic_rcs_sweep, MonostaticResult, BatchSurface, BatchResult,
                   SurfaceBatch, solve_surfaces,

@@ -143,6 +143,8 @@ SIGNATURES = {
     "dmb_nf_apply": ([_P, _DP, _DP, _L], _I),
     "dmb_rhs_plane_waves": ([_P, _DP, _DP, _DP, _L, _I, _DP], _I),
     "dmb_gmres": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
+    "dmb_rhs_pattern_feed": ([_P, _I, _DP, _I, _DP, _DP, _DP, _D, _DP, _I, _I, _DP], _I),
+    "dmb_gradient_impedance": ([_P, _L, _DP, _DP, _IP, _L, _I, _I, _DP], _I),
     "dmb_rhs_dipoles": ([_P, _L, _DP, _DP, _IP, _DP, _I, _DP], _I),
     "dmb_gmres_adjoint": ([_P, _DP, _DP, _L, _D, _I, _I, _I, _I, ctypes.POINTER(GmresStats)], _I),
     "dmb_solve_direct": ([_P, _DP, _DP, _L, _DP], _I),

@@ -246,6 +246,39 @@ class EFIEDevice:
                       int(quad_order), nat.dptr(V))
         return V
 
+    def pattern_feed_rhs(self, pattern: "PatternFeedExcitation", quad_order: int = 3) -> np.ndarray:
+        """assemble_pattern_feed (Excitation.jl:3044-3071) on the device; V (N,)."""
+        th = np.ascontiguousarray(pattern.theta, dtype=np.float64)
+        ph = np.ascontiguousarray(pattern.phi, dtype=np.float64)
+        ft = np.asfortranarray(pattern.Ftheta, dtype=np.complex128)
+        fp = np.asfortranarray(pattern.Fphi, dtype=np.complex128)
+        # column-major complex matrices as interleaved doubles
+        ftv = np.ascontiguousarray(np.stack([ft.real.ravel(order="F"), ft.imag.ravel(order="F")], 1).ravel())
+        fpv = np.ascontiguousarray(np.stack([fp.real.ravel(order="F"), fp.imag.ravel(order="F")], 1).ravel())
+        pc = np.ascontiguousarray(pattern.phase_center, dtype=np.float64)
+        V = np.empty(self.N, dtype=np.complex128)
+        self.ctx.call("dmb_rhs_pattern_feed", th.size, nat.dptr(th), ph.size, nat.dptr(ph), nat.dptr(ftv),
+                      nat.dptr(fpv), float(pattern.frequency), nat.dptr(pc),
+                      1 if pattern.convention == "exp_minus_iwt" else 0, int(quad_order), nat.dptr(V))
+        return V
+
+    def gradient_impedance(self, I, lam, tri_patch, P: int, reactive: bool = False,
+                           quad_order: int = 3) -> np.ndarray:
+        """gradient_impedance (Adjoint.jl:1081-1119) on the device for 0-based
+        per-triangle patch ids; I, lam (N,) or (N, R); returns (P,) or (P, R)."""
+        Ia = nat.c128(I)
+        La = nat.c128(lam)
+        if Ia.shape != La.shape or Ia.shape[0] != self.N:
+            raise ValueError(f"I and lambda must both have {self.N} rows and the same shape")
+        R = 1 if Ia.ndim == 1 else Ia.shape[1]
+        tp = np.ascontiguousarray(tri_patch, dtype=np.int32)
+        if tp.shape != (self.mesh.ntriangles,):
+            raise ValueError(f"tri_patch length {tp.size} does not match mesh triangle count {self.mesh.ntriangles}")
+        g = np.empty((int(P), R), dtype=np.float64, order="F")
+        self.ctx.call("dmb_gradient_impedance", R, nat.dptr(Ia), nat.dptr(La), nat.iptr(tp), int(P),
+                      1 if reactive else 0, int(quad_order), nat.dptr(g))
+        return g[:, 0] if Ia.ndim == 1 else g
+
     # -- batched resident solve -------------------------------------------
     _PC_CODES = {"none": nat.PRECOND_NONE, "lu": nat.PRECOND_NF_LU, "diag": nat.PRECOND_NF_DIAG,
                  "local": nat.PRECOND_LOCAL_INV, "learned": nat.PRECOND_LEARNED}
@@ -554,7 +587,126 @@ def assemble_loop(mesh, rwg, loop: LoopExcitation, quad_order=3, device=None) ->
     return assemble_dipole(mesh, rwg, loop, quad_order=quad_order, device=device)
 
 
-_EXCITATION_TYPES = (PlaneWaveExcitation, DipoleExcitation, LoopExcitation)
+@dataclass
+class PatternFeedExcitation:
+    """Excitation.jl:262-280: field synthesised from far-field coefficients on a
+    spherical grid, E(r) = exp(-ikR)/R (F_theta e_theta + F_phi e_phi) about
+    phase_center; theta/phi in radians, F of shape (len(theta), len(phi))."""
+    theta: np.ndarray
+    phi: np.ndarray
+    Ftheta: np.ndarray
+    Fphi: np.ndarray
+    frequency: float
+    phase_center: np.ndarray
+    convention: str
+
+
+_PATTERN_CONVENTIONS = ("exp_plus_iwt", "exp_minus_iwt")
+
+
+def _validate_pattern_grid(theta, phi):
+    """_validate_pattern_grid (Excitation.jl:999-1025)."""
+    if theta.size < 2:
+        raise ValueError("Pattern feed requires at least 2 theta samples.")
+    if phi.size < 2:
+        raise ValueError("Pattern feed requires at least 2 phi samples.")
+    if not np.all(np.isfinite(theta)):
+        raise ValueError("Theta grid contains non-finite values.")
+    if not np.all(np.isfinite(phi)):
+        raise ValueError("Phi grid contains non-finite values.")
+    if not np.all(np.diff(theta) > 0):
+        raise ValueError("Theta grid must be strictly increasing.")
+    if not np.all(np.diff(phi) > 0):
+        raise ValueError("Phi grid must be strictly increasing.")
+    if theta[0] < -1e-12 or theta[-1] > math.pi + 1e-12:
+        raise ValueError(f"Theta grid must lie in [0, pi] (radians). Got range [{theta[0]}, {theta[-1]}].")
+    span = phi[-1] - phi[0]
+    if span <= 0:
+        raise ValueError("Phi grid span must be positive.")
+    if span >= 2 * math.pi - 1e-12:
+        raise ValueError("Phi grid should cover one open 2 pi period without a duplicate endpoint "
+                         "(e.g., 0:d:2 pi - d).")
+
+
+def _pattern_metadata(frequency, phase_center, convention):
+    """_validated_pattern_feed_metadata (Excitation.jl:1067-1081)."""
+    f = float(frequency)
+    if not (math.isfinite(f) and f > 0.0):
+        raise ValueError(f"Pattern feed frequency must be finite and positive, got {frequency}.")
+    pc = np.asarray(phase_center, dtype=np.float64).reshape(3)
+    if not np.all(np.isfinite(pc)):
+        raise ValueError("Pattern feed phase_center must be finite.")
+    conv = str(convention).lstrip(":")
+    if conv not in _PATTERN_CONVENTIONS:
+        raise ValueError(f"Unsupported pattern convention: {convention} (expected :exp_plus_iwt or :exp_minus_iwt).")
+    return f, pc, conv
+
+
+def make_pattern_feed(theta, phi, Ftheta, Fphi, frequency, phase_center=(0.0, 0.0, 0.0),
+                      angles_in_degrees=False, convention="exp_plus_iwt") -> PatternFeedExcitation:
+    """Excitation.jl:1084-1128."""
+    f, pc, conv = _pattern_metadata(frequency, phase_center, convention)
+    th = np.array(theta, dtype=np.float64)
+    ph = np.array(phi, dtype=np.float64)
+    if angles_in_degrees:
+        th *= math.pi / 180
+        ph *= math.pi / 180
+    _validate_pattern_grid(th, ph)
+    ft = np.asarray(Ftheta, dtype=np.complex128)
+    fp = np.asarray(Fphi, dtype=np.complex128)
+    for name, m in (("Ftheta", ft), ("Fphi", fp)):
+        if m.shape != (th.size, ph.size):
+            raise ValueError(f"{name} has shape {m.shape}, expected {(th.size, ph.size)}.")
+        if not np.all(np.isfinite(m)):
+            raise ValueError(f"{name} contains non-finite coefficients.")
+    return PatternFeedExcitation(th, ph, ft.copy(), fp.copy(), f, pc, conv)
+
+
+_EPS0 = 8.854187817e-12
+_ETA0 = math.sqrt(4 * math.pi * 1e-7 / _EPS0)
+_C0_PATTERN = 299792458.0
+
+
+def _spherical_basis(theta, phi):
+    st, ct, sp, cp = np.sin(theta), np.cos(theta), np.sin(phi), np.cos(phi)
+    rhat = np.stack([st * cp, st * sp, ct], -1)
+    et = np.stack([ct * cp, ct * sp, -st], -1)
+    ep = np.stack([-sp, cp, np.zeros_like(sp)], -1)
+    return rhat, et, ep
+
+
+def make_analytic_dipole_pattern_feed(dipole: DipoleExcitation, theta, phi, phase_center=None,
+                                      angles_in_degrees=False, convention="exp_plus_iwt") -> PatternFeedExcitation:
+    """Excitation.jl:1468-1509: the dipole's far-field coefficients
+    (_dipole_farfield_unphased, :898-...) sampled on the grid; electric:
+    k^2 / (4 pi eps0) (rhat x p) x rhat, magnetic: eta0 k^2 / (4 pi) (m x rhat)."""
+    pc = dipole.position if phase_center is None else phase_center
+    f, pc, conv = _pattern_metadata(dipole.frequency, pc, convention)
+    k = 2 * math.pi * f / _C0_PATTERN
+    th = np.array(theta, dtype=np.float64)
+    ph = np.array(phi, dtype=np.float64)
+    if angles_in_degrees:
+        th *= math.pi / 180
+        ph *= math.pi / 180
+    _validate_pattern_grid(th, ph)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    rhat, et, ep = _spherical_basis(T, P)
+    p = np.asarray(dipole.moment, dtype=np.complex128)
+    if dipole.type == "electric":
+        F = np.cross(np.cross(rhat, p), rhat) * (k * k / (4 * math.pi * _EPS0))
+    else:
+        F = np.cross(p, rhat) * (_ETA0 * k * k / (4 * math.pi))
+    Ft = np.sum(F * et, -1)
+    Fp = np.sum(F * ep, -1)
+    return PatternFeedExcitation(th, ph, Ft, Fp, f, pc, conv)
+
+
+def assemble_pattern_feed(mesh, rwg, pattern: PatternFeedExcitation, quad_order=3, device=None) -> np.ndarray:
+    """Excitation.jl:3044-3071 on the device."""
+    return _with_device(mesh, rwg, device, lambda d: d.pattern_feed_rhs(pattern, quad_order))
+
+
+_EXCITATION_TYPES = (PlaneWaveExcitation, DipoleExcitation, LoopExcitation, PatternFeedExcitation)
 
 
 def assemble_excitation(mesh, rwg, excitation, quad_order=3, device=None) -> np.ndarray:
@@ -565,7 +717,7 @@ def assemble_excitation(mesh, rwg, excitation, quad_order=3, device=None) -> np.
 
 def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=None) -> np.ndarray:
     """One column per excitation; plane waves and dipoles/loops are each
-    assembled in one launch."""
+    assembled in one launch, pattern feeds one launch each."""
     excitations = list(excitations)
     for e in excitations:
         if not isinstance(e, _EXCITATION_TYPES):
@@ -574,7 +726,10 @@ def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=N
     def run(dev):
         V = np.empty((dev.N, len(excitations)), dtype=np.complex128, order="F")
         pw = [i for i, e in enumerate(excitations) if isinstance(e, PlaneWaveExcitation)]
-        dp = [i for i, e in enumerate(excitations) if not isinstance(e, PlaneWaveExcitation)]
+        dp = [i for i, e in enumerate(excitations) if isinstance(e, (DipoleExcitation, LoopExcitation))]
+        for i, e in enumerate(excitations):
+            if isinstance(e, PatternFeedExcitation):
+                V[:, i] = dev.pattern_feed_rhs(e, quad_order)
         if pw:
             es = [excitations[i] for i in pw]
             V[:, pw] = dev.plane_wave_rhs(np.stack([e.k_vec for e in es]), np.array([e.E0 for e in es]),
@@ -607,6 +762,67 @@ def solve_gmres_adjoint(device: EFIEDevice, rhs, preconditioner=None, precond_si
     near-field preconditioner."""
     return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
                         precond_side=precond_side, check_gmres_convergence=check_gmres_convergence, adjoint=True)
+
+
+def solve_adjoint_rhs(device: EFIEDevice, rhs, preconditioner=None, gmres_precond_side="left", gmres_tol=1e-8,
+                      gmres_maxiter=200, check_gmres_convergence=True, check_true_residual=True,
+                      true_residual_factor=100.0):
+    """Adjoint.jl:1029-1078 (solver=:gmres): Z^H lambda = rhs on the device;
+    with check_true_residual the FP64 residual must stay within
+    true_residual_factor x gmres_tol."""
+    lam, stats = solve_gmres_adjoint(device, rhs, preconditioner=preconditioner, precond_side=gmres_precond_side,
+                                     tol=gmres_tol, maxiter=gmres_maxiter,
+                                     check_gmres_convergence=check_gmres_convergence)
+    if check_true_residual and not (stats.true_residual <= true_residual_factor * gmres_tol):
+        raise nat.NotConvergedError(f"adjoint true residual {stats.true_residual:.3e} exceeds "
+                                f"{true_residual_factor} x tol {gmres_tol:.1e}")
+    return lam
+
+
+@dataclass
+class PatchPartition:
+    """Types.jl:1263-1280: tri_patch[t] in 1..P is the patch of triangle t."""
+    tri_patch: np.ndarray
+    P: int
+
+    def __post_init__(self):
+        self.tri_patch = np.asarray(self.tri_patch, dtype=np.int64)
+        if self.P < 0:
+            raise ValueError(f"partition.P must be nonnegative, got {self.P}")
+        if self.tri_patch.size and (self.tri_patch.min() < 1 or self.tri_patch.max() > self.P):
+            raise ValueError(f"partition.tri_patch entries must lie in 1:{self.P}")
+
+
+@dataclass
+class PatchMass:
+    """The patch mass matrices of precompute_patch_mass (Impedance.jl:304-377)
+    held implicitly: their entries are evaluated per triangle on the device
+    whenever a gradient needs them."""
+    device: EFIEDevice
+    partition: PatchPartition
+    quad_order: int
+
+    def __len__(self):
+        return self.partition.P
+
+
+def precompute_patch_mass(mesh, rwg, partition: PatchPartition, quad_order=3, device=None) -> PatchMass:
+    """Impedance.jl:304-377.  The returned object refers to `device` (a new
+    EFIEDevice for mesh / rwg when None)."""
+    if partition.tri_patch.size != mesh.ntriangles:
+        raise ValueError(f"partition.tri_patch length {partition.tri_patch.size} does not match mesh triangle "
+                         f"count {mesh.ntriangles}")
+    return PatchMass(device or EFIEDevice(mesh, rwg), partition, int(quad_order))
+
+
+def gradient_impedance(Mp: PatchMass, I, lam, reactive=False) -> np.ndarray:
+    """Adjoint.jl:1081-1119: g[p] = 2 Re(lambda^H M_p I) (resistive,
+    Z_s = theta_p) or -2 Im(lambda^H M_p I) (reactive, Z_s = i theta_p)."""
+    for name, v in (("I", I), ("lambda", lam)):
+        if not np.all(np.isfinite(np.asarray(v))):
+            raise ValueError(f"{name} must contain only finite values")
+    return Mp.device.gradient_impedance(I, lam, Mp.partition.tri_patch - 1, Mp.partition.P, reactive,
+                                        Mp.quad_order)
 
 
 def solve_forward(device: EFIEDevice, v, solver="direct"):

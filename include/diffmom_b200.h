@@ -222,6 +222,28 @@ dmb_status dmb_rhs_plane_waves(dmb_ctx *ctx, const double *kvecs, const double *
  * N x R column-major. */
 dmb_status dmb_rhs_dipoles(dmb_ctx *ctx, int64_t R, const double *positions, const double *moments,
                            const int *magnetic, const double *frequencies, int quad_order, double *V_out);
+/* assemble_pattern_feed (src/assembly/Excitation.jl:3044-3071) with the field
+ * of _pattern_feed_field_unchecked (:1417-1460): E = exp(-ikR)/R (F_theta
+ * e_theta + F_phi e_phi) about phase_center[3], k = 2 pi frequency /
+ * 299792458, F bilinear on the (theta, phi) grid (radians; theta clamped,
+ * phi periodic).  Ftheta, Fphi: ntheta x nphi column-major complex (re, im
+ * interleaved).  conj_convention = 1 for exp(-i omega t) coefficients
+ * (:exp_minus_iwt).  Grid rules of _validate_pattern_grid (:999-1025).
+ * V_out: N complex values. */
+dmb_status dmb_rhs_pattern_feed(dmb_ctx *ctx, int ntheta, const double *theta, int nphi, const double *phi,
+                                const double *Ftheta, const double *Fphi, double frequency,
+                                const double *phase_center, int conj_convention, int quad_order, double *V_out);
+
+/* ---- impedance gradients ----------------------------------------------- */
+/* gradient_impedance(Mp, I, lambda; reactive) (src/optimization/Adjoint.jl:
+ * 1081-1119) with Mp = precompute_patch_mass(mesh, rwg, partition;
+ * quad_order) (src/assembly/Impedance.jl:304-377), for R (I, lambda) pairs:
+ * g[p + r P] = 2 Re(lambda_r^H M_p I_r), or -2 Im(...) with reactive = 1.
+ * tri_patch: nt 0-based patch ids (PatchPartition.tri_patch - 1); I, lambda:
+ * N x R column-major complex (re, im interleaved); g_out: P x R doubles.
+ * The patch mass entries are evaluated on the fly per triangle. */
+dmb_status dmb_gradient_impedance(dmb_ctx *ctx, int64_t R, const double *I, const double *lambda,
+                                  const int *tri_patch, int64_t P, int reactive, int quad_order, double *g_out);
 
 /* ---- solvers ----------------------------------------------------------- */
 /* solve_gmres (src/solver/IterativeSolve.jl:341-392): GMRES without

@@ -791,6 +791,136 @@ int orc_dipole_field(const double *r, int64_t npts, const double *pos, const dou
 }
 
 /* ------------------------------------------------------------------ */
+/* Pattern feed (Excitation.jl:262-280, 1170-1340, 1417-1460):          */
+/* E(r) = exp(-ikR)/R (F_theta e_theta + F_phi e_phi), bilinear in      */
+/* (theta, phi) on the grid (theta clamped, phi periodic), k = 2 pi f / */
+/* 299792458.  F matrices column-major (ntheta x nphi), complex as      */
+/* interleaved doubles.                                                 */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int nth, nph;
+  const double *th, *ph;
+  const double *Ft, *Fp;
+  double k;
+  v3 pc;
+  int conj;
+} orc_pattern;
+
+/* largest 0-based i with g[i] <= x (g strictly increasing, x >= g[0]) */
+static int search_last(const double *g, int n, double x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) / 2;
+    if (g[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+static void bracket_theta(const double *g, int n, double x, int *i, int *j, double *t) {
+  if (x <= g[0]) { *i = *j = 0; *t = 0.0; return; }
+  if (x >= g[n - 1]) { *i = *j = n - 1; *t = 0.0; return; }
+  int a = search_last(g, n, x);
+  if (a > n - 2) a = n - 2;
+  *i = a; *j = a + 1; *t = (x - g[a]) / (g[a + 1] - g[a]);
+}
+
+static void bracket_phi(const double *g, int n, double x, int *i, int *j, double *t) {
+  const double two_pi = 2.0 * ORC_PI;
+  double r = fmod(x - g[0], two_pi);  /* floored modulo as Julia's mod */
+  if (r != 0.0 && r < 0.0) r += two_pi;
+  double w = r + g[0];
+  if (w <= g[n - 1]) {
+    int a = search_last(g, n, w);
+    if (a == n - 1) { *i = n - 1; *j = 0; *t = (w - g[n - 1]) / (g[0] + two_pi - g[n - 1]); }
+    else { *i = a; *j = a + 1; *t = (w - g[a]) / (g[a + 1] - g[a]); }
+  } else {
+    *i = n - 1; *j = 0; *t = (w - g[n - 1]) / (g[0] + two_pi - g[n - 1]);
+  }
+}
+
+static cplx pat_at(const double *M, int nth, int i, int j) {
+  return M[2 * (i + (int64_t)j * nth)] + I * M[2 * (i + (int64_t)j * nth) + 1];
+}
+
+static cplx pat_bilinear(const double *M, int nth, int it, int jt, double tt, int ip, int jp, double tp) {
+  if (it == jt && ip == jp) return pat_at(M, nth, it, ip);
+  if (it == jt) return (1 - tp) * pat_at(M, nth, it, ip) + tp * pat_at(M, nth, it, jp);
+  if (ip == jp) return (1 - tt) * pat_at(M, nth, it, ip) + tt * pat_at(M, nth, jt, ip);
+  return (1 - tt) * (1 - tp) * pat_at(M, nth, it, ip) + tt * (1 - tp) * pat_at(M, nth, jt, ip) +
+         (1 - tt) * tp * pat_at(M, nth, it, jp) + tt * tp * pat_at(M, nth, jt, jp);
+}
+
+static void pattern_field(v3 r, const orc_pattern *P, cplx *E) {
+  v3 d = {r.x - P->pc.x, r.y - P->pc.y, r.z - P->pc.z};
+  double R = hypot(hypot(d.x, d.y), d.z);
+  if (R == 0.0) { E[0] = E[1] = E[2] = 0.0; return; }
+  double c = d.z / R;
+  if (c < -1.0) c = -1.0;
+  if (c > 1.0) c = 1.0;
+  double th = acos(c), ph = atan2(d.y, d.x);
+  if (ph < 0) ph += 2.0 * ORC_PI;
+  double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+  double et[3] = {ct * cp, ct * sp, -st}, ep[3] = {-sp, cp, 0.0};
+  int it, jt, ip, jp;
+  double tt, tp;
+  bracket_theta(P->th, P->nth, th, &it, &jt, &tt);
+  bracket_phi(P->ph, P->nph, ph, &ip, &jp, &tp);
+  cplx Ft = pat_bilinear(P->Ft, P->nth, it, jt, tt, ip, jp, tp);
+  cplx Fp = pat_bilinear(P->Fp, P->nth, it, jt, tt, ip, jp, tp);
+  if (P->conj) { Ft = conj(Ft); Fp = conj(Fp); }
+  cplx phase = cos(-P->k * R) + I * sin(-P->k * R);
+  for (int a = 0; a < 3; a++) E[a] = ((Ft * et[a] + Fp * ep[a]) / R) * phase;
+}
+
+static orc_pattern make_pattern(int nth, const double *th, int nph, const double *ph, const double *Ft,
+                                const double *Fp, double freq, const double *pc, int conj_conv) {
+  orc_pattern P = {nth, nph, th, ph, Ft, Fp, 2.0 * ORC_PI * freq / 299792458.0, {pc[0], pc[1], pc[2]}, conj_conv};
+  return P;
+}
+
+/* assemble_pattern_feed (Excitation.jl:3044-3071) */
+int orc_pattern_rhs(const orc_cache *c, int nth, const double *th, int nph, const double *ph, const double *Ft,
+                    const double *Fp, double freq, const double *pc, int conj_conv, double *v) {
+  orc_pattern P = make_pattern(nth, th, nph, ph, Ft, Fp, freq, pc, conj_conv);
+  int64_t N = c->n;
+  int nq = c->nq;
+  for (int64_t n = 0; n < N; n++) {
+    cplx acc = 0.0;
+    for (int s = 0; s < 2; s++) {
+      int64_t t = (s == 0 ? c->tplus[n] : c->tminus[n]) - 1;
+      double A = c->area[t];
+      for (int q = 0; q < nq; q++) {
+        v3 rq = c->qp[t * nq + q];
+        v3 fn = c->fv[(n * 2 + s) * nq + q];
+        cplx E[3];
+        pattern_field(rq, &P, E);
+        cplx ip = fn.x * E[0] + fn.y * E[1] + fn.z * E[2];
+        acc += -(2 * c->wq[q]) * (A * ip);
+      }
+    }
+    v[2 * n] = creal(acc);
+    v[2 * n + 1] = cimag(acc);
+  }
+  return 0;
+}
+
+/* pattern_feed_field at points r (npts x 3) for the tests */
+int orc_pattern_field(const double *r, int64_t npts, int nth, const double *th, int nph, const double *ph,
+                      const double *Ft, const double *Fp, double freq, const double *pc, int conj_conv, double *E) {
+  orc_pattern P = make_pattern(nth, th, nph, ph, Ft, Fp, freq, pc, conj_conv);
+  for (int64_t i = 0; i < npts; i++) {
+    v3 rr = {r[3 * i], r[3 * i + 1], r[3 * i + 2]};
+    cplx e[3];
+    pattern_field(rr, &P, e);
+    for (int a = 0; a < 3; a++) {
+      E[6 * i + 2 * a] = creal(e[a]);
+      E[6 * i + 2 * a + 1] = cimag(e[a]);
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Per-triangle surface-impedance loading (Impedance.jl:304-408)       */
 /* Z[m,n] -= zs[t] * sum_q w_q f_m.f_n (2 A_t)                          */
 /* ------------------------------------------------------------------ */
@@ -819,6 +949,45 @@ int orc_apply_impedance(const orc_cache *c, const double *zs, double *Z) {
         Z[2 * (m + n * N) + 1] = cimag(z);
       }
   }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* gradient_impedance (optimization/Adjoint.jl:1081-1119) with the patch */
+/* mass matrices of precompute_patch_mass (Impedance.jl:304-377):        */
+/* s_p = lambda^H M_p I, g_p = 2 Re s_p (resistive) or -2 Im s_p          */
+/* (reactive); tri_patch 0-based, I / lambda / g column-major (R cols).   */
+/* ------------------------------------------------------------------ */
+int orc_gradient_impedance(const orc_cache *c, int64_t R, const double *Iv, const double *Lv,
+                           const int *tri_patch, int64_t P, int reactive, double *g) {
+  int64_t N = c->n;
+  int nq = c->nq;
+  cplx *acc = (cplx *)calloc((size_t)(P * R), sizeof(cplx));
+  if (!acc) return 1;
+  for (int64_t t = 0; t < c->nt; t++) {
+    int64_t ids[6]; int sides[6]; int cnt = 0;
+    for (int64_t n = 0; n < N && cnt < 6; n++) {
+      if (c->tplus[n] - 1 == t) { ids[cnt] = n; sides[cnt++] = 0; }
+      else if (c->tminus[n] - 1 == t) { ids[cnt] = n; sides[cnt++] = 1; }
+    }
+    int64_t p = tri_patch[t];
+    for (int i = 0; i < cnt; i++)
+      for (int j = 0; j < cnt; j++) {
+        double val = 0.0;
+        for (int q = 0; q < nq; q++) {
+          v3 fa = c->fv[(ids[i] * 2 + sides[i]) * nq + q], fb = c->fv[(ids[j] * 2 + sides[j]) * nq + q];
+          val += c->wq[q] * v3dot(fa, fb);
+        }
+        val *= 2 * c->area[t];
+        for (int64_t r = 0; r < R; r++) {
+          int64_t m = ids[i] + r * N, n = ids[j] + r * N;
+          cplx lm = Lv[2 * m] + I * Lv[2 * m + 1], in = Iv[2 * n] + I * Iv[2 * n + 1];
+          acc[p + r * P] += conj(lm) * val * in;
+        }
+      }
+  }
+  for (int64_t i = 0; i < P * R; i++) g[i] = reactive ? -2.0 * cimag(acc[i]) : 2.0 * creal(acc[i]);
+  free(acc);
   return 0;
 }
 

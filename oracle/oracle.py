@@ -68,7 +68,10 @@ def lib():
         L.orc_plane_wave_rhs.argtypes = [_P, _DP, _D, _DP, _DP]
         L.orc_dipole_rhs.argtypes = [_P, _DP, _DP, _I, _D, _DP]
         L.orc_dipole_field.argtypes = [_DP, _L, _DP, _DP, _I, _D, _DP]
+        L.orc_pattern_rhs.argtypes = [_P, _I, _DP, _I, _DP, _DP, _DP, _D, _DP, _I, _DP]
+        L.orc_pattern_field.argtypes = [_DP, _L, _I, _DP, _I, _DP, _DP, _DP, _D, _DP, _I, _DP]
         L.orc_apply_impedance.argtypes = [_P, _DP, _DP]
+        L.orc_gradient_impedance.argtypes = [_P, _L, _DP, _DP, ctypes.POINTER(ctypes.c_int), _L, _I, _DP]
         L.orc_radiation_vectors.argtypes = [_P, _DP, _L, _D, _D, _DP]
         L.orc_adjacent_pair_count.restype = _L
         L.orc_adjacent_pair_count.argtypes = [_P]
@@ -197,6 +200,30 @@ class OracleCache:
                              float(frequency), _d(v))
         return v
 
+    def pattern_rhs(self, theta, phi, Ftheta, Fphi, frequency, phase_center=(0.0, 0.0, 0.0),
+                    conj_convention=False) -> np.ndarray:
+        """assemble_pattern_feed (Excitation.jl:3044-3071); angles in radians,
+        F matrices (ntheta, nphi); conj_convention for exp(-i omega t) data."""
+        a = _pattern_args(theta, phi, Ftheta, Fphi)
+        v = np.zeros(self.N, dtype=np.complex128)
+        lib().orc_pattern_rhs(self.h, a[0], _d(a[1]), a[2], _d(a[3]), _d(a[4]), _d(a[5]), float(frequency),
+                              _d(_v3(phase_center)), 1 if conj_convention else 0, _d(v))
+        return v
+
+    def gradient_impedance(self, I, lam, tri_patch, P, reactive=False) -> np.ndarray:
+        """gradient_impedance (Adjoint.jl:1081-1119) for per-triangle patch ids
+        (0-based); I, lam (N,) or (N, R); returns (P,) or (P, R)."""
+        Ia = np.asfortranarray(np.asarray(I, dtype=np.complex128).reshape(self.N, -1))
+        La = np.asfortranarray(np.asarray(lam, dtype=np.complex128).reshape(self.N, -1))
+        tp = np.ascontiguousarray(tri_patch, dtype=np.int32)
+        R = Ia.shape[1]
+        g = np.zeros((int(P), R), dtype=np.float64, order="F")
+        rc = lib().orc_gradient_impedance(self.h, R, _d(Ia), _d(La), tp.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                          int(P), 1 if reactive else 0, _d(g))
+        if rc != 0:
+            raise MemoryError("oracle gradient: allocation failed")
+        return g[:, 0] if np.asarray(I).ndim == 1 else g
+
     def apply_impedance(self, Z: np.ndarray, zs) -> np.ndarray:
         Zc = np.asfortranarray(Z.copy())
         zsa = np.ascontiguousarray(np.broadcast_to(np.asarray(zs, dtype=np.complex128),
@@ -220,6 +247,28 @@ def dipole_field(points, position, moment, dipole_type="electric", frequency=1e9
     E = np.zeros((r.shape[0], 3), dtype=np.complex128)
     lib().orc_dipole_field(_d(r), r.shape[0], _d(_v3(position)), _d(mm), 1 if dipole_type == "magnetic" else 0,
                            float(frequency), _d(E))
+    return E
+
+
+def _pattern_args(theta, phi, Ftheta, Fphi):
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    ph = np.ascontiguousarray(phi, dtype=np.float64)
+    ft = np.asfortranarray(np.asarray(Ftheta, dtype=np.complex128).reshape(th.size, ph.size))
+    fp = np.asfortranarray(np.asarray(Fphi, dtype=np.complex128).reshape(th.size, ph.size))
+    # column-major complex matrices as interleaved doubles
+    ftv = np.ascontiguousarray(np.stack([ft.real.ravel(order="F"), ft.imag.ravel(order="F")], 1).ravel())
+    fpv = np.ascontiguousarray(np.stack([fp.real.ravel(order="F"), fp.imag.ravel(order="F")], 1).ravel())
+    return th.size, th, ph.size, ph, ftv, fpv
+
+
+def pattern_field(points, theta, phi, Ftheta, Fphi, frequency, phase_center=(0.0, 0.0, 0.0),
+                  conj_convention=False) -> np.ndarray:
+    """_pattern_feed_field_unchecked (Excitation.jl:1417-1460) at points (n x 3)."""
+    r = np.ascontiguousarray(np.atleast_2d(points), dtype=np.float64)
+    a = _pattern_args(theta, phi, Ftheta, Fphi)
+    E = np.zeros((r.shape[0], 3), dtype=np.complex128)
+    lib().orc_pattern_field(_d(r), r.shape[0], a[0], _d(a[1]), a[2], _d(a[3]), _d(a[4]), _d(a[5]),
+                            float(frequency), _d(_v3(phase_center)), 1 if conj_convention else 0, _d(E))
     return E
 
 
