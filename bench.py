@@ -64,10 +64,9 @@ K = 2 * math.pi * FREQ / C0
 R_WAVES = 1024
 SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
-# DRAM bytes per launch of the tensor-core GEMM family (k_tc_syrk + k_tc_gemm)
-# on the headline step, measured with ncu one-pass dram__bytes_read/write.sum
-# over every launch of one step: 104.4 GB in 288 launches
-TC_TRAFFIC_PER_LAUNCH = 104.4e9 / 288
+# DRAM bytes per k_oz_gemm launch on the headline step, measured with ncu
+# one-pass dram__bytes_read/write.sum over the 3 launches of one step
+OZ_TRAFFIC_PER_LAUNCH = 44767341312 / 3  # 3 launches: 13.857 + 13.854 + 17.056 GB
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
@@ -461,36 +460,43 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         "gpu_launches": int(head["launches"]) if head else 0,
     }
     if head is not None:
-        fams = {"k_tc_gemm (Krylov / triangular-sweep GEMMs)": head["kernel_gemm"],
-                "k_tc_syrk + k_tc_pack (factorisation trailing updates)": head["kernel_factor"]}
-        kms = sum(f[0] for f in fams.values())
-        kl = sum(f[1] for f in fams.values())
-        kf = sum(f[2] for f in fams.values())
-        achieved = (kf / 1e12) / (kms / 1e3) if kms > 0 else 0.0
-        line["roofline"] = {
-            "kernel": "k_tc_gemm + k_tc_syrk (tcgen05 3xTF32 complex GEMMs: Z X, panel and factor updates)",
-            "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-            "frac": achieved / bf16 if bf16 else None,
-            "traffic": TC_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
-            "traffic_note": "DRAM bytes per launch (ncu, one-pass dram__bytes metrics, headline step)",
-            "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic complex flops (8 per "
-                           f"complex MAC), the 3xTF32 split executes 3x that at half the bf16 rate",
-            "launches_timed": kl, "kernel_ms_total": kms,
-            "kernel_share_of_step": kms / (head["ms_per_step"] * head["steps"]),
-            "families": {name: {"achieved": (f[2] / 1e12) / (f[0] / 1e3) if f[0] > 0 else 0.0,
-                                "frac": (f[2] / 1e12) / (f[0] / 1e3) / bf16 if f[0] > 0 and bf16 else None,
-                                "launches_timed": f[1], "kernel_ms_total": f[0]}
-                         for name, f in fams.items()}}
+        # dominant kernel: k_oz_gemm, the Z X products of block GMRES (two
+        # Krylov products and the final true residual per step, R columns each)
         ims, il, iw = head["kernel_int8"]
         if il > 0:
-            line["roofline_int8"] = {
-                "kernel": "k_oz_gemm (FP64-accurate Z X from exact int8 slice products, tcgen05 kind::i8)",
-                "bound": "tensor", "achieved": (iw / 1e15) / (ims / 1e3), "peak": 4.5, "unit": "POPS (int8)",
-                "frac": (iw / 1e15) / (ims / 1e3) / 4.5,
-                "peak_source": "nominal dense INT8 (not in MEASURED_PEAKS.json)",
-                "traffic": 17.06e9 if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
+            alg = il * 8.0 * N * N * R_WAVES  # 8 flops per complex MAC, counted once
+            achieved = (alg / 1e12) / (ims / 1e3)
+            line["roofline"] = {
+                "kernel": "k_oz_gemm (Z X with R = %d columns: FP64-accurate complex GEMM from int8 slice "
+                          "products on tcgen05 kind::i8)" % R_WAVES,
+                "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved / bf16 if bf16 else None,
+                "traffic": OZ_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
+                "traffic_note": "DRAM bytes per launch (ncu one-pass dram__bytes metrics, the 3 launches of a "
+                                "headline step)",
+                "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic flops 8 N^2 R per launch "
+                               "(complex MAC = 8 real flops, counted once however the product is executed)",
                 "launches_timed": il, "kernel_ms_total": ims,
-                "kernel_share_of_step": ims / (head["ms_per_step"] * head["steps"])}
+                "kernel_share_of_step": ims / (head["ms_per_step"] * head["steps"]),
+                "executed_int8": {"achieved_pops": (iw / 1e15) / (ims / 1e3), "peak_pops": 4.5,
+                                  "frac": (iw / 1e15) / (ims / 1e3) / 4.5,
+                                  "peak_source": "nominal dense INT8 (not in MEASURED_PEAKS.json)",
+                                  "note": "21 (Krylov) or 26 (residual) int8 slice products of the "
+                                          "real-stacked (2N x 2N) x (2N x R) system per launch"}}
+        fams = {"k_tc_gemm (triangular-sweep GEMMs)": head["kernel_gemm"],
+                "k_tc_syrk + k_tc_pack (factorisation trailing updates)": head["kernel_factor"]}
+        line["roofline_tc"] = {
+            "kernel": "tcgen05 3xTF32 complex GEMMs of the preconditioner (build and apply)",
+            "bound": "tensor", "peak": bf16, "unit": "TFLOP/s",
+            "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic complex flops (8 per complex "
+                           "MAC), the 3xTF32 split executes 3x that at half the bf16 rate",
+            "note": "factor updates run on two side streams beside the panel chain: their event times "
+                    "include time shared with concurrent kernels",
+            "families": {name: {"achieved": (f[2] / 1e12) / (f[0] / 1e3) if f[0] > 0 else 0.0,
+                                "frac": (f[2] / 1e12) / (f[0] / 1e3) / bf16 if f[0] > 0 and bf16 else None,
+                                "launches_timed": f[1], "kernel_ms_total": f[0],
+                                "kernel_share_of_step": f[0] / (head["ms_per_step"] * head["steps"])}
+                         for name, f in fams.items()}}
         line["clocks"] = head.get("clocks")
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(seconds=args.cpu_seconds)
