@@ -226,7 +226,17 @@ dmb_status dmb_rwg_upload(dmb_ctx *c, int64_t n, const int64_t *tplus, const int
     up(c->d_len, c->h_len.data(), 8 * n);
     up(c->d_ap, c->h_ap.data(), 8 * n);
     up(c->d_am, c->h_am.data(), 8 * n);
-    dmb::build_host_topology(c);
+    // the edge adjacency, basis slots and near-field records depend only on
+    // the triangles and the RWG triangle pairs: an identical re-upload keeps them
+    if (!(c->topo_valid && c->topo_tri == c->h_tri && c->topo_tplus == c->h_tplus &&
+          c->topo_tminus == c->h_tminus)) {
+      c->topo_valid = false;
+      dmb::build_host_topology(c);
+      c->topo_tri = c->h_tri;
+      c->topo_tplus = c->h_tplus;
+      c->topo_tminus = c->h_tminus;
+      c->topo_valid = true;
+    }
     c->have_rwg = true;
     c->cache_valid = false;
     c->z_valid = false;

@@ -168,6 +168,9 @@ struct dmb_ctx {
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves
+  // inputs of the current host topology (build_host_topology)
+  bool topo_valid = false;
+  std::vector<int32_t> topo_tri, topo_tplus, topo_tminus;
   DevBuf d_trsm_id;              // scratch: inverses of the 1024-row diagonal blocks of L
   DevBuf d_trsm_t;               // scratch: products of the recursive-doubling levels
   int gm_kcap = 0;              // cached GMRES basis capacity

@@ -957,15 +957,17 @@ def monostatic_rcs_sweep(mesh: TriMesh, freq_hz, excitations, precision: str = "
     exc = list(excitations)
     if not exc or not all(isinstance(e, PlaneWaveExcitation) for e in exc):
         raise ValueError("monostatic_rcs_sweep: excitations must be a non-empty list of plane waves")
-    for e in exc:
-        if abs(float(np.linalg.norm(e.k_vec)) - k) > 1e-8 * k:
-            raise ValueError("monostatic_rcs_sweep: plane-wave |k_vec| must equal 2*pi*freq/c0")
+    kvecs = np.array([e.k_vec for e in exc], dtype=np.float64)
+    pols = np.array([e.pol for e in exc], dtype=np.float64)
+    e0s = np.array([e.E0 for e in exc], dtype=np.float64)
+    if np.any(np.abs(np.linalg.norm(kvecs, axis=1) - k) > 1e-8 * k):
+        raise ValueError("monostatic_rcs_sweep: plane-wave |k_vec| must equal 2*pi*freq/c0")
     rwg = rwg if rwg is not None else build_rwg(mesh)
     dev = device or EFIEDevice(mesh, rwg)
     own = device is None
     try:
         lam = c0 / f
-        sig, st = dev.solve_many(k, [e.k_vec for e in exc], [e.pol for e in exc], [e.E0 for e in exc],
+        sig, st = dev.solve_many(k, kvecs, pols, e0s,
                                  precision=precision, preconditioner=preconditioner,
                                  cutoff=nf_cutoff_lambda * lam, tol=gmres_tol, maxiter=gmres_maxiter,
                                  precond_side=precond_side, quad_order=quad_order)
