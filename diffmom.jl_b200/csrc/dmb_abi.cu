@@ -94,6 +94,9 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->stream3) cudaStreamDestroy(c->stream3);
+    if (c->stream_aux) cudaStreamDestroy(c->stream_aux);
+    for (auto &e : c->aux_ev)
+      if (e) cudaEventDestroy(e);
     for (auto &e : c->la_ev)
       if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
@@ -595,12 +598,37 @@ void check_solve_params(const dmb_solve_params *p) {
 }
 
 // assemble (+ surface impedance) + preconditioner of the resident solves
+void resident_precond(dmb_ctx *c, const dmb_solve_params *p);
+
 void resident_setup(dmb_ctx *c, const dmb_solve_params *p, const double *zs = nullptr) {
   dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
   if (zs) {
     check_finite(zs, 2 * c->nt, "surface impedance");
     dmb::apply_impedance(c, zs);
   }
+  resident_precond(c, p);
+}
+
+// the auxiliary stream starts after everything issued so far on the context
+// stream; aux_join orders the context stream after the auxiliary work
+void aux_fork(dmb_ctx *c) {
+  if (!c->stream_aux) {
+    int least = 0, greatest = 0;
+    DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    DMB_CUDA(cudaStreamCreateWithPriority(&c->stream_aux, cudaStreamNonBlocking, least));
+  }
+  for (auto &e : c->aux_ev)
+    if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  DMB_CUDA(cudaEventRecord(c->aux_ev[0], c->stream));
+  DMB_CUDA(cudaStreamWaitEvent(c->stream_aux, c->aux_ev[0], 0));
+}
+
+void aux_join(dmb_ctx *c) {
+  DMB_CUDA(cudaEventRecord(c->aux_ev[1], c->stream_aux));
+  DMB_CUDA(cudaStreamWaitEvent(c->stream, c->aux_ev[1], 0));
+}
+
+void resident_precond(dmb_ctx *c, const dmb_solve_params *p) {
   if (p->precond_kind == DMB_PRECOND_NF_LU || p->precond_kind == DMB_PRECOND_NF_DIAG) {
     DMB_REQUIRE(!std::isnan(p->cutoff) && p->cutoff >= 0, DMB_ERR_ARGUMENT,
                 "near-field cutoff must be nonnegative and not NaN");
@@ -658,12 +686,22 @@ dmb_status dmb_solve_resident_many(dmb_ctx *c, const dmb_solve_params *p, int64_
       DMB_REQUIRE(E0s[r] != 0.0 || !sigma_out, DMB_ERR_ARGUMENT, "RCS needs a nonzero incident amplitude");
     }
     double t0 = dmb::now_ms();
-    resident_setup(c, p);
+    dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
     const size_t bytes = sizeof(double2) * c->n * R;
     c->d_rhs.ensure(bytes);
     c->d_sol.ensure(bytes);
     c->sol_r = 0;
-    dmb::rhs_plane_waves_dev(c, kvecs, E0s, pols, R, p->quad_order, c->d_rhs.as<double>());
+    // the right-hand sides and the int8 slices of Z need only Z and the mesh:
+    // they run on the auxiliary stream beside the preconditioner build
+    aux_fork(c);
+    {
+      StreamSwap sw(c, c->stream_aux);
+      dmb::rhs_plane_waves_async(c, kvecs, E0s, pols, R, p->quad_order, c->d_rhs.as<double>());
+      if (dmb::krylov_exact_int8(c, R)) dmb::oz_prepare(c);
+    }
+    resident_precond(c, p);
+    aux_join(c);
+    c->tm.rhs_ms = 0.0;  // overlapped with the preconditioner build
     dmb::gmres_dev(c, c->d_rhs.as<double>(), c->d_sol.as<double>(), R, p->tol, p->maxiter, p->precond_kind,
                    p->precond_side, &st);
     c->sol_r = R;

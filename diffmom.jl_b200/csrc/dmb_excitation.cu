@@ -526,6 +526,16 @@ void near_values(dmb_ctx *c, double k, double inv_k2);
 void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols, int64_t R,
                          int quad_order, double *V_dev) {
   double t0 = now_ms();
+  rhs_plane_waves_async(c, kvecs, E0s, pols, R, quad_order, V_dev);
+  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  c->tm.rhs_ms = now_ms() - t0;
+}
+
+// the same without the final host synchronisation (the staging copies of the
+// incidence data have completed when it returns: they come from pageable
+// host memory)
+void rhs_plane_waves_async(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols, int64_t R,
+                           int quad_order, double *V_dev) {
   ensure_cache(c, quad_order);
   c->d_small.ensure(std::max<size_t>(65536, 64 + sizeof(double) * 7 * R));
   double *dk = (double *)((char *)c->d_small.p + 64), *de = dk + 3 * R, *dp = de + R;
@@ -534,8 +544,6 @@ void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, con
   DMB_CUDA(cudaMemcpyAsync(dp, pols, 24 * R, cudaMemcpyHostToDevice, c->stream));
   DMB_LAUNCH(c, k_plane_wave, blocks_for(c->n * R, 128), 128, 0, c->n, R, c->d_tcache.as<TriCache>(),
              c->d_rwg_slot.as<int>(), c->nq, c->d_wq.as<double>(), dk, de, dp, (double2 *)V_dev);
-  DMB_CUDA(cudaStreamSynchronize(c->stream));
-  c->tm.rhs_ms = now_ms() - t0;
 }
 
 void farfield_dev(dmb_ctx *c, const double *rhat, int64_t NO, double k, double eta0, int quad_order,

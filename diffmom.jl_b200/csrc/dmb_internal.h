@@ -96,6 +96,10 @@ struct dmb_ctx {
   // block column
   cudaStream_t stream2 = nullptr, stream3 = nullptr;
   cudaEvent_t la_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // work that only needs Z (right-hand sides, int8 slices of Z) runs here
+  // beside the factorisation (created on first use, low priority)
+  cudaStream_t stream_aux = nullptr;
+  cudaEvent_t aux_ev[2] = {nullptr, nullptr};
   std::mutex mu;
   std::string err;
   int sm_count = 148;
@@ -257,6 +261,8 @@ void nf_build(dmb_ctx *c, double cutoff, int kind);
 void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs);             // in place, c128 device
 void rhs_plane_waves_dev(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols,
                          int64_t R, int quad_order, double *V_dev);
+void rhs_plane_waves_async(dmb_ctx *c, const double *kvecs, const double *E0s, const double *pols, int64_t R,
+                           int quad_order, double *V_dev);
 void rhs_dipoles_dev(dmb_ctx *c, int64_t R, const double *pos, const double *moments, const int *magnetic,
                      const double *freqs, int quad_order, double *V_dev);
 void rhs_pattern_dev(dmb_ctx *c, int nth, const double *theta, int nph, const double *phi, const double *Ft,
@@ -284,10 +290,12 @@ unsigned tc_error_word(dmb_ctx *c);
 void tc_release(dmb_ctx *c);
 // FP64-accurate complex64 Z X on the INT8 tensor cores (dmb_ozaki.cu)
 bool oz_available(dmb_ctx *c);
+bool krylov_exact_int8(dmb_ctx *c, int64_t nrhs);  // the Krylov product is the INT8-slice one
 // lmax: slice-pair levels p + q <= lmax are kept (6: 26 int8 products, ~7e-13
 // normwise; 5: 21 products, ~4e-11 -- enough for the Krylov recurrence)
 constexpr int OZ_LEVELS_RESIDUAL = 6, OZ_LEVELS_KRYLOV = 5;
 void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax = OZ_LEVELS_RESIDUAL);
+void oz_prepare(dmb_ctx *c);
 unsigned oz_error_word(dmb_ctx *c);
 void oz_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);

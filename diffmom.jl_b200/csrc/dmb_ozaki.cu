@@ -374,11 +374,13 @@ bool oz_available(dmb_ctx *c) {
   return 16129.0 * (double)K < 2147483647.0;
 }
 
-void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
-  DMB_REQUIRE(lmax >= 0 && lmax <= OZ_LMAX, DMB_ERR_ARGUMENT, "int8 slice levels out of range");
+// Slices of the current Z (row scales, six int8 slices, tensor map), made
+// once per Z; may run on another stream ahead of the first product, which
+// must then be ordered after it.
+void oz_prepare(dmb_ctx *c) {
   DMB_REQUIRE(oz_available(c), DMB_ERR_STATE, "int8 tensor-core product unavailable for this matrix");
   OzState &st = oz_state(c);
-  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64), Rpad = round_up(R, OZ_BN);
+  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64);
   const int64_t ld = 2 * Kh;
   if (!st.err.p) {
     st.err.ensure(16);
@@ -399,6 +401,14 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
     st.a_version = c->z_version;
     st.a_n = N;
   }
+}
+
+void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
+  DMB_REQUIRE(lmax >= 0 && lmax <= OZ_LMAX, DMB_ERR_ARGUMENT, "int8 slice levels out of range");
+  oz_prepare(c);
+  OzState &st = oz_state(c);
+  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64), Rpad = round_up(R, OZ_BN);
+  const int64_t ld = 2 * Kh;
   st.cs.ensure(sizeof(double) * Rpad);
   st.B.ensure((size_t)OZ_S * Rpad * ld);
   if (st.b_key != Rpad || st.b_n != N) {
