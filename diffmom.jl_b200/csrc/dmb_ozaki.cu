@@ -21,7 +21,9 @@
 // product is ~7e-13 relative (normwise) on EFIE rows; the Krylov products of
 // GMRES keep levels <= 5 (21 products, ~4e-11), the true residuals all levels.
 //
-// Kernel k_oz_gemm: one CTA per 64 x 256 complex output tile, 6 warps:
+// Kernel k_oz_gemm: a persistent grid (one CTA per SM) over 64 x 256 complex
+// output tiles -- whole tiles in data-parallel waves, the tail tiles split
+// stream-K and summed by k_oz_fixup -- 6 warps per CTA:
 //   warp 4 / lane 0   TMA producer over (pair, K chunk) into a 4-stage ring of
 //                     128-byte-swizzled int8 stages (A 128 x 128 B, B 256 x 128 B);
 //   warp 5 / lane 0   tcgen05.mma.kind::i8 (M 128, N 256, K 32) into two
@@ -31,6 +33,7 @@
 //   warps 0-3         drain each level: tcgen05.ld, scale, FP64 store / add.
 // Every wait is bounded (error bit, abort flag, TMEM freed); no multicast.
 #include <algorithm>
+#include <vector>
 #include <cmath>
 
 #include "dmb_device.cuh"
@@ -55,11 +58,11 @@ constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(O
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
 struct OzSched {
-  int n, ngroups;
+  int n;
   int arow[OZ_MAXP];      // first A'' row of the pair's Z slice
   int brow[OZ_MAXP];      // first B'' row of the pair's X slice
   int close[OZ_MAXP];     // 1: the TMEM sum is drained after this pair
-  double gscale[OZ_MAXP]; // per drain: 2^(-7 (L + 2))
+  double lscale[OZ_MAXP]; // weight of the pair's level: 2^(-7 (L + 2))
 };
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -77,15 +80,60 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// Persistent grid of G CTAs over ntiles output tiles (column tile fastest).
+// The first nfull = ntiles / G waves are data-parallel: CTA b computes tiles
+// b, b + G, ... whole, so the CTAs running together share the Z slices of a
+// row of tiles in L2.  The remaining tail tiles are split stream-K: their
+// units (tile, slice pair) are cut into G equal ranges; a range's segment that
+// covers a whole tile writes Y, the (at most two) partial segments of a range
+// go to the CTA's workspace slots, and k_oz_fixup sums each tile's partials in
+// CTA order.  Every role walks the same sequence of segments and of drain
+// groups (a level's pairs, cut at sc.close and at the segment end).
+struct OzSeg {
+  int64_t t;
+  int p0, p1, slot;  // slot -1: whole tile into Y
+};
+struct OzIter {
+  int64_t wave, nfull, b, G, u, u_end;
+  int n, slot;
+};
+__device__ __forceinline__ void oz_iter_init(OzIter &it, int64_t ntiles, int n) {
+  it.G = gridDim.x;
+  it.b = blockIdx.x;
+  it.n = n;
+  it.wave = 0;
+  it.nfull = ntiles / it.G;
+  const int64_t F = it.nfull * it.G, Wt = (ntiles - F) * n;
+  it.u = F * n + Wt * it.b / it.G;
+  it.u_end = F * n + Wt * (it.b + 1) / it.G;
+  it.slot = 0;
+}
+__device__ __forceinline__ bool oz_next_seg(OzIter &it, OzSeg &sg) {
+  if (it.wave < it.nfull) {
+    sg.t = it.wave * it.G + it.b;
+    sg.p0 = 0;
+    sg.p1 = it.n;
+    sg.slot = -1;
+    it.wave++;
+    return true;
+  }
+  if (it.u >= it.u_end) return false;
+  sg.t = it.u / it.n;
+  sg.p0 = (int)(it.u - sg.t * it.n);
+  sg.p1 = (int)min((int64_t)it.n, it.u_end - sg.t * it.n);
+  it.u = sg.t * it.n + sg.p1;
+  sg.slot = (sg.p0 == 0 && sg.p1 == it.n) ? -1 : it.slot++;
+  return true;
+}
+constexpr int OZ_TILE_ELEMS = 64 * OZ_BN;  // complex outputs per tile (workspace slot size)
+
 __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB,
                                                     const __grid_constant__ OzSched sc, int kchunks, int64_t M,
-                                                    int64_t Rv, double2 *__restrict__ Y, int64_t ldy,
+                                                    int64_t Rv, double2 *__restrict__ Y, double2 *__restrict__ P,
+                                                    int64_t ldy, int ncol, int64_t ntiles,
                                                     const double *__restrict__ rs, const double *__restrict__ cs,
                                                     unsigned *err) {
-  const int64_t col0 = (int64_t)blockIdx.x * OZ_BN;
-  const int64_t row0 = (int64_t)blockIdx.y * 64;
-  if (row0 >= M || col0 >= Rv) return;  // uniform
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -129,14 +177,24 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
   if (warp == 4) {
     if (lane == 0) {
       long long t = 0;
-      for (int i = 0; i < sc.n && !*abort_flag; i++) {
-        for (int kc = 0; kc < kchunks; kc++, t++) {
-          const int s = (int)(t % OZ_STAGES);
-          if (t >= OZ_STAGES && !mbar_wait(empty0 + 8 * s, (uint32_t)((t / OZ_STAGES) - 1) & 1u, err, abort_flag))
-            break;
-          mbar_expect_tx(full0 + 8 * s, OZ_A_STAGE + OZ_B_STAGE);
-          tma_load_2d(sA + s * OZ_A_STAGE, &tmA, kc * OZ_BK, sc.arow[i] + (int)(2 * row0), full0 + 8 * s);
-          tma_load_2d(sB + s * OZ_B_STAGE, &tmB, kc * OZ_BK, sc.brow[i] + (int)col0, full0 + 8 * s);
+      OzIter it;
+      oz_iter_init(it, ntiles, sc.n);
+      OzSeg sg;
+      bool go = true;
+      while (go && oz_next_seg(it, sg)) {
+        const int row2 = (int)(2 * 64 * (sg.t / ncol)), colb = (int)(OZ_BN * (sg.t % ncol));
+        for (int i = sg.p0; i < sg.p1 && go; i++) {
+          for (int kc = 0; kc < kchunks; kc++, t++) {
+            const int s = (int)(t % OZ_STAGES);
+            if (*abort_flag ||
+                (t >= OZ_STAGES && !mbar_wait(empty0 + 8 * s, (uint32_t)((t / OZ_STAGES) - 1) & 1u, err, abort_flag))) {
+              go = false;
+              break;
+            }
+            mbar_expect_tx(full0 + 8 * s, OZ_A_STAGE + OZ_B_STAGE);
+            tma_load_2d(sA + s * OZ_A_STAGE, &tmA, kc * OZ_BK, sc.arow[i] + row2, full0 + 8 * s);
+            tma_load_2d(sB + s * OZ_B_STAGE, &tmB, kc * OZ_BK, sc.brow[i] + colb, full0 + 8 * s);
+          }
         }
       }
     }
@@ -144,34 +202,41 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
     if (lane == 0) {
       long long t = 0;
       int g = 0;
-      bool first = true, ok = true;
-      for (int i = 0; i < sc.n && ok; i++) {
-        // group g accumulates in buffer g & 1, free once group g - 2 drained
-        if (first && g >= 2 && !mbar_wait(acce0 + 8 * (g & 1), (uint32_t)((g >> 1) - 1) & 1u, err, abort_flag)) {
-          ok = false;
-          break;
-        }
-        const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
-        for (int kc = 0; kc < kchunks; kc++, t++) {
-          const int s = (int)(t % OZ_STAGES);
-          if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / OZ_STAGES) & 1u, err, abort_flag)) {
+      bool ok = true;
+      OzIter it;
+      oz_iter_init(it, ntiles, sc.n);
+      OzSeg sg;
+      while (ok && oz_next_seg(it, sg)) {
+        bool first = true;
+        for (int i = sg.p0; i < sg.p1 && ok; i++) {
+          // group g accumulates in buffer g & 1, free once group g - 2 drained
+          if (first && g >= 2 &&
+              !mbar_wait(acce0 + 8 * (g & 1), (uint32_t)((g >> 1) - 1) & 1u, err, abort_flag)) {
             ok = false;
             break;
           }
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
+          for (int kc = 0; kc < kchunks; kc++, t++) {
+            const int s = (int)(t % OZ_STAGES);
+            if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / OZ_STAGES) & 1u, err, abort_flag)) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-          for (int k = 0; k < OZ_BK / 32; k++) {
-            const uint64_t ad = sw128_desc(sA + s * OZ_A_STAGE + k * 32);
-            const uint64_t bd = sw128_desc(sB + s * OZ_B_STAGE + k * 32);
-            umma_i8(tmem_acc, ad, bd, (first && kc == 0 && k == 0) ? 0u : 1u);
+            for (int k = 0; k < OZ_BK / 32; k++) {
+              const uint64_t ad = sw128_desc(sA + s * OZ_A_STAGE + k * 32);
+              const uint64_t bd = sw128_desc(sB + s * OZ_B_STAGE + k * 32);
+              umma_i8(tmem_acc, ad, bd, (first && kc == 0 && k == 0) ? 0u : 1u);
+            }
+            umma_commit(empty0 + 8 * s);
           }
-          umma_commit(empty0 + 8 * s);
-        }
-        first = false;
-        if (ok && sc.close[i]) {
-          umma_commit(accf0 + 8 * (g & 1));
-          g++;
-          first = true;
+          first = false;
+          if (ok && (sc.close[i] || i + 1 == sg.p1)) {
+            umma_commit(accf0 + 8 * (g & 1));
+            g++;
+            first = true;
+          }
         }
       }
     }
@@ -179,18 +244,36 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
     // drain warps 0-3 (warp w reads TMEM lanes 32w..32w+31)
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     const int rl = threadIdx.x & 63, qh = threadIdx.x >> 6;
+    int g = 0;
+    bool alive = true;
+    OzIter it;
+    oz_iter_init(it, ntiles, sc.n);
+    OzSeg sg;
+    while (alive && oz_next_seg(it, sg)) {
+    const int64_t row0 = 64 * (sg.t / ncol), col0 = (int64_t)OZ_BN * (sg.t % ncol);
+    // target of this segment: its tile of Y, or a workspace slot (64 x 256,
+    // column-major with leading dimension 64)
+    double2 *Yt = sg.slot < 0 ? Y + col0 * ldy + row0 : P + ((int64_t)blockIdx.x * 2 + sg.slot) * OZ_TILE_ELEMS;
+    const int64_t ldt = sg.slot < 0 ? ldy : 64;
     const int64_t gr = row0 + rl;
     const double rsc = gr < M ? rs[gr] : 0.0;
-    for (int g = 0; g < sc.ngroups; g++) {
+    for (int i = sg.p0, gi = 0; i < sg.p1; gi++) {
+      // the group: pairs i .. j, cut at the level's drain point or the segment end
+      int j = i;
+      while (!sc.close[j] && j + 1 < sg.p1) j++;
+      const double gsc = sc.lscale[i];
+      i = j + 1;
       const bool got = mbar_wait(accf0 + 8 * (g & 1), (uint32_t)(g >> 1) & 1u, err, abort_flag);
       const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
       if (threadIdx.x == 0) *epi_ok = 1;
       epi_sync();
       if (!got) *epi_ok = 0;
       epi_sync();
-      if (!*epi_ok) break;
+      if (!*epi_ok) {
+        alive = false;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const double gsc = sc.gscale[g];
       for (int cc = 0; cc < OZ_BN / 32; cc++) {
         if (col0 + cc * 32 >= Rv) break;  // uniform over the drain warps
         uint32_t v[32];
@@ -211,22 +294,22 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
         if (gr < M) {
           const int64_t gc0 = col0 + cc * 32 + qh;
           double2 old[16];
-          if (g > 0) {
+          if (gi > 0) {
 #pragma unroll
-            for (int i = 0; i < 16; i++)
-              old[i] = (gc0 + 2 * i < Rv) ? Y[(gc0 + 2 * i) * ldy + gr] : make_double2(0, 0);
+            for (int x = 0; x < 16; x++)
+              old[x] = (gc0 + 2 * x < Rv) ? Yt[(gc0 + 2 * x - col0) * ldt + rl] : make_double2(0, 0);
           } else {
 #pragma unroll
-            for (int i = 0; i < 16; i++) old[i] = make_double2(0, 0);
+            for (int x = 0; x < 16; x++) old[x] = make_double2(0, 0);
           }
 #pragma unroll
-          for (int i = 0; i < 16; i++) {
-            const int q = qh + 2 * i;
-            const int64_t gc = gc0 + 2 * i;
+          for (int x = 0; x < 16; x++) {
+            const int q = qh + 2 * x;
+            const int64_t gc = gc0 + 2 * x;
             if (gc < Rv) {
               const double w = rsc * cs[gc] * gsc;
-              Y[gc * ldy + gr] = make_double2(fma((double)E[rl * 33 + q], w, old[i].x),
-                                              fma((double)E[(64 + rl) * 33 + q], w, old[i].y));
+              Yt[(gc - col0) * ldt + rl] = make_double2(fma((double)E[rl * 33 + q], w, old[x].x),
+                                                        fma((double)E[(64 + rl) * 33 + q], w, old[x].y));
             }
           }
         }
@@ -235,12 +318,31 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       epi_sync();
       if (threadIdx.x == 0) mbar_arrive(acce0 + 8 * (g & 1));
+      g++;
+    }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * OZ_BN) : "memory");
+}
+
+// Tail tiles made of partial segments: tile fix[3 i] = the sum, in listed
+// order, of workspace slots fix[3 j + 2] (= 2 CTA + slot) for the entries j of
+// its run (fix[3 i + 1] = run length, given on the run's first entry)
+__global__ void k_oz_fixup(const int64_t *__restrict__ fix, const int *__restrict__ runs, int ncol, int64_t M,
+                           int64_t Rv, double2 *__restrict__ Y, const double2 *__restrict__ P, int64_t ldy) {
+  const int j0 = runs[blockIdx.x];
+  const int64_t t = fix[3 * j0], len = fix[3 * j0 + 1];
+  const int64_t row0 = 64 * (t / ncol), col0 = (int64_t)OZ_BN * (t % ncol);
+  for (int e = threadIdx.x; e < OZ_TILE_ELEMS; e += blockDim.x) {
+    const int64_t r = row0 + (e & 63), c = col0 + (e >> 6);
+    if (r >= M || c >= Rv) continue;
+    double2 acc = make_double2(0, 0);
+    for (int64_t j = 0; j < len; j++) acc = cadd(acc, P[fix[3 * (j0 + j) + 2] * OZ_TILE_ELEMS + e]);
+    Y[c * ldy + r] = acc;
+  }
 }
 
 // sigma (power of two, max/sigma in [0.5, 1)) of each complex row of Z
@@ -345,7 +447,7 @@ int64_t round_up(int64_t v, int64_t m) { return ((v + m - 1) / m) * m; }
 unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 struct OzState {
-  DevBuf A, B, rs, cs, err;
+  DevBuf A, B, rs, cs, err, P, fix, runs;
   CUtensorMap mapA, mapB;
   uint64_t a_version = ~0ull;
   int64_t a_n = -1, b_key = -1, b_n = -1;
@@ -424,7 +526,7 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
   // pairs share one TMEM sum unless int32 headroom forces an earlier drain
   const int64_t maxp = (int64_t)(2147483647.0 / (16129.0 * (double)ld));
   OzSched sc{};
-  int n = 0, g = 0;
+  int n = 0;
   for (int L = 0; L <= lmax; L++) {
     int in_group = 0;
     for (int p = 0; p <= L; p++) {
@@ -433,24 +535,53 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
       sc.arow[n] = (int)(p * 2 * Mpad);
       sc.brow[n] = (int)(q * Rpad);
       sc.close[n] = 0;
+      sc.lscale[n] = std::ldexp(1.0, -OZ_BETA * (L + 2));
       n++;
       if (++in_group == maxp) {
         sc.close[n - 1] = 1;
-        sc.gscale[g++] = std::ldexp(1.0, -OZ_BETA * (L + 2));
         in_group = 0;
       }
     }
-    if (in_group > 0) {
-      sc.close[n - 1] = 1;
-      sc.gscale[g++] = std::ldexp(1.0, -OZ_BETA * (L + 2));
-    }
+    if (in_group > 0) sc.close[n - 1] = 1;
   }
   sc.n = n;
-  sc.ngroups = g;
-  dim3 grid((unsigned)(Rpad / OZ_BN), (unsigned)(Mpad / 64));
+  // persistent grid: data-parallel full waves, stream-K tail (k_oz_gemm);
+  // the host replays the tail split to list each partial tile's slots
+  const int ncol = (int)(Rpad / OZ_BN);
+  const int64_t ntiles = (Mpad / 64) * ncol;
+  const int64_t G = std::min<int64_t>(ntiles, std::max(1, c->sm_count));
+  const int64_t F = (ntiles / G) * G, Wt = (ntiles - F) * n;
+  std::vector<int64_t> fix;  // (tile, run length, 2 CTA + slot) in tile order, then CTA order
+  for (int64_t b = 0; b < G; b++) {
+    int64_t u = F * n + Wt * b / G;
+    const int64_t u_end = F * n + Wt * (b + 1) / G;
+    int slot = 0;
+    while (u < u_end) {
+      const int64_t t = u / n;
+      const int64_t p0 = u - t * n, p1 = std::min<int64_t>(n, u_end - t * n);
+      u = t * n + p1;
+      if (!(p0 == 0 && p1 == n)) fix.insert(fix.end(), {t, 0, 2 * b + slot++});
+    }
+  }
+  std::vector<int> runs;
+  for (size_t j = 0; j < fix.size() / 3; j++) {
+    if (j == 0 || fix[3 * j] != fix[3 * (j - 1)]) runs.push_back((int)j);
+    fix[3 * runs.back() + 1]++;
+  }
+  if (!fix.empty()) {
+    st.P.ensure(sizeof(double2) * G * 2 * OZ_TILE_ELEMS);
+    st.fix.ensure(sizeof(int64_t) * fix.size());
+    st.runs.ensure(sizeof(int) * runs.size());
+    DMB_CUDA(cudaMemcpyAsync(st.fix.p, fix.data(), sizeof(int64_t) * fix.size(), cudaMemcpyHostToDevice, c->stream));
+    DMB_CUDA(cudaMemcpyAsync(st.runs.p, runs.data(), sizeof(int) * runs.size(), cudaMemcpyHostToDevice, c->stream));
+  }
   kt_begin(c);
-  DMB_LAUNCH(c, k_oz_gemm, grid, 192, OZ_SMEM, st.mapA, st.mapB, sc, (int)(ld / OZ_BK), N, R, Y, N,
-             st.rs.as<double>(), st.cs.as<double>(), st.err.as<unsigned>());
+  DMB_LAUNCH(c, k_oz_gemm, (unsigned)G, 192, OZ_SMEM, st.mapA, st.mapB, sc, (int)(ld / OZ_BK), N, R, Y,
+             fix.empty() ? Y : st.P.as<double2>(), N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
+             st.err.as<unsigned>());
+  if (!runs.empty())
+    DMB_LAUNCH(c, k_oz_fixup, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(), ncol, N, R,
+               Y, st.P.as<double2>(), N);
   // int8 work: every kept slice pair is a real (2N x 2N) x (2N x R) product
   kt_end(c, 2.0 * n * (2.0 * N) * (2.0 * N) * (double)R, 1);
 }
@@ -469,7 +600,7 @@ void oz_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_oz_states.size(); i++) {
     if (g_oz_states[i].first != c) continue;
     OzState *st = g_oz_states[i].second;
-    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err}) b->release();
+    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err, &st->P, &st->fix, &st->runs}) b->release();
     delete st;
     g_oz_states.erase(g_oz_states.begin() + i);
     return;

@@ -54,6 +54,28 @@ def test_tensor_core_zx_matches_fp64_accumulation():
     dev.close()
 
 
+def test_int8_product_with_split_tail_tiles():
+    # 4,720 RWG x 600 columns: 74 x 3 = 222 output tiles on 148 SMs -- one
+    # data-parallel wave and a tail whose tiles are split between CTAs and
+    # summed by the fixup kernel
+    dev = _plate(40, side=0.3)
+    dev.assemble(K3, precision="mixed")
+    dev.set_option("tc_min_rhs", 1 << 30)
+    X = _rand(dev.N, 600, 9)
+    Y = dev.matvec(X)
+    dev.set_option("tensor_cores", 0)
+    Ys = dev.matvec(X)
+    dev.set_option("tensor_cores", 1)
+    err = np.linalg.norm(Y - Ys, axis=0) / np.linalg.norm(Ys, axis=0)
+    print(f"split-tail int8-slice product vs SIMT FP64: max column error {err.max():.2e}")
+    assert err.max() <= 2e-11
+    for j in (0, 255, 256, 599):
+        y = dev.matvec(np.ascontiguousarray(X[:, j]))
+        assert np.linalg.norm(Y[:, j] - y) <= 2e-11 * np.linalg.norm(y)
+    np.testing.assert_array_equal(Y, dev.matvec(X))  # deterministic
+    dev.close()
+
+
 def test_fp64_accumulated_zx_matches_column_products():
     # the FP64-accurate Z X of the refinement residuals (int8 tensor-core
     # slices for complex64 Z from 32 right-hand sides, else SIMT FP64) against
