@@ -93,6 +93,9 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     dmb::local_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     if (c->stream2) cudaStreamDestroy(c->stream2);
+    for (auto &kv : c->gm_graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->gm_graphs.clear();
     if (c->stream3) cudaStreamDestroy(c->stream3);
     if (c->stream_aux) cudaStreamDestroy(c->stream_aux);
     for (auto &e : c->aux_ev)
@@ -130,6 +133,10 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       DMB_REQUIRE(value == 0 || value == 8 || value == 16 || value == 32, DMB_ERR_ARGUMENT,
                   "far tile rows must be 0 (autotune), 8, 16 or 32");
       c->far_tile = value;
+      return;
+    }
+    if (option == DMB_OPT_GMRES_GRAPHS) {
+      c->gmres_graphs = value != 0;
       return;
     }
     if (option == DMB_OPT_PRECOND_TF32_TERMS) {
@@ -806,6 +813,9 @@ dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out) {
       delete b;
       return st;
     }
+    // lanes take surfaces of changing sizes (buffers regrow, so captured
+    // GMRES graphs would rarely be replayed): direct launches
+    c->gmres_graphs = false;
     b->lanes.push_back(c);
   }
   *out = b;

@@ -336,32 +336,88 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     first = false;
     DMB_CUDA(cudaMemsetAsync(H, 0, sizeof(double2) * R * (int64_t)(kcap + 1) * kcap, c->stream));
     DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, V, V);
-    int j = 0;
-    for (; j < kcap && total_iters < maxiter; j++, total_iters++) {
-      double2 *Vj = V + (int64_t)j * vstride;
-      apply_operator(c, precond_kind, side, Vj, w, flex ? Zv + (int64_t)j * vstride : tmp, R);
+    // few right-hand sides: iterations between host checks are launch-bound
+    // enough to replay as graphs (kernel timing records events per launch)
+    const bool graphs_ok = R < 32 && !c->kt_enabled;
+    // one Arnoldi + Givens iteration (device work only)
+    auto iteration = [&](int jj) {
+      double2 *Vj = V + (int64_t)jj * vstride;
+      apply_operator(c, precond_kind, side, Vj, w, flex ? Zv + (int64_t)jj * vstride : tmp, R);
       for (int pass = 0; pass < 2; pass++) {
-        DMB_LAUNCH(c, k_dots, dim3(j + 1, (unsigned)R), 256, 0, N, R, j, vstride, V, w, hb, kcap + 1);
-        DMB_LAUNCH(c, k_cgs_update, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, hb, kcap + 1, w);
-        DMB_LAUNCH(c, k_hacc, blocks_for(R, 128), 128, 0, R, j, hb, kcap + 1, H, kcap);
+        DMB_LAUNCH(c, k_dots, dim3(jj + 1, (unsigned)R), 256, 0, N, R, jj, vstride, V, w, hb, kcap + 1);
+        DMB_LAUNCH(c, k_cgs_update, blocks_for(N * R, 256), 256, 0, N, R, jj, vstride, V, hb, kcap + 1, w);
+        DMB_LAUNCH(c, k_hacc, blocks_for(R, 128), 128, 0, R, jj, hb, kcap + 1, H, kcap);
       }
       DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, nrm);
-      DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, w, V + (int64_t)(j + 1) * vstride);
+      DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, w, V + (int64_t)(jj + 1) * vstride);
       DMB_CUDA(cudaMemsetAsync(active, 0, 4, c->stream));
-      DMB_LAUNCH(c, k_givens, blocks_for(R, 128), 128, 0, R, j, kcap, H, nrm, cs, sn, g, st, active);
-      // the host looks at the active count every check_every iterations (a
-      // system that converged in between keeps its own k; its extra basis
-      // vectors are never combined)
-      if ((j + 1) % check_every == 0 || j + 1 == kcap || total_iters + 1 >= maxiter) {
-        unsigned h_active = 0;
-        DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
-        DMB_CUDA(cudaStreamSynchronize(c->stream));
-        if (h_active == 0) {
-          j++;
-          total_iters++;
-          break;
-        }
+      DMB_LAUNCH(c, k_givens, blocks_for(R, 128), 128, 0, R, jj, kcap, H, nrm, cs, sn, g, st, active);
+    };
+    // iterations j0 .. j0 + nb - 1, directly or as a captured graph
+    auto run_block = [&](int j0, int nb) {
+      auto eager = [&] {
+        for (int jj = j0; jj < j0 + nb; jj++) iteration(jj);
+      };
+      if (!(graphs_ok && c->gmres_graphs)) return eager();
+      const std::vector<int64_t> key = {j0, nb, N, R, kcap, vstride, precond_kind, side, flex, c->pc_kind,
+                                        c->z_prec, (int64_t)(uintptr_t)V, (int64_t)(uintptr_t)Zv,
+                                        (int64_t)(uintptr_t)w, (int64_t)(uintptr_t)tmp, (int64_t)(uintptr_t)H,
+                                        (int64_t)(uintptr_t)hb, (int64_t)(uintptr_t)g,
+                                        (int64_t)(uintptr_t)st, (int64_t)g_dev_alloc_epoch.load()};
+      dmb_ctx::GraphEntry &e = c->gm_graphs[key];
+      if (e.exec) {
+        DMB_CUDA(cudaGraphLaunch(e.exec, c->stream));
+        c->launches += e.kernels;
+        return;
       }
+      if (!e.seen) {  // first meeting: direct launches (any lazy allocation happens here)
+        e.seen = true;
+        return eager();
+      }
+      const int64_t l0 = c->launches;
+      int64_t kernels = 0;
+      cudaGraph_t graph = nullptr;
+      bool captured = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (captured) {
+        try {
+          eager();
+        } catch (...) {
+          captured = false;
+        }
+        kernels = c->launches - l0;
+        cudaGraph_t got = nullptr;
+        const bool ended = cudaStreamEndCapture(c->stream, &got) == cudaSuccess;
+        if (captured && ended && got) graph = got;
+        else if (got) cudaGraphDestroy(got);
+      }
+      c->launches = l0;  // captured launches have not run
+      cudaGraphExec_t ex = nullptr;
+      if (graph && cudaGraphInstantiate(&ex, graph, 0) != cudaSuccess) ex = nullptr;
+      if (graph) cudaGraphDestroy(graph);
+      if (!ex) {  // capture not possible here: direct launches from now on
+        (void)cudaGetLastError();
+        c->gmres_graphs = false;
+        return eager();
+      }
+      e.exec = ex;
+      e.kernels = kernels;  // kernels of one replay: the launches of one direct pass
+      DMB_CUDA(cudaGraphLaunch(ex, c->stream));
+      c->launches += kernels;
+    };
+    int j = 0;
+    while (j < kcap && total_iters < maxiter) {
+      // the iterations up to the next host look at the active count (a system
+      // that converged in between keeps its own k; its extra basis vectors
+      // are never combined)
+      int nb = 1;
+      while (j + nb < kcap && total_iters + nb < maxiter && (j + nb) % check_every != 0) nb++;
+      run_block(j, nb);
+      j += nb;
+      total_iters += nb;
+      unsigned h_active = 0;
+      DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
+      DMB_CUDA(cudaStreamSynchronize(c->stream));
+      if (h_active == 0) break;
     }
     // solution update from this cycle
     DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);

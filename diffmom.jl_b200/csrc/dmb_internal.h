@@ -8,6 +8,8 @@
 #include <chrono>
 #include <mutex>
 #include <string>
+#include <atomic>
+#include <map>
 #include <vector>
 
 #include "../../include/diffmom_b200.h"
@@ -35,6 +37,11 @@ struct DmbError {
 // ---------------------------------------------------------------------------
 // device buffer (grow-only, owned by the context)
 // ---------------------------------------------------------------------------
+// bumped by every device (re)allocation or release of a DevBuf: captured CUDA
+// graphs hold raw device addresses and are valid only for the epoch they were
+// captured in
+inline std::atomic<uint64_t> g_dev_alloc_epoch{0};
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -43,6 +50,7 @@ struct DevBuf {
     if (want <= bytes && p) return;
     release();
     if (want == 0) want = 16;
+    g_dev_alloc_epoch++;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
       p = nullptr;
@@ -53,7 +61,10 @@ struct DevBuf {
     bytes = want;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      g_dev_alloc_epoch++;
+      cudaFree(p);
+    }
     p = nullptr;
     bytes = 0;
   }
@@ -167,6 +178,16 @@ struct dmb_ctx {
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
   int far_tile = 0;              // far-pair tile rows (8/16/32), 0 = autotuned
   bool exact_krylov = true;      // many-RHS Krylov product on the INT8 slices (FP64-accurate)
+  // GMRES iterations between host checks replayed as captured CUDA graphs
+  // (few right-hand sides); key: iteration range, shape, buffer addresses and
+  // the allocation epoch
+  bool gmres_graphs = true;
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+    bool seen = false;
+  };
+  std::map<std::vector<int64_t>, GraphEntry> gm_graphs;
   int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
   int far_tile_used = 0;         // shape of the last assembly
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)

@@ -45,6 +45,7 @@ OPT_TC_MIN_RHS = 2
 OPT_FAR_TILE = 3
 OPT_EXACT_KRYLOV = 4
 OPT_PRECOND_TF32_TERMS = 5
+OPT_GMRES_GRAPHS = 6
 
 
 class DiffMoMError(RuntimeError):

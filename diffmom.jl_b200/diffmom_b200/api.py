@@ -88,10 +88,11 @@ class EFIEDevice:
         "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles,
         "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product,
         "precond_tf32_terms" (3/1) for the TF32 products per complex MAC of the
-        complex64 factorisation updates and batched triangular sweeps."""
+        complex64 factorisation updates and batched triangular sweeps,
+        "gmres_graphs" (0/1) for CUDA-graph replay of GMRES iterations."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
-                 "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS}
+                 "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))

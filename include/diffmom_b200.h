@@ -111,6 +111,13 @@ const char *dmb_version(void);
  * preconditioner changes; right-preconditioned GMRES keeps the preconditioned
  * vectors (flexible form), so the solution accuracy is unaffected. */
 #define DMB_OPT_PRECOND_TF32_TERMS 5
+/* DMB_OPT_GMRES_GRAPHS: 1 (default) replays the GMRES iterations between two
+ * host convergence checks of solves with fewer than 32 right-hand sides as
+ * captured CUDA graphs (captured the second time an iteration range is met
+ * with the same problem shape and device buffers, replayed afterwards); 0
+ * launches every kernel directly.  Results are identical either way.  The
+ * lanes of dmb_batch_* contexts launch directly. */
+#define DMB_OPT_GMRES_GRAPHS 6
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair tile rows used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
