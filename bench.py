@@ -66,7 +66,7 @@ SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
 # DRAM bytes per k_oz_gemm launch on the headline step, measured with ncu
 # one-pass dram__bytes_read/write.sum over the 3 launches of one step
-OZ_TRAFFIC_PER_LAUNCH = 44767341312 / 3  # 3 launches: 13.857 + 13.854 + 17.056 GB
+OZ_TRAFFIC_PER_LAUNCH = 52299230208 / 3  # 3 launches: 16.037 + 16.035 + 20.228 GB
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
