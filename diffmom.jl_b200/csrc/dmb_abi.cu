@@ -85,6 +85,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     c->d_sol.release();
     c->d_mono.release();
     c->d_trsm_id.release();
+    c->d_Wraw.release();
     c->d_trsm_t.release();
     c->d_Zv.release();
     c->d_small.release();

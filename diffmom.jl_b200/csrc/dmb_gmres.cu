@@ -195,6 +195,19 @@ __global__ void k_combine(int64_t N, int64_t R, int kmax, int64_t vstride, const
   x[idx] = cadd(x[idx], acc);
 }
 
+// r = b - sum_i y[r][i] W_i(r): the residual of x = sum_i y_i z_i from the
+// stored products W_i = Z z_i
+__global__ void k_resid_products(int64_t N, int64_t R, int kmax, int64_t vstride, const double2 *__restrict__ W,
+                                 const double2 *__restrict__ y, int kcap, const double2 *__restrict__ b,
+                                 double2 *__restrict__ out) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= N * R) return;
+  int64_t r = idx / N, n = idx % N;
+  double2 acc = make_double2(0, 0);
+  for (int i = 0; i < kmax; i++) acc = cadd(acc, cmul(y[r * kcap + i], W[(int64_t)i * vstride + r * N + n]));
+  out[idx] = csub(b[idx], acc);
+}
+
 __global__ void k_sub(int64_t count, const double2 *__restrict__ a, double2 *__restrict__ b) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < count) b[i] = csub(a[i], b[i]);
@@ -208,17 +221,17 @@ namespace dmb {
 // the solution is then sum y_i z_i and needs no further preconditioner
 // application, and an inexact (tensor-core) preconditioner stays consistent.
 void apply_operator(dmb_ctx *c, int precond_kind, int side, const double2 *v, double2 *w, double2 *z,
-                    int64_t R) {
+                    int64_t R, bool full_levels = false) {
   const int64_t N = c->n;
   if (precond_kind == DMB_PRECOND_NONE) {
-    matvec_op(c, v, w, R);
+    matvec_op(c, v, w, R, full_levels);
   } else if (side == DMB_SIDE_LEFT) {
-    matvec_op(c, v, w, R);
+    matvec_op(c, v, w, R, full_levels);
     pc_apply_dev(c, (double *)w, R);
   } else {
     DMB_CUDA(cudaMemcpyAsync(z, v, sizeof(double2) * N * R, cudaMemcpyDeviceToDevice, c->stream));
     pc_apply_dev(c, (double *)z, R);
-    matvec_op(c, z, w, R);
+    matvec_op(c, z, w, R, full_levels);
   }
 }
 
@@ -236,9 +249,15 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   // (decided once per problem shape; repeated solves reuse the buffers); the
   // right-preconditioned form also keeps the preconditioned vectors
   const bool flex = precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_RIGHT;
+  // With the INT8-slice operator and no left preconditioner, the Krylov
+  // products are Z z_i themselves: computed with every slice level (FP64-
+  // accurate) and kept before orthogonalisation, they give the true residual
+  // of x = sum y_i z_i as b - sum y_i Z z_i without another product.
+  const bool prod_resid = krylov_exact_int8(c, R) && (precond_kind == DMB_PRECOND_NONE || side == DMB_SIDE_RIGHT);
+  const int nvec = (flex ? 2 : 1) + (prod_resid ? 1 : 0);
   size_t vec_bytes = sizeof(double2) * N * R;
   if (!(c->gm_key_n == N && c->gm_key_r == R && c->gm_key_maxiter == maxiter && c->gm_key_flex == flex &&
-        c->gm_kcap > 0)) {
+        c->gm_key_nvec == nvec && c->gm_kcap > 0)) {
     size_t freeb = 0, totb = 0;
     DMB_CUDA(cudaMemGetInfo(&freeb, &totb));
     freeb += c->d_V.bytes + c->d_Zv.bytes;  // the current buffers can be reused
@@ -246,18 +265,21 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     // needs a handful of vectors; GMRES restarts if the capacity runs out)
     double budget = freeb * 0.4;
     if (R >= 8) budget = std::min(budget, 8.0 * 1024 * 1024 * 1024);
-    int64_t cap_mem = (int64_t)(budget / (double)(vec_bytes * (flex ? 2 : 1))) - 1;
+    int64_t cap_mem = (int64_t)(budget / (double)(vec_bytes * nvec)) - 1;
     c->gm_kcap = (int)std::max<int64_t>(2, std::min<int64_t>(maxiter, cap_mem));
     c->gm_key_n = N;
     c->gm_key_r = R;
     c->gm_key_maxiter = maxiter;
     c->gm_key_flex = flex;
+    c->gm_key_nvec = nvec;
   }
   const int kcap = c->gm_kcap;
   const int64_t vstride = N * R;
   c->d_V.ensure(vec_bytes * (kcap + 1));
   if (flex) c->d_Zv.ensure(vec_bytes * kcap);
   double2 *Zv = flex ? c->d_Zv.as<double2>() : nullptr;
+  if (prod_resid) c->d_Wraw.ensure(vec_bytes * kcap);
+  double2 *Wraw = prod_resid ? c->d_Wraw.as<double2>() : nullptr;
   c->d_work.ensure(vec_bytes * 2);
   // layout: H[R][(k+1)k] g[R][k+1] sn[R][k] hb[R][k+1] y[R][k] | cs[R][k] nrm[2R] | st[R] | active
   size_t small = sizeof(double2) * R * ((size_t)(kcap + 1) * kcap + 2 * (kcap + 1) + 2 * kcap) +
@@ -292,7 +314,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   const int check_every = (R < 32 && cheap) ? 4 : 1;
   int iters_used = 0;
   DMB_CUDA(cudaMemsetAsync(x, 0, vec_bytes, c->stream));
-  int total_iters = 0, restarts = 0;
+  int total_iters = 0, restarts = 0, cycles = 0, j_last = 0;
   bool first = true, have_true = false;
   std::vector<SysState> hst(R);
   while (true) {
@@ -334,6 +356,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       DMB_CUDA(cudaMemcpyAsync(g, hg.data(), sizeof(double2) * hg.size(), cudaMemcpyHostToDevice, c->stream));
     }
     first = false;
+    cycles++;
     DMB_CUDA(cudaMemsetAsync(H, 0, sizeof(double2) * R * (int64_t)(kcap + 1) * kcap, c->stream));
     DMB_LAUNCH(c, k_scale_cols, blocks_for(N * R, 256), 256, 0, N, R, nrm, V, V);
     // few right-hand sides: iterations between host checks are launch-bound
@@ -342,7 +365,9 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     // one Arnoldi + Givens iteration (device work only)
     auto iteration = [&](int jj) {
       double2 *Vj = V + (int64_t)jj * vstride;
-      apply_operator(c, precond_kind, side, Vj, w, flex ? Zv + (int64_t)jj * vstride : tmp, R);
+      apply_operator(c, precond_kind, side, Vj, w, flex ? Zv + (int64_t)jj * vstride : tmp, R, prod_resid);
+      if (prod_resid)
+        DMB_CUDA(cudaMemcpyAsync(Wraw + (int64_t)jj * vstride, w, vec_bytes, cudaMemcpyDeviceToDevice, c->stream));
       for (int pass = 0; pass < 2; pass++) {
         DMB_LAUNCH(c, k_dots, dim3(jj + 1, (unsigned)R), 256, 0, N, R, jj, vstride, V, w, hb, kcap + 1);
         DMB_LAUNCH(c, k_cgs_update, blocks_for(N * R, 256), 256, 0, N, R, jj, vstride, V, hb, kcap + 1, w);
@@ -420,6 +445,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       if (h_active == 0) break;
     }
     // solution update from this cycle
+    j_last = j;
     DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);
     if (flex) {
       DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, Zv, ybuf, kcap, x);
@@ -446,8 +472,14 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     DMB_REQUIRE(oz_error_word(c) == 0, DMB_ERR_TIMEOUT, "int8 tensor-core GEMM: a pipeline wait expired");
   // true FP64 residual ||b - Z x|| / ||b|| per system
   if (!have_true) {
-    matvec_dev(c, x, w, R);
-    DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
+    if (prod_resid && cycles == 1) {
+      // x = sum y_i z_i from x = 0: b - sum y_i (Z z_i) with the stored products
+      DMB_LAUNCH(c, k_resid_products, blocks_for(N * R, 256), 256, 0, N, R, j_last, vstride, Wraw, ybuf, kcap, b,
+                 w);
+    } else {
+      matvec_dev(c, x, w, R);
+      DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
+    }
     DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, tnrm);
   }
   DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);

@@ -202,6 +202,8 @@ struct dmb_ctx {
   int64_t gm_key_n = 0, gm_key_r = 0;
   int gm_key_maxiter = 0;
   bool gm_key_flex = false;
+  int gm_key_nvec = 0;          // basis-sized vectors kept per iteration
+  DevBuf d_Wraw;                // Z z_i before orthogonalisation (residual from the Krylov products)
 
   // timings
   dmb_timings tm{};
@@ -320,7 +322,9 @@ void oz_prepare(dmb_ctx *c);
 unsigned oz_error_word(dmb_ctx *c);
 void oz_release(dmb_ctx *c);
 void local_release(dmb_ctx *c);
-void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs);  // Krylov operator (may be TC)
+// Krylov operator (may be on the tensor cores); full_levels: the INT8-slice
+// product with every slice level (FP64-accurate) instead of the Krylov levels
+void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs, bool full_levels = false);
 bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs);
 void learned_build(dmb_ctx *c, double radius);
 void ring_step_build(dmb_ctx *c, double radius, bool learned);

@@ -429,9 +429,9 @@ bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs) {
          tc_available(c);
 }
 
-void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs) {
+void matvec_op(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs, bool full_levels) {
   if (krylov_exact_int8(c, nrhs))
-    oz_zx(c, x, y, nrhs, OZ_LEVELS_KRYLOV);
+    oz_zx(c, x, y, nrhs, full_levels ? OZ_LEVELS_RESIDUAL : OZ_LEVELS_KRYLOV);
   else if (matvec_op_inexact(c, nrhs))
     tc_zx(c, x, y, nrhs);
   else

@@ -147,6 +147,15 @@ def test_block_gmres_many_plane_waves(side, exact):
         # left preconditioning (Krylov.jl semantics): the preconditioned residual
         # meets the tolerance; the unpreconditioned one follows within cond(M Z)
         assert st.true_residual <= 1e-3
+    # the reported true residual -- formed from the stored Krylov products when
+    # they are the FP64-accurate ones -- against b - Z x from a separate
+    # FP64-accurate product through the public matvec
+    dev.set_option("exact_krylov", 1)  # the public product then has every slice level
+    Zx = dev.matvec(np.asfortranarray(x))
+    explicit = np.max(np.linalg.norm(V - Zx, axis=0) / np.linalg.norm(V, axis=0))
+    # both come from products accurate to ~1e-12 of |Z||x|: they agree to that
+    # absolute level, five orders below the 1e-6 tolerance
+    assert abs(explicit - st.true_residual) <= 1e-2 * st.true_residual + 2e-11
     dev.close()
 
 
