@@ -64,9 +64,9 @@ K = 2 * math.pi * FREQ / C0
 R_WAVES = 1024
 SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
-# DRAM bytes per k_oz_gemm launch on the headline step, measured with ncu
-# one-pass dram__bytes_read/write.sum over the 3 launches of one step
-OZ_TRAFFIC_PER_LAUNCH = 52299230208 / 3  # 3 launches: 16.037 + 16.035 + 20.228 GB
+# DRAM bytes per k_oz_gemm launch (26 slice products, R = 1,024) on the
+# headline plate, measured with ncu one-pass dram__bytes_read/write.sum
+OZ_TRAFFIC_PER_LAUNCH = 20227765760  # a 26-product launch (the headline's Krylov products): 18.987 + 1.240 GB
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
@@ -460,8 +460,8 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
         "gpu_launches": int(head["launches"]) if head else 0,
     }
     if head is not None:
-        # dominant kernel: k_oz_gemm, the Z X products of block GMRES (two
-        # Krylov products and the final true residual per step, R columns each)
+        # dominant kernel: k_oz_gemm, the Z X products of block GMRES (the
+        # Krylov products, R columns each; the true residual is formed from them)
         ims, il, iw = head["kernel_int8"]
         if il > 0:
             alg = il * 8.0 * N * N * R_WAVES  # 8 flops per complex MAC, counted once
@@ -472,8 +472,8 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                 "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                 "frac": achieved / bf16 if bf16 else None,
                 "traffic": OZ_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
-                "traffic_note": "DRAM bytes per launch (ncu one-pass dram__bytes metrics, the 3 launches of a "
-                                "headline step)",
+                "traffic_note": "DRAM bytes per launch (ncu one-pass dram__bytes metrics of a 26-product "
+                                "launch on the headline plate)",
                 "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic flops 8 N^2 R per launch "
                                "(complex MAC = 8 real flops, counted once however the product is executed)",
                 "launches_timed": il, "kernel_ms_total": ims,
@@ -481,8 +481,9 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                 "executed_int8": {"achieved_pops": (iw / 1e15) / (ims / 1e3), "peak_pops": 4.5,
                                   "frac": (iw / 1e15) / (ims / 1e3) / 4.5,
                                   "peak_source": "nominal dense INT8 (not in MEASURED_PEAKS.json)",
-                                  "note": "21 (Krylov) or 26 (residual) int8 slice products of the "
-                                          "real-stacked (2N x 2N) x (2N x R) system per launch"}}
+                                  "note": "26 int8 slice products of the real-stacked (2N x 2N) x (2N x R) "
+                                          "system per launch (FP64-accurate Krylov products; the true "
+                                          "residual comes from them)"}}
         fams = {"k_tc_gemm (triangular-sweep GEMMs)": head["kernel_gemm"],
                 "k_tc_syrk + k_tc_pack (factorisation trailing updates)": head["kernel_factor"]}
         line["roofline_tc"] = {
