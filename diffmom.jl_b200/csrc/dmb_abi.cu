@@ -89,6 +89,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     c->d_trsm_t.release();
     c->d_Zv.release();
     c->d_small.release();
+    c->aca.release();
     dmb::tc_release(c);
     dmb::oz_release(c);
     dmb::local_release(c);
@@ -109,7 +110,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
   return DMB_OK;
 }
 
-const char *dmb_last_error(const dmb_ctx *c) { return c ? c->err.c_str() : "null context"; }
+const char *dmb_last_error(const dmb_ctx *c) { return c ? c->err.c_str() : dmb_free_error().c_str(); }
 
 dmb_status dmb_get_timings(dmb_ctx *c, dmb_timings *out) {
   return guarded(c, [&] {
@@ -138,6 +139,14 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
     }
     if (option == DMB_OPT_GMRES_GRAPHS) {
       c->gmres_graphs = value != 0;
+      return;
+    }
+    if (option == DMB_OPT_OPERATOR) {
+      DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "operator must be 0 (dense Z) or 1 (H-matrix)");
+      DMB_REQUIRE(value == 0 ? c->z_valid : c->aca.valid, DMB_ERR_STATE,
+                  value == 0 ? "no assembled impedance matrix" : "no H-matrix operator built");
+      if (c->op_kind != value) c->pc_valid = false;
+      c->op_kind = value;
       return;
     }
     if (option == DMB_OPT_PRECOND_TF32_TERMS) {
@@ -187,6 +196,8 @@ dmb_status dmb_mesh_upload(dmb_ctx *c, const double *xyz, const int64_t *tri, in
     c->cache_valid = false;
     c->z_valid = false;
     c->pc_valid = false;
+    c->aca.release();
+    c->op_kind = 0;
   });
 }
 
@@ -252,6 +263,8 @@ dmb_status dmb_rwg_upload(dmb_ctx *c, int64_t n, const int64_t *tplus, const int
     c->cache_valid = false;
     c->z_valid = false;
     c->pc_valid = false;
+    c->aca.release();
+    c->op_kind = 0;
   });
 }
 
@@ -285,7 +298,7 @@ dmb_status dmb_apply_impedance(dmb_ctx *c, const double *zs) {
 
 dmb_status dmb_matvec(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
   return guarded(c, [&] {
-    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(dmb::operator_ready(c), DMB_ERR_STATE, "no assembled impedance matrix");
     DMB_REQUIRE(x && y && nrhs >= 1, DMB_ERR_ARGUMENT, "bad matvec arguments");
     size_t bytes = sizeof(double2) * c->n * nrhs;
     DevBuf bx, by;
@@ -330,6 +343,8 @@ dmb_status dmb_nf_build(dmb_ctx *c, double cutoff, int kind, double *nnz_ratio_o
     DMB_REQUIRE(kind == DMB_PRECOND_NF_LU || kind == DMB_PRECOND_NF_DIAG, DMB_ERR_ARGUMENT,
                 "invalid factorization; expected :lu or :diag");
     DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(c->op_kind == 0, DMB_ERR_STATE,
+                "the operator is an H-matrix: build its near-field preconditioner with dmb_aca_nf_build");
     dmb::nf_build(c, cutoff, kind);
     if (nnz_ratio_out) *nnz_ratio_out = c->nnz_ratio;
   });
@@ -521,7 +536,7 @@ dmb_status dmb_gmres(dmb_ctx *c, const double *rhs, double *x, int64_t nrhs, dou
     DMB_REQUIRE(precond_side == DMB_SIDE_LEFT || precond_side == DMB_SIDE_RIGHT, DMB_ERR_ARGUMENT,
                 "Invalid precond_side (expected :left or :right)");
     DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad GMRES arrays");
-    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(dmb::operator_ready(c), DMB_ERR_STATE, "no assembled impedance matrix");
     check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
     size_t bytes = sizeof(double2) * c->n * nrhs;
     DevBuf bb, bx;
@@ -554,7 +569,7 @@ dmb_status dmb_gmres_adjoint(dmb_ctx *c, const double *rhs, double *x, int64_t n
                     precond_kind == DMB_PRECOND_NF_DIAG,
                 DMB_ERR_ARGUMENT, "adjoint GMRES takes no preconditioner or a near-field one");
     DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad GMRES arrays");
-    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(dmb::operator_ready(c), DMB_ERR_STATE, "no assembled impedance matrix");
     check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
     const int64_t cnt = c->n * nrhs;
     size_t bytes = sizeof(double2) * cnt;
@@ -563,8 +578,15 @@ dmb_status dmb_gmres_adjoint(dmb_ctx *c, const double *rhs, double *x, int64_t n
     bx.ensure(bytes);
     DMB_CUDA(cudaMemcpyAsync(bb.p, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
     // Z and the near-field matrix are complex symmetric: Z^H x = b  <=>
-    // Z conj(x) = conj(b), and the adjoint preconditioner is conj(M^-1)
+    // Z conj(x) = conj(b), and the adjoint preconditioner is conj(M^-1).  An
+    // H-matrix A is not exactly symmetric: the same transformation gives
+    // A^T conj(x) = conj(b), so its products run transposed meanwhile.
     dmb::conj_dev(c, bb.as<double2>(), cnt);
+    struct Transposed {
+      dmb_ctx *c;
+      explicit Transposed(dmb_ctx *ctx) : c(ctx) { c->aca_transposed = c->op_kind == 1; }
+      ~Transposed() { c->aca_transposed = false; }
+    } tr(c);
     dmb::gmres_dev(c, bb.as<double>(), bx.as<double>(), nrhs, tol, maxiter, precond_kind, precond_side, &st);
     dmb::conj_dev(c, bx.as<double2>(), cnt);
     DMB_CUDA(cudaMemcpyAsync(x, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -583,7 +605,7 @@ dmb_status dmb_solve_direct(dmb_ctx *c, const double *rhs, double *x, int64_t nr
                             double *backward_error_out) {
   return guarded(c, [&] {
     DMB_REQUIRE(rhs && x && nrhs >= 1, DMB_ERR_ARGUMENT, "bad solve arrays");
-    DMB_REQUIRE(c->z_valid, DMB_ERR_STATE, "no assembled impedance matrix");
+    DMB_REQUIRE(c->z_valid && c->op_kind == 0, DMB_ERR_STATE, "no assembled impedance matrix");
     check_finite(rhs, 2 * c->n * nrhs, "right-hand side");
     size_t bytes = sizeof(double2) * c->n * nrhs;
     DevBuf bb, bx;

@@ -920,6 +920,7 @@ void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) 
   c->tm.assembly_ms = now_ms() - t0;
   c->z_prec = precision;
   c->z_valid = true;
+  c->op_kind = 0;  // the dense Z is the operator again
   c->z_version++;
   c->k = k;
   c->eta0 = eta0;

@@ -1383,6 +1383,19 @@ void nf_build(dmb_ctx *c, double cutoff, int kind) {
   c->tm.precond_ms = now_ms() - t0;
 }
 
+// factor a near-field matrix already written to d_F (precision of its
+// storage) and make it the context's preconditioner
+void nf_factor_resident(dmb_ctx *c, int kind, int precision) {
+  c->pc_valid = false;
+  if (precision == DMB_PREC_FP64)
+    ldlt_factor(c, c->d_F.as<double2>());
+  else
+    ldlt_factor(c, c->d_F.as<float2>());
+  c->pc_kind = kind;
+  c->pc_prec = precision;
+  c->pc_valid = true;
+}
+
 void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs) {
   DMB_REQUIRE(c->pc_valid, DMB_ERR_STATE, "no preconditioner built");
   const int64_t N = c->n;

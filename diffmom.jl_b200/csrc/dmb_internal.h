@@ -34,6 +34,13 @@ struct DmbError {
     if (!(cond)) throw DmbError{(code), (text)};      \
   } while (0)
 
+// message of the calling thread's last failed entry point that takes no
+// context (returned by dmb_last_error(NULL))
+inline std::string &dmb_free_error() {
+  thread_local std::string msg = "null context";
+  return msg;
+}
+
 // ---------------------------------------------------------------------------
 // device buffer (grow-only, owned by the context)
 // ---------------------------------------------------------------------------
@@ -99,8 +106,49 @@ struct NearRec {
   int ia, ib;     // slots
 };
 
+// H-matrix operator of dmb_aca_build (dmb_aca.cu).  Blocks are kept in task
+// order; their data lives in one complex128 arena (dense: m x n column-major;
+// low-rank: U m x rmax then V n x rmax, both column-major).
+struct AcaBlockDesc {
+  int64_t off_a, off_b;  // arena offsets (complex entries) of data / U and of V
+  int32_t r0, m, c0, n;  // tree-order row / column ranges (0-based first, count)
+  int32_t kind;          // 0 dense, 1 low-rank
+  int32_t rmax;          // capacity of U / V columns (low-rank)
+  int32_t task;          // index in the task list
+  int32_t fallback;      // 1: admissible task stored dense
+};
+struct AcaState {
+  bool valid = false;
+  int64_t n = 0;
+  std::vector<int32_t> perm;        // tree order -> original index (0-based)
+  std::vector<AcaBlockDesc> blocks; // task order
+  std::vector<int32_t> rank;        // per block (low-rank), from the device
+  dmb_aca_info info{};
+  // device: permutation, blocks, arena, per-block ranks / status, product lists
+  DevBuf d_perm, d_blocks, d_arena, d_rank, d_tbuf_off, d_t, d_xp;
+  DevBuf d_lr_list;                       // low-rank block ids (inner-product kernel)
+  DevBuf d_row_off, d_row_items;          // per row leaf: dense blocks then covering low-rank blocks
+  DevBuf d_col_off, d_col_items;          // per column leaf: the same for the adjoint / transpose
+  DevBuf d_leaf;                          // leaf node ranges (first, count)
+  int64_t n_leaves = 0, n_lr = 0, t_total = 0;
+  double k = 0, eta0 = 0;
+  int quad_order = 3;
+  void release() {
+    DevBuf *b[] = {&d_perm, &d_blocks, &d_arena, &d_rank, &d_tbuf_off, &d_t, &d_xp, &d_lr_list,
+                   &d_row_off, &d_row_items, &d_col_off, &d_col_items, &d_leaf};
+    for (DevBuf *x : b) x->release();
+    valid = false;
+  }
+};
+
 struct dmb_ctx {
   int device = 0;
+  // operator of dmb_gmres / dmb_matvec: 0 the resident dense Z, 1 the
+  // H-matrix of dmb_aca_build; aca_transposed: products use A^T (the adjoint
+  // GMRES solves conj-transformed systems)
+  int op_kind = 0;
+  bool aca_transposed = false;
+  AcaState aca;
   cudaStream_t stream = nullptr;
   // factorisation lookahead (created on first use): stream2 takes the rest of
   // each block column's updates, stream3 the trailing matrix beyond the next
@@ -337,6 +385,10 @@ int net_param_count();
 void net_set(dmb_ctx *c, const float *w);
 void net_get(dmb_ctx *c, float *w);
 double now_ms();
+// H-matrix operator (dmb_aca.cu): mode 0 A x, 1 A^H x, 2 A^T x on device
+// complex128 vectors (nrhs columns)
+void aca_apply(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs, int mode);
+bool operator_ready(dmb_ctx *c);
 }  // namespace dmb
 
 // launch bookkeeping: every library kernel launch goes through this macro so

@@ -387,6 +387,10 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
   const int64_t N = c->n;
   const double2 *xd = (const double2 *)x;
   double2 *yd = (double2 *)y;
+  if (c->op_kind == 1) {  // the H-matrix operator of dmb_aca_build
+    aca_apply(c, xd, yd, nrhs, c->aca_transposed ? 2 : 0);
+    return;
+  }
   if (nrhs == 1) {
     unsigned g = blocks_for(N, 8);
     if (c->z_prec == DMB_PREC_FP64)
@@ -421,11 +425,11 @@ void conj_dev(dmb_ctx *c, double2 *x, int64_t count) {
 // tracks the true residual to far below the 1e-6 tolerance and no refinement
 // cycle is needed; the final true residual uses every level.
 bool krylov_exact_int8(dmb_ctx *c, int64_t nrhs) {
-  return c->exact_krylov && c->z_prec == DMB_PREC_MIXED && nrhs >= 32 && oz_available(c);
+  return c->op_kind == 0 && c->exact_krylov && c->z_prec == DMB_PREC_MIXED && nrhs >= 32 && oz_available(c);
 }
 
 bool matvec_op_inexact(dmb_ctx *c, int64_t nrhs) {
-  return !krylov_exact_int8(c, nrhs) && c->z_prec == DMB_PREC_MIXED && nrhs >= c->tc_min_rhs &&
+  return c->op_kind == 0 && !krylov_exact_int8(c, nrhs) && c->z_prec == DMB_PREC_MIXED && nrhs >= c->tc_min_rhs &&
          tc_available(c);
 }
 

@@ -46,6 +46,7 @@ OPT_FAR_TILE = 3
 OPT_EXACT_KRYLOV = 4
 OPT_PRECOND_TF32_TERMS = 5
 OPT_GMRES_GRAPHS = 6
+OPT_OPERATOR = 7
 
 
 class DiffMoMError(RuntimeError):
@@ -109,6 +110,12 @@ class BatchItem(ctypes.Structure):
                 ("solve_ms", ctypes.c_double)]
 
 
+class AcaInfo(ctypes.Structure):
+    _fields_ = [("n_dense", ctypes.c_int64), ("n_lowrank", ctypes.c_int64), ("n_fallback", ctypes.c_int64),
+                ("max_rank_used", ctypes.c_int64), ("entries_stored", ctypes.c_int64),
+                ("n_unconverged", ctypes.c_int64), ("build_ms", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _D = ctypes.c_double
 _I = ctypes.c_int
@@ -163,7 +170,25 @@ SIGNATURES = {
     "dmb_get_stream": ([_P, ctypes.POINTER(ctypes.c_void_p)], _I),
     "dmb_set_kernel_timing": ([_P, _I], _I),
     "dmb_kernel_timing": ([_P, _DP, _LP, _DP], _I),
+    "dmb_aca_plan": ([_DP, _L, _I, _D, _L, _LP, _LP, _LP, _DP, _LP, _LP, _L], _I),
+    "dmb_aca_admissible": ([_DP, _DP, _D, ctypes.POINTER(ctypes.c_int)], _I),
+    "dmb_aca_build": ([_P, _D, _D, _I, _I, _D, _D, _I, _L, _L, ctypes.POINTER(AcaInfo)], _I),
+    "dmb_aca_matvec": ([_P, _DP, _DP, _L, _I], _I),
+    "dmb_aca_blocks": ([_P, _LP], _I),
+    "dmb_aca_block_data": ([_P, _L, _DP, _DP], _I),
+    "dmb_aca_entries": ([_P, _LP, _LP, _L, _DP], _I),
+    "dmb_aca_tree": ([_P, _LP, _DP], _I),
+    "dmb_aca_lowrank": ([_P, _D, _D, _I, _LP, _L, _LP, _L, _D, _I, _L, _DP, _DP, _LP], _I),
+    "dmb_aca_nf_build": ([_P, _I, _I, _DP], _I),
 }
+
+
+def check_free(lib, status: int):
+    """Raise for a failed entry point that takes no context."""
+    if status == DMB_OK:
+        return
+    msg = (lib.dmb_last_error(None) or b"").decode()
+    raise _EXC.get(status, DiffMoMError)(msg or f"libdiffmom_b200 status {status}")
 
 _lib = None
 

@@ -747,20 +747,31 @@ def assemble_multiple_excitations(mesh, rwg, excitations, quad_order=3, device=N
 # ---------------------------------------------------------------------------
 # solvers
 # ---------------------------------------------------------------------------
-def build_nearfield_preconditioner(device: EFIEDevice, cutoff: float, factorization: str = "lu"):
+def build_nearfield_preconditioner(device, cutoff: float | None = None, factorization: str = "lu",
+                                   precision: str = "fp64"):
+    """NearFieldPreconditioner.jl:670-758 for a device with an assembled Z and
+    a distance cutoff; for an ACAOperator (NearFieldPreconditioner.jl:952-1000)
+    the near field is the operator's dense blocks and `cutoff` is unused."""
+    from .aca import ACAOperator
+    if isinstance(device, ACAOperator):
+        return device.build_nearfield(factorization, precision)
+    if cutoff is None:
+        raise ValueError("build_nearfield_preconditioner: a cutoff is required for a dense operator")
     return device.build_nearfield(cutoff, factorization)
 
 
-def solve_gmres(device: EFIEDevice, rhs, preconditioner=None, precond_side="left", tol=1e-8,
+def solve_gmres(device, rhs, preconditioner=None, precond_side="left", tol=1e-8,
                 maxiter=200, check_gmres_convergence=True):
+    """IterativeSolve.jl: GMRES on the dense Z of an EFIEDevice or on an
+    ACAOperator's H-matrix."""
     return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
                         precond_side=precond_side, check_gmres_convergence=check_gmres_convergence)
 
 
-def solve_gmres_adjoint(device: EFIEDevice, rhs, preconditioner=None, precond_side="left", tol=1e-8,
+def solve_gmres_adjoint(device, rhs, preconditioner=None, precond_side="left", tol=1e-8,
                         maxiter=200, check_gmres_convergence=True):
     """IterativeSolve.jl:409-470: GMRES on Z^H x = rhs with the adjoint
-    near-field preconditioner."""
+    near-field preconditioner (dense Z or an ACAOperator)."""
     return device.gmres(rhs, tol=tol, maxiter=maxiter, preconditioner=preconditioner,
                         precond_side=precond_side, check_gmres_convergence=check_gmres_convergence, adjoint=True)
 
@@ -854,18 +865,26 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                      check_gmres_convergence: bool = True, nf_cutoff_lambda: float = 1.0,
                      preconditioner: str = "auto", precond_side: str = "left", quad_order: int = 3,
                      c0: float = C0_DEFAULT, precision: str = "fp64", surface_impedance=None,
-                     verbose: bool = False, device: EFIEDevice | None = None, rwg: RWGData | None = None):
-    """Workflow.jl:67-317 for the dense methods, on the GPU.
+                     verbose: bool = False, device: EFIEDevice | None = None, rwg: RWGData | None = None,
+                     aca_tol: float = 1e-6, aca_leaf_size: int = 64, aca_eta: float = 1.5,
+                     aca_max_rank: int = 50):
+    """Workflow.jl:67-317 on the GPU.
 
-    method: "auto" | "dense_direct" | "dense_gmres".  precision "fp64" is the
+    method: "auto" | "dense_direct" | "dense_gmres" | "aca_gmres".  "auto"
+    picks dense_direct up to dense_direct_limit unknowns and dense_gmres above:
+    the dense matrix of every size the reference sends to ACA (N <= 50,000,
+    40 GB in complex128) fits in one B200's HBM.  "aca_gmres" runs the
+    reference's H-matrix path (build_aca_operator with the aca_* parameters,
+    near-field preconditioner from its dense blocks).  precision "fp64" is the
     plain path; "mixed" assembles far pairs in FP32 (complex64 Z) and factors
-    the preconditioner in FP32 while GMRES keeps FP64 Arnoldi and residuals.
+    the preconditioner in FP32 while GMRES keeps FP64 Arnoldi and residuals
+    (for aca_gmres only the preconditioner is complex64).
     """
     f = float(freq_hz)
     if not (math.isfinite(f) and f > 0):
         raise ValueError(f"solve_scattering: freq_hz must be finite and positive, got {freq_hz}")
-    if method not in ("auto", "dense_direct", "dense_gmres"):
-        raise ValueError("solve_scattering: method must be :auto, :dense_direct, or :dense_gmres")
+    if method not in ("auto", "dense_direct", "dense_gmres", "aca_gmres"):
+        raise ValueError("solve_scattering: method must be :auto, :dense_direct, :dense_gmres, or :aca_gmres")
     if preconditioner not in ("auto", "lu", "diag", "none"):
         raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, or :none")
     lam = c0 / f
@@ -895,14 +914,33 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
             if v.shape != (N,):
                 raise nat.DimensionMismatch(f"solve_scattering: excitation length {v.size} != N={N}")
         t0 = time.perf_counter()
-        dev.assemble(k, quad_order=quad_order, precision=precision)
-        if surface_impedance is not None:
-            dev.apply_impedance(surface_impedance)
+        aca_op = None
+        if sel == "aca_gmres":
+            if surface_impedance is not None:
+                raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres")
+            from .aca import build_aca_operator
+            aca_op = build_aca_operator(mesh, rwg, k, leaf_size=aca_leaf_size, eta=aca_eta, aca_tol=aca_tol,
+                                        max_rank=aca_max_rank, quad_order=quad_order, device=dev)
+        else:
+            dev.assemble(k, quad_order=quad_order, precision=precision)
+            if surface_impedance is not None:
+                dev.apply_impedance(surface_impedance)
         t_asm = time.perf_counter() - t0
         t_pc = 0.0
         iters, resid, tres = -1, float("nan"), float("nan")
         t1 = time.perf_counter()
-        if sel == "dense_direct":
+        if aca_op is not None:
+            pc_used = "lu" if preconditioner == "auto" else preconditioner
+            P = None
+            if pc_used != "none":
+                tp = time.perf_counter()
+                P = aca_op.build_nearfield(pc_used, precision)
+                t_pc = time.perf_counter() - tp
+            t1 = time.perf_counter()
+            I, st = aca_op.gmres(v, tol=gmres_tol, maxiter=gmres_maxiter, preconditioner=P,
+                                 precond_side=precond_side, check_gmres_convergence=check_gmres_convergence)
+            iters, resid, tres = st.niter, st.residual, st.true_residual
+        elif sel == "dense_direct":
             I, berr = dev.solve_direct(v)
             tres = berr
         else:

@@ -82,6 +82,8 @@ typedef struct {
 /* No reference counterpart: owns device buffers, stream and error text. */
 dmb_status dmb_ctx_create(int device, dmb_ctx **out);
 dmb_status dmb_ctx_destroy(dmb_ctx *ctx);
+/* ctx == NULL: the message of the calling thread's last failed call that
+ * takes no context (dmb_aca_plan, dmb_aca_admissible). */
 const char *dmb_last_error(const dmb_ctx *ctx);
 dmb_status dmb_get_timings(dmb_ctx *ctx, dmb_timings *out);
 /* Library version string, e.g. "diffmom_b200 0.1 sm_100a". */
@@ -118,6 +120,10 @@ const char *dmb_version(void);
  * launches every kernel directly.  Results are identical either way.  The
  * lanes of dmb_batch_* contexts launch directly. */
 #define DMB_OPT_GMRES_GRAPHS 6
+/* DMB_OPT_OPERATOR: the operator of dmb_matvec / dmb_gmres / dmb_gmres_adjoint:
+ * 0 the assembled dense Z, 1 the H-matrix of dmb_aca_build (each build or
+ * assembly selects its own; switching drops the preconditioner). */
+#define DMB_OPT_OPERATOR 7
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair tile rows used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
@@ -156,6 +162,7 @@ dmb_status dmb_apply_impedance(dmb_ctx *ctx, const double *zs);
  * (nrhs >= 32, DMB_OPT_EXACT_KRYLOV on) or 3xTF32 (nrhs >= DMB_OPT_TC_MIN_RHS,
  * ~2e-5 relative). */
 dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
+/* (After dmb_aca_build, dmb_matvec applies the context's H-matrix instead.) */
 /* Matrix-free Z*x (MatrixFreeEFIEOperator mul!, src/assembly/EFIE.jl:867-909):
  * entries are recomputed from the geometry on every call, nothing of size
  * N^2 is stored.  Requires a prior dmb_assemble_z or dmb_prepare_operator. */
@@ -350,6 +357,78 @@ dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double
  * trailing updates (3xTF32 tensor cores for complex64 factors; complex flops).
  * dmb_kernel_timing reports family 0. */
 dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
+
+/* ---- H-matrix operator (adaptive cross approximation) ------------------ */
+/* Block plan of build_aca_operator without a GPU: the cluster tree of
+ * build_cluster_tree (src/fast/ClusterTree.jl:82-166; median bisection along
+ * the longest bounding-box axis, stable sort) and the block tasks of
+ * _enum_block_tasks! (src/fast/ACA.jl:696-738) with is_admissible
+ * (src/fast/ClusterTree.jl:223-246, exact decision near the boundary).
+ * centers: n x 3 row-major points.  perm_out (n, may be NULL): tree order ->
+ * original index, 1-based.  nodes_out (5 per node: first, last (1-based tree
+ * order), left, right (1-based node ids, 0 = leaf), level) and boxes_out
+ * (6 per node: bbox_min, bbox_max) may be NULL; *n_nodes_out gets the count.
+ * tasks_out (5 per task: row node, col node (1-based ids), kind 0 = dense,
+ * 1 = low-rank, 0, 0) is written when tasks_cap >= the count, which
+ * *n_tasks_out always receives.  Errors: dmb_last_error(NULL). */
+dmb_status dmb_aca_plan(const double *centers, int64_t n, int leaf_size, double eta, int64_t max_block_tasks,
+                        int64_t *perm_out, int64_t *n_nodes_out, int64_t *nodes_out, double *boxes_out,
+                        int64_t *n_tasks_out, int64_t *tasks_out, int64_t tasks_cap);
+/* is_admissible(tree, i, j; eta) (src/fast/ClusterTree.jl:223-246) for two
+ * boxes given as (bbox_min, bbox_max) 6-vectors; *out = 0 or 1. */
+dmb_status dmb_aca_admissible(const double *box_i, const double *box_j, double eta, int *out);
+
+typedef struct {
+  int64_t n_dense;          /* dense (inadmissible) blocks, fallbacks included */
+  int64_t n_lowrank;        /* low-rank blocks */
+  int64_t n_fallback;       /* admissible blocks stored dense after a non-finite ACA update */
+  int64_t max_rank_used;    /* largest rank of a low-rank block */
+  int64_t entries_stored;   /* complex entries held (dense data + U + V at their ranks) */
+  int64_t n_unconverged;    /* low-rank blocks that reached max_rank without meeting tol */
+  double build_ms;          /* host + device time of the build */
+} dmb_aca_info;
+/* build_aca_operator(mesh, rwg, k; leaf_size, eta, aca_tol, max_rank,
+ * quad_order, eta0, max_block_tasks, max_storage_bytes)
+ * (src/fast/ACA.jl:802-1103) on the device: dense blocks filled with the
+ * FP64 EFIE entries, admissible blocks compressed by partially pivoted ACA
+ * (aca_lowrank, src/fast/ACA.jl:351-554) with the reference's relative
+ * Frobenius stopping rule.  The context's operator becomes this H-matrix:
+ * dmb_gmres / dmb_gmres_adjoint use it until the next dmb_assemble_z. */
+dmb_status dmb_aca_build(dmb_ctx *ctx, double k, double eta0, int quad_order, int leaf_size, double eta,
+                         double aca_tol, int max_rank, int64_t max_block_tasks, int64_t max_storage_bytes,
+                         dmb_aca_info *info_out);
+/* mode 0: y = A x (mul!, src/fast/ACA.jl:1130-1221); 1: y = A^H x
+ * (ACAAdjointOperator, :1231-1323); 2: y = A^T x.  nrhs column-major
+ * right-hand sides, host buffers. */
+dmb_status dmb_aca_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs, int mode);
+/* Blocks in task order, 7 per block: kind (0 dense, 1 low-rank), first row,
+ * last row, first column, last column (1-based tree order), rank (low-rank)
+ * or 0, 1 when the block is a dense fallback of an admissible task. */
+dmb_status dmb_aca_blocks(dmb_ctx *ctx, int64_t *out);
+/* Data of block b (0-based, task order): dense: a_out = m x n column-major;
+ * low-rank: a_out = U (m x rank), b_out = V (n x rank), block = U V^H. */
+dmb_status dmb_aca_block_data(dmb_ctx *ctx, int64_t b, double *a_out, double *b_out);
+/* getindex(A::ACAOperator, i, j) (src/fast/ACA.jl:220-222): EFIE entries
+ * evaluated on the device (1-based m, n). */
+dmb_status dmb_aca_entries(dmb_ctx *ctx, const int64_t *m, const int64_t *n, int64_t count, double *out);
+/* The operator's tree permutation (tree order -> original index, 1-based;
+ * may be NULL) and the RWG centres it was built on (n x 3 row-major; may be
+ * NULL). */
+dmb_status dmb_aca_tree(dmb_ctx *ctx, int64_t *perm_out, double *centers_out);
+/* aca_lowrank(cache, row_indices, col_indices; tol, max_rank,
+ * max_output_bytes) (src/fast/ACA.jl:351-554) on one block of RWG index lists
+ * (1-based) with the EFIE entries of (k, eta0, quad_order).  U_out (m x r) and
+ * V_out (n x r) must hold min(max_rank, m, n) columns; *rank_out = r.  A
+ * non-finite update fails with DMB_ERR_OVERFLOW. */
+dmb_status dmb_aca_lowrank(dmb_ctx *ctx, double k, double eta0, int quad_order, const int64_t *rows, int64_t m,
+                           const int64_t *cols, int64_t n, double tol, int max_rank, int64_t max_output_bytes,
+                           double *U_out, double *V_out, int64_t *rank_out);
+/* build_nearfield_preconditioner(A_aca; factorization)
+ * (src/solver/NearFieldPreconditioner.jl:952-1000): the near-field matrix is
+ * the union of the operator's dense blocks.  kind: DMB_PRECOND_NF_LU or
+ * DMB_PRECOND_NF_DIAG; precision: DMB_PREC_FP64 (complex128 factor) or
+ * DMB_PREC_MIXED (complex64 factor on the tensor cores). */
+dmb_status dmb_aca_nf_build(dmb_ctx *ctx, int kind, int precision, double *nnz_ratio_out);
 
 /* ---- far field --------------------------------------------------------- */
 /* radiation_vectors + compute_farfield (src/postprocessing/FarField.jl:

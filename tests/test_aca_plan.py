@@ -1,0 +1,189 @@
+"""Cluster tree, admissibility and block tasks of the H-matrix operator: the
+library's host code (dmb_aca_plan / dmb_aca_admissible, no GPU) against the
+oracle's restatement of src/fast/ClusterTree.jl and src/fast/ACA.jl:696-738,
+and the oracle itself against facts the reference's tests state."""
+import math
+
+import numpy as np
+import pytest
+
+from diffmom_b200 import (make_rect_plate, make_circular_plate, build_rwg, rwg_centers, build_cluster_tree,
+                          aca_block_tasks, is_admissible, leaf_nodes, cluster_diameter, cluster_distance)
+from diffmom_b200 import _native as nat
+
+import aca_oracle as ao
+
+
+def _plate_centers(nx, ny, a=1.0, b=1.0):
+    m = make_rect_plate(a, b, nx, ny)
+    return rwg_centers(m, build_rwg(m))
+
+
+def _compare(centers, leaf, eta):
+    tree = build_cluster_tree(centers, leaf)
+    otree = ao.build_cluster_tree(centers, leaf)
+    np.testing.assert_array_equal(tree.perm - 1, otree.perm)
+    assert len(tree.nodes) == len(otree.nodes)
+    for nd, on in zip(tree.nodes, otree.nodes):
+        assert (nd.indices.start - 1, nd.indices.stop - 2) == (on.lo, on.hi)
+        assert (nd.left - 1, nd.right - 1, nd.level) == (on.left, on.right, on.level)
+        assert tuple(nd.bbox_min) == on.bmin and tuple(nd.bbox_max) == on.bmax
+    tasks = aca_block_tasks(centers, leaf, eta)
+    otasks = ao.enum_block_tasks(otree, eta)
+    assert [(r - 1, c - 1, 1 if k == "lowrank" else 0) for r, c, k in tasks] == otasks
+    return tree, otasks
+
+
+def test_oracle_pins_reference_scale_fixture():
+    # the reference's scale-invariance test: make_rect_plate(1.0, 1.0, 1, 2)
+    # with leaf_size=1, eta=1.5 has four admissible far blocks, each of rank
+    # at most one (three collinear centres: two 1x1 blocks between the leaves
+    # of the two-point cluster, and that cluster against the third point)
+    c = _plate_centers(1, 2)
+    assert c.shape[0] == 3
+    tree = ao.build_cluster_tree(c, 1)
+    tasks = ao.enum_block_tasks(tree, 1.5)
+    far = [t for t in tasks if t[2] == 1]
+    assert len(far) == 4
+    shapes = sorted((tree.nodes[rn].hi - tree.nodes[rn].lo + 1, tree.nodes[cn].hi - tree.nodes[cn].lo + 1)
+                    for rn, cn, _ in far)
+    assert shapes == [(1, 1), (1, 1), (1, 2), (2, 1)]
+    # every ordered pair of unknowns lies in exactly one block
+    cover = np.zeros((3, 3), int)
+    for rn, cn, _ in tasks:
+        r, cc = tree.nodes[rn], tree.nodes[cn]
+        cover[r.lo:r.hi + 1, cc.lo:cc.hi + 1] += 1
+    assert np.all(cover == 1)
+
+
+@pytest.mark.parametrize("leaf,eta", [(1, 1.5), (4, 1.0), (8, 1.5), (64, 1.5), (16, 0.8)])
+def test_plan_matches_oracle_on_plates(leaf, eta):
+    # regular plates: many equal coordinates, so the stable median split and
+    # boundary-exact admissibility both matter
+    for nx, ny in ((6, 6), (20, 20), (24, 7)):
+        c = _plate_centers(nx, ny)
+        _compare(c, leaf, eta)
+
+
+def test_plan_matches_oracle_on_curved_and_random_points():
+    m = make_circular_plate(0.5, 8, 24)
+    _compare(rwg_centers(m, build_rwg(m)), 8, 1.5)
+    rng = np.random.default_rng(7)
+    pts = rng.standard_normal((700, 3))
+    pts[::7, 2] = 0.0
+    pts[1::7, 2] = -0.0
+    _compare(pts, 16, 1.5)
+    _compare(pts, 3, 2.0)
+
+
+def test_tasks_tile_the_matrix():
+    c = _plate_centers(12, 10)
+    tree, tasks = _compare(c, 8, 1.5)
+    N = c.shape[0]
+    cover = np.zeros((N, N), np.int8)
+    for rn, cn, _ in tasks:
+        r, cc = tree.nodes[rn], tree.nodes[cn]
+        cover[r.indices.start - 1:r.indices.stop - 1, cc.indices.start - 1:cc.indices.stop - 1] += 1
+    assert np.all(cover == 1)
+    # dense blocks pair leaves; the diagonal blocks are never admissible
+    leaves = set(leaf_nodes(tree))
+    for rn, cn, kind in tasks:
+        if kind == 0:
+            assert rn + 1 in leaves and cn + 1 in leaves
+        if rn == cn:
+            assert kind == 0
+
+
+def _box(lo, hi):
+    return ao.Node(0, 0, tuple(lo), tuple(hi))
+
+
+def test_admissibility_exact_on_the_boundary():
+    lib = nat.load_library()
+
+    def lib_adm(a, b, eta):
+        out = nat.ctypes.c_int()
+        bi = np.array(a.bmin + a.bmax, dtype=np.float64)
+        bj = np.array(b.bmin + b.bmax, dtype=np.float64)
+        nat.check_free(lib, lib.dmb_aca_admissible(nat.dptr(bi), nat.dptr(bj), eta, nat.ctypes.byref(out)))
+        return bool(out.value)
+
+    cases = []
+    # diameter 0.3 (in units that are not binary fractions) and gap exactly
+    # 0.2: 0.3 <= 1.5 * 0.2 sits on the boundary in exact arithmetic of the
+    # stored doubles or one ulp beside it
+    for x0 in (0.0, 0.1, 1e-3, 7.0):
+        for d in (0.3, 0.1 * 3, 3.0, 0.7):
+            for g in (d / 1.5, math.nextafter(d / 1.5, 0), math.nextafter(d / 1.5, 1)):
+                a = _box((x0, 0.0, 0.0), (x0 + d, d / 2, 0.0))
+                b = _box((x0 + d + g, 0.0, 0.0), (x0 + 2 * d + g, d, 0.0))
+                cases.append((a, b, 1.5))
+    # diagonal gaps: |gap| = sqrt(gx^2 + gy^2)
+    for gx, gy in ((0.3, 0.4), (3.0, 4.0), (0.1, 0.2)):
+        a = _box((0.0, 0.0, 0.0), (0.75, 0.75, 0.0))
+        b = _box((0.75 + gx, 0.75 + gy, 0.0), (1.5 + gx, 1.5 + gy, 0.0))
+        cases.append((a, b, 0.75 / math.hypot(gx, gy)))
+        cases.append((a, b, math.nextafter(0.75 / math.hypot(gx, gy), 0)))
+    seen = set()
+    for a, b, eta in cases:
+        o = ao.box_admissible(a, b, eta)
+        assert lib_adm(a, b, eta) == o
+        assert lib_adm(b, a, eta) == ao.box_admissible(b, a, eta)
+        seen.add(o)
+    assert seen == {True, False}
+
+
+def test_plan_errors():
+    c = _plate_centers(2, 2)
+    with pytest.raises(ValueError, match="leaf_size"):
+        build_cluster_tree(c, 0)
+    with pytest.raises(ValueError, match="eta"):
+        aca_block_tasks(c, 1, float("nan"))
+    with pytest.raises(ValueError, match="eta"):
+        aca_block_tasks(c, 1, 0.0)
+    with pytest.raises(ValueError, match="max_block_tasks"):
+        aca_block_tasks(c, 1, 1.5, max_block_tasks=1)
+    with pytest.raises(ValueError, match="empty"):
+        build_cluster_tree(np.zeros((0, 3)), 4)
+    bad = c.copy()
+    bad[2, 1] = np.inf
+    with pytest.raises(ValueError, match="finite"):
+        build_cluster_tree(bad, 4)
+
+
+def test_tree_helpers():
+    c = _plate_centers(10, 10)
+    tree = build_cluster_tree(c, 8)
+    leaves = leaf_nodes(tree)
+    assert sum(len(tree.nodes[i - 1].indices) for i in leaves) == c.shape[0]
+    np.testing.assert_array_equal(tree.iperm[tree.perm - 1], np.arange(1, c.shape[0] + 1))
+    ot = ao.build_cluster_tree(c, 8)
+    for i in (1, 2, leaves[0], leaves[-1]):
+        assert cluster_diameter(tree, i) == ao.cluster_diameter(ot, i - 1)
+    for i, j in ((leaves[0], leaves[-1]), (leaves[1], leaves[5]), (2, 3)):
+        assert is_admissible(tree, i, j, 1.5) == ao.is_admissible(ot, i - 1, j - 1, 1.5)
+        assert cluster_distance(tree, i, j) >= 0
+
+
+def test_oracle_aca_and_product_on_a_smooth_kernel():
+    # two separated point clouds: exp(-i k r) / r between them is numerically
+    # low rank, the oracle's ACA meets its relative tolerance, and the
+    # H-matrix product of oracle blocks equals the dense product
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0, 1, (60, 3))
+    y = rng.uniform(0, 1, (50, 3)) + np.array([4.0, 0, 0])
+    r = np.linalg.norm(x[:, None] - y[None], axis=2)
+    B = np.exp(-2j * r) / r
+    for tol in (1e-4, 1e-8):
+        U, V, conv = ao.aca_lowrank(B, tol, 50)
+        assert conv and U.shape[1] < 50
+        assert np.linalg.norm(U @ V.conj().T - B) <= 10 * tol * np.linalg.norm(B)
+    pts = np.vstack([x, y])
+    rr = np.linalg.norm(pts[:, None] - pts[None], axis=2) + np.eye(110)
+    Z = np.exp(-2j * rr) / rr
+    tree, tasks, blocks = ao.build_hmatrix(Z, pts, leaf_size=8, eta=1.5, aca_tol=1e-10, max_rank=40)
+    assert any(b.kind == 1 for b in blocks)
+    v = rng.standard_normal(110) + 1j * rng.standard_normal(110)
+    for mode, A in ((0, Z), (1, Z.conj().T), (2, Z.T)):
+        y_h = ao.hmatrix_matvec(blocks, tree.perm, v, mode)
+        assert np.linalg.norm(y_h - A @ v) <= 1e-8 * np.linalg.norm(A @ v)

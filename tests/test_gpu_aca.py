@@ -1,0 +1,270 @@
+"""H-matrix (ACA) operator on the GPU against the oracle's restatement of
+src/fast/ACA.jl and against the dense FP64 Z, mirroring the reference's
+tests 25-27 (ACA accuracy, operator products, forward and adjoint solves) and
+its scale-invariance checks of the stopping rule."""
+import math
+
+import numpy as np
+import pytest
+
+from diffmom_b200 import (EFIEDevice, make_rect_plate, build_rwg, rwg_centers, build_aca_operator,
+                          build_nearfield_preconditioner, solve_gmres, solve_gmres_adjoint, build_efie_cache,
+                          efie_cache_with_prefactor_scale, aca_lowrank, solve_scattering, make_plane_wave)
+from diffmom_b200 import _native as nat
+import aca_oracle as ao
+
+pytestmark = pytest.mark.gpu
+
+C0 = 299792458.0
+K3 = 2 * math.pi * 3e9 / C0
+
+
+def _plate(n, side=0.1):
+    m = make_rect_plate(side, side, n, n)
+    return m, build_rwg(m)
+
+
+def _dense(m, r, k, quad_order=3, eta0=376.730313668):
+    dev = EFIEDevice(m, r)
+    Z = dev.assemble(k, quad_order=quad_order, eta0=eta0, precision="fp64", copy_out=True)
+    dev.close()
+    return Z
+
+
+def test_blocks_match_oracle_plan_and_entries():
+    # 736-RWG plate: tree and tasks equal the oracle's on the device's centres;
+    # dense blocks equal the oracle's Z entries; every ACA block meets the
+    # tolerance with the oracle's ranks
+    import oracle as orc
+    m, r = _plate(16)
+    A = build_aca_operator(m, r, K3, leaf_size=16, eta=1.5, aca_tol=1e-8, max_rank=50)
+    N = r.nedges
+    ctr = np.empty((N, 3))
+    A.device.ctx.call("dmb_aca_tree", None, nat.dptr(ctr))
+    np.testing.assert_allclose(ctr, rwg_centers(m, r), rtol=0, atol=1e-15)
+    tree = ao.build_cluster_tree(ctr, 16)
+    tasks = ao.enum_block_tasks(tree, 1.5)
+    np.testing.assert_array_equal(A.perm - 1, tree.perm)
+    assert len(A.dense_blocks) + len(A.lowrank_blocks) == len(tasks)
+    assert A.info["n_fallback"] == 0 and len(A.lowrank_blocks) > 0
+    blocks = sorted(A.dense_blocks + A.lowrank_blocks, key=lambda b: b.index)
+    for b, (rn, cn, kind) in zip(blocks, tasks):
+        rr, cc = tree.nodes[rn], tree.nodes[cn]
+        assert (b.row_range.start - 1, b.row_range.stop - 2, b.col_range.start - 1, b.col_range.stop - 2) == \
+            (rr.lo, rr.hi, cc.lo, cc.hi)
+        assert (kind == 1) == hasattr(b, "rank")
+    Zo = orc.OracleCache(m, r, 3).assemble_z(K3)
+    Zd = _dense(m, r, K3)
+    p = A.perm - 1
+    zmax = np.abs(Zo).max()
+    bitwise = total = 0
+    for b in A.dense_blocks:
+        rows, cols = p[b.row_range.start - 1:b.row_range.stop - 1], p[b.col_range.start - 1:b.col_range.stop - 1]
+        D = b.data
+        assert np.abs(D - Zo[np.ix_(rows, cols)]).max() <= 1e-12 * zmax
+        Dd = Zd[np.ix_(rows, cols)]
+        assert np.abs(D - Dd).max() <= 1e-15 * zmax
+        bitwise += int(np.sum(D == Dd))
+        total += D.size
+    same = worst = 0
+    for b in A.lowrank_blocks:
+        rows, cols = p[b.row_range.start - 1:b.row_range.stop - 1], p[b.col_range.start - 1:b.col_range.stop - 1]
+        S = Zo[np.ix_(rows, cols)]
+        err = np.linalg.norm(b.U @ b.V.conj().T - S) / np.linalg.norm(S)
+        worst = max(worst, err)
+        _, Vo, _ = ao.aca_lowrank(S, 1e-8, 50)
+        same += int(Vo.shape[1] == b.rank)
+        assert abs(Vo.shape[1] - b.rank) <= 2
+    print(f"dense entries bitwise equal to the dense assembly: {bitwise}/{total}; "
+          f"ACA ranks equal to the oracle's: {same}/{len(A.lowrank_blocks)}; worst block error {worst:.2e}")
+    assert worst <= 1e-6
+    assert same >= 0.9 * len(A.lowrank_blocks)
+    A.close()
+
+
+@pytest.mark.parametrize("leaf", [8, 32])
+def test_products_match_dense_and_oracle(leaf):
+    # reference test 26: leaf_size=8, eta=1.5, aca_tol=1e-8, max_rank=50;
+    # matvec and adjoint matvec within 1e-5 of the dense product
+    m, r = _plate(24)
+    A = build_aca_operator(m, r, K3, leaf_size=leaf, eta=1.5, aca_tol=1e-8, max_rank=50)
+    Z = _dense(m, r, K3)
+    rng = np.random.default_rng(42)
+    x = rng.standard_normal(A.N) + 1j * rng.standard_normal(A.N)
+    errs = []
+    for mode, M in ((0, Z), (1, Z.conj().T), (2, Z.T)):
+        y = A.matvec(x, mode)
+        ref = M @ x
+        errs.append(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+    print(f"leaf {leaf}: {len(A.dense_blocks)} dense, {len(A.lowrank_blocks)} low-rank blocks, "
+          f"max rank {A.info['max_rank_used']}; product errors vs dense (A, A^H, A^T) "
+          + ", ".join(f"{e:.2e}" for e in errs))
+    assert max(errs) < 1e-5
+    # the same blocks through the oracle's product: only summation order differs
+    ob = []
+    for b in sorted(A.dense_blocks + A.lowrank_blocks, key=lambda b: b.index):
+        r0, mm = b.row_range.start - 1, len(b.row_range)
+        c0, nn = b.col_range.start - 1, len(b.col_range)
+        if hasattr(b, "rank"):
+            ob.append(ao.Block(1, r0, mm, c0, nn, U=b.U, V=b.V))
+        else:
+            ob.append(ao.Block(0, r0, mm, c0, nn, data=b.data))
+    for mode in (0, 1, 2):
+        y = A.matvec(x, mode)
+        yo = ao.hmatrix_matvec(ob, A.perm - 1, x, mode)
+        assert np.linalg.norm(y - yo) <= 1e-13 * np.linalg.norm(yo)
+    # several right-hand sides at once equal the columns one at a time
+    X = np.asfortranarray(rng.standard_normal((A.N, 3)) + 1j * rng.standard_normal((A.N, 3)))
+    Y = A @ X
+    for j in range(3):
+        np.testing.assert_array_equal(Y[:, j], A @ np.ascontiguousarray(X[:, j]))
+    A.close()
+
+
+def test_entries_equal_dense_entries():
+    # getindex falls back to entry evaluation (ACA.jl:220-222); the reference
+    # requires A_aca[i, j] == Z_efie[i, j]
+    m, r = _plate(16)
+    A = build_aca_operator(m, r, K3, leaf_size=8)
+    Z = _dense(m, r, K3)
+    rng = np.random.default_rng(1)
+    i = rng.integers(1, A.N + 1, 300)
+    j = rng.integers(1, A.N + 1, 300)
+    i[:20] = j[:20]  # diagonal (self terms)
+    e = A.entries(i, j)
+    ref = Z[i - 1, j - 1]
+    assert np.abs(e - ref).max() <= 1e-15 * np.abs(Z).max()
+    print(f"entries bitwise equal: {int(np.sum(e == ref))}/300")
+    assert A[3, 5] == complex(A.entries([4], [6])[0])
+    assert A.H[3, 5] == complex(np.conj(A.entries([6], [4])[0]))
+    A.close()
+
+
+def test_scale_invariance_of_the_relative_tolerance():
+    # reference test 25: a common physical scale (eta0 = 1 or 1e-100) must
+    # not change the ranks, and each approximation stays within 1e-12
+    m = make_rect_plate(1.0, 1.0, 1, 2)
+    r = build_rwg(m)
+    ranks, errs = [], []
+    for eta0 in (1.0, 1e-100):
+        A = build_aca_operator(m, r, 2 * math.pi, leaf_size=1, eta=1.5, aca_tol=1e-6, max_rank=3, quad_order=1,
+                               eta0=eta0)
+        Z = _dense(m, r, 2 * math.pi, quad_order=1, eta0=eta0)
+        ranks.append([b.rank for b in A.lowrank_blocks])
+        errs.append(np.linalg.norm(A.to_dense() - Z) / np.linalg.norm(Z))
+        A.close()
+    assert ranks[0] == ranks[1]
+    assert ranks[1] and all(x > 0 for x in ranks[1])
+    assert max(errs) <= 1e-12
+
+
+def test_stopping_rule_scale_invariant_at_extreme_scales():
+    # reference test 25: a block that converges before its rank limit keeps
+    # its rank and factors when every prefactor is scaled by 1e-200 or 1e200
+    m = make_rect_plate(2.0, 1.0, 6, 3)
+    r = build_rwg(m)
+    A = build_aca_operator(m, r, 2 * math.pi, leaf_size=4, eta=1.0, aca_tol=0.1, max_rank=6, quad_order=1,
+                           eta0=1.0)
+    blk = next(b for b in A.lowrank_blocks if b.rank < min(len(b.row_range), len(b.col_range), 6))
+    rows = A.perm[blk.row_range.start - 1:blk.row_range.stop - 1]
+    cols = A.perm[blk.col_range.start - 1:blk.col_range.stop - 1]
+    ref = blk.U @ blk.V.conj().T
+    cache = build_efie_cache(m, r, 2 * math.pi, quad_order=1, eta0=1.0, device=A.device)
+    U0, V0 = aca_lowrank(cache, rows, cols, tol=0.1, max_rank=6)
+    assert U0.shape[1] == blk.rank
+    np.testing.assert_allclose(U0 @ V0.conj().T, ref, rtol=1e-13, atol=0)
+    for scale in (1e-200, 1e200):
+        U, V = aca_lowrank(efie_cache_with_prefactor_scale(cache, 2 * math.pi, scale), rows, cols, tol=0.1,
+                           max_rank=6)
+        assert U.shape[1] == blk.rank
+        np.testing.assert_allclose((U @ V.conj().T) / scale, ref, rtol=5e-13, atol=0)
+    A.close()
+
+
+def test_forward_and_adjoint_solves():
+    # reference test 27: GMRES on the H-matrix with the near-field
+    # preconditioner of its dense blocks, against the dense direct solutions
+    m, r = _plate(24)
+    A = build_aca_operator(m, r, K3, leaf_size=8, eta=1.5, aca_tol=1e-8, max_rank=50)
+    Z = _dense(m, r, K3)
+    dev = EFIEDevice(m, r)
+    v = dev.plane_wave_rhs(np.array([[0, 0, -K3]]), [1.0], np.array([[1.0, 0, 0]]))[:, 0]
+    dev.close()
+    P = build_nearfield_preconditioner(A, factorization="lu")
+    assert 0 < P.nnz_ratio < 1
+    I, st = solve_gmres(A, v, preconditioner=P, tol=1e-8, maxiter=300)
+    I_ref = np.linalg.solve(Z, v)
+    err = np.linalg.norm(I - I_ref) / np.linalg.norm(I_ref)
+    rng = np.random.default_rng(5)
+    rhs_adj = (rng.standard_normal(A.N) + 1j * rng.standard_normal(A.N)) * np.abs(I)
+    lam, st_a = solve_gmres_adjoint(A, rhs_adj, preconditioner=P, tol=1e-8, maxiter=300)
+    lam_ref = np.linalg.solve(Z.conj().T, rhs_adj)
+    err_a = np.linalg.norm(lam - lam_ref) / np.linalg.norm(lam_ref)
+    # residual of the adjoint system on A^H itself (left preconditioning: the
+    # 1e-8 tolerance holds for the preconditioned residual)
+    res_a = np.linalg.norm(A.matvec(lam, 1) - rhs_adj) / np.linalg.norm(rhs_adj)
+    print(f"forward: {st.niter} iterations, error vs direct {err:.2e}; adjoint: {st_a.niter} iterations, "
+          f"error {err_a:.2e}, ||A^H lam - b|| / ||b|| {res_a:.2e}")
+    assert err < 1e-4 and err_a < 1e-3 and res_a <= 1e-6
+    assert abs(res_a - st_a.true_residual) <= 1e-2 * res_a + 1e-12
+    # Jacobi and complex64 near-field factors also converge
+    for fac, prec in (("diag", "fp64"), ("lu", "mixed")):
+        Pk = build_nearfield_preconditioner(A, factorization=fac, precision=prec)
+        I2, st2 = solve_gmres(A, v, preconditioner=Pk, tol=1e-8, maxiter=300)
+        assert np.linalg.norm(I2 - I_ref) / np.linalg.norm(I_ref) < 1e-4
+    A.close()
+
+
+def test_solve_scattering_aca_path():
+    m, r = _plate(24)
+    pw = make_plane_wave(np.array([0, 0, -K3]), 1.0, np.array([1.0, 0, 0]))
+    ra = solve_scattering(m, 3e9, pw, method="aca_gmres", gmres_tol=1e-8, aca_tol=1e-8, aca_leaf_size=16, rwg=r)
+    rd = solve_scattering(m, 3e9, pw, method="dense_gmres", gmres_tol=1e-8, rwg=r)
+    assert ra.method == "aca_gmres" and ra.true_residual <= 1e-7
+    assert np.linalg.norm(ra.I_coeffs - rd.I_coeffs) / np.linalg.norm(rd.I_coeffs) < 1e-4
+
+
+def test_argument_errors():
+    m = make_rect_plate(1.0, 1.0, 2, 2)
+    r = build_rwg(m)
+    k = 2 * math.pi
+    for kw in ({"aca_tol": math.inf}, {"aca_tol": 0.0}, {"max_rank": 0}, {"leaf_size": 0}, {"eta": math.nan},
+               {"max_block_tasks": 0}, {"max_storage_bytes": 0}, {"max_green_cache_bytes": 0},
+               {"max_green_cache_entries": -1}, {"max_adjacency_pairs": 0}, {"max_cache_bytes": 1}):
+        with pytest.raises(ValueError):
+            build_aca_operator(m, r, k, **kw)
+    with pytest.raises(ValueError, match="max_block_tasks"):
+        build_aca_operator(m, r, k, leaf_size=1, eta=1.5, max_block_tasks=1)
+    with pytest.raises(ValueError, match="max_storage_bytes"):
+        build_aca_operator(m, r, k, max_storage_bytes=1)
+    with pytest.raises(ValueError, match="max_green_cache_bytes"):
+        build_aca_operator(m, r, k, quad_order=3, max_green_cache_bytes=16 * 9 - 1)
+    cache = build_efie_cache(m, r, k)
+    for kw in ({"tol": 0.0}, {"tol": math.inf}, {"tol": math.nan}, {"max_rank": 0}, {"max_rank": -1}):
+        with pytest.raises(ValueError):
+            aca_lowrank(cache, [1], [1], **kw)
+    with pytest.raises(ValueError, match="max_output_bytes"):
+        aca_lowrank(cache, [1], [1], tol=1e-6, max_rank=1, max_output_bytes=2 * 16 - 1)
+    cache.device.close()
+
+
+def test_full_size_plate_product():
+    # 10,680-RWG plate (0.3 m, 3 lambda at 3 GHz) with the reference's
+    # solve_scattering defaults (leaf 64, eta 1.5, tol 1e-6, max rank 50): the
+    # H-matrix product tracks the dense FP64 product to the ACA tolerance
+    m, r = _plate(60, side=0.3)
+    A = build_aca_operator(m, r, K3)
+    dev = EFIEDevice(m, r)
+    dev.assemble(K3, precision="fp64")
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(A.N) + 1j * rng.standard_normal(A.N)
+    y = A @ x
+    ref = dev.matvec(x)
+    err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    comp = A.info["entries_stored"] / A.N ** 2
+    print(f"N={A.N}: build {A.info['build_ms']:.1f} ms, {len(A.dense_blocks)} dense / {len(A.lowrank_blocks)} "
+          f"low-rank blocks, max rank {A.info['max_rank_used']}, stored {comp:.3f} of dense, product error {err:.2e}")
+    assert err < 1e-4
+    assert comp < 0.5
+    dev.close()
+    A.close()
