@@ -789,7 +789,7 @@ dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *
 
 dmb_status dmb_kernel_timing_family(dmb_ctx *c, int family, double *ms, int64_t *launches, double *work) {
   return guarded(c, [&] {
-    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1 or 2");
+    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1, 2 or 3");
     kt_collect(c);
     if (ms) *ms = c->kt_ms[family];
     if (launches) *launches = c->kt_launches[family];

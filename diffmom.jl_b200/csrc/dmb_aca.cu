@@ -13,11 +13,12 @@
 //            entry is evaluated on the fly with the same arithmetic as the
 //            dense assembly: the far triangle-pair value of its four slot
 //            pairs plus the precomputed singular records of near pairs.
-//   product  y = A x as three launches per right-hand side: gather x into tree
-//            order, t_b = V_b^H x_b for every low-rank block, then one CTA per
-//            leaf sums its dense rows and U_b t_b of every block covering the
-//            leaf and scatters to the original order.  Fixed summation order,
-//            no atomics; the adjoint and the transpose walk the column leaves.
+//   product  y = A x as four launches per right-hand side: gather x into tree
+//            order; t_b = V_b^H x_b for every low-rank block; the partial
+//            product of every block (D_b x_b or U_b t_b, one CTA per block);
+//            per leaf, the partials of the blocks covering it summed and
+//            scattered to the original order.  Fixed summation order, no
+//            atomics; the adjoint and the transpose use the column side.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -866,68 +867,92 @@ __global__ void __launch_bounds__(256) k_aca_inner(const AcaBlockDesc *__restric
   }
 }
 
-// forward: one CTA per row leaf; items = blocks whose row range covers it
-__global__ void __launch_bounds__(128) k_aca_rows(const AcaBlockDesc *__restrict__ blocks, const int2 *__restrict__ leaf,
-                                                  const int64_t *__restrict__ off, const int *__restrict__ items,
-                                                  const int *__restrict__ rank, const int64_t *__restrict__ toff,
-                                                  const double2 *__restrict__ arena, const double2 *__restrict__ xp,
-                                                  const double2 *__restrict__ t, const int *__restrict__ perm,
-                                                  double2 *__restrict__ y) {
-  const int2 L = leaf[blockIdx.x];
-  for (int i = L.x + threadIdx.x; i < L.x + L.y; i += blockDim.x) {
-    double2 acc = make_double2(0, 0);
-    for (int64_t q = off[blockIdx.x]; q < off[blockIdx.x + 1]; q++) {
-      const int b = items[q];
-      const AcaBlockDesc bd = blocks[b];
-      const int ii = i - bd.r0;
-      if (bd.kind == 0) {
-        const double2 *D = arena + bd.off_a + ii;
-        const double2 *xs = xp + bd.c0;
-        for (int jj = 0; jj < bd.n; jj++) acc = cadd(acc, cmul(D[(int64_t)jj * bd.m], xs[jj]));
-      } else {
-        const double2 *Ui = arena + bd.off_a + ii;
-        const double2 *tb = t + toff[b];
-        const int r = rank[b];
-        for (int p = 0; p < r; p++) acc = cadd(acc, cmul(Ui[(int64_t)p * bd.m], tb[p]));
+// Partial product of every block (one CTA each).  mode 0: z_b = D_b x_cols
+// (dense) or U_b t_b (low-rank), m_b entries at zoff[b]; mode 1 / 2: the
+// column side, n_b entries: D_b^H x_rows / D_b^T x_rows, or V_b t_b /
+// conj(V_b) t_b.
+__global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__restrict__ blocks,
+                                                      const int *__restrict__ rank, const int64_t *__restrict__ toff,
+                                                      const int64_t *__restrict__ zoff,
+                                                      const double2 *__restrict__ arena,
+                                                      const double2 *__restrict__ xp, const double2 *__restrict__ t,
+                                                      int mode, double2 *__restrict__ z) {
+  __shared__ double2 part[256];
+  const int b = blockIdx.x;
+  const AcaBlockDesc bd = blocks[b];
+  double2 *zb = z + zoff[b];
+  const int tid = threadIdx.x;
+  if (mode == 0) {
+    if (bd.kind == 0) {
+      // 64 rows x 4 column groups per pass; the groups are summed in order
+      const double2 *D = arena + bd.off_a, *xs = xp + bd.c0;
+      const int ri = tid & 63, g = tid >> 6;
+      for (int i0 = 0; i0 < bd.m; i0 += 64) {
+        const int i = i0 + ri;
+        double2 acc = make_double2(0, 0);
+        if (i < bd.m)
+          for (int jj = g; jj < bd.n; jj += 4) acc = cadd(acc, cmul(D[i + (int64_t)jj * bd.m], xs[jj]));
+        part[tid] = acc;
+        __syncthreads();
+        if (tid < 64 && i < bd.m)
+          zb[i] = cadd(cadd(part[tid], part[tid + 64]), cadd(part[tid + 128], part[tid + 192]));
+        __syncthreads();
+      }
+    } else {
+      const double2 *U = arena + bd.off_a, *tb = t + toff[b];
+      const int r = rank[b];
+      for (int i = tid; i < bd.m; i += blockDim.x) {
+        double2 acc = make_double2(0, 0);
+        for (int p = 0; p < r; p++) acc = cadd(acc, cmul(U[i + (int64_t)p * bd.m], tb[p]));
+        zb[i] = acc;
       }
     }
-    y[perm[i]] = acc;
+    return;
+  }
+  const bool adj = mode == 1;
+  if (bd.kind == 0) {
+    // a warp per column: the column is contiguous in the block
+    const double2 *D = arena + bd.off_a, *xs = xp + bd.r0;
+    const int lane = tid & 31, nw = blockDim.x >> 5;
+    for (int jj = tid >> 5; jj < bd.n; jj += nw) {
+      const double2 *Dj = D + (int64_t)jj * bd.m;
+      double2 acc = make_double2(0, 0);
+      for (int ii = lane; ii < bd.m; ii += 32) acc = cadd(acc, cmul(adj ? cconj(Dj[ii]) : Dj[ii], xs[ii]));
+      acc = warp_sum2(acc);
+      if (lane == 0) zb[jj] = acc;
+    }
+  } else {
+    const double2 *V = arena + bd.off_b, *tb = t + toff[b];
+    const int r = rank[b];
+    for (int j = tid; j < bd.n; j += blockDim.x) {
+      double2 acc = make_double2(0, 0);
+      for (int p = 0; p < r; p++) {
+        const double2 v = V[j + (int64_t)p * bd.n];
+        acc = cadd(acc, cmul(adj ? v : cconj(v), tb[p]));
+      }
+      zb[j] = acc;
+    }
   }
 }
 
-// adjoint (mode 1) / transpose (mode 2): one CTA per column leaf
-__global__ void __launch_bounds__(128) k_aca_cols(const AcaBlockDesc *__restrict__ blocks, const int2 *__restrict__ leaf,
-                                                  const int64_t *__restrict__ off, const int *__restrict__ items,
-                                                  const int *__restrict__ rank, const int64_t *__restrict__ toff,
-                                                  const double2 *__restrict__ arena, const double2 *__restrict__ xp,
-                                                  const double2 *__restrict__ t, const int *__restrict__ perm, int mode,
-                                                  double2 *__restrict__ y) {
+// y over one leaf: the partial products of the blocks covering it, summed in
+// the leaf's item order, scattered to the original order.  cols: the column
+// side (adjoint / transpose).
+__global__ void __launch_bounds__(64) k_aca_leaf_sum(const AcaBlockDesc *__restrict__ blocks,
+                                                     const int2 *__restrict__ leaf, const int64_t *__restrict__ off,
+                                                     const int *__restrict__ items, const int64_t *__restrict__ zoff,
+                                                     const double2 *__restrict__ z, const int *__restrict__ perm,
+                                                     int cols, double2 *__restrict__ y) {
   const int2 L = leaf[blockIdx.x];
-  const bool adj = mode == 1;
-  for (int j = L.x + threadIdx.x; j < L.x + L.y; j += blockDim.x) {
+  const int64_t q0 = off[blockIdx.x], q1 = off[blockIdx.x + 1];
+  for (int i = L.x + threadIdx.x; i < L.x + L.y; i += blockDim.x) {
     double2 acc = make_double2(0, 0);
-    for (int64_t q = off[blockIdx.x]; q < off[blockIdx.x + 1]; q++) {
+    for (int64_t q = q0; q < q1; q++) {
       const int b = items[q];
-      const AcaBlockDesc bd = blocks[b];
-      const int jj = j - bd.c0;
-      if (bd.kind == 0) {
-        const double2 *D = arena + bd.off_a + (int64_t)jj * bd.m;
-        const double2 *xs = xp + bd.r0;
-        for (int ii = 0; ii < bd.m; ii++) {
-          const double2 d = adj ? cconj(D[ii]) : D[ii];
-          acc = cadd(acc, cmul(d, xs[ii]));
-        }
-      } else {
-        const double2 *Vj = arena + bd.off_b + jj;
-        const double2 *tb = t + toff[b];
-        const int r = rank[b];
-        for (int p = 0; p < r; p++) {
-          const double2 v = adj ? Vj[(int64_t)p * bd.n] : cconj(Vj[(int64_t)p * bd.n]);
-          acc = cadd(acc, cmul(v, tb[p]));
-        }
-      }
+      const int base = cols ? blocks[b].c0 : blocks[b].r0;
+      acc = cadd(acc, z[zoff[b] + (i - base)]);
     }
-    y[perm[j]] = acc;
+    y[perm[i]] = acc;
   }
 }
 
@@ -1071,6 +1096,7 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   Plan P;
   make_plan(ctr.data(), N, leaf_size, eta, max_tasks, P);
+  const double t_plan = now_ms();
   // _validate_aca_task_storage (src/fast/ACA.jl:740-772)
   double planned = 0;
   for (const Task &t : P.tasks) {
@@ -1121,6 +1147,7 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   upload(c, A.d_perm, perm32);
   upload(c, A.d_blocks, A.blocks);
   fill_dense(c, dense_ids);
+  const double t_dense = now_ms();
   // ACA on every admissible block, largest first (the CTAs of the big blocks
   // start in the first wave)
   std::vector<int> rank(A.blocks.size(), 0), status(A.blocks.size(), 0), conv(A.blocks.size(), 1);
@@ -1164,6 +1191,7 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
     DMB_CUDA(cudaMemcpyAsync(conv.data(), d_conv.p, sizeof(int) * conv.size(), cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
   }
+  const double t_lowrank = now_ms();
   // non-finite updates: the block is stored dense (src/fast/ACA.jl:883-946),
   // within the storage budget
   std::vector<int> fb;
@@ -1241,6 +1269,18 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   upload(c, A.d_col_items, citems);
   upload(c, A.d_lr_list, lr_now);
   upload(c, A.d_tbuf_off, toff);
+  // partial-product offsets: row side and column side of every block
+  std::vector<int64_t> zr(A.blocks.size()), zc(A.blocks.size());
+  int64_t sr = 0, sc = 0;
+  for (size_t b = 0; b < A.blocks.size(); b++) {
+    zr[b] = sr;
+    zc[b] = sc;
+    sr += A.blocks[b].m;
+    sc += A.blocks[b].n;
+  }
+  upload(c, A.d_zoff_r, zr);
+  upload(c, A.d_zoff_c, zc);
+  A.d_z.ensure(sizeof(double2) * std::max<int64_t>(1, std::max(sr, sc)));
   std::vector<int32_t> rk(rank.begin(), rank.end());
   upload(c, A.d_rank, rk);
   A.d_t.ensure(sizeof(double2) * std::max<int64_t>(tt, 1));
@@ -1254,6 +1294,9 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   A.info.entries_stored = stored;
   A.info.n_unconverged = uncv;
   A.info.build_ms = now_ms() - t0;
+  A.info.plan_ms = t_plan - t0;
+  A.info.dense_ms = t_dense - t_plan;
+  A.info.lowrank_ms = t_lowrank - t_dense;
   A.valid = true;
   c->op_kind = 1;
   c->aca_transposed = false;
@@ -1266,22 +1309,30 @@ void aca_apply(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs, int mode)
   DMB_REQUIRE(A.valid, DMB_ERR_STATE, "no H-matrix operator built");
   DMB_REQUIRE(mode >= 0 && mode <= 2, DMB_ERR_ARGUMENT, "ACA product mode must be 0, 1 or 2");
   const int64_t N = A.n;
+  // algorithmic bytes of one product: every stored block entry once, x and y
+  const double bytes = 16.0 * ((double)A.info.entries_stored + 2.0 * (double)N);
   for (int64_t r = 0; r < nrhs; r++) {
     const double2 *xr = x + r * N;
     double2 *yr = y + r * N;
+    kt_begin(c);
     DMB_LAUNCH(c, k_aca_gather, blocks_for(N, 256), 256, 0, N, A.d_perm.as<int>(), xr, A.d_xp.as<double2>());
     if (A.n_lr > 0)
       DMB_LAUNCH(c, k_aca_inner, (unsigned)A.n_lr, 256, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_lr_list.as<int>(),
                  A.d_rank.as<int>(), A.d_tbuf_off.as<int64_t>(), A.d_arena.as<double2>(), A.d_xp.as<double2>(), mode,
                  A.d_t.as<double2>());
+    DMB_LAUNCH(c, k_aca_partials, (unsigned)A.blocks.size(), 256, 0, A.d_blocks.as<AcaBlockDesc>(),
+               A.d_rank.as<int>(), A.d_tbuf_off.as<int64_t>(),
+               (mode == 0 ? A.d_zoff_r : A.d_zoff_c).as<int64_t>(), A.d_arena.as<double2>(), A.d_xp.as<double2>(),
+               A.d_t.as<double2>(), mode, A.d_z.as<double2>());
     if (mode == 0)
-      DMB_LAUNCH(c, k_aca_rows, (unsigned)A.n_leaves, 128, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
-                 A.d_row_off.as<int64_t>(), A.d_row_items.as<int>(), A.d_rank.as<int>(), A.d_tbuf_off.as<int64_t>(),
-                 A.d_arena.as<double2>(), A.d_xp.as<double2>(), A.d_t.as<double2>(), A.d_perm.as<int>(), yr);
+      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
+                 A.d_row_off.as<int64_t>(), A.d_row_items.as<int>(), A.d_zoff_r.as<int64_t>(), A.d_z.as<double2>(),
+                 A.d_perm.as<int>(), 0, yr);
     else
-      DMB_LAUNCH(c, k_aca_cols, (unsigned)A.n_leaves, 128, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
-                 A.d_col_off.as<int64_t>(), A.d_col_items.as<int>(), A.d_rank.as<int>(), A.d_tbuf_off.as<int64_t>(),
-                 A.d_arena.as<double2>(), A.d_xp.as<double2>(), A.d_t.as<double2>(), A.d_perm.as<int>(), mode, yr);
+      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
+                 A.d_col_off.as<int64_t>(), A.d_col_items.as<int>(), A.d_zoff_c.as<int64_t>(), A.d_z.as<double2>(),
+                 A.d_perm.as<int>(), 1, yr);
+    kt_end(c, bytes, 3);
   }
 }
 

@@ -130,12 +130,13 @@ struct AcaState {
   DevBuf d_row_off, d_row_items;          // per row leaf: dense blocks then covering low-rank blocks
   DevBuf d_col_off, d_col_items;          // per column leaf: the same for the adjoint / transpose
   DevBuf d_leaf;                          // leaf node ranges (first, count)
+  DevBuf d_zoff_r, d_zoff_c, d_z;         // per-block partial products (row / column side)
   int64_t n_leaves = 0, n_lr = 0, t_total = 0;
   double k = 0, eta0 = 0;
   int quad_order = 3;
   void release() {
     DevBuf *b[] = {&d_perm, &d_blocks, &d_arena, &d_rank, &d_tbuf_off, &d_t, &d_xp, &d_lr_list,
-                   &d_row_off, &d_row_items, &d_col_off, &d_col_items, &d_leaf};
+                   &d_row_off, &d_row_items, &d_col_off, &d_col_items, &d_leaf, &d_zoff_r, &d_zoff_c, &d_z};
     for (DevBuf *x : b) x->release();
     valid = false;
   }
@@ -257,10 +258,11 @@ struct dmb_ctx {
   dmb_timings tm{};
   int64_t launches = 0;
   bool kt_enabled = false;     // dominant-kernel event timing
-  // per family: 0 3xTF32 Krylov / sweep GEMMs, 1 int8 GEMMs, 2 factor updates
-  static constexpr int KT_FAMILIES = 3;
-  double kt_ms[KT_FAMILIES] = {0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0};
-  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0};
+  // per family: 0 3xTF32 Krylov / sweep GEMMs, 1 int8 GEMMs, 2 factor updates,
+  // 3 H-matrix products (one right-hand side, work in bytes)
+  static constexpr int KT_FAMILIES = 4;
+  double kt_ms[KT_FAMILIES] = {0, 0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0, 0};
+  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0, 0};
   std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
   std::vector<double> kt_pending;     // algorithmic work of each recorded launch
   std::vector<int> kt_family;         // family of each recorded launch

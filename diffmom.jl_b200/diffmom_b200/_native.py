@@ -113,7 +113,8 @@ class BatchItem(ctypes.Structure):
 class AcaInfo(ctypes.Structure):
     _fields_ = [("n_dense", ctypes.c_int64), ("n_lowrank", ctypes.c_int64), ("n_fallback", ctypes.c_int64),
                 ("max_rank_used", ctypes.c_int64), ("entries_stored", ctypes.c_int64),
-                ("n_unconverged", ctypes.c_int64), ("build_ms", ctypes.c_double)]
+                ("n_unconverged", ctypes.c_int64), ("build_ms", ctypes.c_double), ("plan_ms", ctypes.c_double),
+                ("dense_ms", ctypes.c_double), ("lowrank_ms", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p

@@ -354,8 +354,10 @@ dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double
 /* Same per kernel family: 0 = tensor-core 3xTF32 Krylov and triangular-sweep
  * GEMMs (work in complex flops, 8 per complex MAC), 1 = INT8-slice
  * FP64-accurate GEMMs (work in int8 multiply-adds x 2), 2 = factorisation
- * trailing updates (3xTF32 tensor cores for complex64 factors; complex flops).
- * dmb_kernel_timing reports family 0. */
+ * trailing updates (3xTF32 tensor cores for complex64 factors; complex flops),
+ * 3 = H-matrix products of dmb_aca_build's operator (one bracket per
+ * right-hand side: gather, low-rank inner products, leaf sums; work in bytes:
+ * the stored blocks plus x and y once).  dmb_kernel_timing reports family 0. */
 dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
 
 /* ---- H-matrix operator (adaptive cross approximation) ------------------ */
@@ -386,6 +388,9 @@ typedef struct {
   int64_t entries_stored;   /* complex entries held (dense data + U + V at their ranks) */
   int64_t n_unconverged;    /* low-rank blocks that reached max_rank without meeting tol */
   double build_ms;          /* host + device time of the build */
+  double plan_ms;           /* of which: cache, tree and block tasks on the host */
+  double dense_ms;          /*           dense block fill */
+  double lowrank_ms;        /*           ACA of the admissible blocks */
 } dmb_aca_info;
 /* build_aca_operator(mesh, rwg, k; leaf_size, eta, aca_tol, max_rank,
  * quad_order, eta0, max_block_tasks, max_storage_bytes)
