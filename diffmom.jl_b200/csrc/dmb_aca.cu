@@ -24,6 +24,7 @@
 #include <cstring>
 #include <functional>
 #include <numeric>
+#include <type_traits>
 
 #include "dmb_device.cuh"
 #include "dmb_internal.h"
@@ -409,38 +410,31 @@ template <int NQ>
 __device__ double2 far_slot_value(const TriCache &A, const TriCache &B, int i, int j, double k, double inv_k2) {
   double m0r = 0, m0i = 0, mar[3] = {0, 0, 0}, mai[3] = {0, 0, 0}, mbr[3] = {0, 0, 0}, mbi[3] = {0, 0, 0},
          mabr = 0, mabi = 0;
-  double qa[NQ][3], la[NQ][3], wa[NQ];
-#pragma unroll
-  for (int a = 0; a < NQ; a++) {
-    wa[a] = A.w2a[a];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      qa[a][d] = A.qp[a][d];
-      la[a][d] = A.ql[a][d];
-    }
-  }
-#pragma unroll
+  // same operations in the same order; the points of A are read where they
+  // are used (cached) instead of held in registers
+#pragma unroll 1
   for (int b = 0; b < NQ; b++) {
-    double qb0 = B.qp[b][0], qb1 = B.qp[b][1], qb2 = B.qp[b][2];
-    double lb0 = B.ql[b][0], lb1 = B.ql[b][1], lb2 = B.ql[b][2];
-    double wb = B.w2a[b];
-#pragma unroll
+    const double qb0 = B.qp[b][0], qb1 = B.qp[b][1], qb2 = B.qp[b][2];
+    const double lb0 = B.ql[b][0], lb1 = B.ql[b][1], lb2 = B.ql[b][2];
+    const double wb = B.w2a[b];
+#pragma unroll 1
     for (int a = 0; a < NQ; a++) {
-      double dx = qa[a][0] - qb0, dy = qa[a][1] - qb1, dz = qa[a][2] - qb2;
+      const double la0 = A.ql[a][0], la1 = A.ql[a][1], la2 = A.ql[a][2];
+      double dx = A.qp[a][0] - qb0, dy = A.qp[a][1] - qb1, dz = A.qp[a][2] - qb2;
       double R = sqrt(dx * dx + dy * dy + dz * dz);
       double sn, cs;
       sincos(k * R, &sn, &cs);
-      double g = (DMB_INV_FOUR_PI / R) * (wa[a] * wb);
+      double g = (DMB_INV_FOUR_PI / R) * (A.w2a[a] * wb);
       double gr = cs * g, gi = -sn * g;
       m0r += gr;
       m0i += gi;
-      mar[0] = fma(gr, la[a][0], mar[0]); mai[0] = fma(gi, la[a][0], mai[0]);
-      mar[1] = fma(gr, la[a][1], mar[1]); mai[1] = fma(gi, la[a][1], mai[1]);
-      mar[2] = fma(gr, la[a][2], mar[2]); mai[2] = fma(gi, la[a][2], mai[2]);
+      mar[0] = fma(gr, la0, mar[0]); mai[0] = fma(gi, la0, mai[0]);
+      mar[1] = fma(gr, la1, mar[1]); mai[1] = fma(gi, la1, mai[1]);
+      mar[2] = fma(gr, la2, mar[2]); mai[2] = fma(gi, la2, mai[2]);
       mbr[0] = fma(gr, lb0, mbr[0]); mbi[0] = fma(gi, lb0, mbi[0]);
       mbr[1] = fma(gr, lb1, mbr[1]); mbi[1] = fma(gi, lb1, mbi[1]);
       mbr[2] = fma(gr, lb2, mbr[2]); mbi[2] = fma(gi, lb2, mbi[2]);
-      double dd = la[a][0] * lb0 + la[a][1] * lb1 + la[a][2] * lb2;
+      double dd = la0 * lb0 + la1 * lb1 + la2 * lb2;
       mabr = fma(gr, dd, mabr);
       mabi = fma(gi, dd, mabi);
     }
@@ -469,9 +463,11 @@ __device__ double2 aca_entry(const AcaGeo &g, int m, int n) {
   const int sn[2] = {g.rslot[2 * n], g.rslot[2 * n + 1]};
   double re = 0, im = 0;
   bool near = false;
-#pragma unroll
+  // the four slot pairs one after another (unrolled, their quadrature loops
+  // would hold four sets of moments in registers)
+#pragma unroll 1
   for (int a = 0; a < 2; a++)
-#pragma unroll
+#pragma unroll 1
     for (int b = 0; b < 2; b++) {
       const int x = sm[a], y = sn[b];
       const int lo = x <= y ? x : y, hi = x <= y ? y : x;
@@ -583,16 +579,44 @@ __device__ void block_argmax(double &v, int &idx, double *sv, int *si) {
     }
 }
 
-// sum over the CTA in a fixed order (lane tree, then warps in order)
-__device__ double block_sum(double v, double *sh) {
-  v = warp_sum(v);
+// three maxima (sh: 96 doubles) and two sums (sh: 64 doubles) with one barrier pair
+__device__ void block_max3(double &a, double &b, double &c, double *sh) {
+  a = warp_max(a);
+  b = warp_max(b);
+  c = warp_max(c);
   const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) sh[w] = v;
+  if ((threadIdx.x & 31) == 0) {
+    sh[w] = a;
+    sh[32 + w] = b;
+    sh[64 + w] = c;
+  }
   __syncthreads();
-  double s = 0;
-  for (int q = 0; q < nw; q++) s += sh[q];
-  return s;
+  a = sh[0];
+  b = sh[32];
+  c = sh[64];
+  for (int q = 1; q < nw; q++) {
+    a = fmax(a, sh[q]);
+    b = fmax(b, sh[32 + q]);
+    c = fmax(c, sh[64 + q]);
+  }
+}
+__device__ void block_sum2(double &a, double &b, double *sh) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    sh[w] = a;
+    sh[32 + w] = b;
+  }
+  __syncthreads();
+  a = 0;
+  b = 0;
+  for (int q = 0; q < nw; q++) {
+    a += sh[q];
+    b += sh[32 + q];
+  }
 }
 __device__ double block_max(double v, double *sh) {
   v = warp_max(v);
@@ -611,17 +635,19 @@ constexpr int ACA_SCR = 10;  // su, nu, sv, nv, term f, term e, <U_p,u> re/im, <
 // One CTA per admissible block: aca_lowrank (src/fast/ACA.jl:351-554).
 // status: 0 ok, 1 non-finite update (the block becomes dense), 2 zero-norm
 // update; conv: 1 converged, 0 stopped otherwise.
-template <int NQ>
-__global__ void __launch_bounds__(256) k_aca_lowrank(AcaGeo g, const AcaBlockDesc *__restrict__ blocks,
-                                                     const int *__restrict__ ids, const int *__restrict__ perm,
-                                                     double2 *__restrict__ arena, const int64_t *__restrict__ foff,
-                                                     unsigned char *__restrict__ flags,
-                                                     const int64_t *__restrict__ soff, double *__restrict__ scr,
-                                                     double tol, int *__restrict__ rank_out,
-                                                     int *__restrict__ status_out, int *__restrict__ conv_out) {
-  __shared__ double sv[8];
-  __shared__ int si[8];
-  __shared__ double sh[8];
+// NT threads per CTA: the launcher buckets the blocks by size (small blocks
+// on narrow CTAs, the few large ones on wide CTAs).
+template <int NQ, int NT>
+__global__ void __launch_bounds__(NT) k_aca_lowrank(AcaGeo g, const AcaBlockDesc *__restrict__ blocks,
+                                                    const int *__restrict__ ids, const int *__restrict__ perm,
+                                                    double2 *__restrict__ arena, const int64_t *__restrict__ foff,
+                                                    unsigned char *__restrict__ flags,
+                                                    const int64_t *__restrict__ soff, double *__restrict__ scr,
+                                                    double tol, int *__restrict__ rank_out,
+                                                    int *__restrict__ status_out, int *__restrict__ conv_out) {
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ double sh[96];
   __shared__ int s_pc, s_stop, s_conv;
   __shared__ double2 s_pivot;
   const int bi = ids[blockIdx.x];
@@ -713,13 +739,12 @@ __global__ void __launch_bounds__(256) k_aca_lowrank(AcaGeo g, const AcaBlockDes
       bad |= !isfinite(v.x) || !isfinite(v.y);
       cv = fmax(cv, fmax(fabs(v.x), fabs(v.y)));
     }
-    const double anybad = block_max(bad ? 1.0 : 0.0, sh);
+    double anybad = bad ? 1.0 : 0.0;
+    block_max3(anybad, cu, cv, sh);
     if (anybad != 0.0) {
       status = 1;
       break;
     }
-    cu = block_max(cu, sh);
-    cv = block_max(cv, sh);
     if (!(cu > 0.0) || !(cv > 0.0)) {
       status = 2;
       break;
@@ -735,8 +760,7 @@ __global__ void __launch_bounds__(256) k_aca_lowrank(AcaGeo g, const AcaBlockDes
       sv2 = fma(xr, xr, sv2);
       sv2 = fma(xi, xi, sv2);
     }
-    su = block_sum(su, sh);
-    sv2 = block_sum(sv2, sh);
+    block_sum2(su, sv2, sh);
     // normalised inner products with the earlier factors: warp w takes the
     // ranks p = w, w + 8, ...
     for (int p = warp; p < k; p += nw) {
@@ -1066,6 +1090,27 @@ void build_leaf_lists(const std::vector<AcaBlockDesc> &B, const std::vector<int2
   for (auto &v : lists) items.insert(items.end(), v.begin(), v.end());
 }
 
+// ACA launch of one size bucket (count blocks from ids / foff / soff)
+template <int NT>
+void launch_lowrank(dmb_ctx *c, unsigned count, const AcaGeo &g, const AcaBlockDesc *blocks, const int *ids,
+                    const int *perm, double2 *arena, const int64_t *foff, unsigned char *flags, const int64_t *soff,
+                    double *scr, double tol, int *rank, int *status, int *conv) {
+  if (count == 0) return;
+  ACA_NQ_DISPATCH(c->nq, DMB_LAUNCH(c, (k_aca_lowrank<NQ, NT>), count, NT, 0, g, blocks, ids, perm, arena, foff,
+                                    flags, soff, scr, tol, rank, status, conv));
+}
+
+void ensure_side_streams(dmb_ctx *c) {
+  if (!c->stream2 || !c->stream3) {
+    int least = 0, greatest = 0;
+    DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
+    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, least));
+  }
+  for (auto &e : c->la_ev)
+    if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
 }  // namespace
 
 namespace dmb {
@@ -1152,11 +1197,18 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   // start in the first wave)
   std::vector<int> rank(A.blocks.size(), 0), status(A.blocks.size(), 0), conv(A.blocks.size(), 1);
   if (!lr_ids.empty()) {
+    // largest first; buckets by m + n: 512-thread CTAs for the few large
+    // blocks (the critical path), 256 for the middle, 64 for the many
+    // leaf-level blocks, launched concurrently on the context's three streams
     std::vector<int> order = lr_ids;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
       const AcaBlockDesc &x = A.blocks[a], &y = A.blocks[b];
-      return (int64_t)x.rmax * (x.m + x.n) > (int64_t)y.rmax * (y.m + y.n);
+      return x.m + x.n != y.m + y.n ? x.m + x.n > y.m + y.n : x.rmax > y.rmax;
     });
+    size_t e512 = 0, e256 = 0;
+    while (e512 < order.size() && A.blocks[order[e512]].m + A.blocks[order[e512]].n > 1024) e512++;
+    e256 = e512;
+    while (e256 < order.size() && A.blocks[order[e256]].m + A.blocks[order[e256]].n > 192) e256++;
     std::vector<int64_t> foff(order.size()), soff(order.size());
     int64_t fo = 0, so = 0;
     for (size_t q = 0; q < order.size(); q++) {
@@ -1180,11 +1232,30 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
     DMB_CUDA(cudaMemsetAsync(d_status.p, 0, sizeof(int) * A.blocks.size(), c->stream));
     DMB_CUDA(cudaMemsetAsync(d_conv.p, 0, sizeof(int) * A.blocks.size(), c->stream));
     AcaGeo g = make_geo(c);
-    ACA_NQ_DISPATCH(c->nq, DMB_LAUNCH(c, k_aca_lowrank<NQ>, (unsigned)order.size(), 256, 0, g,
-                                      A.d_blocks.as<AcaBlockDesc>(), d_ids.as<int>(), A.d_perm.as<int>(),
-                                      A.d_arena.as<double2>(), d_foff.as<int64_t>(), d_flags.as<unsigned char>(),
-                                      d_soff.as<int64_t>(), d_scr.as<double>(), tol, d_rank.as<int>(),
-                                      d_status.as<int>(), d_conv.as<int>()));
+    ensure_side_streams(c);
+    DMB_CUDA(cudaEventRecord(c->la_ev[0], c->stream));
+    DMB_CUDA(cudaStreamWaitEvent(c->stream2, c->la_ev[0], 0));
+    DMB_CUDA(cudaStreamWaitEvent(c->stream3, c->la_ev[0], 0));
+    auto bucket = [&](auto nt_tag, size_t lo, size_t hi) {
+      constexpr int NT = decltype(nt_tag)::value;
+      launch_lowrank<NT>(c, (unsigned)(hi - lo), g, A.d_blocks.as<AcaBlockDesc>(), d_ids.as<int>() + lo,
+                         A.d_perm.as<int>(), A.d_arena.as<double2>(), d_foff.as<int64_t>() + lo,
+                         d_flags.as<unsigned char>(), d_soff.as<int64_t>() + lo, d_scr.as<double>(), tol,
+                         d_rank.as<int>(), d_status.as<int>(), d_conv.as<int>());
+    };
+    bucket(std::integral_constant<int, 512>(), 0, e512);
+    {
+      StreamSwap sw(c, c->stream2);
+      bucket(std::integral_constant<int, 256>(), e512, e256);
+      DMB_CUDA(cudaEventRecord(c->la_ev[1], c->stream2));
+    }
+    {
+      StreamSwap sw(c, c->stream3);
+      bucket(std::integral_constant<int, 64>(), e256, order.size());
+      DMB_CUDA(cudaEventRecord(c->la_ev[2], c->stream3));
+    }
+    DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[1], 0));
+    DMB_CUDA(cudaStreamWaitEvent(c->stream, c->la_ev[2], 0));
     DMB_CUDA(cudaMemcpyAsync(rank.data(), d_rank.p, sizeof(int) * rank.size(), cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaMemcpyAsync(status.data(), d_status.p, sizeof(int) * status.size(), cudaMemcpyDeviceToHost,
                              c->stream));
@@ -1475,10 +1546,9 @@ int aca_lowrank_one(dmb_ctx *c, double k, double eta0, int quad_order, const std
   g.inv_k2 = 1.0 / (k * k);
   g.omega_mu0 = k * eta0;
   int *o = d_out.as<int>();
-  ACA_NQ_DISPATCH(c->nq, DMB_LAUNCH(c, k_aca_lowrank<NQ>, 1, 256, 0, g, d_blk.as<AcaBlockDesc>(), d_ids.as<int>(),
-                                    d_idx.as<int>(), d_arena.as<double2>(), d_foff.as<int64_t>(),
-                                    d_flags.as<unsigned char>(), d_soff.as<int64_t>(), d_scr.as<double>(), tol, o,
-                                    o + 1, o + 2));
+  launch_lowrank<256>(c, 1, g, d_blk.as<AcaBlockDesc>(), d_ids.as<int>(), d_idx.as<int>(), d_arena.as<double2>(),
+                      d_foff.as<int64_t>(), d_flags.as<unsigned char>(), d_soff.as<int64_t>(), d_scr.as<double>(),
+                      tol, o, o + 1, o + 2);
   int h[3];
   DMB_CUDA(cudaMemcpyAsync(h, d_out.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
