@@ -882,6 +882,7 @@ __global__ void __launch_bounds__(256) k_aca_inner(const AcaBlockDesc *__restric
   for (int p = threadIdx.x >> 5; p < r; p += nw) {
     const double2 *Fp = F + (int64_t)p * len;
     double2 acc = make_double2(0, 0);
+#pragma unroll 4
     for (int i = lane; i < len; i += 32) {
       const double2 f = mode == 2 ? Fp[i] : cconj(Fp[i]);
       acc = cadd(acc, cmul(f, xs[i]));
@@ -914,8 +915,10 @@ __global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__rest
       for (int i0 = 0; i0 < bd.m; i0 += 64) {
         const int i = i0 + ri;
         double2 acc = make_double2(0, 0);
-        if (i < bd.m)
+        if (i < bd.m) {
+#pragma unroll 4
           for (int jj = g; jj < bd.n; jj += 4) acc = cadd(acc, cmul(D[i + (int64_t)jj * bd.m], xs[jj]));
+        }
         part[tid] = acc;
         __syncthreads();
         if (tid < 64 && i < bd.m)
@@ -927,6 +930,7 @@ __global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__rest
       const int r = rank[b];
       for (int i = tid; i < bd.m; i += blockDim.x) {
         double2 acc = make_double2(0, 0);
+#pragma unroll 4
         for (int p = 0; p < r; p++) acc = cadd(acc, cmul(U[i + (int64_t)p * bd.m], tb[p]));
         zb[i] = acc;
       }
@@ -941,6 +945,7 @@ __global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__rest
     for (int jj = tid >> 5; jj < bd.n; jj += nw) {
       const double2 *Dj = D + (int64_t)jj * bd.m;
       double2 acc = make_double2(0, 0);
+#pragma unroll 2
       for (int ii = lane; ii < bd.m; ii += 32) acc = cadd(acc, cmul(adj ? cconj(Dj[ii]) : Dj[ii], xs[ii]));
       acc = warp_sum2(acc);
       if (lane == 0) zb[jj] = acc;
@@ -950,6 +955,7 @@ __global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__rest
     const int r = rank[b];
     for (int j = tid; j < bd.n; j += blockDim.x) {
       double2 acc = make_double2(0, 0);
+#pragma unroll 4
       for (int p = 0; p < r; p++) {
         const double2 v = V[j + (int64_t)p * bd.n];
         acc = cadd(acc, cmul(adj ? v : cconj(v), tb[p]));
@@ -960,22 +966,23 @@ __global__ void __launch_bounds__(256) k_aca_partials(const AcaBlockDesc *__rest
 }
 
 // y over one leaf: the partial products of the blocks covering it, summed in
-// the leaf's item order, scattered to the original order.  cols: the column
-// side (adjoint / transpose).
-__global__ void __launch_bounds__(64) k_aca_leaf_sum(const AcaBlockDesc *__restrict__ blocks,
-                                                     const int2 *__restrict__ leaf, const int64_t *__restrict__ off,
-                                                     const int *__restrict__ items, const int64_t *__restrict__ zoff,
+// the leaf's item order, scattered to the original order.  zbase[q] = the
+// item's partial-product offset minus the block's first row (or column), so
+// row i of the leaf reads z[zbase[q] + i].
+__global__ void __launch_bounds__(64) k_aca_leaf_sum(const int2 *__restrict__ leaf, const int64_t *__restrict__ off,
+                                                     const int64_t *__restrict__ zbase,
                                                      const double2 *__restrict__ z, const int *__restrict__ perm,
-                                                     int cols, double2 *__restrict__ y) {
+                                                     double2 *__restrict__ y) {
   const int2 L = leaf[blockIdx.x];
   const int64_t q0 = off[blockIdx.x], q1 = off[blockIdx.x + 1];
   for (int i = L.x + threadIdx.x; i < L.x + L.y; i += blockDim.x) {
     double2 acc = make_double2(0, 0);
-    for (int64_t q = q0; q < q1; q++) {
-      const int b = items[q];
-      const int base = cols ? blocks[b].c0 : blocks[b].r0;
-      acc = cadd(acc, z[zoff[b] + (i - base)]);
+    int64_t q = q0;
+    for (; q + 4 <= q1; q += 4) {  // four independent loads in flight
+      const double2 a = z[zbase[q] + i], b = z[zbase[q + 1] + i], c = z[zbase[q + 2] + i], d = z[zbase[q + 3] + i];
+      acc = cadd(cadd(cadd(cadd(acc, a), b), c), d);
     }
+    for (; q < q1; q++) acc = cadd(acc, z[zbase[q] + i]);
     y[perm[i]] = acc;
   }
 }
@@ -1335,9 +1342,7 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   build_leaf_lists(A.blocks, leaves, false, coff, citems);
   upload(c, A.d_leaf, leaves);
   upload(c, A.d_row_off, roff);
-  upload(c, A.d_row_items, ritems);
   upload(c, A.d_col_off, coff);
-  upload(c, A.d_col_items, citems);
   upload(c, A.d_lr_list, lr_now);
   upload(c, A.d_tbuf_off, toff);
   // partial-product offsets: row side and column side of every block
@@ -1351,6 +1356,11 @@ void aca_build(dmb_ctx *c, double k, double eta0, int quad_order, int leaf_size,
   }
   upload(c, A.d_zoff_r, zr);
   upload(c, A.d_zoff_c, zc);
+  std::vector<int64_t> rzb(ritems.size()), czb(citems.size());
+  for (size_t q = 0; q < ritems.size(); q++) rzb[q] = zr[ritems[q]] - A.blocks[ritems[q]].r0;
+  for (size_t q = 0; q < citems.size(); q++) czb[q] = zc[citems[q]] - A.blocks[citems[q]].c0;
+  upload(c, A.d_row_zbase, rzb);
+  upload(c, A.d_col_zbase, czb);
   A.d_z.ensure(sizeof(double2) * std::max<int64_t>(1, std::max(sr, sc)));
   std::vector<int32_t> rk(rank.begin(), rank.end());
   upload(c, A.d_rank, rk);
@@ -1396,13 +1406,11 @@ void aca_apply(dmb_ctx *c, const double2 *x, double2 *y, int64_t nrhs, int mode)
                (mode == 0 ? A.d_zoff_r : A.d_zoff_c).as<int64_t>(), A.d_arena.as<double2>(), A.d_xp.as<double2>(),
                A.d_t.as<double2>(), mode, A.d_z.as<double2>());
     if (mode == 0)
-      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
-                 A.d_row_off.as<int64_t>(), A.d_row_items.as<int>(), A.d_zoff_r.as<int64_t>(), A.d_z.as<double2>(),
-                 A.d_perm.as<int>(), 0, yr);
+      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_leaf.as<int2>(), A.d_row_off.as<int64_t>(),
+                 A.d_row_zbase.as<int64_t>(), A.d_z.as<double2>(), A.d_perm.as<int>(), yr);
     else
-      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_blocks.as<AcaBlockDesc>(), A.d_leaf.as<int2>(),
-                 A.d_col_off.as<int64_t>(), A.d_col_items.as<int>(), A.d_zoff_c.as<int64_t>(), A.d_z.as<double2>(),
-                 A.d_perm.as<int>(), 1, yr);
+      DMB_LAUNCH(c, k_aca_leaf_sum, (unsigned)A.n_leaves, 64, 0, A.d_leaf.as<int2>(), A.d_col_off.as<int64_t>(),
+                 A.d_col_zbase.as<int64_t>(), A.d_z.as<double2>(), A.d_perm.as<int>(), yr);
     kt_end(c, bytes, 3);
   }
 }

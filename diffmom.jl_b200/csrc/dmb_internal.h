@@ -127,16 +127,17 @@ struct AcaState {
   // device: permutation, blocks, arena, per-block ranks / status, product lists
   DevBuf d_perm, d_blocks, d_arena, d_rank, d_tbuf_off, d_t, d_xp;
   DevBuf d_lr_list;                       // low-rank block ids (inner-product kernel)
-  DevBuf d_row_off, d_row_items;          // per row leaf: dense blocks then covering low-rank blocks
-  DevBuf d_col_off, d_col_items;          // per column leaf: the same for the adjoint / transpose
+  DevBuf d_row_off, d_col_off;            // per row / column leaf: its items (covering blocks, dense first)
   DevBuf d_leaf;                          // leaf node ranges (first, count)
   DevBuf d_zoff_r, d_zoff_c, d_z;         // per-block partial products (row / column side)
+  DevBuf d_row_zbase, d_col_zbase;        // per leaf item: partial offset minus the block's first row / column
   int64_t n_leaves = 0, n_lr = 0, t_total = 0;
   double k = 0, eta0 = 0;
   int quad_order = 3;
   void release() {
     DevBuf *b[] = {&d_perm, &d_blocks, &d_arena, &d_rank, &d_tbuf_off, &d_t, &d_xp, &d_lr_list,
-                   &d_row_off, &d_row_items, &d_col_off, &d_col_items, &d_leaf, &d_zoff_r, &d_zoff_c, &d_z};
+                   &d_row_off, &d_col_off, &d_leaf, &d_zoff_r, &d_zoff_c, &d_z,
+                   &d_row_zbase, &d_col_zbase};
     for (DevBuf *x : b) x->release();
     valid = false;
   }
