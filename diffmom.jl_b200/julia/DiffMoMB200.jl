@@ -68,4 +68,21 @@ function solve_gmres_gpu(d::Device, rhs::Vector{ComplexF64}; tol=1e-8, maxiter=2
         check_gmres_convergence ? 1 : 0, st))
     return x, st[]
 end
+# build_aca_operator(mesh, rwg, k; ...) on the GPU; the device's operator is
+# then the H-matrix (solve_gmres_gpu runs on it until the next assembly)
+function build_aca_operator_gpu(d::Device, k; leaf_size=64, eta=1.5, aca_tol=1e-6, max_rank=50,
+                                quad_order=3, eta0=376.730313668, max_block_tasks=2_000_000,
+                                max_storage_bytes=2_000_000_000)
+    info = zeros(UInt8, 80)   # dmb_aca_info: 6 x Int64 + 4 x Float64
+    check(d.ptr, ccall((:dmb_aca_build, lib), Cint,
+        (Ptr{Cvoid}, Cdouble, Cdouble, Cint, Cint, Cdouble, Cdouble, Cint, Int64, Int64, Ptr{UInt8}),
+        d.ptr, k, eta0, quad_order, leaf_size, eta, aca_tol, max_rank, max_block_tasks,
+        max_storage_bytes, info))
+    return reinterpret(Int64, info[1:48]), reinterpret(Float64, info[49:80])
+end
+
+# build_nearfield_preconditioner(A_aca; factorization) from the H-matrix's dense blocks
+aca_nf_build!(d::Device; factorization=:lu, precision=:fp64) = check(d.ptr,
+    ccall((:dmb_aca_nf_build, lib), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}),
+          d.ptr, factorization === :lu ? 1 : 2, precision === :fp64 ? 0 : 1, C_NULL))
 end # module
