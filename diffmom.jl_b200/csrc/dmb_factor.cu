@@ -586,11 +586,37 @@ __device__ int wait_flags(const volatile unsigned *fl, int cb, int limit, unsign
   return r - cb;
 }
 
+// 64 x 64 matrix (shared memory, row stride NB) times a 64-vector (shared
+// memory) with four threads per output: thread (o = tid >> 2, part = tid & 3)
+// sums 16 terms, two shuffles combine the parts.  TR: the matrix is read
+// transposed (output o takes column o).  Every thread returns the sum of its
+// output.
+template <class FC, bool TR>
+__device__ __forceinline__ double2 gemv64_quad(const FC *__restrict__ M, const double2 *__restrict__ v) {
+  const int o = threadIdx.x >> 2, part = threadIdx.x & 3;
+  double2 a = make_double2(0, 0), b = make_double2(0, 0);
+#pragma unroll
+  for (int k = 0; k < 16; k += 2) {
+    const int c0 = part * 16 + k, c1 = c0 + 1;
+    cfma(a, to_d2(TR ? M[c0 * NB + o] : M[o * NB + c0]), v[c0]);
+    cfma(b, to_d2(TR ? M[c1 * NB + o] : M[o * NB + c1]), v[c1]);
+  }
+  a = cadd(a, b);
+  a.x += __shfl_xor_sync(0xffffffffu, a.x, 1);
+  a.y += __shfl_xor_sync(0xffffffffu, a.y, 1);
+  a.x += __shfl_xor_sync(0xffffffffu, a.x, 2);
+  a.y += __shfl_xor_sync(0xffffffffu, a.y, 2);
+  return a;
+}
+
 // L y = x (x overwritten), L unit lower.  256 threads = 4 row groups x 64
-// columns; each thread accumulates its 16 rows across all solved block rows in
-// registers.  The L block of the last dependency (block row t-1) and the
-// inverse diagonal block are staged in shared memory before any wait, so the
-// critical path after the last flag is an L2 read of y plus on-chip work.
+// columns; while earlier block rows are streamed each thread accumulates its
+// 16 rows across all solved block rows in registers, and those partial sums
+// are reduced before the last wait.  The L block of the last dependency
+// (block row t-1) and the inverse diagonal block are staged in shared memory
+// before any wait, so the critical path after the last flag is one L2 read of
+// y_{t-1} into shared memory and two 64 x 64 products on chip (four threads
+// per row, two shuffles each).
 template <class FC>
 __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restrict__ F, const FC *__restrict__ Linv,
                                                   double2 *x, unsigned *flags, unsigned *tickets, unsigned *err) {
@@ -598,6 +624,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
   FC *Lp = reinterpret_cast<FC *>(smem_raw);
   FC *Li = Lp + NB * NB;
   __shared__ double2 acc[NB];
+  __shared__ double2 ys[NB];
   __shared__ double2 part[2][NB];
   __shared__ int s_t, s_n;
   const int nblk = (int)((N + NB - 1) / NB);
@@ -639,15 +666,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
     }
     cb += n;
   }
-  if (t > 0) {
-    if (threadIdx.x == 0) s_n = wait_flags(fl, t - 1, t, err);
-    __syncthreads();
-    if (s_n == 0) return;
-    __threadfence();
-    const double2 yv = __ldcg(xr + (int64_t)(t - 1) * NB + col);
-#pragma unroll
-    for (int i = 0; i < 16; i++) cfma(p[i], to_d2(Lp[(rg + 4 * i) * NB + col]), yv);
-  }
+  // acc = x_t - (streamed block rows), before the last wait
   if (threadIdx.x < NB) acc[threadIdx.x] = threadIdx.x < bs ? xr[r0 + threadIdx.x] : make_double2(0, 0);
 #pragma unroll
   for (int i = 0; i < 16; i++) {
@@ -656,20 +675,20 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
   }
   __syncthreads();
   if (threadIdx.x < NB) acc[threadIdx.x] = csub(acc[threadIdx.x], cadd(part[0][threadIdx.x], part[1][threadIdx.x]));
-  __syncthreads();
-  // y_t = Linv_tt acc
-#pragma unroll
-  for (int i = 0; i < 16; i++) p[i] = make_double2(0, 0);
-  const double2 av = acc[col];
-#pragma unroll
-  for (int i = 0; i < 16; i++) cfma(p[i], to_d2(Li[(rg + 4 * i) * NB + col]), av);
-#pragma unroll
-  for (int i = 0; i < 16; i++) {
-    double2 v = warp_sum2(p[i]);
-    if ((threadIdx.x & 31) == 0) part[half][rg + 4 * i] = v;
+  if (t > 0) {
+    if (threadIdx.x == 0) s_n = wait_flags(fl, t - 1, t, err);
+    __syncthreads();
+    if (s_n == 0) return;
+    __threadfence();
+    if (threadIdx.x < NB) ys[threadIdx.x] = __ldcg(xr + (int64_t)(t - 1) * NB + threadIdx.x);
+    __syncthreads();
+    const double2 v = gemv64_quad<FC, false>(Lp, ys);
+    if ((threadIdx.x & 3) == 0) acc[threadIdx.x >> 2] = csub(acc[threadIdx.x >> 2], v);
   }
   __syncthreads();
-  if (threadIdx.x < bs) xr[r0 + threadIdx.x] = cadd(part[0][threadIdx.x], part[1][threadIdx.x]);
+  // y_t = Linv_tt acc
+  const double2 y = gemv64_quad<FC, false>(Li, acc);
+  if ((threadIdx.x & 3) == 0 && (threadIdx.x >> 2) < bs) xr[r0 + (threadIdx.x >> 2)] = y;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) atomicExch(fl + t, 1u);
