@@ -215,6 +215,23 @@ class LowRankBlock:
         return self.op._block_data(self.index)[1]
 
 
+def _scaled(Ax: np.ndarray, alpha, beta, y):
+    alpha, beta = complex(alpha), complex(beta)
+    if y is None:
+        out = Ax if alpha == 1 else alpha * Ax
+        return out
+    if y.shape != Ax.shape:
+        raise ValueError(f"output has shape {y.shape}, expected {Ax.shape}")
+    with np.errstate(over="ignore", invalid="ignore"):
+        if beta == 0:
+            y[...] = alpha * Ax
+        else:
+            y[...] = alpha * Ax + beta * y
+    if not np.all(np.isfinite(y)):
+        raise OverflowError("ACA scaled product is outside the representable ComplexF64 range")
+    return y
+
+
 class ACAOperator:
     """H-matrix operator (ACA.jl:173-181) resident on a device context."""
 
@@ -271,8 +288,10 @@ class ACAOperator:
     def __matmul__(self, x):
         return self.matvec(x, 0)
 
-    def mul(self, x):
-        return self.matvec(x, 0)
+    def mul(self, x, alpha=1.0, beta=0.0, y=None):
+        """mul!(y, A, x, alpha, beta) (ACA.jl:1130-1221): alpha A x + beta y;
+        y is overwritten when given, beta = 0 ignores its contents."""
+        return _scaled(self.matvec(x, 0), alpha, beta, y)
 
     def adjoint(self) -> "ACAAdjointOperator":
         return ACAAdjointOperator(self)
@@ -340,8 +359,9 @@ class ACAAdjointOperator:
     def __matmul__(self, x):
         return self.op.matvec(x, 1)
 
-    def mul(self, x):
-        return self.op.matvec(x, 1)
+    def mul(self, x, alpha=1.0, beta=0.0, y=None):
+        """mul!(y, A', x, alpha, beta) (ACA.jl:1231-1323)."""
+        return _scaled(self.op.matvec(x, 1), alpha, beta, y)
 
     def __getitem__(self, ij):
         i, j = ij

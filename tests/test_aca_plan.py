@@ -187,3 +187,38 @@ def test_oracle_aca_and_product_on_a_smooth_kernel():
     for mode, A in ((0, Z), (1, Z.conj().T), (2, Z.T)):
         y_h = ao.hmatrix_matvec(blocks, tree.perm, v, mode)
         assert np.linalg.norm(y_h - A @ v) <= 1e-8 * np.linalg.norm(A @ v)
+
+
+def test_operator_arguments_rejected_before_any_device_work():
+    # build_aca_operator / aca_lowrank validate like ACA.jl:332-340 and
+    # :802-850 before a device context exists
+    from diffmom_b200 import build_aca_operator, aca_lowrank, EFIECache
+    m = make_rect_plate(1.0, 1.0, 2, 2)
+    r = build_rwg(m)
+    for kw in ({"aca_tol": math.inf}, {"aca_tol": 0.0}, {"aca_tol": math.nan}, {"max_rank": 0},
+               {"leaf_size": 0}, {"eta": math.nan}, {"eta": 0.0}, {"max_block_tasks": 0},
+               {"max_storage_bytes": 0}, {"max_green_cache_bytes": 0}, {"max_green_cache_entries": -1},
+               {"max_adjacency_pairs": 0}, {"max_cache_bytes": 1}, {"quad_order": 5},
+               {"quad_order": 3, "max_green_cache_bytes": 16 * 9 - 1}):
+        with pytest.raises(ValueError):
+            build_aca_operator(m, r, 2 * math.pi, **kw)
+    other = build_rwg(make_rect_plate(1.0, 1.0, 2, 2))
+    with pytest.raises(ValueError, match="different mesh"):
+        build_aca_operator(m, other, 2 * math.pi)
+    cache = EFIECache(device=None, k=2 * math.pi)
+    for kw in ({"tol": 0.0}, {"tol": math.inf}, {"tol": math.nan}, {"max_rank": 0}, {"max_rank": -1}):
+        with pytest.raises(ValueError):
+            aca_lowrank(cache, [1], [1], **kw)
+
+
+def test_scaled_product_contract():
+    # mul!(y, A, x, alpha, beta) semantics of the Python operator wrapper
+    from diffmom_b200.aca import _scaled
+    Ax = np.array([1 + 2j, -3.0, 0.5j])
+    np.testing.assert_array_equal(_scaled(Ax, 1.0, 0.0, None), Ax)
+    y = np.array([np.nan, 1.0, 2.0], dtype=complex)  # beta = 0 ignores y
+    np.testing.assert_array_equal(_scaled(Ax, 2.0, 0.0, y), 2.0 * Ax)
+    y = np.array([1.0, 1.0, 1.0], dtype=complex)
+    np.testing.assert_allclose(_scaled(Ax, 0.5 - 1j, 2.0, y), (0.5 - 1j) * Ax + 2.0)
+    with pytest.raises(OverflowError):
+        _scaled(np.array([1e308 + 0j]), 10.0, 0.0, np.zeros(1, complex))

@@ -268,3 +268,23 @@ def test_full_size_plate_product():
     assert comp < 0.5
     dev.close()
     A.close()
+
+
+def test_smallest_meshes_and_scaled_products():
+    # one or a few unknowns: a single dense block (the root is never admissible
+    # against itself); products, the scaled mul! form and a solve still work
+    for nx, ny in ((1, 1), (2, 1), (3, 2)):
+        m = make_rect_plate(0.05, 0.05, nx, ny)
+        r = build_rwg(m)
+        A = build_aca_operator(m, r, K3, leaf_size=64)
+        assert len(A.lowrank_blocks) == 0 and len(A.dense_blocks) == 1
+        Z = _dense(m, r, K3)
+        x = np.arange(1, r.nedges + 1) * (1 - 0.5j)
+        np.testing.assert_allclose(A @ x, Z @ x, rtol=1e-14)
+        y = np.ones(r.nedges, complex)
+        np.testing.assert_allclose(A.mul(x, 2.0, -1j, y), 2.0 * (Z @ x) - 1j * np.ones(r.nedges), rtol=1e-14)
+        np.testing.assert_allclose(A.H @ x, Z.conj().T @ x, rtol=1e-14)
+        P = build_nearfield_preconditioner(A)
+        I, st = solve_gmres(A, Z @ x, preconditioner=P, tol=1e-12, maxiter=50)
+        np.testing.assert_allclose(I, x, rtol=1e-9)
+        A.close()
