@@ -87,6 +87,9 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     c->d_trsm_id.release();
     c->d_Wraw.release();
     c->d_trsm_t.release();
+    c->d_sv_acc.release();
+    c->d_sv_part.release();
+    c->d_sv_inv.release();
     c->d_Zv.release();
     c->d_small.release();
     c->aca.release();

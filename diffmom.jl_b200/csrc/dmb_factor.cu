@@ -961,7 +961,18 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     DMB_REQUIRE(dmb::tc_error_word(c) == 0, DMB_ERR_TIMEOUT, "tensor-core update: a pipeline wait expired");
 }
 
+void ldlt_solve_blocked_c64(dmb_ctx *c, const float2 *F, double2 *x, int64_t R);
+
 template <class C> void ldlt_solve(dmb_ctx *c, const C *F, double2 *x, int64_t R) {
+  if constexpr (std::is_same<C, float2>::value) {
+    // complex64 factor, one right-hand side: blocked sweeps with the 1024-row
+    // block inverses (the flag-ordered sweeps below run a few columns
+    // concurrently and are faster from two on)
+    if (R == 1) {
+      ldlt_solve_blocked_c64(c, F, x, R);
+      return;
+    }
+  }
   const int64_t N = c->n;
   const int nblk = (int)((N + NB - 1) / NB);
   const size_t flag_words = (size_t)R * nblk + R;
@@ -1185,16 +1196,22 @@ __global__ void k_inv_init(int64_t N, const float2 *__restrict__ Linv, double2 *
   X[col * N + r] = v;
 }
 
+template <class TC> __device__ __forceinline__ TC inv_conv(double2 v);
+template <> __device__ __forceinline__ float2 inv_conv<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <> __device__ __forceinline__ double2 inv_conv<double2>(double2 v) { return v; }
+
 // one product of a doubling level; pair slot y of outer block y / ppo covers
 // A = [i0, i0 + s), B = [i0 + s, i0 + s + sb), i0 = o0 + 2 s (y % ppo)
 //   STEP 1: T = F[B, A] (strict lower part of L) x A^-1     (sb x s)
 //   STEP 2: X[B, A] = -B^-1 x T                             (sb x s)
 // 64 x 64 output tiles (grid.x), FP32 SIMT with 16-deep shared stages
-template <int STEP>
+// TC: the arithmetic of the products (float2 for the tensor-core sweeps'
+// inverses, double2 for the one-RHS sweeps')
+template <int STEP, class TC = float2>
 __global__ void __launch_bounds__(256) k_inv_level(int64_t N, int s, const float2 *__restrict__ F,
-                                                   double2 *__restrict__ X, float2 *__restrict__ T) {
-  __shared__ float2 As[16][65];
-  __shared__ float2 Bs[16][65];
+                                                   double2 *__restrict__ X, TC *__restrict__ T) {
+  __shared__ TC As[16][65];
+  __shared__ TC Bs[16][65];
   const int ppo = TP_OUTER / (2 * s);
   const int64_t o0 = (int64_t)(blockIdx.y / ppo) * TP_OUTER;
   const int64_t o1 = min(N, o0 + TP_OUTER);
@@ -1205,13 +1222,13 @@ __global__ void __launch_bounds__(256) k_inv_level(int64_t N, int s, const float
   const int nt = (s + 63) / 64;
   const int ti = blockIdx.x / nt, tj = blockIdx.x % nt;
   if (64 * ti >= sb) return;
-  float2 *Tp = T + (int64_t)blockIdx.y * s * s;  // column-major sb x s, leading dimension s
+  TC *Tp = T + (int64_t)blockIdx.y * s * s;  // column-major sb x s, leading dimension s
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  float2 acc[4][4];
+  TC acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.f, 0.f);
+    for (int j = 0; j < 4; j++) acc[i][j] = czero<TC>();
   // STEP 1: k runs over A's columns from the tile's first column (A^-1 is
   // lower); STEP 2: over B's columns up to the tile's last row (B^-1 is lower)
   const int k_lo = STEP == 1 ? 64 * tj : 0;
@@ -1221,22 +1238,23 @@ __global__ void __launch_bounds__(256) k_inv_level(int64_t N, int s, const float
       if (STEP == 1) {
         const int kk = e & 15, rr = e >> 4;  // k fastest: F rows and X columns are k-contiguous
         const int k = k0 + kk, i = 64 * ti + rr, j = 64 * tj + rr;
-        As[kk][rr] = (k < k_hi && i < sb) ? F[(b0 + i) * N + a0 + k] : make_float2(0.f, 0.f);
+        const float2 f = (k < k_hi && i < sb) ? F[(b0 + i) * N + a0 + k] : make_float2(0.f, 0.f);
+        As[kk][rr] = inv_conv<TC>(make_double2(f.x, f.y));
         const double2 x = (k < k_hi) ? X[(a0 - o0 + j) * N + a0 + k] : make_double2(0.0, 0.0);
-        Bs[kk][rr] = make_float2((float)x.x, (float)x.y);
+        Bs[kk][rr] = inv_conv<TC>(x);
       } else {
         const int rr = e & 63, kk = e >> 6;  // rows fastest for B^-1 (column-major)
         const int k = k0 + kk, i = 64 * ti + rr;
         const double2 x = (k < k_hi && i < sb) ? X[(b0 - o0 + k) * N + b0 + i] : make_double2(0.0, 0.0);
-        As[kk][rr] = make_float2((float)x.x, (float)x.y);
+        As[kk][rr] = inv_conv<TC>(x);
         const int kk2 = e & 15, cc = e >> 4, k2 = k0 + kk2, j = 64 * tj + cc;
-        Bs[kk2][cc] = (k2 < k_hi && j < s) ? Tp[(int64_t)j * s + k2] : make_float2(0.f, 0.f);
+        Bs[kk2][cc] = (k2 < k_hi && j < s) ? Tp[(int64_t)j * s + k2] : czero<TC>();
       }
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < 16; kk++) {
-      float2 a[4], b[4];
+      TC a[4], b[4];
 #pragma unroll
       for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
@@ -1264,29 +1282,155 @@ __global__ void __launch_bounds__(256) k_inv_level(int64_t N, int s, const float
 // Pack the complex64 factor for the tensor-core sweeps (once per
 // factorisation): L'' and (L^T)'', and the inverses of the 1024-row diagonal
 // blocks of L (recursive doubling, k_inv_init / k_inv_level).
+// The 1024-row block inverses of L (once per factorisation): FP32 products
+// into d_trsm_id for the tensor-core sweeps (which round them to TF32
+// anyway), FP64 products into d_sv_inv for the one-RHS sweeps (as accurate as
+// substitution with the stored 64-block inverses).
+template <class TC> void prepare_block_inverses(dmb_ctx *c, const float2 *F) {
+  constexpr bool f64 = std::is_same<TC, double2>::value;
+  uint64_t &ver = f64 ? c->f_inv64 : c->f_inv;
+  if (ver == c->f_version) return;
+  const int64_t N = c->n;
+  DevBuf &dst = f64 ? c->d_sv_inv : c->d_trsm_id;
+  dst.ensure(sizeof(double2) * N * TP_OUTER);
+  double2 *Xid = dst.as<double2>();
+  const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
+  // scratch for the products T: (pair slots) x s x s <= nout x 1024 x 256
+  c->d_trsm_t.ensure(sizeof(TC) * nout * TP_OUTER * (TP_OUTER / 4));
+  TC *T = c->d_trsm_t.as<TC>();
+  DMB_LAUNCH(c, k_inv_init, blocks_for(N * TP_OUTER, 256), 256, 0, N, c->d_dinv.as<float2>(), Xid);
+  for (int s = NB; s < TP_OUTER; s *= 2) {
+    const int nt = (s + 63) / 64;
+    dim3 g((unsigned)(nt * nt), (unsigned)(nout * (TP_OUTER / (2 * s))));
+    DMB_LAUNCH(c, (k_inv_level<1, TC>), g, 256, 0, N, s, F, Xid, T);
+    DMB_LAUNCH(c, (k_inv_level<2, TC>), g, 256, 0, N, s, F, Xid, T);
+  }
+  ver = c->f_version;
+}
+
 void prepare_packed_factor(dmb_ctx *c, const float2 *F) {
   if (c->f_packed == c->f_version) return;
   const int64_t N = c->n;
   trsm_panel_attrs<float2>();
   dmb::tc_trsm_pack_factor(c, F, N);
-  c->d_trsm_id.ensure(sizeof(double2) * N * TP_OUTER);
+  prepare_block_inverses<float2>(c, F);
   double2 *Xid = c->d_trsm_id.as<double2>();
   const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
-  // scratch for the products T: (pair slots) x s x s <= nout x 1024 x 256
-  c->d_trsm_t.ensure(sizeof(float2) * nout * TP_OUTER * (TP_OUTER / 4));
-  float2 *T = c->d_trsm_t.as<float2>();
-  DMB_LAUNCH(c, k_inv_init, blocks_for(N * TP_OUTER, 256), 256, 0, N, c->d_dinv.as<float2>(), Xid);
-  for (int s = NB; s < TP_OUTER; s *= 2) {
-    const int nt = (s + 63) / 64;
-    dim3 g((unsigned)(nt * nt), (unsigned)(nout * (TP_OUTER / (2 * s))));
-    DMB_LAUNCH(c, k_inv_level<1>, g, 256, 0, N, s, F, Xid, T);
-    DMB_LAUNCH(c, k_inv_level<2>, g, 256, 0, N, s, F, Xid, T);
-  }
   for (int64_t o = 0; o < nout; o++) {
     const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
     dmb::tc_trsm_pack_diag(c, o, Xid + o0, N, (int)(o1 - o0));
   }
   c->f_packed = c->f_version;
+}
+
+// ---------------------------------------------------------------------------
+// One-RHS sweeps of a complex64 factor with the 1024-row block inverses X_o:
+//   forward, o = 0, 1, ...:  a = b_o - L[o, <o] y;   y_o = X_o a
+//   backward, o = last..0:   a = z_o - L[>o, o]^T x; x_o = X_o^T a
+// Eleven block steps per sweep at N = 10,680, each two or three launches of
+// bandwidth-bound products (L read once per sweep, X_o once); no waits
+// between CTAs, fixed summation order.
+// ---------------------------------------------------------------------------
+constexpr int SV_IC = 64;  // rows per partial-sum chunk of the column products
+
+// y[i] = (SUB ? b[i] - s : s), s = sum_j M[i ld + j] v[j], i < rows: a warp per row
+template <class MC, bool SUB>
+__global__ void __launch_bounds__(256) k_sv_rowdot(int rows, int cols, const MC *__restrict__ M, int64_t ld,
+                                                   const double2 *__restrict__ v, const double2 *__restrict__ b,
+                                                   double2 *__restrict__ y) {
+  const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (i >= rows) return;
+  const MC *Mi = M + (int64_t)i * ld;
+  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+  int j = lane;
+  for (; j + 32 < cols; j += 64) {
+    cfma(a0, to_d2(Mi[j]), v[j]);
+    cfma(a1, to_d2(Mi[j + 32]), v[j + 32]);
+  }
+  if (j < cols) cfma(a0, to_d2(Mi[j]), v[j]);
+  a0 = warp_sum2(cadd(a0, a1));
+  if (lane == 0) y[i] = SUB ? csub(b[i], a0) : a0;
+}
+
+// part[chunk][j] = sum over the chunk's rows i of M[i ld + j] v[i], j < ncols
+// (chunk = blockIdx.y, SV_IC rows; consecutive threads read consecutive j)
+template <class MC>
+__global__ void __launch_bounds__(256) k_sv_colpart(int nrows, int ncols, const MC *__restrict__ M, int64_t ld,
+                                                    const double2 *__restrict__ v, double2 *__restrict__ part) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ncols) return;
+  const int i0 = blockIdx.y * SV_IC, i1 = min(nrows, i0 + SV_IC);
+  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+  int i = i0;
+  for (; i + 1 < i1; i += 2) {
+    cfma(a0, to_d2(M[(int64_t)i * ld + j]), v[i]);
+    cfma(a1, to_d2(M[(int64_t)(i + 1) * ld + j]), v[i + 1]);
+  }
+  if (i < i1) cfma(a0, to_d2(M[(int64_t)i * ld + j]), v[i]);
+  part[(int64_t)blockIdx.y * ncols + j] = cadd(a0, a1);
+}
+
+// y[j] = (sub ? b[j] - s : s), s = the chunks' partial sums in order
+__global__ void k_sv_colsum(int ncols, int nchunks, const double2 *__restrict__ part, const double2 *__restrict__ b,
+                            int sub, double2 *__restrict__ y) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ncols) return;
+  double2 s = make_double2(0, 0);
+  for (int q = 0; q < nchunks; q++) s = cadd(s, part[(int64_t)q * ncols + j]);
+  y[j] = sub ? csub(b[j], s) : s;
+}
+
+void ldlt_solve_blocked_c64(dmb_ctx *c, const float2 *F, double2 *x, int64_t R) {
+  const int64_t N = c->n;
+  prepare_block_inverses<double2>(c, F);
+  const double2 *X = c->d_sv_inv.as<double2>();
+  const int64_t nout = (N + TP_OUTER - 1) / TP_OUTER;
+  const int max_chunks = (int)std::max<int64_t>((N + SV_IC - 1) / SV_IC, 1);
+  c->d_sv_acc.ensure(sizeof(double2) * TP_OUTER);
+  c->d_sv_part.ensure(sizeof(double2) * (size_t)max_chunks * TP_OUTER);
+  double2 *acc = c->d_sv_acc.as<double2>(), *part = c->d_sv_part.as<double2>();
+  for (int64_t r = 0; r < R; r++) {
+    double2 *xr = x + r * N;
+    for (int64_t o = 0; o < nout; o++) {  // forward
+      const int64_t o0 = o * TP_OUTER;
+      const int w = (int)std::min<int64_t>(TP_OUTER, N - o0);
+      const double2 *a = xr + o0;
+      if (o0 > 0) {
+        DMB_LAUNCH(c, (k_sv_rowdot<float2, true>), blocks_for((int64_t)w * 32, 256), 256, 0, w, (int)o0,
+                   F + o0 * N, N, xr, xr + o0, acc);
+        a = acc;
+      }
+      const int nch = (w + SV_IC - 1) / SV_IC;
+      // y_o[i] = sum_k X_o[i][k] a[k]; X_o column k is contiguous: X[k N + o0 + i]
+      DMB_LAUNCH(c, k_sv_colpart<double2>, dim3(blocks_for(w, 256), (unsigned)nch), 256, 0, w, w, X + o0, N, a,
+                 part);
+      DMB_LAUNCH(c, k_sv_colsum, blocks_for(w, 256), 256, 0, w, nch, part, (const double2 *)nullptr, 0, xr + o0);
+    }
+    DMB_LAUNCH(c, k_scale_by_dinv<float2>, blocks_for(N, 256), 256, 0, N, (int64_t)1, F, xr);
+    for (int64_t o = nout - 1; o >= 0; o--) {  // backward
+      const int64_t o0 = o * TP_OUTER, o1 = std::min<int64_t>(N, o0 + TP_OUTER);
+      const int w = (int)(o1 - o0);
+      const double2 *a = xr + o0;
+      if (o1 < N) {
+        // a[c] = z[o0 + c] - sum_{i >= o1} L[i][o0 + c] x[i]
+        const int nr = (int)(N - o1), nch = (nr + SV_IC - 1) / SV_IC;
+        DMB_LAUNCH(c, k_sv_colpart<float2>, dim3(blocks_for(w, 256), (unsigned)nch), 256, 0, nr, w,
+                   F + o1 * N + o0, N, xr + o1, part);
+        DMB_LAUNCH(c, k_sv_colsum, blocks_for(w, 256), 256, 0, w, nch, part, xr + o0, 1, acc);
+        a = acc;
+      }
+      // x_o[k] = sum_i X_o[i][k] a[i] = sum_i X[k N + o0 + i] a[i]: a warp per output
+      if (a == acc) {
+        DMB_LAUNCH(c, (k_sv_rowdot<double2, false>), blocks_for((int64_t)w * 32, 256), 256, 0, w, w, X + o0, N, a,
+                   (const double2 *)nullptr, xr + o0);
+      } else {
+        // the last block reads and writes x_o: go through the scratch vector
+        DMB_CUDA(cudaMemcpyAsync(acc, xr + o0, sizeof(double2) * w, cudaMemcpyDeviceToDevice, c->stream));
+        DMB_LAUNCH(c, (k_sv_rowdot<double2, false>), blocks_for((int64_t)w * 32, 256), 256, 0, w, w, X + o0, N,
+                   acc, (const double2 *)nullptr, xr + o0);
+      }
+    }
+  }
 }
 
 template <class C> void ldlt_solve_batched(dmb_ctx *c, const C *F, double2 *X, int64_t R) {

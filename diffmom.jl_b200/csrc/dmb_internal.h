@@ -243,6 +243,9 @@ struct dmb_ctx {
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves
+  uint64_t f_inv = ~0ull;        // factor version whose 1024-row block inverses are in d_trsm_id
+  uint64_t f_inv64 = ~0ull;      // ... whose FP64-product block inverses are in d_sv_inv
+  DevBuf d_sv_acc, d_sv_part, d_sv_inv;  // the blocked one-RHS sweeps: scratch and block inverses
   // inputs of the current host topology (build_host_topology)
   bool topo_valid = false;
   std::vector<int32_t> topo_tri, topo_tplus, topo_tminus;
