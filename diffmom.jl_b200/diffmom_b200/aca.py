@@ -235,8 +235,10 @@ def _scaled(Ax: np.ndarray, alpha, beta, y):
 class ACAOperator:
     """H-matrix operator (ACA.jl:173-181) resident on a device context."""
 
-    def __init__(self, device, info: nat.AcaInfo, k: float, eta0: float, quad_order: int):
+    def __init__(self, device, info: nat.AcaInfo, k: float, eta0: float, quad_order: int,
+                 owns_device: bool = False):
         self.device = device
+        self._owns_device = owns_device
         self.N = device.N
         self.shape = (self.N, self.N)
         self.k, self.eta0, self.quad_order = k, eta0, quad_order
@@ -346,7 +348,10 @@ class ACAOperator:
                                  adjoint=adjoint)
 
     def close(self):
-        self.device.close()
+        """Release the device context if build_aca_operator created it (a
+        context passed in by the caller stays open)."""
+        if self._owns_device:
+            self.device.close()
 
 
 class ACAAdjointOperator:
@@ -425,4 +430,4 @@ def build_aca_operator(mesh: TriMesh, rwg: RWGData, k, leaf_size: int = 64, eta:
             dev.close()
         raise
     dev.preconditioner = None
-    return ACAOperator(dev, info, float(k), float(eta0), int(quad_order))
+    return ACAOperator(dev, info, float(k), float(eta0), int(quad_order), owns_device=device is None)
