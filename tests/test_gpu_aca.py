@@ -284,7 +284,8 @@ def test_smallest_meshes_and_scaled_products():
         y = np.ones(r.nedges, complex)
         np.testing.assert_allclose(A.mul(x, 2.0, -1j, y), 2.0 * (Z @ x) - 1j * np.ones(r.nedges), rtol=1e-14)
         np.testing.assert_allclose(A.H @ x, Z.conj().T @ x, rtol=1e-14)
-        P = build_nearfield_preconditioner(A)
-        I, st = solve_gmres(A, Z @ x, preconditioner=P, tol=1e-12, maxiter=50)
-        np.testing.assert_allclose(I, x, rtol=1e-9)
+        for prec in ("fp64", "mixed"):
+            P = build_nearfield_preconditioner(A, precision=prec)
+            I, st = solve_gmres(A, Z @ x, preconditioner=P, tol=1e-12, maxiter=50)
+            np.testing.assert_allclose(I, x, rtol=1e-9)
         A.close()

@@ -100,6 +100,26 @@ def test_fp64_accumulated_zx_matches_column_products():
     dev.close()
 
 
+def test_one_column_blocked_sweeps_match_chained_sweeps():
+    # 4,720 RWG: five 1024-row blocks, the last one ragged.  One column of a
+    # complex64 factor runs the blocked sweeps (FP64-product block inverses),
+    # two columns the flag-ordered 64-row chain: same solve to FP32 level
+    dev = _plate(40, side=0.3)
+    dev.assemble(K3, precision="mixed")
+    dev.build_nearfield(float("inf"), "lu")
+    X = _rand(dev.N, 2, 3)
+    Y2 = dev.nf_apply(X)
+    for j in (0, 1):
+        y1 = dev.nf_apply(np.ascontiguousarray(X[:, j]))
+        err = np.linalg.norm(y1 - Y2[:, j]) / np.linalg.norm(Y2[:, j])
+        res = np.linalg.norm(dev.matvec(y1) - X[:, j]) / np.linalg.norm(X[:, j])
+        print(f"column {j}: blocked vs chained {err:.2e}, residual with Z {res:.2e}")
+        assert err < 1e-5 and res < 1e-3
+    np.testing.assert_array_equal(dev.nf_apply(np.ascontiguousarray(X[:, 0])),
+                                  dev.nf_apply(np.ascontiguousarray(X[:, 0])))  # deterministic
+    dev.close()
+
+
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_batched_nearfield_solve_matches_column_solves(precision):
     dev = _plate(24)
