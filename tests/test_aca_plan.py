@@ -222,3 +222,30 @@ def test_scaled_product_contract():
     np.testing.assert_allclose(_scaled(Ax, 0.5 - 1j, 2.0, y), (0.5 - 1j) * Ax + 2.0)
     with pytest.raises(OverflowError):
         _scaled(np.array([1e308 + 0j]), 10.0, 0.0, np.zeros(1, complex))
+
+
+def test_plan_abi_two_call_protocol_and_task_limit():
+    # dmb_aca_plan: the task count always comes back; the task array is
+    # written only when its capacity suffices; max_block_tasks equal to the
+    # task count passes, one less fails
+    import ctypes
+    lib = nat.load_library()
+    c = np.ascontiguousarray(_plate_centers(8, 8))
+    n = c.shape[0]
+    perm = np.empty(n, np.int64)
+    nn, nt = ctypes.c_int64(), ctypes.c_int64()
+    nat.check_free(lib, lib.dmb_aca_plan(nat.dptr(c), n, 4, 1.5, 1 << 40, nat.lptr(perm), ctypes.byref(nn), None,
+                                         None, ctypes.byref(nt), None, 0))
+    count = nt.value
+    assert count > 1 and sorted(perm.tolist()) == list(range(1, n + 1))
+    small = np.full((count - 1, 5), -7, np.int64)
+    nat.check_free(lib, lib.dmb_aca_plan(nat.dptr(c), n, 4, 1.5, 1 << 40, None, None, None, None,
+                                         ctypes.byref(nt), nat.lptr(small), count - 1))
+    assert nt.value == count and np.all(small == -7)
+    full = np.empty((count, 5), np.int64)
+    nat.check_free(lib, lib.dmb_aca_plan(nat.dptr(c), n, 4, 1.5, count, None, None, None, None,
+                                         ctypes.byref(nt), nat.lptr(full), count))
+    assert set(full[:, 2].tolist()) <= {0, 1} and np.all(full[:, :2] >= 1)
+    with pytest.raises(ValueError, match="max_block_tasks"):
+        nat.check_free(lib, lib.dmb_aca_plan(nat.dptr(c), n, 4, 1.5, count - 1, None, None, None, None,
+                                             ctypes.byref(nt), None, 0))
