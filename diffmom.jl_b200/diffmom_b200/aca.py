@@ -74,10 +74,40 @@ def _plan(centers, leaf_size, eta=1.5, max_block_tasks=_DEFAULT_MAX_ACA_BLOCK_TA
     return perm[:n], nodes[:nn.value], boxes[:nn.value], (tasks[:nt.value] if want_tasks else None)
 
 
-def build_cluster_tree(centers, leaf_size: int = 64) -> ClusterTree:
+_DEFAULT_MAX_CLUSTER_TREE_NODES = 30_000_000
+_DEFAULT_MAX_CLUSTER_TREE_STORAGE_BYTES = 2_000_000_000
+_CLUSTER_NODE_BYTES = 88  # UnitRange{Int} + two Vec3 + three Int
+
+
+def cluster_tree_resource_bounds(N: int, leaf_size: int):
+    """_cluster_tree_resource_bounds (ClusterTree.jl:13-36): the node count of
+    a tree whose leaf count is the next power of two above ceil(N / leaf_size),
+    and its storage (nodes plus perm, iperm and the centre order)."""
+    target = -(-N // leaf_size)
+    leaves = 1
+    while leaves < target:
+        leaves *= 2
+    nodes = 2 * leaves - 1
+    return nodes, nodes * _CLUSTER_NODE_BYTES + 3 * N * 8
+
+
+def build_cluster_tree(centers, leaf_size: int = 64, max_nodes: int = _DEFAULT_MAX_CLUSTER_TREE_NODES,
+                       max_storage_bytes: int = _DEFAULT_MAX_CLUSTER_TREE_STORAGE_BYTES) -> ClusterTree:
     """build_cluster_tree (ClusterTree.jl:82-166): median bisection along the
     longest bounding-box axis of `centers` (N x 3)."""
-    perm, nodes, boxes, _ = _plan(centers, leaf_size, max_block_tasks=1 << 62)
+    c = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+    if c.shape[0] == 0:
+        raise ValueError("build_cluster_tree: centers must not be empty")
+    if leaf_size < 1:
+        raise ValueError(f"build_cluster_tree: leaf_size must be at least 1, got {leaf_size}")
+    if max_nodes < 1 or max_storage_bytes < 1:
+        raise ValueError("cluster-tree resource limits must be positive")
+    nb, sb = cluster_tree_resource_bounds(c.shape[0], leaf_size)
+    if nb > max_nodes:
+        raise ValueError(f"cluster tree requires at most {nb} nodes, exceeding max_nodes={max_nodes}")
+    if sb > max_storage_bytes:
+        raise ValueError(f"cluster-tree arrays require {sb} bytes, exceeding max_storage_bytes={max_storage_bytes}")
+    perm, nodes, boxes, _ = _plan(c, leaf_size, max_block_tasks=1 << 62)
     tree_nodes = [ClusterNode(range(int(r[0]), int(r[1]) + 1), b[:3].copy(), b[3:].copy(), int(r[2]), int(r[3]),
                               int(r[4])) for r, b in zip(nodes, boxes)]
     iperm = np.empty_like(perm)

@@ -249,3 +249,47 @@ def test_plan_abi_two_call_protocol_and_task_limit():
     with pytest.raises(ValueError, match="max_block_tasks"):
         nat.check_free(lib, lib.dmb_aca_plan(nat.dptr(c), n, 4, 1.5, count - 1, None, None, None, None,
                                              ctypes.byref(nt), None, 0))
+
+
+def test_reference_cluster_tree_fixtures():
+    # runtests.jl:9318-9395: resource bounds, invalid centres, tree invariants
+    # and the rounded-boundary admissibility pair
+    from diffmom_b200.aca import cluster_tree_resource_bounds, ClusterTree, ClusterNode
+    c = _plate_centers(12, 12)
+    N = c.shape[0]
+    tree = build_cluster_tree(c, 8)
+    nb, sb = cluster_tree_resource_bounds(N, 8)
+    with pytest.raises(ValueError, match="max_nodes"):
+        build_cluster_tree(c, 8, max_nodes=nb - 1)
+    with pytest.raises(ValueError, match="max_storage_bytes"):
+        build_cluster_tree(c, 8, max_nodes=nb, max_storage_bytes=sb - 1)
+    np.testing.assert_array_equal(build_cluster_tree(c, 8, max_nodes=nb, max_storage_bytes=sb).perm, tree.perm)
+    for bad in ([[math.nan, 0.0, 0.0]], [[-np.finfo(float).max, 0, 0], [np.finfo(float).max, 0, 0]]):
+        with pytest.raises(ValueError):
+            build_cluster_tree(np.array(bad, dtype=float), 8)
+    assert sorted(tree.perm.tolist()) == list(range(1, N + 1))
+    np.testing.assert_array_equal(tree.iperm[tree.perm - 1], np.arange(1, N + 1))
+    assert tree.nodes[0].indices == range(1, N + 1)
+    for i in leaf_nodes(tree):
+        assert len(tree.nodes[i - 1].indices) <= 8
+    assert not is_admissible(tree, leaf_nodes(tree)[0], leaf_nodes(tree)[0])
+    for eta in (math.nan, 0.0):
+        with pytest.raises(ValueError):
+            is_admissible(tree, 1, 1, eta=eta)
+    # the stored boxes sit exactly 1.0 apart after rounding, and the exact
+    # decision separates them: prevfloat(2^-26) stays dense, 2^-26 is admissible
+    bx = math.nextafter(1.0, 0.0)
+
+    def pair(y):
+        nodes = [ClusterNode(range(1, 2), np.array([0.0, 0.0, 0.0]), np.array([0.0, 0.0, 1.0]), 0, 0, 0),
+                 ClusterNode(range(2, 3), np.array([bx, y, 0.0]), np.array([bx, y, 1.0]), 0, 0, 0)]
+        return ClusterTree(nodes, np.array([1, 2]), np.array([1, 2]), 1)
+    inside, outside = pair(math.nextafter(2.0 ** -26, 0.0)), pair(2.0 ** -26)
+    assert cluster_distance(inside, 1, 2) == 1.0 and cluster_distance(outside, 1, 2) == 1.0
+    assert not is_admissible(inside, 1, 2, eta=1.0)
+    assert is_admissible(outside, 1, 2, eta=1.0)
+    # and the oracle's exact rationals agree
+    assert not ao.box_admissible(ao.Node(0, 0, tuple(inside.nodes[0].bbox_min), tuple(inside.nodes[0].bbox_max)),
+                                 ao.Node(0, 0, tuple(inside.nodes[1].bbox_min), tuple(inside.nodes[1].bbox_max)), 1.0)
+    assert ao.box_admissible(ao.Node(0, 0, tuple(outside.nodes[0].bbox_min), tuple(outside.nodes[0].bbox_max)),
+                             ao.Node(0, 0, tuple(outside.nodes[1].bbox_min), tuple(outside.nodes[1].bbox_max)), 1.0)
