@@ -293,3 +293,21 @@ def test_reference_cluster_tree_fixtures():
                                  ao.Node(0, 0, tuple(inside.nodes[1].bbox_min), tuple(inside.nodes[1].bbox_max)), 1.0)
     assert ao.box_admissible(ao.Node(0, 0, tuple(outside.nodes[0].bbox_min), tuple(outside.nodes[0].bbox_max)),
                              ao.Node(0, 0, tuple(outside.nodes[1].bbox_min), tuple(outside.nodes[1].bbox_max)), 1.0)
+
+
+def test_oracle_stopping_rule_is_scale_invariant():
+    # runtests.jl:9456-9500 on the oracle: the relative Frobenius rule in
+    # scaled magnitudes gives the same rank and the same factors (up to the
+    # scale) at 1e-200 and 1e200, where squared norms would under/overflow
+    rng = np.random.default_rng(11)
+    x = rng.uniform(0, 1, (40, 3))
+    y = rng.uniform(0, 1, (30, 3)) + np.array([3.0, 0.5, 0])
+    r = np.linalg.norm(x[:, None] - y[None], axis=2)
+    B = np.exp(-3j * r) / r
+    U0, V0, conv0 = ao.aca_lowrank(B, 1e-3, 20)
+    assert conv0 and U0.shape[1] < 20
+    ref = U0 @ V0.conj().T
+    for scale in (1e-200, 1e200):
+        U, V, conv = ao.aca_lowrank(B * scale, 1e-3, 20)
+        assert conv == conv0 and U.shape[1] == U0.shape[1]
+        np.testing.assert_allclose((U @ V.conj().T) / scale, ref, rtol=5e-13, atol=0)
