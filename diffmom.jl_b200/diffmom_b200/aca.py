@@ -269,6 +269,9 @@ class ACAOperator:
                  owns_device: bool = False):
         self.device = device
         self._owns_device = owns_device
+        # a device context holds one H-matrix: a later build on it replaces
+        # this operator's data, after which this object refuses to run
+        device._aca_current = self
         self.N = device.N
         self.shape = (self.N, self.N)
         self.k, self.eta0, self.quad_order = k, eta0, quad_order
@@ -290,11 +293,18 @@ class ACAOperator:
         iperm[perm - 1] = np.arange(1, self.N + 1)
         self.perm, self.iperm = perm, iperm
 
+    def _check_current(self):
+        if getattr(self.device, "_aca_current", None) is not self:
+            raise nat.DiffMoMError("this H-matrix operator was replaced by a later build_aca_operator "
+                                   "on the same device")
+
     def _select(self):
+        self._check_current()
         self.device.ctx.call("dmb_set_option", nat.OPT_OPERATOR, 1)
 
     def _block_data(self, i):
         if i not in self._cache:
+            self._check_current()
             b = self._blocks[i]
             m, n = int(b[2] - b[1] + 1), int(b[4] - b[3] + 1)
             if b[0] == 0:
@@ -311,6 +321,7 @@ class ACAOperator:
 
     def matvec(self, x, mode: int = 0) -> np.ndarray:
         """mode 0: A x, 1: A^H x, 2: A^T x (x: N or N x R)."""
+        self._check_current()
         X = nat.c128(x)
         nrhs = 1 if X.ndim == 1 else X.shape[1]
         Y = np.empty_like(X)
@@ -334,6 +345,7 @@ class ACAOperator:
 
     def entries(self, m, n) -> np.ndarray:
         """getindex (ACA.jl:220-222): EFIE entries Z[m, n] (1-based)."""
+        self._check_current()
         m = np.ascontiguousarray(np.atleast_1d(m), dtype=np.int64)
         n = np.ascontiguousarray(np.atleast_1d(n), dtype=np.int64)
         out = np.empty(m.size, dtype=np.complex128)

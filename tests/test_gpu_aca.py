@@ -289,3 +289,19 @@ def test_smallest_meshes_and_scaled_products():
             I, st = solve_gmres(A, Z @ x, preconditioner=P, tol=1e-12, maxiter=50)
             np.testing.assert_allclose(I, x, rtol=1e-9)
         A.close()
+
+
+def test_rebuild_on_the_same_device_retires_the_old_operator():
+    from diffmom_b200 import DiffMoMError
+    m, r = _plate(8)
+    dev = EFIEDevice(m, r)
+    A1 = build_aca_operator(m, r, K3, leaf_size=8, device=dev)
+    x = np.ones(r.nedges, complex)
+    y1 = A1 @ x
+    A2 = build_aca_operator(m, r, 2 * K3, leaf_size=8, device=dev)
+    with pytest.raises(DiffMoMError, match="replaced"):
+        A1 @ x
+    assert np.linalg.norm(A2 @ x - y1) > 1e-3 * np.linalg.norm(y1)  # the new wavenumber's operator
+    A2.close()  # the caller's context stays open
+    dev.assemble(K3)
+    dev.close()
