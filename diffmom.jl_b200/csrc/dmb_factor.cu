@@ -1341,14 +1341,17 @@ __global__ void __launch_bounds__(256) k_sv_rowdot(int rows, int cols, const MC 
   const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (i >= rows) return;
   const MC *Mi = M + (int64_t)i * ld;
-  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);
+  // four loads in flight per lane (one warp per row leaves few warps)
+  double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0), a2 = make_double2(0, 0), a3 = make_double2(0, 0);
   int j = lane;
-  for (; j + 32 < cols; j += 64) {
+  for (; j + 96 < cols; j += 128) {
     cfma(a0, to_d2(Mi[j]), v[j]);
     cfma(a1, to_d2(Mi[j + 32]), v[j + 32]);
+    cfma(a2, to_d2(Mi[j + 64]), v[j + 64]);
+    cfma(a3, to_d2(Mi[j + 96]), v[j + 96]);
   }
-  if (j < cols) cfma(a0, to_d2(Mi[j]), v[j]);
-  a0 = warp_sum2(cadd(a0, a1));
+  for (; j < cols; j += 32) cfma(a0, to_d2(Mi[j]), v[j]);
+  a0 = warp_sum2(cadd(cadd(a0, a1), cadd(a2, a3)));
   if (lane == 0) y[i] = SUB ? csub(b[i], a0) : a0;
 }
 
