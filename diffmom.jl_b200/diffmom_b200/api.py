@@ -887,6 +887,8 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
         raise ValueError("solve_scattering: method must be :auto, :dense_direct, :dense_gmres, or :aca_gmres")
     if preconditioner not in ("auto", "lu", "diag", "none"):
         raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, or :none")
+    if method == "aca_gmres" and surface_impedance is not None:
+        raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres")
     lam = c0 / f
     k = _frequency_to_wavenumber(f, c0)
     warnings = []
@@ -916,8 +918,6 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
         t0 = time.perf_counter()
         aca_op = None
         if sel == "aca_gmres":
-            if surface_impedance is not None:
-                raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres")
             from .aca import build_aca_operator
             aca_op = build_aca_operator(mesh, rwg, k, leaf_size=aca_leaf_size, eta=aca_eta, aca_tol=aca_tol,
                                         max_rank=aca_max_rank, quad_order=quad_order, device=dev)

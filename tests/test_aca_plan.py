@@ -311,3 +311,14 @@ def test_oracle_stopping_rule_is_scale_invariant():
         U, V, conv = ao.aca_lowrank(B * scale, 1e-3, 20)
         assert conv == conv0 and U.shape[1] == U0.shape[1]
         np.testing.assert_allclose((U @ V.conj().T) / scale, ref, rtol=5e-13, atol=0)
+
+
+def test_solve_scattering_aca_arguments_rejected_on_the_host():
+    from diffmom_b200 import solve_scattering, make_plane_wave
+    m = make_rect_plate(0.1, 0.1, 2, 2)
+    k = 2 * math.pi * 3e9 / 299792458.0
+    pw = make_plane_wave(np.array([0.0, 0.0, -k]), 1.0, np.array([1.0, 0.0, 0.0]))
+    with pytest.raises(ValueError, match="surface_impedance"):
+        solve_scattering(m, 3e9, pw, method="aca_gmres", surface_impedance=np.ones(m.ntriangles))
+    with pytest.raises(ValueError, match="method"):
+        solve_scattering(m, 3e9, pw, method="mlfma")
