@@ -322,3 +322,29 @@ def test_solve_scattering_aca_arguments_rejected_on_the_host():
         solve_scattering(m, 3e9, pw, method="aca_gmres", surface_impedance=np.ones(m.ntriangles))
     with pytest.raises(ValueError, match="method"):
         solve_scattering(m, 3e9, pw, method="mlfma")
+
+
+def test_oracle_hmatrix_on_an_efie_matrix():
+    # the oracle's build_aca_operator restatement on the oracle's own EFIE Z
+    # (plate of 1.5 wavelengths at 3 GHz): far blocks compress, the product
+    # meets the tolerance, and a looser tolerance never raises a block's rank
+    import oracle as orc
+    m = make_rect_plate(0.15, 0.15, 10, 10)
+    r = build_rwg(m)
+    k = 2 * math.pi * 3e9 / 299792458.0
+    Z = orc.OracleCache(m, r, 3).assemble_z(k)
+    c = rwg_centers(m, r)
+    x = np.random.default_rng(2).standard_normal(r.nedges) + 0j
+    ranks = {}
+    for tol in (1e-8, 1e-4):
+        tree, tasks, blocks = ao.build_hmatrix(Z, c, leaf_size=16, eta=1.5, aca_tol=tol, max_rank=50)
+        lr = [b for b in blocks if b.kind == 1]
+        # small far blocks may need their full rank at tight tolerances; the
+        # far field as a whole compresses
+        stored = sum(b.U.shape[1] * (b.m + b.n) for b in lr)
+        assert lr and stored < sum(b.m * b.n for b in lr)
+        y = ao.hmatrix_matvec(blocks, tree.perm, x, 0)
+        err = np.linalg.norm(y - Z @ x) / np.linalg.norm(Z @ x)
+        assert err < 100 * tol
+        ranks[tol] = [b.U.shape[1] for b in lr]
+    assert all(a >= b for a, b in zip(ranks[1e-8], ranks[1e-4]))
