@@ -322,50 +322,58 @@ def run_ours(args):
     # ---- one incidence on the C3 plate: the reference's H-matrix (ACA) path
     # of solve_scattering (10k < N <= 50k) beside the dense single-RHS path
     if not args.quick and any(want(n) for n in ("plate_1wave_aca", "plate_1wave_dense_mixed")):
-        hbm_peak = measured_peaks()[0]
-        sdev = EFIEDevice(mesh, rwg, device=local)
-        v1 = np.ascontiguousarray(sdev.plane_wave_rhs(np.array([[0.0, 0.0, -K]]), [1.0],
-                                                      np.array([[1.0, 0.0, 0.0]]))[:, 0])
-        x1 = np.empty_like(v1)
-        st1 = nat.GmresStats()
-        info = nat.AcaInfo()
-        if want("plate_1wave_aca"):
-            def aca_step():
-                # build_aca_operator defaults of solve_scattering (leaf 64, eta 1.5,
-                # tol 1e-6, rank 50), near-field LU of its dense blocks (complex64),
-                # GMRES to 1e-6
-                sdev.ctx.call("dmb_aca_build", K, 376.730313668, 3, 64, 1.5, 1e-6, 50, 2_000_000, 4_000_000_000,
-                              ctypes.byref(info))
-                sdev.ctx.call("dmb_aca_nf_build", nat.PRECOND_NF_LU, nat.PREC_MIXED, None)
-                sdev.ctx._check(sdev.ctx.lib.dmb_gmres(sdev.ctx.h, nat.dptr(v1), nat.dptr(x1), 1, 1e-6, 300,
-                                                       nat.PRECOND_NF_LU, nat.SIDE_LEFT, 1, ctypes.byref(st1)))
-                return st1.niter, st1.true_residual, st1.restarts
-            va = run.timed(sdev, aca_step, min(args.steps, 3), 1, 1)
-            va["aca"] = {f: getattr(info, f) for f, _ in nat.AcaInfo._fields_}
-            va["aca"]["stored_fraction_of_dense"] = info.entries_stored / float(N) ** 2
-            # H-matrix product alone: event-timed inside the library (family 3)
-            xr = np.ascontiguousarray(np.random.default_rng(1).standard_normal(N) + 0j)
-            yr = np.empty_like(xr)
-            sdev.ctx.call("dmb_aca_matvec", nat.dptr(xr), nat.dptr(yr), 1, 0)
-            sdev.ctx.call("dmb_set_kernel_timing", 1)
-            for _ in range(20):
+        sdev = None
+        try:
+            hbm_peak = measured_peaks()[0]
+            sdev = EFIEDevice(mesh, rwg, device=local)
+            v1 = np.ascontiguousarray(sdev.plane_wave_rhs(np.array([[0.0, 0.0, -K]]), [1.0],
+                                                          np.array([[1.0, 0.0, 0.0]]))[:, 0])
+            x1 = np.empty_like(v1)
+            st1 = nat.GmresStats()
+            info = nat.AcaInfo()
+            if want("plate_1wave_aca"):
+                def aca_step():
+                    # build_aca_operator defaults of solve_scattering (leaf 64, eta 1.5,
+                    # tol 1e-6, rank 50), near-field LU of its dense blocks (complex64),
+                    # GMRES to 1e-6
+                    sdev.ctx.call("dmb_aca_build", K, 376.730313668, 3, 64, 1.5, 1e-6, 50, 2_000_000, 4_000_000_000,
+                                  ctypes.byref(info))
+                    sdev.ctx.call("dmb_aca_nf_build", nat.PRECOND_NF_LU, nat.PREC_MIXED, None)
+                    sdev.ctx._check(sdev.ctx.lib.dmb_gmres(sdev.ctx.h, nat.dptr(v1), nat.dptr(x1), 1, 1e-6, 300,
+                                                           nat.PRECOND_NF_LU, nat.SIDE_LEFT, 1, ctypes.byref(st1)))
+                    return st1.niter, st1.true_residual, st1.restarts
+                va = run.timed(sdev, aca_step, min(args.steps, 3), 1, 1)
+                va["aca"] = {f: getattr(info, f) for f, _ in nat.AcaInfo._fields_}
+                va["aca"]["stored_fraction_of_dense"] = info.entries_stored / float(N) ** 2
+                # H-matrix product alone: event-timed inside the library (family 3)
+                xr = np.ascontiguousarray(np.random.default_rng(1).standard_normal(N) + 0j)
+                yr = np.empty_like(xr)
                 sdev.ctx.call("dmb_aca_matvec", nat.dptr(xr), nat.dptr(yr), 1, 0)
-            kms, kl, kw = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
-            sdev.ctx.call("dmb_kernel_timing_family", 3, ctypes.byref(kms), ctypes.byref(kl), ctypes.byref(kw))
-            sdev.ctx.call("dmb_set_kernel_timing", 0)
-            gbs = (kw.value / 1e9) / (kms.value / 1e3) if kms.value > 0 else None
-            va["product"] = {"ms": kms.value / max(kl.value, 1), "launch_groups": kl.value,
-                             "bytes_per_product": kw.value / max(kl.value, 1), "achieved_gbs": gbs,
-                             "frac_of_measured_hbm": (gbs / hbm_peak) if gbs else None}
-            variants["plate_1wave_aca"] = va
-        if want("plate_1wave_dense_mixed"):
-            p1 = solve_params(nat, K, nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf, side=1, maxiter=300)
+                sdev.ctx.call("dmb_set_kernel_timing", 1)
+                for _ in range(20):
+                    sdev.ctx.call("dmb_aca_matvec", nat.dptr(xr), nat.dptr(yr), 1, 0)
+                kms, kl, kw = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+                sdev.ctx.call("dmb_kernel_timing_family", 3, ctypes.byref(kms), ctypes.byref(kl), ctypes.byref(kw))
+                sdev.ctx.call("dmb_set_kernel_timing", 0)
+                gbs = (kw.value / 1e9) / (kms.value / 1e3) if kms.value > 0 else None
+                va["product"] = {"ms": kms.value / max(kl.value, 1), "launch_groups": kl.value,
+                                 "bytes_per_product": kw.value / max(kl.value, 1), "achieved_gbs": gbs,
+                                 "frac_of_measured_hbm": (gbs / hbm_peak) if gbs else None}
+                variants["plate_1wave_aca"] = va
+            if want("plate_1wave_dense_mixed"):
+                p1 = solve_params(nat, K, nat.PREC_MIXED, nat.PRECOND_NF_LU, math.inf, side=1, maxiter=300)
 
-            def dense_step():
-                sdev.ctx.call("dmb_solve_resident", ctypes.byref(p1), ctypes.byref(st1))
-                return st1.niter, st1.true_residual, st1.restarts
-            variants["plate_1wave_dense_mixed"] = run.timed(sdev, dense_step, min(args.steps, 3), 1, 1)
-        sdev.close()
+                def dense_step():
+                    sdev.ctx.call("dmb_solve_resident", ctypes.byref(p1), ctypes.byref(st1))
+                    return st1.niter, st1.true_residual, st1.restarts
+                variants["plate_1wave_dense_mixed"] = run.timed(sdev, dense_step, min(args.steps, 3), 1, 1)
+            sdev.close()
+        except Exception as e:  # optional variants: the headline line still prints
+            for name in ("plate_1wave_aca", "plate_1wave_dense_mixed"):
+                if want(name) and name not in variants:
+                    variants[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            if sdev is not None:
+                sdev.close()
 
     # ---- C4 uneven batch of 64 impedance-loaded surfaces -------------------
     if not args.quick and any(want(n) for n in ("c4_batch64_mixed", "c4_batch64_fp64_1lane")):
@@ -484,7 +492,7 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                  ("c2_mixed_nf_lu", "c2_fp64_nf_lu"), ("c5_mixed_learned", "c5_fp64_nf_lu"),
                  ("c5_mixed_nf_lu", "c5_fp64_nf_lu"), ("c5_mixed_local", "c5_fp64_nf_lu"),
                  ("plate_1wave_dense_mixed", "plate_1wave_aca")):
-        if a in variants and b in variants:
+        if "solves_per_s" in variants.get(a, {}) and "solves_per_s" in variants.get(b, {}):
             speed[f"{a}_vs_{b}"] = variants[a]["solves_per_s"] / variants[b]["solves_per_s"]
     line = {
         "metric": METRIC,
