@@ -1,7 +1,8 @@
 """Writes the golden fixtures of the GPU parity tests from the oracle (the CPU
 restatement of the reference algorithm, pinned by tests/test_oracle_golden.py).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py aca      # aca_plan_plate.npz only
 
 c1_plate.npz -- README minimal case: 0.1 x 0.1 m plate, 6 x 6 cells (72
     triangles, 96 RWG), k = 2 pi / 0.1, quad_order 3: the full Z, the x-pol
@@ -10,6 +11,10 @@ c1_plate.npz -- README minimal case: 0.1 x 0.1 m plate, 6 x 6 cells (72
     incidences with their currents.
 c2_sphere_sample.npz -- PEC sphere r = 0.5 lambda at 3 GHz, icosphere 5,120
     triangles / 7,680 RWG: 512 seeded Z entries (quad_order 3) and the RHS.
+aca_plan_plate.npz -- the H-matrix block plan of a 1 x 1 m plate, 12 x 12
+    cells (RWG centres), leaf sizes 4 and 16 at eta 1.5: tree permutation,
+    node ranges / children / levels / boxes and the task list, from the
+    oracle's restatement of ClusterTree.jl and ACA.jl:696-738.
 """
 import math
 import sys
@@ -77,8 +82,28 @@ def c2_sample(out):
     np.savez_compressed(out, k=k, m=m, n=n, z=z, v=v)
 
 
+def aca_plan(out):
+    import aca_oracle as ao
+    from diffmom_b200 import rwg_centers
+    m = make_rect_plate(1.0, 1.0, 12, 12)
+    c = rwg_centers(m, build_rwg(m))
+    arrays = {"centers": c}
+    for leaf in (4, 16):
+        tree = ao.build_cluster_tree(c, leaf)
+        tasks = ao.enum_block_tasks(tree, 1.5)
+        arrays[f"perm_{leaf}"] = np.asarray(tree.perm, dtype=np.int64)
+        arrays[f"nodes_{leaf}"] = np.array([[n.lo, n.hi, n.left, n.right, n.level] for n in tree.nodes], np.int64)
+        arrays[f"boxes_{leaf}"] = np.array([list(n.bmin) + list(n.bmax) for n in tree.nodes])
+        arrays[f"tasks_{leaf}"] = np.array(tasks, dtype=np.int64)
+    np.savez_compressed(out, **arrays)
+
+
 if __name__ == "__main__":
     here = Path(__file__).resolve().parent
-    c1_plate(here / "c1_plate.npz")
-    c2_sample(here / "c2_sphere_sample.npz")
+    if len(sys.argv) > 1 and sys.argv[1] == "aca":
+        aca_plan(here / "aca_plan_plate.npz")
+    else:
+        c1_plate(here / "c1_plate.npz")
+        c2_sample(here / "c2_sphere_sample.npz")
+        aca_plan(here / "aca_plan_plate.npz")
     print("wrote", sorted(p.name for p in here.glob("*.npz")))

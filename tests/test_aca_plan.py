@@ -347,3 +347,21 @@ def test_oracle_hmatrix_on_an_efie_matrix():
         assert err < 100 * tol
         ranks[tol] = [b.U.shape[1] for b in lr]
     assert all(a >= b for a, b in zip(ranks[1e-8], ranks[1e-4]))
+
+
+def test_plan_matches_committed_fixture():
+    # tests/golden/aca_plan_plate.npz (written by tests/golden/make_golden.py
+    # from the oracle): the library's plan, bit for bit
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "aca_plan_plate.npz")
+    c = g["centers"]
+    for leaf in (4, 16):
+        tree = build_cluster_tree(c, leaf)
+        np.testing.assert_array_equal(tree.perm - 1, g[f"perm_{leaf}"])
+        nodes = np.array([[n.indices.start - 1, n.indices.stop - 2, n.left - 1, n.right - 1, n.level]
+                          for n in tree.nodes])
+        np.testing.assert_array_equal(nodes, g[f"nodes_{leaf}"])
+        boxes = np.array([np.concatenate([n.bbox_min, n.bbox_max]) for n in tree.nodes])
+        np.testing.assert_array_equal(boxes, g[f"boxes_{leaf}"])
+        tasks = np.array([(r - 1, cc - 1, 1 if k == "lowrank" else 0) for r, cc, k in aca_block_tasks(c, leaf, 1.5)])
+        np.testing.assert_array_equal(tasks, g[f"tasks_{leaf}"])
