@@ -20,7 +20,8 @@ from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixF
                   SurfaceBatch, solve_surfaces,
                   make_sph_grid, phi_cut_grid, compute_farfield, bistatic_rcs, backscatter_rcs,
                   C0_DEFAULT, ETA0_DEFAULT)
-from .aca import (ClusterNode, ClusterTree, build_cluster_tree, aca_block_tasks, cluster_diameter,
+from .aca import (ClusterNode, ClusterTree, build_cluster_tree, cluster_tree_resource_bounds, aca_block_tasks,
+                  cluster_diameter,
                   cluster_distance, is_admissible, is_leaf, leaf_nodes, EFIECache, build_efie_cache,
                   efie_cache_with_prefactor_scale, aca_lowrank, DenseBlock, LowRankBlock, ACAOperator,
                   ACAAdjointOperator, build_aca_operator)
