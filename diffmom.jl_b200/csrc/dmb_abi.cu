@@ -144,6 +144,14 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->gmres_graphs = value != 0;
       return;
     }
+    if (option == DMB_OPT_TRUE_RESIDUAL) {
+      c->true_residual_judge = value != 0;
+      return;
+    }
+    if (option == DMB_OPT_SPIN_LIMIT) {
+      c->spin_limit = value < 0 ? 20000000LL : (long long)value;
+      return;
+    }
     if (option == DMB_OPT_OPERATOR) {
       DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "operator must be 0 (dense Z) or 1 (H-matrix)");
       DMB_REQUIRE(value == 0 ? c->z_valid : c->aca.valid, DMB_ERR_STATE,
@@ -364,6 +372,7 @@ dmb_status dmb_nf_apply(dmb_ctx *c, const double *x, double *y, int64_t nrhs) {
     dmb::pc_apply_dev(c, bx.as<double>(), nrhs);
     DMB_CUDA(cudaMemcpyAsync(y, bx.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     DMB_CUDA(cudaStreamSynchronize(c->stream));
+    DMB_REQUIRE((dmb::read_err_word(c) & 4u) == 0, DMB_ERR_TIMEOUT, "triangular solve wait expired");
   });
 }
 
@@ -792,7 +801,7 @@ dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *
 
 dmb_status dmb_kernel_timing_family(dmb_ctx *c, int family, double *ms, int64_t *launches, double *work) {
   return guarded(c, [&] {
-    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1, 2 or 3");
+    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1, 2, 3 or 4");
     kt_collect(c);
     if (ms) *ms = c->kt_ms[family];
     if (launches) *launches = c->kt_launches[family];

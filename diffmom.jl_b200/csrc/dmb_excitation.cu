@@ -673,20 +673,15 @@ constexpr int64_t kNoAllocMaxTriangles = 32768;
 // complex128 = 3 MiB, held by every GPU that loads the library until exit.
 static __device__ __align__(256) double2 g_mf_noalloc_scratch[2 * 3 * kNoAllocMaxTriangles];
 
-std::mutex g_noalloc_mu;
-double2 *g_noalloc_addr[64] = {};  // device address of the array, per device ordinal
-
 // Host code must not use g_mf_noalloc_scratch directly (its host-side name is a
-// stand-in, not a device address); look the address up once per device.
-double2 *noalloc_scratch(int device) {
-  DMB_REQUIRE(device >= 0 && device < 64, DMB_ERR_ARGUMENT, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void *p = nullptr;
-    DMB_CUDA(cudaGetSymbolAddress(&p, g_mf_noalloc_scratch));
-    g_noalloc_addr[device] = static_cast<double2 *>(p);
-  }
-  return g_noalloc_addr[device];
+// stand-in, not a device address).  The address is looked up on every call,
+// with the context's device current: cudaGetSymbolAddress allocates nothing,
+// and a fresh lookup stays right if the device's context was reset and the
+// module reloaded elsewhere since an earlier call.
+double2 *noalloc_scratch() {
+  void *p = nullptr;
+  DMB_CUDA(cudaGetSymbolAddress(&p, g_mf_noalloc_scratch));
+  return static_cast<double2 *>(p);
 }
 
 }  // namespace
@@ -703,7 +698,7 @@ extern "C" dmb_status dmb_matvec_free_noalloc(dmb_ctx *c, const double *x_dev, d
                 "dmb_matvec_free_noalloc supports at most " + std::to_string(kNoAllocMaxTriangles) +
                     " triangles, mesh has " + std::to_string(c->nt));
     const int64_t N = c->n, nt = c->nt;
-    double2 *xs = noalloc_scratch(c->device);
+    double2 *xs = noalloc_scratch();
     double2 *ys = xs + 3 * kNoAllocMaxTriangles;
     // slots without a basis function are never read, but the input half is
     // cleared so no value of an earlier call can leak into this one

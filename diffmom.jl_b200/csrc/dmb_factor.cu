@@ -571,10 +571,10 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
 // ---------------------------------------------------------------------------
 // wait until flag[cb] is set; return how many consecutive flags from cb on are
 // set (>= 1), or 0 when the wait expired (error bit 4 recorded)
-__device__ int wait_flags(const volatile unsigned *fl, int cb, int limit, unsigned *err) {
+__device__ int wait_flags(const volatile unsigned *fl, int cb, int limit, unsigned *err, long long spin_limit) {
   long long it = 0;
   while (fl[cb] == 0u) {
-    if (++it > SPIN_LIMIT) {
+    if (++it > spin_limit) {
       atomicOr(err, 4u);
       return 0;
     }
@@ -619,7 +619,8 @@ __device__ __forceinline__ double2 gemv64_quad(const FC *__restrict__ M, const d
 // per row, two shuffles each).
 template <class FC>
 __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restrict__ F, const FC *__restrict__ Linv,
-                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err) {
+                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err,
+                                                  long long spin_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FC *Lp = reinterpret_cast<FC *>(smem_raw);
   FC *Li = Lp + NB * NB;
@@ -649,7 +650,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
   for (int i = 0; i < 16; i++) p[i] = make_double2(0, 0);
   int cb = 0;
   while (cb < t - 1) {
-    if (threadIdx.x == 0) s_n = wait_flags(fl, cb, t - 1, err);
+    if (threadIdx.x == 0) s_n = wait_flags(fl, cb, t - 1, err, spin_limit);
     __syncthreads();
     const int n = s_n;
     __syncthreads();
@@ -676,7 +677,7 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
   __syncthreads();
   if (threadIdx.x < NB) acc[threadIdx.x] = csub(acc[threadIdx.x], cadd(part[0][threadIdx.x], part[1][threadIdx.x]));
   if (t > 0) {
-    if (threadIdx.x == 0) s_n = wait_flags(fl, t - 1, t, err);
+    if (threadIdx.x == 0) s_n = wait_flags(fl, t - 1, t, err, spin_limit);
     __syncthreads();
     if (s_n == 0) return;
     __threadfence();
@@ -700,7 +701,8 @@ __global__ void __launch_bounds__(256) k_trsv_fwd(int64_t N, const FC *__restric
 // dependency (block row t+1) and Linv_tt are staged before any wait.
 template <class FC>
 __global__ void __launch_bounds__(256) k_trsv_bwd(int64_t N, const FC *__restrict__ F, const FC *__restrict__ Linv,
-                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err) {
+                                                  double2 *x, unsigned *flags, unsigned *tickets, unsigned *err,
+                                                  long long spin_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FC *Lp = reinterpret_cast<FC *>(smem_raw);
   FC *Li = Lp + NB * NB;
@@ -729,7 +731,7 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int64_t N, const FC *__restric
   double2 s = make_double2(0, 0);
   int q0 = 0;
   while (q0 < tk - 1) {
-    if (threadIdx.x == 0) s_n = wait_flags(fl, q0, tk - 1, err);
+    if (threadIdx.x == 0) s_n = wait_flags(fl, q0, tk - 1, err, spin_limit);
     __syncthreads();
     const int n = s_n;
     __syncthreads();
@@ -745,7 +747,7 @@ __global__ void __launch_bounds__(256) k_trsv_bwd(int64_t N, const FC *__restric
     q0 += n;
   }
   if (tk > 0) {
-    if (threadIdx.x == 0) s_n = wait_flags(fl, tk - 1, tk, err);
+    if (threadIdx.x == 0) s_n = wait_flags(fl, tk - 1, tk, err, spin_limit);
     __syncthreads();
     if (s_n == 0) return;
     __threadfence();
@@ -856,6 +858,10 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     kt_begin(c);
     if (use_tc) {
       dmb::tc_ldlt_update_c64(c, N, r0, c_hi, jcol, K, (float2 *)F, (const float2 *)Wb, NBW, woff, slot);
+    } else if constexpr (std::is_same<C, double2>::value) {
+      // complex128 factor: the FP64-pipe GEMM (128 x 64 tiles, lower triangle)
+      dmb::zgemm64_lower_update(c, rest, c_hi - r0, K, (const double2 *)Wb + r0 * NBW + woff, NBW,
+                                (const double2 *)F + r0 * N + jcol, N, (double2 *)F + r0 * N + r0, N);
     } else {
       dim3 g(blocks_for(rest, 64), blocks_for(c_hi - r0, 64));
       DMB_LAUNCH(c, k_ldlt_update<C>, g, 256, 0, N, r0, c_hi, jcol, K, F, Wb, NBW, woff, 0, (C *)nullptr, err);
@@ -985,10 +991,10 @@ template <class C> void ldlt_solve(dmb_ctx *c, const C *F, double2 *x, int64_t R
   DMB_CUDA(cudaMemsetAsync(err, 0, 4 * (flag_words + 1), c->stream));
   set_smem_attrs<C>();
   const size_t sm = 2 * sizeof(C) * NB * NB;
-  DMB_LAUNCH(c, k_trsv_fwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err);
+  DMB_LAUNCH(c, k_trsv_fwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err, c->spin_limit);
   DMB_LAUNCH(c, k_scale_by_dinv<C>, blocks_for(N * R, 256), 256, 0, N, R, F, x);
   DMB_CUDA(cudaMemsetAsync(tickets, 0, 4 * flag_words, c->stream));
-  DMB_LAUNCH(c, k_trsv_bwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err);
+  DMB_LAUNCH(c, k_trsv_bwd<C>, g, 256, sm, N, F, Linv, x, flags, tickets, err, c->spin_limit);
 }
 
 // ---------------------------------------------------------------------------
@@ -1149,6 +1155,15 @@ template <class C> void trsm_update(dmb_ctx *c, const C *F, int64_t N, int64_t r
   if (std::is_same<C, float2>::value && R >= c->tc_min_rhs && dmb::tc_available(c)) {
     dmb::tc_trsm_update(c, (const float2 *)F, N, r_lo, r_hi, k_lo, w, bwd, X, R);
     return;
+  }
+  if constexpr (std::is_same<C, double2>::value) {
+    if (M >= 128 && R >= 16) {  // complex128 factor: the FP64-pipe GEMM
+      if (bwd)
+        dmb::zgemm64_sub(c, true, M, R, w, F + k_lo * N + r_lo, N, X + k_lo, N, X + r_lo, N);
+      else
+        dmb::zgemm64_sub(c, false, M, R, w, F + r_lo * N + k_lo, N, X + k_lo, N, X + r_lo, N);
+      return;
+    }
   }
   dim3 g(blocks_for(M, 64), blocks_for(R, 64));
   if (bwd)

@@ -92,11 +92,16 @@ __global__ void k_scale_cols(int64_t N, int64_t R, const double *__restrict__ nr
 }
 
 struct SysState {
-  double beta;   // ||r0||
-  double eps;    // stopping threshold
-  double resid;  // |g_{j+1}|
-  int k;         // basis size used (iterations)
-  int done;      // 1 converged, 2 breakdown/zero rhs
+  double beta;     // ||r0||
+  double eps;      // stopping threshold
+  double resid;    // |g_k|: the estimate at the solution's basis size k
+  double resid_x;  // |g_kx|: the estimate with every processed column
+  int k;           // basis size of the solution (iterations)
+  int kx;          // Hessenberg columns processed (>= k: a converged system
+                   // keeps being rotated while others iterate, so it can be
+                   // reactivated without losing its Krylov space)
+  int done;        // 1 converged, 2 breakdown/zero rhs, 3 non-finite
+  int pad;
 };
 
 // start: g = (beta, 0, ...); thresholds
@@ -108,7 +113,10 @@ __global__ void k_init_state(int64_t R, const double *__restrict__ nrm, double t
   s.beta = nrm[r];
   s.eps = tol * nrm[r];
   s.resid = nrm[r];
+  s.resid_x = nrm[r];
   s.k = 0;
+  s.kx = 0;
+  s.pad = 0;
   s.done = nrm[r] == 0.0 ? 2 : 0;
   st[r] = s;
   double2 *gr = g + r * (int64_t)(kcap + 1);
@@ -123,7 +131,7 @@ __global__ void k_givens(int64_t R, int j, int kcap, double2 *__restrict__ H, co
   int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R) return;
   SysState s = st[r];
-  if (s.done) return;
+  if (s.done >= 2) return;
   double2 *Hc = H + r * (int64_t)(kcap + 1) * kcap + (int64_t)j * (kcap + 1);
   double *c = cs + r * (int64_t)kcap;
   double2 *sv = sn + r * (int64_t)kcap;
@@ -157,11 +165,15 @@ __global__ void k_givens(int64_t R, int j, int kcap, double2 *__restrict__ H, co
   double2 gj = gr[j];
   gr[j] = cscale(gj, cc);
   gr[j + 1] = cscale(cmul(cconj(ss), gj), -1.0);
-  s.k = j + 1;
-  s.resid = hypot(gr[j + 1].x, gr[j + 1].y);
-  if (s.resid <= s.eps) s.done = 1;
-  else if (hnext[r] == 0.0) s.done = 2;  // lucky breakdown: exact solution in the space
-  if (!isfinite(s.resid)) s.done = 3;
+  s.kx = j + 1;
+  s.resid_x = hypot(gr[j + 1].x, gr[j + 1].y);
+  if (s.done == 0) {
+    s.k = j + 1;
+    s.resid = s.resid_x;
+    if (s.resid <= s.eps) s.done = 1;
+    else if (hnext[r] == 0.0) s.done = 2;  // lucky breakdown: exact solution in the space
+    if (!isfinite(s.resid)) s.done = 3;
+  }
   st[r] = s;
   if (!s.done) atomicAdd(active, 1u);
 }
@@ -317,6 +329,16 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   int total_iters = 0, restarts = 0, cycles = 0, j_last = 0;
   bool first = true, have_true = false;
   std::vector<SysState> hst(R);
+  // judge passes: per system, the factor by which the next cycle must reduce
+  // its starting (preconditioned, for left) residual; 0 = keep the threshold
+  std::vector<double> judge_scale(R, 0.0);
+  // left preconditioning without an inexact operator: the judge continues the
+  // cycle instead of restarting it
+  const bool left_judge = c->true_residual_judge && precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_LEFT &&
+                          !inexact;
+  int judge_continuations = 0;
+  std::vector<double> hn_final(2 * R);
+  for (int judge_pass = 0;; judge_pass++) {
   while (true) {
     // r0 = b - Z x (x = 0 on the first cycle), preconditioned on the left
     if (first) {
@@ -339,7 +361,13 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       bool any = false;
       for (int64_t r = 0; r < R; r++) {
         hst[r].k = 0;
+        hst[r].kx = 0;
         hst[r].resid = hn[r];
+        hst[r].resid_x = hn[r];
+        if (judge_scale[r] > 0) {
+          hst[r].eps = hn[r] * judge_scale[r];
+          judge_scale[r] = 0;
+        }
         if (inexact && hst[r].done == 1 && !(hn[r] <= hst[r].eps)) hst[r].done = 0;
         if (!hst[r].done) {
           hg[(size_t)r * (kcap + 1)] = make_double2(hn[r], 0);
@@ -442,6 +470,46 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       unsigned h_active = 0;
       DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
       DMB_CUDA(cudaStreamSynchronize(c->stream));
+      // Left preconditioning stops on the preconditioned residual.  With the
+      // judge on, the trial solution of this cycle is checked against the
+      // unpreconditioned FP64 residual; a system that fails it continues the
+      // same Arnoldi process (its Krylov space kept) with its threshold
+      // lowered by the factor the true residual still needs, margin 2.
+      while (h_active == 0 && left_judge) {
+        DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);
+        DMB_CUDA(cudaMemcpyAsync(tmp, x, vec_bytes, cudaMemcpyDeviceToDevice, c->stream));
+        DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, tmp);
+        matvec_dev(c, tmp, w, R);
+        DMB_LAUNCH(c, k_sub, blocks_for(N * R, 256), 256, 0, N * R, b, w);
+        DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, tnrm);
+        DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);
+        std::vector<double> hr(2 * R);
+        DMB_CUDA(cudaMemcpyAsync(hr.data(), nrm + R, 16 * R, cudaMemcpyDeviceToHost, c->stream));
+        DMB_CUDA(cudaMemcpyAsync(hst.data(), st, sizeof(SysState) * R, cudaMemcpyDeviceToHost, c->stream));
+        DMB_CUDA(cudaStreamSynchronize(c->stream));
+        bool changed = false;
+        for (int64_t r = 0; r < R; r++) {
+          const double bn = hr[r], rn = hr[R + r];
+          SysState &sr = hst[r];
+          if (sr.done != 1 || !(bn > 0) || !std::isfinite(rn) || rn <= tol * bn) continue;
+          const double eps_new = sr.resid * std::min(0.5, 0.5 * tol * bn / rn);
+          if (sr.resid_x <= eps_new) {  // the columns processed since already suffice
+            if (sr.kx == sr.k) continue;
+            sr.k = sr.kx;
+            sr.resid = sr.resid_x;
+          } else {
+            sr.done = 0;
+            sr.k = sr.kx;
+            sr.resid = sr.resid_x;
+            h_active++;
+          }
+          sr.eps = eps_new;
+          changed = true;
+        }
+        if (!changed) break;
+        judge_continuations++;
+        DMB_CUDA(cudaMemcpyAsync(st, hst.data(), sizeof(SysState) * R, cudaMemcpyHostToDevice, c->stream));
+      }
       if (h_active == 0) break;
     }
     // solution update from this cycle
@@ -483,9 +551,26 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
     DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, w, tnrm);
   }
   DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);
-  std::vector<double> hn(2 * R);
-  DMB_CUDA(cudaMemcpyAsync(hn.data(), nrm + R, 16 * R, cudaMemcpyDeviceToHost, c->stream));
+  DMB_CUDA(cudaMemcpyAsync(hn_final.data(), nrm + R, 16 * R, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
+  // The judge: a system that stopped on its recurrence estimate (or on the
+  // preconditioned residual, for left preconditioning) with a true residual
+  // above tol is refined by another cycle from its current x; that cycle must
+  // reduce its starting residual by the factor the true residual still needs
+  // (with a margin of 2).
+  if (!c->true_residual_judge || total_iters >= maxiter || judge_pass >= 16) break;
+  bool refine = false;
+  for (int64_t r = 0; r < R; r++) {
+    const double bn = hn_final[r], rn = hn_final[R + r];
+    if (!(bn > 0) || !std::isfinite(rn) || rn <= tol * bn || hst[r].done == 3) continue;
+    hst[r].done = 0;
+    judge_scale[r] = std::min(0.5, 0.5 * tol * bn / rn);
+    refine = true;
+  }
+  if (!refine) break;
+  have_true = false;
+  }  // judge passes
+  const std::vector<double> &hn = hn_final;
   double tres = 0, eres = 0;
   bool solved = true;
   for (int64_t r = 0; r < R; r++) {
@@ -500,12 +585,14 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       eres = std::max(eres, est);
     }
     if (!std::isfinite(rel)) solved = false;
+    if (c->true_residual_judge && !(rel <= tol)) solved = false;
   }
   out->niter = iters_used;
   out->solved = solved ? 1 : 0;
   out->residual = eres;
   out->true_residual = tres;
   out->restarts = restarts;
+  out->reserved = judge_continuations;
   c->tm.solve_ms = now_ms() - t0;
   c->tm.gmres_ms = c->tm.solve_ms;
 }

@@ -232,6 +232,13 @@ struct dmb_ctx {
   // (few right-hand sides); key: iteration range, shape, buffer addresses and
   // the allocation epoch
   bool gmres_graphs = true;
+  // GMRES judges convergence on ||b - Z x|| / ||b|| (FP64-accurate product):
+  // a system whose recurrence estimate met the tolerance but whose true
+  // residual did not is refined by further cycles from its current iterate
+  bool true_residual_judge = true;
+  // polls of a triangular-solve chain wait before it gives up (DMB_ERR_TIMEOUT);
+  // DMB_OPT_SPIN_LIMIT lowers it to exercise the timeout path
+  long long spin_limit = 20000000;
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;
     int64_t kernels = 0;
@@ -263,10 +270,11 @@ struct dmb_ctx {
   int64_t launches = 0;
   bool kt_enabled = false;     // dominant-kernel event timing
   // per family: 0 3xTF32 Krylov / sweep GEMMs, 1 int8 GEMMs, 2 factor updates,
-  // 3 H-matrix products (one right-hand side, work in bytes)
-  static constexpr int KT_FAMILIES = 4;
-  double kt_ms[KT_FAMILIES] = {0, 0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0, 0};
-  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0, 0};
+  // 3 H-matrix products (one right-hand side, work in bytes), 4 FP64-pipe
+  // complex128 Z X and sweep GEMMs
+  static constexpr int KT_FAMILIES = 5;
+  double kt_ms[KT_FAMILIES] = {0, 0, 0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0, 0, 0};
+  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
   std::vector<double> kt_pending;     // algorithmic work of each recorded launch
   std::vector<int> kt_family;         // family of each recorded launch
@@ -332,6 +340,16 @@ void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision);
 void copy_z_out(dmb_ctx *c, double *Z_out);
 void z_entries(dmb_ctx *c, const int64_t *m, const int64_t *n, int64_t count, double *out);
 void apply_impedance(dmb_ctx *c, const double *zs);
+// FP64 complex GEMMs on the FP64 pipe (dmb_zgemm64.cu): Y = Z X (column-major
+// N x R), Y(m, r) -= sum_k A(m, k) B[r ldb + k] (A(m, k) = A[m lda + k], or
+// A[k lda + m] when a_transposed; Y column-major), and the lower-triangle
+// trailing update F[m][j] -= sum_k W[m][k] L[j][k] (row-major, j <= m)
+void zgemm64_zx(dmb_ctx *c, const double2 *Z, const double2 *X, double2 *Y, int64_t N, int64_t R);
+void zgemm64_sub(dmb_ctx *c, bool a_transposed, int64_t M, int64_t R, int64_t K, const double2 *A, int64_t lda,
+                 const double2 *B, int64_t ldb, double2 *Y, int64_t ldy);
+void zgemm64_lower_update(dmb_ctx *c, int64_t M, int64_t C, int64_t K, const double2 *W, int64_t ldw,
+                          const double2 *Lrows, int64_t ldl, double2 *F, int64_t ldf);
+unsigned read_err_word(dmb_ctx *c);  // error word of the triangular solves (bit 2: a wait expired)
 void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs);  // device buffers, c128
 void conj_dev(dmb_ctx *c, double2 *x, int64_t count);
 void nf_build(dmb_ctx *c, double cutoff, int kind);

@@ -397,6 +397,8 @@ void matvec_dev(dmb_ctx *c, const void *x, void *y, int64_t nrhs) {
       DMB_LAUNCH(c, k_gemv<double2>, g, 256, 0, N, c->d_Z.as<double2>(), xd, yd);
     else
       DMB_LAUNCH(c, k_gemv<float2>, g, 256, 0, N, c->d_Z.as<float2>(), xd, yd);
+  } else if (c->z_prec == DMB_PREC_FP64 && nrhs >= 16) {
+    zgemm64_zx(c, c->d_Z.as<double2>(), xd, yd, N, nrhs);
   } else if (nrhs < 32 || c->z_prec == DMB_PREC_FP64) {
     dim3 g(blocks_for(N, 64), blocks_for(nrhs, 64));
     if (c->z_prec == DMB_PREC_FP64)

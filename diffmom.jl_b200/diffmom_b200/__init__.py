@@ -25,6 +25,7 @@ from .aca import (ClusterNode, ClusterTree, build_cluster_tree, cluster_tree_res
                   cluster_distance, is_admissible, is_leaf, leaf_nodes, EFIECache, build_efie_cache,
                   efie_cache_with_prefactor_scale, aca_lowrank, DenseBlock, LowRankBlock, ACAOperator,
                   ACAAdjointOperator, build_aca_operator)
-from ._native import load_library, LIB_PATH, DiffMoMError, NotConvergedError, FactorizationBreakdown
+from ._native import (load_library, LIB_PATH, DiffMoMError, NotConvergedError, FactorizationBreakdown,
+                      DeviceWaitTimeout)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -47,6 +47,8 @@ OPT_EXACT_KRYLOV = 4
 OPT_PRECOND_TF32_TERMS = 5
 OPT_GMRES_GRAPHS = 6
 OPT_OPERATOR = 7
+OPT_TRUE_RESIDUAL = 8
+OPT_SPIN_LIMIT = 9
 
 
 class DiffMoMError(RuntimeError):
@@ -65,6 +67,11 @@ class DimensionMismatch(ValueError):
     pass
 
 
+class DeviceWaitTimeout(DiffMoMError, TimeoutError):
+    """A bounded wait inside a kernel gave up (DMB_ERR_TIMEOUT): the call's
+    results are invalid, the context stays usable."""
+
+
 _EXC = {
     DMB_ERR_ARGUMENT: ValueError,          # ArgumentError
     DMB_ERR_OVERFLOW: OverflowError,       # OverflowError
@@ -74,7 +81,7 @@ _EXC = {
     DMB_ERR_CUDA: DiffMoMError,
     DMB_ERR_STATE: DiffMoMError,
     DMB_ERR_BREAKDOWN: FactorizationBreakdown,
-    DMB_ERR_TIMEOUT: DiffMoMError,
+    DMB_ERR_TIMEOUT: DeviceWaitTimeout,
 }
 
 

@@ -89,10 +89,15 @@ class EFIEDevice:
         "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product,
         "precond_tf32_terms" (3/1) for the TF32 products per complex MAC of the
         complex64 factorisation updates and batched triangular sweeps,
-        "gmres_graphs" (0/1) for CUDA-graph replay of GMRES iterations."""
+        "gmres_graphs" (0/1) for CUDA-graph replay of GMRES iterations,
+        "true_residual" (1 = default: GMRES refines until ||b - Z x|| / ||b||
+        meets the tolerance; 0: it stops where Krylov.gmres stops),
+        "spin_limit" (polls of a chained triangular-sweep wait before the call
+        fails with TimeoutError; negative restores the default)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
-                 "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS}
+                 "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,
+                 "true_residual": nat.OPT_TRUE_RESIDUAL, "spin_limit": nat.OPT_SPIN_LIMIT}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))
@@ -861,6 +866,7 @@ class ScatteringResult:
 
 def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                      dense_direct_limit: int = 2000, dense_gmres_limit: int = 10000,
+                     mlfma_threshold: int = 50000, max_dense_matrix_bytes: int = 2_000_000_000,
                      gmres_tol: float = 1e-6, gmres_maxiter: int = 300,
                      check_gmres_convergence: bool = True, nf_cutoff_lambda: float = 1.0,
                      preconditioner: str = "auto", precond_side: str = "left", quad_order: int = 3,
@@ -871,20 +877,40 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
     """Workflow.jl:67-317 on the GPU.
 
     method: "auto" | "dense_direct" | "dense_gmres" | "aca_gmres".  "auto"
-    picks dense_direct up to dense_direct_limit unknowns and dense_gmres above:
-    the dense matrix of every size the reference sends to ACA (N <= 50,000,
-    40 GB in complex128) fits in one B200's HBM.  "aca_gmres" runs the
-    reference's H-matrix path (build_aca_operator with the aca_* parameters,
-    near-field preconditioner from its dense blocks).  precision "fp64" is the
-    plain path; "mixed" assembles far pairs in FP32 (complex64 Z) and factors
-    the preconditioner in FP32 while GMRES keeps FP64 Arnoldi and residuals
-    (for aca_gmres only the preconditioner is complex64).
+    selects as the reference does (Workflow.jl:147-160): dense_direct up to
+    dense_direct_limit unknowns, dense_gmres up to dense_gmres_limit,
+    aca_gmres up to mlfma_threshold; above it the reference's MLFMA, which
+    this library does not provide (ValueError).  On a B200 the dense methods
+    are faster than the H-matrix at every size the reference sends to ACA
+    (N <= 50,000 fits in HBM): pass method="dense_gmres" (or a larger
+    dense_gmres_limit) to keep them.  The dense methods check the matrix
+    payload (N^2 x 16 bytes in FP64, x 8 in mixed precision) against
+    max_dense_matrix_bytes before assembly, as the reference does
+    (Workflow.jl:169-174).  "aca_gmres" runs the reference's H-matrix path
+    (build_aca_operator with the aca_* parameters, near-field preconditioner
+    from its dense blocks).  precision "fp64" is the plain path; "mixed"
+    assembles far pairs in FP32 (complex64 Z) and factors the preconditioner
+    in FP32 while GMRES keeps FP64 Arnoldi and residuals (for aca_gmres only
+    the preconditioner is complex64).  GMRES judges convergence on the
+    unpreconditioned FP64 residual (refining a left-preconditioned solve until
+    it passes).
     """
     f = float(freq_hz)
     if not (math.isfinite(f) and f > 0):
         raise ValueError(f"solve_scattering: freq_hz must be finite and positive, got {freq_hz}")
     if method not in ("auto", "dense_direct", "dense_gmres", "aca_gmres"):
-        raise ValueError("solve_scattering: method must be :auto, :dense_direct, :dense_gmres, or :aca_gmres")
+        raise ValueError("solve_scattering: method must be :auto, :dense_direct, :dense_gmres, or :aca_gmres "
+                         "(:mlfma is not provided by this library)")
+    if dense_direct_limit < 0:
+        raise ValueError(f"solve_scattering: dense_direct_limit must be nonnegative, got {dense_direct_limit}")
+    if dense_gmres_limit < dense_direct_limit:
+        raise ValueError(f"solve_scattering: dense_gmres_limit ({dense_gmres_limit}) must be at least "
+                         f"dense_direct_limit ({dense_direct_limit})")
+    if mlfma_threshold < dense_gmres_limit:
+        raise ValueError(f"solve_scattering: mlfma_threshold ({mlfma_threshold}) must be at least "
+                         f"dense_gmres_limit ({dense_gmres_limit})")
+    if not (isinstance(max_dense_matrix_bytes, (int, np.integer)) and max_dense_matrix_bytes > 0):
+        raise ValueError(f"max_dense_matrix_bytes must be a positive integer, got {max_dense_matrix_bytes}")
     if preconditioner not in ("auto", "lu", "diag", "none"):
         raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, or :none")
     if method == "aca_gmres" and surface_impedance is not None:
@@ -904,7 +930,24 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
         raise ValueError("solve_scattering: mesh produces no RWG unknowns")
     sel = method
     if method == "auto":
-        sel = "dense_direct" if N <= dense_direct_limit else "dense_gmres"
+        if N <= dense_direct_limit:
+            sel = "dense_direct"
+        elif N <= dense_gmres_limit:
+            sel = "dense_gmres"
+        elif N <= mlfma_threshold:
+            sel = "aca_gmres"
+        else:
+            raise ValueError(f"solve_scattering: N={N} is above mlfma_threshold={mlfma_threshold}; the MLFMA "
+                             "path is not provided by this library (pass method=\"aca_gmres\" or "
+                             "\"dense_gmres\")")
+        if sel == "aca_gmres" and surface_impedance is not None:
+            raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres "
+                             "(auto-selected above dense_gmres_limit; pass method=\"dense_gmres\")")
+    if sel in ("dense_direct", "dense_gmres"):
+        payload = N * N * (16 if precision == "fp64" else 8)
+        if payload > max_dense_matrix_bytes:
+            raise ValueError(f"solve_scattering dense EFIE matrix requires {payload} raw bytes, exceeding "
+                             f"max_dense_matrix_bytes={max_dense_matrix_bytes}")
     dev = device or EFIEDevice(mesh, rwg)
     own = device is None
     try:

@@ -81,6 +81,23 @@ function build_aca_operator_gpu(d::Device, k; leaf_size=64, eta=1.5, aca_tol=1e-
     return reinterpret(Int64, info[1:48]), reinterpret(Float64, info[49:80])
 end
 
+# matrixfree_efie_operator(mesh, rwg, k; ...) then mul!(y, A, x) on the device
+# (entries recomputed on every product; nothing of size N^2 is stored)
+prepare_operator!(d::Device, k; quad_order=3, eta0=376.730313668) = check(d.ptr,
+    ccall((:dmb_prepare_operator, lib), Cint, (Ptr{Cvoid}, Cdouble, Cdouble, Cint), d.ptr, k, eta0, quad_order))
+function matvec_free_gpu!(d::Device, y::Vector{ComplexF64}, x::Vector{ComplexF64})
+    check(d.ptr, ccall((:dmb_matvec_free, lib), Cint, (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{ComplexF64}),
+                       d.ptr, x, y))
+    return y
+end
+# The same product for callers that must not allocate device memory once set
+# up (a CuArray pool that owns the device memory, a fixed budget): x and y are
+# device vectors, e.g. pointer(x::CuVector{ComplexF64}); at most 32,768
+# triangles; calls on one device must not overlap.
+matvec_free_noalloc!(d::Device, y_dev::Ptr{ComplexF64}, x_dev::Ptr{ComplexF64}) = check(d.ptr,
+    ccall((:dmb_matvec_free_noalloc, lib), Cint, (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{ComplexF64}),
+          d.ptr, x_dev, y_dev))
+
 # build_nearfield_preconditioner(A_aca; factorization) from the H-matrix's dense blocks
 aca_nf_build!(d::Device; factorization=:lu, precision=:fp64) = check(d.ptr,
     ccall((:dmb_aca_nf_build, lib), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}),

@@ -63,8 +63,9 @@ typedef struct {
   int32_t solved;       /* 1 when every right-hand side met the tolerance */
   double residual;      /* last residual estimate (max over RHS), relative */
   double true_residual; /* ||b - Z x|| / ||b|| in FP64 (max over RHS) */
-  int32_t restarts;
-  int32_t reserved;
+  int32_t restarts;     /* restart / refinement cycles */
+  int32_t reserved;     /* times the true-residual judge continued a left-
+                           preconditioned cycle (DMB_OPT_TRUE_RESIDUAL) */
 } dmb_gmres_stats;
 
 typedef struct {
@@ -124,6 +125,24 @@ const char *dmb_version(void);
  * 0 the assembled dense Z, 1 the H-matrix of dmb_aca_build (each build or
  * assembly selects its own; switching drops the preconditioner). */
 #define DMB_OPT_OPERATOR 7
+/* DMB_OPT_TRUE_RESIDUAL: 1 (default) makes the unpreconditioned FP64 residual
+ * ||b - Z x|| / ||b|| the judge of dmb_gmres / dmb_gmres_adjoint and the
+ * resident solves.  For left preconditioning (Krylov.gmres stops on the
+ * preconditioned residual, IterativeSolve.jl:364-384) the trial solution is
+ * checked when a system's estimate meets the tolerance, and a system whose
+ * true residual does not continues the same Arnoldi process with a lower
+ * threshold; a system that still misses it after its cycle (basis capacity,
+ * inexact operator) is refined by further cycles from its current iterate.
+ * All within maxiter; a system counts as solved only once its true residual
+ * meets the tolerance.  0 stops exactly where Krylov.gmres stops (iteration
+ * counts of the reference). */
+#define DMB_OPT_TRUE_RESIDUAL 8
+/* DMB_OPT_SPIN_LIMIT: polls a waiting CTA of the chained triangular sweeps
+ * (complex128 factors, and 2-7 right-hand sides of complex64 ones) makes
+ * before it gives up; the call then fails with DMB_ERR_TIMEOUT and the context
+ * stays usable.  A negative value restores the default (2e7 polls, seconds);
+ * small values exercise the timeout path without any GPU fault. */
+#define DMB_OPT_SPIN_LIMIT 9
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair tile rows used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
@@ -167,6 +186,8 @@ dmb_status dmb_matvec(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
  * entries are recomputed from the geometry on every call, nothing of size
  * N^2 is stored.  Requires a prior dmb_assemble_z or dmb_prepare_operator. */
 dmb_status dmb_prepare_operator(dmb_ctx *ctx, double k, double eta0, int quad_order);
+/* The near-field entries are added with atomics, so repeated products agree
+ * to rounding (about 1e-15 relative), not bit for bit. */
 dmb_status dmb_matvec_free(dmb_ctx *ctx, const double *x, double *y);
 /* No counterpart in the reference.  The same matrix-free product for callers
  * that cannot allocate device memory mid-run (device memory owned by an
@@ -174,9 +195,12 @@ dmb_status dmb_matvec_free(dmb_ctx *ctx, const double *x, double *y);
  * x_dev and y_dev are DEVICE pointers to N complex128 values, and the call
  * allocates nothing -- its slot-space scratch is a static device array of
  * 3 MiB held by every GPU that loads the library until exit.  Meshes with more
- * than 32,768 triangles are rejected with DMB_ERR_BUDGET.  The first call on
- * a device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array and
+ * than 32,768 triangles are rejected with DMB_ERR_BUDGET.  Every call looks up
+ * that array's device address (cudaGetSymbolAddress, which allocates nothing)
+ * with the context's device current; the first lookup on a device may load
+ * the module, so make the first call before any stream capture.  Not for use
+ * across a reset of the device (cudaDeviceReset) by another part of the
+ * process while a call is running.  All calls share the array and
  * it keeps the last call's contents, so calls that overlap on the GPU (other
  * contexts or threads on the same device at the same time) race.  Requires a
  * prior dmb_prepare_operator (or dmb_assemble_z) on the context. */
@@ -357,7 +381,10 @@ dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double
  * trailing updates (3xTF32 tensor cores for complex64 factors; complex flops),
  * 3 = H-matrix products of dmb_aca_build's operator (one bracket per
  * right-hand side: gather, low-rank inner products, leaf sums; work in bytes:
- * the stored blocks plus x and y once).  dmb_kernel_timing reports family 0. */
+ * the stored blocks plus x and y once), 4 = FP64-pipe complex128 GEMMs (Z X
+ * of a complex128 Z with >= 16 right-hand sides and the many-column sweep
+ * updates of a complex128 factor; complex flops).  dmb_kernel_timing reports
+ * family 0. */
 dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
 
 /* ---- H-matrix operator (adaptive cross approximation) ------------------ */

@@ -192,25 +192,28 @@ def test_forward_and_adjoint_solves():
     dev.close()
     P = build_nearfield_preconditioner(A, factorization="lu")
     assert 0 < P.nnz_ratio < 1
-    I, st = solve_gmres(A, v, preconditioner=P, tol=1e-8, maxiter=300)
+    # with these small leaves the near-field preconditioner is weak: Krylov.gmres
+    # semantics stop after ~290 iterations at a preconditioned residual of 1e-8
+    # (true residual ~1e-7); the FP64 true-residual judge continues to ~310
+    I, st = solve_gmres(A, v, preconditioner=P, tol=1e-8, maxiter=400)
+    assert st.true_residual <= 1e-8
     I_ref = np.linalg.solve(Z, v)
     err = np.linalg.norm(I - I_ref) / np.linalg.norm(I_ref)
     rng = np.random.default_rng(5)
     rhs_adj = (rng.standard_normal(A.N) + 1j * rng.standard_normal(A.N)) * np.abs(I)
-    lam, st_a = solve_gmres_adjoint(A, rhs_adj, preconditioner=P, tol=1e-8, maxiter=300)
+    lam, st_a = solve_gmres_adjoint(A, rhs_adj, preconditioner=P, tol=1e-8, maxiter=400)
     lam_ref = np.linalg.solve(Z.conj().T, rhs_adj)
     err_a = np.linalg.norm(lam - lam_ref) / np.linalg.norm(lam_ref)
-    # residual of the adjoint system on A^H itself (left preconditioning: the
-    # 1e-8 tolerance holds for the preconditioned residual)
+    # residual of the adjoint system on A^H itself: the judge holds it to 1e-8
     res_a = np.linalg.norm(A.matvec(lam, 1) - rhs_adj) / np.linalg.norm(rhs_adj)
     print(f"forward: {st.niter} iterations, error vs direct {err:.2e}; adjoint: {st_a.niter} iterations, "
           f"error {err_a:.2e}, ||A^H lam - b|| / ||b|| {res_a:.2e}")
-    assert err < 1e-4 and err_a < 1e-3 and res_a <= 1e-6
+    assert err < 1e-4 and err_a < 1e-3 and res_a <= 1.0001e-8
     assert abs(res_a - st_a.true_residual) <= 1e-2 * res_a + 1e-12
     # Jacobi and complex64 near-field factors also converge
     for fac, prec in (("diag", "fp64"), ("lu", "mixed")):
         Pk = build_nearfield_preconditioner(A, factorization=fac, precision=prec)
-        I2, st2 = solve_gmres(A, v, preconditioner=Pk, tol=1e-8, maxiter=300)
+        I2, st2 = solve_gmres(A, v, preconditioner=Pk, tol=1e-8, maxiter=800)
         assert np.linalg.norm(I2 - I_ref) / np.linalg.norm(I_ref) < 1e-4
     A.close()
 

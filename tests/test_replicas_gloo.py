@@ -1,5 +1,7 @@
-"""The replica plumbing of the bench (barrier, max over ranks, whole-job
-rate) with world_size 2 on the gloo backend, CPU only."""
+"""The multi-GPU plumbing of the bench with world_size 2 on the gloo backend,
+CPU only: barrier, max over ranks, whole-job rate, the partition of an
+incidence sweep into disjoint shares and the gather of the per-incidence
+results to rank 0."""
 import json
 import os
 import socket
@@ -24,9 +26,15 @@ def _worker(rank, ws, port, out):
     ms = 100.0 + 50.0 * rank          # rank 1 is the slower replica
     mx = replicas.max_over_ranks(ms)
     rate = replicas.aggregate_rate(1024, mx)
+    # a sweep of 7 incidences: rank 0 takes 4, rank 1 takes 3; each "solves"
+    # its share (sigma = incidence index + 0.5) and rank 0 gathers them all
+    start, count = replicas.shard(7, ws, rank)
+    sig = [i + 0.5 for i in range(start, start + count)]
+    got = replicas.gather_to_rank0(sig)
     replicas.barrier()
     with open(f"{out}.{rank}", "w") as f:
-        json.dump({"ws": replicas.replica_env()[0], "max": mx, "rate": rate}, f)
+        json.dump({"ws": replicas.replica_env()[0], "max": mx, "rate": rate, "share": [start, count],
+                   "gathered": None if got is None else got.tolist()}, f)
     replicas.finalize()
 
 
@@ -40,6 +48,23 @@ def test_two_replicas_on_gloo(tmp_path):
         assert r["ws"] == 2
         assert r["max"] == 150.0                       # both ranks see the slower one
         assert r["rate"] == pytest.approx(2 * 1024 / 0.150)
+    assert res[0]["share"] == [0, 4] and res[1]["share"] == [4, 3]
+    assert res[0]["gathered"] == [i + 0.5 for i in range(7)]   # every incidence once, in order
+    assert res[1]["gathered"] is None
+
+
+def test_shard_partitions_every_unit_once():
+    from diffmom_b200 import replicas
+    for total in (0, 1, 7, 1024, 2048 + 3):
+        for ws in (1, 2, 3, 8):
+            seen = []
+            for r in range(ws):
+                a, n = replicas.shard(total, ws, r)
+                seen.extend(range(a, a + n))
+                assert n in (total // ws, total // ws + 1)
+            assert seen == list(range(total))
+    with pytest.raises(ValueError):
+        replicas.shard(4, 2, 2)
 
 
 def test_single_process_is_a_no_op(monkeypatch):
@@ -50,4 +75,5 @@ def test_single_process_is_a_no_op(monkeypatch):
     replicas.barrier()
     assert replicas.max_over_ranks(3.5) == 3.5
     assert replicas.aggregate_rate(10, 1000.0) == 10.0
+    assert list(replicas.gather_to_rank0([1.0, 2.0])) == [1.0, 2.0]
     replicas.finalize()

@@ -46,6 +46,22 @@ def test_noalloc_matches_allocating_entry_point_two_calls():
         assert np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref) < TOL
 
 
+def test_noalloc_at_the_maximum_mesh_size():
+    # exactly 32,768 triangles (128 x 128 plate): the output half starts at
+    # slot 3 x 32,768 and the last slots of both halves are used
+    m = make_rect_plate(1.0, 1.0, 128, 128)
+    assert m.ntriangles == 32768
+    r = build_rwg(m)
+    op = matrixfree_efie_operator(m, r, 2 * math.pi)
+    rng = np.random.default_rng(12)
+    for _ in range(2):
+        x = rng.standard_normal(r.nedges) + 1j * rng.standard_normal(r.nedges)
+        y_ref = op @ x
+        y = _noalloc(op, x)
+        assert np.all(np.isfinite(y))
+        assert np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref) < TOL
+
+
 def test_noalloc_rejects_meshes_above_the_maximum():
     m = make_rect_plate(1.0, 1.0, 130, 130)  # 33,800 triangles > 32,768
     r = build_rwg(m)
