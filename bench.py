@@ -200,7 +200,8 @@ class Runner:
         if clk:
             res["clocks"] = clk.stop()
         if kernel_timing:
-            for fam, key in ((0, "kernel_gemm"), (1, "kernel_int8"), (2, "kernel_factor"), (4, "kernel_fp64")):
+            for fam, key in ((0, "kernel_gemm"), (1, "kernel_int8"), (2, "kernel_factor"), (4, "kernel_fp64"),
+                             (5, "kernel_assembly")):
                 kms, kl, kf = ct.c_double(), ct.c_int64(), ct.c_double()
                 dev.ctx.call("dmb_kernel_timing_family", fam, ct.byref(kms), ct.byref(kl), ct.byref(kf))
                 res[key] = (kms.value, kl.value, kf.value)
@@ -477,7 +478,11 @@ def run_ours(args):
             variants[name] = {"ms_per_step": ms, "solves_per_s": ws * 64 / (ms / 1e3), "steps": reps,
                               "warmup": 1 if prec == "fp64" else args.warmup, "launches": None, "lanes": lanes,
                               "last": (int(last.gmres_iters.max()), float(last.true_residual.max())),
-                              "buckets": buckets, "sum_N2": float(np.sum(last.N.astype(float) ** 2))}
+                              "buckets": buckets, "sum_N2": float(np.sum(last.N.astype(float) ** 2)),
+                              "assembly_ms_all_surfaces": float(last.assembly_ms),
+                              "assembly": "every surface's Z by one far-pair tile launch (task list of all "
+                                          "surfaces' RWG tile pairs, largest first) + one near-values and one "
+                                          "near-sums launch"}
 
     # ---- C2 sphere, one incidence -----------------------------------------
     if not args.quick and (want("c2_fp64_nf_lu") or want("c2_mixed_nf_lu")):
@@ -657,8 +662,29 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                                 "launches_timed": f[1], "kernel_ms_total": f[0],
                                 "kernel_share_of_step": f[0] / (head["ms_per_step"] * head["steps"])}
                          for name, f in fams.items()}}
+        line["roofline_assembly"] = assembly_roofline(head, full, hbm, N)
         line["clocks"] = head.get("clocks")
     return line
+
+
+def assembly_roofline(head, full, hbm, N):
+    """The far-pair tile kernel of the assembly (k_far_tile): the bytes of Z it
+    writes (16 N^2 complex128, 8 N^2 complex64 -- it reads only L2-resident
+    triangle panels) per event-timed launch, against the measured copy
+    bandwidth; the FP32 / FP64 pipe figures come from the ncu capture."""
+    out = {"kernel": "k_far_tile (far triangle pairs written straight into Z by RWG tiles)", "bound": "fp64/fp32 pipe",
+           "unit": "GB/s", "peak_hbm": hbm, "note": "algorithmic bytes: Z written once (16 N^2 B complex128, "
+           "8 N^2 B complex64); the kernel is bound by the FP32 / FP64 pipes, not by HBM"}
+    for key, v, esz in (("mixed_c64", head, 8.0), ("fp64_c128", full, 16.0)):
+        if not v or "kernel_assembly" not in v:
+            continue
+        ms, launches, work = v["kernel_assembly"]
+        if launches > 0 and ms > 0:
+            per = ms / launches
+            out[key] = {"launches_timed": launches, "ms_per_launch": per,
+                        "achieved_gbs": (esz * N * N / 1e9) / (per / 1e3),
+                        "frac_hbm": (esz * N * N / 1e9) / (per / 1e3) / hbm if hbm else None}
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <thread>
+#include <functional>
 
 #include "dmb_device.cuh"
 #include "dmb_internal.h"
@@ -77,7 +78,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
                       &c->d_tminus, &c->d_vpo, &c->d_vmo, &c->d_len, &c->d_ap, &c->d_am,
                       &c->d_slot_rwg, &c->d_slot_side, &c->d_wq, &c->d_centers, &c->d_adj_off,
                       &c->d_adj_nb, &c->d_near_rec, &c->d_near_val, &c->d_near_entry_mn,
-                      &c->d_near_entry_off, &c->d_Z, &c->d_S, &c->d_F, &c->d_dinv, &c->d_W,
+                      &c->d_near_entry_off, &c->d_Z, &c->d_F, &c->d_dinv, &c->d_W,
                       &c->d_flags, &c->d_li_idx, &c->d_li_cnt, &c->d_li_inv, &c->d_net, &c->d_V,
                       &c->d_H, &c->d_work, &c->d_vecs, &c->d_scal};
     for (DevBuf *b : bufs) b->release();
@@ -96,6 +97,7 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
     dmb::tc_release(c);
     dmb::oz_release(c);
     dmb::local_release(c);
+    dmb::far_release(c);
     for (auto &e : c->kt_pool) cudaEventDestroy(e);
     if (c->stream2) cudaStreamDestroy(c->stream2);
     for (auto &kv : c->gm_graphs)
@@ -135,8 +137,8 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       return;
     }
     if (option == DMB_OPT_FAR_TILE) {
-      DMB_REQUIRE(value == 0 || value == 8 || value == 16 || value == 32, DMB_ERR_ARGUMENT,
-                  "far tile rows must be 0 (autotune), 8, 16 or 32");
+      DMB_REQUIRE(value == 0 || value == 16 || value == 32 || value == 64, DMB_ERR_ARGUMENT,
+                  "far tile width must be 0 (autotune), 16, 32 or 64");
       c->far_tile = value;
       return;
     }
@@ -150,6 +152,11 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
     }
     if (option == DMB_OPT_SPIN_LIMIT) {
       c->spin_limit = value < 0 ? 20000000LL : (long long)value;
+      return;
+    }
+    if (option == DMB_OPT_TUNE_TC_GEMM || option == DMB_OPT_TUNE_TC_SYRK) {
+      DMB_REQUIRE(value >= 0 && value <= 2, DMB_ERR_ARGUMENT, "autotuner pin must be 0 (tuned), 1 or 2");
+      c->tune_pin[option == DMB_OPT_TUNE_TC_GEMM ? dmb::TUNE_TC_GEMM_BN : dmb::TUNE_TC_SYRK_STAGES] = value;
       return;
     }
     if (option == DMB_OPT_OPERATOR) {
@@ -175,11 +182,27 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
   });
 }
 
-dmb_status dmb_get_far_tile(dmb_ctx *c, int *rows_out) {
+dmb_status dmb_get_far_tile(dmb_ctx *c, int *width_out) {
   return guarded(c, [&] {
-    DMB_REQUIRE(rows_out, DMB_ERR_ARGUMENT, "output is NULL");
-    *rows_out = c->far_tile_used;
+    DMB_REQUIRE(width_out, DMB_ERR_ARGUMENT, "output is NULL");
+    *width_out = c->far_tile_used;
   });
+}
+
+dmb_status dmb_tune_report(char *buf, size_t cap, size_t *len_out) {
+  try {
+    const std::string r = dmb::tune_report();
+    if (len_out) *len_out = r.size();
+    if (buf && cap > 0) {
+      const size_t n = std::min(cap - 1, r.size());
+      std::memcpy(buf, r.data(), n);
+      buf[n] = 0;
+    }
+    return DMB_OK;
+  } catch (const DmbError &e) {
+    dmb_free_error() = e.msg;
+    return (dmb_status)e.code;
+  }
 }
 
 dmb_status dmb_mesh_upload(dmb_ctx *c, const double *xyz, const int64_t *tri, int64_t nv, int64_t nt) {
@@ -801,7 +824,7 @@ dmb_status dmb_kernel_timing(dmb_ctx *c, double *ms, int64_t *launches, double *
 
 dmb_status dmb_kernel_timing_family(dmb_ctx *c, int family, double *ms, int64_t *launches, double *work) {
   return guarded(c, [&] {
-    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0, 1, 2, 3 or 4");
+    DMB_REQUIRE(family >= 0 && family < dmb_ctx::KT_FAMILIES, DMB_ERR_ARGUMENT, "kernel family must be 0 to 5");
     kt_collect(c);
     if (ms) *ms = c->kt_ms[family];
     if (launches) *launches = c->kt_launches[family];
@@ -829,29 +852,31 @@ dmb_status dmb_farfield(dmb_ctx *c, const double *rhat, int64_t NO, double k, do
 }
 
 // ---- batches of independent surfaces -----------------------------------
+// One context per surface of a call (kept and reused by later calls: their
+// buffers only grow), so every surface's Z can be assembled by the same
+// launches; `lanes` host threads then run the per-surface stages.
 struct dmb_batch {
   int device = 0;
-  std::vector<dmb_ctx *> lanes;
+  int lanes = 1;
+  std::vector<dmb_ctx *> slots;
+  dmb::BatchAsmBufs asm_bufs;
+  cudaStream_t stream = nullptr;  // the batch-wide launches
+  double last_assembly_ms = 0;
   std::string err;
 };
 
 dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out) {
   if (!out || lanes < 1 || lanes > 64) return DMB_ERR_ARGUMENT;
   *out = nullptr;
+  if (cudaSetDevice(device) != cudaSuccess) return DMB_ERR_CUDA;
   auto *b = new dmb_batch();
   b->device = device;
-  for (int i = 0; i < lanes; i++) {
-    dmb_ctx *c = nullptr;
-    dmb_status st = dmb_ctx_create(device, &c);
-    if (st != DMB_OK) {
-      for (dmb_ctx *l : b->lanes) dmb_ctx_destroy(l);
-      delete b;
-      return st;
-    }
-    // lanes take surfaces of changing sizes (buffers regrow, so captured
-    // GMRES graphs would rarely be replayed): direct launches
-    c->gmres_graphs = false;
-    b->lanes.push_back(c);
+  b->lanes = lanes;
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&b->stream, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+    delete b;
+    return DMB_ERR_CUDA;
   }
   *out = b;
   return DMB_OK;
@@ -859,31 +884,42 @@ dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out) {
 
 dmb_status dmb_batch_destroy(dmb_batch *b) {
   if (!b) return DMB_OK;
-  for (dmb_ctx *c : b->lanes) dmb_ctx_destroy(c);
+  cudaSetDevice(b->device);
+  for (dmb_ctx *c : b->slots) dmb_ctx_destroy(c);
+  b->asm_bufs.far_jobs.release();
+  b->asm_bufs.far_tasks.release();
+  b->asm_bufs.far_err.release();
+  b->asm_bufs.near_jobs.release();
+  if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return DMB_OK;
 }
 
 const char *dmb_batch_last_error(const dmb_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
+dmb_status dmb_batch_assembly_ms(const dmb_batch *b, double *ms_out) {
+  if (!b || !ms_out) return DMB_ERR_ARGUMENT;
+  *ms_out = b->last_assembly_ms;
+  return DMB_OK;
+}
+
 namespace {
-// one surface on one lane: upload, assemble (+ impedance), preconditioner,
-// RHS, GMRES, monostatic sigma; device times from events on the lane stream
-dmb_status batch_item(dmb_ctx *c, const dmb_solve_params *p, dmb_batch_item &it, cudaEvent_t ev_start) {
-  dmb_status st = dmb_mesh_upload(c, it.xyz, it.tri, it.nv, it.nt);
-  if (st == DMB_OK)
-    st = dmb_rwg_upload(c, it.n, it.tplus, it.tminus, it.evert, it.vplus_opp, it.vminus_opp, it.len,
-                        it.area_plus, it.area_minus);
-  if (st != DMB_OK) return st;
+// the stages of one surface after the batch-wide assembly: impedance
+// loading, preconditioner, RHS, GMRES, monostatic sigma; device times from
+// events on the surface's stream (started after the assembly)
+dmb_status batch_item(dmb_ctx *c, const dmb_solve_params *p, dmb_batch_item &it, cudaEvent_t ev_start,
+                      cudaEvent_t ev_asm) {
   return guarded(c, [&] {
-    check_finite(it.kvec, 3, "plane-wave k_vec");
-    check_finite(it.pol, 3, "plane-wave polarization");
-    DMB_REQUIRE(std::isfinite(it.E0) && it.E0 != 0.0, DMB_ERR_ARGUMENT, "plane-wave E0 must be finite, nonzero");
     cudaEvent_t e0, e1;
     DMB_CUDA(cudaEventCreate(&e0));
     DMB_CUDA(cudaEventCreate(&e1));
+    DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_asm, 0));
     DMB_CUDA(cudaEventRecord(e0, c->stream));
-    resident_setup(c, p, it.zs);
+    if (it.zs) {
+      check_finite(it.zs, 2 * c->nt, "surface impedance");
+      dmb::apply_impedance(c, it.zs);
+    }
+    resident_precond(c, p);
     const size_t bytes = sizeof(double2) * c->n;
     c->d_rhs.ensure(bytes);
     c->d_sol.ensure(bytes);
@@ -912,6 +948,39 @@ dmb_status batch_item(dmb_ctx *c, const dmb_solve_params *p, dmb_batch_item &it,
     resident_check(gs);
   });
 }
+
+// run fn(i) for i in [0, count) on `lanes` host threads (items in the given
+// order); the first failure stops the others and is reported
+dmb_status lanes_run(dmb_batch *b, int64_t count, const std::vector<int64_t> &order,
+                     const std::function<dmb_status(int64_t)> &fn) {
+  std::atomic<int64_t> next{0};
+  std::atomic<int> failed{0};
+  std::mutex emu;
+  dmb_status first_code = DMB_OK;
+  std::vector<std::thread> workers;
+  const int L = (int)std::min<int64_t>(b->lanes, count);
+  for (int l = 0; l < L; l++) {
+    workers.emplace_back([&] {
+      cudaSetDevice(b->device);
+      while (!failed.load()) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= count) break;
+        const int64_t s = order[i];
+        const dmb_status st = fn(s);
+        if (st != DMB_OK) {
+          std::lock_guard<std::mutex> lk(emu);
+          if (first_code == DMB_OK) {
+            first_code = st;
+            b->err = "surface " + std::to_string(s) + ": " + b->slots[s]->err;
+          }
+          failed.store(1);
+        }
+      }
+    });
+  }
+  for (auto &w : workers) w.join();
+  return first_code;
+}
 }  // namespace
 
 dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_item *items, int64_t count,
@@ -926,53 +995,66 @@ dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_it
   if (!(std::isfinite(p->tol) && p->tol > 0) || p->maxiter < 1)
     return fail(DMB_ERR_ARGUMENT, "GMRES tol must be finite and positive and maxiter >= 1");
   if (cudaSetDevice(b->device) != cudaSuccess) return fail(DMB_ERR_CUDA, "cudaSetDevice failed");
+  while ((int64_t)b->slots.size() < count) {
+    dmb_ctx *c = nullptr;
+    const dmb_status st = dmb_ctx_create(b->device, &c);
+    if (st != DMB_OK) return fail(st, "could not create a surface context");
+    // surfaces of changing sizes regrow buffers, so captured GMRES graphs
+    // would rarely be replayed: direct launches
+    c->gmres_graphs = false;
+    b->slots.push_back(c);
+  }
+  for (int64_t i = 0; i < count; i++) {
+    const dmb_batch_item &it = items[i];
+    for (const double *v : {it.kvec, it.pol})
+      for (int d = 0; d < 3; d++)
+        if (!std::isfinite(v[d])) return fail(DMB_ERR_ARGUMENT, "surface " + std::to_string(i) + ": plane-wave "
+                                                                  "k_vec and polarization must be finite");
+    if (!(std::isfinite(items[i].E0) && items[i].E0 != 0.0))
+      return fail(DMB_ERR_ARGUMENT, "surface " + std::to_string(i) + ": plane-wave E0 must be finite, nonzero");
+  }
   std::vector<int64_t> order(count);
   for (int64_t i = 0; i < count; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t c2) { return items[a].n > items[c2].n; });
-  const int L = (int)b->lanes.size();
-  cudaEvent_t ev_start;
-  std::vector<cudaEvent_t> ev_end(L);
-  if (cudaEventCreate(&ev_start) != cudaSuccess) return fail(DMB_ERR_CUDA, "cudaEventCreate failed");
-  for (auto &e : ev_end) cudaEventCreate(&e);
-  cudaEventRecord(ev_start, b->lanes[0]->stream);
-  std::atomic<int64_t> next{0};
-  std::atomic<int> failed{0};
-  std::mutex emu;
-  dmb_status first_code = DMB_OK;
-  std::vector<std::thread> workers;
-  for (int l = 0; l < L; l++) {
-    workers.emplace_back([&, l] {
-      cudaSetDevice(b->device);
-      dmb_ctx *c = b->lanes[l];
-      cudaStreamWaitEvent(c->stream, ev_start, 0);
-      while (!failed.load()) {
-        const int64_t i = next.fetch_add(1);
-        if (i >= count) break;
-        dmb_batch_item &it = items[order[i]];
-        const dmb_status st = batch_item(c, p, it, ev_start);  // each call takes the lane's mutex
-        if (st != DMB_OK) {
-          std::lock_guard<std::mutex> lk(emu);
-          if (first_code == DMB_OK) {
-            first_code = st;
-            b->err = "surface " + std::to_string(order[i]) + ": " + c->err;
-          }
-          failed.store(1);
-        }
-      }
-      cudaEventRecord(ev_end[l], c->stream);
-    });
+  // 1. uploads and host topology, lanes in parallel
+  dmb_status st = lanes_run(b, count, order, [&](int64_t s) {
+    dmb_ctx *c = b->slots[s];
+    const dmb_batch_item &it = items[s];
+    dmb_status r = dmb_mesh_upload(c, it.xyz, it.tri, it.nv, it.nt);
+    if (r == DMB_OK)
+      r = dmb_rwg_upload(c, it.n, it.tplus, it.tminus, it.evert, it.vplus_opp, it.vminus_opp, it.len,
+                         it.area_plus, it.area_minus);
+    return r;
+  });
+  if (st != DMB_OK) return st;
+  // 2. every surface's impedance matrix: the far tiles of all surfaces in one
+  // launch, their near values and near sums in one launch each
+  cudaEvent_t ev_start = nullptr, ev_asm = nullptr;
+  cudaEventCreate(&ev_start);
+  cudaEventCreate(&ev_asm);
+  std::vector<dmb_ctx *> cs(b->slots.begin(), b->slots.begin() + count);
+  {
+    dmb_ctx *c0 = cs[0];
+    std::lock_guard<std::mutex> lk(c0->mu);
+    try {
+      StreamSwap sw(c0, b->stream);
+      DMB_CUDA(cudaEventRecord(ev_start, b->stream));
+      b->last_assembly_ms = dmb::assemble_batch(cs, p->k, p->eta0, p->quad_order, p->precision, b->asm_bufs);
+      DMB_CUDA(cudaEventRecord(ev_asm, b->stream));
+    } catch (const DmbError &e) {
+      cudaEventDestroy(ev_start);
+      cudaEventDestroy(ev_asm);
+      return fail((dmb_status)e.code, "batched assembly: " + e.msg);
+    }
   }
-  for (auto &w : workers) w.join();
+  // 3. the per-surface stages, largest surface first
+  st = lanes_run(b, count, order, [&](int64_t s) { return batch_item(b->slots[s], p, items[s], ev_start, ev_asm); });
   double total = 0;
-  for (int l = 0; l < L; l++) {
-    cudaEventSynchronize(ev_end[l]);
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, ev_start, ev_end[l]) == cudaSuccess) total = std::max(total, (double)ms);
-  }
+  for (int64_t i = 0; i < count; i++) total = std::max(total, items[i].latency_ms);
   cudaEventDestroy(ev_start);
-  for (auto &e : ev_end) cudaEventDestroy(e);
+  cudaEventDestroy(ev_asm);
   if (device_ms_out) *device_ms_out = total;
-  return first_code;
+  return st;
 }
 
 }  // extern "C"

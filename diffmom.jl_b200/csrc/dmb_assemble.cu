@@ -2,14 +2,12 @@
 //
 // Reference path: assemble_Z_efie (src/assembly/EFIE.jl:699-753) evaluates
 // every RWG pair (m <= n) as a sum over its 2x2 triangle pairs
-// (_efie_entry, EFIE.jl:439-512).  Here the work is reorganised around
-// TRIANGLE pairs, the minimal formulation:
+// (_efie_entry, EFIE.jl:439-512).  Here:
 //
-//   far pairs   (not self, not edge-adjacent): one thread per unordered pair
-//               (ta <= tb) forms 8 complex quadrature moments of G and
-//               contracts them into the 3x3 block of its basis slots; the
-//               block lands in the triangle-slot matrix S (3Nt x 3Nt).
-//   gather      Z[m][n] = -i*omega*mu0 * sum over the 4 slot pairs of (m, n).
+//   far pairs   (not self, not edge-adjacent): dmb_fartile.cu, one CTA per
+//               tile of RWG pairs, triangle panels staged in shared memory,
+//               Z entries written directly (the four triangle pairs of an
+//               entry summed in a fixed order).
 //   near pairs  self (EFIE.jl:534-606) and edge-adjacent (EFIE.jl:611-684)
 //               terms are evaluated per (pair, test slot, source slot) record
 //               with the reference's canonical rule (the lower RWG index is
@@ -210,208 +208,6 @@ __global__ void k_rwg_centers(int n, const TriCache *__restrict__ tc, const int 
   }
 }
 
-__device__ __forceinline__ bool tri_adjacent(const int *__restrict__ off, const int *__restrict__ nb,
-                                             int ta, int tb) {
-  for (int i = off[ta]; i < off[ta + 1]; i++)
-    if (nb[i] == tb) return true;
-  return false;
-}
-
-// ---------------------------------------------------------------------------
-// K2: far triangle pairs.  Moments over the Nq x Nq product rule, local
-// (centroid-relative) coordinates for the bilinear basis factors:
-//   M0  = sum W G,  Ma = sum W G ra',  Mb = sum W G rb',  Mab = sum W G ra'.rb'
-//   block(i,j) = s_i s_j [Mab - Ma.pj' - Mb.pi' + (pi'.pj') M0] - dv_i dv_j M0 / k^2
-// FP64 flavour: R from the global quadrature points as the reference does.
-// ---------------------------------------------------------------------------
-// Tiles of TY test triangles x TX = 256 / TY source triangles, one thread per
-// pair; the grid covers the whole nt x nt square and tiles entirely below the
-// diagonal return at once (only ta <= tb pairs are computed).  The tile shape
-// is picked per mesh-size bucket by the autotuner in assemble().
-template <int NQ, int TY>
-__global__ void __launch_bounds__(256) k_far_f64(int nt, const TriCache *__restrict__ tc,
-                                                 const int *__restrict__ aoff, const int *__restrict__ anb,
-                                                 double k, double inv_k2, double2 *__restrict__ S,
-                                                 int64_t ldS) {
-  constexpr int TX = 256 / TY;
-  const int rb = blockIdx.y * TY, cb = blockIdx.x * TX;
-  if (rb > cb + TX - 1) return;  // uniform: tile below the diagonal
-  int ta = rb + (int)threadIdx.x / TX;
-  int tb = cb + (int)threadIdx.x % TX;
-  if (ta >= nt || tb >= nt || ta > tb) return;
-  const TriCache &A = tc[ta];
-  const TriCache &B = tc[tb];
-  double2 *out0 = S + (int64_t)(3 * ta) * ldS + 3 * tb;
-  if (ta == tb || tri_adjacent(aoff, anb, ta, tb)) {
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) out0[i * ldS + j] = make_double2(0.0, 0.0);
-    return;
-  }
-  double m0r = 0, m0i = 0, mar[3] = {0, 0, 0}, mai[3] = {0, 0, 0}, mbr[3] = {0, 0, 0},
-         mbi[3] = {0, 0, 0}, mabr = 0, mabi = 0;
-  double qa[NQ][3], la[NQ][3], wa[NQ];
-#pragma unroll
-  for (int a = 0; a < NQ; a++) {
-    wa[a] = A.w2a[a];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      qa[a][d] = A.qp[a][d];
-      la[a][d] = A.ql[a][d];
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < NQ; b++) {
-    double qb0 = B.qp[b][0], qb1 = B.qp[b][1], qb2 = B.qp[b][2];
-    double lb0 = B.ql[b][0], lb1 = B.ql[b][1], lb2 = B.ql[b][2];
-    double wb = B.w2a[b];
-#pragma unroll
-    for (int a = 0; a < NQ; a++) {
-      double dx = qa[a][0] - qb0, dy = qa[a][1] - qb1, dz = qa[a][2] - qb2;
-      double R = sqrt(dx * dx + dy * dy + dz * dz);
-      double sn, cs;
-      sincos(k * R, &sn, &cs);
-      double g = (DMB_INV_FOUR_PI / R) * (wa[a] * wb);
-      double gr = cs * g, gi = -sn * g;  // exp(-ikR)/(4 pi R) * W
-      m0r += gr;
-      m0i += gi;
-      mar[0] = fma(gr, la[a][0], mar[0]); mai[0] = fma(gi, la[a][0], mai[0]);
-      mar[1] = fma(gr, la[a][1], mar[1]); mai[1] = fma(gi, la[a][1], mai[1]);
-      mar[2] = fma(gr, la[a][2], mar[2]); mai[2] = fma(gi, la[a][2], mai[2]);
-      mbr[0] = fma(gr, lb0, mbr[0]); mbi[0] = fma(gi, lb0, mbi[0]);
-      mbr[1] = fma(gr, lb1, mbr[1]); mbi[1] = fma(gi, lb1, mbi[1]);
-      mbr[2] = fma(gr, lb2, mbr[2]); mbi[2] = fma(gi, lb2, mbi[2]);
-      double dd = la[a][0] * lb0 + la[a][1] * lb1 + la[a][2] * lb2;
-      mabr = fma(gr, dd, mabr);
-      mabi = fma(gi, dd, mabi);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    double si = A.s[i], dvi = A.dv[i];
-    double pi0 = A.pl[i][0], pi1 = A.pl[i][1], pi2 = A.pl[i][2];
-    // Mb . pi'
-    double mbpr = mbr[0] * pi0 + mbr[1] * pi1 + mbr[2] * pi2;
-    double mbpi = mbi[0] * pi0 + mbi[1] * pi1 + mbi[2] * pi2;
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      double sj = B.s[j], dvj = B.dv[j];
-      double pj0 = B.pl[j][0], pj1 = B.pl[j][1], pj2 = B.pl[j][2];
-      double mapr = mar[0] * pj0 + mar[1] * pj1 + mar[2] * pj2;
-      double mapi = mai[0] * pj0 + mai[1] * pj1 + mai[2] * pj2;
-      double pp = pi0 * pj0 + pi1 * pj1 + pi2 * pj2;
-      double ss = si * sj, sc = dvi * dvj * inv_k2;
-      double vr = ss * (mabr - mapr - mbpr + pp * m0r) - sc * m0r;
-      double vi = ss * (mabi - mapi - mbpi + pp * m0i) - sc * m0i;
-      out0[i * ldS + j] = make_double2(vr, vi);
-    }
-  }
-}
-
-// FP32 flavour: R from centroid difference (rounded from FP64) plus local
-// offsets, all quadrature arithmetic in FP32.
-template <int NQ, int TY>
-__global__ void __launch_bounds__(256) k_far_f32(int nt, const TriCache *__restrict__ tc,
-                                                 const int *__restrict__ aoff, const int *__restrict__ anb,
-                                                 float k, float inv_k2, float2 *__restrict__ S,
-                                                 int64_t ldS) {
-  constexpr int TX = 256 / TY;
-  const int rb = blockIdx.y * TY, cb = blockIdx.x * TX;
-  if (rb > cb + TX - 1) return;  // uniform: tile below the diagonal
-  int ta = rb + (int)threadIdx.x / TX;
-  int tb = cb + (int)threadIdx.x % TX;
-  if (ta >= nt || tb >= nt || ta > tb) return;
-  const TriCache &A = tc[ta];
-  const TriCache &B = tc[tb];
-  float2 *out0 = S + (int64_t)(3 * ta) * ldS + 3 * tb;
-  if (ta == tb || tri_adjacent(aoff, anb, ta, tb)) {
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) out0[i * ldS + j] = make_float2(0.f, 0.f);
-    return;
-  }
-  float dc0 = (float)(A.cen[0] - B.cen[0]), dc1 = (float)(A.cen[1] - B.cen[1]),
-        dc2 = (float)(A.cen[2] - B.cen[2]);
-  float m0r = 0, m0i = 0, mar[3] = {0, 0, 0}, mai[3] = {0, 0, 0}, mbr[3] = {0, 0, 0},
-        mbi[3] = {0, 0, 0}, mabr = 0, mabi = 0;
-  float la[NQ][3], wa[NQ];
-#pragma unroll
-  for (int a = 0; a < NQ; a++) {
-    wa[a] = (float)A.w2a[a];
-#pragma unroll
-    for (int d = 0; d < 3; d++) la[a][d] = (float)A.ql[a][d];
-  }
-  const float c4pi = 0.0795774715f;
-#pragma unroll
-  for (int b = 0; b < NQ; b++) {
-    float lb0 = (float)B.ql[b][0], lb1 = (float)B.ql[b][1], lb2 = (float)B.ql[b][2];
-    float wb = (float)B.w2a[b];
-#pragma unroll
-    for (int a = 0; a < NQ; a++) {
-      float dx = dc0 + (la[a][0] - lb0), dy = dc1 + (la[a][1] - lb1), dz = dc2 + (la[a][2] - lb2);
-      float R2 = dx * dx + dy * dy + dz * dz;
-      float rinv = rsqrtf(R2);
-      float R = R2 * rinv;
-      float sn, cs;
-      sincosf(k * R, &sn, &cs);
-      float g = (c4pi * rinv) * (wa[a] * wb);
-      float gr = cs * g, gi = -sn * g;
-      m0r += gr;
-      m0i += gi;
-      mar[0] = fmaf(gr, la[a][0], mar[0]); mai[0] = fmaf(gi, la[a][0], mai[0]);
-      mar[1] = fmaf(gr, la[a][1], mar[1]); mai[1] = fmaf(gi, la[a][1], mai[1]);
-      mar[2] = fmaf(gr, la[a][2], mar[2]); mai[2] = fmaf(gi, la[a][2], mai[2]);
-      mbr[0] = fmaf(gr, lb0, mbr[0]); mbi[0] = fmaf(gi, lb0, mbi[0]);
-      mbr[1] = fmaf(gr, lb1, mbr[1]); mbi[1] = fmaf(gi, lb1, mbi[1]);
-      mbr[2] = fmaf(gr, lb2, mbr[2]); mbi[2] = fmaf(gi, lb2, mbi[2]);
-      float dd = la[a][0] * lb0 + la[a][1] * lb1 + la[a][2] * lb2;
-      mabr = fmaf(gr, dd, mabr);
-      mabi = fmaf(gi, dd, mabi);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    float si = (float)A.s[i], dvi = (float)A.dv[i];
-    float pi0 = (float)A.pl[i][0], pi1 = (float)A.pl[i][1], pi2 = (float)A.pl[i][2];
-    float mbpr = mbr[0] * pi0 + mbr[1] * pi1 + mbr[2] * pi2;
-    float mbpi = mbi[0] * pi0 + mbi[1] * pi1 + mbi[2] * pi2;
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      float sj = (float)B.s[j], dvj = (float)B.dv[j];
-      float pj0 = (float)B.pl[j][0], pj1 = (float)B.pl[j][1], pj2 = (float)B.pl[j][2];
-      float mapr = mar[0] * pj0 + mar[1] * pj1 + mar[2] * pj2;
-      float mapi = mai[0] * pj0 + mai[1] * pj1 + mai[2] * pj2;
-      float pp = pi0 * pj0 + pi1 * pj1 + pi2 * pj2;
-      float ss = si * sj, sc = dvi * dvj * inv_k2;
-      float vr = ss * (mabr - mapr - mbpr + pp * m0r) - sc * m0r;
-      float vi = ss * (mabi - mapi - mbpi + pp * m0i) - sc * m0i;
-      out0[i * ldS + j] = make_float2(vr, vi);
-    }
-  }
-}
-
-// gather: Z[m][n] = -i w mu0 * sum_{a,b in +,-} S_sym(slot(m,a), slot(n,b))
-template <class SC, class ZC>
-__global__ void k_gather(int64_t N, const int *__restrict__ rslot, const SC *__restrict__ S,
-                         int64_t ldS, double omega_mu0, ZC *__restrict__ Z) {
-  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int64_t m = blockIdx.y;
-  if (n >= N) return;
-  int sm[2] = {rslot[2 * m], rslot[2 * m + 1]};
-  int sn[2] = {rslot[2 * n], rslot[2 * n + 1]};
-  double re = 0, im = 0;
-#pragma unroll
-  for (int a = 0; a < 2; a++)
-#pragma unroll
-    for (int b = 0; b < 2; b++) {
-      int x = sm[a], y = sn[b];
-      int64_t idx = x <= y ? (int64_t)x * ldS + y : (int64_t)y * ldS + x;
-      double2 v = to_d2(S[idx]);
-      re += v.x;
-      im += v.y;
-    }
-  // (-i w) * (re + i im) = (w im, -w re)
-  store_c(Z + m * N + n, make_double2(omega_mu0 * im, -omega_mu0 * re));
-}
-
 // ---------------------------------------------------------------------------
 // near-singular terms (device restatement of EFIE.jl:534-684 and
 // SingularIntegrals.jl:146-203)
@@ -500,13 +296,9 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
 }
 
 // one near record: self (ta == tb) or edge-adjacent (ta outer, tb analytic)
-__global__ void k_near_values(int64_t nrec, const NearRec *__restrict__ recs,
-                              const TriCache *__restrict__ tc, int nq, const double *__restrict__ wq_std,
-                              const double *__restrict__ wq_hi, double k, double inv_k2,
-                              double2 *__restrict__ vals) {
-  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrec) return;
-  NearRec rc = recs[r];
+__device__ double2 near_value(const NearRec rc, const TriCache *__restrict__ tc, int nq,
+                              const double *__restrict__ wq_std, const double *__restrict__ wq_hi, double k,
+                              double inv_k2) {
   const TriCache &A = tc[rc.ta];
   const TriCache &B = tc[rc.tb];
   double dvm = A.dv[rc.ia], dvn = B.dv[rc.ib];
@@ -595,16 +387,23 @@ __global__ void k_near_values(int64_t nrec, const NearRec *__restrict__ recs,
     vr = vs.x + vg;
     vi = vs.y;
   }
-  vals[r] = make_double2(vr, vi);
+  return make_double2(vr, vi);
+}
+
+__global__ void k_near_values(int64_t nrec, const NearRec *__restrict__ recs,
+                              const TriCache *__restrict__ tc, int nq, const double *__restrict__ wq_std,
+                              const double *__restrict__ wq_hi, double k, double inv_k2,
+                              double2 *__restrict__ vals) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrec) return;
+  vals[r] = near_value(recs[r], tc, nq, wq_std, wq_hi, k, inv_k2);
 }
 
 // sum the records of each near entry in fixed order, add to Z[m][n], Z[n][m]
 template <class ZC>
-__global__ void k_near_add(int64_t nent, const int2 *__restrict__ mn, const int64_t *__restrict__ off,
-                           const double2 *__restrict__ vals, double omega_mu0, int64_t N,
-                           ZC *__restrict__ Z) {
-  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nent) return;
+__device__ __forceinline__ void near_add_entry(int64_t e, const int2 *__restrict__ mn,
+                                               const int64_t *__restrict__ off, const double2 *__restrict__ vals,
+                                               double omega_mu0, int64_t N, ZC *__restrict__ Z) {
   double re = 0, im = 0;
   for (int64_t r = off[e]; r < off[e + 1]; r++) {
     re += vals[r].x;
@@ -618,6 +417,56 @@ __global__ void k_near_add(int64_t nent, const int2 *__restrict__ mn, const int6
     ZC *b = Z + (int64_t)p.y * N + p.x;
     store_c(b, cadd(to_d2(*b), add));
   }
+}
+
+template <class ZC>
+__global__ void k_near_add(int64_t nent, const int2 *__restrict__ mn, const int64_t *__restrict__ off,
+                           const double2 *__restrict__ vals, double omega_mu0, int64_t N,
+                           ZC *__restrict__ Z) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  near_add_entry(e, mn, off, vals, omega_mu0, N, Z);
+}
+
+// Near terms of many surfaces in one launch each (uneven surface batches):
+// thread -> (surface, record / entry) through the jobs' prefix offsets.
+struct NearJob {
+  const NearRec *recs;
+  const TriCache *tc;
+  const double *wq;       // 7 standard + 7 high-order weights
+  double2 *vals;
+  const int2 *mn;
+  const int64_t *eoff;
+  void *Z;
+  int64_t N, rec0, ent0;  // first record / entry of the surface in the batch
+  double k, inv_k2, omega_mu0;
+  int nq;
+};
+
+__device__ __forceinline__ int near_job_of(const NearJob *jobs, int njobs, int64_t g, bool entries) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if ((entries ? jobs[mid].ent0 : jobs[mid].rec0) <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_near_values_batched(const NearJob *__restrict__ jobs, int njobs, int64_t total) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const NearJob &jb = jobs[near_job_of(jobs, njobs, g, false)];
+  const int64_t r = g - jb.rec0;
+  jb.vals[r] = near_value(jb.recs[r], jb.tc, jb.nq, jb.wq, jb.wq + 7, jb.k, jb.inv_k2);
+}
+
+template <class ZC>
+__global__ void k_near_add_batched(const NearJob *__restrict__ jobs, int njobs, int64_t total) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const NearJob &jb = jobs[near_job_of(jobs, njobs, g, true)];
+  near_add_entry(g - jb.ent0, jb.mn, jb.eoff, jb.vals, jb.omega_mu0, jb.N, reinterpret_cast<ZC *>(jb.Z));
 }
 
 }  // namespace
@@ -795,6 +644,7 @@ void ensure_cache(dmb_ctx *c, int quad_order) {
   DMB_CUDA(cudaStreamSynchronize(c->stream));
   c->cache_valid = true;
   c->cache_quad_order = quad_order;
+  c->cache_gen++;
 }
 
 // value of every near record (self / edge-adjacent term per slot pair)
@@ -806,51 +656,8 @@ void near_values(dmb_ctx *c, double k, double inv_k2) {
              c->d_near_val.as<double2>());
 }
 
-// Far-pair tile autotuner: per (device, mesh-size bucket, precision,
-// quadrature size) the three tile shapes (8 x 32, 16 x 16, 32 x 8 triangle
-// pairs per CTA) are each timed once with CUDA events on the context stream
-// (after one untimed launch that loads the kernel) and the fastest is kept for
-// the process.  DMB_OPT_FAR_TILE pins a shape instead.  Every shape computes
-// the same pair blocks bit for bit; the caller's final launch writes S.
-template <class Launch>
-int far_tile_rows(dmb_ctx *c, int64_t nt, bool f64, Launch &&launch) {
-  if (c->far_tile > 0) return c->far_tile_used = c->far_tile;
-  int bucket = 0;
-  while ((int64_t)1 << (bucket + 1) <= nt) bucket++;
-  const int64_t key = ((int64_t)c->device << 24) | ((int64_t)bucket << 8) | ((f64 ? 1 : 0) << 4) | c->nq;
-  static std::mutex mu;
-  static std::vector<std::pair<int64_t, int>> table;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    for (auto &e : table)
-      if (e.first == key) return c->far_tile_used = e.second;
-  }
-  cudaEvent_t e0, e1;
-  DMB_CUDA(cudaEventCreate(&e0));
-  DMB_CUDA(cudaEventCreate(&e1));
-  int best = 16;
-  float best_ms = 0;
-  for (int ty : {8, 16, 32}) {
-    launch(ty);
-    DMB_CUDA(cudaEventRecord(e0, c->stream));
-    launch(ty);
-    DMB_CUDA(cudaEventRecord(e1, c->stream));
-    DMB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    DMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (best_ms == 0 || ms < best_ms) {
-      best_ms = ms;
-      best = ty;
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  std::lock_guard<std::mutex> lk(mu);
-  table.push_back({key, best});
-  return c->far_tile_used = best;
-}
-
-void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) {
+// EFIE prefactors with the reference's argument checks (EFIE.jl:699-720)
+static void prefactors(double k, double eta0, int precision, double &inv_k2, double &omega_mu0) {
   DMB_REQUIRE(std::isfinite(k) && k != 0.0, DMB_ERR_ARGUMENT,
               "EFIE wavenumber must be finite and nonzero, got " + std::to_string(k));
   DMB_REQUIRE(std::isfinite(eta0) && eta0 != 0.0, DMB_ERR_ARGUMENT,
@@ -860,50 +667,36 @@ void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) 
   double k2 = k * k;
   DMB_REQUIRE(std::isfinite(k2) && k2 != 0.0, DMB_ERR_OVERFLOW,
               "EFIE wavenumber squared is not representable");
-  double inv_k2 = 1.0 / k2;
-  double omega_mu0 = k * eta0;
+  inv_k2 = 1.0 / k2;
+  omega_mu0 = k * eta0;
   DMB_REQUIRE(std::isfinite(omega_mu0) && omega_mu0 != 0.0, DMB_ERR_OVERFLOW,
               "EFIE k*eta0 prefactor is not representable");
+}
+
+static void mark_assembled(dmb_ctx *c, double k, double eta0, int precision) {
+  c->z_prec = precision;
+  c->z_valid = true;
+  c->op_kind = 0;  // the dense Z is the operator again
+  c->z_version++;
+  c->k = k;
+  c->eta0 = eta0;
+  c->pc_valid = false;
+}
+
+void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) {
+  double inv_k2, omega_mu0;
+  prefactors(k, eta0, precision, inv_k2, omega_mu0);
   ensure_cache(c, quad_order);
   double t0 = now_ms();
-  const int64_t nt = c->nt, N = c->n;
-  const int64_t ldS = 3 * nt;
+  const int64_t N = c->n;
   const bool f64 = precision == DMB_PREC_FP64;
   size_t esz = f64 ? sizeof(double2) : sizeof(float2);
-  c->d_S.ensure((size_t)ldS * ldS * esz);
-  c->d_Z.ensure((size_t)N * N * esz);
-  const TriCache *tc = c->d_tcache.as<TriCache>();
-  const int *aoff = c->d_adj_off.as<int>(), *anb = c->d_adj_nb.as<int>();
+  c->d_Z.ensure((size_t)std::max<int64_t>(N, 1) * std::max<int64_t>(N, 1) * esz);
   DMB_REQUIRE(c->nq == 1 || c->nq == 3 || c->nq == 4 || c->nq == 7, DMB_ERR_ARGUMENT,
               "unsupported quadrature size");
-  auto far = [&](int ty) {
-    const int tx = 256 / ty;
-    dim3 g((unsigned)((nt + tx - 1) / tx), (unsigned)((nt + ty - 1) / ty));
-#define FAR_CASE(NQV, TYV)                                                                          \
-  if (c->nq == NQV && ty == TYV) {                                                                 \
-    if (f64)                                                                                       \
-      DMB_LAUNCH(c, (k_far_f64<NQV, TYV>), g, 256, 0, (int)nt, tc, aoff, anb, k, inv_k2,          \
-                 c->d_S.as<double2>(), ldS);                                                       \
-    else                                                                                           \
-      DMB_LAUNCH(c, (k_far_f32<NQV, TYV>), g, 256, 0, (int)nt, tc, aoff, anb, (float)k,            \
-                 (float)inv_k2, c->d_S.as<float2>(), ldS);                                         \
-  }
-#define FAR_SHAPES(NQV) FAR_CASE(NQV, 8) FAR_CASE(NQV, 16) FAR_CASE(NQV, 32)
-    FAR_SHAPES(1)
-    FAR_SHAPES(3)
-    FAR_SHAPES(4)
-    FAR_SHAPES(7)
-#undef FAR_SHAPES
-#undef FAR_CASE
-  };
-  far(far_tile_rows(c, nt, f64, far));
-  dim3 g((unsigned)((N + 255) / 256), (unsigned)N);
-  if (f64)
-    DMB_LAUNCH(c, (k_gather<double2, double2>), g, 256, 0, N, c->d_rwg_slot.as<int>(),
-               c->d_S.as<double2>(), ldS, omega_mu0, c->d_Z.as<double2>());
-  else
-    DMB_LAUNCH(c, (k_gather<float2, float2>), g, 256, 0, N, c->d_rwg_slot.as<int>(),
-               c->d_S.as<float2>(), ldS, omega_mu0, c->d_Z.as<float2>());
+  // far triangle pairs straight into Z by RWG tiles (dmb_fartile.cu)
+  const int T = far_tile_width(c, f64, k, inv_k2, omega_mu0);
+  far_tiles(c, T, f64, k, inv_k2, omega_mu0);
   // near-singular records (always FP64)
   if (c->n_near_rec > 0) {
     near_values(c, k, inv_k2);
@@ -916,15 +709,83 @@ void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision) 
                  c->n_near_entry, c->d_near_entry_mn.as<int2>(), c->d_near_entry_off.as<int64_t>(),
                  c->d_near_val.as<double2>(), omega_mu0, N, c->d_Z.as<float2>());
   }
-  DMB_CUDA(cudaStreamSynchronize(c->stream));
+  DMB_REQUIRE(far_error_word(c, f64) == 0, DMB_ERR_TIMEOUT, "assembly: a far-pair panel copy wait expired");
   c->tm.assembly_ms = now_ms() - t0;
-  c->z_prec = precision;
-  c->z_valid = true;
-  c->op_kind = 0;  // the dense Z is the operator again
-  c->z_version++;
-  c->k = k;
-  c->eta0 = eta0;
-  c->pc_valid = false;
+  mark_assembled(c, k, eta0, precision);
+}
+
+double assemble_batch(const std::vector<dmb_ctx *> &cs, double k, double eta0, int quad_order, int precision,
+                      BatchAsmBufs &bufs) {
+  if (cs.empty()) return 0.0;
+  double inv_k2, omega_mu0;
+  prefactors(k, eta0, precision, inv_k2, omega_mu0);
+  const bool f64 = precision == DMB_PREC_FP64;
+  const size_t esz = f64 ? sizeof(double2) : sizeof(float2);
+  dmb_ctx *big = cs[0], *c0 = cs[0];
+  for (dmb_ctx *c : cs) {
+    ensure_cache(c, quad_order);
+    c->d_Z.ensure((size_t)std::max<int64_t>(c->n, 1) * std::max<int64_t>(c->n, 1) * esz);
+    if (c->n > big->n) big = c;
+  }
+  // tile width of the largest surface's size bucket (autotuned there)
+  const int T = far_tile_width(big, f64, k, inv_k2, omega_mu0);
+  for (dmb_ctx *c : cs) c->far_tile_used = T;
+  cudaEvent_t e0, e1;
+  DMB_CUDA(cudaEventCreate(&e0));
+  DMB_CUDA(cudaEventCreate(&e1));
+  DMB_CUDA(cudaEventRecord(e0, c0->stream));
+  far_tiles_batched(cs, T, f64, k, inv_k2, omega_mu0, bufs.far_jobs, bufs.far_tasks, bufs.far_err);
+  std::vector<NearJob> jobs;
+  int64_t nrec = 0, nent = 0;
+  for (dmb_ctx *c : cs) {
+    if (c->n_near_rec == 0) continue;
+    NearJob jb;
+    jb.recs = c->d_near_rec.as<NearRec>();
+    jb.tc = c->d_tcache.as<TriCache>();
+    jb.wq = c->d_wq.as<double>();
+    jb.vals = c->d_near_val.as<double2>();
+    jb.mn = c->d_near_entry_mn.as<int2>();
+    jb.eoff = c->d_near_entry_off.as<int64_t>();
+    jb.Z = c->d_Z.p;
+    jb.N = c->n;
+    jb.rec0 = nrec;
+    jb.ent0 = nent;
+    jb.k = k;
+    jb.inv_k2 = inv_k2;
+    jb.omega_mu0 = omega_mu0;
+    jb.nq = c->nq;
+    jobs.push_back(jb);
+    nrec += c->n_near_rec;
+    nent += c->n_near_entry;
+  }
+  if (!jobs.empty()) {
+    bufs.near_jobs.ensure(jobs.size() * sizeof(NearJob));
+    DMB_CUDA(cudaMemcpyAsync(bufs.near_jobs.p, jobs.data(), jobs.size() * sizeof(NearJob), cudaMemcpyHostToDevice,
+                             c0->stream));
+    const int nj = (int)jobs.size();
+    DMB_LAUNCH(c0, k_near_values_batched, (unsigned)((nrec + 127) / 128), 128, 0, bufs.near_jobs.as<NearJob>(), nj,
+               nrec);
+    if (f64)
+      DMB_LAUNCH(c0, k_near_add_batched<double2>, (unsigned)((nent + 255) / 256), 256, 0,
+                 bufs.near_jobs.as<NearJob>(), nj, nent);
+    else
+      DMB_LAUNCH(c0, k_near_add_batched<float2>, (unsigned)((nent + 255) / 256), 256, 0,
+                 bufs.near_jobs.as<NearJob>(), nj, nent);
+  }
+  DMB_CUDA(cudaEventRecord(e1, c0->stream));
+  DMB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  DMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  unsigned err = 0;
+  DMB_CUDA(cudaMemcpy(&err, bufs.far_err.p, 4, cudaMemcpyDeviceToHost));
+  DMB_REQUIRE(err == 0, DMB_ERR_TIMEOUT, "batched assembly: a far-pair panel copy wait expired");
+  for (dmb_ctx *c : cs) {
+    c->tm.assembly_ms = ms;
+    mark_assembled(c, k, eta0, precision);
+  }
+  return ms;
 }
 
 }  // namespace dmb

@@ -143,6 +143,28 @@ struct AcaState {
   }
 };
 
+namespace dmb {
+// families of the online autotuner (dmb_tune.cu)
+enum TuneFamily { TUNE_TC_GEMM_BN = 0, TUNE_TC_SYRK_STAGES = 1, TUNE_FAMILIES = 2 };
+struct TuneMark {
+  bool active = false;
+  int family = 0, cand = 0;
+  int64_t b1 = 0, b2 = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+}  // namespace dmb
+
+// Panels of the far-pair tile kernel (dmb_fartile.cu) for one precision:
+// per RWG tile of width T the triangles carrying its functions, packed from
+// the per-triangle cache; valid for one (T, quadrature size, cache build).
+struct FarTileState {
+  bool valid = false;
+  int T = 0, nq = 0, ntiles = 0;
+  uint64_t cache_gen = 0;
+  int64_t ntasks = 0;
+  DevBuf d_panels, d_cnt, d_tasks, d_job, d_err;
+};
+
 struct dmb_ctx {
   int device = 0;
   // operator of dmb_gmres / dmb_matvec: 0 the resident dense Z, 1 the
@@ -173,6 +195,7 @@ struct dmb_ctx {
   std::vector<double> h_len, h_ap, h_am;
   bool have_mesh = false, have_rwg = false, cache_valid = false;
   int cache_quad_order = 0;
+  uint64_t cache_gen = 0;  // bumped by every rebuild of the per-triangle cache
 
   // device geometry
   DevBuf d_xyz, d_tri, d_tcache, d_rwg_slot;  // rwg_slot: 2 ints per RWG (3t+i)
@@ -197,7 +220,7 @@ struct dmb_ctx {
   int z_prec = -1;    // DMB_PREC_*
   bool z_valid = false;
   double k = 0, eta0 = 376.730313668;
-  DevBuf d_S;         // triangle-slot scratch (3Nt x 3Nt)
+  FarTileState ft[2];  // far-pair tile panels: [0] FP32, [1] FP64
 
   // preconditioner
   int pc_kind = DMB_PRECOND_NONE;
@@ -226,7 +249,7 @@ struct dmb_ctx {
   DevBuf d_small;
   bool use_tensor_cores = true;  // complex64 factor update on tcgen05 (else FP32 SIMT)
   int tc_min_rhs = 64;           // batched Z X / triangular solves on tcgen05 from this many RHS
-  int far_tile = 0;              // far-pair tile rows (8/16/32), 0 = autotuned
+  int far_tile = 0;              // far-pair RWG tile width (FP64 16/32, FP32 32/64), 0 = autotuned
   bool exact_krylov = true;      // many-RHS Krylov product on the INT8 slices (FP64-accurate)
   // GMRES iterations between host checks replayed as captured CUDA graphs
   // (few right-hand sides); key: iteration range, shape, buffer addresses and
@@ -246,7 +269,9 @@ struct dmb_ctx {
   };
   std::map<std::vector<int64_t>, GraphEntry> gm_graphs;
   int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
-  int far_tile_used = 0;         // shape of the last assembly
+  int far_tile_used = 0;         // tile width of the last assembly
+  // autotuner pins per family (0: tuned, k: candidate k - 1)
+  int tune_pin[dmb::TUNE_FAMILIES] = {0, 0};
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves
@@ -271,10 +296,11 @@ struct dmb_ctx {
   bool kt_enabled = false;     // dominant-kernel event timing
   // per family: 0 3xTF32 Krylov / sweep GEMMs, 1 int8 GEMMs, 2 factor updates,
   // 3 H-matrix products (one right-hand side, work in bytes), 4 FP64-pipe
-  // complex128 Z X and sweep GEMMs
-  static constexpr int KT_FAMILIES = 5;
-  double kt_ms[KT_FAMILIES] = {0, 0, 0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0, 0, 0};
-  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0, 0, 0};
+  // complex128 Z X and sweep GEMMs, 5 far-pair tiles of the assembly (work in
+  // bytes of Z written)
+  static constexpr int KT_FAMILIES = 6;
+  double kt_ms[KT_FAMILIES] = {0, 0, 0, 0, 0, 0}, kt_flops[KT_FAMILIES] = {0, 0, 0, 0, 0, 0};
+  int64_t kt_launches[KT_FAMILIES] = {0, 0, 0, 0, 0, 0};
   std::vector<cudaEvent_t> kt_pool;   // (start, end) pairs recorded around launches
   std::vector<double> kt_pending;     // algorithmic work of each recorded launch
   std::vector<int> kt_family;         // family of each recorded launch
@@ -336,6 +362,30 @@ void ensure_cache(dmb_ctx *c, int quad_order);
 void gradient_impedance_dev(dmb_ctx *c, int64_t R, const double2 *I_dev, const double2 *L_dev,
                             const int *tri_patch, int64_t P, int reactive, int quad_order, double *g_dev);
 void build_host_topology(dmb_ctx *c);
+// far-pair part of Z by RWG tiles (dmb_fartile.cu)
+bool far_tile_width_valid(int T, bool f64);
+void far_panels(dmb_ctx *c, int T, bool f64);
+void far_tiles(dmb_ctx *c, int T, bool f64, double k, double inv_k2, double omega_mu0);
+int far_tile_width(dmb_ctx *c, bool f64, double k, double inv_k2, double omega_mu0);
+unsigned far_error_word(dmb_ctx *c, bool f64);
+void far_release(dmb_ctx *c);
+void far_tiles_batched(const std::vector<dmb_ctx *> &cs, int T, bool f64, double k, double inv_k2,
+                       double omega_mu0, DevBuf &d_jobs, DevBuf &d_tasks, DevBuf &d_err);
+// impedance matrices of many surfaces: far tiles in one launch, near values
+// and near sums in one launch each, on the stream of cs[0] (dmb_assemble.cu);
+// returns the device time of the three launches
+struct BatchAsmBufs {
+  DevBuf far_jobs, far_tasks, far_err, near_jobs;
+};
+double assemble_batch(const std::vector<dmb_ctx *> &cs, double k, double eta0, int quad_order, int precision,
+                      BatchAsmBufs &bufs);
+// online autotuner (dmb_tune.cu): candidate for a (family, bucket), and the
+// event bracket of a launch while the bucket is being measured
+int64_t tune_bucket(int64_t v);  // floor(log2(v))
+int tune_choose(dmb_ctx *c, int family, int64_t b1, int64_t b2, int ncand);
+bool tune_begin(dmb_ctx *c, int family, int64_t b1, int64_t b2, int cand, TuneMark &mk);
+void tune_end(dmb_ctx *c, TuneMark &mk);
+std::string tune_report();
 void assemble(dmb_ctx *c, double k, double eta0, int quad_order, int precision);
 void copy_z_out(dmb_ctx *c, double *Z_out);
 void z_entries(dmb_ctx *c, const int64_t *m, const int64_t *n, int64_t count, double *out);

@@ -46,10 +46,9 @@ constexpr int TC_A_STAGE = TC_BM * TC_BK * 4;  // 16 KB
 constexpr int TC_B_STAGE = TC_BN * TC_BK * 4;  // 32 KB
 constexpr int TC_SMEM = TC_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 /*barriers*/ + 1024 /*align*/;
 constexpr int TC_SMEM_128 = TC_STAGES * (TC_A_STAGE + TC_B_STAGE / 2) + 1024 + 1024;
-// factor-update pipeline depth: 4 stages, one CTA per SM (measured ahead of
-// 2 stages with two co-resident CTAs per SM, 119 vs 113 TFLOP/s)
-constexpr int TC_SYRK_STAGES = 4;
-constexpr int TC_SYRK_SMEM = TC_SYRK_STAGES * (TC_A_STAGE + TC_B_STAGE) + 1024 + 1024;
+// factor-update pipeline depth, picked by the autotuner per update shape:
+// 4 stages with one CTA per SM, or 2 stages with two co-resident CTAs per SM
+constexpr int tc_syrk_smem(int stages) { return stages * (TC_A_STAGE + TC_B_STAGE) + 1024 + 1024; }
 
 // instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
@@ -555,8 +554,8 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<TC_SYRK_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  TC_SYRK_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(4)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(2)));
     st.attr = true;
   }
   const int64_t rest = N - r0, ncols = std::min<int64_t>(c_hi, N) - r0;
@@ -568,8 +567,17 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
              N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<float>(), bB.as<float>());
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
   const int cpb = 16 * c->precond_tf32_terms;
-  DMB_LAUNCH(c, k_tc_syrk<TC_SYRK_STAGES>, grid, 128, TC_SYRK_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
-             r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
+  const int64_t tb1 = dmb::tune_bucket((rest + 63) / 64), tb2 = dmb::tune_bucket((ncols + TC_BN - 1) / TC_BN) * 8 + kslot;
+  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, 2);
+  dmb::TuneMark mk;
+  dmb::tune_begin(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, cand, mk);
+  if (cand == 0)
+    DMB_LAUNCH(c, k_tc_syrk<4>, grid, 128, tc_syrk_smem(4), st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
+               r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
+  else
+    DMB_LAUNCH(c, k_tc_syrk<2>, grid, 128, tc_syrk_smem(2), st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
+               r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
+  dmb::tune_end(c, mk);
 }
 
 unsigned tc_error_word(dmb_ctx *c) {
@@ -715,10 +723,15 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   }
   DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk, N,
              st.Pb.as<float>());
-  // triangular diagonal-block products with few row tiles: 128-wide tiles
-  // double the CTAs (measured faster only there)
-  const bool narrow = tri != 0 && (Rpad / TC_BN) * (Mpad / 64) < 2 * (int64_t)c->sm_count;
+  // tile width from the autotuner, per (row tiles, columns, triangular
+  // kind): 256 or 128 complex columns (128 doubles the CTAs of launches with
+  // few row tiles); both give the same bits
+  const int64_t tb1 = dmb::tune_bucket(Mpad / 64), tb2 = (Rpad / 128) * 4 + tri;
+  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, 2);
+  const bool narrow = cand == 1;
   const int cpb = 16 * c->precond_tf32_terms;
+  dmb::TuneMark mk;
+  dmb::tune_begin(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, cand, mk);
   kt_begin(c);
   if (narrow) {
     dim3 grid((unsigned)(Rpad / 128), (unsigned)(Mpad / 64));
@@ -731,6 +744,7 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   }
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
+  dmb::tune_end(c, mk);
 }
 
 // one sweep of the batched solve with the packed factor:

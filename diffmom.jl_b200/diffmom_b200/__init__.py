@@ -19,7 +19,8 @@ from .api import (EFIEDevice, assemble_Z_efie, matrixfree_efie_operator, MatrixF
                   monostatic_rcs_sweep, MonostaticResult, BatchSurface, BatchResult,
                   SurfaceBatch, solve_surfaces,
                   make_sph_grid, phi_cut_grid, compute_farfield, bistatic_rcs, backscatter_rcs,
-                  C0_DEFAULT, ETA0_DEFAULT)
+                  C0_DEFAULT, ETA0_DEFAULT, tune_report)
+from .learned import train_learned_network, training_bodies, load_default_network
 from .aca import (ClusterNode, ClusterTree, build_cluster_tree, cluster_tree_resource_bounds, aca_block_tasks,
                   cluster_diameter,
                   cluster_distance, is_admissible, is_leaf, leaf_nodes, EFIECache, build_efie_cache,

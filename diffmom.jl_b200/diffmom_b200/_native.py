@@ -49,6 +49,8 @@ OPT_GMRES_GRAPHS = 6
 OPT_OPERATOR = 7
 OPT_TRUE_RESIDUAL = 8
 OPT_SPIN_LIMIT = 9
+OPT_TUNE_TC_GEMM = 10
+OPT_TUNE_TC_SYRK = 11
 
 
 class DiffMoMError(RuntimeError):
@@ -141,10 +143,12 @@ SIGNATURES = {
     "dmb_get_timings": ([_P, ctypes.POINTER(Timings)], _I),
     "dmb_set_option": ([_P, _I, _I], _I),
     "dmb_get_far_tile": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
+    "dmb_tune_report": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], _I),
     "dmb_kernel_timing_family": ([_P, _I, _DP, ctypes.POINTER(ctypes.c_int64), _DP], _I),
     "dmb_batch_create": ([_I, _I, ctypes.POINTER(_P)], _I),
     "dmb_batch_destroy": ([_P], _I),
     "dmb_batch_last_error": ([_P], ctypes.c_char_p),
+    "dmb_batch_assembly_ms": ([_P, _DP], _I),
     "dmb_batch_solve": ([_P, ctypes.POINTER(SolveParams), ctypes.POINTER(BatchItem), _L, _DP], _I),
     "dmb_mesh_upload": ([_P, _DP, _LP, _L, _L], _I),
     "dmb_rwg_upload": ([_P, _L, _LP, _LP, _LP, _LP, _LP, _DP, _DP, _DP], _I),

@@ -85,7 +85,8 @@ class EFIEDevice:
         """Implementation switches: "tensor_cores" (0/1) for the complex64
         factorisation update, "tc_min_rhs" (>= 1) for the right-hand-side count
         from which Z X and the batched near-field solves use the tensor cores,
-        "far_tile" (0 = autotuned, 8/16/32) for the assembly's far-pair tiles,
+        "far_tile" (0 = autotuned; FP64 16/32, mixed 32/64) for the width of
+        the RWG tiles of the assembly's far-pair kernel,
         "exact_krylov" (0/1) for the FP64-accurate INT8-slice Krylov product,
         "precond_tf32_terms" (3/1) for the TF32 products per complex MAC of the
         complex64 factorisation updates and batched triangular sweeps,
@@ -93,11 +94,15 @@ class EFIEDevice:
         "true_residual" (1 = default: GMRES refines until ||b - Z x|| / ||b||
         meets the tolerance; 0: it stops where Krylov.gmres stops),
         "spin_limit" (polls of a chained triangular-sweep wait before the call
-        fails with TimeoutError; negative restores the default)."""
+        fails with TimeoutError; negative restores the default),
+        "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; 1 or 2 pins a candidate:
+        256- or 128-wide sweep GEMM tiles, 4- or 2-stage factor-update
+        pipelines)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
                  "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,
-                 "true_residual": nat.OPT_TRUE_RESIDUAL, "spin_limit": nat.OPT_SPIN_LIMIT}
+                 "true_residual": nat.OPT_TRUE_RESIDUAL, "spin_limit": nat.OPT_SPIN_LIMIT,
+                 "tune_tc_gemm": nat.OPT_TUNE_TC_GEMM, "tune_tc_syrk": nat.OPT_TUNE_TC_SYRK}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))
@@ -105,7 +110,7 @@ class EFIEDevice:
             self.preconditioner = None
 
     def far_tile(self) -> int:
-        """Far-pair tile rows the last assembly used (autotuned unless pinned)."""
+        """Far-pair RWG tile width the last assembly used (autotuned unless pinned)."""
         v = ctypes.c_int()
         self.ctx.call("dmb_get_far_tile", ctypes.byref(v))
         return v.value
@@ -864,6 +869,16 @@ class ScatteringResult:
     timings: dict = field(default_factory=dict)
 
 
+def tune_report() -> str:
+    """The online autotuner's measurements and choices so far (this process)."""
+    lib = nat.load_library()
+    n = ctypes.c_size_t()
+    nat.check_free(lib, lib.dmb_tune_report(None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    nat.check_free(lib, lib.dmb_tune_report(buf, n.value + 1, ctypes.byref(n)))
+    return buf.value.decode()
+
+
 def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                      dense_direct_limit: int = 2000, dense_gmres_limit: int = 10000,
                      mlfma_threshold: int = 50000, max_dense_matrix_bytes: int = 2_000_000_000,
@@ -873,7 +888,7 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                      c0: float = C0_DEFAULT, precision: str = "fp64", surface_impedance=None,
                      verbose: bool = False, device: EFIEDevice | None = None, rwg: RWGData | None = None,
                      aca_tol: float = 1e-6, aca_leaf_size: int = 64, aca_eta: float = 1.5,
-                     aca_max_rank: int = 50):
+                     aca_max_rank: int = 50, local_radius_lambda: float = 0.2, network=None):
     """Workflow.jl:67-317 on the GPU.
 
     method: "auto" | "dense_direct" | "dense_gmres" | "aca_gmres".  "auto"
@@ -894,6 +909,19 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
     the preconditioner is complex64).  GMRES judges convergence on the
     unpreconditioned FP64 residual (refining a left-preconditioned solve until
     it passes).
+
+    preconditioner: "auto" / "lu" / "diag" / "none" as the reference
+    (near-field LU at nf_cutoff_lambda wavelengths), plus two sparse right
+    preconditioners of this library for the dense GMRES path, built from each
+    RWG's near block within local_radius_lambda wavelengths (<= 64
+    neighbours): "local" (exact local-inverse rows) and "learned" (those rows
+    corrected by one ring-residual step whose direction the trained network
+    modulates; weights from ``network`` -- a checkpoint path or a weight
+    vector -- else the library's default weights, diffmom_b200/learned.py).
+    Both are applied on the right whatever precond_side says.  If GMRES with
+    either does not reach gmres_tol within gmres_maxiter, the near-field LU
+    preconditioner is built and the system solved again with it (the
+    fallback; a warning says so).
     """
     f = float(freq_hz)
     if not (math.isfinite(f) and f > 0):
@@ -911,8 +939,11 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
                          f"dense_gmres_limit ({dense_gmres_limit})")
     if not (isinstance(max_dense_matrix_bytes, (int, np.integer)) and max_dense_matrix_bytes > 0):
         raise ValueError(f"max_dense_matrix_bytes must be a positive integer, got {max_dense_matrix_bytes}")
-    if preconditioner not in ("auto", "lu", "diag", "none"):
-        raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, or :none")
+    if preconditioner not in ("auto", "lu", "diag", "none", "local", "learned"):
+        raise ValueError("solve_scattering: preconditioner must be :auto, :lu, :diag, :none, :local or :learned")
+    if not (math.isfinite(local_radius_lambda) and local_radius_lambda > 0):
+        raise ValueError(f"solve_scattering: local_radius_lambda must be finite and positive, got "
+                         f"{local_radius_lambda}")
     if method == "aca_gmres" and surface_impedance is not None:
         raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres")
     lam = c0 / f
@@ -943,6 +974,9 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
         if sel == "aca_gmres" and surface_impedance is not None:
             raise ValueError("solve_scattering: surface_impedance is not supported by :aca_gmres "
                              "(auto-selected above dense_gmres_limit; pass method=\"dense_gmres\")")
+    if preconditioner in ("local", "learned") and sel != "dense_gmres":
+        raise ValueError(f"solve_scattering: preconditioner :{preconditioner} needs method :dense_gmres "
+                         f"(selected :{sel})")
     if sel in ("dense_direct", "dense_gmres"):
         payload = N * N * (16 if precision == "fp64" else 8)
         if payload > max_dense_matrix_bytes:
@@ -989,14 +1023,43 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
         else:
             pc_used = "lu" if preconditioner == "auto" else preconditioner
             P = None
-            if pc_used != "none":
+            side = precond_side
+            if pc_used in ("local", "learned"):
+                tp = time.perf_counter()
+                if pc_used == "learned":
+                    if network is None:
+                        from .learned import load_default_network
+                        load_default_network(dev)
+                    elif isinstance(network, (str, bytes)) or hasattr(network, "__fspath__"):
+                        dev.load_network(network)
+                    else:
+                        dev.set_network_weights(network)
+                P = dev.build_local(local_radius_lambda * lam, mode=pc_used)
+                t_pc = time.perf_counter() - tp
+                side = "right"
+            elif pc_used != "none":
                 tp = time.perf_counter()
                 P = dev.build_nearfield(nf_cutoff_lambda * lam, pc_used)
                 t_pc = time.perf_counter() - tp
             t1 = time.perf_counter()
+            local = pc_used in ("local", "learned")
             I, st = dev.gmres(v, tol=gmres_tol, maxiter=gmres_maxiter, preconditioner=P,
-                              precond_side=precond_side,
-                              check_gmres_convergence=check_gmres_convergence)
+                              precond_side=side, check_gmres_convergence=check_gmres_convergence and not local)
+            if local and not st.solved:
+                # the near-field sparse preconditioner is the fallback
+                warnings.append(f"GMRES with the {pc_used} preconditioner did not converge in {st.niter} "
+                                f"iterations; solved again with the near-field LU preconditioner")
+                tp = time.perf_counter()
+                P = dev.build_nearfield(nf_cutoff_lambda * lam, "lu")
+                t_pc += time.perf_counter() - tp
+                I, st2 = dev.gmres(v, tol=gmres_tol, maxiter=gmres_maxiter, preconditioner=P,
+                                   precond_side=precond_side, check_gmres_convergence=False)
+                st = GmresResult(st.niter + st2.niter, st2.solved, st2.residual, st2.true_residual,
+                                 st.restarts + st2.restarts)
+                if check_gmres_convergence and not st.solved:
+                    raise nat.NotConvergedError(
+                        f"GMRES did not converge: niter={st.niter}, true residual {st.true_residual:.3e}, "
+                        f"tol={gmres_tol} (the {pc_used} preconditioner and its near-field LU fallback)")
             iters, resid, tres = st.niter, st.residual, st.true_residual
         t_solve = time.perf_counter() - t1
         tm = dev.timings()
@@ -1074,15 +1137,18 @@ class BatchResult:
     gmres_iters: np.ndarray
     true_residual: np.ndarray
     latency_ms: np.ndarray     # device time from the batch start to each surface's end
-    solve_ms: np.ndarray       # device time of each surface's own solve
+    solve_ms: np.ndarray       # device time of each surface's stages after the batch-wide assembly
     device_ms: float           # device time of the whole batch
     N: np.ndarray
     currents: list | None
+    assembly_ms: float = 0.0   # device time of the batch-wide assembly (one far-pair launch for all surfaces)
 
 
 class SurfaceBatch:
     """Many independent surfaces (each its own mesh, basis, impedance and
-    plane wave) solved by `lanes` concurrent device contexts, largest first."""
+    plane wave): every surface's impedance matrix assembled by one far-pair
+    launch (plus one launch each for the near terms), then the per-surface
+    stages on `lanes` concurrent host threads and streams, largest first."""
 
     def __init__(self, lanes: int = 8, device: int = 0):
         self.lib = nat.load_library()
@@ -1153,13 +1219,15 @@ class SurfaceBatch:
         if st != nat.DMB_OK:
             msg = (self.lib.dmb_batch_last_error(self.h) or b"").decode()
             raise nat._EXC.get(st, nat.DiffMoMError)(msg)
+        ams = ctypes.c_double()
+        self.lib.dmb_batch_assembly_ms(self.h, ctypes.byref(ams))
         return BatchResult(sigma=np.array([it.sigma for it in items]),
                            gmres_iters=np.array([it.stats.niter for it in items]),
                            true_residual=np.array([it.stats.true_residual for it in items]),
                            latency_ms=np.array([it.latency_ms for it in items]),
                            solve_ms=np.array([it.solve_ms for it in items]),
                            device_ms=dms.value, N=np.array([it.n for it in items]),
-                           currents=outs if return_currents else None)
+                           currents=outs if return_currents else None, assembly_ms=ams.value)
 
 
 def solve_surfaces(surfaces, freq_hz, lanes: int = 8, precision: str = "mixed", preconditioner: str = "lu",

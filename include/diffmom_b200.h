@@ -99,9 +99,11 @@ const char *dmb_version(void);
  * then confirms convergence on the FP64 residual and refines where needed. */
 #define DMB_OPT_TENSOR_CORES 1
 #define DMB_OPT_TC_MIN_RHS 2
-/* DMB_OPT_FAR_TILE: far triangle-pair tile shape of the assembly, as test
- * rows per 256-pair CTA (8, 16 or 32); 0 (default) lets the autotuner pick it
- * per mesh-size bucket (timed once per process). */
+/* DMB_OPT_FAR_TILE: width T of the RWG tiles of the assembly's far-pair
+ * kernel (one CTA per T x T block of Z): 16 or 32 for FP64, 32 or 64 for
+ * mixed precision; 0 (default) lets the autotuner pick it per mesh-size
+ * bucket (each width timed once per process).  Every width writes the same
+ * bits. */
 #define DMB_OPT_FAR_TILE 3
 /* DMB_OPT_EXACT_KRYLOV: 1 (default) runs the many-RHS GMRES operator on the
  * FP64-accurate INT8-slice product (no refinement cycle needed); 0 runs it in
@@ -143,9 +145,23 @@ const char *dmb_version(void);
  * stays usable.  A negative value restores the default (2e7 polls, seconds);
  * small values exercise the timeout path without any GPU fault. */
 #define DMB_OPT_SPIN_LIMIT 9
+/* DMB_OPT_TUNE_TC_GEMM / DMB_OPT_TUNE_TC_SYRK: pin a candidate of the online
+ * autotuner (0, the default, lets it choose): the tile width of the
+ * tensor-core sweep GEMMs (1: 256, 2: 128 complex columns) and the pipeline of
+ * the complex64 factor updates (1: 4 stages, one CTA per SM; 2: 2 stages, two
+ * CTAs per SM).  Unpinned, each launch shape bucket runs every candidate on
+ * its first real calls, timed with events, and keeps the fastest for the
+ * process; the candidates give the same bits. */
+#define DMB_OPT_TUNE_TC_GEMM 10
+#define DMB_OPT_TUNE_TC_SYRK 11
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
-/* The far-pair tile rows used by the last assembly on this context. */
-dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *rows_out);
+/* The far-pair RWG tile width used by the last assembly on this context. */
+dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *width_out);
+/* The autotuner's measurements and choices so far (all contexts of the
+ * process), one line per (device, kernel family, shape bucket); writes at
+ * most cap - 1 characters and a terminating zero, *len_out = full length.
+ * No reference counterpart. */
+dmb_status dmb_tune_report(char *buf, size_t cap, size_t *len_out);
 
 /* ---- mesh and basis ---------------------------------------------------- */
 /* TriMesh (src/Types.jl:123-126): xyz 3 x Nv column-major, tri 3 x Nt
@@ -337,10 +353,17 @@ dmb_status dmb_copy_solution(dmb_ctx *ctx, double *I_out);
  * 67-317) over independent bodies, each with its own mesh and RWG basis, an
  * optional per-triangle surface impedance (assemble_full_Z with
  * precompute_patch_mass, Impedance.jl:304-408) and its own plane wave, plus
- * backscatter_rcs (Diagnostics.jl:460-517).  A batch owns `lanes` contexts,
- * each with its own stream and host thread; surfaces are taken largest-first
- * and the GPU runs the lanes' kernels concurrently.  The solve of each surface
- * follows dmb_solve_resident with `p` (kvec/pol/E0 of p are ignored). */
+ * backscatter_rcs (Diagnostics.jl:460-517).  A batch keeps one device context
+ * per surface of a call (reused, buffers grow only).  dmb_batch_solve
+ * uploads the surfaces on `lanes` host threads, then assembles EVERY
+ * surface's impedance matrix with one far-pair tile launch (a task list of
+ * all surfaces' RWG tile pairs, largest surface first) and one launch each
+ * for the near values and near sums, and then runs the per-surface stages
+ * (impedance loading, preconditioner, right-hand side, GMRES, sigma) on the
+ * `lanes` host threads, largest surface first, each surface on its own
+ * stream.  The solve of each surface follows dmb_solve_resident with `p`
+ * (kvec/pol/E0 of p are ignored).  The batch holds the device memory of its
+ * largest call until dmb_batch_destroy. */
 typedef struct dmb_batch dmb_batch;
 typedef struct {
   /* inputs: host arrays in the layouts of dmb_mesh_upload / dmb_rwg_upload */
@@ -357,11 +380,14 @@ typedef struct {
   double sigma;           /* monostatic RCS at -k_hat */
   dmb_gmres_stats stats;
   double latency_ms;      /* device time from the batch start to the end of this surface */
-  double solve_ms;        /* device time of this surface's solve */
+  double solve_ms;        /* device time of this surface's stages after the batch-wide assembly */
 } dmb_batch_item;
 dmb_status dmb_batch_create(int device, int lanes, dmb_batch **out);
 dmb_status dmb_batch_destroy(dmb_batch *b);
 const char *dmb_batch_last_error(const dmb_batch *b);
+/* Device time of the last dmb_batch_solve's batch-wide assembly (the far
+ * tiles, near values and near sums of all its surfaces). */
+dmb_status dmb_batch_assembly_ms(const dmb_batch *b, double *ms_out);
 /* device_ms_out (may be NULL): device time of the whole batch. */
 dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_item *items, int64_t count,
                            double *device_ms_out);
@@ -383,8 +409,9 @@ dmb_status dmb_kernel_timing(dmb_ctx *ctx, double *ms, int64_t *launches, double
  * right-hand side: gather, low-rank inner products, leaf sums; work in bytes:
  * the stored blocks plus x and y once), 4 = FP64-pipe complex128 GEMMs (Z X
  * of a complex128 Z with >= 16 right-hand sides and the many-column sweep
- * updates of a complex128 factor; complex flops).  dmb_kernel_timing reports
- * family 0. */
+ * updates of a complex128 factor; complex flops), 5 = far-pair tiles of the
+ * assembly (work in bytes of Z written: N^2 x 16 for complex128, x 8 for
+ * complex64).  dmb_kernel_timing reports family 0. */
 dmb_status dmb_kernel_timing_family(dmb_ctx *ctx, int family, double *ms, int64_t *launches, double *work);
 
 /* ---- H-matrix operator (adaptive cross approximation) ------------------ */

@@ -259,3 +259,34 @@ def test_fp64_factor_and_sweeps_on_the_fp64_gemm():
     print(f"FP64 factor + sweeps, 40 columns: {err:.2e}")
     assert err < 1e-10
     dev.close()
+
+
+def test_autotuner_candidates_identical():
+    """Every candidate of the online autotuner writes the same bits: the
+    complex64 factor (4- or 2-stage update pipelines) and a batched sweep
+    (256- or 128-wide GEMM tiles), pinned one at a time, against the tuned
+    run; the tuner's report lists what it measured."""
+    from diffmom_b200 import tune_report
+    dev = _plate(36)  # 3,960 RWG: four 1,024-row sweep blocks, ragged last
+    dev.assemble(K3, precision="mixed")
+    X = _rand(dev.N, 200, 3)
+    out = {}
+    for syrk in (0, 1, 2):
+        for gemm in (0, 1, 2):
+            if syrk and gemm:
+                continue
+            dev.set_option("tune_tc_syrk", syrk)
+            dev.set_option("tune_tc_gemm", gemm)
+            dev.build_nearfield(math.inf, "lu")
+            out[(syrk, gemm)] = dev.nf_apply(X)
+    ref = out[(0, 0)]
+    for key, Y in out.items():
+        assert np.array_equal(Y, ref), key
+    dev.set_option("tune_tc_syrk", 0)
+    dev.set_option("tune_tc_gemm", 0)
+    rep = tune_report()
+    print(rep)
+    assert "k_tc_gemm" in rep and "k_tc_syrk" in rep
+    with pytest.raises(Exception):
+        dev.set_option("tune_tc_gemm", 3)
+    dev.close()

@@ -80,6 +80,52 @@ def test_assembly_fp64_sphere_and_disk(sphere2):
     dd.close()
 
 
+def _junction_mesh():
+    """A 6 x 6 plate in z = 0 with a 6 x 3 fin standing on its middle line
+    x = 0: the junction edges carry three triangles (no RWG function on them),
+    so the triangles along the line have more than three edge neighbours."""
+    from diffmom_b200 import TriMesh
+    n = 6
+    xs = np.linspace(-0.05, 0.05, n + 1)
+    xyz = [(x, y, 0.0) for y in xs for x in xs]
+    idx = lambda i, j: j * (n + 1) + i + 1
+    tri = []
+    for j in range(n):
+        for i in range(n):
+            tri.append((idx(i, j), idx(i + 1, j), idx(i + 1, j + 1)))
+            tri.append((idx(i, j), idx(i + 1, j + 1), idx(i, j + 1)))
+    mid = n // 2
+    zs = np.linspace(0.0, 0.05, 4)
+    fin = {}
+    for jz, z in enumerate(zs):
+        for j in range(n + 1):
+            if jz == 0:
+                fin[(j, jz)] = idx(mid, j)
+            else:
+                xyz.append((xs[mid], xs[j], z))
+                fin[(j, jz)] = len(xyz)
+    for jz in range(len(zs) - 1):
+        for j in range(n):
+            a, b, c, d = fin[(j, jz)], fin[(j + 1, jz)], fin[(j + 1, jz + 1)], fin[(j, jz + 1)]
+            tri.append((a, b, c))
+            tri.append((a, c, d))
+    return TriMesh(np.array(xyz), np.array(tri))
+
+
+def test_assembly_junction_mesh():
+    m = _junction_mesh()
+    r = build_rwg(m)
+    k = 2 * math.pi * 3e9 / C0
+    c = orc.OracleCache(m, r, 3)
+    Zo = c.assemble_z(k)
+    dev = EFIEDevice(m, r)
+    Z = dev.assemble(k, copy_out=True)
+    assert _rel_entrywise(Z, Zo) < ZTOL
+    Zm = dev.assemble(k, precision="mixed", copy_out=True)
+    assert np.linalg.norm(Zm - Zo) / np.linalg.norm(Zo) < 2e-6
+    dev.close()
+
+
 def test_assembly_deterministic(plate6):
     m, r, k, dev, c = plate6
     Z1 = dev.assemble(k, copy_out=True)
