@@ -25,9 +25,10 @@ Variants reported beside it (same timing rules, fewer steps where slow):
                   lambda, 500-6,000 RWG, one incidence each (seed 20260004):
                   mixed on 8 lanes vs plain FP64 one surface at a time;
                   per size-bucket solve times
-  c5_*            perturbed ellipsoid (seed 99), 9,720 RWG, one incidence:
-                  FP64 near-field vs mixed + learned right preconditioner
-                  (network trained beforehand, untimed, on 3 other bodies)
+  c5_*            perturbed ellipsoid (seed 99), 9,720 RWG (c5_17k_*: 17,280),
+                  one incidence: FP64 near-field vs mixed + local, plain ring
+                  step and learned right preconditioners (the library's
+                  default weights, trained on 48 other generated bodies)
 
 ``e2e`` times the headline through the public API (monostatic_rcs_sweep)
 with host buffers: mesh/RWG/incidence upload and the sigma download inside
@@ -521,39 +522,42 @@ def run_ours(args):
     if not args.quick and any(want(n) for n in ("c5_fp64_nf_lu", "c5_mixed_nf_lu", "c5_mixed_learned",
                                                  "c5_mixed_local")):
         r_nb = 0.2 * LAM
-        tdev = None
-        losses = []
-        t0 = time.perf_counter()
-        for seed in (11, 12, 13):   # training bodies (untimed setup)
-            body = make_perturbed_ellipsoid(LAM, seed, frequency=8)
-            brwg = build_rwg(body)
-            if tdev is None:
-                tdev = EFIEDevice(body, brwg, device=local)
-            else:
-                tdev.upload(body, brwg)
-            tdev.assemble(K, precision="mixed")
-            losses.append([tdev.train_network(r_nb, epochs=3, batch=256, lr=3e-3, seed=seed) for _ in range(2)])
-        train_s = time.perf_counter() - t0
+        from diffmom_b200.learned import DEFAULT_WEIGHTS
         body = make_perturbed_ellipsoid(LAM, 99, frequency=18)
         brwg = build_rwg(body)
-        tdev.upload(body, brwg)
-        for name, prec, pc, cut, side in (
-                ("c5_fp64_nf_lu", nat.PREC_FP64, nat.PRECOND_NF_LU, 1.0 * LAM, 0),
-                ("c5_mixed_nf_lu", nat.PREC_MIXED, nat.PRECOND_NF_LU, 1.0 * LAM, 0),
-                ("c5_mixed_local", nat.PREC_MIXED, nat.PRECOND_LOCAL_INV, r_nb, 1),
-                ("c5_mixed_learned", nat.PREC_MIXED, nat.PRECOND_LEARNED, r_nb, 1)):
-            if not want(name):
-                continue
-            p = solve_params(nat, K, prec, pc, cut, side=side, maxiter=600)
-            st = nat.GmresStats()
+        tdev = EFIEDevice(body, brwg, device=local)
+        # the library's default weights: trained on the GPU over 48 generated
+        # bodies (python -m diffmom_b200.learned), none of them this one
+        net_note = "default weights (48 generated training bodies)"
+        if DEFAULT_WEIGHTS.exists():
+            tdev.load_network(DEFAULT_WEIGHTS)
+        else:
+            from diffmom_b200.learned import train_learned_network, training_bodies
+            rep = train_learned_network(tdev, training_bodies(16))
+            net_note = f"trained here (untimed) on 16 generated bodies, {rep.gpu_s:.1f} s"
+            tdev.upload(body, brwg)
+        for freq_f, tag in ((18, "c5"), (24, "c5_17k")):
+            if freq_f != 18:
+                body = make_perturbed_ellipsoid(LAM, 99, frequency=freq_f)
+                brwg = build_rwg(body)
+                tdev.upload(body, brwg)
+            cases = [("c5_fp64_nf_lu", nat.PREC_FP64, nat.PRECOND_NF_LU, 1.0 * LAM, 0),
+                     ("c5_mixed_nf_lu", nat.PREC_MIXED, nat.PRECOND_NF_LU, 1.0 * LAM, 0)] if tag == "c5" else []
+            cases += [(f"{tag}_mixed_local", nat.PREC_MIXED, nat.PRECOND_LOCAL_INV, r_nb, 1),
+                      (f"{tag}_mixed_ring", nat.PREC_MIXED, nat.PRECOND_RING, r_nb, 1),
+                      (f"{tag}_mixed_learned", nat.PREC_MIXED, nat.PRECOND_LEARNED, r_nb, 1)]
+            for name, prec, pc, cut, side in cases:
+                if not want(name) and not want(name.replace("c5_17k", "c5")):
+                    continue
+                st = nat.GmresStats()
+                p = solve_params(nat, K, prec, pc, cut, side=side, maxiter=600)
 
-            def step(p=p, st=st):
-                tdev.ctx.call("dmb_solve_resident", ctypes.byref(p), ctypes.byref(st))
-                return st.niter, st.true_residual
-            variants[name] = run.timed(tdev, step, min(args.steps, 5), args.warmup, 1)
-        for name in variants:
-            if name.startswith("c5_"):
-                variants[name]["training_s_untimed"] = train_s
+                def step(p=p, st=st):
+                    tdev.ctx.call("dmb_solve_resident", ctypes.byref(p), ctypes.byref(st))
+                    return st.niter, st.true_residual
+                variants[name] = run.timed(tdev, step, min(args.steps, 5), args.warmup, 1)
+                variants[name]["N_rwg"] = brwg.nedges
+                variants[name]["network"] = net_note
         tdev.close()
 
     line = make_line(args, ws, N, mesh, head, variants, e2e) if rank == 0 else None
@@ -603,6 +607,8 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
     for a, b in (("c4_batch64_mixed", "c4_batch64_fp64"), ("c4_batch64_fp64", "c4_batch64_fp64_1lane"),
                  ("c2_mixed_nf_lu", "c2_fp64_nf_lu"), ("c5_mixed_learned", "c5_fp64_nf_lu"),
                  ("c5_mixed_nf_lu", "c5_fp64_nf_lu"), ("c5_mixed_local", "c5_fp64_nf_lu"),
+                 ("c5_mixed_learned", "c5_mixed_local"), ("c5_mixed_learned", "c5_mixed_ring"),
+                 ("c5_17k_mixed_learned", "c5_17k_mixed_local"), ("c5_17k_mixed_learned", "c5_17k_mixed_ring"),
                  ("plate_1wave_dense_mixed", "plate_1wave_aca")):
         if "solves_per_s" in variants.get(a, {}) and "solves_per_s" in variants.get(b, {}):
             speed[f"{a}_vs_{b}"] = variants[a]["solves_per_s"] / variants[b]["solves_per_s"]

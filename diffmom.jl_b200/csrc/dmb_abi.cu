@@ -78,7 +78,8 @@ dmb_status dmb_ctx_destroy(dmb_ctx *c) {
                       &c->d_tminus, &c->d_vpo, &c->d_vmo, &c->d_len, &c->d_ap, &c->d_am,
                       &c->d_slot_rwg, &c->d_slot_side, &c->d_wq, &c->d_centers, &c->d_adj_off,
                       &c->d_adj_nb, &c->d_near_rec, &c->d_near_val, &c->d_near_entry_mn,
-                      &c->d_near_entry_off, &c->d_Z, &c->d_F, &c->d_dinv, &c->d_W,
+                      &c->d_near_entry_off, &c->d_near_row_off, &c->d_near_row_ent, &c->d_near_row_col,
+                      &c->d_near_entry_sum, &c->d_Z, &c->d_F, &c->d_dinv, &c->d_W,
                       &c->d_flags, &c->d_li_idx, &c->d_li_cnt, &c->d_li_inv, &c->d_net, &c->d_V,
                       &c->d_H, &c->d_work, &c->d_vecs, &c->d_scal};
     for (DevBuf *b : bufs) b->release();
@@ -700,6 +701,8 @@ void resident_precond(dmb_ctx *c, const dmb_solve_params *p) {
     dmb::nf_build(c, p->cutoff, p->precond_kind);
   } else if (p->precond_kind == DMB_PRECOND_LOCAL_INV) {
     dmb::local_inverse_build(c, p->cutoff, 64);
+  } else if (p->precond_kind == DMB_PRECOND_RING) {
+    dmb::ring_step_build(c, p->cutoff, false);
   } else if (p->precond_kind == DMB_PRECOND_LEARNED) {
     dmb::learned_build(c, p->cutoff);
   }

@@ -588,9 +588,34 @@ void build_host_topology(dmb_ctx *c) {
   up(c->d_adj_off, c->adj_off.data(), c->adj_off.size() * 4);
   up(c->d_adj_nb, c->adj_nb.data(), c->adj_nb.size() * 4);
   up(c->d_rwg_slot, rslot.data(), rslot.size() * 4);
+  // per RWG row: the near entries that touch it (as m or as n), in entry
+  // order, with the other index
+  std::vector<int64_t> roff(N + 1, 0);
+  for (auto &e : ent) {
+    roff[e.x + 1]++;
+    if (e.x != e.y) roff[e.y + 1]++;
+  }
+  for (int64_t m = 0; m < N; m++) roff[m + 1] += roff[m];
+  std::vector<int32_t> rent(roff[N]), rcol(roff[N]);
+  {
+    std::vector<int64_t> cur(roff.begin(), roff.end() - 1);
+    for (size_t e = 0; e < ent.size(); e++) {
+      const int32_t m = ent[e].x, n = ent[e].y;
+      rent[cur[m]] = (int32_t)e;
+      rcol[cur[m]++] = n;
+      if (m != n) {
+        rent[cur[n]] = (int32_t)e;
+        rcol[cur[n]++] = m;
+      }
+    }
+  }
   up(c->d_near_rec, recs.data(), recs.size() * sizeof(NearRec));
   up(c->d_near_entry_mn, ent.data(), ent.size() * sizeof(int2));
   up(c->d_near_entry_off, eoff.data(), eoff.size() * sizeof(int64_t));
+  up(c->d_near_row_off, roff.data(), roff.size() * sizeof(int64_t));
+  up(c->d_near_row_ent, rent.data(), rent.size() * 4);
+  up(c->d_near_row_col, rcol.data(), rcol.size() * 4);
+  c->d_near_entry_sum.ensure(std::max<size_t>(16, ent.size() * sizeof(double2)));
   c->d_near_val.ensure(std::max<size_t>(16, recs.size() * sizeof(double2)));
   up(c->d_slot_rwg, slot_rwg.data(), slot_rwg.size() * 4);
   up(c->d_slot_side, slot_side.data(), slot_side.size() * 4);

@@ -492,22 +492,27 @@ __global__ void k_mf_gather(int64_t N, const int *__restrict__ rslot, const doub
   y[m] = cadd(Ys[rslot[2 * m]], Ys[rslot[2 * m + 1]]);
 }
 
-// near entries: y[m] += v x[n]; y[n] += v x[m] (m != n)
-__global__ void k_mf_near(int64_t nent, const int2 *__restrict__ mn, const int64_t *__restrict__ off,
-                          const double2 *__restrict__ vals, const double2 *__restrict__ x, double2 *__restrict__ y) {
+// value of each near entry: its records summed in order (once per prepared
+// operator)
+__global__ void k_near_entry_sum(int64_t nent, const int64_t *__restrict__ off, const double2 *__restrict__ vals,
+                                 double2 *__restrict__ esum) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nent) return;
   double2 v = make_double2(0, 0);
   for (int64_t r = off[e]; r < off[e + 1]; r++) v = cadd(v, vals[r]);
-  int2 p = mn[e];
-  double2 a = cmul(v, x[p.y]);
-  atomicAdd(&y[p.x].x, a.x);
-  atomicAdd(&y[p.x].y, a.y);
-  if (p.x != p.y) {
-    double2 b = cmul(v, x[p.x]);
-    atomicAdd(&y[p.y].x, b.x);
-    atomicAdd(&y[p.y].y, b.y);
-  }
+  esum[e] = v;
+}
+
+// near part per row, in the row's fixed entry order: y[m] += sum v_e x[other]
+// (one thread per row, no atomics: repeated products are bitwise equal)
+__global__ void k_mf_near_rows(int64_t N, const int64_t *__restrict__ roff, const int *__restrict__ rent,
+                               const int *__restrict__ rcol, const double2 *__restrict__ esum,
+                               const double2 *__restrict__ x, double2 *__restrict__ y) {
+  int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  double2 acc = make_double2(0, 0);
+  for (int64_t q = roff[m]; q < roff[m + 1]; q++) acc = cadd(acc, cmul(esum[rent[q]], x[rcol[q]]));
+  y[m] = cadd(y[m], acc);
 }
 
 __global__ void k_times_minus_i_w(int64_t N, double w, double2 *__restrict__ y) {
@@ -646,10 +651,13 @@ void matvec_free_dev(dmb_ctx *c, const double *x, double *y) {
              ys.as<double2>());
   DMB_LAUNCH(c, k_mf_gather, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(), ys.as<double2>(),
              (double2 *)y);
-  if (c->n_near_entry > 0)
-    DMB_LAUNCH(c, k_mf_near, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
-               c->d_near_entry_mn.as<int2>(), c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(),
+  if (c->n_near_entry > 0) {
+    DMB_LAUNCH(c, k_near_entry_sum, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
+               c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(), c->d_near_entry_sum.as<double2>());
+    DMB_LAUNCH(c, k_mf_near_rows, blocks_for(N, 256), 256, 0, N, c->d_near_row_off.as<int64_t>(),
+               c->d_near_row_ent.as<int>(), c->d_near_row_col.as<int>(), c->d_near_entry_sum.as<double2>(),
                (const double2 *)x, (double2 *)y);
+  }
   DMB_LAUNCH(c, k_times_minus_i_w, blocks_for(N, 256), 256, 0, N, c->k * c->eta0, (double2 *)y);
   DMB_CUDA(cudaStreamSynchronize(c->stream));
 }
@@ -708,10 +716,13 @@ extern "C" dmb_status dmb_matvec_free_noalloc(dmb_ctx *c, const double *x_dev, d
     DMB_LAUNCH(c, k_mf_far, (unsigned)nt, 256, 0, (int)nt, c->nq, c->d_tcache.as<TriCache>(),
                c->d_adj_off.as<int>(), c->d_adj_nb.as<int>(), c->k, 1.0 / (c->k * c->k), xs, ys);
     DMB_LAUNCH(c, k_mf_gather, blocks_for(N, 256), 256, 0, N, c->d_rwg_slot.as<int>(), ys, (double2 *)y_dev);
-    if (c->n_near_entry > 0)
-      DMB_LAUNCH(c, k_mf_near, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
-                 c->d_near_entry_mn.as<int2>(), c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(),
+    if (c->n_near_entry > 0) {
+      DMB_LAUNCH(c, k_near_entry_sum, blocks_for(c->n_near_entry, 256), 256, 0, c->n_near_entry,
+                 c->d_near_entry_off.as<int64_t>(), c->d_near_val.as<double2>(), c->d_near_entry_sum.as<double2>());
+      DMB_LAUNCH(c, k_mf_near_rows, blocks_for(N, 256), 256, 0, N, c->d_near_row_off.as<int64_t>(),
+                 c->d_near_row_ent.as<int>(), c->d_near_row_col.as<int>(), c->d_near_entry_sum.as<double2>(),
                  (const double2 *)x_dev, (double2 *)y_dev);
+    }
     DMB_LAUNCH(c, k_times_minus_i_w, blocks_for(N, 256), 256, 0, N, c->k * c->eta0, (double2 *)y_dev);
     DMB_CUDA(cudaStreamSynchronize(c->stream));
     c->err.clear();

@@ -222,9 +222,69 @@ __device__ __forceinline__ void ldlt_diag_block(int64_t N, int64_t j, int b, C *
     }
 }
 
+// Elimination of the 16 x 16 diagonal sub-block at s0 by one warp, all in
+// registers: lane (ih = lane >> 4, c = lane & 15) holds rows i = ih + 2 m
+// (m = 0..7) of column c.  The block is kept in full (both triangles: it is
+// complex symmetric and every update keeps it so), which puts each value a
+// pivot step needs -- the pivot, A[k][c] = A[c][k], X[k][c] and A[i][k] -- in
+// a register whose index is known at compile time on a lane known per lane,
+// so one shuffle fetches it; no shared memory, no warp barriers.  On return
+// the lower triangle holds L (strict) and D, X the unit-lower inverse.
+// 1/d = conj(d) / |d|^2 with one reciprocal on the serial path; a pivot whose
+// |d|^2 is zero, non-finite or outside the FP32 range (|d| below ~1e-19 or
+// above ~1e19) is a breakdown (false, uniform over the warp).
+__device__ __forceinline__ bool elim16_warp(float2 (*A)[65], float2 (*Xs)[17], int s0, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  const int c = lane & 15, ih = lane >> 4;
+  float2 a[8], x[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    const int i = ih + 2 * m;
+    a[m] = (c <= i) ? A[s0 + i][s0 + c] : A[s0 + c][s0 + i];
+    x[m] = (i == c) ? make_float2(1.f, 0.f) : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    const int kl = (k & 1) << 4, km = k >> 1;  // row k lives on lanes kl | col, register km
+    float2 d;
+    d.x = __shfl_sync(FULL, a[km].x, kl | k);
+    d.y = __shfl_sync(FULL, a[km].y, kl | k);
+    const float d2 = d.x * d.x + d.y * d.y;
+    if (!(d2 > 0.f) || !isfinite(d2)) return false;
+    const float rd = __frcp_rn(d2);
+    const float2 inv_d = make_float2(d.x * rd, -d.y * rd);
+    float2 akc, xk;
+    akc.x = __shfl_sync(FULL, a[km].x, kl | c);
+    akc.y = __shfl_sync(FULL, a[km].y, kl | c);
+    xk.x = __shfl_sync(FULL, x[km].x, kl | c);  // X[k][c], final at step k
+    xk.y = __shfl_sync(FULL, x[km].y, kl | c);
+    const float2 lc = cmul(akc, inv_d);  // L[c][k] (c > k)
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      const int i = ih + 2 * m;
+      float2 aik;  // A[i][k]: lane (ih << 4) | k, register m
+      aik.x = __shfl_sync(FULL, a[m].x, (ih << 4) | k);
+      aik.y = __shfl_sync(FULL, a[m].y, (ih << 4) | k);
+      if (i > k) {
+        const float2 lik = cmul(aik, inv_d);
+        if (c > k) a[m] = csub(a[m], cmul(aik, lc));
+        else if (c == k) a[m] = lik;  // L[i][k]
+        x[m] = csub(x[m], cmul(lik, xk));
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    const int i = ih + 2 * m;
+    if (c <= i) A[s0 + i][s0 + c] = a[m];
+    Xs[i][c] = x[m];
+  }
+  return true;
+}
+
 // Blocked form of ldlt_diag_block for complex64 blocks (same results up to
 // rounding): four 16-wide sub-panels; warp 0 eliminates the 16 x 16 diagonal
-// sub-block with warp-level synchronisation only (and forms its unit-lower
+// sub-block in registers (elim16_warp, which also forms its unit-lower
 // inverse), then the CTA computes the sub-panel below it and the trailing
 // update.  The 64 x 64 inverse is assembled from the four 16 x 16 inverses by
 // block forward substitution.  About 20 CTA barriers instead of 128.
@@ -264,50 +324,11 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
   for (int s = 0; s < 4; s++) {
     const int s0 = 16 * s;
     if (t < 32) {
-      // lane owns sub-block elements (i, c) = ((lane >> 4) + 2 m, lane & 15)
-      const int c = t & 15, ih = t >> 4;
-#pragma unroll
-      for (int m = 0; m < 8; m++) {
-        const int i = ih + 2 * m;
-        Xd[s][i][c] = (i == c) ? make_float2(1.f, 0.f) : make_float2(0.f, 0.f);
-      }
-      __syncwarp();
-      for (int k = 0; k < 16; k++) {
-        // 1/d = conj(d) / |d|^2 with one reciprocal on the serial path; a
-        // pivot whose |d|^2 is zero, non-finite or outside the FP32 range
-        // (|d| below ~1e-19 or above ~1e19) counts as a breakdown
-        const float2 d = A[s0 + k][s0 + k];
-        const float d2 = d.x * d.x + d.y * d.y;
-        if (!(d2 > 0.f) || !isfinite(d2)) {  // uniform over the warp
-          if (t == 0) {
-            atomicOr(err, 2u);
-            *bad = 1;
-          }
-          break;
+      if (!elim16_warp(A, Xd[s], s0, t)) {  // uniform over the warp
+        if (t == 0) {
+          atomicOr(err, 2u);
+          *bad = 1;
         }
-        const float rd = __frcp_rn(d2);
-        const float2 inv_d = make_float2(d.x * rd, -d.y * rd);
-        const float2 lc = cmul(A[s0 + c][s0 + k], inv_d);  // L[c][k] (c > k)
-        const float2 xk = Xd[s][k][c];                     // X[k][c], final at step k
-        float2 na[8], nx[8];
-#pragma unroll
-        for (int m = 0; m < 8; m++) {
-          const int i = ih + 2 * m;
-          const float2 aik = A[s0 + i][s0 + k];
-          na[m] = A[s0 + i][s0 + c];
-          nx[m] = Xd[s][i][c];
-          if (c > k && c <= i) na[m] = csub(na[m], cmul(aik, lc));
-          if (c == k && i > k) na[m] = cmul(aik, inv_d);
-          if (i > k) nx[m] = csub(nx[m], cmul(cmul(aik, inv_d), xk));
-        }
-        __syncwarp();
-#pragma unroll
-        for (int m = 0; m < 8; m++) {
-          const int i = ih + 2 * m;
-          if (c <= i) A[s0 + i][s0 + c] = na[m];
-          Xd[s][i][c] = nx[m];
-        }
-        __syncwarp();
       }
     }
     __syncthreads();
@@ -1598,7 +1619,7 @@ void pc_apply_dev(dmb_ctx *c, double *x, int64_t nrhs) {
     }
     return;
   }
-  if (c->pc_kind == DMB_PRECOND_LOCAL_INV || c->pc_kind == DMB_PRECOND_LEARNED) {
+  if (c->pc_kind == DMB_PRECOND_LOCAL_INV || c->pc_kind == DMB_PRECOND_LEARNED || c->pc_kind == DMB_PRECOND_RING) {
     dmb::local_apply_dev(c, x, nrhs);
     return;
   }

@@ -213,6 +213,10 @@ struct dmb_ctx {
   std::vector<int32_t> adj_off, adj_nb;
   DevBuf d_adj_off, d_adj_nb;
   DevBuf d_near_rec, d_near_val, d_near_entry_mn, d_near_entry_off;
+  // the near entries touching each RWG row (CSR, entry order) and the summed
+  // value of each entry: the matrix-free product gathers its near part per
+  // row in a fixed order (no atomics)
+  DevBuf d_near_row_off, d_near_row_ent, d_near_row_col, d_near_entry_sum;
   int64_t n_near_rec = 0, n_near_entry = 0;
 
   // impedance matrix (row-major == column-major since Z is symmetric)

@@ -16,7 +16,10 @@
 //
 // Learned step.  A small network reads per-neighbour features (relative
 // position, block coupling, local-inverse entry, ring gradient) and predicts a
-// complex modulation o_j of the direction, d_j = g_j (1 + o_j).  It is trained
+// complex modulation o_j of the direction; the step searches the plane of g
+// and g o exactly (2 x 2 least squares on the ring residual), so it is never
+// worse than the plain step and reaches the target row when o is ideal
+// (d_j = g_j (1 + o_j) with the plain step's eta).  It is trained
 // on the GPU by the kernels below toward the least-squares rows
 // t = argmin ||Z[E_m, S_m] t - e_m|| (exact local solves the method generates):
 // the ideal modulation is o*_j = (z_j - t_j) / (eta g_j) - 1 (clipped), weighted
@@ -434,6 +437,86 @@ __global__ void __launch_bounds__(128) k_ring_step(int64_t N, const ZC *__restri
   }
 }
 
+// Learned step with a two-direction line search: d1 = g and d2 = g o (the
+// network's per-entry modulation); (alpha, beta) minimise the ring residual
+// ||r - B (alpha d1 + beta d2)|| exactly (2 x 2 normal equations), so the
+// learned step is never worse than the plain step on any row (beta = 0 is
+// one of its choices), and with the ideal modulation (alpha = beta = eta) it
+// lands on the least-squares row.  A degenerate pair (q2 parallel to q1, or
+// zero) falls back to the plain step.
+template <class ZC>
+__global__ void __launch_bounds__(128) k_ring_step2(int64_t N, const ZC *__restrict__ Z, const int *__restrict__ idx_s,
+                                                    const int *__restrict__ cnt_s, const int *__restrict__ idx_e,
+                                                    const int *__restrict__ cnt_e, const double2 *__restrict__ rows,
+                                                    const double2 *__restrict__ rring, const double2 *__restrict__ grad,
+                                                    const float *__restrict__ o, double2 *__restrict__ rows_out) {
+  __shared__ int si[KS], ei[KL];
+  __shared__ double2 d1[KS], d2[KS];
+  __shared__ double red[4][8];
+  __shared__ double2 s_ab[2];
+  const int64_t m = blockIdx.x;
+  const int ks = cnt_s[m], ke = cnt_e[m];
+  for (int i = threadIdx.x; i < ks; i += blockDim.x) {
+    si[i] = idx_s[m * KS + i];
+    const double2 g = grad[m * KS + i];
+    d1[i] = g;
+    d2[i] = cmul(g, make_double2(o[(m * KS + i) * 2], o[(m * KS + i) * 2 + 1]));
+  }
+  for (int i = threadIdx.x; i < ke; i += blockDim.x) ei[i] = idx_e[m * KL + i];
+  __syncthreads();
+  // a11 = |q1|^2, a22 = |q2|^2, a12 = q1^H q2, h1 = q1^H r, h2 = q2^H r
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int e = threadIdx.x; e < ke; e += blockDim.x) {
+    double2 q1 = make_double2(0, 0), q2 = make_double2(0, 0);
+    for (int j = 0; j < ks; j++) {
+      const double2 z = to_d2(Z[(int64_t)ei[e] * N + si[j]]);
+      cfma(q1, z, d1[j]);
+      cfma(q2, z, d2[j]);
+    }
+    const double2 re = rring[m * KL + e];
+    const double2 a12 = cmul(cconj(q1), q2), h1 = cmul(cconj(q1), re), h2 = cmul(cconj(q2), re);
+    acc[0] += cabs2(q1);
+    acc[1] += cabs2(q2);
+    acc[2] += a12.x;
+    acc[3] += a12.y;
+    acc[4] += h1.x;
+    acc[5] += h1.y;
+    acc[6] += h2.x;
+    acc[7] += h2.y;
+  }
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    acc[q] = warp_sum(acc[q]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32][q] = acc[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[8];
+    for (int q = 0; q < 8; q++) t[q] = red[0][q] + red[1][q] + red[2][q] + red[3][q];
+    const double a11 = t[0], a22 = t[1];
+    const double2 a12 = make_double2(t[2], t[3]), h1 = make_double2(t[4], t[5]), h2 = make_double2(t[6], t[7]);
+    const double det = a11 * a22 - cabs2(a12);
+    double2 al = make_double2(0, 0), be = make_double2(0, 0);
+    if (a11 > 0 && a22 > 0 && det > 1e-10 * a11 * a22) {
+      // Cramer: alpha = (a22 h1 - a12 h2) / det, beta = (a11 h2 - conj(a12) h1) / det
+      const double2 na = csub(cscale(h1, a22), cmul(a12, h2));
+      const double2 nb = csub(cscale(h2, a11), cmul(cconj(a12), h1));
+      al = cscale(na, 1.0 / det);
+      be = cscale(nb, 1.0 / det);
+    } else if (a11 > 0) {
+      al = cscale(h1, 1.0 / a11);
+    }
+    s_ab[0] = al;
+    s_ab[1] = be;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < KS; j += blockDim.x) {
+    double2 v = make_double2(0, 0);
+    if (j < ks) v = csub(csub(rows[m * KS + j], cmul(s_ab[0], d1[j])), cmul(s_ab[1], d2[j]));
+    rows_out[m * KS + j] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // network features (per neighbour j of row m):
 //   0-2 (c_j - c_m)/r, 3 |c_j - c_m|/r, 4-5 Z[m][j]/Z[m][m], 6-7 z_j/z_m,
@@ -767,11 +850,23 @@ void ring_grad(dmb_ctx *c) {
 }
 
 // one line-searched ring step of the rows along g (1 + o); rows_s updated in
-// place through rows_corr; eta recorded
+// place through rows_corr; eta recorded.  With the network's modulation o the
+// step searches the plane of g and g o (k_ring_step2).
 void ring_step(dmb_ctx *c, const float *o) {
   LocalState &st = lstate(c);
   st.rows_corr.ensure(sizeof(double2) * c->n * KS);
   st.eta.ensure(sizeof(double2) * c->n);
+  if (o) {
+    if (c->z_prec == DMB_PREC_FP64)
+      DMB_LAUNCH(c, k_ring_step2<double2>, (unsigned)c->n, 128, 0, c->n, c->d_Z.as<double2>(), st.idx_s.as<int>(),
+                 st.cnt_s.as<int>(), st.idx_l.as<int>(), st.cnt_l.as<int>(), st.rows_s.as<double2>(),
+                 st.rring.as<double2>(), st.gring.as<double2>(), o, st.rows_corr.as<double2>());
+    else
+      DMB_LAUNCH(c, k_ring_step2<float2>, (unsigned)c->n, 128, 0, c->n, c->d_Z.as<float2>(), st.idx_s.as<int>(),
+                 st.cnt_s.as<int>(), st.idx_l.as<int>(), st.cnt_l.as<int>(), st.rows_s.as<double2>(),
+                 st.rring.as<double2>(), st.gring.as<double2>(), o, st.rows_corr.as<double2>());
+    return;
+  }
   if (c->z_prec == DMB_PREC_FP64)
     DMB_LAUNCH(c, k_ring_step<double2>, (unsigned)c->n, 128, 0, c->n, c->d_Z.as<double2>(), st.idx_s.as<int>(),
                st.cnt_s.as<int>(), st.idx_l.as<int>(), st.cnt_l.as<int>(), st.rows_s.as<double2>(),
@@ -861,7 +956,7 @@ void ring_step_build(dmb_ctx *c, double radius, bool learned) {
   DMB_CUDA(cudaMemcpyAsync(st.rows_s.p, st.rows_corr.p, sizeof(double2) * c->n * KS, cudaMemcpyDeviceToDevice,
                            c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
-  c->pc_kind = learned ? DMB_PRECOND_LEARNED : DMB_PRECOND_LOCAL_INV;
+  c->pc_kind = learned ? DMB_PRECOND_LEARNED : DMB_PRECOND_RING;
   c->tm.precond_ms = now_ms() - t0;
 }
 

@@ -36,6 +36,7 @@ PRECOND_NF_LU = 1
 PRECOND_NF_DIAG = 2
 PRECOND_LOCAL_INV = 3
 PRECOND_LEARNED = 4
+PRECOND_RING = 5
 
 SIDE_LEFT = 0
 SIDE_RIGHT = 1

@@ -176,7 +176,7 @@ class EFIEDevice:
         if mode not in codes:
             raise ValueError(f"unknown local preconditioner mode {mode!r}")
         self.ctx.call("dmb_local_build", float(radius), codes[mode])
-        kind = nat.PRECOND_LEARNED if mode == "learned" else nat.PRECOND_LOCAL_INV
+        kind = {"learned": nat.PRECOND_LEARNED, "ring": nat.PRECOND_RING}.get(mode, nat.PRECOND_LOCAL_INV)
         self.preconditioner = NearFieldPreconditionerData(self, kind, float(radius), 64.0 / self.N)
         return self.preconditioner
 
@@ -292,7 +292,7 @@ class EFIEDevice:
 
     # -- batched resident solve -------------------------------------------
     _PC_CODES = {"none": nat.PRECOND_NONE, "lu": nat.PRECOND_NF_LU, "diag": nat.PRECOND_NF_DIAG,
-                 "local": nat.PRECOND_LOCAL_INV, "learned": nat.PRECOND_LEARNED}
+                 "local": nat.PRECOND_LOCAL_INV, "learned": nat.PRECOND_LEARNED, "ring": nat.PRECOND_RING}
 
     def solve_many(self, k: float, kvecs, pols, E0s=None, precision: str = "mixed",
                    preconditioner: str = "lu", cutoff: float = math.inf, tol: float = 1e-6,

@@ -54,6 +54,7 @@ typedef int dmb_status;
 #define DMB_PRECOND_NF_DIAG 2    /* Jacobi on the diagonal, 1e-10*max floor */
 #define DMB_PRECOND_LOCAL_INV 3  /* per-RWG near-block local inverses */
 #define DMB_PRECOND_LEARNED 4    /* learned correction of the local inverses */
+#define DMB_PRECOND_RING 5       /* plain ring-step correction of the local inverses */
 
 #define DMB_SIDE_LEFT 0
 #define DMB_SIDE_RIGHT 1
@@ -243,7 +244,8 @@ dmb_status dmb_nf_apply(dmb_ctx *ctx, const double *x, double *y, int64_t nrhs);
  *           modulation (DMB_PRECOND_LEARNED).
  *   mode 2: least-squares rows min || Z[E_m, S_m] z - e_m || (the exact rows
  *           the network is trained toward).
- *   mode 3: local inverse + one plain line-searched ring step (o = 0). */
+ *   mode 3: local inverse + one plain line-searched ring step (o = 0)
+ *           (DMB_PRECOND_RING): the learned method without its network. */
 dmb_status dmb_local_build(dmb_ctx *ctx, double radius, int mode);
 /* Train the network on the current body (resident Z): features of the
  * local-inverse rows and their ring gradients as input; targets from the
