@@ -240,6 +240,194 @@ __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TC_BN) : "memory");
 }
 
+// Persistent form of k_tc_syrk (autotuner candidate): a grid of at most one
+// CTA per SM walks the lower tiles of the update (column tile outer, row
+// tiles inner, tiles above the diagonal never launched) with 6 warps:
+//   warp 4 / lane 0   TMA producer over (tile, K chunk) into a 4-stage ring;
+//   warp 5 / lane 0   tcgen05.mma (M 128, N 256, K 8) into one of two
+//                     256-column TMEM accumulators, in turn, so the next tile
+//                     accumulates while the last one drains;
+//   warps 0-3         drain: tcgen05.ld, stage through shared memory,
+//                     C -= acc on c <= r, release the accumulator.
+// Same MMA sequence per tile as k_tc_syrk, so the same bits.  Every wait is
+// bounded (error bit, abort flag, TMEM freed).
+constexpr int TCP_STAGES = 4;
+constexpr int TCP_E_BYTES = TC_BM * 33 * 4;
+constexpr int TCP_SMEM = TCP_STAGES * (TC_A_STAGE + TC_B_STAGE) + TCP_E_BYTES + 256 + 1024;
+
+__device__ __forceinline__ void tcp_tile(int64_t t, int nrt, int nct, int &rt, int &ct) {
+  for (ct = 0; ct < nct; ct++) {
+    const int64_t n = nrt - 4 * ct;
+    if (n <= 0) break;
+    if (t < n) {
+      rt = (int)(4 * ct + t);
+      return;
+    }
+    t -= n;
+  }
+  rt = -1;
+}
+
+__device__ __forceinline__ void tcp_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tcp_epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__global__ void __launch_bounds__(192, 1) k_tc_syrk_p(const __grid_constant__ CUtensorMap tmA,
+                                                      const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
+                                                      int64_t N, int64_t j0, int64_t c_hi, int nchunks, int cpb,
+                                                      int nrt, int nct, int64_t ntiles, unsigned *err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char *gbase = smem_raw + (base - raw);
+  const uint32_t sA = base;
+  const uint32_t sB = base + TCP_STAGES * TC_A_STAGE;
+  float *E = reinterpret_cast<float *>(gbase + TCP_STAGES * (TC_A_STAGE + TC_B_STAGE));
+  const uint32_t sBar = sB + TCP_STAGES * TC_B_STAGE + TCP_E_BYTES;
+  uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
+  volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
+  volatile int *epi_ok = reinterpret_cast<volatile int *>(bar_ptr + 18);
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * TCP_STAGES, accf0 = sBar + 16 * TCP_STAGES, acce0 = accf0 + 16;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TCP_STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, 1);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(const_cast<uint32_t *>(tmem_slot))),
+                 "r"(2 * TC_BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = *tmem_slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      long long t = 0;
+      bool go = true;
+      for (int64_t tile = blockIdx.x; tile < ntiles && go; tile += gridDim.x) {
+        int rt, ct;
+        tcp_tile(tile, nrt, nct, rt, ct);
+        const int64_t row0 = (int64_t)rt * 64, col0 = (int64_t)ct * TC_BN;
+        for (int kc = 0; kc < nchunks; kc++, t++) {
+          const int s = (int)(t % TCP_STAGES);
+          if (*abort_flag || (t >= TCP_STAGES &&
+                              !mbar_wait(empty0 + 8 * s, (uint32_t)((t / TCP_STAGES) - 1) & 1u, err, abort_flag))) {
+            go = false;
+            break;
+          }
+          mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
+          const int kx = tc_kx(kc, cpb);
+          tma_load_2d(sA + s * TC_A_STAGE, &tmA, kx, (int)(2 * row0), full0 + 8 * s);
+          tma_load_2d(sB + s * TC_B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
+        }
+      }
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      long long t = 0;
+      int i = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, i++) {
+        const int buf = i & 1;
+        if (i >= 2 && !mbar_wait(acce0 + 8 * buf, (uint32_t)((i >> 1) - 1) & 1u, err, abort_flag)) {
+          ok = false;
+          break;
+        }
+        const uint32_t tmem_acc = tmem_d + (uint32_t)(buf * TC_BN);
+        for (int kc = 0; kc < nchunks; kc++, t++) {
+          const int s = (int)(t % TCP_STAGES);
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / TCP_STAGES) & 1u, err, abort_flag)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+          for (int k = 0; k < TC_BK / 8; k++) {
+            const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
+            const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
+            umma_tf32(tmem_acc, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+          }
+          umma_commit(empty0 + 8 * s);
+        }
+        if (ok) umma_commit(accf0 + 8 * buf);
+      }
+    }
+  } else {
+    // drain warps 0-3 (warp w reads TMEM lanes 32w..32w+31)
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    int i = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+      const int buf = i & 1;
+      int rt, ct;
+      tcp_tile(tile, nrt, nct, rt, ct);
+      const int64_t row0 = (int64_t)rt * 64, col0 = (int64_t)ct * TC_BN;
+      const bool got = mbar_wait(accf0 + 8 * buf, (uint32_t)(i >> 1) & 1u, err, abort_flag);
+      if (threadIdx.x == 0) *epi_ok = 1;
+      tcp_epi_sync();
+      if (!got) *epi_ok = 0;
+      tcp_epi_sync();
+      if (!*epi_ok) break;  // uniform over the drain warps
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tmem_acc = tmem_d + (uint32_t)(buf * TC_BN);
+      for (int cc = 0; cc < TC_BN / 32; cc++) {
+        uint32_t v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(tmem_acc + lane_base + (uint32_t)(cc * 32)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int row = warp * 32 + lane;
+#pragma unroll
+        for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
+        tcp_epi_sync();
+        const int q = threadIdx.x & 31, rr = threadIdx.x >> 5;
+        const int64_t gc = j0 + col0 + cc * 32 + q;
+        float2 cv[16];
+#pragma unroll
+        for (int r16 = 0; r16 < 16; r16++) {
+          const int64_t gr = j0 + row0 + rr + 4 * r16;
+          cv[r16] = (gr < N && gc < c_hi && gc <= gr) ? F[gr * N + gc] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int r16 = 0; r16 < 16; r16++) {
+          const int r = rr + 4 * r16;
+          const int64_t gr = j0 + row0 + r;
+          if (gr < N && gc < c_hi && gc <= gr)
+            F[gr * N + gc] = make_float2(cv[r16].x - E[r * 33 + q], cv[r16].y - E[(64 + r) * 33 + q]);
+        }
+        tcp_epi_sync();
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      tcp_epi_sync();
+      if (threadIdx.x == 0) tcp_arrive(acce0 + 8 * buf);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * TC_BN) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // General complex GEMM  Y (op)= A B^T  for many right-hand sides.
 //
@@ -556,6 +744,7 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   if (!st.attr) {
     DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(4)));
     DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(2)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk_p, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM));
     st.attr = true;
   }
   const int64_t rest = N - r0, ncols = std::min<int64_t>(c_hi, N) - r0;
@@ -568,10 +757,19 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
   const int cpb = 16 * c->precond_tf32_terms;
   const int64_t tb1 = dmb::tune_bucket((rest + 63) / 64), tb2 = dmb::tune_bucket((ncols + TC_BN - 1) / TC_BN) * 8 + kslot;
-  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, 2);
+  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, 3);
   dmb::TuneMark mk;
   dmb::tune_begin(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, cand, mk);
-  if (cand == 0)
+  if (cand == 2) {
+    // persistent: lower tiles only, at most one CTA per SM
+    const int nrt = (int)((rest + 63) / 64), nct = (int)((ncols + TC_BN - 1) / TC_BN);
+    int64_t ntiles = 0;
+    for (int ct = 0; ct < nct; ct++) ntiles += std::max<int64_t>(0, nrt - 4 * ct);
+    const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, c->sm_count));
+    if (ntiles > 0)
+      DMB_LAUNCH(c, k_tc_syrk_p, G, 192, TCP_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N, r0,
+                 std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, nrt, nct, ntiles, st.err.as<unsigned>());
+  } else if (cand == 0)
     DMB_LAUNCH(c, k_tc_syrk<4>, grid, 128, tc_syrk_smem(4), st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
                r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
   else

@@ -95,9 +95,9 @@ class EFIEDevice:
         meets the tolerance; 0: it stops where Krylov.gmres stops),
         "spin_limit" (polls of a chained triangular-sweep wait before the call
         fails with TimeoutError; negative restores the default),
-        "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; 1 or 2 pins a candidate:
-        256- or 128-wide sweep GEMM tiles, 4- or 2-stage factor-update
-        pipelines)."""
+        "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; k pins candidate k:
+        256- or 128-wide sweep GEMM tiles; 4-stage, 2-stage or persistent
+        factor-update schedules)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
                  "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,

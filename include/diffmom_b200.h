@@ -148,9 +148,10 @@ const char *dmb_version(void);
 #define DMB_OPT_SPIN_LIMIT 9
 /* DMB_OPT_TUNE_TC_GEMM / DMB_OPT_TUNE_TC_SYRK: pin a candidate of the online
  * autotuner (0, the default, lets it choose): the tile width of the
- * tensor-core sweep GEMMs (1: 256, 2: 128 complex columns) and the pipeline of
+ * tensor-core sweep GEMMs (1: 256, 2: 128 complex columns) and the schedule of
  * the complex64 factor updates (1: 4 stages, one CTA per SM; 2: 2 stages, two
- * CTAs per SM).  Unpinned, each launch shape bucket runs every candidate on
+ * CTAs per SM; 3: persistent grid over the lower tiles only, double-buffered
+ * accumulators).  Unpinned, each launch shape bucket runs every candidate on
  * its first real calls, timed with events, and keeps the fastest for the
  * process; the candidates give the same bits. */
 #define DMB_OPT_TUNE_TC_GEMM 10

@@ -271,7 +271,7 @@ def test_autotuner_candidates_identical():
     dev.assemble(K3, precision="mixed")
     X = _rand(dev.N, 200, 3)
     out = {}
-    for syrk in (0, 1, 2):
+    for syrk in (0, 1, 2, 3):
         for gemm in (0, 1, 2):
             if syrk and gemm:
                 continue
@@ -289,4 +289,6 @@ def test_autotuner_candidates_identical():
     assert "k_tc_gemm" in rep and "k_tc_syrk" in rep
     with pytest.raises(Exception):
         dev.set_option("tune_tc_gemm", 3)
+    with pytest.raises(Exception):
+        dev.set_option("tune_tc_syrk", 4)
     dev.close()
