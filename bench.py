@@ -560,7 +560,7 @@ def run_ours(args):
                 variants[name]["network"] = net_note
         tdev.close()
 
-    line = make_line(args, ws, N, mesh, head, variants, e2e) if rank == 0 else None
+    line = make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks) if rank == 0 else None
     if rank == 0:
         line["fp64_peaks_measured"] = fp64_peaks
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -591,7 +591,7 @@ def clean(v):
     return out
 
 
-def make_line(args, ws, N, mesh, head, variants, e2e):
+def make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks=None):
     hbm, bf16, src = measured_peaks()
     base = variants.get("c3_fp64_plain")
     speed = {}
@@ -668,27 +668,37 @@ def make_line(args, ws, N, mesh, head, variants, e2e):
                                 "launches_timed": f[1], "kernel_ms_total": f[0],
                                 "kernel_share_of_step": f[0] / (head["ms_per_step"] * head["steps"])}
                          for name, f in fams.items()}}
-        line["roofline_assembly"] = assembly_roofline(head, full, hbm, N)
+        line["roofline_assembly"] = assembly_roofline(head, full, hbm, N, mesh.ntriangles,
+                                                      (fp64_peaks or {}).get("cublas_dgemm_tflops"))
         line["clocks"] = head.get("clocks")
     return line
 
 
-def assembly_roofline(head, full, hbm, N):
-    """The far-pair tile kernel of the assembly (k_far_tile): the bytes of Z it
-    writes (16 N^2 complex128, 8 N^2 complex64 -- it reads only L2-resident
-    triangle panels) per event-timed launch, against the measured copy
-    bandwidth; the FP32 / FP64 pipe figures come from the ncu capture."""
-    out = {"kernel": "k_far_tile (far triangle pairs written straight into Z by RWG tiles)", "bound": "fp64/fp32 pipe",
-           "unit": "GB/s", "peak_hbm": hbm, "note": "algorithmic bytes: Z written once (16 N^2 B complex128, "
-           "8 N^2 B complex64); the kernel is bound by the FP32 / FP64 pipes, not by HBM"}
+def assembly_roofline(head, full, hbm, N, Nt, fp64_peak):
+    """The far-pair tile kernel of the assembly (k_far_tile), per event-timed
+    launch: algorithmic flops on the pinned triangle-pair convention -- 600
+    flops per ordered far triangle pair, P_far = Nt^2 - Nt - 2N (9 quadrature
+    pairs x (14 kernel + 32 moment flops) + 186 for the 3 x 3 combination) --
+    against the measured FP64 peak (cuBLAS DGEMM of this run) for the FP64
+    flavour, and the bytes of Z it writes (16 N^2 complex128, 8 N^2 complex64;
+    it reads only L2-resident triangle panels) against the measured copy
+    bandwidth.  Pipe utilisation comes from the ncu capture (profiles/)."""
+    p_far = float(Nt) * Nt - Nt - 2.0 * N
+    flops = 600.0 * p_far
+    out = {"kernel": "k_far_tile (far triangle pairs written straight into Z by RWG tiles)",
+           "bound": "fp64 pipe (fp32 pipe for the mixed flavour)", "unit": "TFLOP/s",
+           "algorithmic_flops_per_launch": flops, "peak_fp64": fp64_peak, "peak_hbm_gbs": hbm,
+           "note": "600 flops per ordered far triangle pair (pinned convention); Z written once"}
     for key, v, esz in (("mixed_c64", head, 8.0), ("fp64_c128", full, 16.0)):
         if not v or "kernel_assembly" not in v:
             continue
         ms, launches, work = v["kernel_assembly"]
         if launches > 0 and ms > 0:
             per = ms / launches
-            out[key] = {"launches_timed": launches, "ms_per_launch": per,
-                        "achieved_gbs": (esz * N * N / 1e9) / (per / 1e3),
+            ach = (flops / 1e12) / (per / 1e3)
+            out[key] = {"launches_timed": launches, "ms_per_launch": per, "achieved_tflops": ach,
+                        "frac_fp64_peak": ach / fp64_peak if (fp64_peak and esz == 16.0) else None,
+                        "z_write_gbs": (esz * N * N / 1e9) / (per / 1e3),
                         "frac_hbm": (esz * N * N / 1e9) / (per / 1e3) / hbm if hbm else None}
     return out
 

@@ -13,7 +13,7 @@
 // one per tile -- and each CTA stages its two panels into shared memory with
 // the bulk-copy engine (cp.async.bulk completing on an mbarrier, bounded
 // wait).
-//   phase 1  every thread takes triangle pairs (a, b) of the two panels: the
+//   phase 1  the CTA's threads stride over the triangle pairs (a, b) of the two panels: the
 //            quadrature points come from shared memory into registers, the
 //            Nq x Nq moments of the Green function are formed and contracted
 //            into the 3 x 3 block of the two triangles' basis slots; a slot
@@ -104,6 +104,42 @@ __device__ __forceinline__ bool csr_adjacent(const int *__restrict__ off, const 
   return false;
 }
 
+// sin(kR), cos(kR) from those of k Rc and the Taylor series of the short
+// remainder d = k (R - Rc); a remainder above 0.75 (coarse meshes) takes the
+// direct evaluation.  Series terms through d^16 / d^17: the first omitted
+// term is below 1e-18 at |d| = 0.75.
+__device__ __forceinline__ void phase_exp(double k, double R, double Rc, double s0, double c0, double &sn,
+                                          double &cs) {
+  const double d = k * (R - Rc);
+  if (fabs(d) > 0.75) {
+    sincos(k * R, &sn, &cs);
+    return;
+  }
+  const double u = d * d;
+  double cd = 1.0 / 20922789888000.0;  // 1/16!
+  cd = fma(cd, u, -1.0 / 87178291200.0);
+  cd = fma(cd, u, 1.0 / 479001600.0);
+  cd = fma(cd, u, -1.0 / 3628800.0);
+  cd = fma(cd, u, 1.0 / 40320.0);
+  cd = fma(cd, u, -1.0 / 720.0);
+  cd = fma(cd, u, 1.0 / 24.0);
+  cd = fma(cd, u, -0.5);
+  cd = fma(cd, u, 1.0);
+  double sd = 1.0 / 355687428096000.0;  // 1/17!
+  sd = fma(sd, u, -1.0 / 1307674368000.0);
+  sd = fma(sd, u, 1.0 / 6227020800.0);
+  sd = fma(sd, u, -1.0 / 39916800.0);
+  sd = fma(sd, u, 1.0 / 362880.0);
+  sd = fma(sd, u, -1.0 / 5040.0);
+  sd = fma(sd, u, 1.0 / 120.0);
+  sd = fma(sd, u, -1.0 / 6.0);
+  sd = fma(sd, u, 1.0);
+  sd *= d;
+  // angle sum: (c0 + i s0)(cd + i sd)
+  cs = fma(c0, cd, -s0 * sd);
+  sn = fma(s0, cd, c0 * sd);
+}
+
 template <class SC>
 __device__ __forceinline__ double2 tile_entry(const SC *S, int lds, int a, int b) {
   const SC *r0 = S + (2 * a) * lds + 2 * b;
@@ -112,9 +148,14 @@ __device__ __forceinline__ double2 tile_entry(const SC *S, int lds, int a, int b
   return make_double2((pp.x + mm.x) + (pm.x + mp.x), (pp.y + mm.y) + (pm.y + mp.y));
 }
 
+// CTA size: 256 threads for the FP32 flavour (80 registers, several CTAs per
+// SM); 192 for the FP64 flavour, whose ~160 registers per thread would allow
+// only one 256-thread CTA per SM -- two 192-thread CTAs keep 12 warps resident.
+template <bool F64> struct FarThreads { static constexpr int value = F64 ? 192 : 256; };
+
 template <int NQ, int T, bool F64>
-__global__ void __launch_bounds__(256) k_far_tile(const FarJob *__restrict__ jobs, const int4 *__restrict__ tasks,
-                                                  unsigned *err) {
+__global__ void __launch_bounds__(FarThreads<F64>::value, F64 ? 2 : 3)
+    k_far_tile(const FarJob *__restrict__ jobs, const int4 *__restrict__ tasks, unsigned *err) {
   constexpr int P = 2 * T, LDS = 2 * T;
   typedef Panel<NQ, P, F64> L;
   typedef typename L::R R;
@@ -187,6 +228,13 @@ __global__ void __launch_bounds__(256) k_far_tile(const FarJob *__restrict__ job
       const double k = jb.k;
       const double ca0 = cenA[ia], ca1 = cenA[P + ia], ca2 = cenA[2 * P + ia];
       const double cb0 = cenB[ib], cb1 = cenB[P + ib], cb2 = cenB[2 * P + ib];
+      // phase of the centroid distance, once per pair: exp(-ik R) =
+      // exp(-ik Rc) exp(-ik (R - Rc)) with the short second factor from
+      // its Taylor series (|k (R - Rc)| <= 0.75: truncation below 1e-18)
+      const double cdx = ca0 - cb0, cdy = ca1 - cb1, cdz = ca2 - cb2;
+      const double Rc = sqrt(cdx * cdx + cdy * cdy + cdz * cdz);
+      double s0, c0;
+      sincos(k * Rc, &s0, &c0);
 #pragma unroll
       for (int bq = 0; bq < NQ; bq++) {
         const double qb0 = qB[(3 * bq + 0) * P + ib], qb1 = qB[(3 * bq + 1) * P + ib],
@@ -200,10 +248,12 @@ __global__ void __launch_bounds__(256) k_far_tile(const FarJob *__restrict__ job
           const double la0 = qa0 - ca0, la1 = qa1 - ca1, la2 = qa2 - ca2;
           const double wa = wA[aq * P + ia];
           double dx = qa0 - qb0, dy = qa1 - qb1, dz = qa2 - qb2;
-          double Rr = sqrt(dx * dx + dy * dy + dz * dz);
+          const double R2 = dx * dx + dy * dy + dz * dz;
+          const double rinv = rsqrt(R2);
+          const double Rr = R2 * rinv;
           double sn, cs_;
-          sincos(k * Rr, &sn, &cs_);
-          double g = (DMB_INV_FOUR_PI / Rr) * (wa * wb);
+          phase_exp(k, Rr, Rc, s0, c0, sn, cs_);
+          double g = (DMB_INV_FOUR_PI * rinv) * (wa * wb);
           double gr = cs_ * g, gi = -sn * g;  // exp(-ikR)/(4 pi R) * W
           m0r += gr;
           m0i += gi;
@@ -376,7 +426,7 @@ void far_launch_t(dmb_ctx *c, const FarJob *d_jobs, const int4 *d_tasks, int64_t
   std::call_once(once, [&] {
     cudaFuncSetAttribute(k_far_tile<NQ, T, F64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
-  DMB_LAUNCH(c, (k_far_tile<NQ, T, F64>), (unsigned)ntasks, 256, smem, d_jobs, d_tasks, err);
+  DMB_LAUNCH(c, (k_far_tile<NQ, T, F64>), (unsigned)ntasks, FarThreads<F64>::value, smem, d_jobs, d_tasks, err);
 }
 
 template <int NQ, int T, bool F64>

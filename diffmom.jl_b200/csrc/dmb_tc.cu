@@ -756,7 +756,8 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
              N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<float>(), bB.as<float>());
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
   const int cpb = 16 * c->precond_tf32_terms;
-  const int64_t tb1 = dmb::tune_bucket((rest + 63) / 64), tb2 = dmb::tune_bucket((ncols + TC_BN - 1) / TC_BN) * 8 + kslot;
+  // bucket: row tiles (log2) and the K width of the update
+  const int64_t tb1 = dmb::tune_bucket((rest + 63) / 64), tb2 = kslot;
   const int cand = dmb::tune_choose(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, 3);
   dmb::TuneMark mk;
   dmb::tune_begin(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, cand, mk);

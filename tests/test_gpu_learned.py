@@ -102,25 +102,20 @@ def _iters(dev, v, P, side="right", maxiter=600):
 
 
 def test_learned_preconditioner_ablation():
-    # perturbed ellipsoids (semi-axes U[0.5,1.5] lambda, 8 harmonics <= 10 %),
-    # geodesic frequency 8 -> 1,920 RWG; train on three bodies, test on a fourth
+    """What the trained network gains over the same method without it, on a
+    body none of the training bodies is: the library's default weights
+    (trained on the GPU over 48 generated perturbed ellipsoids, seeds
+    1000-1047) against the plain ring step (the learned step with the network
+    switched off), the exact local inverse, the near-field LDL^T and no
+    preconditioner; GMRES to 1e-6 judged on the FP64 residual."""
+    from diffmom_b200.learned import DEFAULT_WEIGHTS
     lam = C0 / 3e9
     k = 2 * math.pi / lam
     r = 0.2 * lam
-    dev = None
-    losses = []
-    for seed in (11, 12, 13):
-        body = make_perturbed_ellipsoid(lam, seed, frequency=8)
-        rwg = build_rwg(body)
-        if dev is None:
-            dev = EFIEDevice(body, rwg)
-        else:
-            dev.upload(body, rwg)
-        dev.assemble(k, precision="mixed")
-        losses.append([dev.train_network(r, epochs=3, batch=256, lr=3e-3, seed=seed) for _ in range(2)])
-    test_body = make_perturbed_ellipsoid(lam, 99, frequency=8)
+    test_body = make_perturbed_ellipsoid(lam, 99, frequency=8)   # 1,920 RWG
     trwg = build_rwg(test_body)
-    dev.upload(test_body, trwg)
+    dev = EFIEDevice(test_body, trwg)
+    dev.load_network(DEFAULT_WEIGHTS)
     dev.assemble(k, precision="mixed")
     v = dev.plane_wave_rhs([[0, 0, -k]], [1.0], [[1, 0, 0]])[:, 0]
     it_none, x_none = _iters(dev, v, None)
@@ -130,11 +125,33 @@ def test_learned_preconditioner_ablation():
     it_ls, x_ls = _iters(dev, v, dev.build_local(r, mode="ls"))
     it_nf, x_nf = _iters(dev, v, dev.build_nearfield(0.2 * lam, "lu"), side="left")
     print(f"GMRES iterations: none {it_none}, near-field LDL^T {it_nf}, local inverse {it_local}, "
-          f"ring step {it_ring}, learned ring step {it_learned}, least-squares target {it_ls}; "
-          f"training loss per body {losses}")
+          f"ring step {it_ring}, learned ring step {it_learned}, least-squares target {it_ls}")
     for x in (x_local, x_learned, x_nf):
         assert np.linalg.norm(x - x_none) / np.linalg.norm(x_none) < 1e-4
     assert it_local < it_none
     assert it_ring < it_local
-    assert it_learned <= it_ring
+    # the network's gain: strictly fewer iterations than the plain ring step,
+    # and at least 10 % fewer than the exact local inverse
+    assert it_learned < it_ring
+    assert it_learned <= 0.9 * it_local
+    dev.close()
+
+
+def test_training_streams_generated_bodies():
+    """GPU training over a stream of generated bodies (forward, backward and
+    Adam on the device) from the untrained network: finite losses, weights
+    that change, and a learned preconditioner that converges with them."""
+    from diffmom_b200.learned import train_learned_network, training_bodies
+    m = make_rect_plate(0.1, 0.1, 2, 2)
+    dev = EFIEDevice(m, build_rwg(m))
+    w0 = dev.network_weights()
+    rep = train_learned_network(dev, training_bodies(6, frequencies=(6, 7)), epochs=2)
+    assert rep.bodies == 6 and rep.rwg_total > 0
+    assert all(np.isfinite(rep.losses))
+    assert not np.array_equal(dev.network_weights(), w0)
+    lam = C0 / 3e9
+    k = 2 * math.pi / lam
+    dev.assemble(k, precision="mixed")
+    v = dev.plane_wave_rhs([[0, 0, -k]], [1.0], [[1, 0, 0]])[:, 0]
+    _iters(dev, v, dev.build_local(0.2 * lam, learned=True))
     dev.close()
