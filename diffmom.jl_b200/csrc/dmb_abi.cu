@@ -155,6 +155,12 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->spin_limit = value < 0 ? 20000000LL : (long long)value;
       return;
     }
+    if (option == DMB_OPT_PRECOND_BF16) {
+      DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "DMB_OPT_PRECOND_BF16 must be 0 or 1");
+      if (c->precond_bf16 != (value != 0)) c->pc_valid = false;
+      c->precond_bf16 = value != 0;
+      return;
+    }
     if (option == DMB_OPT_TUNE_TC_GEMM || option == DMB_OPT_TUNE_TC_SYRK) {
       const int ncand = option == DMB_OPT_TUNE_TC_GEMM ? 2 : 3;
       DMB_REQUIRE(value >= 0 && value <= ncand, DMB_ERR_ARGUMENT,

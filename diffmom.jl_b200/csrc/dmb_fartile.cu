@@ -206,9 +206,11 @@ __global__ void __launch_bounds__(FarThreads<F64>::value, F64 ? 2 : 3)
   const int *moreA = reinterpret_cast<const int *>(pa + L::OFF_MORE);
 
   // ---- phase 1: triangle pairs -> tile slot matrix ----------------------
-  const int npair = ua * ub;
-  for (int p = threadIdx.x; p < npair; p += blockDim.x) {
-    const int ia = p / ub, ib = p - ia * ub;
+  // thread -> pairs p = tid, tid + blockDim, ... as (ia, ib) = (p / ub, p % ub),
+  // stepped without a division per pair
+  const int dq = blockDim.x / ub, dr = blockDim.x - dq * ub;
+  int ia = threadIdx.x / ub, ib = threadIdx.x - (threadIdx.x / ub) * ub;
+  for (; ia < ua; ia += dq, ib += dr, ia += (ib >= ub) ? 1 : 0, ib -= (ib >= ub) ? ub : 0) {
     const int ta = triA[ia], tb = triB[ib];
     const int rs[3] = {slA[ia], slA[P + ia], slA[2 * P + ia]};
     const int cs[3] = {slB[ib], slB[P + ib], slB[2 * P + ib]};

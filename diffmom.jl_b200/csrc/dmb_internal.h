@@ -273,6 +273,7 @@ struct dmb_ctx {
   };
   std::map<std::vector<int64_t>, GraphEntry> gm_graphs;
   int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
+  bool precond_bf16 = false;     // those operands split into BF16 pieces instead of TF32 (kind::f16 MMA)
   int far_tile_used = 0;         // tile width of the last assembly
   // autotuner pins per family (0: tuned, k: candidate k - 1)
   int tune_pin[dmb::TUNE_FAMILIES] = {0, 0};

@@ -25,6 +25,7 @@
 // No TMA multicast, no clusters.  Every mbarrier wait is bounded: on expiry
 // the kernel records an error bit, stops issuing, frees its TMEM and returns.
 #include <cuda.h>
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstring>
@@ -50,30 +51,54 @@ constexpr int TC_SMEM_128 = TC_STAGES * (TC_A_STAGE + TC_B_STAGE / 2) + 1024 + 1
 // 4 stages with one CTA per SM, or 2 stages with two co-resident CTAs per SM
 constexpr int tc_syrk_smem(int stages) { return stages * (TC_A_STAGE + TC_B_STAGE) + 1024 + 1024; }
 
-// instruction descriptor: D f32, A/B tf32, both K-major, N = 256, M = 128
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
-
-template <int BN>
-__device__ __forceinline__ void umma_tf32_n(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+// One tcgen05.mma (M 128, N = BN, 32 bytes of K) on TF32 operands (K 8) or,
+// with BF, on BF16 operands (kind::f16, both operands BF16, K 16); FP32
+// accumulation either way.
+template <int BN, bool BF>
+__device__ __forceinline__ void umma_op(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  constexpr uint32_t fmt = BF ? 1u : 2u;  // operand format: BF16 (kind::f16) / TF32 (kind::tf32)
+  constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
                              ((uint32_t)(TC_BM >> 4) << 24);
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
+  if constexpr (BF)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate)
-      : "memory");
+// Split of an FP32 value into the two operand pieces of the three-product
+// scheme: TF32 hi = tf32(x), lo = tf32(x - hi) (~21 bits), or BF16 hi =
+// bf16(x), lo = bf16(x - hi) (~16 bits).
+__device__ __forceinline__ void split_op(float x, float &hi, float &lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - hi);
 }
+__device__ __forceinline__ void split_op(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+// the same from a double (the residual taken in double)
+__device__ __forceinline__ void split_op_d(double x, float &hi, float &lo) {
+  hi = tf32_rna((float)x);
+  lo = tf32_rna((float)(x - (double)hi));
+}
+__device__ __forceinline__ void split_op_d(double x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn((float)x);
+  lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+}
+__device__ __forceinline__ float neg_op(float v) { return -v; }
+__device__ __forceinline__ __nv_bfloat16 neg_op(__nv_bfloat16 v) { return __hneg(v); }
+template <bool BF> struct OpElem { typedef float T; };
+template <> struct OpElem<true> { typedef __nv_bfloat16 T; };
 
 // ---------------------------------------------------------------------------
 // operand packing for the trailing update, rows m in [0, rest) relative to r0,
@@ -84,9 +109,10 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
 // with W[r0 + m][woff + k] (stride wstride) and L[r0 + m][jcol + k]; k >= K zero.
 // grid (rest, Kpad / 256), 256 threads.
 // ---------------------------------------------------------------------------
+template <class E>
 __global__ void k_tc_pack(int64_t rest, int64_t ncols, int64_t N, int64_t r0, int64_t jcol, int K, int64_t ld,
                           const float2 *__restrict__ F, const float2 *__restrict__ W, int wstride, int woff,
-                          float *__restrict__ Ap, float *__restrict__ Bp) {
+                          E *__restrict__ Ap, E *__restrict__ Bp) {
   const int64_t m = blockIdx.x;
   const int kb = blockIdx.y, kk = threadIdx.x, k = kb * 256 + kk;
   if (m >= rest) return;
@@ -95,28 +121,33 @@ __global__ void k_tc_pack(int64_t rest, int64_t ncols, int64_t N, int64_t r0, in
     w = W[(r0 + m) * wstride + woff + k];
     if (m < ncols) l = F[(r0 + m) * N + jcol + k];
   }
-  float wrh = tf32_rna(w.x), wih = tf32_rna(w.y);
-  float wrl = tf32_rna(w.x - wrh), wil = tf32_rna(w.y - wih);
+  E wrh, wrl, wih, wil;
+  split_op(w.x, wrh, wrl);
+  split_op(w.y, wih, wil);
   int64_t bi = m / 64, r = m % 64;
-  float *ar = Ap + (128 * bi + r) * ld + kb * 1536;
-  float *ai = Ap + (128 * bi + 64 + r) * ld + kb * 1536;
+  E *ar = Ap + (128 * bi + r) * ld + kb * 1536;
+  E *ai = Ap + (128 * bi + 64 + r) * ld + kb * 1536;
   const int S = 256;
-  ar[kk] = wrh; ar[S + kk] = -wih; ar[2 * S + kk] = wrh; ar[3 * S + kk] = -wih; ar[4 * S + kk] = wrl; ar[5 * S + kk] = -wil;
+  ar[kk] = wrh; ar[S + kk] = neg_op(wih); ar[2 * S + kk] = wrh; ar[3 * S + kk] = neg_op(wih);
+  ar[4 * S + kk] = wrl; ar[5 * S + kk] = neg_op(wil);
   ai[kk] = wih; ai[S + kk] = wrh;  ai[2 * S + kk] = wih; ai[3 * S + kk] = wrh;  ai[4 * S + kk] = wil; ai[5 * S + kk] = wrl;
   if (m < ncols) {
-    float lrh = tf32_rna(l.x), lih = tf32_rna(l.y);
-    float lrl = tf32_rna(l.x - lrh), lil = tf32_rna(l.y - lih);
-    float *br = Bp + m * ld + kb * 1536;
+    E lrh, lrl, lih, lil;
+    split_op(l.x, lrh, lrl);
+    split_op(l.y, lih, lil);
+    E *br = Bp + m * ld + kb * 1536;
     br[kk] = lrh; br[S + kk] = lih;  br[2 * S + kk] = lrl; br[3 * S + kk] = lil;  br[4 * S + kk] = lrh; br[5 * S + kk] = lih;
   }
 }
 
-// Packed K blocks hold 1536 floats per 256 complex K: segments [hi x hi |
-// hi x lo | lo x hi] of 512 floats each.  cpb = K chunks of 32 floats streamed
-// per block: 48 (3xTF32, all three products) or 16 (1xTF32, hi x hi only).
-__device__ __forceinline__ int tc_kx(int kc, int cpb) { return (kc / cpb) * 1536 + (kc % cpb) * TC_BK; }
+// Packed K blocks hold 1536 elements per 256 complex K: segments [hi x hi |
+// hi x lo | lo x hi] of 512 elements each.  A K chunk is one 128-byte swizzle
+// row: 32 TF32 or 64 BF16 elements.  cpb = chunks streamed per block: 48 / 24
+// (TF32 / BF16, all three products) or 16 / 8 (hi x hi only).
+template <bool BF>
+__device__ __forceinline__ int tc_kx(int kc, int cpb) { return (kc / cpb) * 1536 + (kc % cpb) * (BF ? 64 : 32); }
 
-template <int STAGES>
+template <int STAGES, bool BF>
 __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
                                                     int64_t N, int64_t j0, int64_t rest, int64_t c_hi, int nchunks,
@@ -166,7 +197,7 @@ __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __
       const int s = kc % STAGES;
       if (kc >= STAGES && !mbar_wait(empty0 + 8 * s, ((kc / STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
-      const int kx = tc_kx(kc, cpb);
+      const int kx = tc_kx<BF>(kc, cpb);
       tma_load_2d(sA + s * TC_A_STAGE, &tmA, kx, (int)(2 * row0), full0 + 8 * s);
       tma_load_2d(sB + s * TC_B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
     }
@@ -184,7 +215,7 @@ __global__ void __launch_bounds__(128, (STAGES <= 2 ? 2 : 1)) k_tc_syrk(const __
       for (int k = 0; k < TC_BK / 8; k++) {
         const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
         const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
-        umma_tf32(tmem_d, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+        umma_op<TC_BN, BF>(tmem_d, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
       }
       umma_commit(empty0 + 8 * s);
     }
@@ -273,6 +304,7 @@ __device__ __forceinline__ void tcp_arrive(uint32_t bar) {
 }
 __device__ __forceinline__ void tcp_epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+template <bool BF>
 __global__ void __launch_bounds__(192, 1) k_tc_syrk_p(const __grid_constant__ CUtensorMap tmA,
                                                       const __grid_constant__ CUtensorMap tmB, float2 *__restrict__ F,
                                                       int64_t N, int64_t j0, int64_t c_hi, int nchunks, int cpb,
@@ -331,7 +363,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_syrk_p(const __grid_constant__ CU
             break;
           }
           mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + TC_B_STAGE);
-          const int kx = tc_kx(kc, cpb);
+          const int kx = tc_kx<BF>(kc, cpb);
           tma_load_2d(sA + s * TC_A_STAGE, &tmA, kx, (int)(2 * row0), full0 + 8 * s);
           tma_load_2d(sB + s * TC_B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
         }
@@ -360,7 +392,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_syrk_p(const __grid_constant__ CU
           for (int k = 0; k < TC_BK / 8; k++) {
             const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
             const uint64_t bd = sw128_desc(sB + s * TC_B_STAGE + k * 32);
-            umma_tf32(tmem_acc, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
+            umma_op<TC_BN, BF>(tmem_acc, ad, bd, (kc > 0 || k > 0) ? 1u : 0u);
           }
           umma_commit(empty0 + 8 * s);
         }
@@ -446,7 +478,7 @@ __global__ void __launch_bounds__(192, 1) k_tc_syrk_p(const __grid_constant__ CU
 // operator, 1 = triangular-solve GEMMs.  BN (256 or 128) is the tile width in
 // complex columns: the 128-wide form doubles the CTAs of launches that would
 // otherwise fill fewer than two waves.
-template <int ROLE, int BN>
+template <int ROLE, int BN, bool BF>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
                                                     int nchunks, int cpb, int64_t M, int64_t Rv,
@@ -501,7 +533,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
       const int s = i % TC_STAGES, kc = kc0 + i;
       if (i >= TC_STAGES && !mbar_wait(empty0 + 8 * s, ((i / TC_STAGES) - 1) & 1, err, abort_flag)) break;
       mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + B_STAGE);
-      const int kx = tc_kx(kc, cpb);
+      const int kx = tc_kx<BF>(kc, cpb);
       tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kx, a_row0 + (int)(2 * row0), full0 + 8 * s);
       tma_load_2d(sB + s * B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
     }
@@ -518,7 +550,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
       for (int k = 0; k < TC_BK / 8; k++) {
         const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
         const uint64_t bd = sw128_desc(sB + s * B_STAGE + k * 32);
-        umma_tf32_n<BN>(tmem_d, ad, bd, (i > 0 || k > 0) ? 1u : 0u);
+        umma_op<BN, BF>(tmem_d, ad, bd, (i > 0 || k > 0) ? 1u : 0u);
       }
       umma_commit(empty0 + 8 * s);
     }
@@ -585,10 +617,13 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
 }
 
 // split one complex value into the six 256-strided A'' / B'' segment entries
-__device__ __forceinline__ void put_a(float *ar, float *ai, int kk, float vr, float vi) {
-  const float rh = tf32_rna(vr), ih = tf32_rna(vi);
-  const float rl = tf32_rna(vr - rh), il = tf32_rna(vi - ih);
-  ar[kk] = rh; ar[256 + kk] = -ih; ar[512 + kk] = rh; ar[768 + kk] = -ih; ar[1024 + kk] = rl; ar[1280 + kk] = -il;
+template <class E>
+__device__ __forceinline__ void put_a(E *ar, E *ai, int kk, float vr, float vi) {
+  E rh, rl, ih, il;
+  split_op(vr, rh, rl);
+  split_op(vi, ih, il);
+  ar[kk] = rh; ar[256 + kk] = neg_op(ih); ar[512 + kk] = rh; ar[768 + kk] = neg_op(ih); ar[1024 + kk] = rl;
+  ar[1280 + kk] = neg_op(il);
   ai[kk] = ih; ai[256 + kk] = rh;  ai[512 + kk] = ih; ai[768 + kk] = rh;  ai[1024 + kk] = il; ai[1280 + kk] = rl;
 }
 
@@ -597,9 +632,9 @@ __device__ __forceinline__ void put_a(float *ar, float *ai, int kk, float vr, fl
 // diagonal of the source (k < m, or k > m for TRANS: L^T from the lower
 // factor).  32 x 32 tiles through shared memory so both the read and the
 // write are coalesced; the grid covers exactly Mpad x Kpad.
-template <bool TRANS, bool LOWER, class SC>
+template <bool TRANS, bool LOWER, class SC, class E>
 __global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kpad, const SC *__restrict__ S,
-                                                int64_t ld, float *__restrict__ Ap) {
+                                                int64_t ld, E *__restrict__ Ap) {
   __shared__ float2 tile[32][33];
   // LOWER: tiles holding only excluded (zero) elements are not written -- the
   // triangular-sweep GEMMs read the packed factor only in the included part
@@ -624,22 +659,24 @@ __global__ void __launch_bounds__(256) k_pack_a(int64_t M, int64_t K, int64_t Kp
   for (int i = ty; i < 32; i += 8) {
     const int64_t m = m0 + i, k = k0 + tx;
     const float2 v = tile[i][tx];
-    float *ar = Ap + (128 * (m / 64) + m % 64) * lda + (k / 256) * 1536;
+    E *ar = Ap + (128 * (m / 64) + m % 64) * lda + (k / 256) * 1536;
     put_a(ar, ar + 64 * lda, (int)(k % 256), v.x, v.y);
   }
 }
 
 // B'' from complex128 column-major right-hand sides: row r, complex K index k
 // holds X[k + r ldx] (zero for k >= Kv or r >= R).  The grid covers Rpad rows.
+template <class E>
 __global__ void k_pack_b(int64_t R, int64_t Kv, int64_t Kpad, const double2 *__restrict__ X, int64_t ldx,
-                         float *__restrict__ Bp) {
+                         E *__restrict__ Bp) {
   const int64_t r = blockIdx.y;
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= Kpad) return;
   const double2 v = (r < R && k < Kv) ? X[r * ldx + k] : make_double2(0, 0);
-  const float rh = tf32_rna((float)v.x), ih = tf32_rna((float)v.y);
-  const float rl = tf32_rna((float)(v.x - (double)rh)), il = tf32_rna((float)(v.y - (double)ih));
-  float *br = Bp + r * 6 * Kpad + (k / 256) * 1536;
+  E rh, rl, ih, il;
+  split_op_d(v.x, rh, rl);
+  split_op_d(v.y, ih, il);
+  E *br = Bp + r * 6 * Kpad + (k / 256) * 1536;
   const int kk = (int)(k % 256);
   br[kk] = rh; br[256 + kk] = ih; br[512 + kk] = rl; br[768 + kk] = il; br[1024 + kk] = rh; br[1280 + kk] = ih;
 }
@@ -652,6 +689,14 @@ __global__ void k_pack_b(int64_t R, int64_t Kv, int64_t Kpad, const double2 *__r
 void make_map(CUtensorMap *map, float *base, uint64_t rows, uint32_t box_rows, uint64_t ld = TC_K) {
   make_map_bytes(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ld, ld * sizeof(float), rows, TC_BK, box_rows);
 }
+// the same over TF32 (bf false) or BF16 (bf true) elements: boxes of one
+// 128-byte row (32 or 64 elements) x box_rows rows
+void make_map_op(CUtensorMap *map, void *base, bool bf, uint64_t rows, uint32_t box_rows, uint64_t ld) {
+  if (bf)
+    make_map_bytes(map, base, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, ld, ld * 2, rows, 64, box_rows);
+  else
+    make_map_bytes(map, base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ld, ld * sizeof(float), rows, TC_BK, box_rows);
+}
 
 // factor updates pack their operands into one of TC_UPD_SLOTS buffer pairs,
 // one per stream that issues them, so updates of disjoint column ranges run
@@ -662,6 +707,7 @@ struct TcState {
   DevBuf A[TC_UPD_SLOTS], B[TC_UPD_SLOTS], err;
   CUtensorMap mapAK[TC_UPD_SLOTS][4], mapBK[TC_UPD_SLOTS][4];
   int64_t n_key[TC_UPD_SLOTS] = {-1, -1, -1};
+  int upd_fmt[TC_UPD_SLOTS] = {-1, -1, -1};  // operand format of the slot's maps (0 TF32, 1 BF16)
   bool attr = false;
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
   // sides, packed triangular-solve panels
@@ -674,6 +720,7 @@ struct TcState {
   DevBuf Lp, Ltp, Dfp, Dbp;
   CUtensorMap mapL, mapLt, mapDf, mapDb;
   int64_t lp_n = -1;
+  int lp_fmt = -1, pb_fmt = -1;  // operand formats of the packed factor / of Pb's maps
   int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key = -1;
   bool gemm_attr = false;
 };
@@ -697,9 +744,11 @@ void ensure_gemm(dmb_ctx *c, TcState &st) {
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.gemm_attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<0, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<0, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
     st.gemm_attr = true;
   }
 }
@@ -727,24 +776,29 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   const int64_t npadA = ((N + 63) / 64) * 64;
   const int64_t npadB = ((N + TC_BN - 1) / TC_BN) * TC_BN;
   const int64_t Kpad = ((K + 255) / 256) * 256, ld = 6 * Kpad;
-  if (st.n_key[slot] != N) {
+  const bool bf = c->precond_bf16;
+  if (st.n_key[slot] != N || st.upd_fmt[slot] != (int)bf) {
     bA.ensure(sizeof(float) * 2 * npadA * 6 * 1024);
     bB.ensure(sizeof(float) * npadB * 6 * 1024);
     DMB_CUDA(cudaMemsetAsync(bB.p, 0, sizeof(float) * npadB * 6 * 1024, c->stream));
     for (int i = 0; i < 4; i++) {
-      make_map(&st.mapAK[slot][i], bA.as<float>(), (uint64_t)(2 * npadA), TC_BM, 1536 * (i + 1));
-      make_map(&st.mapBK[slot][i], bB.as<float>(), (uint64_t)npadB, TC_BN, 1536 * (i + 1));
+      make_map_op(&st.mapAK[slot][i], bA.p, bf, (uint64_t)(2 * npadA), TC_BM, 1536 * (i + 1));
+      make_map_op(&st.mapBK[slot][i], bB.p, bf, (uint64_t)npadB, TC_BN, 1536 * (i + 1));
     }
     st.n_key[slot] = N;
+    st.upd_fmt[slot] = (int)bf;
   }
   if (!st.err.p) {
     st.err.ensure(16);
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(4)));
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(2)));
-    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk_p, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(4)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(2)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk_p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(4)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_syrk_smem(2)));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_syrk_p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCP_SMEM));
     st.attr = true;
   }
   const int64_t rest = N - r0, ncols = std::min<int64_t>(c_hi, N) - r0;
@@ -752,10 +806,14 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   const int kslot = (int)(Kpad / 256) - 1;
   // A'' rows past `rest` and B'' rows past `ncols` keep stale values: they only
   // feed output rows >= N and columns >= c_hi, which the epilogue skips
-  DMB_LAUNCH(c, k_tc_pack, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
-             N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<float>(), bB.as<float>());
+  if (bf)
+    DMB_LAUNCH(c, k_tc_pack<__nv_bfloat16>, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
+               N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<__nv_bfloat16>(), bB.as<__nv_bfloat16>());
+  else
+    DMB_LAUNCH(c, k_tc_pack<float>, dim3((unsigned)rest, (unsigned)(Kpad / 256)), 256, 0, rest, ncols,
+               N, r0, jcol, K, ld, F, W, wstride, woff, bA.as<float>(), bB.as<float>());
   dim3 grid((unsigned)((rest + 63) / 64), (unsigned)((ncols + TC_BN - 1) / TC_BN));
-  const int cpb = 16 * c->precond_tf32_terms;
+  const int cpb = (bf ? 8 : 16) * c->precond_tf32_terms;
   // bucket: row tiles (log2) and the K width of the update
   const int64_t tb1 = dmb::tune_bucket((rest + 63) / 64), tb2 = kslot;
   const int cand = dmb::tune_choose(c, dmb::TUNE_TC_SYRK_STAGES, tb1, tb2, 3);
@@ -767,15 +825,29 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
     int64_t ntiles = 0;
     for (int ct = 0; ct < nct; ct++) ntiles += std::max<int64_t>(0, nrt - 4 * ct);
     const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, c->sm_count));
-    if (ntiles > 0)
-      DMB_LAUNCH(c, k_tc_syrk_p, G, 192, TCP_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N, r0,
-                 std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, nrt, nct, ntiles, st.err.as<unsigned>());
-  } else if (cand == 0)
-    DMB_LAUNCH(c, k_tc_syrk<4>, grid, 128, tc_syrk_smem(4), st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
-               r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
-  else
-    DMB_LAUNCH(c, k_tc_syrk<2>, grid, 128, tc_syrk_smem(2), st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
-               r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>());
+    if (ntiles > 0) {
+      if (bf)
+        DMB_LAUNCH(c, k_tc_syrk_p<true>, G, 192, TCP_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N, r0,
+                   std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, nrt, nct, ntiles,
+                   st.err.as<unsigned>());
+      else
+        DMB_LAUNCH(c, k_tc_syrk_p<false>, G, 192, TCP_SMEM, st.mapAK[slot][kslot], st.mapBK[slot][kslot], F, N,
+                   r0, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, nrt, nct, ntiles,
+                   st.err.as<unsigned>());
+    }
+  } else {
+#define SYRK_LAUNCH(STG, BFV)                                                                                     \
+  DMB_LAUNCH(c, (k_tc_syrk<STG, BFV>), grid, 128, tc_syrk_smem(STG), st.mapAK[slot][kslot], st.mapBK[slot][kslot], \
+             F, N, r0, rest, std::min<int64_t>(c_hi, N), (int)(Kpad / 256) * cpb, cpb, st.err.as<unsigned>())
+    if (cand == 0) {
+      if (bf) SYRK_LAUNCH(4, true);
+      else SYRK_LAUNCH(4, false);
+    } else {
+      if (bf) SYRK_LAUNCH(2, true);
+      else SYRK_LAUNCH(2, false);
+    }
+#undef SYRK_LAUNCH
+  }
   dmb::tune_end(c, mk);
 }
 
@@ -799,7 +871,7 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
   if (st.zp_version != c->z_version || st.zp_n != N) {
     st.Zp.ensure(sizeof(float) * 2 * Mpad * ld);
     dim3 g((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
-    DMB_LAUNCH(c, (k_pack_a<false, false, float2>), g, 256, 0, N, N, Kpad, c->d_Z.as<float2>(), N,
+    DMB_LAUNCH(c, (k_pack_a<false, false, float2, float>), g, 256, 0, N, N, Kpad, c->d_Z.as<float2>(), N,
                st.Zp.as<float>());
     make_map(&st.mapZ, st.Zp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
     st.zp_version = c->z_version;
@@ -811,11 +883,11 @@ void tc_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R) {
     st.xp_key = Rpad;
     st.xp_n = N;
   }
-  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, N, Kpad, X, N,
+  DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, N, Kpad, X, N,
              st.Xp.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, (k_tc_gemm<0, 256>), grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), 48, N, R, Y, N, 0, 0,
+  DMB_LAUNCH(c, (k_tc_gemm<0, 256, false>), grid, 128, TC_SMEM, st.mapZ, st.mapX, 0, 0, (int)(ld / TC_BK), 48, N, R, Y, N, 0, 0,
              st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)N * (double)N * (double)R);
 }
@@ -841,26 +913,27 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
     for (int i = 0; i < 4; i++) make_map(&st.mapPaK[i], st.Pa.as<float>(), (uint64_t)(2 * Npad), TC_BM, 1536 * (i + 1));
     st.pa_key = Npad;
   }
-  if (st.pb_key != Rpad) {
+  if (st.pb_key != Rpad || st.pb_fmt != 0) {
     st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
     for (int i = 0; i < 4; i++) {
       make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
       make_map(&st.mapPbK128[i], st.Pb.as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
     }
     st.pb_key = Rpad;
+    st.pb_fmt = 0;
   }
   dim3 ga((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
   if (backward)
-    DMB_LAUNCH(c, (k_pack_a<true, false, float2>), ga, 256, 0, M, (int64_t)width, Kpad, F + k_lo * N + r_lo, N,
-               st.Pa.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<true, false, float2, float>), ga, 256, 0, M, (int64_t)width, Kpad, F + k_lo * N + r_lo,
+               N, st.Pa.as<float>());
   else
-    DMB_LAUNCH(c, (k_pack_a<false, false, float2>), ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo, N,
-               st.Pa.as<float>());
-  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)width, Kpad, X + k_lo,
-             N, st.Pb.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<false, false, float2, float>), ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo,
+               N, st.Pa.as<float>());
+  DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)width, Kpad,
+             X + k_lo, N, st.Pb.as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), 48, M, R,
+  DMB_LAUNCH(c, (k_tc_gemm<1, 256, false>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), 48, M, R,
              X + r_lo, N, 1, 0, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
@@ -874,36 +947,57 @@ void tc_trsm_pack_factor(dmb_ctx *c, const float2 *F, int64_t N) {
   ensure_gemm(c, st);
   const int64_t Mpad = round_up(N, 64), Kpad = round_up(N, 256), ld = 6 * Kpad;
   const int64_t nout = (N + TB - 1) / TB;
-  if (st.lp_n != N) {
+  const bool bf = c->precond_bf16;
+  if (st.lp_n != N || st.lp_fmt != (int)bf) {
     st.Lp.ensure(sizeof(float) * 2 * Mpad * ld);
     st.Ltp.ensure(sizeof(float) * 2 * Mpad * ld);
     st.Dfp.ensure(sizeof(float) * 2 * TB * nout * 6 * TB);
     st.Dbp.ensure(sizeof(float) * 2 * TB * nout * 6 * TB);
-    make_map(&st.mapL, st.Lp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
-    make_map(&st.mapLt, st.Ltp.as<float>(), (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
-    make_map(&st.mapDf, st.Dfp.as<float>(), (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
-    make_map(&st.mapDb, st.Dbp.as<float>(), (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
+    make_map_op(&st.mapL, st.Lp.p, bf, (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
+    make_map_op(&st.mapLt, st.Ltp.p, bf, (uint64_t)(2 * Mpad), TC_BM, (uint64_t)ld);
+    make_map_op(&st.mapDf, st.Dfp.p, bf, (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
+    make_map_op(&st.mapDb, st.Dbp.p, bf, (uint64_t)(2 * TB * nout), TC_BM, 6 * TB);
     // diagonal-block buffers: rows of a short last block stay zero
     DMB_CUDA(cudaMemsetAsync(st.Dfp.p, 0, st.Dfp.bytes, c->stream));
     DMB_CUDA(cudaMemsetAsync(st.Dbp.p, 0, st.Dbp.bytes, c->stream));
     st.lp_n = N;
+    st.lp_fmt = (int)bf;
   }
   dim3 g((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
-  DMB_LAUNCH(c, (k_pack_a<false, true, float2>), g, 256, 0, N, N, Kpad, F, N, st.Lp.as<float>());
-  DMB_LAUNCH(c, (k_pack_a<true, true, float2>), g, 256, 0, N, N, Kpad, F, N, st.Ltp.as<float>());
+  if (bf) {
+    DMB_LAUNCH(c, (k_pack_a<false, true, float2, __nv_bfloat16>), g, 256, 0, N, N, Kpad, F, N,
+               st.Lp.as<__nv_bfloat16>());
+    DMB_LAUNCH(c, (k_pack_a<true, true, float2, __nv_bfloat16>), g, 256, 0, N, N, Kpad, F, N,
+               st.Ltp.as<__nv_bfloat16>());
+  } else {
+    DMB_LAUNCH(c, (k_pack_a<false, true, float2, float>), g, 256, 0, N, N, Kpad, F, N, st.Lp.as<float>());
+    DMB_LAUNCH(c, (k_pack_a<true, true, float2, float>), g, 256, 0, N, N, Kpad, F, N, st.Ltp.as<float>());
+  }
 }
 
 // inverse of diagonal block o (ow x ow, column-major in Xb with leading
 // dimension ld) -> forward operand, its transpose -> backward operand
 void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int ow) {
   TcState &st = tc_state(c);
+  dim3 g(TB / 32, TB / 32);
+  // in the format of the packed factor (tc_trsm_pack_factor ran first)
+  if (st.lp_fmt == 1) {
+    __nv_bfloat16 *df = st.Dfp.as<__nv_bfloat16>() + o * 2 * TB * 6 * TB;
+    __nv_bfloat16 *db = st.Dbp.as<__nv_bfloat16>() + o * 2 * TB * 6 * TB;
+    DMB_LAUNCH(c, (k_pack_a<true, false, double2, __nv_bfloat16>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB,
+               Xb, ld, df);
+    DMB_LAUNCH(c, (k_pack_a<false, false, double2, __nv_bfloat16>), g, 256, 0, (int64_t)ow, (int64_t)ow,
+               (int64_t)TB, Xb, ld, db);
+    return;
+  }
   float *df = st.Dfp.as<float>() + o * 2 * TB * 6 * TB;
   float *db = st.Dbp.as<float>() + o * 2 * TB * 6 * TB;
-  dim3 g(TB / 32, TB / 32);
   // forward: A(m, k) = Linv[m][k] = Xb[m + k ld]
-  DMB_LAUNCH(c, (k_pack_a<true, false, double2>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld, df);
+  DMB_LAUNCH(c, (k_pack_a<true, false, double2, float>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld,
+             df);
   // backward: A(m, k) = Linv[k][m] = Xb[k + m ld]
-  DMB_LAUNCH(c, (k_pack_a<false, false, double2>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld, db);
+  DMB_LAUNCH(c, (k_pack_a<false, false, double2, float>), g, 256, 0, (int64_t)ow, (int64_t)ow, (int64_t)TB, Xb, ld,
+             db);
 }
 
 // Y (op)= A_packed[rows a_row0.., K from a_kx0] * X[k0 : k0 + w], B packed here
@@ -912,35 +1006,44 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   if (M <= 0) return;
   const int64_t Kpad = round_up(w, 256), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
   const int kslot = (int)(Kpad / 256) - 1;
-  if (st.pb_key != Rpad) {
+  // operands in the format of the packed factor
+  const bool bf = st.lp_fmt == 1;
+  if (st.pb_key != Rpad || st.pb_fmt != (int)bf) {
     st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
     for (int i = 0; i < 4; i++) {
-      make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
-      make_map(&st.mapPbK128[i], st.Pb.as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
+      make_map_op(&st.mapPbK[i], st.Pb.p, bf, (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+      make_map_op(&st.mapPbK128[i], st.Pb.p, bf, (uint64_t)Rpad, 128, 1536 * (i + 1));
     }
     st.pb_key = Rpad;
+    st.pb_fmt = (int)bf;
   }
-  DMB_LAUNCH(c, k_pack_b, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk, N,
-             st.Pb.as<float>());
+  if (bf)
+    DMB_LAUNCH(c, k_pack_b<__nv_bfloat16>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w,
+               Kpad, Xk, N, st.Pb.as<__nv_bfloat16>());
+  else
+    DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk,
+               N, st.Pb.as<float>());
   // tile width from the autotuner, per (row tiles, columns, triangular
   // kind): 256 or 128 complex columns (128 doubles the CTAs of launches with
   // few row tiles); both give the same bits
   const int64_t tb1 = dmb::tune_bucket(Mpad / 64), tb2 = (Rpad / 128) * 4 + tri;
   const int cand = dmb::tune_choose(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, 2);
   const bool narrow = cand == 1;
-  const int cpb = 16 * c->precond_tf32_terms;
+  const int cpb = (bf ? 8 : 16) * c->precond_tf32_terms;
   dmb::TuneMark mk;
   dmb::tune_begin(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, cand, mk);
   kt_begin(c);
+#define GEMM_LAUNCH(BNV, BFV, MAPB, SMEMV)                                                                       \
+  DMB_LAUNCH(c, (k_tc_gemm<1, BNV, BFV>), dim3((unsigned)(Rpad / BNV), (unsigned)(Mpad / 64)), 128, SMEMV, mapA, \
+             MAPB[kslot], a_row0, a_kx0, (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>())
   if (narrow) {
-    dim3 grid((unsigned)(Rpad / 128), (unsigned)(Mpad / 64));
-    DMB_LAUNCH(c, (k_tc_gemm<1, 128>), grid, 128, TC_SMEM_128, mapA, st.mapPbK128[kslot], a_row0, a_kx0,
-               (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>());
+    if (bf) GEMM_LAUNCH(128, true, st.mapPbK128, TC_SMEM_128);
+    else GEMM_LAUNCH(128, false, st.mapPbK128, TC_SMEM_128);
   } else {
-    dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
-    DMB_LAUNCH(c, (k_tc_gemm<1, 256>), grid, 128, TC_SMEM, mapA, st.mapPbK[kslot], a_row0, a_kx0,
-               (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>());
+    if (bf) GEMM_LAUNCH(256, true, st.mapPbK, TC_SMEM);
+    else GEMM_LAUNCH(256, false, st.mapPbK, TC_SMEM);
   }
+#undef GEMM_LAUNCH
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
   dmb::tune_end(c, mk);

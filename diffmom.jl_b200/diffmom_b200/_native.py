@@ -52,6 +52,7 @@ OPT_TRUE_RESIDUAL = 8
 OPT_SPIN_LIMIT = 9
 OPT_TUNE_TC_GEMM = 10
 OPT_TUNE_TC_SYRK = 11
+OPT_PRECOND_BF16 = 12
 
 
 class DiffMoMError(RuntimeError):

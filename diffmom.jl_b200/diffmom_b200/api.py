@@ -97,16 +97,18 @@ class EFIEDevice:
         fails with TimeoutError; negative restores the default),
         "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; k pins candidate k:
         256- or 128-wide sweep GEMM tiles; 4-stage, 2-stage or persistent
-        factor-update schedules)."""
+        factor-update schedules), "precond_bf16" (0/1: BF16 instead of TF32
+        operand pieces for the complex64 factor updates and packed sweeps)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
                  "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,
                  "true_residual": nat.OPT_TRUE_RESIDUAL, "spin_limit": nat.OPT_SPIN_LIMIT,
-                 "tune_tc_gemm": nat.OPT_TUNE_TC_GEMM, "tune_tc_syrk": nat.OPT_TUNE_TC_SYRK}
+                 "tune_tc_gemm": nat.OPT_TUNE_TC_GEMM, "tune_tc_syrk": nat.OPT_TUNE_TC_SYRK,
+                 "precond_bf16": nat.OPT_PRECOND_BF16}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")
         self.ctx.call("dmb_set_option", codes[name], int(value))
-        if name in ("tensor_cores", "precond_tf32_terms"):
+        if name in ("tensor_cores", "precond_tf32_terms", "precond_bf16"):
             self.preconditioner = None
 
     def far_tile(self) -> int:
