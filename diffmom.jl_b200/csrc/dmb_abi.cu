@@ -156,9 +156,9 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       return;
     }
     if (option == DMB_OPT_PRECOND_BF16) {
-      DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "DMB_OPT_PRECOND_BF16 must be 0 or 1");
-      if (c->precond_bf16 != (value != 0)) c->pc_valid = false;
-      c->precond_bf16 = value != 0;
+      DMB_REQUIRE(value >= -1 && value <= 1, DMB_ERR_ARGUMENT, "DMB_OPT_PRECOND_BF16 must be -1, 0 or 1");
+      if (c->precond_bf16 != value) c->pc_valid = false;
+      c->precond_bf16 = value;
       return;
     }
     if (option == DMB_OPT_TUNE_TC_GEMM || option == DMB_OPT_TUNE_TC_SYRK) {
@@ -762,6 +762,12 @@ dmb_status dmb_solve_resident_many(dmb_ctx *c, const dmb_solve_params *p, int64_
       DMB_REQUIRE(E0s[r] != 0.0 || !sigma_out, DMB_ERR_ARGUMENT, "RCS needs a nonzero incident amplitude");
     }
     double t0 = dmb::now_ms();
+    // the preconditioner of this solve may use BF16 operand pieces (auto mode)
+    struct Scope {
+      dmb_ctx *c;
+      ~Scope() { c->pc_bf16_scope = false; }
+    } scope{c};
+    c->pc_bf16_scope = true;
     dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
     const size_t bytes = sizeof(double2) * c->n * R;
     c->d_rhs.ensure(bytes);

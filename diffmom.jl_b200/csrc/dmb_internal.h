@@ -273,7 +273,14 @@ struct dmb_ctx {
   };
   std::map<std::vector<int64_t>, GraphEntry> gm_graphs;
   int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
-  bool precond_bf16 = false;     // those operands split into BF16 pieces instead of TF32 (kind::f16 MMA)
+  // those operands split into BF16 pieces (kind::f16 MMA) instead of TF32:
+  // 1 always, 0 never, -1 (default) inside the many-right-hand-side resident
+  // solves only (pc_bf16_scope set), where right-preconditioned GMRES with
+  // FP64-accurate Krylov products and the FP64 residual as the judge makes the
+  // preconditioner's precision a matter of iteration count alone
+  int precond_bf16 = -1;
+  bool pc_bf16_scope = false;
+  bool pc_bf16() const { return precond_bf16 > 0 || (precond_bf16 < 0 && pc_bf16_scope); }
   int far_tile_used = 0;         // tile width of the last assembly
   // autotuner pins per family (0: tuned, k: candidate k - 1)
   int tune_pin[dmb::TUNE_FAMILIES] = {0, 0};

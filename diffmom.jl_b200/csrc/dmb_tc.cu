@@ -776,7 +776,7 @@ void tc_ldlt_update_c64(dmb_ctx *c, int64_t N, int64_t r0, int64_t c_hi, int64_t
   const int64_t npadA = ((N + 63) / 64) * 64;
   const int64_t npadB = ((N + TC_BN - 1) / TC_BN) * TC_BN;
   const int64_t Kpad = ((K + 255) / 256) * 256, ld = 6 * Kpad;
-  const bool bf = c->precond_bf16;
+  const bool bf = c->pc_bf16();
   if (st.n_key[slot] != N || st.upd_fmt[slot] != (int)bf) {
     bA.ensure(sizeof(float) * 2 * npadA * 6 * 1024);
     bB.ensure(sizeof(float) * npadB * 6 * 1024);
@@ -947,7 +947,7 @@ void tc_trsm_pack_factor(dmb_ctx *c, const float2 *F, int64_t N) {
   ensure_gemm(c, st);
   const int64_t Mpad = round_up(N, 64), Kpad = round_up(N, 256), ld = 6 * Kpad;
   const int64_t nout = (N + TB - 1) / TB;
-  const bool bf = c->precond_bf16;
+  const bool bf = c->pc_bf16();
   if (st.lp_n != N || st.lp_fmt != (int)bf) {
     st.Lp.ensure(sizeof(float) * 2 * Mpad * ld);
     st.Ltp.ensure(sizeof(float) * 2 * Mpad * ld);

@@ -97,8 +97,10 @@ class EFIEDevice:
         fails with TimeoutError; negative restores the default),
         "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; k pins candidate k:
         256- or 128-wide sweep GEMM tiles; 4-stage, 2-stage or persistent
-        factor-update schedules), "precond_bf16" (0/1: BF16 instead of TF32
-        operand pieces for the complex64 factor updates and packed sweeps)."""
+        factor-update schedules), "precond_bf16" (1 / 0 / -1 = default: BF16
+        instead of TF32 operand pieces for the complex64 factor updates and
+        packed sweeps always / never / inside the many-incidence resident
+        solves only)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
                  "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,

@@ -156,12 +156,14 @@ const char *dmb_version(void);
  * process; the candidates give the same bits. */
 #define DMB_OPT_TUNE_TC_GEMM 10
 #define DMB_OPT_TUNE_TC_SYRK 11
-/* DMB_OPT_PRECOND_BF16: 1 splits the operands of the complex64 factor updates
- * and of the packed many-RHS sweeps into BF16 pieces (hi + lo, ~16 bits, the
- * three products on the kind::f16 tensor-core path at twice the TF32 rate,
- * FP32 accumulation) instead of TF32 pieces (~21 bits); 0 (default) keeps
- * TF32.  Only the preconditioner changes (right-preconditioned GMRES keeps its
- * preconditioned vectors and the FP64 residual stays the judge). */
+/* DMB_OPT_PRECOND_BF16: the operands of the complex64 factor updates and of
+ * the packed many-RHS sweeps as BF16 pieces (hi + lo, ~16 bits, the three
+ * products on the kind::f16 tensor-core path at twice the TF32 rate, FP32
+ * accumulation) instead of TF32 pieces (~21 bits).  1: always; 0: never; -1
+ * (default): inside dmb_solve_resident_many only, whose right-preconditioned
+ * GMRES keeps its preconditioned vectors, forms its Krylov products
+ * FP64-accurately and is judged on the FP64 residual, so the preconditioner's
+ * precision changes the iteration count, not the result. */
 #define DMB_OPT_PRECOND_BF16 12
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair RWG tile width used by the last assembly on this context. */
