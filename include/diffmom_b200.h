@@ -110,10 +110,10 @@ const char *dmb_version(void);
  * FP64-accurate INT8-slice product (no refinement cycle needed); 0 runs it in
  * 3xTF32 with FP64-residual refinement. */
 #define DMB_OPT_EXACT_KRYLOV 4
-/* DMB_OPT_PRECOND_TF32_TERMS: TF32 products per complex MAC in the tensor-core
+/* DMB_OPT_PRECOND_TF32_TERMS: products per complex MAC in the tensor-core
  * updates of the complex64 factorisation and in the batched triangular sweeps
- * that apply it: 3 (default, hi*hi + hi*lo + lo*hi: FP32-level accuracy) or 1
- * (hi*hi only: TF32-level accuracy, a third of the tensor-core work).  Only the
+ * that apply it: 3 (default, hi*hi + hi*lo + lo*hi) or 1 (hi*hi only, a third
+ * of the tensor-core work); the pieces are TF32 or BF16 (DMB_OPT_PRECOND_BF16).  Only the
  * preconditioner changes; right-preconditioned GMRES keeps the preconditioned
  * vectors (flexible form), so the solution accuracy is unaffected. */
 #define DMB_OPT_PRECOND_TF32_TERMS 5
