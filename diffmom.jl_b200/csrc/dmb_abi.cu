@@ -16,6 +16,14 @@
 
 namespace {
 
+// Marks a resident solve: inside it the complex64 preconditioner's
+// tensor-core work may use BF16 operand pieces (DMB_OPT_PRECOND_BF16 = -1).
+struct PcBf16Scope {
+  dmb_ctx *c;
+  explicit PcBf16Scope(dmb_ctx *ctx) : c(ctx) { c->pc_bf16_scope = true; }
+  ~PcBf16Scope() { c->pc_bf16_scope = false; }
+};
+
 template <class F> dmb_status guarded(dmb_ctx *c, F &&f) {
   if (!c) return DMB_ERR_ARGUMENT;
   std::lock_guard<std::mutex> lk(c->mu);
@@ -730,6 +738,7 @@ dmb_status dmb_solve_resident(dmb_ctx *c, const dmb_solve_params *p, dmb_gmres_s
     check_finite(p->kvec, 3, "plane-wave k_vec");
     check_finite(p->pol, 3, "plane-wave polarization");
     double t0 = dmb::now_ms();
+    PcBf16Scope bf_scope(c);
     resident_setup(c, p);
     size_t bytes = sizeof(double2) * c->n;
     c->d_rhs.ensure(bytes);
@@ -762,12 +771,7 @@ dmb_status dmb_solve_resident_many(dmb_ctx *c, const dmb_solve_params *p, int64_
       DMB_REQUIRE(E0s[r] != 0.0 || !sigma_out, DMB_ERR_ARGUMENT, "RCS needs a nonzero incident amplitude");
     }
     double t0 = dmb::now_ms();
-    // the preconditioner of this solve may use BF16 operand pieces (auto mode)
-    struct Scope {
-      dmb_ctx *c;
-      ~Scope() { c->pc_bf16_scope = false; }
-    } scope{c};
-    c->pc_bf16_scope = true;
+    PcBf16Scope bf_scope(c);
     dmb::assemble(c, p->k, p->eta0, p->quad_order, p->precision);
     const size_t bytes = sizeof(double2) * c->n * R;
     c->d_rhs.ensure(bytes);
@@ -932,6 +936,7 @@ dmb_status batch_item(dmb_ctx *c, const dmb_solve_params *p, dmb_batch_item &it,
     DMB_CUDA(cudaEventCreate(&e1));
     DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_asm, 0));
     DMB_CUDA(cudaEventRecord(e0, c->stream));
+    PcBf16Scope bf_scope(c);
     if (it.zs) {
       check_finite(it.zs, 2 * c->nt, "surface impedance");
       dmb::apply_impedance(c, it.zs);
@@ -1033,7 +1038,18 @@ dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_it
   std::vector<int64_t> order(count);
   for (int64_t i = 0; i < count; i++) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t c2) { return items[a].n > items[c2].n; });
-  // 1. uploads and host topology, lanes in parallel
+  cudaEvent_t ev_start = nullptr, ev_asm = nullptr;
+  cudaEventCreate(&ev_start);
+  cudaEventCreate(&ev_asm);
+  // the batch's device time starts here: it includes the surfaces' set-up
+  cudaEventRecord(ev_start, b->stream);
+  // 1. uploads, host topology, per-triangle caches and far-pair panels,
+  // lanes in parallel (each surface on its own stream); the panels need the
+  // tile width, known once the tuner has timed the largest surface's size
+  // bucket (on a first call they are built in step 2 instead)
+  const bool f64 = p->precision == DMB_PREC_FP64;
+  int64_t nmax = 0;
+  for (int64_t i = 0; i < count; i++) nmax = std::max<int64_t>(nmax, items[i].n);
   dmb_status st = lanes_run(b, count, order, [&](int64_t s) {
     dmb_ctx *c = b->slots[s];
     const dmb_batch_item &it = items[s];
@@ -1041,21 +1057,27 @@ dmb_status dmb_batch_solve(dmb_batch *b, const dmb_solve_params *p, dmb_batch_it
     if (r == DMB_OK)
       r = dmb_rwg_upload(c, it.n, it.tplus, it.tminus, it.evert, it.vplus_opp, it.vminus_opp, it.len,
                          it.area_plus, it.area_minus);
+    if (r == DMB_OK)
+      r = guarded(c, [&] {
+        dmb::ensure_cache(c, p->quad_order);
+        const int T = dmb::far_tile_width_known(c, nmax, f64);
+        if (T > 0) dmb::far_panels(c, T, f64);
+      });
     return r;
   });
-  if (st != DMB_OK) return st;
+  if (st != DMB_OK) {
+    cudaEventDestroy(ev_start);
+    cudaEventDestroy(ev_asm);
+    return st;
+  }
   // 2. every surface's impedance matrix: the far tiles of all surfaces in one
   // launch, their near values and near sums in one launch each
-  cudaEvent_t ev_start = nullptr, ev_asm = nullptr;
-  cudaEventCreate(&ev_start);
-  cudaEventCreate(&ev_asm);
   std::vector<dmb_ctx *> cs(b->slots.begin(), b->slots.begin() + count);
   {
     dmb_ctx *c0 = cs[0];
     std::lock_guard<std::mutex> lk(c0->mu);
     try {
       StreamSwap sw(c0, b->stream);
-      DMB_CUDA(cudaEventRecord(ev_start, b->stream));
       b->last_assembly_ms = dmb::assemble_batch(cs, p->k, p->eta0, p->quad_order, p->precision, b->asm_bufs);
       DMB_CUDA(cudaEventRecord(ev_asm, b->stream));
     } catch (const DmbError &e) {

@@ -566,17 +566,35 @@ unsigned far_error_word(dmb_ctx *c, bool f64) {
 // kernel) and the fastest is kept for the process.  DMB_OPT_FAR_TILE pins a
 // width instead.  Every width writes the same Z bit for bit (the per-entry
 // arithmetic does not depend on the tiling).
+static std::mutex g_far_tune_mu;
+static std::vector<std::pair<int64_t, int>> g_far_tune;  // (device, size bucket, precision, nq) -> width
+
+static int64_t far_tune_key(int device, int64_t n, bool f64, int nq) {
+  int bucket = 0;
+  while ((int64_t)1 << (bucket + 1) <= n) bucket++;
+  return ((int64_t)device << 24) | ((int64_t)bucket << 8) | ((f64 ? 1 : 0) << 4) | nq;
+}
+
+// The width the tuner already chose for a mesh of n RWG functions (or the
+// context's pin), 0 if that bucket has not been timed yet.
+int far_tile_width_known(dmb_ctx *c, int64_t n, bool f64) {
+  if (c->far_tile > 0) return far_tile_width_valid(c->far_tile, f64) ? c->far_tile : 0;
+  const int64_t key = far_tune_key(c->device, n, f64, c->nq);
+  std::lock_guard<std::mutex> lk(g_far_tune_mu);
+  for (auto &e : g_far_tune)
+    if (e.first == key) return e.second;
+  return 0;
+}
+
 int far_tile_width(dmb_ctx *c, bool f64, double k, double inv_k2, double omega_mu0) {
   if (c->far_tile > 0) {
     DMB_REQUIRE(far_tile_width_valid(c->far_tile, f64), DMB_ERR_ARGUMENT,
                 "DMB_OPT_FAR_TILE must be " + std::string(f64 ? "16 or 32" : "32 or 64") + " for this precision");
     return c->far_tile_used = c->far_tile;
   }
-  int bucket = 0;
-  while ((int64_t)1 << (bucket + 1) <= c->n) bucket++;
-  const int64_t key = ((int64_t)c->device << 24) | ((int64_t)bucket << 8) | ((f64 ? 1 : 0) << 4) | c->nq;
-  static std::mutex mu;
-  static std::vector<std::pair<int64_t, int>> table;
+  const int64_t key = far_tune_key(c->device, c->n, f64, c->nq);
+  auto &mu = g_far_tune_mu;
+  auto &table = g_far_tune;
   {
     std::lock_guard<std::mutex> lk(mu);
     for (auto &e : table)

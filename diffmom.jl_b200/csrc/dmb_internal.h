@@ -274,10 +274,10 @@ struct dmb_ctx {
   std::map<std::vector<int64_t>, GraphEntry> gm_graphs;
   int precond_tf32_terms = 3;    // TF32 products of the complex64 factor updates and packed sweeps (3 or 1)
   // those operands split into BF16 pieces (kind::f16 MMA) instead of TF32:
-  // 1 always, 0 never, -1 (default) inside the many-right-hand-side resident
-  // solves only (pc_bf16_scope set), where right-preconditioned GMRES with
-  // FP64-accurate Krylov products and the FP64 residual as the judge makes the
-  // preconditioner's precision a matter of iteration count alone
+  // 1 always, 0 never, -1 (default) inside the resident solves only
+  // (dmb_solve_resident[_many], batch surfaces: pc_bf16_scope set), whose
+  // GMRES is judged on the FP64 residual, so the preconditioner's precision is
+  // a matter of iteration count alone
   int precond_bf16 = -1;
   bool pc_bf16_scope = false;
   bool pc_bf16() const { return precond_bf16 > 0 || (precond_bf16 < 0 && pc_bf16_scope); }
@@ -379,6 +379,7 @@ bool far_tile_width_valid(int T, bool f64);
 void far_panels(dmb_ctx *c, int T, bool f64);
 void far_tiles(dmb_ctx *c, int T, bool f64, double k, double inv_k2, double omega_mu0);
 int far_tile_width(dmb_ctx *c, bool f64, double k, double inv_k2, double omega_mu0);
+int far_tile_width_known(dmb_ctx *c, int64_t n, bool f64);  // 0: not tuned yet
 unsigned far_error_word(dmb_ctx *c, bool f64);
 void far_release(dmb_ctx *c);
 void far_tiles_batched(const std::vector<dmb_ctx *> &cs, int T, bool f64, double k, double inv_k2,

@@ -160,10 +160,10 @@ const char *dmb_version(void);
  * the packed many-RHS sweeps as BF16 pieces (hi + lo, ~16 bits, the three
  * products on the kind::f16 tensor-core path at twice the TF32 rate, FP32
  * accumulation) instead of TF32 pieces (~21 bits).  1: always; 0: never; -1
- * (default): inside dmb_solve_resident_many only, whose right-preconditioned
- * GMRES keeps its preconditioned vectors, forms its Krylov products
- * FP64-accurately and is judged on the FP64 residual, so the preconditioner's
- * precision changes the iteration count, not the result. */
+ * (default): inside the resident solves only (dmb_solve_resident,
+ * dmb_solve_resident_many, dmb_batch_solve), whose GMRES is judged on the FP64
+ * residual, so the preconditioner's precision changes the iteration count,
+ * not the result; dmb_nf_build / dmb_nf_apply / dmb_gmres keep TF32 pieces. */
 #define DMB_OPT_PRECOND_BF16 12
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair RWG tile width used by the last assembly on this context. */
