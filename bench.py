@@ -645,9 +645,10 @@ def make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks=None):
         if il > 0:
             alg = il * 8.0 * N * N * R_WAVES  # 8 flops per complex MAC, counted once
             achieved = (alg / 1e12) / (ims / 1e3)
+            prods = iw / (il * 8.0 * N * N * R_WAVES)  # int8 products per launch
             line["roofline"] = {
-                "kernel": "k_oz_gemm (Z X with R = %d columns: FP64-accurate complex GEMM from int8 slice "
-                          "products on tcgen05 kind::i8)" % R_WAVES,
+                "kernel": "k_oz_gemm (Z X with R = %d columns: FP64-accurate complex GEMM from int8 residue "
+                          "products on tcgen05 kind::i8, CRT recombination)" % R_WAVES,
                 "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                 "frac": achieved / bf16 if bf16 else None,
                 "traffic": OZ_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
@@ -660,9 +661,9 @@ def make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks=None):
                 "executed_int8": {"achieved_pops": (iw / 1e15) / (ims / 1e3), "peak_pops": 4.5,
                                   "frac": (iw / 1e15) / (ims / 1e3) / 4.5,
                                   "peak_source": "nominal dense INT8 (not in MEASURED_PEAKS.json)",
-                                  "note": "26 int8 slice products of the real-stacked (2N x 2N) x (2N x R) "
-                                          "system per launch (FP64-accurate Krylov products; the true "
-                                          "residual comes from them)"}}
+                                  "note": "%.0f int8 products (one per modulus) of the real-stacked "
+                                          "(2N x 2N) x (2N x R) system per launch (FP64-accurate Krylov "
+                                          "products; the true residual comes from them)" % prods}}
         fams = {"k_tc_gemm (triangular-sweep GEMMs)": head["kernel_gemm"],
                 "k_tc_syrk + k_tc_pack (factorisation trailing updates)": head["kernel_factor"]}
         line["roofline_tc"] = {

@@ -141,6 +141,11 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->pc_valid = false;
       return;
     }
+    if (option == DMB_OPT_INT8_SCHEME) {
+      DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "int8 scheme must be 0 (residues) or 1 (slices)");
+      c->int8_scheme = value;
+      return;
+    }
     if (option == DMB_OPT_EXACT_KRYLOV) {
       c->exact_krylov = value != 0;
       return;

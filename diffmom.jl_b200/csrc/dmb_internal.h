@@ -279,6 +279,7 @@ struct dmb_ctx {
   // GMRES is judged on the FP64 residual, so the preconditioner's precision is
   // a matter of iteration count alone
   int precond_bf16 = -1;
+  int int8_scheme = 0;  // FP64-accurate INT8 product: 0 residues modulo coprime moduli (CRT), 1 fixed-point slices
   bool pc_bf16_scope = false;
   bool pc_bf16() const { return precond_bf16 > 0 || (precond_bf16 < 0 && pc_bf16_scope); }
   int far_tile_used = 0;         // tile width of the last assembly
@@ -449,8 +450,10 @@ void tc_release(dmb_ctx *c);
 // FP64-accurate complex64 Z X on the INT8 tensor cores (dmb_ozaki.cu)
 bool oz_available(dmb_ctx *c);
 bool krylov_exact_int8(dmb_ctx *c, int64_t nrhs);  // the Krylov product is the INT8-slice one
-// lmax: slice-pair levels p + q <= lmax are kept (6: 26 int8 products, ~7e-13
-// normwise; 5: 21 products, ~4e-11 -- enough for the Krylov recurrence)
+// lmax: the accuracy class.  Residue scheme: 6 -> 13 moduli (13 int8
+// products, ~1e-13 normwise), 5 -> 12 moduli (12 products, ~1e-12).  Slice
+// scheme: slice-pair levels p + q <= lmax are kept (6: 26 int8 products,
+// ~7e-13; 5: 21 products, ~4e-11 -- enough for the Krylov recurrence)
 constexpr int OZ_LEVELS_RESIDUAL = 6, OZ_LEVELS_KRYLOV = 5;
 void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax = OZ_LEVELS_RESIDUAL);
 void oz_prepare(dmb_ctx *c);

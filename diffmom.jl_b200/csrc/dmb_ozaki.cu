@@ -2,24 +2,48 @@
 // the INT8 tensor cores (tcgen05.mma.kind::i8, exact int32 accumulation):
 // the refinement and true residuals of the batched solves.
 //
-// Method (error-free splitting, Ozaki, Ogita, Oishi & Rump, "Error-free
-// transformations of matrix multiplication by using fast routines of matrix
-// multiplication and its applications", Numer. Algorithms 59, 2012, here with
-// fixed-point int8 slices):
-//   * complex as one real product: row m of Z gives a real row [Zr, -Zi] and an
-//     imaginary row [Zi, Zr] against the column [Xr; Xi] (K = 2N);
-//   * each complex row m is scaled by sigma_m = 2^e (the smallest power of two
-//     above max_k max(|Zr|, |Zi|)), each column r of X by tau_r likewise, and
-//     the scaled values in (-1, 1) are cut into OZ_S slices of OZ_BETA = 7
+// Complex as one real product: row m of Z gives a real row [Zr, -Zi] and an
+// imaginary row [Zi, Zr] against the column [Xr; Xi] (K = 2N).  Each complex
+// row m of Z is scaled by sigma_m = 2^e (the smallest power of two above
+// max_k max(|Zr|, |Zi|)), each column r of X by tau_r likewise.  Two ways of
+// making the FP64-accurate product from exact int8 products:
+//
+// Residue scheme (default; the modular-arithmetic emulation of Ozaki, Uchino
+// and Imamura, "Ozaki Scheme II: a GEMM-oriented emulation of floating-point
+// matrix multiplication using an integer modular technique", 2025):
+//   * the scaled values become integers A' = rint(2^a Z / sigma) and
+//     B' = rint(2^b X / tau), |A'| <= 2^a, |B'| <= 2^b, with a + b chosen so
+//     that the exact integer product C' = A' B' satisfies
+//     K 2^(a + b) < M / 2, M the product of the moduli (13 pairwise coprime
+//     moduli <= 256: M ~ 2^102.5, a = b = 43 at K = 21,504);
+//   * per modulus m_i the symmetric residues A' mod m_i, B' mod m_i fit int8,
+//     and their int8 product is exact in int32 (128^2 K < 2^31), so
+//     C'_i = (A'_i B'_i) mod m_i = C' mod m_i;
+//   * Chinese remainder theorem as a fraction: C' / M = sum_i C'_i y_i / m_i
+//     (mod 1), y_i = (M / m_i)^-1 mod m_i.  The drains accumulate the 96-bit
+//     fixed-point fraction S = sum_i C'_i f_i (mod 2^96), f_i =
+//     round(2^96 y_i / m_i), as a uint64 high word (in Y's place) and a
+//     uint32 low word (scratch); S / 2^96 is C' / M to within 2^-85, and
+//     Y = (int64(hi) + lo 2^-32) M 2^-64 2^-(a + b) sigma tau.  (A 64-bit
+//     fraction alone leaves ~2^-53 M of C', about 1e-12 of an EFIE row's
+//     product.)  One int8 product per modulus: 13 for the residuals (~1e-13
+//     normwise), 12 for the Krylov operator (b reduced by the missing modulus,
+//     ~1e-11).  Integer sums are associative: every split of the moduli over
+//     CTAs gives the same bits.
+// Slice scheme (Ozaki, Ogita, Oishi & Rump, "Error-free transformations of
+// matrix multiplication by using fast routines of matrix multiplication and
+// its applications", Numer. Algorithms 59, 2012, with fixed-point int8
+// slices):
+//   * the scaled values in (-1, 1) are cut into OZ_S slices of OZ_BETA = 7
 //     bits, v = sum_p a_p 2^(-7(p+1)) with integer a_p in [-127, 127] (exact in
 //     double arithmetic);
 //   * slice products a_p . b_q are exact in int32 (127^2 x 2N < 2^31 per pair);
 //     pairs with p + q <= OZ_LMAX (0-based) are kept, summed in TMEM per level
 //     (as many pairs per drain as int32 allows) and drained into FP64 with the
 //     exact power-of-two weights sigma_m tau_r 2^(-7(L+2)).
-// With OZ_S = 6 and all levels up to OZ_LMAX = 6 (26 int8 products) the
-// product is ~7e-13 relative (normwise) on EFIE rows; the Krylov products of
-// GMRES keep levels <= 5 (21 products, ~4e-11), the true residuals all levels.
+//   With OZ_S = 6 and all levels up to OZ_LMAX = 6 (26 int8 products) the
+//   product is ~7e-13 relative (normwise) on EFIE rows; the Krylov products
+//   keep levels <= 5 (21 products, ~4e-11).
 //
 // Kernel k_oz_gemm: a persistent grid (one CTA per SM) over 64 x 256 complex
 // output tiles -- whole tiles in data-parallel waves, the tail tiles split
@@ -30,7 +54,10 @@
 //                     256-column s32 TMEM accumulators used in turn (one
 //                     level accumulates while the other drains), one commit
 //                     per drain;
-//   warps 0-3         drain each level: tcgen05.ld, scale, FP64 store / add.
+//   warps 0-3         drain each level (slices: tcgen05.ld, scale, FP64
+//                     store / add) or modulus (residues: tcgen05.ld, reduce
+//                     mod m_i, uint64 fraction add; the last modulus of a tile
+//                     converts to FP64).
 // Every wait is bounded (error bit, abort flag, TMEM freed); no multicast.
 #include <algorithm>
 #include <vector>
@@ -57,13 +84,37 @@ constexpr int OZ_SMEM = OZ_STAGES * (OZ_A_STAGE + OZ_B_STAGE) + OZ_E_BYTES + 256
 constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
+// pairwise coprime moduli, largest first (255 = 3 5 17, 253 = 11 23,
+// 247 = 13 19, 217 = 7 31, the rest prime)
+constexpr int OZ_NMOD = 13;
+constexpr int OZ_MODULI[OZ_NMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211};
+
 struct OzSched {
   int n;
-  int arow[OZ_MAXP];      // first A'' row of the pair's Z slice
-  int brow[OZ_MAXP];      // first B'' row of the pair's X slice
+  int arow[OZ_MAXP];      // first A'' row of the pair's Z slice / residue plane
+  int brow[OZ_MAXP];      // first B'' row of the pair's X slice / residue plane
   int close[OZ_MAXP];     // 1: the TMEM sum is drained after this pair
-  double lscale[OZ_MAXP]; // weight of the pair's level: 2^(-7 (L + 2))
+  double lscale[OZ_MAXP]; // slices: weight of the pair's level, 2^(-7 (L + 2))
+  // residues: modulus, reduction constants (oz_mod), CRT fraction
+  // round(2^96 y_i / m_i) as high 64 and low 32 bits
+  int mod[OZ_MAXP];
+  unsigned mmul[OZ_MAXP], moff[OZ_MAXP];
+  unsigned long long frac[OZ_MAXP];
+  unsigned fraclo[OZ_MAXP];
+  double cscale;          // residues: M 2^-64 2^-(a + b)
 };
+
+// v mod m in [0, m) for an int8-product sum |v| <= 2^31 - 2^14 and
+// 199 <= m <= 256, in integer arithmetic: u = v + moff (moff = m
+// floor(2^31 / m), so 0 < u < 2^32 and u = v mod m), q = floor(u mmul /
+// 2^39) with mmul = ceil(2^39 / m) is floor(u / m) or one more (the error of
+// u mmul / 2^39 is below u / 2^39 < 2^-7), one correction.
+__device__ __forceinline__ unsigned oz_mod(int v, unsigned m, unsigned mmul, unsigned moff) {
+  const unsigned u = (unsigned)v + moff;
+  const unsigned q = __umulhi(u, mmul) >> 7;
+  const int r = (int)(u - q * m);
+  return (unsigned)(r < 0 ? r + (int)m : r);
+}
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
@@ -126,13 +177,20 @@ __device__ __forceinline__ bool oz_next_seg(OzIter &it, OzSeg &sg) {
   return true;
 }
 constexpr int OZ_TILE_ELEMS = 64 * OZ_BN;  // complex outputs per tile (workspace slot size)
+constexpr int OZ_S_ELEMS = 128 * OZ_BN;    // residues: fraction sums per tile (real-stacked rows)
 
-__global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUtensorMap tmA,
+// warps per CTA: slices 4 drain + producer + MMA issuer; residues 8 drain
+// (two per TMEM lane quarter, each on half of the columns) + producer + MMA
+template <bool CRT> constexpr int oz_threads() { return CRT ? 320 : 192; }
+
+template <bool CRT>
+__global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB,
                                                     const __grid_constant__ OzSched sc, int kchunks, int64_t M,
                                                     int64_t Rv, double2 *__restrict__ Y, double2 *__restrict__ P,
                                                     int64_t ldy, int ncol, int64_t ntiles,
                                                     const double *__restrict__ rs, const double *__restrict__ cs,
+                                                    unsigned long long *__restrict__ Sh, unsigned *__restrict__ Sl,
                                                     unsigned *err) {
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -158,7 +216,7 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(accf0 + 8 * b, 1);
-      mbar_init(acce0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, CRT ? 8 : 1);  // residues: one arrival per drain warp
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -174,7 +232,8 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem_d = *tmem_slot;
 
-  if (warp == 4) {
+  constexpr int W_PROD = CRT ? 8 : 4, W_MMA = CRT ? 9 : 5;
+  if (warp == W_PROD) {
     if (lane == 0) {
       long long t = 0;
       OzIter it;
@@ -198,7 +257,7 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
         }
       }
     }
-  } else if (warp == 5) {
+  } else if (warp == W_MMA) {
     if (lane == 0) {
       long long t = 0;
       int g = 0;
@@ -238,6 +297,87 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
             first = true;
           }
         }
+      }
+    }
+  } else if (CRT) {
+    // residue drains: each of warps 0-7 works alone on the 32 TMEM lanes =
+    // tile rows of its quarter (warp & 3; rows 0-63: real parts of the 64
+    // complex rows, 64-127: imaginary parts) and on half of the columns
+    // (warp >> 2).  Per modulus a thread reads its row's int32 sums, 16
+    // columns at a time, reduces them mod m_i and adds C'_i f_i to the 96-bit
+    // fraction sum of each element, kept in the CTA's scratch tile (high
+    // words Sh, low words Sl; column-major with the 128 rows contiguous, so a
+    // warp's accesses are coalesced).  The last modulus of a whole tile
+    // writes the FP64 result into Y instead.  Each warp arrives on the
+    // accumulator-empty barrier by itself (count 8).
+    const int row = (warp & 3) * 32 + lane;
+    const int chalf = warp >> 2;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    int g = 0;
+    bool alive = true;
+    OzIter it;
+    oz_iter_init(it, ntiles, sc.n);
+    OzSeg sg;
+    while (alive && oz_next_seg(it, sg)) {
+      const int64_t row0 = 64 * (sg.t / ncol), col0 = (int64_t)OZ_BN * (sg.t % ncol);
+      const int64_t sbase = ((int64_t)blockIdx.x * 3 + (sg.slot < 0 ? 2 : sg.slot)) * OZ_S_ELEMS + row;
+      unsigned long long *Sht = Sh + sbase;
+      unsigned *Slt = Sl + sbase;
+      const int64_t gr = row0 + (row & 63);
+      const bool row_ok = gr < M;
+      const double rsc = row_ok ? rs[gr] * sc.cscale : 0.0;
+      // this warp's 16-column groups that hold data
+      const int cc0 = chalf * (OZ_BN / 32);
+      const int cc1 = (int)min((int64_t)(cc0 + OZ_BN / 32), (Rv - col0 + 15) / 16);
+      for (int i = sg.p0; i < sg.p1; i++) {
+        const bool first = i == sg.p0;
+        const bool fin = sg.slot < 0 && i + 1 == sg.p1;
+        const unsigned gm = (unsigned)sc.mod[i], gmul = sc.mmul[i], goff = sc.moff[i];
+        const unsigned long long gfr = sc.frac[i], gfl = sc.fraclo[i];
+        // warp-uniform outcome: the loads below are warp-collective
+        const bool got = mbar_wait(accf0 + 8 * (g & 1), (uint32_t)(g >> 1) & 1u, err, abort_flag);
+        if (!__all_sync(0xffffffffu, got)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tacc = tmem_d + (uint32_t)((g & 1) * OZ_BN) + lane_base;
+        for (int cc = cc0; cc < cc1; cc++) {
+          unsigned long long oh[16];
+          unsigned ol[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) {
+            oh[q] = first ? 0ull : Sht[(int64_t)(cc * 16 + q) * 128];
+            ol[q] = first ? 0u : Slt[(int64_t)(cc * 16 + q) * 128];
+          }
+          uint32_t v[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15])
+              : "r"(tacc + (uint32_t)(cc * 16)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int q = 0; q < 16; q++) {
+            const int c = cc * 16 + q;
+            const unsigned long long u = oz_mod((int)v[q], gm, gmul, goff);
+            const unsigned long long tl = (unsigned long long)ol[q] + u * gfl;
+            const unsigned long long th = oh[q] + u * gfr + (tl >> 32);
+            if (fin) {
+              if (row_ok && col0 + c < Rv)
+                reinterpret_cast<double *>(Y)[2 * ((col0 + c) * ldy + gr) + (row >> 6)] =
+                    fma((double)(unsigned)tl, 0x1p-32, (double)(long long)th) * rsc * cs[col0 + c];
+            } else {
+              Sht[(int64_t)c * 128] = th;
+              Slt[(int64_t)c * 128] = (unsigned)tl;
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * (g & 1));
+        g++;
       }
     }
   } else {
@@ -331,17 +471,41 @@ __global__ void __launch_bounds__(192, 1) k_oz_gemm(const __grid_constant__ CUte
 // Tail tiles made of partial segments: tile fix[3 i] = the sum, in listed
 // order, of workspace slots fix[3 j + 2] (= 2 CTA + slot) for the entries j of
 // its run (fix[3 i + 1] = run length, given on the run's first entry)
+// (residues: the partial fraction sums of a tile sit in the scratch tiles of
+// the CTAs that computed them, high and low words, rows 0-63 real and 64-127
+// imaginary parts; they are added mod 2^96 and converted with the scales)
+template <bool CRT>
 __global__ void k_oz_fixup(const int64_t *__restrict__ fix, const int *__restrict__ runs, int ncol, int64_t M,
-                           int64_t Rv, double2 *__restrict__ Y, const double2 *__restrict__ P, int64_t ldy) {
+                           int64_t Rv, double2 *__restrict__ Y, const double2 *__restrict__ P, int64_t ldy,
+                           const double *__restrict__ rs, const double *__restrict__ cs, double cscale,
+                           const unsigned long long *__restrict__ Sh, const unsigned *__restrict__ Sl) {
   const int j0 = runs[blockIdx.x];
   const int64_t t = fix[3 * j0], len = fix[3 * j0 + 1];
   const int64_t row0 = 64 * (t / ncol), col0 = (int64_t)OZ_BN * (t % ncol);
   for (int e = threadIdx.x; e < OZ_TILE_ELEMS; e += blockDim.x) {
     const int64_t r = row0 + (e & 63), c = col0 + (e >> 6);
     if (r >= M || c >= Rv) continue;
-    double2 acc = make_double2(0, 0);
-    for (int64_t j = 0; j < len; j++) acc = cadd(acc, P[fix[3 * (j0 + j) + 2] * OZ_TILE_ELEMS + e]);
-    Y[c * ldy + r] = acc;
+    if constexpr (CRT) {
+      // slot s = 2 CTA + k: scratch tile 3 CTA + k
+      unsigned long long hr = 0, hi = 0, lr = 0, li = 0;
+      for (int64_t j = 0; j < len; j++) {
+        const int64_t sl = fix[3 * (j0 + j) + 2];
+        const int64_t o = ((sl >> 1) * 3 + (sl & 1)) * OZ_S_ELEMS + (e >> 6) * 128 + (e & 63);
+        hr += Sh[o];
+        hi += Sh[o + 64];
+        lr += Sl[o];
+        li += Sl[o + 64];
+      }
+      hr += lr >> 32;
+      hi += li >> 32;
+      const double w = rs[r] * cs[c] * cscale;
+      Y[c * ldy + r] = make_double2(fma((double)(unsigned)lr, 0x1p-32, (double)(long long)hr) * w,
+                                    fma((double)(unsigned)li, 0x1p-32, (double)(long long)hi) * w);
+    } else {
+      double2 acc = make_double2(0, 0);
+      for (int64_t j = 0; j < len; j++) acc = cadd(acc, P[fix[3 * (j0 + j) + 2] * OZ_TILE_ELEMS + e]);
+      Y[c * ldy + r] = acc;
+    }
   }
 }
 
@@ -443,14 +607,171 @@ __global__ void k_oz_slice_b(int64_t N, int64_t R, int64_t Kh, int64_t Rpad, con
   }
 }
 
+// the first n moduli and their reciprocals, for the residue kernels
+struct OzMods {
+  int n;
+  double m[OZ_NMOD], minv[OZ_NMOD];
+};
+
+// symmetric residue of the integer-valued a (|a| < 2^52) modulo m, as int8:
+// [-(m-1)/2, (m-1)/2] for odd m, [-128, 127] for m = 256
+__device__ __forceinline__ int oz_res(double a, double m, double minv) {
+  const double q = rint(a * minv);
+  double r = fma(-q, m, a);  // exact: a - q m is an integer of a few bits
+  if (r > 0.5 * m) r -= m;
+  else if (r < -0.5 * m) r += m;
+  const int v = (int)r;
+  return v == 128 ? -128 : v;
+}
+__device__ __forceinline__ int oz_neg8(int v) { return v == -128 ? -128 : -v; }  // -(-128) = 128 = -128 mod 256
+__device__ __forceinline__ uint32_t oz_pack4(int a, int b, int c, int d) {
+  return (uint32_t)(a & 255) | ((uint32_t)(b & 255) << 8) | ((uint32_t)(c & 255) << 16) | ((uint32_t)(d & 255) << 24);
+}
+
+// Z residue planes: plane i occupies rows [i 2Mpad, (i+1) 2Mpad) in the layout
+// of the slices (complex row m -> rows 128 (m/64) + m%64 ([Zr | -Zi]) and that
+// + 64 ([Zi | Zr])), entries A' mod m_i with A' = rint(2^a Z / sigma_m).  One
+// thread per 16 consecutive k (16-byte stores).
+__global__ void __launch_bounds__(128) k_oz_res_a(int64_t N, int64_t Kh, int64_t Mpad, const float2 *__restrict__ Z,
+                                                  const double *__restrict__ rs, double two_a, OzMods md,
+                                                  signed char *__restrict__ A) {
+  const int64_t m = blockIdx.y;
+  const int64_t k0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16;
+  if (k0 >= Kh) return;
+  const double sc = m < N ? two_a / rs[m] : 0.0;  // power of two: exact
+  double ar[16], ai[16];
+#pragma unroll
+  for (int u = 0; u < 16; u++) {
+    const int64_t k = k0 + u;
+    const float2 z = (m < N && k < N) ? Z[m * N + k] : make_float2(0.f, 0.f);
+    ar[u] = rint((double)z.x * sc);
+    ai[u] = rint((double)z.y * sc);
+  }
+  const int64_t ld = 2 * Kh, plane = 2 * Mpad * ld;
+  const int64_t rr = 128 * (m / 64) + m % 64, ri = rr + 64;
+  for (int i = 0; i < md.n; i++) {
+    int pr[16], pi[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      pr[u] = oz_res(ar[u], md.m[i], md.minv[i]);
+      pi[u] = oz_res(ai[u], md.m[i], md.minv[i]);
+    }
+    uint4 vr, vni, vi;
+    vr = make_uint4(oz_pack4(pr[0], pr[1], pr[2], pr[3]), oz_pack4(pr[4], pr[5], pr[6], pr[7]),
+                    oz_pack4(pr[8], pr[9], pr[10], pr[11]), oz_pack4(pr[12], pr[13], pr[14], pr[15]));
+    vi = make_uint4(oz_pack4(pi[0], pi[1], pi[2], pi[3]), oz_pack4(pi[4], pi[5], pi[6], pi[7]),
+                    oz_pack4(pi[8], pi[9], pi[10], pi[11]), oz_pack4(pi[12], pi[13], pi[14], pi[15]));
+    vni = make_uint4(oz_pack4(oz_neg8(pi[0]), oz_neg8(pi[1]), oz_neg8(pi[2]), oz_neg8(pi[3])),
+                     oz_pack4(oz_neg8(pi[4]), oz_neg8(pi[5]), oz_neg8(pi[6]), oz_neg8(pi[7])),
+                     oz_pack4(oz_neg8(pi[8]), oz_neg8(pi[9]), oz_neg8(pi[10]), oz_neg8(pi[11])),
+                     oz_pack4(oz_neg8(pi[12]), oz_neg8(pi[13]), oz_neg8(pi[14]), oz_neg8(pi[15])));
+    signed char *Ap = A + i * plane;
+    *reinterpret_cast<uint4 *>(Ap + rr * ld + k0) = vr;
+    *reinterpret_cast<uint4 *>(Ap + rr * ld + Kh + k0) = vni;
+    *reinterpret_cast<uint4 *>(Ap + ri * ld + k0) = vi;
+    *reinterpret_cast<uint4 *>(Ap + ri * ld + Kh + k0) = vr;
+  }
+}
+
+// X residue planes: plane i occupies rows [i Rpad, (i+1) Rpad); row r =
+// [Xr | Xi] mod m_i with B' = rint(2^b X / tau_r)
+__global__ void __launch_bounds__(128) k_oz_res_b(int64_t N, int64_t R, int64_t Kh, int64_t Rpad,
+                                                  const double2 *__restrict__ X, const double *__restrict__ cs,
+                                                  double two_b, OzMods md, signed char *__restrict__ B) {
+  const int64_t r = blockIdx.y;
+  const int64_t k0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16;
+  if (k0 >= Kh) return;
+  const double sc = r < R ? two_b / cs[r] : 0.0;
+  double br[16], bi[16];
+#pragma unroll
+  for (int u = 0; u < 16; u++) {
+    const int64_t k = k0 + u;
+    const double2 x = (r < R && k < N) ? X[r * N + k] : make_double2(0.0, 0.0);
+    br[u] = rint(x.x * sc);
+    bi[u] = rint(x.y * sc);
+  }
+  const int64_t ld = 2 * Kh, plane = Rpad * ld;
+  for (int i = 0; i < md.n; i++) {
+    int pr[16], pi[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      pr[u] = oz_res(br[u], md.m[i], md.minv[i]);
+      pi[u] = oz_res(bi[u], md.m[i], md.minv[i]);
+    }
+    signed char *Bp = B + i * plane + r * ld;
+    *reinterpret_cast<uint4 *>(Bp + k0) =
+        make_uint4(oz_pack4(pr[0], pr[1], pr[2], pr[3]), oz_pack4(pr[4], pr[5], pr[6], pr[7]),
+                   oz_pack4(pr[8], pr[9], pr[10], pr[11]), oz_pack4(pr[12], pr[13], pr[14], pr[15]));
+    *reinterpret_cast<uint4 *>(Bp + Kh + k0) =
+        make_uint4(oz_pack4(pi[0], pi[1], pi[2], pi[3]), oz_pack4(pi[4], pi[5], pi[6], pi[7]),
+                   oz_pack4(pi[8], pi[9], pi[10], pi[11]), oz_pack4(pi[12], pi[13], pi[14], pi[15]));
+  }
+}
+
+// Host side of the residue scheme: exponents a (Z) and b (X) and the CRT
+// constants of the first nm moduli.  The exact integer product C' needs
+// K 2^(a + b) < M / 2, checked in 128-bit integers.
+struct CrtConst {
+  unsigned __int128 M = 1;
+  double log2M = 0;
+  unsigned long long frac[OZ_NMOD];
+  unsigned fraclo[OZ_NMOD];
+};
+CrtConst crt_const(int nm) {
+  CrtConst k;
+  for (int i = 0; i < nm; i++) {
+    k.M *= (unsigned)OZ_MODULI[i];
+    k.log2M += std::log2((double)OZ_MODULI[i]);
+  }
+  for (int i = 0; i < nm; i++) {
+    const int mi = OZ_MODULI[i];
+    int Mi = 1;  // (M / m_i) mod m_i
+    for (int j = 0; j < nm; j++)
+      if (j != i) Mi = (Mi * (OZ_MODULI[j] % mi)) % mi;
+    int y = 1;
+    while ((Mi * y) % mi != 1) y++;  // m_i <= 256: direct search
+    const unsigned __int128 f = (((unsigned __int128)y << 96) + (unsigned)(mi / 2)) / (unsigned)mi;  // < 2^96
+    k.frac[i] = (unsigned long long)(f >> 32);
+    k.fraclo[i] = (unsigned)(f & 0xffffffffu);
+  }
+  return k;
+}
+bool crt_fits(int64_t K, int e, const CrtConst &k) {  // K 2^e < M / 2
+  return e >= 0 && e <= 100 && ((unsigned __int128)K << (e + 1)) < k.M;  // K < 2^18
+}
+int crt_exp_a(int64_t K) {  // a = b for all moduli
+  const CrtConst k = crt_const(OZ_NMOD);
+  int a = (int)std::floor((k.log2M - 1.0 - std::log2((double)K)) / 2.0);
+  a = std::min(a, 52);
+  while (a > 0 && !crt_fits(K, 2 * a, k)) a--;
+  return a;
+}
+int crt_exp_b(int64_t K, int a, const CrtConst &k) {
+  int b = (int)std::floor(k.log2M - 1.0 - std::log2((double)K)) - a;
+  b = std::min(b, 52);
+  while (b > 0 && !crt_fits(K, a + b, k)) b--;
+  return b;
+}
+OzMods oz_mods(int nm) {
+  OzMods md{};
+  md.n = nm;
+  for (int i = 0; i < OZ_NMOD; i++) {
+    md.m[i] = OZ_MODULI[i];
+    md.minv[i] = 1.0 / OZ_MODULI[i];
+  }
+  return md;
+}
+
 int64_t round_up(int64_t v, int64_t m) { return ((v + m - 1) / m) * m; }
 unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 struct OzState {
-  DevBuf A, B, rs, cs, err, P, fix, runs;
+  DevBuf A, B, rs, cs, err, P, fix, runs, Sh, Sl;
   CUtensorMap mapA, mapB;
   uint64_t a_version = ~0ull;
   int64_t a_n = -1, b_key = -1, b_n = -1;
+  int a_scheme = -1, b_scheme = -1;
+  int crt_a = 0;  // residues: the Z exponent a of the current planes
   bool attr = false;
 };
 
@@ -469,39 +790,51 @@ OzState &oz_state(dmb_ctx *c) {
 
 namespace dmb {
 
-// Is the int8 path usable for this Z (int32 headroom for at least one pair)?
+// Is the int8 path usable for this Z (int32 headroom for one product of
+// int8 operands: |slice| <= 127, |residue| <= 128)?
 bool oz_available(dmb_ctx *c) {
   if (!tc_available(c) || c->z_prec != DMB_PREC_MIXED) return false;
   const int64_t K = 2 * round_up(c->n, OZ_BK);
-  return 16129.0 * (double)K < 2147483647.0;
+  return (c->int8_scheme == 0 ? 16384.0 : 16129.0) * (double)K < 2147483647.0;
 }
 
-// Slices of the current Z (row scales, six int8 slices, tensor map), made
-// once per Z; may run on another stream ahead of the first product, which
-// must then be ordered after it.
+// Operand planes of the current Z (row scales, int8 residues or slices,
+// tensor map), made once per Z; may run on another stream ahead of the first
+// product, which must then be ordered after it.
 void oz_prepare(dmb_ctx *c) {
   DMB_REQUIRE(oz_available(c), DMB_ERR_STATE, "int8 tensor-core product unavailable for this matrix");
   OzState &st = oz_state(c);
   const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64);
   const int64_t ld = 2 * Kh;
+  const bool crt = c->int8_scheme == 0;
+  const int planes = crt ? OZ_NMOD : OZ_S;
   if (!st.err.p) {
     st.err.ensure(16);
     DMB_CUDA(cudaMemsetAsync(st.err.p, 0, 16, c->stream));
   }
   if (!st.attr) {
-    DMB_CUDA(cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_oz_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+    DMB_CUDA(cudaFuncSetAttribute(k_oz_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
     st.attr = true;
   }
-  if (st.a_version != c->z_version || st.a_n != N) {
+  if (st.a_version != c->z_version || st.a_n != N || st.a_scheme != c->int8_scheme) {
     st.rs.ensure(sizeof(double) * Mpad);
-    st.A.ensure((size_t)OZ_S * 2 * Mpad * ld);
+    st.A.ensure((size_t)planes * 2 * Mpad * ld);
     DMB_LAUNCH(c, k_oz_row_scale, (unsigned)N, 256, 0, N, c->d_Z.as<float2>(), st.rs.as<double>());
-    DMB_LAUNCH(c, k_oz_slice_a, dim3(blocks_for(Kh, 256), (unsigned)Mpad), 256, 0, N, Kh, Mpad,
-               c->d_Z.as<float2>(), st.rs.as<double>(), st.A.as<signed char>());
+    if (crt) {
+      st.crt_a = crt_exp_a(ld);
+      DMB_LAUNCH(c, k_oz_res_a, dim3(blocks_for(Kh / 16, 128), (unsigned)Mpad), 128, 0, N, Kh, Mpad,
+                 c->d_Z.as<float2>(), st.rs.as<double>(), std::ldexp(1.0, st.crt_a), oz_mods(OZ_NMOD),
+                 st.A.as<signed char>());
+    } else {
+      DMB_LAUNCH(c, k_oz_slice_a, dim3(blocks_for(Kh, 256), (unsigned)Mpad), 256, 0, N, Kh, Mpad,
+                 c->d_Z.as<float2>(), st.rs.as<double>(), st.A.as<signed char>());
+    }
     make_map_bytes(&st.mapA, st.A.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, (uint64_t)ld, (uint64_t)ld,
-                   (uint64_t)(OZ_S * 2 * Mpad), OZ_BK, OZ_BM);
+                   (uint64_t)(planes * 2 * Mpad), OZ_BK, OZ_BM);
     st.a_version = c->z_version;
     st.a_n = N;
+    st.a_scheme = c->int8_scheme;
   }
 }
 
@@ -511,38 +844,64 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
   OzState &st = oz_state(c);
   const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64), Rpad = round_up(R, OZ_BN);
   const int64_t ld = 2 * Kh;
+  const bool crt = c->int8_scheme == 0;
+  const int planes = crt ? OZ_NMOD : OZ_S;
   st.cs.ensure(sizeof(double) * Rpad);
-  st.B.ensure((size_t)OZ_S * Rpad * ld);
-  if (st.b_key != Rpad || st.b_n != N) {
+  st.B.ensure((size_t)planes * Rpad * ld);
+  if (st.b_key != Rpad || st.b_n != N || st.b_scheme != c->int8_scheme) {
     make_map_bytes(&st.mapB, st.B.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, (uint64_t)ld, (uint64_t)ld,
-                   (uint64_t)(OZ_S * Rpad), OZ_BK, OZ_BN);
+                   (uint64_t)(planes * Rpad), OZ_BK, OZ_BN);
     st.b_key = Rpad;
     st.b_n = N;
+    st.b_scheme = c->int8_scheme;
   }
   DMB_LAUNCH(c, k_oz_col_scale, (unsigned)R, 256, 0, N, X, st.cs.as<double>());
-  DMB_LAUNCH(c, k_oz_slice_b, dim3(blocks_for(Kh, 256), (unsigned)Rpad), 256, 0, N, R, Kh, Rpad, X,
-             st.cs.as<double>(), st.B.as<signed char>());
-  // pair schedule: levels L = p + q <= OZ_LMAX, largest terms first; a level's
-  // pairs share one TMEM sum unless int32 headroom forces an earlier drain
-  const int64_t maxp = (int64_t)(2147483647.0 / (16129.0 * (double)ld));
   OzSched sc{};
   int n = 0;
-  for (int L = 0; L <= lmax; L++) {
-    int in_group = 0;
-    for (int p = 0; p <= L; p++) {
-      const int q = L - p;
-      if (p >= OZ_S || q >= OZ_S) continue;
-      sc.arow[n] = (int)(p * 2 * Mpad);
-      sc.brow[n] = (int)(q * Rpad);
-      sc.close[n] = 0;
-      sc.lscale[n] = std::ldexp(1.0, -OZ_BETA * (L + 2));
-      n++;
-      if (++in_group == maxp) {
-        sc.close[n - 1] = 1;
-        in_group = 0;
-      }
+  if (crt) {
+    // one product per modulus: 13 for the residuals, 12 for the Krylov
+    // operator (the Z planes are shared; X gets the bits the moduli allow)
+    const int nm = lmax >= OZ_LEVELS_RESIDUAL ? OZ_NMOD : OZ_NMOD - 1;
+    const CrtConst k = crt_const(nm);
+    const int b = crt_exp_b(ld, st.crt_a, k);
+    DMB_REQUIRE(b >= 24, DMB_ERR_STATE, "int8 residue product: too few bits left for X");
+    DMB_LAUNCH(c, k_oz_res_b, dim3(blocks_for(Kh / 16, 128), (unsigned)Rpad), 128, 0, N, R, Kh, Rpad, X,
+               st.cs.as<double>(), std::ldexp(1.0, b), oz_mods(nm), st.B.as<signed char>());
+    for (int i = 0; i < nm; i++, n++) {
+      sc.arow[n] = (int)(i * 2 * Mpad);
+      sc.brow[n] = (int)(i * Rpad);
+      sc.close[n] = 1;
+      sc.lscale[n] = 0.0;
+      sc.mod[n] = OZ_MODULI[i];
+      sc.mmul[n] = (unsigned)((((uint64_t)1 << 39) + OZ_MODULI[i] - 1) / OZ_MODULI[i]);
+      sc.moff[n] = (unsigned)(OZ_MODULI[i] * ((1u << 31) / OZ_MODULI[i]));
+      sc.frac[n] = k.frac[i];
+      sc.fraclo[n] = k.fraclo[i];
     }
-    if (in_group > 0) sc.close[n - 1] = 1;
+    sc.cscale = std::ldexp((double)k.M, -64 - st.crt_a - b);
+  } else {
+    DMB_LAUNCH(c, k_oz_slice_b, dim3(blocks_for(Kh, 256), (unsigned)Rpad), 256, 0, N, R, Kh, Rpad, X,
+               st.cs.as<double>(), st.B.as<signed char>());
+    // pair schedule: levels L = p + q <= lmax, largest terms first; a level's
+    // pairs share one TMEM sum unless int32 headroom forces an earlier drain
+    const int64_t maxp = (int64_t)(2147483647.0 / (16129.0 * (double)ld));
+    for (int L = 0; L <= lmax; L++) {
+      int in_group = 0;
+      for (int p = 0; p <= L; p++) {
+        const int q = L - p;
+        if (p >= OZ_S || q >= OZ_S) continue;
+        sc.arow[n] = (int)(p * 2 * Mpad);
+        sc.brow[n] = (int)(q * Rpad);
+        sc.close[n] = 0;
+        sc.lscale[n] = std::ldexp(1.0, -OZ_BETA * (L + 2));
+        n++;
+        if (++in_group == maxp) {
+          sc.close[n - 1] = 1;
+          in_group = 0;
+        }
+      }
+      if (in_group > 0) sc.close[n - 1] = 1;
+    }
   }
   sc.n = n;
   // persistent grid: data-parallel full waves, stream-K tail (k_oz_gemm);
@@ -569,20 +928,39 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
     fix[3 * runs.back() + 1]++;
   }
   if (!fix.empty()) {
-    st.P.ensure(sizeof(double2) * G * 2 * OZ_TILE_ELEMS);
     st.fix.ensure(sizeof(int64_t) * fix.size());
     st.runs.ensure(sizeof(int) * runs.size());
     DMB_CUDA(cudaMemcpyAsync(st.fix.p, fix.data(), sizeof(int64_t) * fix.size(), cudaMemcpyHostToDevice, c->stream));
     DMB_CUDA(cudaMemcpyAsync(st.runs.p, runs.data(), sizeof(int) * runs.size(), cudaMemcpyHostToDevice, c->stream));
   }
+  // residues: fraction sums in three scratch tiles per CTA (two partial-
+  // segment slots and the whole-tile accumulator), high and low words
+  if (crt) {
+    st.Sh.ensure(sizeof(unsigned long long) * G * 3 * OZ_S_ELEMS);
+    st.Sl.ensure(sizeof(unsigned) * G * 3 * OZ_S_ELEMS);
+  }
+  if (!fix.empty() && !crt) st.P.ensure(sizeof(double2) * G * 2 * OZ_TILE_ELEMS);
   kt_begin(c);
-  DMB_LAUNCH(c, k_oz_gemm, (unsigned)G, 192, OZ_SMEM, st.mapA, st.mapB, sc, (int)(ld / OZ_BK), N, R, Y,
-             fix.empty() ? Y : st.P.as<double2>(), N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
-             st.err.as<unsigned>());
-  if (!runs.empty())
-    DMB_LAUNCH(c, k_oz_fixup, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(), ncol, N, R,
-               Y, st.P.as<double2>(), N);
-  // int8 work: every kept slice pair is a real (2N x 2N) x (2N x R) product
+  double2 *Pw = fix.empty() || crt ? Y : st.P.as<double2>();
+  if (crt)
+    DMB_LAUNCH(c, k_oz_gemm<true>, (unsigned)G, oz_threads<true>(), OZ_SMEM, st.mapA, st.mapB, sc,
+               (int)(ld / OZ_BK), N, R, Y, Pw, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
+               st.Sh.as<unsigned long long>(), st.Sl.as<unsigned>(), st.err.as<unsigned>());
+  else
+    DMB_LAUNCH(c, k_oz_gemm<false>, (unsigned)G, oz_threads<false>(), OZ_SMEM, st.mapA, st.mapB, sc,
+               (int)(ld / OZ_BK), N, R, Y, Pw, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
+               (unsigned long long *)nullptr, (unsigned *)nullptr, st.err.as<unsigned>());
+  if (!runs.empty()) {
+    if (crt)
+      DMB_LAUNCH(c, k_oz_fixup<true>, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(), ncol,
+                 N, R, Y, Pw, N, st.rs.as<double>(), st.cs.as<double>(), sc.cscale,
+                 st.Sh.as<unsigned long long>(), st.Sl.as<unsigned>());
+    else
+      DMB_LAUNCH(c, k_oz_fixup<false>, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(),
+                 ncol, N, R, Y, st.P.as<double2>(), N, st.rs.as<double>(), st.cs.as<double>(), sc.cscale,
+                 (const unsigned long long *)nullptr, (const unsigned *)nullptr);
+  }
+  // int8 work: every product is a real (2N x 2N) x (2N x R) product
   kt_end(c, 2.0 * n * (2.0 * N) * (2.0 * N) * (double)R, 1);
 }
 
@@ -600,7 +978,7 @@ void oz_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_oz_states.size(); i++) {
     if (g_oz_states[i].first != c) continue;
     OzState *st = g_oz_states[i].second;
-    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err, &st->P, &st->fix, &st->runs}) b->release();
+    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err, &st->P, &st->fix, &st->runs, &st->Sh, &st->Sl}) b->release();
     delete st;
     g_oz_states.erase(g_oz_states.begin() + i);
     return;

@@ -1025,7 +1025,9 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
                N, st.Pb.as<float>());
   // tile width from the autotuner, per (row tiles, columns, triangular
   // kind): 256 or 128 complex columns (128 doubles the CTAs of launches with
-  // few row tiles); both give the same bits
+  // few row tiles); both give the same bits.  (A persistent, double-buffered
+  // form of this kernel was measured slower on every sweep shape: these
+  // launches are one or two waves, so there is no next tile to overlap.)
   const int64_t tb1 = dmb::tune_bucket(Mpad / 64), tb2 = (Rpad / 128) * 4 + tri;
   const int cand = dmb::tune_choose(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, 2);
   const bool narrow = cand == 1;

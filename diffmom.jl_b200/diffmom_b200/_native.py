@@ -53,6 +53,7 @@ OPT_SPIN_LIMIT = 9
 OPT_TUNE_TC_GEMM = 10
 OPT_TUNE_TC_SYRK = 11
 OPT_PRECOND_BF16 = 12
+OPT_INT8_SCHEME = 13
 
 
 class DiffMoMError(RuntimeError):

@@ -165,6 +165,16 @@ const char *dmb_version(void);
  * residual, so the preconditioner's precision changes the iteration count,
  * not the result; dmb_nf_build / dmb_nf_apply / dmb_gmres keep TF32 pieces. */
 #define DMB_OPT_PRECOND_BF16 12
+/* DMB_OPT_INT8_SCHEME: how the FP64-accurate complex64 Z X (refinement and
+ * true residuals, the exact Krylov operator) is made of exact int8
+ * tensor-core products.  0 (default): residues modulo 13 pairwise coprime
+ * moduli <= 256 of Z and X scaled to 44-bit integers, one int8 product per
+ * modulus, recombined by the Chinese remainder theorem as a 64-bit fixed-point
+ * fraction of the moduli's product (13 products, 12 for the Krylov operator).
+ * 1: seven-bit fixed-point slices, products of slice pairs up to a level
+ * (26 products, 21 for the Krylov operator).  Both are deterministic and
+ * agree with the FP64 product to ~1e-12 normwise. */
+#define DMB_OPT_INT8_SCHEME 13
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair RWG tile width used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *width_out);
