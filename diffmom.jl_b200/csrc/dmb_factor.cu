@@ -222,17 +222,28 @@ __device__ __forceinline__ void ldlt_diag_block(int64_t N, int64_t j, int b, C *
     }
 }
 
+// 1 / x for a positive normal float: the hardware approximation refined by
+// one Newton-Raphson step, r <- r (2 - x r)
+__device__ __forceinline__ float rcp_nr(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r * fmaf(-x, r, 2.f);
+}
+__device__ __forceinline__ float2 csel(bool p, float2 a, float2 b) { return make_float2(p ? a.x : b.x, p ? a.y : b.y); }
+
 // Elimination of the 16 x 16 diagonal sub-block at s0 by one warp, all in
 // registers: lane (ih = lane >> 4, c = lane & 15) holds rows i = ih + 2 m
 // (m = 0..7) of column c.  The block is kept in full (both triangles: it is
 // complex symmetric and every update keeps it so), which puts each value a
 // pivot step needs -- the pivot, A[k][c] = A[c][k], X[k][c] and A[i][k] -- in
 // a register whose index is known at compile time on a lane known per lane,
-// so one shuffle fetches it; no shared memory, no warp barriers.  On return
-// the lower triangle holds L (strict) and D, X the unit-lower inverse.
-// 1/d = conj(d) / |d|^2 with one reciprocal on the serial path; a pivot whose
-// |d|^2 is zero, non-finite or outside the FP32 range (|d| below ~1e-19 or
-// above ~1e19) is a breakdown (false, uniform over the warp).
+// so one shuffle fetches it; no shared memory, no warp barriers.  The updates
+// are selects, not branches (the lane conditions differ within the warp).  On
+// return the lower triangle holds L (strict) and D, X the unit-lower inverse.
+// 1/d = conj(d) / |d|^2 with |d|^2 inverted by rcp_nr; a pivot whose |d|^2 is
+// zero, non-finite or outside the FP32 normal range (|d| below ~1e-19 or above
+// ~1e19) is a breakdown (false, uniform over the warp, decided after the 16
+// steps).
 __device__ __forceinline__ bool elim16_warp(float2 (*A)[65], float2 (*Xs)[17], int s0, int lane) {
   const unsigned FULL = 0xffffffffu;
   const int c = lane & 15, ih = lane >> 4;
@@ -243,36 +254,38 @@ __device__ __forceinline__ bool elim16_warp(float2 (*A)[65], float2 (*Xs)[17], i
     a[m] = (c <= i) ? A[s0 + i][s0 + c] : A[s0 + c][s0 + i];
     x[m] = (i == c) ? make_float2(1.f, 0.f) : make_float2(0.f, 0.f);
   }
+  bool ok = true;
 #pragma unroll
   for (int k = 0; k < 16; k++) {
-    const int kl = (k & 1) << 4, km = k >> 1;  // row k lives on lanes kl | col, register km
-    float2 d;
+    const int kl = (k & 1) << 4, km = k >> 1;
+    float2 d, akc, xk, aik[8];
     d.x = __shfl_sync(FULL, a[km].x, kl | k);
     d.y = __shfl_sync(FULL, a[km].y, kl | k);
-    const float d2 = d.x * d.x + d.y * d.y;
-    if (!(d2 > 0.f) || !isfinite(d2)) return false;
-    const float rd = __frcp_rn(d2);
-    const float2 inv_d = make_float2(d.x * rd, -d.y * rd);
-    float2 akc, xk;
     akc.x = __shfl_sync(FULL, a[km].x, kl | c);
     akc.y = __shfl_sync(FULL, a[km].y, kl | c);
-    xk.x = __shfl_sync(FULL, x[km].x, kl | c);  // X[k][c], final at step k
+    xk.x = __shfl_sync(FULL, x[km].x, kl | c);
     xk.y = __shfl_sync(FULL, x[km].y, kl | c);
-    const float2 lc = cmul(akc, inv_d);  // L[c][k] (c > k)
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      aik[m].x = __shfl_sync(FULL, a[m].x, (ih << 4) | k);
+      aik[m].y = __shfl_sync(FULL, a[m].y, (ih << 4) | k);
+    }
+    const float d2 = fmaf(d.x, d.x, d.y * d.y);
+    ok = ok && (d2 >= 1.17549435e-38f) && (d2 <= 3.40282347e38f);
+    const float rd = rcp_nr(d2);
+    const float2 inv_d = make_float2(d.x * rd, -d.y * rd);
+    const float2 lc = cmul(akc, inv_d);
 #pragma unroll
     for (int m = 0; m < 8; m++) {
       const int i = ih + 2 * m;
-      float2 aik;  // A[i][k]: lane (ih << 4) | k, register m
-      aik.x = __shfl_sync(FULL, a[m].x, (ih << 4) | k);
-      aik.y = __shfl_sync(FULL, a[m].y, (ih << 4) | k);
-      if (i > k) {
-        const float2 lik = cmul(aik, inv_d);
-        if (c > k) a[m] = csub(a[m], cmul(aik, lc));
-        else if (c == k) a[m] = lik;  // L[i][k]
-        x[m] = csub(x[m], cmul(lik, xk));
-      }
+      const bool below = i > k;
+      const float2 lik = cmul(aik[m], inv_d);
+      const float2 upd = csub(a[m], cmul(aik[m], lc));
+      a[m] = csel(below && c > k, upd, csel(below && c == k, lik, a[m]));
+      x[m] = csel(below, csub(x[m], cmul(lik, xk)), x[m]);
     }
   }
+  if (!__all_sync(FULL, ok)) return false;
 #pragma unroll
   for (int m = 0; m < 8; m++) {
     const int i = ih + 2 * m;
@@ -282,14 +295,17 @@ __device__ __forceinline__ bool elim16_warp(float2 (*A)[65], float2 (*Xs)[17], i
   return true;
 }
 
+
 // Blocked form of ldlt_diag_block for complex64 blocks (same results up to
 // rounding): four 16-wide sub-panels; warp 0 eliminates the 16 x 16 diagonal
 // sub-block in registers (elim16_warp, which also forms its unit-lower
-// inverse), then the CTA computes the sub-panel below it and the trailing
-// update.  The 64 x 64 inverse is assembled from the four 16 x 16 inverses by
-// block forward substitution.  About 20 CTA barriers instead of 128.
+// inverse), then the CTA computes the sub-panel below it (up to three rows
+// per thread, accumulated together) and the trailing update (four columns per
+// thread).  The 64 x 64 inverse is assembled from the four 16 x 16 inverses
+// by recursive doubling (16-wide pairs, then the 32-wide halves), each phase
+// a small product with several independent sums per thread.
 // Rows and columns at or beyond b are padded with the identity (D = 1, L = 0).
-constexpr size_t DIAG_BLOCKED_SMEM = sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17) + 16;
+constexpr size_t DIAG_BLOCKED_SMEM = sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17 + 16) + 16;
 
 __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restrict__ F, float2 *__restrict__ Linv,
                                   unsigned *__restrict__ err, unsigned char *smem) {
@@ -297,11 +313,10 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
   float2(*Wp)[17] = reinterpret_cast<float2(*)[17]>(smem + sizeof(float2) * 64 * 65);
   float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem + sizeof(float2) * (64 * 65 + 64 * 17));
   float2(*LI)[65] = reinterpret_cast<float2(*)[65]>(smem + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
-  volatile int *bad =
-      reinterpret_cast<volatile int *>(smem + sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17));
+  float2 *dinv = reinterpret_cast<float2 *>(smem + sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17));
+  volatile int *bad = reinterpret_cast<volatile int *>(dinv + 16);
   const int t = threadIdx.x;  // 256 threads
   {
-    // all 16 loads of a thread in flight before the shared stores
     float2 v[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
@@ -332,65 +347,146 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
       }
     }
     __syncthreads();
-    if (*bad) return;  // uniform
+      if (*bad) return;
     if (s == 3) break;
-    // sub-panel below: W = A21 X^T, L21 = W D^-1 (rows s0 + 16 .. 63)
     const int nr = 48 - s0;
-    for (int e = t; e < nr * 16; e += blockDim.x) {
-      const int r = s0 + 16 + (e >> 4), c = e & 15;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int k = 0; k <= c; k++) cfma(acc, A[r][s0 + k], Xd[s][c][k]);
-      Wp[r][c] = acc;
+    // 1 / D of the 16 pivots; sub-panel W = A21 X^T with up to three outputs
+    // per thread accumulated together
+    if (t < 16) {
+      const float2 dd = A[s0 + t][s0 + t];
+      const float rd = rcp_nr(fmaf(dd.x, dd.x, dd.y * dd.y));
+      dinv[t] = make_float2(dd.x * rd, -dd.y * rd);
     }
-    __syncthreads();
-    for (int e = t; e < nr * 16; e += blockDim.x) {
-      const int r = s0 + 16 + (e >> 4), c = e & 15;
-      A[r][s0 + c] = cdiv(Wp[r][c], A[s0 + c][s0 + c]);
-    }
-    __syncthreads();
-    // trailing update A22 -= W L21^T on the lower part
-    for (int e = t; e < nr * nr; e += blockDim.x) {
-      const int i = s0 + 16 + e / nr, jj = s0 + 16 + e % nr;
-      if (jj > i) continue;
-      float2 acc = make_float2(0.f, 0.f);
+    {
+      float2 acc[3];
+      int rr[3];
+      const int c = t & 15;
 #pragma unroll
-      for (int k = 0; k < 16; k++) cfma(acc, Wp[i][k], A[jj][s0 + k]);
-      A[i][jj] = csub(A[i][jj], acc);
+      for (int u = 0; u < 3; u++) {
+        acc[u] = make_float2(0.f, 0.f);
+        rr[u] = s0 + 16 + (t >> 4) + 16 * u;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        if (k <= c) {
+          const float2 xk = Xd[s][c][k];
+#pragma unroll
+          for (int u = 0; u < 3; u++)
+            if (rr[u] < 64) cfma(acc[u], A[rr[u]][s0 + k], xk);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 3; u++)
+        if (rr[u] < 64) Wp[rr[u]][c] = acc[u];
     }
     __syncthreads();
-  }
-  // L (strict lower) and D back to F
+    for (int e = t; e < nr * 16; e += blockDim.x) {
+      const int r = s0 + 16 + (e >> 4), c = e & 15;
+      A[r][s0 + c] = cmul(Wp[r][c], dinv[c]);
+    }
+    __syncthreads();
+    // trailing update A22 -= W L21^T on the lower part: thread -> (row, 4 columns)
+    {
+      const int ncq = (nr + 3) / 4;  // column quads
+      for (int e = t; e < nr * ncq; e += blockDim.x) {
+        const int i = s0 + 16 + e / ncq, j0 = s0 + 16 + 4 * (e % ncq);
+        if (j0 > i) continue;
+        float2 acc[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+          const float2 w = Wp[i][k];
+#pragma unroll
+          for (int q = 0; q < 4; q++) cfma(acc[q], w, A[min(j0 + q, 63)][s0 + k]);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (j0 + q <= i) A[i][j0 + q] = csub(A[i][j0 + q], acc[q]);
+      }
+    }
+    __syncthreads();
+    }
   for (int e = t; e < 64 * 64; e += blockDim.x) {
     const int i = e >> 6, c = e & 63;
     if (i < b && c <= i) F[(j + i) * N + j + c] = A[i][c];
   }
-  // Linv (LI in shared memory): diagonal 16-blocks from Xd, zero above, then
-  // block rows I = 1..3: LI[I][J] = -X_I sum_{K=J..I-1} L[I][K] LI[K][J]
+  // Linv by recursive doubling: 16-level pairs, then the 32-level block
+  //   [[X0, 0], [-X1 L10 X0, X1]]
   for (int e = t; e < 64 * 64; e += blockDim.x) {
     const int i = e >> 6, c = e & 63;
     LI[i][c] = ((i >> 4) == (c >> 4)) ? Xd[i >> 4][i & 15][c & 15] : make_float2(0.f, 0.f);
   }
-  __syncthreads();
-  for (int I = 1; I < 4; I++) {
-    // Wp rows 16 J + r hold T_J = sum_K L[I][K] LI[K][J] for J < I
-    for (int e = t; e < I * 256; e += blockDim.x) {
-      const int J = e >> 8, r = (e >> 4) & 15, c = e & 15;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int k = 16 * J; k < 16 * I; k++) cfma(acc, A[16 * I + r][k], LI[k][16 * J + c]);
-      Wp[16 * J + r][c] = acc;
+  // phase A: T_h = L[32h+16.., 32h..] Xd[2h] (two 16 x 16 products, 2 outputs per thread)
+  {
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int e = t + 256 * u, h = e >> 8, r = (e >> 4) & 15, c = e & 15;
+      float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 16; k += 2) {
+        cfma(p0, A[32 * h + 16 + r][32 * h + k], Xd[2 * h][k][c]);
+        cfma(p1, A[32 * h + 16 + r][32 * h + k + 1], Xd[2 * h][k + 1][c]);
+      }
+      Wp[32 * h + r][c] = cadd(p0, p1);
     }
-    __syncthreads();
-    for (int e = t; e < I * 256; e += blockDim.x) {
-      const int J = e >> 8, r = (e >> 4) & 15, c = e & 15;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int k = 0; k <= r; k++) cfma(acc, Xd[I][r][k], Wp[16 * J + k][c]);
-      LI[16 * I + r][16 * J + c] = make_float2(-acc.x, -acc.y);
-    }
-    __syncthreads();
   }
+  __syncthreads();
+  // phase B: LI[32h+16+r][32h+c] = -Xd[2h+1] T_h
+  {
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int e = t + 256 * u, h = e >> 8, r = (e >> 4) & 15, c = e & 15;
+      float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 16; k += 2) {
+        if (k <= r) cfma(p0, Xd[2 * h + 1][r][k], Wp[32 * h + k][c]);
+        if (k + 1 <= r) cfma(p1, Xd[2 * h + 1][r][k + 1], Wp[32 * h + k + 1][c]);
+      }
+      const float2 acc = cadd(p0, p1);
+      LI[32 * h + 16 + r][32 * h + c] = make_float2(-acc.x, -acc.y);
+    }
+  }
+  __syncthreads();
+  // phase C: U = L[32.., 0..32) X_a (32 x 32, X_a lower: k >= c), 4 outputs
+  // per thread; U goes to Wp as two 32 x 16 halves (Wp[r][c] for c < 16,
+  // Wp[32 + r][c - 16] for c >= 16)
+  {
+    const int c = t & 31, r0 = t >> 5;  // rows r0, r0 + 8, r0 + 16, r0 + 24
+    float2 p[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      if (k >= c) {
+        const float2 x = LI[k][c];
+#pragma unroll
+        for (int q = 0; q < 4; q++) cfma(p[q], A[32 + r0 + 8 * q][k], x);
+      }
+    }
+    __syncthreads();  // Wp of phase B is consumed
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = r0 + 8 * q;
+      if (c < 16) Wp[r][c] = p[q];
+      else Wp[32 + r][c - 16] = p[q];
+    }
+  }
+  __syncthreads();
+  // phase D: LI[32 + r][c] = -X_b U, X_b = LI[32.., 32..] lower (k <= r)
+  {
+    const int c = t & 31, r0 = t >> 5;
+    float2 p[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+      const float2 u = c < 16 ? Wp[k][c] : Wp[32 + k][c - 16];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (k <= r0 + 8 * q) cfma(p[q], LI[32 + r0 + 8 * q][32 + k], u);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) LI[32 + r0 + 8 * q][c] = make_float2(-p[q].x, -p[q].y);
+  }
+  __syncthreads();
   for (int e = t; e < 64 * 64; e += blockDim.x) Linv[e] = LI[e >> 6][e & 63];
+  __syncthreads();
 }
-
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
                                                    C *__restrict__ Linv, unsigned *__restrict__ err) {

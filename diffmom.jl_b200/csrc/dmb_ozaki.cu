@@ -116,6 +116,31 @@ __device__ __forceinline__ unsigned oz_mod(int v, unsigned m, unsigned mmul, uns
   return (unsigned)(r < 0 ? r + (int)m : r);
 }
 
+// Global accesses to the fraction-sum scratch marked evict-last in L2: the
+// CTAs' running sums (a few tens of MB) are re-read once per modulus, while
+// the int8 operand planes stream through L2 once per product.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long ld_keep(const unsigned long long *a, uint64_t pol) {
+  unsigned long long v;
+  asm volatile("ld.global.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ unsigned ld_keep(const unsigned *a, uint64_t pol) {
+  unsigned v;
+  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_keep(unsigned long long *a, unsigned long long v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(a), "l"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep(unsigned *a, unsigned v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol) : "memory");
+}
+
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -312,6 +337,7 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
     // accumulator-empty barrier by itself (count 8).
     const int row = (warp & 3) * 32 + lane;
     const int chalf = warp >> 2;
+    const uint64_t keep = l2_evict_last_policy();
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     int g = 0;
     bool alive = true;
@@ -347,8 +373,8 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
           unsigned ol[16];
 #pragma unroll
           for (int q = 0; q < 16; q++) {
-            oh[q] = first ? 0ull : Sht[(int64_t)(cc * 16 + q) * 128];
-            ol[q] = first ? 0u : Slt[(int64_t)(cc * 16 + q) * 128];
+            oh[q] = first ? 0ull : ld_keep(Sht + (int64_t)(cc * 16 + q) * 128, keep);
+            ol[q] = first ? 0u : ld_keep(Slt + (int64_t)(cc * 16 + q) * 128, keep);
           }
           uint32_t v[16];
           asm volatile(
@@ -369,8 +395,8 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
                 reinterpret_cast<double *>(Y)[2 * ((col0 + c) * ldy + gr) + (row >> 6)] =
                     fma((double)(unsigned)tl, 0x1p-32, (double)(long long)th) * rsc * cs[col0 + c];
             } else {
-              Sht[(int64_t)c * 128] = th;
-              Slt[(int64_t)c * 128] = (unsigned)tl;
+              st_keep(Sht + (int64_t)c * 128, th, keep);
+              st_keep(Slt + (int64_t)c * 128, (unsigned)tl, keep);
             }
           }
         }
