@@ -11,12 +11,13 @@ the 1,024 right-hand sides, GMRES to 1e-6 relative FP64 residual for all of
 them, monostatic sigma on the device.  ``value`` = incidences solved per
 second (mixed: complex64 Z with FP32 far pairs and FP64 singular terms,
 block GMRES preconditioned by the complex64 LDL^T of Z -- tensor-core updates
-and sweeps on BF16 hi + lo operand pieces -- with FP64-accurate INT8-slice
-Krylov products, FP64 Arnoldi and the FP64 residual as the judge).
+and sweeps on BF16 hi + lo operand pieces -- with FP64-accurate Krylov
+products from int8 residues modulo 13 moduli (Chinese-remainder
+recombination), FP64 Arnoldi and the FP64 residual as the judge).
 
 Variants reported beside it (same timing rules, fewer steps where slow):
   c3_mixed_tf32_refined  the headline with the Krylov product in 3xTF32 and
-                  FP64-residual refinement instead of INT8 slices
+                  FP64-residual refinement instead of the INT8 product
   c3_mixed_precond_tf32x3 / _tf32x1  the headline with the preconditioner's
                   tensor-core operands as TF32 pieces (3 or 1 products)
   c3_fp64_plain   the same job in plain FP64 (FP64 Z, the reference's
@@ -68,9 +69,9 @@ K = 2 * math.pi * FREQ / C0
 R_WAVES = 1024
 SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
-# DRAM bytes per k_oz_gemm launch (26 slice products, R = 1,024) on the
+# DRAM bytes per k_oz_gemm launch (13 residue products, R = 1,024) on the
 # headline plate, measured with ncu one-pass dram__bytes_read/write.sum
-OZ_TRAFFIC_PER_LAUNCH = 20227765760  # a 26-product launch (the headline's Krylov products): 18.987 + 1.240 GB
+OZ_TRAFFIC_PER_LAUNCH = 16105352192  # mean of the step's two launches: 12.919 + 3.186 GB
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
@@ -630,7 +631,7 @@ def make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks=None):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "c64 Z (fp32 far pairs, fp64 singular terms), BF16x3 (hi+lo) tensor-core factor updates/sweeps, int8-slice FP64-accurate Z X, fp64 Arnoldi",
+        "dtype": "c64 Z (fp32 far pairs, fp64 singular terms), BF16x3 (hi+lo) tensor-core factor updates/sweeps, int8-residue (CRT) FP64-accurate Z X, fp64 Arnoldi",
         "data": "synthetic plate mesh and seeded incidences (seed 20260001)",
         "config": config_dict(N, mesh.ntriangles, ws),
         "variants": {k: clean(v) for k, v in variants.items()},
@@ -652,8 +653,8 @@ def make_line(args, ws, N, mesh, head, variants, e2e, fp64_peaks=None):
                 "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                 "frac": achieved / bf16 if bf16 else None,
                 "traffic": OZ_TRAFFIC_PER_LAUNCH if PLATE_CELLS == 60 and R_WAVES == 1024 else None,
-                "traffic_note": "DRAM bytes per launch (ncu one-pass dram__bytes metrics of a 26-product "
-                                "launch on the headline plate)",
+                "traffic_note": "DRAM bytes per launch (ncu one-pass dram__bytes metrics of the step's two "
+                                "13-product launches on the headline plate)",
                 "peak_source": f"{src} dense bf16 (MEASURED_PEAKS.json); algorithmic flops 8 N^2 R per launch "
                                "(complex MAC = 8 real flops, counted once however the product is executed)",
                 "launches_timed": il, "kernel_ms_total": ims,
@@ -857,7 +858,7 @@ def config_dict(N, ntri, ws):
     return {"workload": WORKLOAD, "N_rwg": N, "N_tri": ntri, "incidences": R_WAVES,
             "quad_order": 3, "gmres_tol": 1e-6,
             "precond": "complex64 LDL^T of Z (near-field cutoff = inf), right (flexible form)",
-            "krylov_product": "FP64-accurate INT8-slice Z X on tcgen05 (kind::i8)",
+            "krylov_product": "FP64-accurate Z X from int8 residues modulo 13 moduli on tcgen05 (kind::i8), CRT recombination",
             "variant": "c3_mixed_batched", "parallelism": f"incidence shards x{ws} (1,024 per GPU, no data-path collective)",
             "l2": "inputs larger than L2 (Z 912 MB complex64; packed factor 2 x 2.8 GB)"}
 
