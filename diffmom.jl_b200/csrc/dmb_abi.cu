@@ -175,7 +175,7 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       return;
     }
     if (option == DMB_OPT_TUNE_TC_GEMM || option == DMB_OPT_TUNE_TC_SYRK) {
-      const int ncand = option == DMB_OPT_TUNE_TC_GEMM ? 2 : 3;
+      const int ncand = 3;
       DMB_REQUIRE(value >= 0 && value <= ncand, DMB_ERR_ARGUMENT,
                   "autotuner pin must be 0 (tuned) or a candidate 1.." + std::to_string(ncand));
       c->tune_pin[option == DMB_OPT_TUNE_TC_GEMM ? dmb::TUNE_TC_GEMM_BN : dmb::TUNE_TC_SYRK_STAGES] = value;

@@ -616,6 +616,190 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(BN) : "memory");
 }
 
+// Persistent form of k_tc_gemm (autotuner candidate): a grid of at most one
+// CTA per SM walks the tiles (column tile fastest), 6 warps as in k_tc_syrk_p
+// (producer, MMA issuer, 4 drain warps) with two TMEM accumulators, so a
+// tile's epilogue (the read-modify-write of complex128 Y) overlaps the next
+// tile's main loop.  Same MMA sequence per tile as k_tc_gemm: the same bits.
+template <int BN, bool BF>
+__global__ void __launch_bounds__(192, 1) k_tc_gemm_p(const __grid_constant__ CUtensorMap tmA,
+                                                      const __grid_constant__ CUtensorMap tmB, int a_row0, int a_kx0,
+                                                      int nchunks, int cpb, int64_t M, int64_t Rv,
+                                                      double2 *__restrict__ Y, int64_t ldy, int mode, int tri,
+                                                      int ntc, int64_t ntiles, unsigned *err) {
+  constexpr int B_STAGE = BN * TC_BK * 4;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char *gbase = smem_raw + (base - raw);
+  const uint32_t sA = base;
+  const uint32_t sB = base + TCP_STAGES * TC_A_STAGE;
+  float *E = reinterpret_cast<float *>(gbase + TCP_STAGES * (TC_A_STAGE + B_STAGE));
+  const uint32_t sBar = sB + TCP_STAGES * B_STAGE + TCP_E_BYTES;
+  uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
+  volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 16);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 17);
+  volatile int *epi_ok = reinterpret_cast<volatile int *>(bar_ptr + 18);
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * TCP_STAGES, accf0 = sBar + 16 * TCP_STAGES, acce0 = accf0 + 16;
+  // K chunk range of a row tile (triangular A: only the 256-wide K blocks
+  // that meet the tile's rows)
+  auto krange = [&](int64_t row0, int &kc0, int &kc1) {
+    kc0 = 0;
+    kc1 = nchunks;
+    if (tri == 1) kc1 = min(nchunks, cpb * (int)((row0 + 64 + 255) / 256));
+    else if (tri == 2) kc0 = cpb * (int)(row0 / 256);
+  };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TCP_STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, 1);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(const_cast<uint32_t *>(tmem_slot))),
+                 "r"(2 * BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = *tmem_slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      long long t = 0;
+      bool go = true;
+      for (int64_t tile = blockIdx.x; tile < ntiles && go; tile += gridDim.x) {
+        const int64_t row0 = (tile / ntc) * 64, col0 = (tile % ntc) * BN;
+        int kc0, kc1;
+        krange(row0, kc0, kc1);
+        for (int kc = kc0; kc < kc1; kc++, t++) {
+          const int s = (int)(t % TCP_STAGES);
+          if (*abort_flag || (t >= TCP_STAGES &&
+                              !mbar_wait(empty0 + 8 * s, (uint32_t)((t / TCP_STAGES) - 1) & 1u, err, abort_flag))) {
+            go = false;
+            break;
+          }
+          mbar_expect_tx(full0 + 8 * s, TC_A_STAGE + B_STAGE);
+          const int kx = tc_kx<BF>(kc, cpb);
+          tma_load_2d(sA + s * TC_A_STAGE, &tmA, a_kx0 + kx, a_row0 + (int)(2 * row0), full0 + 8 * s);
+          tma_load_2d(sB + s * B_STAGE, &tmB, kx, (int)col0, full0 + 8 * s);
+        }
+      }
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      long long t = 0;
+      int i = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, i++) {
+        const int64_t row0 = (tile / ntc) * 64;
+        int kc0, kc1;
+        krange(row0, kc0, kc1);
+        const int buf = i & 1;
+        if (i >= 2 && !mbar_wait(acce0 + 8 * buf, (uint32_t)((i >> 1) - 1) & 1u, err, abort_flag)) {
+          ok = false;
+          break;
+        }
+        const uint32_t tmem_acc = tmem_d + (uint32_t)(buf * BN);
+        for (int kc = kc0; kc < kc1; kc++, t++) {
+          const int s = (int)(t % TCP_STAGES);
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / TCP_STAGES) & 1u, err, abort_flag)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+          for (int k = 0; k < TC_BK / 8; k++) {
+            const uint64_t ad = sw128_desc(sA + s * TC_A_STAGE + k * 32);
+            const uint64_t bd = sw128_desc(sB + s * B_STAGE + k * 32);
+            umma_op<BN, BF>(tmem_acc, ad, bd, (kc > kc0 || k > 0) ? 1u : 0u);
+          }
+          umma_commit(empty0 + 8 * s);
+        }
+        if (ok) umma_commit(accf0 + 8 * buf);
+      }
+    }
+  } else {
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int rl = threadIdx.x & 63, qh = threadIdx.x >> 6;
+    int i = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+      const int buf = i & 1;
+      const int64_t row0 = (tile / ntc) * 64, col0 = (tile % ntc) * BN;
+      const bool got = mbar_wait(accf0 + 8 * buf, (uint32_t)(i >> 1) & 1u, err, abort_flag);
+      if (threadIdx.x == 0) *epi_ok = 1;
+      tcp_epi_sync();
+      if (!got) *epi_ok = 0;
+      tcp_epi_sync();
+      if (!*epi_ok) break;  // uniform over the drain warps
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tmem_acc = tmem_d + (uint32_t)(buf * BN);
+      const int64_t gr = row0 + rl;
+      for (int cc = 0; cc < BN / 32; cc++) {
+        if (col0 + cc * 32 >= Rv) break;  // uniform
+        uint32_t v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(tmem_acc + lane_base + (uint32_t)(cc * 32)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int row = warp * 32 + lane;
+#pragma unroll
+        for (int q = 0; q < 32; q++) E[row * 33 + q] = __uint_as_float(v[q]);
+        tcp_epi_sync();
+        if (gr < M) {
+          const int64_t gc0 = col0 + cc * 32 + qh;
+          if (mode == 0) {
+#pragma unroll
+            for (int r16 = 0; r16 < 16; r16++) {
+              const int q = qh + 2 * r16;
+              if (gc0 + 2 * r16 < Rv)
+                Y[(gc0 + 2 * r16) * ldy + gr] = make_double2(E[rl * 33 + q], E[(64 + rl) * 33 + q]);
+            }
+          } else {
+            double2 cv[16];
+#pragma unroll
+            for (int r16 = 0; r16 < 16; r16++)
+              cv[r16] = (gc0 + 2 * r16 < Rv) ? __ldcs(Y + (gc0 + 2 * r16) * ldy + gr) : make_double2(0, 0);
+#pragma unroll
+            for (int r16 = 0; r16 < 16; r16++) {
+              const int q = qh + 2 * r16;
+              if (gc0 + 2 * r16 < Rv)
+                __stcs(Y + (gc0 + 2 * r16) * ldy + gr,
+                       make_double2(cv[r16].x - E[rl * 33 + q], cv[r16].y - E[(64 + rl) * 33 + q]));
+            }
+          }
+        }
+        tcp_epi_sync();
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      tcp_epi_sync();
+      if (threadIdx.x == 0) tcp_arrive(acce0 + 8 * buf);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * BN) : "memory");
+}
+
+template <int BN> constexpr int tcgp_smem() { return TCP_STAGES * (TC_A_STAGE + BN * TC_BK * 4) + TCP_E_BYTES + 256 + 1024; }
+
 // split one complex value into the six 256-strided A'' / B'' segment entries
 template <class E>
 __device__ __forceinline__ void put_a(E *ar, E *ai, int kk, float vr, float vi) {
@@ -749,6 +933,10 @@ void ensure_gemm(dmb_ctx *c, TcState &st) {
     DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
     DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm<1, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_128));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm_p<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tcgp_smem<256>()));
+    DMB_CUDA(cudaFuncSetAttribute(k_tc_gemm_p<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tcgp_smem<256>()));
     st.gemm_attr = true;
   }
 }
@@ -1023,29 +1211,42 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   else
     DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk,
                N, st.Pb.as<float>());
-  // tile width from the autotuner, per (row tiles, columns, triangular
-  // kind): 256 or 128 complex columns (128 doubles the CTAs of launches with
-  // few row tiles); both give the same bits.  (A persistent, double-buffered
-  // form of this kernel was measured slower on every sweep shape: these
-  // launches are one or two waves, so there is no next tile to overlap.)
+  // launch shape from the autotuner, per (row tiles, columns, triangular
+  // kind): one CTA per 64 x 256 or 64 x 128 complex tile (128 doubles the
+  // CTAs of launches with few row tiles), or the persistent 256-wide form (one
+  // CTA per SM, a tile's epilogue overlapping the next tile's main loop; it
+  // pays only with several tiles per CTA); all three give the same bits
   const int64_t tb1 = dmb::tune_bucket(Mpad / 64), tb2 = (Rpad / 128) * 4 + tri;
-  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, 2);
-  const bool narrow = cand == 1;
+  const int cand = dmb::tune_choose(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, 3);
   const int cpb = (bf ? 8 : 16) * c->precond_tf32_terms;
+  const int nchunks = (int)(Kpad / 256) * cpb;
   dmb::TuneMark mk;
   dmb::tune_begin(c, dmb::TUNE_TC_GEMM_BN, tb1, tb2, cand, mk);
   kt_begin(c);
+  if (cand < 2) {
 #define GEMM_LAUNCH(BNV, BFV, MAPB, SMEMV)                                                                       \
   DMB_LAUNCH(c, (k_tc_gemm<1, BNV, BFV>), dim3((unsigned)(Rpad / BNV), (unsigned)(Mpad / 64)), 128, SMEMV, mapA, \
-             MAPB[kslot], a_row0, a_kx0, (int)(Kpad / 256) * cpb, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>())
-  if (narrow) {
-    if (bf) GEMM_LAUNCH(128, true, st.mapPbK128, TC_SMEM_128);
-    else GEMM_LAUNCH(128, false, st.mapPbK128, TC_SMEM_128);
-  } else {
-    if (bf) GEMM_LAUNCH(256, true, st.mapPbK, TC_SMEM);
-    else GEMM_LAUNCH(256, false, st.mapPbK, TC_SMEM);
-  }
+             MAPB[kslot], a_row0, a_kx0, nchunks, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>())
+    if (cand == 1) {
+      if (bf) GEMM_LAUNCH(128, true, st.mapPbK128, TC_SMEM_128);
+      else GEMM_LAUNCH(128, false, st.mapPbK128, TC_SMEM_128);
+    } else {
+      if (bf) GEMM_LAUNCH(256, true, st.mapPbK, TC_SMEM);
+      else GEMM_LAUNCH(256, false, st.mapPbK, TC_SMEM);
+    }
 #undef GEMM_LAUNCH
+  } else {
+    // tiles: Mpad / 64 row tiles x ceil(R / 256) column tiles, column fastest
+    const int ntc = (int)((R + 255) / 256);
+    const int64_t ntiles = (Mpad / 64) * ntc;
+    const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, c->sm_count));
+    if (bf)
+      DMB_LAUNCH(c, (k_tc_gemm_p<256, true>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[kslot], a_row0, a_kx0,
+                 nchunks, cpb, M, R, Y, N, mode, tri, ntc, ntiles, st.err.as<unsigned>());
+    else
+      DMB_LAUNCH(c, (k_tc_gemm_p<256, false>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[kslot], a_row0,
+                 a_kx0, nchunks, cpb, M, R, Y, N, mode, tri, ntc, ntiles, st.err.as<unsigned>());
+  }
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
   dmb::tune_end(c, mk);

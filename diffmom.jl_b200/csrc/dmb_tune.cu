@@ -91,7 +91,7 @@ TuneEntry &entry(int device, int family, int64_t b1, int64_t b2, int ncand) {
 
 const char *family_name(int f) {
   switch (f) {
-    case dmb::TUNE_TC_GEMM_BN: return "k_tc_gemm tile width (256 / 128 complex columns)";
+    case dmb::TUNE_TC_GEMM_BN: return "k_tc_gemm shape (256 / 128 complex columns per tile / persistent 256)";
     case dmb::TUNE_TC_SYRK_STAGES:
       return "k_tc_syrk schedule (4 stages, 1 CTA/SM / 2 stages, 2 CTAs/SM / persistent, lower tiles only)";
     default: return "?";

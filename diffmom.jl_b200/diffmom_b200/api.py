@@ -96,7 +96,8 @@ class EFIEDevice:
         "spin_limit" (polls of a chained triangular-sweep wait before the call
         fails with TimeoutError; negative restores the default),
         "tune_tc_gemm" / "tune_tc_syrk" (0 = autotuned; k pins candidate k:
-        256- or 128-wide sweep GEMM tiles; 4-stage, 2-stage or persistent
+        256- or 128-wide sweep GEMM tiles or a persistent 256-wide grid;
+        4-stage, 2-stage or persistent
         factor-update schedules), "precond_bf16" (1 / 0 / -1 = default: BF16
         instead of TF32 operand pieces for the complex64 factor updates and
         packed sweeps always / never / inside the many-incidence resident

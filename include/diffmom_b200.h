@@ -148,7 +148,8 @@ const char *dmb_version(void);
 #define DMB_OPT_SPIN_LIMIT 9
 /* DMB_OPT_TUNE_TC_GEMM / DMB_OPT_TUNE_TC_SYRK: pin a candidate of the online
  * autotuner (0, the default, lets it choose): the tile width of the
- * tensor-core sweep GEMMs (1: 256, 2: 128 complex columns) and the schedule of
+ * tensor-core sweep GEMMs (1: 256, 2: 128 complex columns per tile; 3:
+ * persistent grid of 256-column tiles, double-buffered accumulators) and the schedule of
  * the complex64 factor updates (1: 4 stages, one CTA per SM; 2: 2 stages, two
  * CTAs per SM; 3: persistent grid over the lower tiles only, double-buffered
  * accumulators).  Unpinned, each launch shape bucket runs every candidate on

@@ -292,9 +292,9 @@ def test_fp64_factor_and_sweeps_on_the_fp64_gemm():
 def test_autotuner_candidates_identical():
     """Every candidate of the online autotuner writes the same bits: the
     complex64 factor (4- or 2-stage update pipelines, persistent lower-tile
-    grid) and a batched sweep (256- or 128-wide GEMM tiles), pinned one at a
-    time, against the tuned run, with TF32 and with BF16 operand pieces; the
-    tuner's report lists what it measured."""
+    grid) and a batched sweep (256- or 128-wide GEMM tiles, or the persistent
+    256-wide grid), pinned one at a time, against the tuned run, with TF32 and
+    with BF16 operand pieces; the tuner's report lists what it measured."""
     from diffmom_b200 import tune_report
     dev = _plate(36)  # 3,960 RWG: four 1,024-row sweep blocks, ragged last
     dev.assemble(K3, precision="mixed")
@@ -303,7 +303,7 @@ def test_autotuner_candidates_identical():
         dev.set_option("precond_bf16", bf)
         out = {}
         for syrk in (0, 1, 2, 3):
-            for gemm in (0, 1, 2):
+            for gemm in (0, 1, 2, 3):
                 if syrk and gemm:
                     continue
                 dev.set_option("tune_tc_syrk", syrk)
@@ -320,7 +320,7 @@ def test_autotuner_candidates_identical():
     print(rep)
     assert "k_tc_gemm" in rep and "k_tc_syrk" in rep
     with pytest.raises(Exception):
-        dev.set_option("tune_tc_gemm", 3)
+        dev.set_option("tune_tc_gemm", 4)
     with pytest.raises(Exception):
         dev.set_option("tune_tc_syrk", 4)
     dev.close()
