@@ -1111,8 +1111,10 @@ void ensure_side_streams(dmb_ctx *c) {
   if (!c->stream2 || !c->stream3) {
     int least = 0, greatest = 0;
     DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
-    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, least));
+    // the same priorities as the factorisation's lookahead streams
+    const int mid = greatest < least ? greatest + 1 : least;
+    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, mid));
+    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, mid));
   }
   for (auto &e : c->la_ev)
     if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

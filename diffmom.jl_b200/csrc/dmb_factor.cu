@@ -948,10 +948,14 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   // err word, then two words (ticket, ready flag) per panel step
   c->d_flags.ensure(std::max<size_t>(64, 4 * (4 + 2 * (size_t)nblk)));
   if (!c->stream2 || !c->stream3) {
+    // the panel chain (context stream) first, then the lookahead updates,
+    // then auxiliary work (right-hand sides, int8 operand planes), which only
+    // fills SMs the factorisation leaves idle
     int least = 0, greatest = 0;
     DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, least));
-    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, least));
+    const int mid = greatest < least ? greatest + 1 : least;
+    if (!c->stream2) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, mid));
+    if (!c->stream3) DMB_CUDA(cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, mid));
   }
   for (auto &e : c->la_ev)
     if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
