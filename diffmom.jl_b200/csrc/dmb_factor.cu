@@ -307,8 +307,99 @@ __device__ __forceinline__ bool elim16_warp(float2 (*A)[65], float2 (*Xs)[17], i
 // Rows and columns at or beyond b are padded with the identity (D = 1, L = 0).
 constexpr size_t DIAG_BLOCKED_SMEM = sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17 + 16) + 16;
 
+// The diagonal tile as the blocked factorisation expects it in shared memory:
+// lower triangle of F at (j, j), zeros above, identity padding beyond b.
+__device__ __forceinline__ void diag_tile_load(int64_t N, int64_t j, int b, const float2 *__restrict__ F,
+                                               float2 (*A)[65]) {
+  const int t = threadIdx.x;
+  float2 v[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int e = t + 256 * m, i = e >> 6, c = e & 63;
+    v[m] = make_float2(0.f, 0.f);
+    if (i < b && c < b) {
+      if (c <= i) v[m] = __ldcg(F + (j + i) * N + j + c);
+    } else if (i == c) {
+      v[m] = make_float2(1.f, 0.f);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    const int e = t + 256 * m;
+    A[e >> 6][e & 63] = v[m];
+  }
+}
+
+// The panel step's update of the next diagonal tile, applied to the tile in
+// shared memory: A[r][c] -= sum_{k<K} W[j + r][woff + k] F[j + c][jcol + k]
+// for c <= r < b (the same products and order as ldlt_tile_update).  The K
+// chunks of 16 are staged in two buffers (the space of the inverse, unused
+// until the end of the factorisation), the next chunk's loads in flight while
+// the current one is multiplied.
+__device__ __forceinline__ void diag_tile_update_smem(int64_t N, int64_t j, int b, int64_t jcol, int K,
+                                                      const float2 *__restrict__ F, const float2 *__restrict__ W,
+                                                      int wstride, int woff, float2 (*A)[65],
+                                                      float2 (*St)[16][65]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float2 acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) acc[i][jj] = make_float2(0.f, 0.f);
+  const int nch = (K + 15) / 16;
+  float2 rw[4], rl[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q, kk = e & 15, rr = e >> 4;
+      const bool ok = rr < b && k0 + kk < K;
+      rw[q] = ok ? __ldcg(W + (j + rr) * wstride + woff + k0 + kk) : make_float2(0.f, 0.f);
+      rl[q] = ok ? __ldcg(F + (j + rr) * N + jcol + k0 + kk) : make_float2(0.f, 0.f);
+    }
+  };
+  auto stage = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q, kk = e & 15, rr = e >> 4;
+      St[2 * buf][kk][rr] = rw[q];
+      St[2 * buf + 1][kk][rr] = rl[q];
+    }
+  };
+  fetch(0);
+  stage(0);
+  __syncthreads();
+  for (int c = 0; c < nch; c++) {
+    if (c + 1 < nch) fetch(16 * (c + 1));
+    const int buf = c & 1;
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      float2 a[4], l[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = St[2 * buf][kk][ty + 16 * i];
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) l[jj] = St[2 * buf + 1][kk][tx + 16 * jj];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) cfma(acc[i][jj], a[i], l[jj]);
+    }
+    if (c + 1 < nch) stage(buf ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      const int r = ty + 16 * i, cc = tx + 16 * jj;
+      if (r < b && cc <= r) A[r][cc] = csub(A[r][cc], acc[i][jj]);
+    }
+  __syncthreads();
+}
+
+// loaded: the tile is already in shared memory (diag_tile_load, possibly
+// updated by diag_tile_update_smem)
 __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restrict__ F, float2 *__restrict__ Linv,
-                                  unsigned *__restrict__ err, unsigned char *smem) {
+                                  unsigned *__restrict__ err, unsigned char *smem, bool loaded = false) {
   float2(*A)[65] = reinterpret_cast<float2(*)[65]>(smem);
   float2(*Wp)[17] = reinterpret_cast<float2(*)[17]>(smem + sizeof(float2) * 64 * 65);
   float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem + sizeof(float2) * (64 * 65 + 64 * 17));
@@ -316,7 +407,7 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
   float2 *dinv = reinterpret_cast<float2 *>(smem + sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17));
   volatile int *bad = reinterpret_cast<volatile int *>(dinv + 16);
   const int t = threadIdx.x;  // 256 threads
-  {
+  if (!loaded) {
     float2 v[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
@@ -500,14 +591,24 @@ __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, 
 // Panel: W = A21 Linv^T (row r: W[r][c] = sum_{k<=c} A21[r][k] Linv[c][k]),
 // then L21 = W D^-1, for the 64 rows from r0.  Reads go through L2 (the
 // fused step kernel reads blocks written by another CTA of the same launch).
+// a_in_smem: the A21 tile is already in As (ldlt_strip_update_smem)
 template <class C>
 __device__ __forceinline__ void ldlt_panel_rows(int64_t N, int64_t j, int b, int64_t r0, C *__restrict__ F,
                                                 const C *__restrict__ Linv, C *__restrict__ W, int wstride,
-                                                int woff, unsigned char *smem_raw) {
+                                                int woff, unsigned char *smem_raw, bool a_in_smem = false) {
   C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
   C(*Li)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw + sizeof(C) * NB * (NB + 1));
   C *dg = reinterpret_cast<C *>(smem_raw + 2 * sizeof(C) * NB * (NB + 1));
-  {
+  if (a_in_smem) {
+    C vl[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) vl[m] = __ldcg(Linv + threadIdx.x + 256 * m);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m;
+      Li[e / NB][e % NB] = vl[m];
+    }
+  } else {
     // 256 threads: all 32 loads of a thread in flight before the shared stores
     C va[16], vl[16];
 #pragma unroll
@@ -604,6 +705,58 @@ __device__ __forceinline__ void ldlt_tile_update(int64_t N, int64_t r0, int64_t 
     }
 }
 
+// The panel step's strip update of a column-0 tile (rows r0.., the next
+// panel's columns c0.. = its diagonal block's), kept in shared memory as the
+// A21 tile of the panel rows that follow (As: its first b columns, zeros
+// beyond): the same products as ldlt_tile_update, without the round trip
+// through F.  Ws / Ls staging past the panel's As / Li / dg space.
+template <class C>
+__device__ __forceinline__ void ldlt_strip_update_smem(int64_t N, int64_t r0, int64_t c0, int b, int64_t jcol,
+                                                       int K, const C *__restrict__ F, const C *__restrict__ W,
+                                                       int wstride, int woff, unsigned char *smem_raw) {
+  C(*As)[NB + 1] = reinterpret_cast<C(*)[NB + 1]>(smem_raw);
+  C(*Ws)[65] = reinterpret_cast<C(*)[65]>(smem_raw + 2 * sizeof(C) * NB * (NB + 1) + sizeof(C) * NB);
+  C(*Ls)[65] = reinterpret_cast<C(*)[65]>(smem_raw + 2 * sizeof(C) * NB * (NB + 1) + sizeof(C) * NB +
+                                          sizeof(C) * 16 * 65);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  C acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) acc[i][jj] = czero<C>();
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+      int kk = e & 15, rr = e >> 4;
+      int64_t r = r0 + rr;
+      bool kin = k0 + kk < K;
+      Ws[kk][rr] = (r < N && kin) ? __ldcg(W + r * wstride + woff + k0 + kk) : czero<C>();
+      Ls[kk][rr] = (rr < b && kin) ? __ldcg(F + (c0 + rr) * N + jcol + k0 + kk) : czero<C>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      C a[4], l[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = Ws[kk][ty + 16 * i];
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) l[jj] = Ls[kk][tx + 16 * jj];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) cfma(acc[i][jj], a[i], l[jj]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      const int rr = ty + 16 * i, k = tx + 16 * jj;
+      const int64_t r = r0 + rr;
+      As[rr][k] = (r < N && k < b) ? csub(__ldcg(F + r * N + c0 + k), acc[i][jj]) : czero<C>();
+    }
+}
+
 // Trailing / strip update on tiles (grid.x row tiles, grid.y column tiles from
 // r_lo; tiles entirely above the diagonal exit at once).
 //
@@ -651,19 +804,34 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
   if (r0 >= N || c0 > r0 + 63) return;
   C(*Ws)[65] = reinterpret_cast<C(*)[65]>(smem_raw);
   C(*Ls)[65] = reinterpret_cast<C(*)[65]>(smem_raw + sizeof(C) * 16 * 65);
-  ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
   if (t == 0) {
-    __syncthreads();
-    if constexpr (std::is_same<C, float2>::value)
-      ldlt_diag_blocked(N, r_lo, nb_next, F, Linv_next, err, smem_raw);
-    else
+    // the next diagonal tile: loaded once, updated and factored in shared
+    // memory (complex64); the update's K chunks are staged in the space of
+    // the tile's inverse
+    if constexpr (std::is_same<C, float2>::value) {
+      float2(*A)[65] = reinterpret_cast<float2(*)[65]>(smem_raw);
+      float2(*St)[16][65] =
+          reinterpret_cast<float2(*)[16][65]>(smem_raw + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
+      diag_tile_load(N, r_lo, nb_next, F, A);
+      diag_tile_update_smem(N, r_lo, nb_next, jcol, K, F, W, wstride, woff, A, St);
+      ldlt_diag_blocked(N, r_lo, nb_next, F, Linv_next, err, smem_raw, true);
+    } else {
+      ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
+      __syncthreads();
       ldlt_diag_block<C>(N, r_lo, nb_next, F, Linv_next, err, reinterpret_cast<C *>(smem_raw));
+    }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
     return;
   }
-  if (ct != 0) return;
+  if (ct != 0) {
+    ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
+    return;
+  }
+  // column 0: the strip tile is the next panel's A21 tile; it stays in
+  // shared memory for the panel rows after the diagonal block is published
+  ldlt_strip_update_smem<C>(N, r0, c0, nb_next, jcol, K, F, W, wstride, woff, smem_raw);
   if (threadIdx.x == 0) {
     long long it = 0;
     int ok = 1;
@@ -680,7 +848,7 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
   }
   __syncthreads();
   if (!s_ok) return;
-  ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw);
+  ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw, true);
 }
 
 // ---------------------------------------------------------------------------
