@@ -396,14 +396,16 @@ __device__ __forceinline__ void diag_tile_update_smem(int64_t N, int64_t j, int 
   __syncthreads();
 }
 
-// loaded: the tile is already in shared memory (diag_tile_load, possibly
-// updated by diag_tile_update_smem)
-__device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restrict__ F, float2 *__restrict__ Linv,
-                                  unsigned *__restrict__ err, unsigned char *smem, bool loaded = false) {
+// Phase 1 of the blocked factorisation: L and D of the diagonal tile (in
+// shared memory, written back to F) and the unit-lower inverses Xd of its
+// four 16 x 16 diagonal blocks.  loaded: the tile is already in shared memory
+// (diag_tile_load, possibly updated by diag_tile_update_smem).  Returns false
+// after a breakdown (uniform).
+__device__ bool ldlt_diag_phase1(int64_t N, int64_t j, int b, float2 *__restrict__ F, unsigned *__restrict__ err,
+                                 unsigned char *smem, bool loaded) {
   float2(*A)[65] = reinterpret_cast<float2(*)[65]>(smem);
   float2(*Wp)[17] = reinterpret_cast<float2(*)[17]>(smem + sizeof(float2) * 64 * 65);
   float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem + sizeof(float2) * (64 * 65 + 64 * 17));
-  float2(*LI)[65] = reinterpret_cast<float2(*)[65]>(smem + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
   float2 *dinv = reinterpret_cast<float2 *>(smem + sizeof(float2) * (2 * 64 * 65 + 64 * 17 + 4 * 16 * 17));
   volatile int *bad = reinterpret_cast<volatile int *>(dinv + 16);
   const int t = threadIdx.x;  // 256 threads
@@ -438,7 +440,7 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
       }
     }
     __syncthreads();
-      if (*bad) return;
+    if (*bad) return false;  // uniform
     if (s == 3) break;
     const int nr = 48 - s0;
     // 1 / D of the 16 pivots; sub-panel W = A21 X^T with up to three outputs
@@ -500,6 +502,18 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
     const int i = e >> 6, c = e & 63;
     if (i < b && c <= i) F[(j + i) * N + j + c] = A[i][c];
   }
+  return true;
+}
+
+// Phase 2: the unit-lower inverse of the factored tile (L in shared memory)
+// by recursive doubling from the four 16 x 16 inverses of phase 1, and its
+// store to Linv.
+__device__ void ldlt_diag_phase2(float2 *__restrict__ Linv, unsigned char *smem, bool skip_diag_blocks = false) {
+  float2(*A)[65] = reinterpret_cast<float2(*)[65]>(smem);
+  float2(*Wp)[17] = reinterpret_cast<float2(*)[17]>(smem + sizeof(float2) * 64 * 65);
+  float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem + sizeof(float2) * (64 * 65 + 64 * 17));
+  float2(*LI)[65] = reinterpret_cast<float2(*)[65]>(smem + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
+  const int t = threadIdx.x;
   // Linv by recursive doubling: 16-level pairs, then the 32-level block
   //   [[X0, 0], [-X1 L10 X0, X1]]
   for (int e = t; e < 64 * 64; e += blockDim.x) {
@@ -575,8 +589,18 @@ __device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restric
     for (int q = 0; q < 4; q++) LI[32 + r0 + 8 * q][c] = make_float2(-p[q].x, -p[q].y);
   }
   __syncthreads();
-  for (int e = t; e < 64 * 64; e += blockDim.x) Linv[e] = LI[e >> 6][e & 63];
+  // (skip_diag_blocks: the 16 x 16 diagonal blocks were stored already)
+  for (int e = t; e < 64 * 64; e += blockDim.x)
+    if (!skip_diag_blocks || (e >> 10) != ((e & 63) >> 4)) Linv[e] = LI[e >> 6][e & 63];
   __syncthreads();
+}
+
+// Blocked form of ldlt_diag_block for complex64 blocks: phase 1 (with the
+// 16 x 16 inverses), the store of L and D, phase 2.
+__device__ void ldlt_diag_blocked(int64_t N, int64_t j, int b, float2 *__restrict__ F, float2 *__restrict__ Linv,
+                                  unsigned *__restrict__ err, unsigned char *smem, bool loaded = false) {
+  if (!ldlt_diag_phase1(N, j, b, F, err, smem, loaded)) return;
+  ldlt_diag_phase2(Linv, smem);
 }
 template <class C>
 __global__ void __launch_bounds__(256) k_ldlt_diag(int64_t N, int64_t j, int b, C *__restrict__ F,
@@ -656,6 +680,90 @@ __global__ void __launch_bounds__(256) k_ldlt_panel(int64_t N, int64_t j, int b,
                                                     int woff) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ldlt_panel_rows<C>(N, j, b, j + b + (int64_t)blockIdx.x * NB, F, Linv, W, wstride, woff, smem_raw);
+}
+
+// Panel rows of the fused step by blocked forward substitution, W L11^T =
+// A21 in four 16-column blocks: T_J = A21_J - sum_{K<J} W_K L_JK^T, then
+// W_J = T_J X_J^T with X_J the inverse of L_JJ (the diagonal 16 x 16 blocks
+// of the tile's inverse, published with L and D before the rest of the
+// inverse exists).  A21 is already in As (ldlt_strip_update_smem); T and W
+// overwrite it in place.  L21 = W D^-1 to F, W to the panel buffer.
+__device__ __forceinline__ void ldlt_panel_rows_blk(int64_t N, int64_t j, int b, int64_t r0,
+                                                    float2 *__restrict__ F, const float2 *__restrict__ Linv,
+                                                    float2 *__restrict__ W, int wstride, int woff,
+                                                    unsigned char *smem_raw) {
+  float2(*As)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(smem_raw);
+  float2(*Lb)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(smem_raw + sizeof(float2) * NB * (NB + 1));
+  float2 *dinv = reinterpret_cast<float2 *>(smem_raw + 2 * sizeof(float2) * NB * (NB + 1));
+  float2(*X)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem_raw + 2 * sizeof(float2) * NB * (NB + 1) +
+                                                          sizeof(float2) * NB);
+  {
+    float2 v[16], xv[4];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m, c = e >> 6, k = e & 63;
+      v[m] = (c < b && k <= c) ? __ldcg(F + (j + c) * N + j + k) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q, J = e >> 8, i = (e >> 4) & 15, c = e & 15;
+      xv[q] = __ldcg(Linv + (16 * J + i) * NB + 16 * J + c);
+    }
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m;
+      Lb[e >> 6][e & 63] = v[m];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = threadIdx.x + 256 * q;
+      X[e >> 8][(e >> 4) & 15][e & 15] = xv[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < b) dinv[threadIdx.x] = cdiv(make_float2(1.f, 0.f), Lb[threadIdx.x][threadIdx.x]);
+  const int c = threadIdx.x & 15, rq = threadIdx.x >> 4;  // rows rq + 16 q
+  for (int J = 0; J < 4; J++) {
+    if (16 * J >= b) break;  // uniform
+    float2 tq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) tq[q] = As[rq + 16 * q][16 * J + c];
+    for (int k = 0; k < 16 * J; k++) {
+      const float2 l = Lb[16 * J + c][k];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float2 w = As[rq + 16 * q][k];
+        tq[q].x -= w.x * l.x - w.y * l.y;
+        tq[q].y -= w.x * l.y + w.y * l.x;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; q++) As[rq + 16 * q][16 * J + c] = tq[q];
+    __syncthreads();
+    float2 wq[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      if (k <= c) {
+        const float2 x = X[J][c][k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) cfma(wq[q], As[rq + 16 * q][16 * J + k], x);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; q++) As[rq + 16 * q][16 * J + c] = wq[q];
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e >> 6, cc = e & 63;
+    const int64_t gr = r0 + r;
+    if (gr < N && cc < b) {
+      const float2 w = As[r][cc];
+      W[gr * wstride + woff + cc] = w;
+      F[gr * N + j + cc] = cmul(w, dinv[cc]);
+    }
+  }
 }
 
 // F[r][c] -= sum_{k<K} W[r][woff+k] F[c][jcol+k] on the 64 x 64 tile at
@@ -814,15 +922,29 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
           reinterpret_cast<float2(*)[16][65]>(smem_raw + sizeof(float2) * (64 * 65 + 64 * 17 + 4 * 16 * 17));
       diag_tile_load(N, r_lo, nb_next, F, A);
       diag_tile_update_smem(N, r_lo, nb_next, jcol, K, F, W, wstride, woff, A, St);
-      ldlt_diag_blocked(N, r_lo, nb_next, F, Linv_next, err, smem_raw, true);
+      // L, D and the 16 x 16 diagonal blocks of the inverse are published
+      // first (the panel rows need only them); the rest of the tile's
+      // inverse, for the solves, is formed while the panel rows run
+      const bool ok = ldlt_diag_phase1(N, r_lo, nb_next, F, err, smem_raw, true);
+      if (ok) {
+        float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem_raw + sizeof(float2) * (64 * 65 + 64 * 17));
+        for (int e = threadIdx.x; e < 4 * 256; e += 256) {
+          const int s = e >> 8, i = (e >> 4) & 15, c = e & 15;
+          Linv_next[(16 * s + i) * NB + 16 * s + c] = Xd[s][i][c];
+        }
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
+      if (ok) ldlt_diag_phase2(Linv_next, smem_raw, true);
     } else {
       ldlt_tile_update<C>(N, r0, c0, c_hi, jcol, K, F, W, wstride, woff, Ws, Ls);
       __syncthreads();
       ldlt_diag_block<C>(N, r_lo, nb_next, F, Linv_next, err, reinterpret_cast<C *>(smem_raw));
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
     }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
     return;
   }
   if (ct != 0) {
@@ -848,7 +970,10 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
   }
   __syncthreads();
   if (!s_ok) return;
-  ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw, true);
+  if constexpr (std::is_same<C, float2>::value)
+    ldlt_panel_rows_blk(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw);
+  else
+    ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw, true);
 }
 
 // ---------------------------------------------------------------------------
