@@ -976,6 +976,73 @@ __global__ void __launch_bounds__(256) k_ldlt_step(int64_t N, int64_t r_lo, int6
     ldlt_panel_rows<C>(N, r_lo, nb_next, r0, F, Linv_next, W, wstride, woff_next, smem_raw, true);
 }
 
+// The first 64-wide block of a middle panel (complex64), one launch: the
+// CTA holding ticket 0 factors the diagonal tile at j (phase 1), publishes
+// L, D and the 16 x 16 inverse blocks, then forms the rest of the inverse
+// (phase 2); every other CTA loads its 64 rows of the block column, waits for
+// the publication (bounded, error bit 4 on expiry) and runs its panel rows
+// by blocked forward substitution.  Replaces k_ldlt_diag + k_ldlt_panel.
+__global__ void __launch_bounds__(256) k_ldlt_first(int64_t N, int64_t j, int b, float2 *__restrict__ F,
+                                                    float2 *__restrict__ Linv, float2 *__restrict__ W, int wstride,
+                                                    int woff, unsigned *__restrict__ sync,
+                                                    unsigned *__restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned s_ticket;
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(&sync[0], 1u);
+  __syncthreads();
+  const unsigned t = s_ticket;
+  if (t == 0) {
+    const bool ok = ldlt_diag_phase1(N, j, b, F, err, smem_raw, false);
+    if (ok) {
+      float2(*Xd)[16][17] = reinterpret_cast<float2(*)[16][17]>(smem_raw + sizeof(float2) * (64 * 65 + 64 * 17));
+      for (int e = threadIdx.x; e < 4 * 256; e += 256) {
+        const int s = e >> 8, i = (e >> 4) & 15, c = e & 15;
+        Linv[(16 * s + i) * NB + 16 * s + c] = Xd[s][i][c];
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicExch(&sync[1], 1u);
+    if (ok) ldlt_diag_phase2(Linv, smem_raw, true);
+    return;
+  }
+  const int64_t r0 = j + b + (int64_t)(t - 1) * NB;
+  if (r0 >= N) return;
+  {
+    float2(*As)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(smem_raw);
+    float2 va[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m, rr = e >> 6, k = e & 63;
+      const int64_t r = r0 + rr;
+      va[m] = (r < N && k < b) ? __ldcg(F + r * N + j + k) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int e = threadIdx.x + 256 * m;
+      As[e >> 6][e & 63] = va[m];
+    }
+  }
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    int ok = 1;
+    while (*((volatile unsigned *)&sync[1]) == 0u) {
+      if (++it > SPIN_LIMIT) {
+        atomicOr(err, 4u);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  ldlt_panel_rows_blk(N, j, b, r0, F, Linv, W, wstride, woff, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // ticket-ordered triangular solves (one right-hand side per grid.y)
 // ---------------------------------------------------------------------------
@@ -1210,6 +1277,9 @@ template <class C> void set_smem_attrs() {
                                 (int)diag_smem<C>()));
   DMB_CUDA(cudaFuncSetAttribute(k_ldlt_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)std::max(panel, diag_smem<C>())));
+  if constexpr (std::is_same<C, float2>::value)
+    DMB_CUDA(cudaFuncSetAttribute(k_ldlt_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max(panel, diag_smem<C>())));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_fwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * sizeof(C) * NB * NB)));
   DMB_CUDA(cudaFuncSetAttribute(k_trsv_bwd<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1239,7 +1309,8 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   c->d_W.ensure(sizeof(C) * N * NBW * 2);
   c->d_dinv.ensure(sizeof(C) * (size_t)nblk * NB * NB);  // Linv blocks
   // err word, then two words (ticket, ready flag) per panel step
-  c->d_flags.ensure(std::max<size_t>(64, 4 * (4 + 2 * (size_t)nblk)));
+  // (then two more per 64-block for the first block of each middle panel)
+  c->d_flags.ensure(std::max<size_t>(64, 4 * (4 + 4 * (size_t)nblk)));
   if (!c->stream2 || !c->stream3) {
     // the panel chain (context stream) first, then the lookahead updates,
     // then auxiliary work (right-hand sides, int8 operand planes), which only
@@ -1255,7 +1326,7 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
   unsigned *err = c->d_flags.as<unsigned>();
   C *Linv = c->d_dinv.as<C>();
   unsigned *step_sync = err + 4;
-  DMB_CUDA(cudaMemsetAsync(err, 0, 4 * (4 + 2 * (size_t)nblk), c->stream));
+  DMB_CUDA(cudaMemsetAsync(err, 0, 4 * (4 + 4 * (size_t)nblk), c->stream));
   // the fused panel step (strip + next diagonal block + next panel) for
   // complex64 factors; complex128 factors keep separate launches (their
   // 134 KB panel staging would allow one CTA per SM)
@@ -1345,8 +1416,15 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
       for (int64_t j = J; j < JE; j += NB) {
         const int b = (int)std::min<int64_t>(NB, N - j);
         C *Lblk = Linv + (j / NB) * NB * NB;
-        if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, diag_smem<C>(), N, j, b, F, Lblk, err);
         const int64_t rest = N - j - b;
+        if constexpr (std::is_same<C, float2>::value) {
+          if (!diag_done) {  // the first block of the middle panel: factor + panel rows in one launch
+            DMB_LAUNCH(c, k_ldlt_first, 1 + blocks_for(std::max<int64_t>(rest, 0), NB), 256, sm_step, N, j, b, F,
+                       Lblk, Wb, NBW, (int)(j - J2), step_sync + 2 * nblk + 2 * (j / NB), err);
+            diag_done = panel_done = true;
+          }
+        }
+        if (!diag_done) DMB_LAUNCH(c, k_ldlt_diag<C>, 1, 256, diag_smem<C>(), N, j, b, F, Lblk, err);
         if (rest <= 0) break;
         if (!panel_done)
           DMB_LAUNCH(c, k_ldlt_panel<C>, blocks_for(rest, NB), 256, sm_panel, N, j, b, F, Lblk, Wb, NBW,
