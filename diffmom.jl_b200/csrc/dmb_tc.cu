@@ -895,8 +895,11 @@ struct TcState {
   bool attr = false;
   // general GEMMs: packed Z (keyed by the Z version), packed right-hand
   // sides, packed triangular-solve panels
-  DevBuf Zp, Xp, Pa, Pb;
-  CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4], mapPbK128[4];
+  // Pb: packed right-hand-side blocks of the sweeps, four slots (0: the
+  // diagonal-block product, 1-3: the off-diagonal products of successive
+  // blocks, read by the lookahead stream too)
+  DevBuf Zp, Xp, Pa, Pb[4];
+  CUtensorMap mapZ, mapX, mapPaK[4], mapPbK[4][4], mapPbK128[4][4];
   uint64_t zp_version = ~0ull;
   // factor packed once per factorisation for the batched triangular solves:
   // L'' (strict lower), (L^T)'' and the inverses of the 1024-row diagonal
@@ -904,8 +907,9 @@ struct TcState {
   DevBuf Lp, Ltp, Dfp, Dbp;
   CUtensorMap mapL, mapLt, mapDf, mapDb;
   int64_t lp_n = -1;
-  int lp_fmt = -1, pb_fmt = -1;  // operand formats of the packed factor / of Pb's maps
-  int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key = -1;
+  int lp_fmt = -1, pb_fmt[4] = {-1, -1, -1, -1};  // operand formats of the packed factor / of Pb's maps
+  int64_t zp_n = -1, xp_key = -1, xp_n = -1, pa_key = -1, pb_key[4] = {-1, -1, -1, -1};
+  cudaEvent_t sw_ev[3][4] = {};  // pipelined sweeps: packed / next-block / rest events, ring of 4
   bool gemm_attr = false;
 };
 
@@ -1101,14 +1105,14 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
     for (int i = 0; i < 4; i++) make_map(&st.mapPaK[i], st.Pa.as<float>(), (uint64_t)(2 * Npad), TC_BM, 1536 * (i + 1));
     st.pa_key = Npad;
   }
-  if (st.pb_key != Rpad || st.pb_fmt != 0) {
-    st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
+  if (st.pb_key[0] != Rpad || st.pb_fmt[0] != 0) {
+    st.Pb[0].ensure(sizeof(float) * Rpad * 6 * 1024);
     for (int i = 0; i < 4; i++) {
-      make_map(&st.mapPbK[i], st.Pb.as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
-      make_map(&st.mapPbK128[i], st.Pb.as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
+      make_map(&st.mapPbK[0][i], st.Pb[0].as<float>(), (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+      make_map(&st.mapPbK128[0][i], st.Pb[0].as<float>(), (uint64_t)Rpad, 128, 1536 * (i + 1));
     }
-    st.pb_key = Rpad;
-    st.pb_fmt = 0;
+    st.pb_key[0] = Rpad;
+    st.pb_fmt[0] = 0;
   }
   dim3 ga((unsigned)(Kpad / 32), (unsigned)(Mpad / 32));
   if (backward)
@@ -1118,10 +1122,10 @@ void tc_trsm_update(dmb_ctx *c, const float2 *F, int64_t N, int64_t r_lo, int64_
     DMB_LAUNCH(c, (k_pack_a<false, false, float2, float>), ga, 256, 0, M, (int64_t)width, Kpad, F + r_lo * N + k_lo,
                N, st.Pa.as<float>());
   DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)width, Kpad,
-             X + k_lo, N, st.Pb.as<float>());
+             X + k_lo, N, st.Pb[0].as<float>());
   dim3 grid((unsigned)(Rpad / TC_BN), (unsigned)(Mpad / 64));
   kt_begin(c);
-  DMB_LAUNCH(c, (k_tc_gemm<1, 256, false>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[kslot], 0, 0, (int)(ld / TC_BK), 48, M, R,
+  DMB_LAUNCH(c, (k_tc_gemm<1, 256, false>), grid, 128, TC_SMEM, st.mapPaK[kslot], st.mapPbK[0][kslot], 0, 0, (int)(ld / TC_BK), 48, M, R,
              X + r_lo, N, 1, 0, st.err.as<unsigned>());
   kt_end(c, 8.0 * (double)M * (double)width * (double)R);
 }
@@ -1188,29 +1192,34 @@ void tc_trsm_pack_diag(dmb_ctx *c, int64_t o, const double2 *Xb, int64_t ld, int
              db);
 }
 
-// Y (op)= A_packed[rows a_row0.., K from a_kx0] * X[k0 : k0 + w], B packed here
-void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0, int a_kx0, int64_t M, int w,
-                    const double2 *Xk, double2 *Y, int64_t N, int64_t R, int mode, int tri) {
-  if (M <= 0) return;
-  const int64_t Kpad = round_up(w, 256), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
-  const int kslot = (int)(Kpad / 256) - 1;
-  // operands in the format of the packed factor
-  const bool bf = st.lp_fmt == 1;
-  if (st.pb_key != Rpad || st.pb_fmt != (int)bf) {
-    st.Pb.ensure(sizeof(float) * Rpad * 6 * 1024);
+// B'' of the sweeps: X[k0 : k0 + w] (R columns) packed into slot `slot`
+void pack_b_slot(dmb_ctx *c, TcState &st, int slot, int w, const double2 *Xk, int64_t N, int64_t R) {
+  const int64_t Kpad = round_up(w, 256), Rpad = round_up(R, TC_BN);
+  const bool bf = st.lp_fmt == 1;  // operands in the format of the packed factor
+  if (st.pb_key[slot] != Rpad || st.pb_fmt[slot] != (int)bf) {
+    st.Pb[slot].ensure(sizeof(float) * Rpad * 6 * 1024);
     for (int i = 0; i < 4; i++) {
-      make_map_op(&st.mapPbK[i], st.Pb.p, bf, (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
-      make_map_op(&st.mapPbK128[i], st.Pb.p, bf, (uint64_t)Rpad, 128, 1536 * (i + 1));
+      make_map_op(&st.mapPbK[slot][i], st.Pb[slot].p, bf, (uint64_t)Rpad, TC_BN, 1536 * (i + 1));
+      make_map_op(&st.mapPbK128[slot][i], st.Pb[slot].p, bf, (uint64_t)Rpad, 128, 1536 * (i + 1));
     }
-    st.pb_key = Rpad;
-    st.pb_fmt = (int)bf;
+    st.pb_key[slot] = Rpad;
+    st.pb_fmt[slot] = (int)bf;
   }
   if (bf)
     DMB_LAUNCH(c, k_pack_b<__nv_bfloat16>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w,
-               Kpad, Xk, N, st.Pb.as<__nv_bfloat16>());
+               Kpad, Xk, N, st.Pb[slot].as<__nv_bfloat16>());
   else
     DMB_LAUNCH(c, k_pack_b<float>, dim3((unsigned)(Kpad / 256), (unsigned)Rpad), 256, 0, R, (int64_t)w, Kpad, Xk,
-               N, st.Pb.as<float>());
+               N, st.Pb[slot].as<float>());
+}
+
+// Y (op)= A_packed[rows a_row0.., K from a_kx0] * B'' of slot `slot` (K = w)
+void gemm_packed(dmb_ctx *c, TcState &st, int slot, const CUtensorMap &mapA, int a_row0, int a_kx0, int64_t M,
+                 int w, double2 *Y, int64_t N, int64_t R, int mode, int tri) {
+  if (M <= 0) return;
+  const int64_t Kpad = round_up(w, 256), Mpad = round_up(M, 64), Rpad = round_up(R, TC_BN);
+  const int kslot = (int)(Kpad / 256) - 1;
+  const bool bf = st.lp_fmt == 1;
   // launch shape from the autotuner, per (row tiles, columns, triangular
   // kind): one CTA per 64 x 256 or 64 x 128 complex tile (128 doubles the
   // CTAs of launches with few row tiles), or the persistent 256-wide form (one
@@ -1228,11 +1237,11 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
   DMB_LAUNCH(c, (k_tc_gemm<1, BNV, BFV>), dim3((unsigned)(Rpad / BNV), (unsigned)(Mpad / 64)), 128, SMEMV, mapA, \
              MAPB[kslot], a_row0, a_kx0, nchunks, cpb, M, R, Y, N, mode, tri, st.err.as<unsigned>())
     if (cand == 1) {
-      if (bf) GEMM_LAUNCH(128, true, st.mapPbK128, TC_SMEM_128);
-      else GEMM_LAUNCH(128, false, st.mapPbK128, TC_SMEM_128);
+      if (bf) GEMM_LAUNCH(128, true, st.mapPbK128[slot], TC_SMEM_128);
+      else GEMM_LAUNCH(128, false, st.mapPbK128[slot], TC_SMEM_128);
     } else {
-      if (bf) GEMM_LAUNCH(256, true, st.mapPbK, TC_SMEM);
-      else GEMM_LAUNCH(256, false, st.mapPbK, TC_SMEM);
+      if (bf) GEMM_LAUNCH(256, true, st.mapPbK[slot], TC_SMEM);
+      else GEMM_LAUNCH(256, false, st.mapPbK[slot], TC_SMEM);
     }
 #undef GEMM_LAUNCH
   } else {
@@ -1241,15 +1250,24 @@ void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0
     const int64_t ntiles = (Mpad / 64) * ntc;
     const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, c->sm_count));
     if (bf)
-      DMB_LAUNCH(c, (k_tc_gemm_p<256, true>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[kslot], a_row0, a_kx0,
+      DMB_LAUNCH(c, (k_tc_gemm_p<256, true>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[slot][kslot], a_row0, a_kx0,
                  nchunks, cpb, M, R, Y, N, mode, tri, ntc, ntiles, st.err.as<unsigned>());
     else
-      DMB_LAUNCH(c, (k_tc_gemm_p<256, false>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[kslot], a_row0,
+      DMB_LAUNCH(c, (k_tc_gemm_p<256, false>), dim3(G), 192, tcgp_smem<256>(), mapA, st.mapPbK[slot][kslot], a_row0,
                  a_kx0, nchunks, cpb, M, R, Y, N, mode, tri, ntc, ntiles, st.err.as<unsigned>());
   }
   // a triangular A does half the MACs
   kt_end(c, (tri ? 4.0 : 8.0) * (double)M * (double)w * (double)R);
   dmb::tune_end(c, mk);
+}
+
+
+// Y (op)= A_packed[rows a_row0.., K from a_kx0] * X[k0 : k0 + w], B packed here
+void gemm_prepacked(dmb_ctx *c, TcState &st, const CUtensorMap &mapA, int a_row0, int a_kx0, int64_t M, int w,
+                    const double2 *Xk, double2 *Y, int64_t N, int64_t R, int mode, int tri) {
+  if (M <= 0) return;
+  pack_b_slot(c, st, 0, w, Xk, N, R);
+  gemm_packed(c, st, 0, mapA, a_row0, a_kx0, M, w, Y, N, R, mode, tri);
 }
 
 // one sweep of the batched solve with the packed factor:
@@ -1260,17 +1278,77 @@ void tc_trsm_sweep(dmb_ctx *c, int64_t N, double2 *X, int64_t R, bool backward) 
   TcState &st = tc_state(c);
   DMB_REQUIRE(st.lp_n == N, DMB_ERR_STATE, "factor not packed for the batched solves");
   const int64_t nout = (N + TB - 1) / TB;
+  // Pipelined over two streams.  Main stream, per block o: the diagonal-block
+  // product (X_o = Linv_o X_o, B'' in slot 0), X_o packed into slot 1 +
+  // o mod 3, then the update of the block the sweep meets next (the critical
+  // one).  Lookahead stream: the update of the block after that, then of all
+  // remaining rows.  Each row block is updated by one stream at a time:
+  // before block o's diagonal product the main stream waits for the
+  // lookahead update of block o made by block o - 2 (which follows every
+  // earlier lookahead update), and before its critical update of block o + 1
+  // for the one made by block o - 1.  A packed slot is reused three blocks
+  // later, after the main stream has waited for a later lookahead event.
+  if (!c->stream2) {
+    int least = 0, greatest = 0;
+    DMB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    const int mid = greatest < least ? greatest + 1 : least;
+    DMB_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, mid));
+  }
+  for (auto &row : st.sw_ev)
+    for (auto &e : row)
+      if (!e) DMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t *ev_pack = st.sw_ev[0], *ev_next = st.sw_ev[1], *ev_rest = st.sw_ev[2];
+  // rows of the block the sweep meets s blocks after block o (-1 for none)
+  auto block_rows = [&](int64_t o, int64_t s, int64_t &r0, int64_t &r1) {
+    const int64_t q = backward ? o - s : o + s;
+    if (q < 0 || q >= nout) return false;
+    r0 = q * TB;
+    r1 = std::min<int64_t>(N, r0 + TB);
+    return true;
+  };
   for (int64_t s = 0; s < nout; s++) {
     const int64_t o = backward ? nout - 1 - s : s;
     const int64_t o0 = o * TB, o1 = std::min<int64_t>(N, o0 + TB);
     const int ow = (int)(o1 - o0);
+    const int slot = 1 + (int)(s % 3);
+    if (s >= 2) DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_next[(s - 2) % 4], 0));
     gemm_prepacked(c, st, backward ? st.mapDb : st.mapDf, (int)(2 * TB * o), 0, ow, ow, X + o0, X + o0, N, R, 0,
                    backward ? 2 : 1);
-    if (backward)
-      gemm_prepacked(c, st, st.mapLt, 0, (int)(6 * o0), o0, ow, X + o0, X, N, R, 1, 0);
-    else
-      gemm_prepacked(c, st, st.mapL, (int)(2 * o1), (int)(6 * o0), N - o1, ow, X + o0, X + o1, N, R, 1, 0);
+    pack_b_slot(c, st, slot, ow, X + o0, N, R);
+    DMB_CUDA(cudaEventRecord(ev_pack[s % 4], c->stream));
+    // the off-diagonal product on rows [ra, rb): backward reads rows of the
+    // packed L^T'' (K from o0), forward rows of L''
+    auto update = [&](int64_t ra, int64_t rb) {
+      if (rb <= ra) return;
+      if (backward)
+        gemm_packed(c, st, slot, st.mapLt, (int)(2 * ra), (int)(6 * o0), rb - ra, ow, X + ra, N, R, 1, 0);
+      else
+        gemm_packed(c, st, slot, st.mapL, (int)(2 * ra), (int)(6 * o0), rb - ra, ow, X + ra, N, R, 1, 0);
+    };
+    int64_t c0, c1;
+    if (block_rows(o, 1, c0, c1)) {
+      if (s >= 1) DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_next[(s - 1) % 4], 0));
+      update(c0, c1);
+    }
+    {
+      StreamSwap sw(c, c->stream2);
+      DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_pack[s % 4], 0));
+      int64_t n0, n1;
+      if (block_rows(o, 2, n0, n1)) update(n0, n1);
+      DMB_CUDA(cudaEventRecord(ev_next[s % 4], c->stream));
+      // the rest: rows beyond the block after next
+      if (backward) {
+        int64_t e0, e1;
+        if (block_rows(o, 3, e0, e1)) update(0, e1);
+      } else {
+        int64_t e0, e1;
+        if (block_rows(o, 3, e0, e1)) update(e0, N);
+      }
+      DMB_CUDA(cudaEventRecord(ev_rest[s % 4], c->stream));
+    }
   }
+  // the sweep ends when the lookahead stream is done
+  DMB_CUDA(cudaStreamWaitEvent(c->stream, ev_rest[(nout - 1) % 4], 0));
 }
 
 // drop the context's packed operands (called when the context is destroyed)
@@ -1279,8 +1357,12 @@ void tc_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_tc_states.size(); i++) {
     if (g_tc_states[i].first != c) continue;
     TcState *st = g_tc_states[i].second;
-    for (DevBuf *b : {&st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb, &st->Lp, &st->Ltp, &st->Dfp, &st->Dbp})
+    for (DevBuf *b : {&st->err, &st->Zp, &st->Xp, &st->Pa, &st->Pb[0], &st->Pb[1], &st->Pb[2], &st->Pb[3],
+                      &st->Lp, &st->Ltp, &st->Dfp, &st->Dbp})
       b->release();
+    for (auto &row : st->sw_ev)
+      for (auto &e : row)
+        if (e) cudaEventDestroy(e);
     for (int slot = 0; slot < TC_UPD_SLOTS; slot++) {
       st->A[slot].release();
       st->B[slot].release();
