@@ -1388,19 +1388,33 @@ template <class C> void ldlt_factor(dmb_ctx *c, C *F) {
     DMB_CUDA(cudaEventRecord(done, s));
     (which == 1 ? pend2 : pend3) = true;
   };
-  // after a 256-wide middle panel: the rest of its block column
+  // after a 256-wide middle panel: the rest of its block column, and the
+  // first 256 columns of the next block column (the next block column's first
+  // panel): on stream3 behind the trailing update that also covers them, or,
+  // after the block column's last panel, on the main stream once stream3 has
+  // joined.  The trailing update at the block column's end then leaves those
+  // 256 columns out, so no K = 1,024 update sits on the chain.
   auto update_block_column = [&](int64_t r0, int64_t c_hi, int64_t jcol, int K, const C *Wb, int woff) {
     join2();
     const int64_t cmid = std::min<int64_t>(c_hi, r0 + NBO);
     update(r0, cmid, jcol, K, Wb, woff, 0);
     side(1, cmid, c_hi, jcol, K, Wb, woff);
+    const int64_t n0 = c_hi, n1 = std::min<int64_t>(N, c_hi + NBO);
+    if (n0 < n1) {
+      if (r0 >= c_hi) {  // the block column's last panel
+        join3();
+        update(n0, n1, jcol, K, Wb, woff, 0);
+      } else {
+        side(2, n0, n1, jcol, K, Wb, woff);
+      }
+    }
   };
-  // after a block column: the trailing matrix
+  // after a block column: the trailing matrix beyond the next block column's
+  // first panel
   auto update_trailing = [&](int64_t r0, int64_t jcol, int K, const C *Wb) {
     join2();
     join3();
     const int64_t c1 = std::min<int64_t>(N, r0 + NBO), c2 = std::min<int64_t>(N, r0 + NBW);
-    update(r0, c1, jcol, K, Wb, 0, 0);
     side(1, c1, c2, jcol, K, Wb, 0);
     side(2, c2, N, jcol, K, Wb, 0);
   };
