@@ -20,10 +20,11 @@
 //     and their int8 product is exact in int32 (128^2 K < 2^31), so
 //     C'_i = (A'_i B'_i) mod m_i = C' mod m_i;
 //   * Chinese remainder theorem as a fraction: C' / M = sum_i C'_i y_i / m_i
-//     (mod 1), y_i = (M / m_i)^-1 mod m_i.  The drains accumulate the 96-bit
-//     fixed-point fraction S = sum_i C'_i f_i (mod 2^96), f_i =
-//     round(2^96 y_i / m_i), as a uint64 high word (in Y's place) and a
-//     uint32 low word (scratch); S / 2^96 is C' / M to within 2^-85, and
+//     (mod 1), y_i = (M / m_i)^-1 mod m_i.  The drains keep each C'_i (one
+//     byte) in residue planes and the drain of a tile's last modulus forms
+//     the 96-bit fixed-point fraction S = sum_i C'_i f_i (mod 2^96), f_i =
+//     round(2^96 y_i / m_i), as a uint64 high word and a uint32 low word;
+//     S / 2^96 is C' / M to within 2^-85, and
 //     Y = (int64(hi) + lo 2^-32) M 2^-64 2^-(a + b) sigma tau.  (A 64-bit
 //     fraction alone leaves ~2^-53 M of C', about 1e-12 of an EFIE row's
 //     product.)  One int8 product per modulus: 13 for the residuals (~1e-13
@@ -55,9 +56,10 @@
 //                     level accumulates while the other drains), one commit
 //                     per drain;
 //   warps 0-3         drain each level (slices: tcgen05.ld, scale, FP64
-//                     store / add) or modulus (residues: tcgen05.ld, reduce
-//                     mod m_i, uint64 fraction add; the last modulus of a tile
-//                     converts to FP64).
+//                     store / add); residues: warps 0-7 drain each modulus
+//                     (tcgen05.ld, reduce mod m_i, one byte per element into
+//                     the tile's residue planes; the last modulus of a tile
+//                     reads the other residues back and converts to FP64).
 // Every wait is bounded (error bit, abort flag, TMEM freed); no multicast.
 #include <algorithm>
 #include <vector>
@@ -116,29 +118,25 @@ __device__ __forceinline__ unsigned oz_mod(int v, unsigned m, unsigned mmul, uns
   return (unsigned)(r < 0 ? r + (int)m : r);
 }
 
-// Global accesses to the fraction-sum scratch marked evict-last in L2: the
-// CTAs' running sums (a few tens of MB) are re-read once per modulus, while
-// the int8 operand planes stream through L2 once per product.
+// Global accesses to the residue planes marked evict-last in L2: a CTA's
+// planes (416 KB) are read back at its tile's last modulus, while the int8
+// operand planes stream through L2 once per product.
 __device__ __forceinline__ uint64_t l2_evict_last_policy() {
   uint64_t p;
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
-__device__ __forceinline__ unsigned long long ld_keep(const unsigned long long *a, uint64_t pol) {
-  unsigned long long v;
-  asm volatile("ld.global.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(a), "l"(pol));
+__device__ __forceinline__ uint4 ld_keep4(const uint4 *a, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(a), "l"(pol));
   return v;
 }
-__device__ __forceinline__ unsigned ld_keep(const unsigned *a, uint64_t pol) {
-  unsigned v;
-  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ void st_keep(unsigned long long *a, unsigned long long v, uint64_t pol) {
-  asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(a), "l"(v), "l"(pol) : "memory");
-}
-__device__ __forceinline__ void st_keep(unsigned *a, unsigned v, uint64_t pol) {
-  asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol) : "memory");
+__device__ __forceinline__ void st_keep4(uint4 *a, uint4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w), "l"(pol)
+               : "memory");
 }
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -202,7 +200,25 @@ __device__ __forceinline__ bool oz_next_seg(OzIter &it, OzSeg &sg) {
   return true;
 }
 constexpr int OZ_TILE_ELEMS = 64 * OZ_BN;  // complex outputs per tile (workspace slot size)
-constexpr int OZ_S_ELEMS = 128 * OZ_BN;    // residues: fraction sums per tile (real-stacked rows)
+// residues of one tile: OZ_NMOD planes of 128 real-stacked rows x 256 columns,
+// one byte each; in a plane, 16-column groups of 128 rows x 16 bytes (row r's
+// 16 residues of group g at byte g 2048 + 16 r)
+constexpr int OZ_RES_PLANE = 128 * OZ_BN;
+constexpr int64_t OZ_RES_TILE = (int64_t)OZ_NMOD * OZ_RES_PLANE;
+
+// S = sum over the 16 residues packed in p (bytes, element q in byte q) of
+// r_q f, f = fh 2^32 + fl, accumulated as th 2^32 + tl (tl < 2^44 for up to
+// 13 terms, so no carry is lost before the final fold)
+__device__ __forceinline__ void oz_frac_add(const uint4 p, unsigned long long fh, unsigned long long fl,
+                                            unsigned long long (&th)[16], unsigned long long (&tl)[16]) {
+  const unsigned w[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const unsigned long long u = (w[q >> 2] >> (8 * (q & 3))) & 0xffu;
+    tl[q] += u * fl;
+    th[q] += u * fh;
+  }
+}
 
 // warps per CTA: slices 4 drain + producer + MMA issuer; residues 8 drain
 // (two per TMEM lane quarter, each on half of the columns) + producer + MMA
@@ -215,8 +231,7 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
                                                     int64_t Rv, double2 *__restrict__ Y, double2 *__restrict__ P,
                                                     int64_t ldy, int ncol, int64_t ntiles,
                                                     const double *__restrict__ rs, const double *__restrict__ cs,
-                                                    unsigned long long *__restrict__ Sh, unsigned *__restrict__ Sl,
-                                                    unsigned *err) {
+                                                    unsigned char *__restrict__ Rres, unsigned *err) {
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -329,16 +344,19 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
     // tile rows of its quarter (warp & 3; rows 0-63: real parts of the 64
     // complex rows, 64-127: imaginary parts) and on half of the columns
     // (warp >> 2).  Per modulus a thread reads its row's int32 sums, 16
-    // columns at a time, reduces them mod m_i and adds C'_i f_i to the 96-bit
-    // fraction sum of each element, kept in the CTA's scratch tile (high
-    // words Sh, low words Sl; column-major with the 128 rows contiguous, so a
-    // warp's accesses are coalesced).  The last modulus of a whole tile
-    // writes the FP64 result into Y instead.  Each warp arrives on the
-    // accumulator-empty barrier by itself (count 8).
+    // columns at a time, reduces them mod m_i and stores the 16 residues as
+    // one 16-byte word into the tile's plane i (a warp writes 512 contiguous
+    // bytes).  The last modulus of a whole tile instead reads the other
+    // planes' words of the same 16 elements back, forms the CRT fraction and
+    // writes Y.  Whole tiles use the CTA's own planes; tail tiles (split
+    // stream-K over CTAs) have planes of their own and are converted by
+    // k_oz_fixup.  Each warp arrives on the accumulator-empty barrier by
+    // itself (count 8).
     const int row = (warp & 3) * 32 + lane;
     const int chalf = warp >> 2;
     const uint64_t keep = l2_evict_last_policy();
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const int64_t ftile = (ntiles / gridDim.x) * gridDim.x;  // the first tail tile
     int g = 0;
     bool alive = true;
     OzIter it;
@@ -346,9 +364,9 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
     OzSeg sg;
     while (alive && oz_next_seg(it, sg)) {
       const int64_t row0 = 64 * (sg.t / ncol), col0 = (int64_t)OZ_BN * (sg.t % ncol);
-      const int64_t sbase = ((int64_t)blockIdx.x * 3 + (sg.slot < 0 ? 2 : sg.slot)) * OZ_S_ELEMS + row;
-      unsigned long long *Sht = Sh + sbase;
-      unsigned *Slt = Sl + sbase;
+      const bool tail = sg.t >= ftile;
+      const int64_t rt = tail ? (int64_t)gridDim.x + (sg.t - ftile) : (int64_t)blockIdx.x;
+      uint4 *Rt = reinterpret_cast<uint4 *>(Rres + rt * OZ_RES_TILE) + row;
       const int64_t gr = row0 + (row & 63);
       const bool row_ok = gr < M;
       const double rsc = row_ok ? rs[gr] * sc.cscale : 0.0;
@@ -356,10 +374,8 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
       const int cc0 = chalf * (OZ_BN / 32);
       const int cc1 = (int)min((int64_t)(cc0 + OZ_BN / 32), (Rv - col0 + 15) / 16);
       for (int i = sg.p0; i < sg.p1; i++) {
-        const bool first = i == sg.p0;
-        const bool fin = sg.slot < 0 && i + 1 == sg.p1;
+        const bool fin = !tail && i + 1 == sc.n;
         const unsigned gm = (unsigned)sc.mod[i], gmul = sc.mmul[i], goff = sc.moff[i];
-        const unsigned long long gfr = sc.frac[i], gfl = sc.fraclo[i];
         // warp-uniform outcome: the loads below are warp-collective
         const bool got = mbar_wait(accf0 + 8 * (g & 1), (uint32_t)(g >> 1) & 1u, err, abort_flag);
         if (!__all_sync(0xffffffffu, got)) {
@@ -369,13 +385,6 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tacc = tmem_d + (uint32_t)((g & 1) * OZ_BN) + lane_base;
         for (int cc = cc0; cc < cc1; cc++) {
-          unsigned long long oh[16];
-          unsigned ol[16];
-#pragma unroll
-          for (int q = 0; q < 16; q++) {
-            oh[q] = first ? 0ull : ld_keep(Sht + (int64_t)(cc * 16 + q) * 128, keep);
-            ol[q] = first ? 0u : ld_keep(Slt + (int64_t)(cc * 16 + q) * 128, keep);
-          }
           uint32_t v[16];
           asm volatile(
               "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -384,19 +393,27 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
                 "=r"(v[15])
               : "r"(tacc + (uint32_t)(cc * 16)));
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          unsigned w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-          for (int q = 0; q < 16; q++) {
-            const int c = cc * 16 + q;
-            const unsigned long long u = oz_mod((int)v[q], gm, gmul, goff);
-            const unsigned long long tl = (unsigned long long)ol[q] + u * gfl;
-            const unsigned long long th = oh[q] + u * gfr + (tl >> 32);
-            if (fin) {
-              if (row_ok && col0 + c < Rv)
-                reinterpret_cast<double *>(Y)[2 * ((col0 + c) * ldy + gr) + (row >> 6)] =
-                    fma((double)(unsigned)tl, 0x1p-32, (double)(long long)th) * rsc * cs[col0 + c];
-            } else {
-              st_keep(Sht + (int64_t)c * 128, th, keep);
-              st_keep(Slt + (int64_t)c * 128, (unsigned)tl, keep);
+          for (int q = 0; q < 16; q++) w[q >> 2] |= oz_mod((int)v[q], gm, gmul, goff) << (8 * (q & 3));
+          if (!fin) {
+            st_keep4(Rt + i * (OZ_RES_PLANE / 16) + cc * 128, make_uint4(w[0], w[1], w[2], w[3]), keep);
+            continue;
+          }
+          unsigned long long th[16], tl[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) th[q] = tl[q] = 0ull;
+          for (int j = 0; j < i; j++)
+            oz_frac_add(ld_keep4(Rt + j * (OZ_RES_PLANE / 16) + cc * 128, keep), sc.frac[j], sc.fraclo[j], th, tl);
+          oz_frac_add(make_uint4(w[0], w[1], w[2], w[3]), sc.frac[i], sc.fraclo[i], th, tl);
+          if (row_ok) {
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+              const int64_t c = col0 + cc * 16 + q;
+              const unsigned long long hi = th[q] + (tl[q] >> 32);
+              if (c < Rv)
+                reinterpret_cast<double *>(Y)[2 * (c * ldy + gr) + (row >> 6)] =
+                    fma((double)(unsigned)tl[q], 0x1p-32, (double)(long long)hi) * rsc * cs[c];
             }
           }
         }
@@ -494,43 +511,53 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * OZ_BN) : "memory");
 }
 
-// Tail tiles made of partial segments: tile fix[3 i] = the sum, in listed
-// order, of workspace slots fix[3 j + 2] (= 2 CTA + slot) for the entries j of
-// its run (fix[3 i + 1] = run length, given on the run's first entry)
-// (residues: the partial fraction sums of a tile sit in the scratch tiles of
-// the CTAs that computed them, high and low words, rows 0-63 real and 64-127
-// imaginary parts; they are added mod 2^96 and converted with the scales)
-template <bool CRT>
+// Tail tiles made of partial segments (slice scheme): tile fix[3 i] = the
+// sum, in listed order, of workspace slots fix[3 j + 2] (= 2 CTA + slot) for
+// the entries j of its run (fix[3 i + 1] = run length, given on the run's
+// first entry)
 __global__ void k_oz_fixup(const int64_t *__restrict__ fix, const int *__restrict__ runs, int ncol, int64_t M,
-                           int64_t Rv, double2 *__restrict__ Y, const double2 *__restrict__ P, int64_t ldy,
-                           const double *__restrict__ rs, const double *__restrict__ cs, double cscale,
-                           const unsigned long long *__restrict__ Sh, const unsigned *__restrict__ Sl) {
+                           int64_t Rv, double2 *__restrict__ Y, const double2 *__restrict__ P, int64_t ldy) {
   const int j0 = runs[blockIdx.x];
   const int64_t t = fix[3 * j0], len = fix[3 * j0 + 1];
   const int64_t row0 = 64 * (t / ncol), col0 = (int64_t)OZ_BN * (t % ncol);
   for (int e = threadIdx.x; e < OZ_TILE_ELEMS; e += blockDim.x) {
     const int64_t r = row0 + (e & 63), c = col0 + (e >> 6);
     if (r >= M || c >= Rv) continue;
-    if constexpr (CRT) {
-      // slot s = 2 CTA + k: scratch tile 3 CTA + k
-      unsigned long long hr = 0, hi = 0, lr = 0, li = 0;
-      for (int64_t j = 0; j < len; j++) {
-        const int64_t sl = fix[3 * (j0 + j) + 2];
-        const int64_t o = ((sl >> 1) * 3 + (sl & 1)) * OZ_S_ELEMS + (e >> 6) * 128 + (e & 63);
-        hr += Sh[o];
-        hi += Sh[o + 64];
-        lr += Sl[o];
-        li += Sl[o + 64];
-      }
-      hr += lr >> 32;
-      hi += li >> 32;
-      const double w = rs[r] * cs[c] * cscale;
-      Y[c * ldy + r] = make_double2(fma((double)(unsigned)lr, 0x1p-32, (double)(long long)hr) * w,
-                                    fma((double)(unsigned)li, 0x1p-32, (double)(long long)hi) * w);
-    } else {
-      double2 acc = make_double2(0, 0);
-      for (int64_t j = 0; j < len; j++) acc = cadd(acc, P[fix[3 * (j0 + j) + 2] * OZ_TILE_ELEMS + e]);
-      Y[c * ldy + r] = acc;
+    double2 acc = make_double2(0, 0);
+    for (int64_t j = 0; j < len; j++) acc = cadd(acc, P[fix[3 * (j0 + j) + 2] * OZ_TILE_ELEMS + e]);
+    Y[c * ldy + r] = acc;
+  }
+}
+
+// Tail tiles of the residue scheme (tile ftile + blockIdx.x): every modulus
+// was drained into the tile's own residue planes, by whichever CTAs computed
+// it; each element's residues are read back and converted to FP64 as the
+// last drain of a whole tile does (the same integer sum, so the same bits)
+__global__ void __launch_bounds__(256) k_oz_crt_tail(const __grid_constant__ OzSched sc, int ncol, int64_t M,
+                                                     int64_t Rv, int64_t ftile, int G, double2 *__restrict__ Y,
+                                                     int64_t ldy, const double *__restrict__ rs,
+                                                     const double *__restrict__ cs,
+                                                     const unsigned char *__restrict__ Rres) {
+  const int64_t t = ftile + blockIdx.x;
+  const int64_t row0 = 64 * (t / ncol), col0 = (int64_t)OZ_BN * (t % ncol);
+  const uint4 *Rt = reinterpret_cast<const uint4 *>(Rres + ((int64_t)G + blockIdx.x) * OZ_RES_TILE);
+  for (int e = threadIdx.x; e < 128 * (OZ_BN / 16); e += blockDim.x) {
+    const int row = e & 127, cc = e >> 7;  // consecutive threads: consecutive rows
+    const int64_t gr = row0 + (row & 63);
+    if (gr >= M || col0 + cc * 16 >= Rv) continue;
+    unsigned long long th[16], tl[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) th[q] = tl[q] = 0ull;
+    for (int j = 0; j < sc.n; j++)
+      oz_frac_add(Rt[j * (OZ_RES_PLANE / 16) + cc * 128 + row], sc.frac[j], sc.fraclo[j], th, tl);
+    const double rsc = rs[gr] * sc.cscale;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int64_t c = col0 + cc * 16 + q;
+      const unsigned long long hi = th[q] + (tl[q] >> 32);
+      if (c < Rv)
+        reinterpret_cast<double *>(Y)[2 * (c * ldy + gr) + (row >> 6)] =
+            fma((double)(unsigned)tl[q], 0x1p-32, (double)(long long)hi) * rsc * cs[c];
     }
   }
 }
@@ -792,7 +819,7 @@ int64_t round_up(int64_t v, int64_t m) { return ((v + m - 1) / m) * m; }
 unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 struct OzState {
-  DevBuf A, B, rs, cs, err, P, fix, runs, Sh, Sl;
+  DevBuf A, B, rs, cs, err, P, fix, runs, Rres;
   CUtensorMap mapA, mapB;
   uint64_t a_version = ~0ull;
   int64_t a_n = -1, b_key = -1, b_n = -1;
@@ -930,61 +957,59 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
     }
   }
   sc.n = n;
-  // persistent grid: data-parallel full waves, stream-K tail (k_oz_gemm);
-  // the host replays the tail split to list each partial tile's slots
+  // persistent grid: data-parallel full waves, stream-K tail (k_oz_gemm)
   const int ncol = (int)(Rpad / OZ_BN);
   const int64_t ntiles = (Mpad / 64) * ncol;
   const int64_t G = std::min<int64_t>(ntiles, std::max(1, c->sm_count));
   const int64_t F = (ntiles / G) * G, Wt = (ntiles - F) * n;
-  std::vector<int64_t> fix;  // (tile, run length, 2 CTA + slot) in tile order, then CTA order
-  for (int64_t b = 0; b < G; b++) {
-    int64_t u = F * n + Wt * b / G;
-    const int64_t u_end = F * n + Wt * (b + 1) / G;
-    int slot = 0;
-    while (u < u_end) {
-      const int64_t t = u / n;
-      const int64_t p0 = u - t * n, p1 = std::min<int64_t>(n, u_end - t * n);
-      u = t * n + p1;
-      if (!(p0 == 0 && p1 == n)) fix.insert(fix.end(), {t, 0, 2 * b + slot++});
-    }
-  }
-  std::vector<int> runs;
-  for (size_t j = 0; j < fix.size() / 3; j++) {
-    if (j == 0 || fix[3 * j] != fix[3 * (j - 1)]) runs.push_back((int)j);
-    fix[3 * runs.back() + 1]++;
-  }
-  if (!fix.empty()) {
-    st.fix.ensure(sizeof(int64_t) * fix.size());
-    st.runs.ensure(sizeof(int) * runs.size());
-    DMB_CUDA(cudaMemcpyAsync(st.fix.p, fix.data(), sizeof(int64_t) * fix.size(), cudaMemcpyHostToDevice, c->stream));
-    DMB_CUDA(cudaMemcpyAsync(st.runs.p, runs.data(), sizeof(int) * runs.size(), cudaMemcpyHostToDevice, c->stream));
-  }
-  // residues: fraction sums in three scratch tiles per CTA (two partial-
-  // segment slots and the whole-tile accumulator), high and low words
   if (crt) {
-    st.Sh.ensure(sizeof(unsigned long long) * G * 3 * OZ_S_ELEMS);
-    st.Sl.ensure(sizeof(unsigned) * G * 3 * OZ_S_ELEMS);
-  }
-  if (!fix.empty() && !crt) st.P.ensure(sizeof(double2) * G * 2 * OZ_TILE_ELEMS);
-  kt_begin(c);
-  double2 *Pw = fix.empty() || crt ? Y : st.P.as<double2>();
-  if (crt)
+    // residue planes: one tile's worth per CTA (its whole tiles, one at a
+    // time) and one per tail tile (its moduli drained by several CTAs,
+    // converted by k_oz_crt_tail)
+    st.Rres.ensure((size_t)(G + ntiles - F) * OZ_RES_TILE);
+    kt_begin(c);
     DMB_LAUNCH(c, k_oz_gemm<true>, (unsigned)G, oz_threads<true>(), OZ_SMEM, st.mapA, st.mapB, sc,
-               (int)(ld / OZ_BK), N, R, Y, Pw, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
-               st.Sh.as<unsigned long long>(), st.Sl.as<unsigned>(), st.err.as<unsigned>());
-  else
+               (int)(ld / OZ_BK), N, R, Y, Y, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
+               st.Rres.as<unsigned char>(), st.err.as<unsigned>());
+    if (ntiles > F)
+      DMB_LAUNCH(c, k_oz_crt_tail, (unsigned)(ntiles - F), 256, 0, sc, ncol, N, R, F, (int)G, Y, N,
+                 st.rs.as<double>(), st.cs.as<double>(), st.Rres.as<unsigned char>());
+  } else {
+    // the host replays the tail split to list each partial tile's slots
+    std::vector<int64_t> fix;  // (tile, run length, 2 CTA + slot) in tile order, then CTA order
+    for (int64_t b = 0; b < G; b++) {
+      int64_t u = F * n + Wt * b / G;
+      const int64_t u_end = F * n + Wt * (b + 1) / G;
+      int slot = 0;
+      while (u < u_end) {
+        const int64_t t = u / n;
+        const int64_t p0 = u - t * n, p1 = std::min<int64_t>(n, u_end - t * n);
+        u = t * n + p1;
+        if (!(p0 == 0 && p1 == n)) fix.insert(fix.end(), {t, 0, 2 * b + slot++});
+      }
+    }
+    std::vector<int> runs;
+    for (size_t j = 0; j < fix.size() / 3; j++) {
+      if (j == 0 || fix[3 * j] != fix[3 * (j - 1)]) runs.push_back((int)j);
+      fix[3 * runs.back() + 1]++;
+    }
+    if (!fix.empty()) {
+      st.fix.ensure(sizeof(int64_t) * fix.size());
+      st.runs.ensure(sizeof(int) * runs.size());
+      DMB_CUDA(cudaMemcpyAsync(st.fix.p, fix.data(), sizeof(int64_t) * fix.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+      DMB_CUDA(cudaMemcpyAsync(st.runs.p, runs.data(), sizeof(int) * runs.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+      st.P.ensure(sizeof(double2) * G * 2 * OZ_TILE_ELEMS);
+    }
+    kt_begin(c);
+    double2 *Pw = fix.empty() ? Y : st.P.as<double2>();
     DMB_LAUNCH(c, k_oz_gemm<false>, (unsigned)G, oz_threads<false>(), OZ_SMEM, st.mapA, st.mapB, sc,
                (int)(ld / OZ_BK), N, R, Y, Pw, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
-               (unsigned long long *)nullptr, (unsigned *)nullptr, st.err.as<unsigned>());
-  if (!runs.empty()) {
-    if (crt)
-      DMB_LAUNCH(c, k_oz_fixup<true>, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(), ncol,
-                 N, R, Y, Pw, N, st.rs.as<double>(), st.cs.as<double>(), sc.cscale,
-                 st.Sh.as<unsigned long long>(), st.Sl.as<unsigned>());
-    else
-      DMB_LAUNCH(c, k_oz_fixup<false>, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(),
-                 ncol, N, R, Y, st.P.as<double2>(), N, st.rs.as<double>(), st.cs.as<double>(), sc.cscale,
-                 (const unsigned long long *)nullptr, (const unsigned *)nullptr);
+               (unsigned char *)nullptr, st.err.as<unsigned>());
+    if (!runs.empty())
+      DMB_LAUNCH(c, k_oz_fixup, (unsigned)runs.size(), 256, 0, st.fix.as<int64_t>(), st.runs.as<int>(), ncol, N, R,
+                 Y, st.P.as<double2>(), N);
   }
   // int8 work: every product is a real (2N x 2N) x (2N x R) product
   kt_end(c, 2.0 * n * (2.0 * N) * (2.0 * N) * (double)R, 1);
@@ -1004,7 +1029,7 @@ void oz_release(dmb_ctx *c) {
   for (size_t i = 0; i < g_oz_states.size(); i++) {
     if (g_oz_states[i].first != c) continue;
     OzState *st = g_oz_states[i].second;
-    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err, &st->P, &st->fix, &st->runs, &st->Sh, &st->Sl}) b->release();
+    for (DevBuf *b : {&st->A, &st->B, &st->rs, &st->cs, &st->err, &st->P, &st->fix, &st->runs, &st->Rres}) b->release();
     delete st;
     g_oz_states.erase(g_oz_states.begin() + i);
     return;
