@@ -71,7 +71,7 @@ SEED = 20260001
 METRIC = "EFIE solves/s (assemble+GMRES to 1e-6) mixed/learned vs plain FP64, 1 B200"
 # DRAM bytes per k_oz_gemm launch (13 residue products, R = 1,024) on the
 # headline plate, measured with ncu one-pass dram__bytes_read/write.sum
-OZ_TRAFFIC_PER_LAUNCH = 16105352192  # mean of the step's two launches: 12.919 + 3.186 GB
+OZ_TRAFFIC_PER_LAUNCH = 12300295168  # mean of the step's two launches: 11.900 + 0.400 GB
 WORKLOAD = "pec_plate_0.3m_3GHz_60x60_10680rwg_1024planewaves_monostatic"
 
 
