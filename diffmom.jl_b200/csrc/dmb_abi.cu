@@ -181,6 +181,11 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       c->tune_pin[option == DMB_OPT_TUNE_TC_GEMM ? dmb::TUNE_TC_GEMM_BN : dmb::TUNE_TC_SYRK_STAGES] = value;
       return;
     }
+    if (option == DMB_OPT_TUNE_INT8_TILE) {
+      DMB_REQUIRE(value >= 0 && value <= 2, DMB_ERR_ARGUMENT, "int8 tile pin must be 0 (tuned), 1 or 2");
+      c->tune_pin[dmb::TUNE_OZ_TILE] = value;
+      return;
+    }
     if (option == DMB_OPT_OPERATOR) {
       DMB_REQUIRE(value == 0 || value == 1, DMB_ERR_ARGUMENT, "operator must be 0 (dense Z) or 1 (H-matrix)");
       DMB_REQUIRE(value == 0 ? c->z_valid : c->aca.valid, DMB_ERR_STATE,

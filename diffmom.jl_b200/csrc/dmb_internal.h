@@ -145,7 +145,7 @@ struct AcaState {
 
 namespace dmb {
 // families of the online autotuner (dmb_tune.cu)
-enum TuneFamily { TUNE_TC_GEMM_BN = 0, TUNE_TC_SYRK_STAGES = 1, TUNE_FAMILIES = 2 };
+enum TuneFamily { TUNE_TC_GEMM_BN = 0, TUNE_TC_SYRK_STAGES = 1, TUNE_OZ_TILE = 2, TUNE_FAMILIES = 3 };
 struct TuneMark {
   bool active = false;
   int family = 0, cand = 0;
@@ -284,7 +284,7 @@ struct dmb_ctx {
   bool pc_bf16() const { return precond_bf16 > 0 || (precond_bf16 < 0 && pc_bf16_scope); }
   int far_tile_used = 0;         // tile width of the last assembly
   // autotuner pins per family (0: tuned, k: candidate k - 1)
-  int tune_pin[dmb::TUNE_FAMILIES] = {0, 0};
+  int tune_pin[dmb::TUNE_FAMILIES] = {0, 0, 0};
   uint64_t z_version = 0;        // bumped whenever Z changes (packed operand caches key on it)
   uint64_t f_version = 0;        // bumped by every LDL^T factorisation
   uint64_t f_packed = ~0ull;     // factor version packed for the batched triangular solves

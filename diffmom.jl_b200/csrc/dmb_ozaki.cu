@@ -60,7 +60,7 @@
 //                     (tcgen05.ld, reduce mod m_i, one byte per element into
 //                     the tile's residue planes; the last modulus of a tile
 //                     reads the other residues back and converts to FP64).
-// Every wait is bounded (error bit, abort flag, TMEM freed); no multicast.
+// Every wait is bounded (error bit, abort flag, TMEM freed); every TMA load fills one CTA.
 #include <algorithm>
 #include <vector>
 #include <cmath>
@@ -511,6 +511,305 @@ __global__ void __launch_bounds__(oz_threads<CRT>(), 1) k_oz_gemm(const __grid_c
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * OZ_BN) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Residue scheme on CTA pairs (tcgen05 cta_group::2): a cluster of two CTAs
+// on one TPC computes a 128 x 256 complex tile (256 real-stacked rows) as one
+// M = 256, N = 256 int8 MMA per K step, issued by the even CTA.  Each CTA
+// loads its own 128 A rows and half of the 256 B rows (plain TMA tile loads
+// into its own shared memory, both completing on the even CTA's full
+// barrier), so per int8 MAC an SM reads a third less operand data than with
+// the one-SM 128 x 256 tile.  The accumulator rows of each CTA sit in its own
+// TMEM (rows 0-127 even, 128-255 odd CTA, all 256 columns), so each CTA
+// drains its 64 complex rows exactly as k_oz_gemm does (residue planes, CRT
+// at the last modulus).  The MMA's commits arrive on the barriers of both
+// CTAs (one commit, two-CTA mask); the odd CTA's drain warps arrive on the
+// even CTA's accumulator-empty barrier.  Every wait is bounded (error bit 8,
+// per-CTA abort flag, TMEM freed).  Measured on the headline product it runs
+// at the same tensor-pipe activity as the one-SM tile (68 %) and is not
+// faster (4.7-4.8 vs 4.25 ms): the launch is bound by the int8 MMA issue
+// under the power cap, not by the operand feed; the autotuner keeps it as a
+// candidate.
+constexpr int OZP_STAGES = 6;
+constexpr int OZP_A_STAGE = 128 * OZ_BK, OZP_B_STAGE = 128 * OZ_BK;  // per CTA
+constexpr int OZP_SMEM = OZP_STAGES * (OZP_A_STAGE + OZP_B_STAGE) + 256 /*barriers*/ + 1024 /*align*/;
+// D s32, A/B signed int8, K-major, N = 256, M = 256 (the pair)
+constexpr uint32_t OZP_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                               ((uint32_t)(256 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the even CTA's copy of a local shared address
+__device__ __forceinline__ uint32_t to_even_cta(uint32_t saddr) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(0u));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// TMA tile load into this CTA's shared memory, completing on an mbarrier of
+// either CTA of the pair
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                                 uint32_t bar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+      : "memory");
+}
+__device__ __forceinline__ void umma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(OZP_IDESC), "r"(accumulate)
+      : "memory");
+}
+// arrive (once per CTA) on the barrier at this offset in both CTAs of the
+// pair when the MMAs issued so far have completed
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+      "h"((unsigned short)3)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+// bounded wait with cluster-scope acquire (arrivals from the other CTA)
+__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity, unsigned *err,
+                                                  volatile int *abort) {
+  for (long long it = 0; it < TC_WAIT_LIMIT; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 1023) == 1023 && *abort) return false;
+  }
+  atomicOr(err, 8u);
+  *abort = 1;
+  return false;
+}
+
+// work of cluster b of G over npairs pair tiles: whole pair tiles in
+// data-parallel waves, the tail split stream-K as in k_oz_gemm
+__device__ __forceinline__ void oz_iter_init_pair(OzIter &it, int64_t npairs, int n) {
+  it.G = gridDim.x / 2;
+  it.b = blockIdx.x / 2;
+  it.n = n;
+  it.wave = 0;
+  it.nfull = npairs / it.G;
+  const int64_t F = it.nfull * it.G, Wt = (npairs - F) * n;
+  it.u = F * n + Wt * it.b / it.G;
+  it.u_end = F * n + Wt * (it.b + 1) / it.G;
+  it.slot = 0;
+}
+
+__global__ void __launch_bounds__(320, 1) k_oz_pair(const __grid_constant__ CUtensorMap tmA,
+                                                    const __grid_constant__ CUtensorMap tmB,
+                                                    const __grid_constant__ OzSched sc, int kchunks, int64_t M,
+                                                    int64_t Rv, double2 *__restrict__ Y, int64_t ldy, int ncol,
+                                                    int64_t npairs, const double *__restrict__ rs,
+                                                    const double *__restrict__ cs, unsigned char *__restrict__ Rres,
+                                                    unsigned *err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char *gbase = smem_raw + (base - raw);
+  const uint32_t sA = base;
+  const uint32_t sB = base + OZP_STAGES * OZP_A_STAGE;
+  const uint32_t sBar = sB + OZP_STAGES * OZP_B_STAGE;
+  uint64_t *bar_ptr = reinterpret_cast<uint64_t *>(gbase + (sBar - base));
+  volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bar_ptr + 20);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(bar_ptr + 21);
+  // full[s] (even CTA: both CTAs' loads), empty[s] (each CTA: its stage
+  // consumed), accf[b] (each CTA: accumulator b full), acce[b] (even CTA:
+  // accumulator b drained by both CTAs, 16 warp arrivals)
+  const uint32_t full0 = sBar, empty0 = sBar + 8 * OZP_STAGES, accf0 = sBar + 16 * OZP_STAGES, acce0 = accf0 + 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < OZP_STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(accf0 + 8 * b, 1);
+      mbar_init(acce0 + 8 * b, 16);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(const_cast<uint32_t *>(tmem_slot))),
+                 "r"(2 * OZ_BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  // both CTAs' barriers initialised and TMEM allocated before any use
+  cluster_sync_all();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = *tmem_slot;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      const uint32_t full_even = to_even_cta(full0);
+      long long t = 0;
+      OzIter it;
+      oz_iter_init_pair(it, npairs, sc.n);
+      OzSeg sg;
+      bool go = true;
+      while (go && oz_next_seg(it, sg)) {
+        // this CTA's 128 A rows and 128 B rows of the pair tile
+        const int arow = (int)(256 * (sg.t / ncol) + 128 * rank);
+        const int brow = (int)(OZ_BN * (sg.t % ncol) + 128 * rank);
+        for (int i = sg.p0; i < sg.p1 && go; i++) {
+          for (int kc = 0; kc < kchunks; kc++, t++) {
+            const int s = (int)(t % OZP_STAGES);
+            if (*abort_flag || (t >= OZP_STAGES && !mbar_wait(empty0 + 8 * s, (uint32_t)((t / OZP_STAGES) - 1) & 1u,
+                                                              err, abort_flag))) {
+              go = false;
+              break;
+            }
+            if (rank == 0) mbar_expect_tx(full0 + 8 * s, 2 * (OZP_A_STAGE + OZP_B_STAGE));
+            tma_load_2d_pair(sA + s * OZP_A_STAGE, &tmA, kc * OZ_BK, sc.arow[i] + arow, full_even + 8 * s);
+            tma_load_2d_pair(sB + s * OZP_B_STAGE, &tmB, kc * OZ_BK, sc.brow[i] + brow, full_even + 8 * s);
+          }
+        }
+      }
+    }
+  } else if (warp == 9) {
+    if (lane == 0 && rank == 0) {
+      long long t = 0;
+      int g = 0;
+      bool ok = true;
+      OzIter it;
+      oz_iter_init_pair(it, npairs, sc.n);
+      OzSeg sg;
+      while (ok && oz_next_seg(it, sg)) {
+        for (int i = sg.p0; i < sg.p1 && ok; i++) {
+          // modulus g accumulates in buffer g & 1, free once modulus g - 2 is
+          // drained by both CTAs
+          if (g >= 2 && !mbar_wait_cluster(acce0 + 8 * (g & 1), (uint32_t)((g >> 1) - 1) & 1u, err, abort_flag)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t tmem_acc = tmem_d + (uint32_t)((g & 1) * OZ_BN);
+          for (int kc = 0; kc < kchunks; kc++, t++) {
+            const int s = (int)(t % OZP_STAGES);
+            if (!mbar_wait(full0 + 8 * s, (uint32_t)(t / OZP_STAGES) & 1u, err, abort_flag)) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int k = 0; k < OZ_BK / 32; k++) {
+              const uint64_t ad = sw128_desc(sA + s * OZP_A_STAGE + k * 32);
+              const uint64_t bd = sw128_desc(sB + s * OZP_B_STAGE + k * 32);
+              umma_i8_pair(tmem_acc, ad, bd, (kc == 0 && k == 0) ? 0u : 1u);
+            }
+            umma_commit_pair(empty0 + 8 * s);
+          }
+          if (ok) umma_commit_pair(accf0 + 8 * (g & 1));
+          g++;
+        }
+      }
+    }
+  } else {
+    // residue drains of this CTA's 64 complex rows (as in k_oz_gemm)
+    const int row = (warp & 3) * 32 + lane;
+    const int chalf = warp >> 2;
+    const uint64_t keep = l2_evict_last_policy();
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const uint32_t acce_even = to_even_cta(acce0);
+    const int64_t G2 = gridDim.x / 2;
+    const int64_t fpair = (npairs / G2) * G2;  // the first tail pair tile
+    int g = 0;
+    bool alive = true;
+    OzIter it;
+    oz_iter_init_pair(it, npairs, sc.n);
+    OzSeg sg;
+    while (alive && oz_next_seg(it, sg)) {
+      const int64_t prow = sg.t / ncol;
+      const int64_t row0 = 128 * prow + 64 * rank, col0 = (int64_t)OZ_BN * (sg.t % ncol);
+      const bool tail = sg.t >= fpair;
+      const int64_t rt = tail ? 2 * G2 + 2 * (sg.t - fpair) + rank : (int64_t)blockIdx.x;
+      uint4 *Rt = reinterpret_cast<uint4 *>(Rres + rt * OZ_RES_TILE) + row;
+      const int64_t gr = row0 + (row & 63);
+      const bool row_ok = gr < M;
+      const double rsc = row_ok ? rs[gr] * sc.cscale : 0.0;
+      const int cc0 = chalf * (OZ_BN / 32);
+      const int cc1 = (int)min((int64_t)(cc0 + OZ_BN / 32), (Rv - col0 + 15) / 16);
+      for (int i = sg.p0; i < sg.p1; i++) {
+        const bool fin = !tail && i + 1 == sc.n;
+        const unsigned gm = (unsigned)sc.mod[i], gmul = sc.mmul[i], goff = sc.moff[i];
+        const bool got = mbar_wait(accf0 + 8 * (g & 1), (uint32_t)(g >> 1) & 1u, err, abort_flag);
+        if (!__all_sync(0xffffffffu, got)) {
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tacc = tmem_d + (uint32_t)((g & 1) * OZ_BN) + lane_base;
+        for (int cc = cc0; cc < cc1; cc++) {
+          uint32_t v[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15])
+              : "r"(tacc + (uint32_t)(cc * 16)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          unsigned w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+          for (int q = 0; q < 16; q++) w[q >> 2] |= oz_mod((int)v[q], gm, gmul, goff) << (8 * (q & 3));
+          if (!fin) {
+            st_keep4(Rt + i * (OZ_RES_PLANE / 16) + cc * 128, make_uint4(w[0], w[1], w[2], w[3]), keep);
+            continue;
+          }
+          unsigned long long th[16], tl[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) th[q] = tl[q] = 0ull;
+          for (int j = 0; j < i; j++)
+            oz_frac_add(ld_keep4(Rt + j * (OZ_RES_PLANE / 16) + cc * 128, keep), sc.frac[j], sc.fraclo[j], th, tl);
+          oz_frac_add(make_uint4(w[0], w[1], w[2], w[3]), sc.frac[i], sc.fraclo[i], th, tl);
+          if (row_ok) {
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+              const int64_t c = col0 + cc * 16 + q;
+              const unsigned long long hi = th[q] + (tl[q] >> 32);
+              if (c < Rv)
+                reinterpret_cast<double *>(Y)[2 * (c * ldy + gr) + (row >> 6)] =
+                    fma((double)(unsigned)tl[q], 0x1p-32, (double)(long long)hi) * rsc * cs[c];
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(acce_even + 8 * (g & 1));
+        g++;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  // neither CTA frees TMEM or exits while the other may still use its
+  // barriers or the MMA may still write its accumulators
+  cluster_sync_all();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(2 * OZ_BN) : "memory");
+}
+
 // Tail tiles made of partial segments (slice scheme): tile fix[3 i] = the
 // sum, in listed order, of workspace slots fix[3 j + 2] (= 2 CTA + slot) for
 // the entries j of its run (fix[3 i + 1] = run length, given on the run's
@@ -529,17 +828,20 @@ __global__ void k_oz_fixup(const int64_t *__restrict__ fix, const int *__restric
   }
 }
 
-// Tail tiles of the residue scheme (tile ftile + blockIdx.x): every modulus
-// was drained into the tile's own residue planes, by whichever CTAs computed
-// it; each element's residues are read back and converted to FP64 as the
-// last drain of a whole tile does (the same integer sum, so the same bits)
+// Tail tiles of the residue scheme: every modulus was drained into the
+// tile's own residue planes (G + blockIdx.x), by whichever CTAs computed it;
+// each element's residues are read back and converted to FP64 as the last
+// drain of a whole tile does (the same integer sum, so the same bits).  One
+// CTA per 64 x 256 tile: tile ftile + blockIdx.x of k_oz_gemm, or (pair)
+// half blockIdx.x & 1 of pair tile ftile + blockIdx.x / 2 of k_oz_pair.
 __global__ void __launch_bounds__(256) k_oz_crt_tail(const __grid_constant__ OzSched sc, int ncol, int64_t M,
-                                                     int64_t Rv, int64_t ftile, int G, double2 *__restrict__ Y,
-                                                     int64_t ldy, const double *__restrict__ rs,
-                                                     const double *__restrict__ cs,
+                                                     int64_t Rv, int64_t ftile, int G, int pair,
+                                                     double2 *__restrict__ Y, int64_t ldy,
+                                                     const double *__restrict__ rs, const double *__restrict__ cs,
                                                      const unsigned char *__restrict__ Rres) {
-  const int64_t t = ftile + blockIdx.x;
-  const int64_t row0 = 64 * (t / ncol), col0 = (int64_t)OZ_BN * (t % ncol);
+  const int64_t t = pair ? ftile + blockIdx.x / 2 : ftile + blockIdx.x;
+  const int64_t row0 = pair ? 128 * (t / ncol) + 64 * (blockIdx.x & 1) : 64 * (t / ncol);
+  const int64_t col0 = (int64_t)OZ_BN * (t % ncol);
   const uint4 *Rt = reinterpret_cast<const uint4 *>(Rres + ((int64_t)G + blockIdx.x) * OZ_RES_TILE);
   for (int e = threadIdx.x; e < 128 * (OZ_BN / 16); e += blockDim.x) {
     const int row = e & 127, cc = e >> 7;  // consecutive threads: consecutive rows
@@ -820,12 +1122,12 @@ unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 struct OzState {
   DevBuf A, B, rs, cs, err, P, fix, runs, Rres;
-  CUtensorMap mapA, mapB;
+  CUtensorMap mapA, mapB, mapB128;
   uint64_t a_version = ~0ull;
   int64_t a_n = -1, b_key = -1, b_n = -1;
   int a_scheme = -1, b_scheme = -1;
   int crt_a = 0;  // residues: the Z exponent a of the current planes
-  bool attr = false;
+  bool attr = false, pair_attr = false;
 };
 
 std::mutex g_oz_mu;
@@ -857,7 +1159,7 @@ bool oz_available(dmb_ctx *c) {
 void oz_prepare(dmb_ctx *c) {
   DMB_REQUIRE(oz_available(c), DMB_ERR_STATE, "int8 tensor-core product unavailable for this matrix");
   OzState &st = oz_state(c);
-  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64);
+  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 128);
   const int64_t ld = 2 * Kh;
   const bool crt = c->int8_scheme == 0;
   const int planes = crt ? OZ_NMOD : OZ_S;
@@ -895,7 +1197,7 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
   DMB_REQUIRE(lmax >= 0 && lmax <= OZ_LMAX, DMB_ERR_ARGUMENT, "int8 slice levels out of range");
   oz_prepare(c);
   OzState &st = oz_state(c);
-  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 64), Rpad = round_up(R, OZ_BN);
+  const int64_t N = c->n, Kh = round_up(N, OZ_BK), Mpad = round_up(N, 128), Rpad = round_up(R, OZ_BN);
   const int64_t ld = 2 * Kh;
   const bool crt = c->int8_scheme == 0;
   const int planes = crt ? OZ_NMOD : OZ_S;
@@ -904,6 +1206,8 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
   if (st.b_key != Rpad || st.b_n != N || st.b_scheme != c->int8_scheme) {
     make_map_bytes(&st.mapB, st.B.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, (uint64_t)ld, (uint64_t)ld,
                    (uint64_t)(planes * Rpad), OZ_BK, OZ_BN);
+    make_map_bytes(&st.mapB128, st.B.p, CU_TENSOR_MAP_DATA_TYPE_UINT8, (uint64_t)ld, (uint64_t)ld,
+                   (uint64_t)(planes * Rpad), OZ_BK, 128);
     st.b_key = Rpad;
     st.b_n = N;
     st.b_scheme = c->int8_scheme;
@@ -959,21 +1263,65 @@ void oz_zx(dmb_ctx *c, const double2 *X, double2 *Y, int64_t R, int lmax) {
   sc.n = n;
   // persistent grid: data-parallel full waves, stream-K tail (k_oz_gemm)
   const int ncol = (int)(Rpad / OZ_BN);
-  const int64_t ntiles = (Mpad / 64) * ncol;
+  const int64_t ntiles = (round_up(N, 64) / 64) * ncol;
   const int64_t G = std::min<int64_t>(ntiles, std::max(1, c->sm_count));
   const int64_t F = (ntiles / G) * G, Wt = (ntiles - F) * n;
   if (crt) {
-    // residue planes: one tile's worth per CTA (its whole tiles, one at a
-    // time) and one per tail tile (its moduli drained by several CTAs,
-    // converted by k_oz_crt_tail)
-    st.Rres.ensure((size_t)(G + ntiles - F) * OZ_RES_TILE);
-    kt_begin(c);
-    DMB_LAUNCH(c, k_oz_gemm<true>, (unsigned)G, oz_threads<true>(), OZ_SMEM, st.mapA, st.mapB, sc,
-               (int)(ld / OZ_BK), N, R, Y, Y, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
-               st.Rres.as<unsigned char>(), st.err.as<unsigned>());
-    if (ntiles > F)
-      DMB_LAUNCH(c, k_oz_crt_tail, (unsigned)(ntiles - F), 256, 0, sc, ncol, N, R, F, (int)G, Y, N,
-                 st.rs.as<double>(), st.cs.as<double>(), st.Rres.as<unsigned char>());
+    // tile shape from the autotuner, per (row tiles, column tiles): one-SM
+    // 64 x 256 complex tiles (k_oz_gemm) or CTA-pair 128 x 256 tiles
+    // (k_oz_pair); both give the same bits (integer sums)
+    const int64_t tb1 = dmb::tune_bucket(Mpad / 128), tb2 = ncol;
+    const int cand = dmb::tune_choose(c, dmb::TUNE_OZ_TILE, tb1, tb2, 2);
+    dmb::TuneMark mk;
+    if (cand == 1) {
+      // residue planes: as below, per CTA of the pairs and per half of a
+      // tail pair tile
+      const int64_t npairs = (Mpad / 128) * ncol;
+      const int64_t G2 = std::min<int64_t>(npairs, std::max(1, c->sm_count / 2));
+      const int64_t F2 = (npairs / G2) * G2;
+      st.Rres.ensure((size_t)(2 * G2 + 2 * (npairs - F2)) * OZ_RES_TILE);
+      if (!st.pair_attr) {
+        DMB_CUDA(cudaFuncSetAttribute(k_oz_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, OZP_SMEM));
+        st.pair_attr = true;
+      }
+      kt_begin(c);
+      dmb::tune_begin(c, dmb::TUNE_OZ_TILE, tb1, tb2, cand, mk);
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(2 * G2));
+      cfg.blockDim = dim3(320);
+      cfg.dynamicSmemBytes = OZP_SMEM;
+      cfg.stream = c->stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 2;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      DMB_CUDA(cudaLaunchKernelEx(&cfg, k_oz_pair, st.mapA, st.mapB128, sc, (int)(ld / OZ_BK), (int64_t)N,
+                                  (int64_t)R, Y, (int64_t)N, ncol, npairs, (const double *)st.rs.as<double>(),
+                                  (const double *)st.cs.as<double>(), st.Rres.as<unsigned char>(),
+                                  st.err.as<unsigned>()));
+      c->launches++;
+      dmb::tune_end(c, mk);
+      if (npairs > F2)
+        DMB_LAUNCH(c, k_oz_crt_tail, (unsigned)(2 * (npairs - F2)), 256, 0, sc, ncol, N, R, F2, (int)(2 * G2), 1, Y,
+                   N, st.rs.as<double>(), st.cs.as<double>(), st.Rres.as<unsigned char>());
+    } else {
+      // residue planes: one tile's worth per CTA (its whole tiles, one at a
+      // time) and one per tail tile (its moduli drained by several CTAs,
+      // converted by k_oz_crt_tail)
+      st.Rres.ensure((size_t)(G + ntiles - F) * OZ_RES_TILE);
+      kt_begin(c);
+      dmb::tune_begin(c, dmb::TUNE_OZ_TILE, tb1, tb2, cand, mk);
+      DMB_LAUNCH(c, k_oz_gemm<true>, (unsigned)G, oz_threads<true>(), OZ_SMEM, st.mapA, st.mapB, sc,
+                 (int)(ld / OZ_BK), N, R, Y, Y, N, ncol, ntiles, st.rs.as<double>(), st.cs.as<double>(),
+                 st.Rres.as<unsigned char>(), st.err.as<unsigned>());
+      dmb::tune_end(c, mk);
+      if (ntiles > F)
+        DMB_LAUNCH(c, k_oz_crt_tail, (unsigned)(ntiles - F), 256, 0, sc, ncol, N, R, F, (int)G, 0, Y, N,
+                   st.rs.as<double>(), st.cs.as<double>(), st.Rres.as<unsigned char>());
+    }
   } else {
     // the host replays the tail split to list each partial tile's slots
     std::vector<int64_t> fix;  // (tile, run length, 2 CTA + slot) in tile order, then CTA order

@@ -22,7 +22,7 @@
 //                     tcgen05.commit frees each stage and finally signals done;
 //   all 4 warps       tcgen05.ld the accumulator (warp w owns lanes 32w..),
 //                     stage through shared memory, C -= acc on c <= r.
-// No TMA multicast, no clusters.  Every mbarrier wait is bounded: on expiry
+// Each TMA load fills one CTA's shared memory; no clusters.  Every mbarrier wait is bounded: on expiry
 // the kernel records an error bit, stops issuing, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>

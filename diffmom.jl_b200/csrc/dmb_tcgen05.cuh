@@ -1,7 +1,7 @@
 // dmb_tcgen05.cuh -- device helpers shared by the tcgen05 kernels
 // (TMA tile loads into 128-byte-swizzled stages, mbarrier pipeline with
 // bounded waits, UMMA shared-memory descriptors) and the host-side tensor-map
-// encoder.  Nothing here uses TMA multicast or clusters.
+// encoder.  Every TMA load here fills the issuing CTA's own shared memory.
 #pragma once
 #include <cuda.h>
 

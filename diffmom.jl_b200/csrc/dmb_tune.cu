@@ -94,6 +94,7 @@ const char *family_name(int f) {
     case dmb::TUNE_TC_GEMM_BN: return "k_tc_gemm shape (256 / 128 complex columns per tile / persistent 256)";
     case dmb::TUNE_TC_SYRK_STAGES:
       return "k_tc_syrk schedule (4 stages, 1 CTA/SM / 2 stages, 2 CTAs/SM / persistent, lower tiles only)";
+    case dmb::TUNE_OZ_TILE: return "k_oz_gemm tile (one SM, 64 x 256 complex / CTA pair, 128 x 256 complex)";
     default: return "?";
   }
 }

@@ -54,6 +54,7 @@ OPT_TUNE_TC_GEMM = 10
 OPT_TUNE_TC_SYRK = 11
 OPT_PRECOND_BF16 = 12
 OPT_INT8_SCHEME = 13
+OPT_TUNE_INT8_TILE = 14
 
 
 class DiffMoMError(RuntimeError):

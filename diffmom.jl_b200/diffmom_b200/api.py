@@ -103,13 +103,15 @@ class EFIEDevice:
         packed sweeps always / never / inside the many-incidence resident
         solves only), "int8_scheme" (0 = default: the FP64-accurate Z X from
         int8 residues modulo 13 coprime moduli, recombined by the Chinese
-        remainder theorem; 1: from seven-bit fixed-point slices)."""
+        remainder theorem; 1: from seven-bit fixed-point slices),
+        "tune_int8_tile" (0 = autotuned; 1: one-SM 64 x 256 tiles; 2: CTA-pair
+        128 x 256 tiles of the residue-scheme int8 product)."""
         codes = {"tensor_cores": nat.OPT_TENSOR_CORES, "tc_min_rhs": nat.OPT_TC_MIN_RHS,
                  "far_tile": nat.OPT_FAR_TILE, "exact_krylov": nat.OPT_EXACT_KRYLOV,
                  "precond_tf32_terms": nat.OPT_PRECOND_TF32_TERMS, "gmres_graphs": nat.OPT_GMRES_GRAPHS,
                  "true_residual": nat.OPT_TRUE_RESIDUAL, "spin_limit": nat.OPT_SPIN_LIMIT,
                  "tune_tc_gemm": nat.OPT_TUNE_TC_GEMM, "tune_tc_syrk": nat.OPT_TUNE_TC_SYRK,
-                 "int8_scheme": nat.OPT_INT8_SCHEME,
+                 "int8_scheme": nat.OPT_INT8_SCHEME, "tune_int8_tile": nat.OPT_TUNE_INT8_TILE,
                  "precond_bf16": nat.OPT_PRECOND_BF16}
         if name not in codes:
             raise ValueError(f"unknown option {name!r}")

@@ -170,12 +170,19 @@ const char *dmb_version(void);
  * true residuals, the exact Krylov operator) is made of exact int8
  * tensor-core products.  0 (default): residues modulo 13 pairwise coprime
  * moduli <= 256 of Z and X scaled to 44-bit integers, one int8 product per
- * modulus, recombined by the Chinese remainder theorem as a 64-bit fixed-point
+ * modulus, recombined by the Chinese remainder theorem as a 96-bit fixed-point
  * fraction of the moduli's product (13 products, 12 for the Krylov operator).
  * 1: seven-bit fixed-point slices, products of slice pairs up to a level
  * (26 products, 21 for the Krylov operator).  Both are deterministic and
  * agree with the FP64 product to ~1e-12 normwise. */
 #define DMB_OPT_INT8_SCHEME 13
+/* DMB_OPT_TUNE_INT8_TILE: pin the tile shape of the residue-scheme int8
+ * product (0, the default, lets the online autotuner choose per shape
+ * bucket): 1: one SM per 64 x 256 complex output tile (M 128 int8 MMA);
+ * 2: a CTA pair (two SMs of a cluster, tcgen05 cta_group::2, M 256 MMA) per
+ * 128 x 256 complex tile, each SM loading half of the right-hand operand.
+ * Both give the same bits. */
+#define DMB_OPT_TUNE_INT8_TILE 14
 dmb_status dmb_set_option(dmb_ctx *ctx, int option, int value);
 /* The far-pair RWG tile width used by the last assembly on this context. */
 dmb_status dmb_get_far_tile(dmb_ctx *ctx, int *width_out);

@@ -80,6 +80,28 @@ def test_int8_product_with_split_tail_tiles(scheme, tol):
     dev.close()
 
 
+def test_int8_tile_candidates_identical():
+    """The residue-scheme int8 product on one-SM 64 x 256 complex tiles and on
+    CTA-pair 128 x 256 tiles (a two-CTA cluster, tcgen05 cta_group::2) writes
+    the same bits: whole tiles, a stream-K tail of pair tiles (600 columns),
+    four column tiles per row (1,024) and a single ragged one (100)."""
+    dev = _plate(40, side=0.3)  # 4,720 RWG: 37 pair rows of tiles, ragged last
+    dev.assemble(K3, precision="mixed")
+    dev.set_option("tc_min_rhs", 1 << 30)
+    for R in (600, 1024, 100):
+        X = _rand(dev.N, R, 11 + R)
+        out = {}
+        for pin in (1, 2, 0):
+            dev.set_option("tune_int8_tile", pin)
+            out[pin] = dev.matvec(X)
+        assert np.array_equal(out[1], out[2]), R
+        assert np.array_equal(out[1], out[0]), R
+    dev.set_option("tune_int8_tile", 0)
+    with pytest.raises(Exception):
+        dev.set_option("tune_int8_tile", 3)
+    dev.close()
+
+
 def test_int8_residue_scheme_krylov_class():
     # the Krylov operator of the many-RHS solves uses 12 moduli (fewer bits
     # for X, ~1e-11 normwise): right-preconditioned block GMRES with either
