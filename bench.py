@@ -303,6 +303,8 @@ def run_ours(args):
     assert count == R_WAVES and start % R_WAVES == 0
     kv, e0, pol = waves(R_WAVES, seed=SEED + start // R_WAVES)
     dev = EFIEDevice(mesh, rwg, device=local)
+    if args.int8_tile:
+        dev.set_option("tune_int8_tile", args.int8_tile)
     sig = np.empty(R_WAVES)
 
     def c3_step(precision, precond, cutoff, side=1):
@@ -918,6 +920,8 @@ def main():
     ap.add_argument("--plate-cells", type=int, default=60,
                     help="profiling case: plate of this many cells per side (same cell size)")
     ap.add_argument("--waves", type=int, default=1024, help="profiling case: number of incidences")
+    ap.add_argument("--int8-tile", type=int, default=0, choices=[0, 1, 2],
+                    help="profiling: pin the int8 product's tile on the headline device (1: one SM, 2: CTA pair)")
     ap.add_argument("--assembly-case", action="store_true",
                     help="profiling case: assemble the 7,680-RWG sphere once in FP64 (tile width 32) and once "
                          "in mixed precision (tile width 64), print the times and exit")
