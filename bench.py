@@ -13,7 +13,7 @@ second (mixed: complex64 Z with FP32 far pairs and FP64 singular terms,
 block GMRES preconditioned by the complex64 LDL^T of Z -- tensor-core updates
 and sweeps on BF16 hi + lo operand pieces -- with FP64-accurate Krylov
 products from int8 residues modulo 13 moduli (Chinese-remainder
-recombination), FP64 Arnoldi and the FP64 residual as the judge).
+recombination), FP64 Arnoldi and the FP64 residual as the criterion).
 
 Variants reported beside it (same timing rules, fewer steps where slow):
   c3_mixed_tf32_refined  the headline with the Krylov product in 3xTF32 and

@@ -161,7 +161,7 @@ dmb_status dmb_set_option(dmb_ctx *c, int option, int value) {
       return;
     }
     if (option == DMB_OPT_TRUE_RESIDUAL) {
-      c->true_residual_judge = value != 0;
+      c->true_residual_check = value != 0;
       return;
     }
     if (option == DMB_OPT_SPIN_LIMIT) {

@@ -329,16 +329,16 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   int total_iters = 0, restarts = 0, cycles = 0, j_last = 0;
   bool first = true, have_true = false;
   std::vector<SysState> hst(R);
-  // judge passes: per system, the factor by which the next cycle must reduce
+  // check passes: per system, the factor by which the next cycle must reduce
   // its starting (preconditioned, for left) residual; 0 = keep the threshold
-  std::vector<double> judge_scale(R, 0.0);
-  // left preconditioning without an inexact operator: the judge continues the
+  std::vector<double> recheck_scale(R, 0.0);
+  // left preconditioning without an inexact operator: the check continues the
   // cycle instead of restarting it
-  const bool left_judge = c->true_residual_judge && precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_LEFT &&
-                          !inexact;
-  int judge_continuations = 0;
+  const bool left_recheck = c->true_residual_check && precond_kind != DMB_PRECOND_NONE && side == DMB_SIDE_LEFT &&
+                            !inexact;
+  int recheck_continuations = 0;
   std::vector<double> hn_final(2 * R);
-  for (int judge_pass = 0;; judge_pass++) {
+  for (int check_pass = 0;; check_pass++) {
   while (true) {
     // r0 = b - Z x (x = 0 on the first cycle), preconditioned on the left
     if (first) {
@@ -364,9 +364,9 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
         hst[r].kx = 0;
         hst[r].resid = hn[r];
         hst[r].resid_x = hn[r];
-        if (judge_scale[r] > 0) {
-          hst[r].eps = hn[r] * judge_scale[r];
-          judge_scale[r] = 0;
+        if (recheck_scale[r] > 0) {
+          hst[r].eps = hn[r] * recheck_scale[r];
+          recheck_scale[r] = 0;
         }
         if (inexact && hst[r].done == 1 && !(hn[r] <= hst[r].eps)) hst[r].done = 0;
         if (!hst[r].done) {
@@ -471,11 +471,11 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       DMB_CUDA(cudaMemcpyAsync(&h_active, active, 4, cudaMemcpyDeviceToHost, c->stream));
       DMB_CUDA(cudaStreamSynchronize(c->stream));
       // Left preconditioning stops on the preconditioned residual.  With the
-      // judge on, the trial solution of this cycle is checked against the
+      // check on, the trial solution of this cycle is checked against the
       // unpreconditioned FP64 residual; a system that fails it continues the
       // same Arnoldi process (its Krylov space kept) with its threshold
       // lowered by the factor the true residual still needs, margin 2.
-      while (h_active == 0 && left_judge) {
+      while (h_active == 0 && left_recheck) {
         DMB_LAUNCH(c, k_backsolve, blocks_for(R, 128), 128, 0, R, kcap, H, g, st, ybuf);
         DMB_CUDA(cudaMemcpyAsync(tmp, x, vec_bytes, cudaMemcpyDeviceToDevice, c->stream));
         DMB_LAUNCH(c, k_combine, blocks_for(N * R, 256), 256, 0, N, R, j, vstride, V, ybuf, kcap, tmp);
@@ -507,7 +507,7 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
           changed = true;
         }
         if (!changed) break;
-        judge_continuations++;
+        recheck_continuations++;
         DMB_CUDA(cudaMemcpyAsync(st, hst.data(), sizeof(SysState) * R, cudaMemcpyHostToDevice, c->stream));
       }
       if (h_active == 0) break;
@@ -553,23 +553,23 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
   DMB_LAUNCH(c, k_norms, (unsigned)R, 256, 0, N, b, nrm + R);
   DMB_CUDA(cudaMemcpyAsync(hn_final.data(), nrm + R, 16 * R, cudaMemcpyDeviceToHost, c->stream));
   DMB_CUDA(cudaStreamSynchronize(c->stream));
-  // The judge: a system that stopped on its recurrence estimate (or on the
+  // The true-residual check: a system that stopped on its recurrence estimate (or on the
   // preconditioned residual, for left preconditioning) with a true residual
   // above tol is refined by another cycle from its current x; that cycle must
   // reduce its starting residual by the factor the true residual still needs
   // (with a margin of 2).
-  if (!c->true_residual_judge || total_iters >= maxiter || judge_pass >= 16) break;
+  if (!c->true_residual_check || total_iters >= maxiter || check_pass >= 16) break;
   bool refine = false;
   for (int64_t r = 0; r < R; r++) {
     const double bn = hn_final[r], rn = hn_final[R + r];
     if (!(bn > 0) || !std::isfinite(rn) || rn <= tol * bn || hst[r].done == 3) continue;
     hst[r].done = 0;
-    judge_scale[r] = std::min(0.5, 0.5 * tol * bn / rn);
+    recheck_scale[r] = std::min(0.5, 0.5 * tol * bn / rn);
     refine = true;
   }
   if (!refine) break;
   have_true = false;
-  }  // judge passes
+  }  // check passes
   const std::vector<double> &hn = hn_final;
   double tres = 0, eres = 0;
   bool solved = true;
@@ -585,14 +585,14 @@ void gmres_dev(dmb_ctx *c, const double *b_dev, double *x_dev, int64_t R, double
       eres = std::max(eres, est);
     }
     if (!std::isfinite(rel)) solved = false;
-    if (c->true_residual_judge && !(rel <= tol)) solved = false;
+    if (c->true_residual_check && !(rel <= tol)) solved = false;
   }
   out->niter = iters_used;
   out->solved = solved ? 1 : 0;
   out->residual = eres;
   out->true_residual = tres;
   out->restarts = restarts;
-  out->reserved = judge_continuations;
+  out->reserved = recheck_continuations;
   c->tm.solve_ms = now_ms() - t0;
   c->tm.gmres_ms = c->tm.solve_ms;
 }

@@ -259,10 +259,10 @@ struct dmb_ctx {
   // (few right-hand sides); key: iteration range, shape, buffer addresses and
   // the allocation epoch
   bool gmres_graphs = true;
-  // GMRES judges convergence on ||b - Z x|| / ||b|| (FP64-accurate product):
+  // GMRES tests convergence on ||b - Z x|| / ||b|| (FP64-accurate product):
   // a system whose recurrence estimate met the tolerance but whose true
   // residual did not is refined by further cycles from its current iterate
-  bool true_residual_judge = true;
+  bool true_residual_check = true;
   // polls of a triangular-solve chain wait before it gives up (DMB_ERR_TIMEOUT);
   // DMB_OPT_SPIN_LIMIT lowers it to exercise the timeout path
   long long spin_limit = 20000000;
@@ -276,7 +276,7 @@ struct dmb_ctx {
   // those operands split into BF16 pieces (kind::f16 MMA) instead of TF32:
   // 1 always, 0 never, -1 (default) inside the resident solves only
   // (dmb_solve_resident[_many], batch surfaces: pc_bf16_scope set), whose
-  // GMRES is judged on the FP64 residual, so the preconditioner's precision is
+  // GMRES is checked on the FP64 residual, so the preconditioner's precision is
   // a matter of iteration count alone
   int precond_bf16 = -1;
   int int8_scheme = 0;  // FP64-accurate INT8 product: 0 residues modulo coprime moduli (CRT), 1 fixed-point slices

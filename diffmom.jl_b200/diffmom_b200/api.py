@@ -916,7 +916,7 @@ def solve_scattering(mesh: TriMesh, freq_hz, excitation, method: str = "auto",
     from its dense blocks).  precision "fp64" is the plain path; "mixed"
     assembles far pairs in FP32 (complex64 Z) and factors the preconditioner
     in FP32 while GMRES keeps FP64 Arnoldi and residuals (for aca_gmres only
-    the preconditioner is complex64).  GMRES judges convergence on the
+    the preconditioner is complex64).  GMRES tests convergence on the
     unpreconditioned FP64 residual (refining a left-preconditioned solve until
     it passes).
 

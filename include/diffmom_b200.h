@@ -65,7 +65,7 @@ typedef struct {
   double residual;      /* last residual estimate (max over RHS), relative */
   double true_residual; /* ||b - Z x|| / ||b|| in FP64 (max over RHS) */
   int32_t restarts;     /* restart / refinement cycles */
-  int32_t reserved;     /* times the true-residual judge continued a left-
+  int32_t reserved;     /* times the true-residual check continued a left-
                            preconditioned cycle (DMB_OPT_TRUE_RESIDUAL) */
 } dmb_gmres_stats;
 
@@ -129,7 +129,7 @@ const char *dmb_version(void);
  * assembly selects its own; switching drops the preconditioner). */
 #define DMB_OPT_OPERATOR 7
 /* DMB_OPT_TRUE_RESIDUAL: 1 (default) makes the unpreconditioned FP64 residual
- * ||b - Z x|| / ||b|| the judge of dmb_gmres / dmb_gmres_adjoint and the
+ * ||b - Z x|| / ||b|| the convergence test of dmb_gmres / dmb_gmres_adjoint and the
  * resident solves.  For left preconditioning (Krylov.gmres stops on the
  * preconditioned residual, IterativeSolve.jl:364-384) the trial solution is
  * checked when a system's estimate meets the tolerance, and a system whose
@@ -162,7 +162,7 @@ const char *dmb_version(void);
  * products on the kind::f16 tensor-core path at twice the TF32 rate, FP32
  * accumulation) instead of TF32 pieces (~21 bits).  1: always; 0: never; -1
  * (default): inside the resident solves only (dmb_solve_resident,
- * dmb_solve_resident_many, dmb_batch_solve), whose GMRES is judged on the FP64
+ * dmb_solve_resident_many, dmb_batch_solve), whose GMRES is checked on the FP64
  * residual, so the preconditioner's precision changes the iteration count,
  * not the result; dmb_nf_build / dmb_nf_apply / dmb_gmres keep TF32 pieces. */
 #define DMB_OPT_PRECOND_BF16 12

@@ -194,7 +194,7 @@ def test_forward_and_adjoint_solves():
     assert 0 < P.nnz_ratio < 1
     # with these small leaves the near-field preconditioner is weak: Krylov.gmres
     # semantics stop after ~290 iterations at a preconditioned residual of 1e-8
-    # (true residual ~1e-7); the FP64 true-residual judge continues to ~310
+    # (true residual ~1e-7); the FP64 true-residual criterion continues to ~310
     I, st = solve_gmres(A, v, preconditioner=P, tol=1e-8, maxiter=400)
     assert st.true_residual <= 1e-8
     I_ref = np.linalg.solve(Z, v)
@@ -204,7 +204,7 @@ def test_forward_and_adjoint_solves():
     lam, st_a = solve_gmres_adjoint(A, rhs_adj, preconditioner=P, tol=1e-8, maxiter=400)
     lam_ref = np.linalg.solve(Z.conj().T, rhs_adj)
     err_a = np.linalg.norm(lam - lam_ref) / np.linalg.norm(lam_ref)
-    # residual of the adjoint system on A^H itself: the judge holds it to 1e-8
+    # residual of the adjoint system on A^H itself: the criterion holds it to 1e-8
     res_a = np.linalg.norm(A.matvec(lam, 1) - rhs_adj) / np.linalg.norm(rhs_adj)
     print(f"forward: {st.niter} iterations, error vs direct {err:.2e}; adjoint: {st_a.niter} iterations, "
           f"error {err_a:.2e}, ||A^H lam - b|| / ||b|| {res_a:.2e}")

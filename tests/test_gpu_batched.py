@@ -105,7 +105,7 @@ def test_int8_tile_candidates_identical():
 def test_int8_residue_scheme_krylov_class():
     # the Krylov operator of the many-RHS solves uses 12 moduli (fewer bits
     # for X, ~1e-11 normwise): right-preconditioned block GMRES with either
-    # scheme meets the FP64 judge in the same number of iterations, and the
+    # scheme meets the FP64 criterion in the same number of iterations, and the
     # true residual formed from the stored products (13 moduli) matches an
     # explicit b - Z x
     dev = _plate(30)
@@ -208,7 +208,7 @@ def test_block_gmres_many_plane_waves(side, exact):
           f"true residual "
           f"{st.true_residual:.2e}, max current error vs FP64 {err.max():.2e}")
     assert st.solved
-    # the unpreconditioned FP64 residual is the judge on either side: a left-
+    # the unpreconditioned FP64 residual is the criterion on either side: a left-
     # preconditioned system that stopped on its preconditioned residual is
     # refined until ||b - Z x|| / ||b|| <= 1e-6
     assert st.true_residual <= 1e-6
@@ -352,7 +352,7 @@ def test_bf16_preconditioner_operands():
     """BF16 operand pieces (hi + lo, kind::f16 tensor cores) for the complex64
     factor updates and packed sweeps: the preconditioner apply stays within
     1e-3 of the TF32-piece one, and block GMRES with it still meets the FP64
-    residual (the judge) with the same solution."""
+    residual (the criterion) with the same solution."""
     dev = _plate(36)  # 3,960 RWG: four 1,024-row sweep blocks, ragged last
     dev.set_option("precond_bf16", 0)
     dev.assemble(K3, precision="mixed")

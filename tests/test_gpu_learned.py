@@ -2,7 +2,7 @@
 training kernels against a torch-CPU autograd restatement of the same network,
 checkpoint round trip, and the ablation that shows what the trained network
 gains over the plain local-inverse rows (with the near-field LDL^T and no
-preconditioner beside it).  The FP64 true residual is the judge."""
+preconditioner beside it).  The FP64 true residual is the criterion."""
 import math
 
 import numpy as np
@@ -107,7 +107,7 @@ def test_learned_preconditioner_ablation():
     (trained on the GPU over 48 generated perturbed ellipsoids, seeds
     1000-1047) against the plain ring step (the learned step with the network
     switched off), the exact local inverse, the near-field LDL^T and no
-    preconditioner; GMRES to 1e-6 judged on the FP64 residual."""
+    preconditioner; GMRES to 1e-6 checked on the FP64 residual."""
     from diffmom_b200.learned import DEFAULT_WEIGHTS
     lam = C0 / 3e9
     k = 2 * math.pi / lam

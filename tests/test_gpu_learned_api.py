@@ -1,7 +1,7 @@
 """solve_scattering with the learned right preconditioner (the library's
 default weights, trained over generated bodies by diffmom_b200.learned) and
 its near-field LU fallback, against the near-field LU path on the same body.
-The unpreconditioned FP64 residual is the judge of every solve."""
+The unpreconditioned FP64 residual is the criterion of every solve."""
 import math
 
 import numpy as np

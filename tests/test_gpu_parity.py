@@ -264,7 +264,7 @@ def test_gmres_nearfield_vs_direct(sphere2, side):
     v = c.plane_wave_rhs([0, 0, -k], 1.0, [1, 0, 0])
     Io = np.linalg.solve(Zo, v)
     P = dev.build_nearfield(0.25 * 2 * math.pi / k, "lu")
-    # Krylov.gmres stopping semantics (the judge off): iteration count against
+    # Krylov.gmres stopping semantics (that criterion off): iteration count against
     # the oracle's restatement
     dev.set_option("true_residual", 0)
     I, st = dev.gmres(v, tol=1e-8, maxiter=200, preconditioner=P, precond_side=side)
@@ -275,7 +275,7 @@ def test_gmres_nearfield_vs_direct(sphere2, side):
     Znf = orc.nearfield_matrix(Zo, rwg_centers(m, r), 0.25 * 2 * math.pi / k)
     xo, it_o, ok = orc.gmres(Zo, v, M=np.linalg.inv(Znf), side=side, rtol=1e-8, itmax=200)
     assert ok and abs(st.niter - it_o) <= 2
-    # default: the unpreconditioned FP64 residual is the judge -- a left-
+    # default: the unpreconditioned FP64 residual is the criterion -- a left-
     # preconditioned solve is refined until ||b - Z x|| / ||b|| <= tol
     I2, st2 = dev.gmres(v, tol=1e-8, maxiter=200, preconditioner=P, precond_side=side)
     I2 = I2.reshape(-1)
